@@ -1,0 +1,1896 @@
+/*
+ * CPU oracle: C restatement of Hydra's doubly periodic QG "caps" time step.
+ * TEST INFRASTRUCTURE ONLY (the checker and the timed CPU baseline); the
+ * product never links it.  See casl_oracle.h for scope and the parity note
+ * ("parity unpinned": no reference outputs can be produced on this machine).
+ *
+ * Conventions used throughout:
+ *   - Physical arrays are Fortran (ny,nx): element (iy,ix) at [(ix-1)*ny+iy-1].
+ *   - Spectral arrays are Fortran (nx,ny): element (kx,ky) at [(ky-1)*nx+kx-1].
+ *   - Contour arrays are 1-based: xq[1..nptq], nextq values in 1..nptq.
+ *   - Built with -ffp-contract=off: every a*b+c rounds twice, as gfortran
+ *     does on x86-64 without -march flags.
+ */
+#include "casl_oracle.h"
+
+#include <math.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define PI_D 3.141592653589793238462643383279502884197169399375105820974944592307816
+#define ZERO 0.0
+#define ONE 1.0
+#define TWO 2.0
+#define F12 0.5
+#define F13 (1.0 / 3.0)
+#define F14 0.25
+#define F16 (1.0 / 6.0)
+
+/* Fortran intrinsics with their exact semantics. */
+static inline double f_dint(double x) { return (double)(long long)x; } /* dble(int(x)) */
+static inline int f_int(double x) { return (int)x; }                  /* int(): truncation */
+static inline int f_nint(double x) { return (int)lround(x); }         /* nint(): half away */
+static inline double f_sign1(double b) { return copysign(1.0, b); }   /* sign(one,b) */
+static inline int f_isign1(int b) { return b >= 0 ? 1 : -1; }         /* sign(1,b) */
+
+/* Integer power correctly rounded, as gfortran folds x**k in PARAMETERs. */
+static double pow_cr(double x, int k) {
+#ifdef __SIZEOF_FLOAT128__
+  __float128 r = 1, b = x;
+  for (int i = 0; i < k; i++) r *= b;
+  return (double)r;
+#else
+  long double r = 1;
+  for (int i = 0; i < k; i++) r *= x;
+  return (double)r;
+#endif
+}
+
+typedef struct {
+  int n, h;
+  double *cwr, *cwi;  /* e^{-2 pi i k / h}, k < h/2 */
+  double *twr, *twi;  /* e^{-2 pi i k / n}, k <= h */
+  double *re, *im;    /* scratch of length h */
+} fftplan;
+
+struct o_state {
+  o_params p;
+  int nx, ny, nxf, nyf, nxu, nyu, nwx, nwy;
+  /* constants.f90 / contours.f90 parameters */
+  double pi, twopi, small, small3, oms, hlx, hlxi, xmin, xmax, hly, hlyi, ymin, ymax;
+  double kdsq, srwfm, therm, domarea, aspect, glx, glxi, gly, glyi, garea, dsumi;
+  double glxf, glxfi, glyf, glyfi, glxu, glxui, glyu, glyui;
+  double amu, ell, dm, dm2, d4small, dmsq, dmi, elf, densf;
+  int beffect, btropic, heating, friction;
+  /* grids */
+  double *xgf, *ygf, *xgu, *ygu;
+  int *ixp, *iyp, *ibx, *iby;
+  double w00[16 * 16], w10[16 * 16], w01[16 * 16], w11[16 * 16];
+  int *ixfw, *ix0w, *ix1w, *iyfw, *iy0w, *iy1w;
+  /* spectral tables */
+  double *rkx, *hrkx, *rky, *hrky, *bety;
+  double *rksq, *qdiss, *green, *flo, *fhi, *rk;
+  fftplan px, py;
+  double *fwork;
+  /* contours */
+  double *xq, *yq, qjump;
+  int *nextq, *indq, *npq, *i1q, *i2q;
+  int nq, nptq;
+  /* fields */
+  double *qr, *qs, *uu, *vv, *pp, *qq, *qc, *qd, *qspre, *emq, *epq;
+  /* time stepping */
+  double t, dt, dt2, dt3, dt6, twist, dtmax, tinit;
+  int ireg, contex;
+  double zzrms, zzmax, uumax;
+};
+
+#define PHY(s, iy, ix) ((size_t)((ix)-1) * (size_t)(s)->ny + (size_t)((iy)-1))
+#define SPC(s, kx, ky) ((size_t)((ky)-1) * (size_t)(s)->nx + (size_t)((kx)-1))
+
+static void *xcalloc(size_t n, size_t sz) {
+  void *p = calloc(n ? n : 1, sz);
+  if (!p) {
+    fprintf(stderr, "casl_oracle: out of memory (%zu x %zu)\n", n, sz);
+    abort();
+  }
+  return p;
+}
+
+/* ======================================================================
+ * FFT.  Restates the transform of stafft.f90 forfft/revfft (lines 187-406):
+ *   forward  X(k+1)   =  Re F(k) / sqrt(n),  k = 0..n/2
+ *            X(n+1-k) =  Im F(k) / sqrt(n),  k = 1..n/2-1,
+ *            F(k) = sum_j x_j exp(-2 pi i j k / n)         ("Hermitian form",
+ *            stafft.f90:55-58; normalisation stafft.f90:275)
+ *   reverse  its exact inverse (sine sign flip, DC/Nyquist halving and
+ *            2/sqrt(n) of stafft.f90:311-324,394).
+ * Computed by a half-length complex radix-2 FFT (n a power of two).
+ * ====================================================================== */
+static int is_pow2(int n) { return n >= 4 && (n & (n - 1)) == 0; }
+
+static void plan_init(fftplan *pl, int n) {
+  pl->n = n;
+  pl->h = n / 2;
+  int h = pl->h;
+  pl->cwr = xcalloc(h, sizeof(double));
+  pl->cwi = xcalloc(h, sizeof(double));
+  pl->twr = xcalloc(h + 1, sizeof(double));
+  pl->twi = xcalloc(h + 1, sizeof(double));
+  pl->re = xcalloc(h, sizeof(double));
+  pl->im = xcalloc(h, sizeof(double));
+  const double twopi = 2.0 * PI_D;
+  for (int k = 0; k < h; k++) {
+    double a = twopi * (double)k / (double)h;
+    pl->cwr[k] = cos(a);
+    pl->cwi[k] = -sin(a);
+  }
+  for (int k = 0; k <= h; k++) {
+    double a = twopi * (double)k / (double)n;
+    pl->twr[k] = cos(a);
+    pl->twi[k] = -sin(a);
+  }
+}
+
+static void plan_free(fftplan *pl) {
+  free(pl->cwr); free(pl->cwi); free(pl->twr); free(pl->twi); free(pl->re); free(pl->im);
+}
+
+/* In-place complex FFT of length h; dir=-1 forward (e^{-i}), +1 backward, no scaling. */
+static void cfft(const fftplan *pl, double *re, double *im, int dir) {
+  int h = pl->h;
+  for (int i = 1, j = 0; i < h; i++) {
+    int bit = h >> 1;
+    for (; j & bit; bit >>= 1) j ^= bit;
+    j ^= bit;
+    if (i < j) {
+      double t = re[i]; re[i] = re[j]; re[j] = t;
+      t = im[i]; im[i] = im[j]; im[j] = t;
+    }
+  }
+  for (int len = 2; len <= h; len <<= 1) {
+    int half = len >> 1, step = h / len;
+    for (int i = 0; i < h; i += len) {
+      for (int k = 0; k < half; k++) {
+        double wr = pl->cwr[k * step];
+        double wi = dir < 0 ? pl->cwi[k * step] : -pl->cwi[k * step];
+        int a = i + k, b = i + k + half;
+        double tr = wr * re[b] - wi * im[b];
+        double ti = wr * im[b] + wi * re[b];
+        re[b] = re[a] - tr; im[b] = im[a] - ti;
+        re[a] = re[a] + tr; im[a] = im[a] + ti;
+      }
+    }
+  }
+}
+
+/* One forward real transform: in[j*st], out[k*st] in Hermitian form. */
+static void rfft_one(const fftplan *pl, const double *in, double *out, size_t st) {
+  int n = pl->n, h = pl->h;
+  double *re = pl->re, *im = pl->im;
+  for (int j = 0; j < h; j++) {
+    re[j] = in[(size_t)(2 * j) * st];
+    im[j] = in[(size_t)(2 * j + 1) * st];
+  }
+  cfft(pl, re, im, -1);
+  double normfac = 1.0 / sqrt((double)n);
+  /* k = 0 and k = h */
+  double f0 = re[0] + im[0], fh = re[0] - im[0];
+  double xr[2] = {f0, fh};
+  out[0] = xr[0] * normfac;
+  out[(size_t)h * st] = xr[1] * normfac;
+  for (int k = 1; k < h; k++) {
+    double zr = re[k], zi = im[k], cr = re[h - k], ci = -im[h - k]; /* conj Z(h-k) */
+    double er = 0.5 * (zr + cr), ei = 0.5 * (zi + ci);
+    double dr = zr - cr, di = zi - ci;                /* 2 i O e... */
+    /* O = (Z - conj Z(h-k)) / (2 i) */
+    double orr = 0.5 * di, oi = -0.5 * dr;
+    double wr = pl->twr[k], wi = pl->twi[k];
+    double fr = er + (wr * orr - wi * oi);
+    double fi = ei + (wr * oi + wi * orr);
+    out[(size_t)k * st] = fr * normfac;
+    out[(size_t)(n - k) * st] = fi * normfac;
+  }
+}
+
+/* One reverse real transform: Hermitian in[k*st] -> out[j*st]. */
+static void irfft_one(const fftplan *pl, const double *in, double *out, size_t st) {
+  int n = pl->n, h = pl->h;
+  double *re = pl->re, *im = pl->im;
+  /* F(k) = X(k) + i X(n-k); F(0), F(h) real. */
+  {
+    double F0 = in[0], Fh = in[(size_t)h * st];
+    re[0] = 0.5 * (F0 + Fh);
+    im[0] = 0.5 * (F0 - Fh);
+  }
+  for (int k = 1; k < h; k++) {
+    double fr = in[(size_t)k * st], fi = in[(size_t)(n - k) * st];
+    double gr = in[(size_t)(h - k) * st], gi = -in[(size_t)(n - (h - k)) * st]; /* conj F(h-k) */
+    double er = 0.5 * (fr + gr), ei = 0.5 * (fi + gi);
+    double dr = 0.5 * (fr - gr), di = 0.5 * (fi - gi);
+    /* O = (F - conj F(h-k)) e^{+2 pi i k/n} / 2 */
+    double wr = pl->twr[k], wi = -pl->twi[k];
+    double orr = dr * wr - di * wi, oi = dr * wi + di * wr;
+    /* Z = E + i O */
+    re[k] = er - oi;
+    im[k] = ei + orr;
+  }
+  cfft(pl, re, im, +1);
+  double normfac = 2.0 / sqrt((double)n);
+  for (int j = 0; j < h; j++) {
+    out[(size_t)(2 * j) * st] = re[j] * normfac;
+    out[(size_t)(2 * j + 1) * st] = im[j] * normfac;
+  }
+}
+
+static void forfft_plan(const fftplan *pl, int m, double *x, double *tmp) {
+  int n = pl->n;
+  double *buf = tmp + n;
+  for (int i = 0; i < m; i++) {
+    for (int k = 0; k < n; k++) buf[k] = x[i + (size_t)m * k];
+    rfft_one(pl, buf, tmp, 1);
+    for (int k = 0; k < n; k++) x[i + (size_t)m * k] = tmp[k];
+  }
+}
+
+static void revfft_plan(const fftplan *pl, int m, double *x, double *tmp) {
+  int n = pl->n;
+  double *buf = tmp + n;
+  for (int i = 0; i < m; i++) {
+    for (int k = 0; k < n; k++) buf[k] = x[i + (size_t)m * k];
+    irfft_one(pl, buf, tmp, 1);
+    for (int k = 0; k < n; k++) x[i + (size_t)m * k] = tmp[k];
+  }
+}
+
+/* Stand-alone versions (a temporary plan per call). */
+void o_forfft(int m, int n, double *x) {
+  if (!is_pow2(n)) return;
+  fftplan pl;
+  plan_init(&pl, n);
+  double *tmp = xcalloc(2 * (size_t)n, sizeof(double));
+  forfft_plan(&pl, m, x, tmp);
+  free(tmp);
+  plan_free(&pl);
+}
+
+void o_revfft(int m, int n, double *x) {
+  if (!is_pow2(n)) return;
+  fftplan pl;
+  plan_init(&pl, n);
+  double *tmp = xcalloc(2 * (size_t)n, sizeof(double));
+  revfft_plan(&pl, m, x, tmp);
+  free(tmp);
+  plan_free(&pl);
+}
+
+/* ptospc (sta2dfft.f90:103-132): x-transform, transpose, y-transform. */
+void o_ptospc(o_state *s, double *rvar, double *svar) {
+  int nx = s->nx, ny = s->ny;
+  forfft_plan(&s->px, ny, rvar, s->fwork);
+  for (int kx = 1; kx <= nx; kx++)
+    for (int iy = 1; iy <= ny; iy++) svar[SPC(s, kx, iy)] = rvar[PHY(s, iy, kx)];
+  forfft_plan(&s->py, nx, svar, s->fwork);
+}
+
+/* spctop (sta2dfft.f90:136-165). */
+void o_spctop(o_state *s, double *svar, double *rvar) {
+  int nx = s->nx, ny = s->ny;
+  revfft_plan(&s->py, nx, svar, s->fwork);
+  for (int kx = 1; kx <= nx; kx++)
+    for (int iy = 1; iy <= ny; iy++) rvar[PHY(s, iy, kx)] = svar[SPC(s, kx, iy)];
+  revfft_plan(&s->px, ny, rvar, s->fwork);
+}
+
+/* xderiv (sta2dfft.f90:169-203). */
+static void xderiv(o_state *s, const double *rkx, const double *var, double *der) {
+  int nx = s->nx, ny = s->ny, nwx = nx / 2, nxp2 = nx + 2;
+  for (int ky = 1; ky <= ny; ky++) {
+    der[SPC(s, 1, ky)] = 0.0;
+    for (int kx = 2; kx <= nx - nwx; kx++) {
+      int dkx = 2 * (kx - 1), kxc = nxp2 - kx;
+      der[SPC(s, kx, ky)] = -rkx[dkx - 1] * var[SPC(s, kxc, ky)];
+      der[SPC(s, kxc, ky)] = rkx[dkx - 1] * var[SPC(s, kx, ky)];
+    }
+  }
+  if (nx % 2 == 0) {
+    int kxc = nwx + 1;
+    for (int ky = 1; ky <= ny; ky++) der[SPC(s, kxc, ky)] = 0.0;
+  }
+}
+
+/* yderiv (sta2dfft.f90:207-245). */
+static void yderiv(o_state *s, const double *rky, const double *var, double *der) {
+  int nx = s->nx, ny = s->ny, nwy = ny / 2, nyp2 = ny + 2;
+  for (int kx = 1; kx <= nx; kx++) der[SPC(s, kx, 1)] = 0.0;
+  for (int ky = 2; ky <= ny - nwy; ky++) {
+    int kyc = nyp2 - ky;
+    double fac = rky[2 * (ky - 1) - 1];
+    for (int kx = 1; kx <= nx; kx++) {
+      der[SPC(s, kx, ky)] = -fac * var[SPC(s, kx, kyc)];
+      der[SPC(s, kx, kyc)] = fac * var[SPC(s, kx, ky)];
+    }
+  }
+  if (ny % 2 == 0) {
+    int kyc = nwy + 1;
+    for (int kx = 1; kx <= nx; kx++) der[SPC(s, kx, kyc)] = 0.0;
+  }
+}
+
+/* ======================================================================
+ * Set-up: constants.f90, contours.f90:38-132, spectral.f90:42-158.
+ * ====================================================================== */
+static void init_constants(o_state *s) {
+  const o_params *p = &s->p;
+  s->pi = PI_D;
+  s->twopi = 2.0 * s->pi;
+  s->small = 1.0e-12;
+  s->small3 = s->small * s->small * s->small;
+  s->oms = ONE - s->small;
+  s->hlx = F12 * p->ellx; s->hlxi = ONE / s->hlx; s->xmin = -s->hlx; s->xmax = s->hlx;
+  s->hly = F12 * p->elly; s->hlyi = ONE / s->hly; s->ymin = -s->hly; s->ymax = s->hly;
+  s->kdsq = pow_cr(p->kd, 2);
+  s->srwfm = p->beta * p->kd / (ONE + s->kdsq);
+  s->therm = p->rtherm * s->kdsq;
+  s->domarea = p->ellx * p->elly;
+  s->aspect = p->ellx / p->elly;
+  s->glx = p->ellx / (double)s->nx; s->glxi = (double)s->nx / p->ellx;
+  s->gly = p->elly / (double)s->ny; s->glyi = (double)s->ny / p->elly;
+  s->garea = s->glx * s->gly;
+  s->dsumi = ONE / (double)(s->nx * s->ny);
+  s->glxf = p->ellx / (double)s->nxf; s->glxfi = (double)s->nxf / p->ellx;
+  s->glyf = p->elly / (double)s->nyf; s->glyfi = (double)s->nyf / p->elly;
+  s->glxu = p->ellx / (double)s->nxu; s->glxui = (double)s->nxu / p->ellx;
+  s->glyu = p->elly / (double)s->nyu; s->glyui = (double)s->nyu / p->elly;
+  s->amu = 0.2;
+  s->ell = 6.25 * s->glx;
+  s->dm = pow_cr(s->amu, 2) * s->ell / 4.0;
+  s->dm2 = pow_cr(s->dm, 2);
+  s->d4small = s->small * pow_cr(s->glx, 4);
+  s->dmsq = 4.0 * s->dm2;
+  s->dmi = TWO / s->dm;
+  s->elf = ONE / pow_cr(s->ell, 2);
+  s->densf = ONE / (s->amu * sqrt(s->ell));
+  s->beffect = p->beta != 0.0;
+  s->btropic = p->kd == 0.0;
+  s->heating = p->rtherm > 0.0;
+  s->friction = p->rekman > 0.0;
+}
+
+static void init_contours(o_state *s) {
+  int nx = s->nx, ny = s->ny;
+  s->ixp = xcalloc(nx + 1, sizeof(int));
+  s->iyp = xcalloc(ny + 1, sizeof(int));
+  for (int ix = 1; ix <= nx - 1; ix++) s->ixp[ix] = ix + 1;
+  s->ixp[nx] = 1;
+  for (int iy = 1; iy <= ny - 1; iy++) s->iyp[iy] = iy + 1;
+  s->iyp[ny] = 1;
+  s->xgf = xcalloc(s->nxf + 1, sizeof(double));
+  s->ygf = xcalloc(s->nyf + 1, sizeof(double));
+  for (int ix = 1; ix <= s->nxf; ix++) s->xgf[ix] = s->xmin + s->glxf * (double)(ix - 1);
+  for (int iy = 1; iy <= s->nyf; iy++) s->ygf[iy] = s->ymin + s->glyf * (double)(iy - 1);
+  s->xgu = xcalloc(s->nxu + 1, sizeof(double));
+  s->ygu = xcalloc(s->nyu + 1, sizeof(double));
+  for (int ix = 1; ix <= s->nxu; ix++) s->xgu[ix] = s->xmin + s->glxu * (double)(ix - 1);
+  for (int iy = 1; iy <= s->nyu; iy++) s->ygu[iy] = s->ymin + s->glyu * (double)(iy - 1);
+  s->ibx = xcalloc(s->nxu + 2, sizeof(int));
+  s->iby = xcalloc(s->nyu + 2, sizeof(int));
+  s->ibx[1] = s->nxu - 1;
+  for (int ix = 2; ix <= s->nxu + 1; ix++) s->ibx[ix] = ix - 2;
+  s->iby[1] = s->nyu - 1;
+  for (int iy = 2; iy <= s->nyu + 1; iy++) s->iby[iy] = iy - 2;
+  const int mgu = 16;
+  double fac = ONE / (double)mgu;
+  for (int ixf = 1; ixf <= mgu; ixf++) {
+    double pxf = fac * (double)(ixf - 1), pxc = ONE - pxf;
+    for (int iyf = 1; iyf <= mgu; iyf++) {
+      double pyf = fac * (double)(iyf - 1), pyc = ONE - pyf;
+      int k = (ixf - 1) * mgu + (iyf - 1);
+      s->w00[k] = pyc * pxc;
+      s->w10[k] = pyf * pxc;
+      s->w01[k] = pyc * pxf;
+      s->w11[k] = pyf * pxf;
+    }
+  }
+  s->ixfw = xcalloc(s->nxu + 1, sizeof(int));
+  s->ix0w = xcalloc(s->nxu + 1, sizeof(int));
+  s->ix1w = xcalloc(s->nxu + 1, sizeof(int));
+  s->iyfw = xcalloc(s->nyu + 1, sizeof(int));
+  s->iy0w = xcalloc(s->nyu + 1, sizeof(int));
+  s->iy1w = xcalloc(s->nyu + 1, sizeof(int));
+  for (int ix = 1; ix <= s->nxu; ix++) {
+    int ixx = (ix - 1) / mgu;
+    s->ix0w[ix] = 1 + ixx;
+    s->ix1w[ix] = 2 + ixx - nx * (s->ix0w[ix] / nx);
+    s->ixfw[ix] = ix - mgu * ixx;
+  }
+  for (int iy = 1; iy <= s->nyu; iy++) {
+    int iyy = (iy - 1) / mgu;
+    s->iy0w[iy] = 1 + iyy;
+    s->iy1w[iy] = 2 + iyy - ny * (s->iy0w[iy] / ny);
+    s->iyfw[iy] = iy - mgu * iyy;
+  }
+}
+
+static void init_spectral(o_state *s) {
+  const o_params *p = &s->p;
+  int nx = s->nx, ny = s->ny, nwx = s->nwx, nwy = s->nwy;
+  s->rkx = xcalloc(nx, sizeof(double));
+  s->hrkx = xcalloc(nx, sizeof(double));
+  s->rky = xcalloc(ny, sizeof(double));
+  s->hrky = xcalloc(ny, sizeof(double));
+  s->bety = xcalloc(ny, sizeof(double));
+  size_t nn = (size_t)nx * ny;
+  s->rksq = xcalloc(nn, sizeof(double));
+  s->qdiss = xcalloc(nn, sizeof(double));
+  s->green = xcalloc(nn, sizeof(double));
+  s->flo = xcalloc(nn, sizeof(double));
+  s->fhi = xcalloc(nn, sizeof(double));
+  s->rk = xcalloc(nn, sizeof(double));
+  /* init2dfft (sta2dfft.f90:40-97): kx(k) = (pi/lx) k */
+  {
+    double sc = s->pi / p->ellx;
+    for (int k = 1; k <= nx; k++) s->hrkx[k - 1] = sc * (double)k;
+    sc = s->pi / p->elly;
+    for (int k = 1; k <= ny; k++) s->hrky[k - 1] = sc * (double)k;
+  }
+  double *rkxf = xcalloc(nx, sizeof(double)), *rkyf = xcalloc(ny, sizeof(double));
+  /* spectral.f90:57-86 */
+  s->rkx[0] = 0.0;
+  for (int kx = 1; kx <= nwx - 1; kx++) {
+    s->rkx[kx] = s->hrkx[2 * kx - 1];
+    s->rkx[nx - kx] = s->hrkx[2 * kx - 1];
+  }
+  s->rkx[nwx] = s->hrkx[nx - 1];
+  double scx = s->twopi / p->ellx, rkxmax = scx * (double)nwx;
+  for (int kx = 0; kx < nx; kx++) {
+    rkxf[kx] = s->rkx[kx] * exp(-36.0 * pow(s->rkx[kx] / rkxmax, 36.0));
+    s->hrkx[kx] = s->hrkx[kx] * exp(-36.0 * pow(s->hrkx[kx] / rkxmax, 36.0));
+  }
+  s->rky[0] = 0.0;
+  for (int ky = 1; ky <= nwy - 1; ky++) {
+    s->rky[ky] = s->hrky[2 * ky - 1];
+    s->rky[ny - ky] = s->hrky[2 * ky - 1];
+  }
+  s->rky[nwy] = s->hrky[ny - 1];
+  double scy = s->twopi / p->elly, rkymax = scy * (double)nwy;
+  for (int ky = 0; ky < ny; ky++) {
+    rkyf[ky] = s->rky[ky] * exp(-36.0 * pow(s->rky[ky] / rkymax, 36.0));
+    s->hrky[ky] = s->hrky[ky] * exp(-36.0 * pow(s->hrky[ky] / rkymax, 36.0));
+  }
+  /* spectral.f90:95-106 */
+  double fac = 36.0 / (double)(nx * ny);
+  double a2 = rkxmax * rkxmax, b2 = rkymax * rkymax;
+  double rkmsi = ONE / (a2 > b2 ? a2 : b2);
+  for (int ky = 1; ky <= ny; ky++)
+    for (int kx = 1; kx <= nx; kx++) {
+      double rksqu = s->rkx[kx - 1] * s->rkx[kx - 1] + s->rky[ky - 1] * s->rky[ky - 1];
+      size_t k = SPC(s, kx, ky);
+      s->rk[k] = sqrt(rksqu);
+      s->qdiss[k] = p->cdamp * pow(rkmsi * rksqu, p->nnu);
+      double f = fac * rksqu;
+      s->flo[k] = ONE / (ONE + f * f);
+      s->fhi[k] = ONE - s->flo[k];
+      s->rksq[k] = rkxf[kx - 1] * rkxf[kx - 1] + rkyf[ky - 1] * rkyf[ky - 1];
+    }
+  /* Green function (spectral.f90:135-147) */
+  s->green[SPC(s, 1, 1)] = 0.0;
+  for (int kx = 2; kx <= nx; kx++)
+    s->green[SPC(s, kx, 1)] = -ONE / (s->rkx[kx - 1] * s->rkx[kx - 1] + s->kdsq);
+  for (int ky = 2; ky <= ny; ky++)
+    s->green[SPC(s, 1, ky)] = -ONE / (s->rky[ky - 1] * s->rky[ky - 1] + s->kdsq);
+  for (int ky = 2; ky <= ny; ky++)
+    for (int kx = 2; kx <= nx; kx++)
+      s->green[SPC(s, kx, ky)] =
+          -ONE / (s->rkx[kx - 1] * s->rkx[kx - 1] + s->rky[ky - 1] * s->rky[ky - 1] + s->kdsq);
+  for (int iy = 1; iy <= ny; iy++) s->bety[iy - 1] = p->beta * (s->gly * (double)(iy - 1) + s->ymin);
+  free(rkxf);
+  free(rkyf);
+}
+
+o_state *o_create(const o_params *p) {
+  if (!p || p->nx != p->ny || !is_pow2(p->nx) || p->ellx <= 0 || p->elly <= 0) return NULL;
+  o_state *s = xcalloc(1, sizeof(o_state));
+  s->p = *p;
+  if (s->p.nlevm <= 0) s->p.nlevm = 2000;
+  if (s->p.npm <= 0) s->p.npm = 500L * p->nx * p->ny;
+  if (s->p.nm <= 0) s->p.nm = s->p.npm / 20 + s->p.npm / 200;
+  if (s->p.nregmax <= 0) s->p.nregmax = 20;
+  if (s->p.twistmax <= 0) s->p.twistmax = 2.5;
+  s->nx = p->nx; s->ny = p->ny;
+  s->nxf = 4 * s->nx; s->nyf = 4 * s->ny;
+  s->nxu = 16 * s->nx; s->nyu = 16 * s->ny;
+  s->nwx = s->nx / 2; s->nwy = s->ny / 2;
+  init_constants(s);
+  init_contours(s);
+  init_spectral(s);
+  plan_init(&s->px, s->nx);
+  plan_init(&s->py, s->ny);
+  s->fwork = xcalloc(2 * (size_t)(s->nx > s->ny ? s->nx : s->ny), sizeof(double));
+  size_t nn = (size_t)s->nx * s->ny;
+  s->qr = xcalloc(nn, sizeof(double)); s->qs = xcalloc(nn, sizeof(double));
+  s->uu = xcalloc(nn, sizeof(double)); s->vv = xcalloc(nn, sizeof(double));
+  s->pp = xcalloc(nn, sizeof(double)); s->qq = xcalloc(nn, sizeof(double));
+  s->qc = xcalloc(nn, sizeof(double)); s->qd = xcalloc(nn, sizeof(double));
+  s->qspre = xcalloc(nn, sizeof(double));
+  s->emq = xcalloc(nn, sizeof(double)); s->epq = xcalloc(nn, sizeof(double));
+  long npm = s->p.npm, nm = s->p.nm;
+  s->xq = xcalloc(npm + 2, sizeof(double));
+  s->yq = xcalloc(npm + 2, sizeof(double));
+  s->nextq = xcalloc(npm + 2, sizeof(int));
+  s->indq = xcalloc(nm + 2, sizeof(int));
+  s->npq = xcalloc(nm + 2, sizeof(int));
+  s->i1q = xcalloc(nm + 2, sizeof(int));
+  s->i2q = xcalloc(nm + 2, sizeof(int));
+  return s;
+}
+
+void o_destroy(o_state *s) {
+  if (!s) return;
+  void *ptrs[] = {s->xgf, s->ygf, s->xgu, s->ygu, s->ixp, s->iyp, s->ibx, s->iby, s->ixfw,
+                  s->ix0w, s->ix1w, s->iyfw, s->iy0w, s->iy1w, s->rkx, s->hrkx, s->rky, s->hrky,
+                  s->bety, s->rksq, s->qdiss, s->green, s->flo, s->fhi, s->rk, s->fwork, s->qr,
+                  s->qs, s->uu, s->vv, s->pp, s->qq, s->qc, s->qd, s->qspre, s->emq, s->epq,
+                  s->xq, s->yq, s->nextq, s->indq, s->npq, s->i1q, s->i2q};
+  for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); i++) free(ptrs[i]);
+  plan_free(&s->px);
+  plan_free(&s->py);
+  free(s);
+}
+
+const double *o_table(o_state *s, int which) {
+  switch (which) {
+    case 0: return s->green;
+    case 1: return s->flo;
+    case 2: return s->fhi;
+    case 3: return s->qdiss;
+    case 4: return s->rksq;
+    case 5: return s->rk;
+    case 6: return s->rkx;
+    case 7: return s->hrkx;
+    case 8: return s->rky;
+    case 9: return s->hrky;
+    case 10: return s->bety;
+  }
+  return NULL;
+}
+
+double *o_field(o_state *s, int which) {
+  double *f[] = {s->qs, s->qd, s->qc, s->qq, s->pp, s->qspre, s->emq, s->epq, s->uu, s->vv, s->qr};
+  if (which < 0 || which > 10) return NULL;
+  return f[which];
+}
+
+double o_scalar(o_state *s, int which) {
+  switch (which) {
+    case 0: return s->t;
+    case 1: return s->dt;
+    case 2: return s->twist;
+    case 3: return (double)s->ireg;
+    case 4: return s->zzrms;
+    case 5: return s->zzmax;
+    case 6: return s->uumax;
+    case 7: return s->qjump;
+  }
+  return 0.0;
+}
+
+void o_set_scalar(o_state *s, int which, double v) {
+  switch (which) {
+    case 0: s->t = v; break;
+    case 1: s->dt = v; s->dt2 = v * F12; s->dt3 = v * F13; s->dt6 = v * F16; break;
+    case 2: s->twist = v; break;
+    case 3: s->ireg = (int)v; break;
+    case 7: s->qjump = v; break;
+  }
+}
+
+/* ======================================================================
+ * Contours
+ * ====================================================================== */
+int o_set_contours(o_state *s, int nq, int nptq, double qjump, const double *xq,
+                   const double *yq, const int *nextq, const int *indq, const int *npq,
+                   const int *i1q, const int *i2q) {
+  if (nptq < 0 || nptq > s->p.npm || nq < 0 || nq > s->p.nm) return 1;
+  s->nq = nq;
+  s->nptq = nptq;
+  s->qjump = qjump;
+  for (int i = 1; i <= nptq; i++) {
+    s->xq[i] = xq[i - 1];
+    s->yq[i] = yq[i - 1];
+    s->nextq[i] = nextq[i - 1];
+  }
+  for (int j = 1; j <= nq; j++) {
+    s->indq[j] = indq[j - 1];
+    s->npq[j] = npq[j - 1];
+    s->i1q[j] = i1q[j - 1];
+    s->i2q[j] = i2q[j - 1];
+  }
+  s->contex = nptq > 0;
+  return 0;
+}
+
+void o_get_counts(o_state *s, int *nq, int *nptq, double *qjump) {
+  if (nq) *nq = s->nq;
+  if (nptq) *nptq = s->nptq;
+  if (qjump) *qjump = s->qjump;
+}
+
+void o_get_contours(o_state *s, double *xq, double *yq, int *nextq, int *indq, int *npq,
+                    int *i1q, int *i2q) {
+  for (int i = 1; i <= s->nptq; i++) {
+    if (xq) xq[i - 1] = s->xq[i];
+    if (yq) yq[i - 1] = s->yq[i];
+    if (nextq) nextq[i - 1] = s->nextq[i];
+  }
+  for (int j = 1; j <= s->nq; j++) {
+    if (indq) indq[j - 1] = s->indq[j];
+    if (npq) npq[j - 1] = s->npq[j];
+    if (i1q) i1q[j - 1] = s->i1q[j];
+    if (i2q) i2q[j - 1] = s->i2q[j];
+  }
+}
+
+/* ======================================================================
+ * velint (contours.f90:136-169)
+ * ====================================================================== */
+void o_velint(o_state *s, const double *uu, const double *vv, double *uq, double *vq) {
+  for (int i = 1; i <= s->nptq; i++) {
+    double xx = s->glxi * (s->xq[i] - s->xmin);
+    int ix0 = 1 + f_int(xx);
+    double pxc = (double)ix0 - xx;
+    double px = ONE - pxc;
+    int ix1 = s->ixp[ix0];
+    double yy = s->glyi * (s->yq[i] - s->ymin);
+    int iy0 = 1 + f_int(yy);
+    double pyc = (double)iy0 - yy;
+    double py = ONE - pyc;
+    int iy1 = s->iyp[iy0];
+    uq[i - 1] = pyc * (pxc * uu[PHY(s, iy0, ix0)] + px * uu[PHY(s, iy0, ix1)]) +
+                py * (pxc * uu[PHY(s, iy1, ix0)] + px * uu[PHY(s, iy1, ix1)]);
+    vq[i - 1] = pyc * (pxc * vv[PHY(s, iy0, ix0)] + px * vv[PHY(s, iy0, ix1)]) +
+                py * (pxc * vv[PHY(s, iy1, ix0)] + px * vv[PHY(s, iy1, ix1)]);
+  }
+}
+
+/* ======================================================================
+ * con2grid (contours.f90:173-346).  The fine-grid q values are sums of
+ * +-qjump; alongside the faithful floating-point accumulation the oracle
+ * keeps the integer count of those jumps (the PV level index), which is
+ * what the CUDA path reproduces bit for bit.
+ * ====================================================================== */
+void o_con2grid(o_state *s, double *qc, int *levels) {
+  int nx = s->nx, ny = s->ny, nxf = s->nxf, nyf = s->nyf, nptq = s->nptq;
+  if (nptq == 0) {
+    memset(qc, 0, sizeof(double) * (size_t)nx * ny);
+    if (levels) memset(levels, 0, sizeof(int) * (size_t)nxf * nyf);
+    return;
+  }
+  const double ellx = s->p.ellx, elly = s->p.elly, hlx = s->hlx, hly = s->hly;
+  const double hlxi = s->hlxi, hlyi = s->hlyi, xmin = s->xmin, ymin = s->ymin;
+  const double glxfi = s->glxfi, glyfi = s->glyfi, qjump = s->qjump, small = s->small;
+  double *xq = s->xq, *yq = s->yq;
+  int *nextq = s->nextq;
+  int *ixc = xcalloc(nptq + 1, sizeof(int)), *nxc = xcalloc(nptq + 1, sizeof(int));
+  double *dx = xcalloc(nptq + 1, sizeof(double)), *dy = xcalloc(nptq + 1, sizeof(double));
+  char *crossx = xcalloc(nptq + 1, 1);
+  double *qjx = xcalloc(nxf + 1, sizeof(double)), *qbot = xcalloc(nxf + 1, sizeof(double));
+  int *ljx = xcalloc(nxf + 1, sizeof(int)), *lbot = xcalloc(nxf + 1, sizeof(int));
+  size_t ldq = (size_t)nyf + 1;
+  double *qa = xcalloc(ldq * nxf, sizeof(double));
+  int *la = levels ? xcalloc(ldq * nxf, sizeof(int)) : NULL;
+#define QA(iy, ix) qa[(size_t)((ix)-1) * ldq + (size_t)((iy)-1)]
+#define LA(iy, ix) la[(size_t)((ix)-1) * ldq + (size_t)((iy)-1)]
+
+  for (int i = 1; i <= nptq; i++) ixc[i] = 1 + f_int(glxfi * (xq[i] - xmin));
+  for (int i = 1; i <= nptq; i++) {
+    int ia = nextq[i];
+    double xx = xq[ia] - xq[i];
+    dx[i] = xx - ellx * f_dint(xx * hlxi);
+    double yy = yq[ia] - yq[i];
+    dy[i] = yy - elly * f_dint(yy * hlyi);
+    int ixdif = ixc[ia] - ixc[i];
+    nxc[i] = ixdif - nxf * ((2 * ixdif) / nxf);
+    crossx[i] = nxc[i] != 0;
+    if (fabs(yy) > hly) {
+      double cc = f_sign1(dy[i]);
+      double p = -(yq[i] - hly * cc) / (dy[i] + small);
+      int ix = 1 + f_int(glxfi * fmod(ellx + hlx + xq[i] + p * dx[i], ellx));
+      qjx[ix] = qjx[ix] - qjump * cc;
+      ljx[ix] -= (int)cc;
+    }
+  }
+  qbot[1] = ZERO;
+  lbot[1] = 0;
+  for (int ix = 1; ix <= nxf - 1; ix++) {
+    qbot[ix + 1] = qbot[ix] + qjx[ix];
+    lbot[ix + 1] = lbot[ix] + ljx[ix];
+  }
+  for (int i = 1; i <= nptq; i++) {
+    if (!crossx[i]) continue;
+    int jump = f_isign1(nxc[i]);
+    int ixbeg = ixc[i] + (jump - 1) / 2 + nxf;
+    double sgn = f_sign1(dx[i]);
+    double sqjump = qjump * sgn;
+    int ncr = 0;
+    while (ncr != nxc[i]) {
+      int ix = 1 + (ixbeg + ncr) % nxf;
+      double xx = s->xgf[ix] - xq[i];
+      double px0 = (xx - ellx * f_dint(xx * hlxi)) / dx[i];
+      double yy = yq[i] + px0 * dy[i];
+      int iy = 2 + f_int(glyfi * (yy - elly * f_dint(yy * hlyi) - ymin));
+      QA(iy, ix) = QA(iy, ix) + sqjump;
+      if (la) LA(iy, ix) += (int)sgn;
+      ncr = ncr + jump;
+    }
+  }
+  for (int ix = 1; ix <= nxf; ix++) {
+    QA(1, ix) = qbot[ix];
+    if (la) LA(1, ix) = lbot[ix];
+    for (int iy = 2; iy <= nyf; iy++) {
+      QA(iy, ix) = QA(iy, ix) + QA(iy - 1, ix);
+      if (la) LA(iy, ix) += LA(iy - 1, ix);
+    }
+  }
+  if (levels) {
+    for (int ix = 1; ix <= nxf; ix++)
+      for (int iy = 1; iy <= nyf; iy++)
+        levels[(size_t)(ix - 1) * nyf + (iy - 1)] = LA(iy, ix);
+  }
+  if (s->beffect) {
+    for (int ix = 1; ix <= nxf; ix++)
+      for (int iy = 1; iy <= nyf; iy++) QA(iy, ix) = QA(iy, ix) - s->p.beta * s->ygf[iy];
+  }
+  /* Nine-point averaging to the coarse grid (contours.f90:290-327); the
+   * periodic wrap column uses index nyff as the reference does. */
+  {
+    int nh = nyf / 2 + 1;
+    double *qod0 = xcalloc(nh, sizeof(double)), *qod1 = xcalloc(nh, sizeof(double));
+    double *qod2 = xcalloc(nh, sizeof(double));
+    double *qev0 = xcalloc(nh, sizeof(double)), *qev1 = xcalloc(nh, sizeof(double));
+    double *qev2 = xcalloc(nh, sizeof(double));
+    int nxh = nxf, nyh = nyf;
+    while (nxh > nx) {
+      nxh = nxh / 2;
+      int nyff = nyh;
+      nyh = nyh / 2;
+      for (int iy = 1; iy <= nyh; iy++) {
+        int miy = 2 * iy;
+        qod2[iy] = QA(miy - 1, nyff);
+        qev2[iy] = QA(miy, nyff);
+      }
+      qev2[0] = QA(nyff, nyff);
+      for (int ix = 1; ix <= nxh; ix++) {
+        int mix = 2 * ix, mixm1 = mix - 1;
+        for (int iy = 1; iy <= nyh; iy++) {
+          int miy = 2 * iy;
+          qod1[iy] = QA(miy - 1, mixm1);
+          qod0[iy] = QA(miy - 1, mix);
+          qev1[iy] = QA(miy, mixm1);
+          qev0[iy] = QA(miy, mix);
+        }
+        qev1[0] = qev1[nyh];
+        qev0[0] = qev0[nyh];
+        for (int iy = 1; iy <= nyh; iy++) {
+          QA(iy, ix) = 0.0625 * (qev0[iy] + qev0[iy - 1] + qev2[iy] + qev2[iy - 1]) +
+                       0.125 * (qev1[iy] + qev1[iy - 1] + qod0[iy] + qod2[iy]) +
+                       0.25 * qod1[iy];
+        }
+        for (int iy = 1; iy <= nyh; iy++) {
+          qod2[iy] = qod0[iy];
+          qev2[iy] = qev0[iy];
+        }
+        qev2[0] = qev0[0];
+      }
+    }
+    free(qod0); free(qod1); free(qod2); free(qev0); free(qev1); free(qev2);
+  }
+  double qavg0 = ZERO;
+  for (int ix = 1; ix <= nx; ix++)
+    for (int iy = 1; iy <= ny; iy++) qavg0 = qavg0 + QA(iy, ix);
+  qavg0 = qavg0 / (double)(nx * ny);
+  for (int ix = 1; ix <= nx; ix++)
+    for (int iy = 1; iy <= ny; iy++) qc[PHY(s, iy, ix)] = QA(iy, ix) - qavg0;
+#undef QA
+#undef LA
+  free(ixc); free(nxc); free(dx); free(dy); free(crossx); free(qjx); free(qbot);
+  free(ljx); free(lbot); free(qa); free(la);
+}
+
+/* ======================================================================
+ * renode (contours.f90:687-933)
+ * ====================================================================== */
+static int renode_cap(o_state *s, const double *xd0, const double *yd0, int npd,
+                      double *xr0, double *yr0, long cap) {
+  const double ellx = s->p.ellx, elly = s->p.elly, hlxi = s->hlxi, hlyi = s->hlyi;
+  const double small = s->small, small3 = s->small3, oms = s->oms;
+  const double dmsq = s->dmsq, elf = s->elf, dmi = s->dmi, densf = s->densf;
+  const double *xd = xd0 - 1, *yd = yd0 - 1; /* 1-based views */
+  double *xr = xr0 - 1, *yr = yr0 - 1;
+  size_t m = (size_t)npd + 2;
+  double *dx = xcalloc(m, sizeof(double)), *dy = xcalloc(m, sizeof(double));
+  double *a = xcalloc(m, sizeof(double)), *b = xcalloc(m, sizeof(double));
+  double *c = xcalloc(m, sizeof(double)), *d = xcalloc(m, sizeof(double));
+  double *e = xcalloc(m, sizeof(double)), *u = xcalloc(m, sizeof(double));
+  double *v = xcalloc(m, sizeof(double));
+  int *node = xcalloc(m, sizeof(int)), *next = xcalloc(m, sizeof(int));
+  char *corner = xcalloc(m, 1);
+  int npr = 0;
+
+  for (int i = 0; i <= npd - 1; i++) next[i] = i + 1;
+  next[npd] = 1;
+  for (int i = 1; i <= npd; i++) {
+    int ia = next[i];
+    double xx = xd[ia] - xd[i];
+    dx[i] = xx - ellx * f_dint(xx * hlxi);
+    double yy = yd[ia] - yd[i];
+    dy[i] = yy - elly * f_dint(yy * hlyi);
+  }
+  for (int i = 1; i <= npd; i++) {
+    v[i] = dx[i] * dx[i] + dy[i] * dy[i];
+    e[i] = sqrt(v[i]);
+  }
+  for (int ib = 1; ib <= npd; ib++) {
+    int i = next[ib];
+    u[i] = v[ib];
+    a[i] = -dx[ib];
+    c[i] = -dy[ib];
+  }
+  int ncorn = 0;
+  for (int i = 1; i <= npd; i++) {
+    corner[i] = dx[i] * a[i] + dy[i] * c[i] > ZERO;
+    if (corner[i]) {
+      ncorn = ncorn + 1;
+      node[ncorn] = i;
+      b[i] = ZERO;
+    } else {
+      double t1 = a[i] * v[i] - dx[i] * u[i];
+      double t2 = c[i] * v[i] - dy[i] * u[i];
+      b[i] = (dx[i] * c[i] - a[i] * dy[i]) / sqrt(t1 * t1 + t2 * t2 + small3);
+    }
+  }
+  for (int i = 1; i <= npd; i++) {
+    int ia = next[i];
+    u[i] = e[i] * (b[ia] + b[i]);
+    c[i] = e[i] * (b[ia] - b[i]);
+  }
+  for (int i = 1; i <= npd; i++) {
+    a[i] = F16 * c[i] - F12 * u[i];
+    b[i] = F12 * (u[i] - c[i]);
+    c[i] = F13 * c[i];
+  }
+  for (int i = 1; i <= npd; i++) {
+    double ww = ONE / (v[i] + dmsq);
+    u[i] = ww * sqrt(elf * v[i] + u[i] * u[i]);
+    v[i] = ww * e[i];
+  }
+  for (int ib = 1; ib <= npd; ib++) {
+    int i = next[ib];
+    d[i] = (u[ib] + u[i]) / (v[ib] + v[i] + small);
+  }
+  for (int i = 1; i <= npd; i++) {
+    int ia = next[i];
+    u[i] = F12 * (d[i] + d[ia]);
+  }
+  for (int i = 1; i <= npd; i++) {
+    double t = densf * sqrt(u[i]) + u[i];
+    e[i] = e[i] * (dmi < t ? dmi : t);
+  }
+  double sum = ZERO;
+  for (int i = 1; i <= npd; i++) sum = sum + e[i];
+  npr = f_nint(sum) + 1;
+  if (npr < 3) {
+    npr = 0;
+    goto done;
+  }
+  if (ncorn <= 1 && npr > cap) {
+    npr = -1;
+    goto done;
+  }
+#define PLACE(im, i, p)                                            \
+  do {                                                             \
+    double eta = (p) * (a[i] + (p) * (b[i] + (p) * c[i]));         \
+    double xx = xd[i] + (p) * dx[i] - eta * dy[i];                 \
+    xr[im] = oms * (xx - ellx * f_dint(xx * hlxi));                \
+    double yy = yd[i] + (p) * dy[i] + eta * dx[i];                 \
+    yr[im] = oms * (yy - elly * f_dint(yy * hlyi));                \
+  } while (0)
+  if (ncorn == 0) {
+    double fac = (double)npr / sum;
+    for (int i = 1; i <= npd; i++) e[i] = fac * e[i];
+    xr[1] = xd[1];
+    yr[1] = yd[1];
+    double acc = ZERO;
+    int i = 0;
+    for (int im = 2; im <= npr; im++) {
+      while (acc < ONE) {
+        i = i + 1;
+        acc = acc + e[i];
+      }
+      acc = acc - ONE;
+      double p = ONE - acc / e[i];
+      PLACE(im, i, p);
+    }
+  } else if (ncorn == 1) {
+    double fac = (double)npr / sum;
+    for (int i = 1; i <= npd; i++) e[i] = fac * e[i];
+    int i = node[1];
+    xr[1] = xd[i];
+    yr[1] = yd[i];
+    double acc = ZERO;
+    i = i - 1;
+    for (int im = 2; im <= npr; im++) {
+      while (acc < ONE) {
+        i = next[i];
+        acc = acc + e[i];
+      }
+      acc = acc - ONE;
+      double p = ONE - acc / e[i];
+      PLACE(im, i, p);
+    }
+  } else {
+    npr = 0;
+    node[ncorn + 1] = node[1];
+    int ibeg = node[1];
+    for (int k = 1; k <= ncorn; k++) {
+      int iend = node[k + 1];
+      int i = ibeg;
+      double ssum = ZERO;
+      while (i != iend) {
+        ssum = ssum + e[i];
+        i = next[i];
+      }
+      if (ssum > small) {
+        int npseg = f_nint(ssum) + 1;
+        if (npr + npseg > cap) {
+          npr = -1;
+          goto done;
+        }
+        double fac = (double)npseg / ssum;
+        i = ibeg;
+        while (i != iend) {
+          e[i] = fac * e[i];
+          i = next[i];
+        }
+        xr[npr + 1] = xd[ibeg];
+        yr[npr + 1] = yd[ibeg];
+        if (npseg > 1) {
+          double acc = ZERO;
+          i = ibeg - 1;
+          for (int im = npr + 2; im <= npr + npseg; im++) {
+            while (acc < ONE) {
+              i = next[i];
+              acc = acc + e[i];
+            }
+            acc = acc - ONE;
+            double p = ONE - acc / e[i];
+            PLACE(im, i, p);
+          }
+        }
+        npr = npr + npseg;
+      }
+      ibeg = iend;
+    }
+  }
+#undef PLACE
+done:
+  free(dx); free(dy); free(a); free(b); free(c); free(d); free(e); free(u); free(v);
+  free(node); free(next); free(corner);
+  return npr;
+}
+
+int o_renode(o_state *s, const double *xd, const double *yd, int npd, double *xr, double *yr) {
+  return renode_cap(s, xd, yd, npd, xr, yr, 0x7fffffffL);
+}
+
+/* ======================================================================
+ * surgery (contours.f90:350-683)
+ * ====================================================================== */
+int o_surgery(o_state *s) {
+  if (s->nq == 0) return 0;
+  const double ellx = s->p.ellx, elly = s->p.elly, hlxi = s->hlxi, hlyi = s->hlyi;
+  const double xmin = s->xmin, ymin = s->ymin, oms = s->oms, aspect = s->aspect;
+  const double d4small = s->d4small, dm2 = s->dm2;
+  const int nx = s->nx, ny = s->ny;
+  int nq = s->nq, nptq = s->nptq;
+  double *xq = s->xq, *yq = s->yq;
+  int *nextq = s->nextq;
+  long npm = s->p.npm;
+
+  double *xa = xcalloc(npm + 2, sizeof(double)), *ya = xcalloc(npm + 2, sizeof(double));
+  double *dx = xcalloc(nptq + 2, sizeof(double)), *dy = xcalloc(nptq + 2, sizeof(double));
+  double *dsq = xcalloc(nptq + 2, sizeof(double));
+  int *i1a = xcalloc(s->p.nm + 2, sizeof(int)), *i2a = xcalloc(s->p.nm + 2, sizeof(int));
+  int *jq1 = xcalloc(nq + 2, sizeof(int)), *jq2 = xcalloc(nq + 2, sizeof(int));
+  int *iq1 = xcalloc(nq + 2, sizeof(int)), *iq2 = xcalloc(nq + 2, sizeof(int));
+  int *levq = xcalloc(nq + 2, sizeof(int));
+  int ngbs = nx * ny;
+  int *nspb = xcalloc(ngbs + 2, sizeof(int)), *kb1 = xcalloc(ngbs + 2, sizeof(int));
+  int *kb2 = xcalloc(ngbs + 2, sizeof(int));
+  int *nexta = xcalloc(npm + 2, sizeof(int));
+  char *avail = xcalloc(nptq + 2, 1);
+  double *xd = xcalloc(nptq + 2, sizeof(double)), *yd = xcalloc(nptq + 2, sizeof(double));
+  size_t segcap = 4 * (size_t)nptq + 16;
+  int *loc = xcalloc(segcap, sizeof(int)), *list = xcalloc(segcap, sizeof(int));
+  int *node = xcalloc(segcap, sizeof(int));
+
+  int levp = s->indq[1], nlev = 1;
+  jq1[1] = 1;
+  levq[1] = levp;
+  for (int j = 2; j <= nq; j++) {
+    int lev = s->indq[j];
+    if (lev > levp) {
+      jq2[nlev] = j - 1;
+      nlev = nlev + 1;
+      jq1[nlev] = j;
+      levq[nlev] = lev;
+      levp = lev;
+    }
+  }
+  jq2[nlev] = nq;
+  for (int lev = 1; lev <= nlev; lev++) {
+    iq1[lev] = s->i1q[jq1[lev]];
+    iq2[lev] = s->i2q[jq2[lev]];
+  }
+  for (int i = 1; i <= nptq - 1; i++) {
+    double xx = xq[i + 1] - xq[i];
+    dx[i] = xx - ellx * f_dint(xx * hlxi);
+    double yy = yq[i + 1] - yq[i];
+    dy[i] = yy - elly * f_dint(yy * hlyi);
+    dsq[i] = dx[i] * dx[i] + dy[i] * dy[i];
+    avail[i] = 1;
+  }
+  avail[nptq] = 1;
+  for (int j = 1; j <= nq; j++) {
+    int ie = s->i2q[j], is = s->i1q[j];
+    double xx = xq[is] - xq[ie];
+    dx[ie] = xx - ellx * f_dint(xx * hlxi);
+    double yy = yq[is] - yq[ie];
+    dy[ie] = yy - elly * f_dint(yy * hlyi);
+    dsq[ie] = dx[ie] * dx[ie] + dy[ie] * dy[ie];
+  }
+
+  int nqn = 0, nptqn = 0, err = 0;
+  for (int lev = 1; lev <= nlev && !err; lev++) {
+    int ibeg = iq1[lev], iend = iq2[lev];
+    int nptlev = iend - ibeg + 1;
+    double fnq = (double)nptlev;
+    double fnbx = 1.2 * sqrt(fnq * aspect);
+    double fnby = fnbx / aspect;
+    int nbx = f_nint(fnbx);
+    nbx = nbx < nx ? nbx : nx;
+    nbx = nbx > 1 ? nbx : 1;
+    int nby = f_nint(fnby);
+    nby = nby < ny ? nby : ny;
+    nby = nby > 1 ? nby : 1;
+    int nbox = nbx * nby;
+    double bwxi = oms * (double)nbx / ellx;
+    double bwyi = oms * (double)nby / elly;
+    for (int mb = 1; mb <= nbox; mb++) nspb[mb] = 0;
+    int nseg = 0;
+    double dnbx = (double)nbx, dnby = (double)nby;
+    for (int ib = ibeg; ib <= iend; ib++) {
+      int i = nextq[ib];
+      int mbx1, mbx2, mby1, mby2;
+      if (dx[i] > ZERO) {
+        mbx1 = f_int(dnbx + bwxi * (xq[i] - xmin));
+        mbx2 = f_int(dnbx + bwxi * (xq[i] + dx[i] - xmin));
+      } else {
+        mbx1 = f_int(dnbx + bwxi * (xq[i] + dx[i] - xmin));
+        mbx2 = f_int(dnbx + bwxi * (xq[i] - xmin));
+      }
+      if (dy[i] > ZERO) {
+        mby1 = f_int(dnby + bwyi * (yq[i] - ymin));
+        mby2 = f_int(dnby + bwyi * (yq[i] + dy[i] - ymin));
+      } else {
+        mby1 = f_int(dnby + bwyi * (yq[i] + dy[i] - ymin));
+        mby2 = f_int(dnby + bwyi * (yq[i] - ymin));
+      }
+      for (int mbx = mbx1; mbx <= mbx2; mbx++) {
+        int mmbx = mbx % nbx;
+        for (int mby = mby1; mby <= mby2; mby++) {
+          int mb = nby * mmbx + mby % nby + 1;
+          nspb[mb] = nspb[mb] + 1;
+          nseg = nseg + 1;
+          if ((size_t)nseg >= segcap) {
+            segcap *= 2;
+            loc = realloc(loc, segcap * sizeof(int));
+            list = realloc(list, segcap * sizeof(int));
+            node = realloc(node, segcap * sizeof(int));
+          }
+          loc[nseg] = mb;
+          list[nseg] = ib;
+        }
+      }
+    }
+    kb1[1] = 1;
+    for (int mb = 1; mb <= nbox - 1; mb++) kb1[mb + 1] = kb1[mb] + nspb[mb];
+    for (int mb = 1; mb <= nbox; mb++) kb2[mb] = kb1[mb] - 1;
+    for (int k = 1; k <= nseg; k++) {
+      int mb = loc[k];
+      int ks = kb2[mb] + 1;
+      node[ks] = list[k];
+      kb2[mb] = ks;
+    }
+    /* search (contours.f90:528-613) */
+    for (int ib = ibeg; ib <= iend; ib++) {
+      int i = nextq[ib];
+      int mb = nby * f_int(bwxi * (xq[i] - xmin)) + f_int(bwyi * (yq[i] - ymin)) + 1;
+      for (int k = kb1[mb]; k <= kb2[mb]; k++) {
+        int isb = node[k];
+        int is = nextq[isb];
+        if ((long)(is - ib) * (long)(is - i) == 0) continue;
+        double xx = xq[is] - xq[i];
+        double delx = xx - ellx * f_dint(xx * hlxi);
+        double yy = yq[is] - yq[i];
+        double dely = yy - elly * f_dint(yy * hlyi);
+        double aa = delx * dx[is] + dely * dy[is];
+        if (aa * (aa + dsq[is]) + d4small < ZERO) {
+          double cr = delx * dy[is] - dely * dx[is];
+          double cc = cr * cr;
+          if (cc * (cc - dm2 * dsq[is]) < ZERO) {
+            double dxa, dya;
+            if (dsq[is] + TWO * aa < ZERO) {
+              dxa = F12 * (delx + dx[is]);
+              dya = F12 * (dely + dy[is]);
+              isb = is;
+              is = nextq[is];
+            } else {
+              dxa = F12 * delx;
+              dya = F12 * dely;
+            }
+            xx = xq[i] + dxa;
+            xq[i] = oms * (xx - ellx * f_dint(xx * hlxi));
+            yy = yq[i] + dya;
+            yq[i] = oms * (yy - elly * f_dint(yy * hlyi));
+            dx[i] = dx[i] - dxa;
+            dy[i] = dy[i] - dya;
+            dsq[i] = dx[i] * dx[i] + dy[i] * dy[i];
+            nextq[isb] = i;
+            dx[isb] = dx[isb] - dxa;
+            dy[isb] = dy[isb] - dya;
+            dsq[isb] = dx[isb] * dx[isb] + dy[isb] * dy[isb];
+            xq[is] = xq[i];
+            yq[is] = yq[i];
+            dx[is] = dx[is] + dxa;
+            dy[is] = dy[is] + dya;
+            dsq[is] = dx[is] * dx[is] + dy[is] * dy[is];
+            nextq[ib] = is;
+            dx[ib] = dx[ib] + dxa;
+            dy[ib] = dy[ib] + dya;
+            dsq[ib] = dx[ib] * dx[ib] + dy[ib] * dy[ib];
+            i = is;
+            if (i == ib) break;
+          }
+        }
+      }
+    }
+    /* rebuild (contours.f90:621-663) */
+    int levt = levq[lev];
+    for (int i = ibeg; i <= iend; i++) {
+      if (!avail[i]) continue;
+      nqn = nqn + 1;
+      int npd = 1;
+      xd[1] = xq[i];
+      yd[1] = yq[i];
+      avail[i] = 0;
+      int is = nextq[i];
+      while (is != i) {
+        npd = npd + 1;
+        xd[npd] = xq[is];
+        yd[npd] = yq[is];
+        avail[is] = 0;
+        is = nextq[is];
+      }
+      int npn = npd;
+      if (npd > 3)
+        npn = renode_cap(s, xd + 1, yd + 1, npd, xa + nptqn + 1, ya + nptqn + 1, npm - nptqn);
+      if (npn < 0 || nqn > s->p.nm) {
+        err = 1;
+        break;
+      }
+      if (npn > 3) {
+        s->npq[nqn] = npn;
+        i1a[nqn] = nptqn + 1;
+        nptqn = nptqn + npn;
+        i2a[nqn] = nptqn;
+        s->indq[nqn] = levt;
+        for (int k = i1a[nqn]; k <= nptqn - 1; k++) nexta[k] = k + 1;
+        nexta[nptqn] = i1a[nqn];
+      } else {
+        nqn = nqn - 1;
+      }
+    }
+  }
+  for (int i = 1; i <= nptqn; i++) {
+    xq[i] = xa[i];
+    yq[i] = ya[i];
+    nextq[i] = nexta[i];
+  }
+  for (int j = 1; j <= nqn; j++) {
+    s->i1q[j] = i1a[j];
+    s->i2q[j] = i2a[j];
+  }
+  s->nq = nqn;
+  s->nptq = nptqn;
+  free(xa); free(ya); free(dx); free(dy); free(dsq); free(i1a); free(i2a); free(jq1);
+  free(jq2); free(iq1); free(iq2); free(levq); free(nspb); free(kb1); free(kb2);
+  free(nexta); free(avail); free(xd); free(yd); free(loc); free(list); free(node);
+  return err;
+}
+
+/* ======================================================================
+ * Spectral inversion, gradient (spectral.f90:304-366)
+ * ====================================================================== */
+void o_main_invert(o_state *s, const double *qq, double *uu, double *vv, double *pp) {
+  size_t nn = (size_t)s->nx * s->ny;
+  double *vtmp = xcalloc(nn, sizeof(double));
+  for (size_t k = 0; k < nn; k++) pp[k] = s->green[k] * qq[k];
+  xderiv(s, s->hrkx, pp, vtmp);
+  o_spctop(s, vtmp, vv);
+  yderiv(s, s->hrky, pp, vtmp);
+  o_spctop(s, vtmp, uu);
+  for (size_t k = 0; k < nn; k++) uu[k] = -uu[k];
+  free(vtmp);
+}
+
+void o_gradient(o_state *s, const double *ff, double *ffx, double *ffy) {
+  size_t nn = (size_t)s->nx * s->ny;
+  double *vtmp = xcalloc(nn, sizeof(double));
+  xderiv(s, s->hrkx, ff, vtmp);
+  o_spctop(s, vtmp, ffx);
+  yderiv(s, s->hrky, ff, vtmp);
+  o_spctop(s, vtmp, ffy);
+  free(vtmp);
+}
+
+/* inversion (evolution.f90:494-520) */
+void o_inversion(o_state *s) {
+  size_t nn = (size_t)s->nx * s->ny;
+  double *qa = xcalloc(nn, sizeof(double));
+  o_con2grid(s, qa, NULL);
+  o_ptospc(s, qa, s->qc);
+  for (size_t k = 0; k < nn; k++)
+    s->qq[k] = s->flo[k] * (s->qs[k] - s->qc[k]) + s->qc[k] + s->qd[k];
+  o_main_invert(s, s->qq, s->uu, s->vv, s->pp);
+  free(qa);
+}
+
+/* source (evolution.f90:432-490) */
+static void source(o_state *s, double *sqs, double *sqd, int lev) {
+  size_t nn = (size_t)s->nx * s->ny;
+  double *qqx = xcalloc(nn, sizeof(double)), *qqy = xcalloc(nn, sizeof(double));
+  o_gradient(s, s->qd, qqx, qqy);
+  for (size_t k = 0; k < nn; k++) qqx[k] = -s->uu[k] * qqx[k] - s->vv[k] * qqy[k];
+  o_ptospc(s, qqx, sqd);
+  o_gradient(s, s->qs, qqx, qqy);
+  if (s->beffect) {
+    for (size_t k = 0; k < nn; k++)
+      qqx[k] = -s->uu[k] * qqx[k] - s->vv[k] * (qqy[k] + s->p.beta);
+  } else {
+    for (size_t k = 0; k < nn; k++) qqx[k] = -s->uu[k] * qqx[k] - s->vv[k] * qqy[k];
+  }
+  o_ptospc(s, qqx, sqs);
+  if (s->heating) {
+    /* Thermal damping needs an equilibrium streamfunction (psieq.r8), which
+     * no configuration of this path uses; ppeq = 0 here. */
+    if (s->friction) {
+      for (size_t k = 0; k < nn; k++)
+        sqd[k] = sqd[k] + s->therm * (s->pp[k] - 0.0) - s->p.rekman * (s->qq[k] + s->kdsq * s->pp[k]);
+    } else {
+      for (size_t k = 0; k < nn; k++) sqd[k] = sqd[k] + s->therm * (s->pp[k] - 0.0);
+    }
+  } else {
+    for (size_t k = 0; k < nn; k++)
+      sqd[k] = sqd[k] - s->p.rekman * (s->qq[k] + s->kdsq * s->pp[k]);
+  }
+  if (lev != 0) {
+    if (lev == 1) {
+      for (size_t k = 0; k < nn; k++) sqd[k] = s->epq[k] * sqd[k];
+    } else {
+      for (size_t k = 0; k < nn; k++) sqd[k] = s->epq[k] * s->epq[k] * sqd[k];
+    }
+  }
+  free(qqx);
+  free(qqy);
+}
+
+/* adapt (evolution.f90:524-608) with the fixed-dt override.  Save flags and
+ * the monitor file are not produced (no saves inside this path). */
+static void adapt(o_state *s) {
+  size_t nn = (size_t)s->nx * s->ny;
+  double *ss = xcalloc(nn, sizeof(double)), *zz = xcalloc(nn, sizeof(double));
+  const double dtfac = s->pi / 10.0, cflmax = 0.7;
+  if (s->btropic) {
+    memcpy(ss, s->qq, nn * sizeof(double));
+  } else {
+    for (size_t k = 0; k < nn; k++) ss[k] = s->qq[k] + s->kdsq * s->pp[k];
+  }
+  o_spctop(s, ss, zz);
+  double sum = 0.0, zmax = 0.0;
+  for (size_t k = 0; k < nn; k++) {
+    zz[k] = zz[k] * zz[k];
+    sum = sum + zz[k];
+  }
+  zmax = zz[0];
+  for (size_t k = 1; k < nn; k++) zmax = zz[k] > zmax ? zz[k] : zmax;
+  double zzrms = sqrt(s->dsumi * sum);
+  double zzmax = sqrt(zmax) + s->small;
+  double umax = 0.0;
+  for (size_t k = 0; k < nn; k++) {
+    double w = s->uu[k] * s->uu[k] + s->vv[k] * s->vv[k];
+    if (k == 0 || w > umax) umax = w;
+  }
+  double uumax = sqrt(umax) + s->small;
+  double a = s->glx * cflmax / uumax;
+  double zm = zzmax > s->srwfm ? zzmax : s->srwfm;
+  double b = dtfac / zm;
+  double dtacc = a < b ? a : b;
+  if (s->p.fixed_dt > 0.0) {
+    s->dt = s->p.fixed_dt;
+  } else {
+    /* dtmax is 0.2*min(tgsave,tcsave) in the reference; here a parameter. */
+    s->dtmax = s->p.dtmax > 0.0 ? s->p.dtmax : 1.0e30;
+    s->dt = dtacc < s->dtmax ? dtacc : s->dtmax;
+  }
+  s->dt2 = s->dt * F12;
+  s->dt3 = s->dt * F13;
+  s->dt6 = s->dt * F16;
+  s->twist = s->twist + s->dt * zzmax;
+  s->zzrms = zzrms;
+  s->zzmax = zzmax;
+  s->uumax = uumax;
+  double dfac = s->dt2 * zzrms;
+  for (size_t k = 0; k < nn; k++) {
+    s->epq[k] = exp(dfac * s->qdiss[k]);
+    s->emq[k] = ONE / s->epq[k];
+  }
+  free(ss);
+  free(zz);
+}
+
+/* advance (evolution.f90:166-326) */
+void o_advance(o_state *s) {
+  size_t nn = (size_t)s->nx * s->ny;
+  int nptq = s->nptq;
+  double *qsi = xcalloc(nn, sizeof(double)), *qsf = xcalloc(nn, sizeof(double));
+  double *sqs = xcalloc(nn, sizeof(double)), *qdi = xcalloc(nn, sizeof(double));
+  double *qdf = xcalloc(nn, sizeof(double)), *sqd = xcalloc(nn, sizeof(double));
+  double *xqi = xcalloc(nptq + 1, sizeof(double)), *yqi = xcalloc(nptq + 1, sizeof(double));
+  double *xqf = xcalloc(nptq + 1, sizeof(double)), *yqf = xcalloc(nptq + 1, sizeof(double));
+  double *uq = xcalloc(nptq + 1, sizeof(double)), *vq = xcalloc(nptq + 1, sizeof(double));
+  const double ellx = s->p.ellx, elly = s->p.elly, hlxi = s->hlxi, hlyi = s->hlyi, oms = s->oms;
+  double *xq = s->xq, *yq = s->yq;
+#define WRAPX(v) (oms * ((v)-ellx * f_dint((v)*hlxi)))
+#define WRAPY(v) (oms * ((v)-elly * f_dint((v)*hlyi)))
+
+  /* RK4 predictor step to t0 + dt/2 */
+  o_inversion(s);
+  for (size_t k = 0; k < nn; k++) {
+    s->qs[k] = s->flo[k] * (s->qs[k] - s->qc[k]) + s->qc[k] + s->qd[k];
+    s->qd[k] = s->fhi[k] * (s->qs[k] - s->qc[k]);
+  }
+  adapt(s);
+  double dt = s->dt, dt2 = s->dt2, dt3 = s->dt3, dt6 = s->dt6;
+  source(s, sqs, sqd, 0);
+  if (s->contex) {
+    o_velint(s, s->uu, s->vv, uq + 1, vq + 1);
+    for (int i = 1; i <= nptq; i++) {
+      xqi[i] = xq[i];
+      yqi[i] = yq[i];
+      double xx = xqi[i] + dt2 * uq[i], yy = yqi[i] + dt2 * vq[i];
+      xq[i] = WRAPX(xx);
+      yq[i] = WRAPY(yy);
+      xx = xqi[i] + dt6 * uq[i];
+      yy = yqi[i] + dt6 * vq[i];
+      xqf[i] = WRAPX(xx);
+      yqf[i] = WRAPY(yy);
+    }
+  }
+  for (size_t k = 0; k < nn; k++) {
+    qsi[k] = s->qs[k];
+    s->qs[k] = qsi[k] + dt2 * sqs[k];
+    qsf[k] = qsi[k] + dt6 * sqs[k];
+    qdi[k] = s->qd[k];
+    s->qd[k] = s->emq[k] * (qdi[k] + dt2 * sqd[k]);
+    qdf[k] = qdi[k] + dt6 * sqd[k];
+  }
+  /* RK4 corrector step at t0 + dt/2 */
+  s->t = s->t + dt2;
+  o_inversion(s);
+  source(s, sqs, sqd, 1);
+  if (s->contex) {
+    o_velint(s, s->uu, s->vv, uq + 1, vq + 1);
+    for (int i = 1; i <= nptq; i++) {
+      double xx = xqi[i] + dt2 * uq[i], yy = yqi[i] + dt2 * vq[i];
+      xq[i] = WRAPX(xx);
+      yq[i] = WRAPY(yy);
+      xx = xqf[i] + dt3 * uq[i];
+      yy = yqf[i] + dt3 * vq[i];
+      xqf[i] = WRAPX(xx);
+      yqf[i] = WRAPY(yy);
+    }
+  }
+  for (size_t k = 0; k < nn; k++) {
+    s->qs[k] = qsi[k] + dt2 * sqs[k];
+    qsf[k] = qsf[k] + dt3 * sqs[k];
+    s->qd[k] = s->emq[k] * (qdi[k] + dt2 * sqd[k]);
+    qdf[k] = qdf[k] + dt3 * sqd[k];
+  }
+  /* RK4 predictor step at t0 + dt */
+  o_inversion(s);
+  source(s, sqs, sqd, 1);
+  if (s->contex) {
+    o_velint(s, s->uu, s->vv, uq + 1, vq + 1);
+    for (int i = 1; i <= nptq; i++) {
+      double xx = xqi[i] + dt * uq[i], yy = yqi[i] + dt * vq[i];
+      xq[i] = WRAPX(xx);
+      yq[i] = WRAPY(yy);
+      xx = xqf[i] + dt3 * uq[i];
+      yy = yqf[i] + dt3 * vq[i];
+      xqf[i] = WRAPX(xx);
+      yqf[i] = WRAPY(yy);
+    }
+  }
+  for (size_t k = 0; k < nn; k++) {
+    s->qs[k] = qsi[k] + dt * sqs[k];
+    qsf[k] = qsf[k] + dt3 * sqs[k];
+    s->emq[k] = s->emq[k] * s->emq[k];
+    s->qd[k] = s->emq[k] * (qdi[k] + dt * sqd[k]);
+    qdf[k] = qdf[k] + dt3 * sqd[k];
+  }
+  /* RK4 corrector step at t0 + dt */
+  s->t = s->t + dt2;
+  o_inversion(s);
+  source(s, sqs, sqd, 2);
+  if (s->contex) {
+    o_velint(s, s->uu, s->vv, uq + 1, vq + 1);
+    for (int i = 1; i <= nptq; i++) {
+      double xx = xqf[i] + dt6 * uq[i], yy = yqf[i] + dt6 * vq[i];
+      xq[i] = WRAPX(xx);
+      yq[i] = WRAPY(yy);
+    }
+  }
+  for (size_t k = 0; k < nn; k++) {
+    s->qs[k] = qsf[k] + dt6 * sqs[k];
+    s->qd[k] = s->emq[k] * (qdf[k] + dt6 * sqd[k]);
+  }
+#undef WRAPX
+#undef WRAPY
+  free(qsi); free(qsf); free(sqs); free(qdi); free(qdf); free(sqd);
+  free(xqi); free(yqi); free(xqf); free(yqf); free(uq); free(vq);
+}
+
+/* ======================================================================
+ * Recontouring (congen.f90:24-441)
+ * ====================================================================== */
+typedef struct {
+  double *qa; /* (nyu+1, nxu) */
+  size_t ldq;
+} ugrid;
+
+#define UQA(g, iy, ix) (g)->qa[(size_t)((ix)-1) * (g)->ldq + (size_t)((iy)-1)]
+
+/* con2ugrid (congen.f90:338-441) */
+static void con2ugrid(o_state *s, ugrid *g) {
+  int nxu = s->nxu, nyu = s->nyu, nptq = s->nptq;
+  const double ellx = s->p.ellx, elly = s->p.elly, hlx = s->hlx, hly = s->hly;
+  const double hlxi = s->hlxi, hlyi = s->hlyi, xmin = s->xmin, ymin = s->ymin;
+  const double glxui = s->glxui, glyui = s->glyui, qjump = s->qjump, small = s->small;
+  double *xq = s->xq, *yq = s->yq;
+  int *nextq = s->nextq;
+  double *qjx = xcalloc(nxu + 1, sizeof(double));
+  int *ixc = xcalloc(nptq + 1, sizeof(int)), *nxc = xcalloc(nptq + 1, sizeof(int));
+  double *dx = xcalloc(nptq + 1, sizeof(double)), *dy = xcalloc(nptq + 1, sizeof(double));
+  char *crossx = xcalloc(nptq + 1, 1);
+  for (int i = 1; i <= nptq; i++) ixc[i] = f_int(glxui * (xq[i] - xmin));
+  for (int i = 1; i <= nptq; i++) {
+    int ia = nextq[i];
+    double xx = xq[ia] - xq[i];
+    dx[i] = xx - ellx * f_dint(xx * hlxi);
+    double yy = yq[ia] - yq[i];
+    dy[i] = yy - elly * f_dint(yy * hlyi);
+    int ixdif = ixc[ia] - ixc[i];
+    nxc[i] = ixdif - nxu * ((2 * ixdif) / nxu);
+    crossx[i] = nxc[i] != 0;
+    if (fabs(yy) > hly) {
+      double cc = f_sign1(dy[i]);
+      double p = -(yq[i] - hly * cc) / (dy[i] + small);
+      int ix = 1 + f_int(glxui * fmod(ellx + hlx + xq[i] + p * dx[i], ellx));
+      qjx[ix] = qjx[ix] - qjump * cc;
+    }
+  }
+  UQA(g, 1, 1) = ZERO;
+  for (int ix = 1; ix <= nxu - 1; ix++) UQA(g, 1, ix + 1) = UQA(g, 1, ix) + qjx[ix];
+  for (int ix = 1; ix <= nxu; ix++)
+    for (int iy = 2; iy <= nyu + 1; iy++) UQA(g, iy, ix) = ZERO;
+  for (int i = 1; i <= nptq; i++) {
+    if (!crossx[i]) continue;
+    int jump = f_isign1(nxc[i]);
+    int ixbeg = ixc[i] + (1 + jump) / 2 + nxu;
+    double sqjump = qjump * (double)jump;
+    int ncr = 0;
+    while (ncr != nxc[i]) {
+      int ix = 1 + (ixbeg + ncr) % nxu;
+      double xx = s->xgu[ix] - xq[i];
+      double px0 = (xx - ellx * f_dint(xx * hlxi)) / dx[i];
+      double yy = yq[i] + px0 * dy[i];
+      int iy = 2 + f_int(glyui * (yy - elly * f_dint(yy * hlyi) - ymin));
+      UQA(g, iy, ix) = UQA(g, iy, ix) + sqjump;
+      ncr = ncr + jump;
+    }
+  }
+  for (int ix = 1; ix <= nxu; ix++)
+    for (int iy = 2; iy <= nyu; iy++) UQA(g, iy, ix) = UQA(g, iy, ix) + UQA(g, iy - 1, ix);
+  double qavg = ZERO;
+  for (int ix = 1; ix <= nxu; ix++)
+    for (int iy = 1; iy <= nyu; iy++) qavg = qavg + UQA(g, iy, ix);
+  qavg = qavg / ((double)nxu * (double)nyu);
+  for (int ix = 1; ix <= nxu; ix++)
+    for (int iy = 1; iy <= nyu; iy++) UQA(g, iy, ix) = UQA(g, iy, ix) - qavg;
+  free(qjx); free(ixc); free(nxc); free(dx); free(dy); free(crossx);
+}
+
+/* ugrid2con (congen.f90:132-334).  Writes the new contours into s. */
+static int ugrid2con(o_state *s, ugrid *g) {
+  const int nxu = s->nxu, nyu = s->nyu, nlevm = s->p.nlevm;
+  const double elly = s->p.elly, ellx = s->p.ellx, hlxi = s->hlxi, hlyi = s->hlyi;
+  const double oms = s->oms, glxu = s->glxu, glyu = s->glyu, qjump = s->qjump;
+  const long long nxny = (long long)nxu * (long long)nyu;
+  int *icrtab = xcalloc((size_t)nxny * 2 + 2, sizeof(int));
+  signed char *noctab = xcalloc((size_t)nxny + 1, 1);
+  double *qdx = xcalloc(nxu + 2, sizeof(double)), *qdy = xcalloc(nyu + 2, sizeof(double));
+  int *isx = xcalloc(nxu + 2, sizeof(int)), *isy = xcalloc(nyu + 2, sizeof(int));
+  size_t crcap = 1 << 16;
+  long long *kib = xcalloc(crcap + 1, sizeof(long long));
+  double *xcr = xcalloc(crcap + 1, sizeof(double)), *ycr = xcalloc(crcap + 1, sizeof(double));
+  char *freec = xcalloc(crcap + 1, 1);
+  long npm = s->p.npm;
+  double *xa = xcalloc(npm + 2, sizeof(double)), *ya = xcalloc(npm + 2, sizeof(double));
+  size_t dcap = 1 << 16;
+  double *xd = xcalloc(dcap + 1, sizeof(double)), *yd = xcalloc(dcap + 1, sizeof(double));
+  int na = 0, npta = 0, err = 0;
+#define ICR(k, j) icrtab[(size_t)((j)-1) * (size_t)nxny + (size_t)((k)-1)]
+
+  double qjumpi = ONE / qjump;
+  double qoff = qjump * (double)nlevm;
+  double qamax = UQA(g, 1, 1), qamin = UQA(g, 1, 1);
+  for (int ix = 1; ix <= nxu; ix++)
+    for (int iy = 1; iy <= nyu; iy++) {
+      double v = UQA(g, iy, ix);
+      qamax = qamax > v ? qamax : v;
+      qamin = qamin < v ? qamin : v;
+    }
+  int levbeg = f_int((qoff + qamin) * qjumpi + F12) + 1;
+  int levend = f_int((qoff + qamax) * qjumpi + F12);
+  for (int lev = levbeg; lev <= levend && !err; lev++) {
+    int levt = lev - nlevm + (lev - 1) / nlevm - 1;
+    long ncr = 0;
+    double qtmp = ((double)lev - F12) * qjump - qoff;
+    memset(noctab, 0, (size_t)nxny + 1);
+#define ADDCR()                                                           \
+  do {                                                                    \
+    if ((size_t)ncr + 1 > crcap) {                                        \
+      crcap *= 2;                                                         \
+      kib = realloc(kib, (crcap + 1) * sizeof(long long));                \
+      xcr = realloc(xcr, (crcap + 1) * sizeof(double));                   \
+      ycr = realloc(ycr, (crcap + 1) * sizeof(double));                   \
+      freec = realloc(freec, crcap + 1);                                  \
+    }                                                                     \
+    ncr = ncr + 1;                                                        \
+  } while (0)
+    for (int ix = 1; ix <= nxu; ix++) {
+      double xgt = s->xgu[ix];
+      for (int iy = 1; iy <= nyu; iy++) {
+        qdy[iy] = UQA(g, iy, ix) - qtmp;
+        isy[iy] = (int)f_sign1(qdy[iy]);
+      }
+      qdy[nyu + 1] = qdy[1];
+      isy[nyu + 1] = isy[1];
+      for (int iy = 1; iy <= nyu; iy++) {
+        if (isy[iy] != isy[iy + 1]) {
+          ADDCR();
+          int inc = (1 - isy[iy]) / 2;
+          long long kaa = (long long)(iy - 1) * nxu + 1;
+          kib[ncr] = kaa + s->ibx[ix + inc];
+          long long kob = kaa + s->ibx[ix + 1 - inc];
+          noctab[kob] = noctab[kob] + 1;
+          ICR(kob, noctab[kob]) = (int)ncr;
+          xcr[ncr] = xgt;
+          double yy = s->ygu[iy] - glyu * qdy[iy] / (qdy[iy + 1] - qdy[iy]);
+          ycr[ncr] = oms * (yy - elly * f_dint(yy * hlyi));
+        }
+      }
+    }
+    for (int iy = 1; iy <= nyu; iy++) {
+      double ygt = s->ygu[iy];
+      for (int ix = 1; ix <= nxu; ix++) {
+        qdx[ix] = UQA(g, iy, ix) - qtmp;
+        isx[ix] = (int)f_sign1(qdx[ix]);
+      }
+      qdx[nxu + 1] = qdx[1];
+      isx[nxu + 1] = isx[1];
+      for (int ix = 1; ix <= nxu; ix++) {
+        if (isx[ix] != isx[ix + 1]) {
+          ADDCR();
+          int inc = (1 - isx[ix]) / 2;
+          kib[ncr] = (long long)nxu * s->iby[iy + 1 - inc] + ix;
+          long long kob = (long long)nxu * s->iby[iy + inc] + ix;
+          noctab[kob] = noctab[kob] + 1;
+          ICR(kob, noctab[kob]) = (int)ncr;
+          ycr[ncr] = ygt;
+          double xx = s->xgu[ix] - glxu * qdx[ix] / (qdx[ix + 1] - qdx[ix]);
+          xcr[ncr] = oms * (xx - ellx * f_dint(xx * hlxi));
+        }
+      }
+    }
+#undef ADDCR
+    for (long icr = 1; icr <= ncr; icr++) freec[icr] = 1;
+    for (long icr = 1; icr <= ncr; icr++) {
+      if (!freec[icr]) continue;
+      if (na + 1 > s->p.nm) { err = 2; break; }
+      na = na + 1;
+      s->indq[na] = levt;
+      int ibeg = npta + 1;
+      s->i1q[na] = ibeg;
+      int npd = 1;
+      xd[1] = xcr[icr];
+      yd[1] = ycr[icr];
+      long long k = kib[icr];
+      int noc = noctab[k];
+      long icrn = ICR(k, noc);
+      while (icrn != icr) {
+        noctab[k] = (signed char)(noc - 1);
+        npd = npd + 1;
+        if ((size_t)npd > dcap) {
+          dcap *= 2;
+          xd = realloc(xd, (dcap + 1) * sizeof(double));
+          yd = realloc(yd, (dcap + 1) * sizeof(double));
+        }
+        xd[npd] = xcr[icrn];
+        yd[npd] = ycr[icrn];
+        freec[icrn] = 0;
+        k = kib[icrn];
+        noc = noctab[k];
+        icrn = ICR(k, noc);
+      }
+      /* renode three times (congen.f90:295-310) */
+      int keep = 0, npa = 0;
+      long room = npm - npta;
+      do {
+        npa = renode_cap(s, xd + 1, yd + 1, npd, xa + ibeg, ya + ibeg, room);
+        if (npa <= 0) break;
+        npd = renode_cap(s, xa + ibeg, ya + ibeg, npa, xd + 1, yd + 1, (long)dcap);
+        if (npd <= 0) break;
+        npa = renode_cap(s, xd + 1, yd + 1, npd, xa + ibeg, ya + ibeg, room);
+        if (npa <= 0) break;
+        keep = 1;
+      } while (0);
+      if (npa < 0 || npd < 0) { err = 1; break; }
+      if (keep) {
+        s->npq[na] = npa;
+        npta = npta + npa;
+        int iend = ibeg + npa - 1;
+        s->i2q[na] = iend;
+        for (int i = ibeg; i <= iend - 1; i++) s->nextq[i] = i + 1;
+        s->nextq[iend] = ibeg;
+      } else {
+        na = na - 1;
+      }
+      freec[icr] = 0;
+    }
+  }
+#undef ICR
+  for (int i = 1; i <= npta; i++) {
+    s->xq[i] = xa[i];
+    s->yq[i] = ya[i];
+  }
+  s->nq = na;
+  s->nptq = npta;
+  free(icrtab); free(noctab); free(qdx); free(qdy); free(isx); free(isy); free(kib);
+  free(xcr); free(ycr); free(freec); free(xa); free(ya); free(xd); free(yd);
+  return err;
+}
+
+/* recontour (congen.f90:24-128); qq(ny,nx) is the residual (or full) field. */
+int o_recontour(o_state *s, double *qq) {
+  int nx = s->nx, ny = s->ny, nxu = s->nxu, nyu = s->nyu;
+  ugrid g;
+  g.ldq = (size_t)nyu + 1;
+  g.qa = xcalloc(g.ldq * nxu, sizeof(double));
+  if (s->nq > 0) {
+    con2ugrid(s, &g);
+    for (int ix = 1; ix <= nxu; ix++) {
+      int ixf = s->ixfw[ix], ix0 = s->ix0w[ix], ix1 = s->ix1w[ix];
+      for (int iy = 1; iy <= nyu; iy++) {
+        int iyf = s->iyfw[iy], iy0 = s->iy0w[iy], iy1 = s->iy1w[iy];
+        int w = (ixf - 1) * 16 + (iyf - 1);
+        UQA(&g, iy, ix) = UQA(&g, iy, ix) + s->w00[w] * qq[PHY(s, iy0, ix0)] +
+                          s->w10[w] * qq[PHY(s, iy1, ix0)] + s->w01[w] * qq[PHY(s, iy0, ix1)] +
+                          s->w11[w] * qq[PHY(s, iy1, ix1)];
+      }
+    }
+  } else {
+    double ql1 = 0.0;
+    for (size_t k = 0; k < (size_t)nx * ny; k++) ql1 = ql1 + fabs(qq[k]);
+    ql1 = s->garea * ql1;
+    if (ql1 < s->small) {
+      free(g.qa);
+      s->nq = 0;
+      s->nptq = 0;
+      return 0;
+    }
+    if (s->beffect) {
+      for (int ix = 1; ix <= nx; ix++)
+        for (int iy = 1; iy <= ny; iy++)
+          qq[PHY(s, iy, ix)] = qq[PHY(s, iy, ix)] - s->p.beta * (s->ymin + s->gly * (double)(iy - 1));
+    }
+    for (int ix = 1; ix <= nxu; ix++) {
+      int ixf = s->ixfw[ix], ix0 = s->ix0w[ix], ix1 = s->ix1w[ix];
+      for (int iy = 1; iy <= nyu; iy++) {
+        int iyf = s->iyfw[iy], iy0 = s->iy0w[iy], iy1 = s->iy1w[iy];
+        int w = (ixf - 1) * 16 + (iyf - 1);
+        UQA(&g, iy, ix) = s->w00[w] * qq[PHY(s, iy0, ix0)] + s->w10[w] * qq[PHY(s, iy1, ix0)] +
+                          s->w01[w] * qq[PHY(s, iy0, ix1)] + s->w11[w] * qq[PHY(s, iy1, ix1)];
+      }
+    }
+    if (s->beffect) {
+      for (int ix = 1; ix <= nxu; ix++)
+        for (int iy = 1; iy <= nyu; iy++) UQA(&g, iy, ix) = UQA(&g, iy, ix) + s->p.beta * s->ygu[iy];
+    }
+  }
+  int err = ugrid2con(s, &g);
+  free(g.qa);
+  s->contex = s->nptq > 0;
+  return err;
+}
+
+/* ======================================================================
+ * Driver (caps.f90 / evolution.f90)
+ * ====================================================================== */
+/* init (evolution.f90:96-131) */
+static void evo_init(o_state *s) {
+  size_t nn = (size_t)s->nx * s->ny;
+  s->contex = s->nptq > 0;
+  double *qa = xcalloc(nn, sizeof(double));
+  o_con2grid(s, qa, NULL);
+  o_ptospc(s, qa, s->qc);
+  for (size_t k = 0; k < nn; k++) {
+    s->qd[k] = s->fhi[k] * (s->qs[k] - s->qc[k]);
+    s->qspre[k] = s->qs[k];
+  }
+  free(qa);
+}
+
+/* prepare (evolution.f90:135-162) */
+static void evo_prepare(o_state *s) {
+  size_t nn = (size_t)s->nx * s->ny;
+  double *qa = xcalloc(nn, sizeof(double));
+  o_con2grid(s, qa, NULL);
+  o_ptospc(s, qa, s->qc);
+  for (size_t k = 0; k < nn; k++) {
+    s->qs[k] = s->flo[k] * (s->qs[k] - s->qc[k]) + s->qc[k] + s->qd[k];
+    s->qd[k] = s->qs[k] - s->qc[k];
+  }
+  memcpy(qa, s->qd, nn * sizeof(double));
+  o_spctop(s, qa, s->qr);
+  free(qa);
+}
+
+int o_initialise(o_state *s, const double *qq_init) {
+  size_t nn = (size_t)s->nx * s->ny;
+  s->t = 0.0;
+  s->tinit = 0.0;
+  memcpy(s->qr, qq_init, nn * sizeof(double));
+  if (s->beffect) {
+    for (int ix = 1; ix <= s->nx; ix++)
+      for (int iy = 1; iy <= s->ny; iy++) s->qr[PHY(s, iy, ix)] -= s->bety[iy - 1];
+    s->qjump = s->p.beta * s->p.elly / (double)s->p.ncontq;
+  } else {
+    double mx = s->qr[0], mn = s->qr[0];
+    for (size_t k = 0; k < nn; k++) {
+      mx = s->qr[k] > mx ? s->qr[k] : mx;
+      mn = s->qr[k] < mn ? s->qr[k] : mn;
+    }
+    s->qjump = (mx - mn) / (double)s->p.ncontq;
+  }
+  double *ff = xcalloc(nn, sizeof(double));
+  memcpy(ff, s->qr, nn * sizeof(double));
+  o_ptospc(s, ff, s->qs);
+  free(ff);
+  s->nq = 0;
+  s->nptq = 0;
+  s->dt = 0.0;
+  s->dtmax = 0.0;
+  /* recont + evolution init */
+  int err = o_recontour(s, s->qr);
+  if (err) return err;
+  evo_init(s);
+  s->twist = 0.0;
+  s->ireg = 0;
+  return 0;
+}
+
+static int nodes_ok(o_state *s) {
+  for (int i = 1; i <= s->nptq; i++) {
+    double x = s->xq[i], y = s->yq[i];
+    if (!(x >= s->xmin && x < s->xmax && y >= s->ymin && y < s->ymax)) return 0;
+  }
+  return 1;
+}
+
+int o_step(o_state *s) {
+  int force = s->p.force_surgery;
+  if (!nodes_ok(s)) return 4;
+  if (force || s->twist > s->p.twistmax) {
+    s->ireg = s->ireg + 1;
+    if (s->ireg == s->p.nregmax) {
+      evo_prepare(s);
+      int err = o_recontour(s, s->qr);
+      if (err) return err;
+      evo_init(s);
+      s->twist = 0.0;
+      s->ireg = 0;
+      if (force || s->twist > s->p.twistmax) {
+        s->ireg = s->ireg + 1;
+        if (o_surgery(s)) return 3;
+        s->twist = s->twist - s->p.twistmax;
+      }
+    } else {
+      if (o_surgery(s)) return 3;
+      s->twist = s->twist - s->p.twistmax;
+    }
+  }
+  o_advance(s);
+  return nodes_ok(s) ? 0 : 4;
+}
+
+/* ======================================================================
+ * Diagnostics
+ * ====================================================================== */
+void o_diagnostics(o_state *s, double *out) {
+  size_t nn = (size_t)s->nx * s->ny;
+  double ek = 0.0;
+  for (size_t k = 0; k < nn; k++) ek = ek + (s->uu[k] * s->uu[k] + s->vv[k] * s->vv[k]);
+  ek = F12 * s->garea * ek;
+  double ep = 0.0;
+  double *ss = xcalloc(nn, sizeof(double)), *zz = xcalloc(nn, sizeof(double));
+  if (!s->btropic) {
+    memcpy(ss, s->pp, nn * sizeof(double));
+    o_spctop(s, ss, zz);
+    for (size_t k = 0; k < nn; k++) ep = ep + zz[k] * zz[k];
+    ep = F12 * s->garea * s->kdsq * ep;
+  }
+  memcpy(ss, s->qq, nn * sizeof(double));
+  o_spctop(s, ss, zz);
+  double l2 = 0.0;
+  for (size_t k = 0; k < nn; k++) l2 = l2 + zz[k] * zz[k];
+  l2 = s->garea * l2;
+  /* Circulation carried by the contours: qjump times the signed area
+   * enclosed by every contour (shoelace over periodic increments). */
+  double circ = 0.0;
+  for (int j = 1; j <= s->nq; j++) {
+    int i0 = s->i1q[j], i = i0;
+    double x = 0.0, y = 0.0, a = 0.0;
+    do {
+      int ia = s->nextq[i];
+      double xx = s->xq[ia] - s->xq[i];
+      double ddx = xx - s->p.ellx * f_dint(xx * s->hlxi);
+      double yy = s->yq[ia] - s->yq[i];
+      double ddy = yy - s->p.elly * f_dint(yy * s->hlyi);
+      a = a + (x * ddy - y * ddx);
+      x = x + ddx;
+      y = y + ddy;
+      i = ia;
+    } while (i != i0);
+    circ = circ + F12 * a;
+  }
+  circ = s->qjump * circ;
+  out[0] = ek;
+  out[1] = ep;
+  out[2] = l2;
+  out[3] = circ;
+  free(ss);
+  free(zz);
+}
