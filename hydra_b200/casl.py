@@ -1,0 +1,263 @@
+"""Host-side mirror of Hydra's QG caps module interface over the CUDA C-ABI.
+
+``CaslGPU`` holds one simulation on one GPU and exposes the reference's
+module procedures under their reference names (``con2grid``, ``velint``,
+``main_invert``, ``gradient``, ``inversion``, ``advance``, ``surgery``,
+``renode``, ``recontour``, ``ptospc``, ``spctop``) plus the driver loop of
+caps.f90 (``initialise``, ``step``).  Every call goes through
+``libhydra_casl.so`` (include/hydra_casl.h); there is no CPU fallback: if the
+library or a GPU is missing, construction raises.
+
+Array convention: a physical field q(ny,nx) is an (nx, ny) C-contiguous
+float64 array indexed [ix-1, iy-1]; a spectral field s(nx,ny) is (ny, nx)
+indexed [ky-1, kx-1]; contour index arrays are 1-based as in the reference.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libhydra_casl.so")
+
+CASL_OK, CASL_EINVAL, CASL_ECAPACITY, CASL_ECUDA, CASL_ENOMEM, CASL_EDOMAIN, CASL_ETIMEOUT, \
+    CASL_EUNSUPPORTED = range(8)
+
+FIELDS = {"qs": 0, "qd": 1, "qc": 2, "qq": 3, "pp": 4, "qspre": 5, "emq": 6, "epq": 7,
+          "uu": 8, "vv": 9, "qr": 10}
+SCALARS = {"t": 0, "dt": 1, "twist": 2, "ireg": 3, "zzrms": 4, "zzmax": 5, "uumax": 6, "qjump": 7}
+
+
+class CaslError(RuntimeError):
+    def __init__(self, code: int, where: str, msg: str):
+        super().__init__(f"{where}: {msg} (code {code})")
+        self.code = code
+
+
+class CaslParams(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int), ("ny", C.c_int), ("ncontq", C.c_int),
+        ("ellx", C.c_double), ("elly", C.c_double), ("kd", C.c_double), ("beta", C.c_double),
+        ("rtherm", C.c_double), ("rekman", C.c_double), ("cdamp", C.c_double), ("nnu", C.c_double),
+        ("npm", C.c_longlong), ("nm", C.c_longlong), ("nlevm", C.c_int),
+        ("fixed_dt", C.c_double), ("dtmax", C.c_double), ("force_surgery", C.c_int),
+        ("nregmax", C.c_int), ("twistmax", C.c_double),
+    ]
+
+
+_lib = None
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+# name -> (restype, argtypes); the same list is checked against the header by tests
+SIGNATURES = {
+    "casl_create": (C.c_int, [C.POINTER(CaslParams), C.c_int, C.POINTER(C.c_void_p)]),
+    "casl_destroy": (None, [C.c_void_p]),
+    "casl_error_string": (C.c_char_p, [C.c_int]),
+    "casl_last_cuda_error": (C.c_int, [C.c_void_p]),
+    "casl_synchronize": (C.c_int, [C.c_void_p]),
+    "casl_set_contours": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_double, _dp, _dp, _ip, _ip, _ip, _ip, _ip]),
+    "casl_get_counts": (C.c_int, [C.c_void_p, _ip, _ip, _dp]),
+    "casl_get_contours": (C.c_int, [C.c_void_p, _dp, _dp, _ip, _ip, _ip, _ip, _ip]),
+    "casl_set_field": (C.c_int, [C.c_void_p, C.c_int, _dp]),
+    "casl_get_field": (C.c_int, [C.c_void_p, C.c_int, _dp]),
+    "casl_get_scalar": (C.c_int, [C.c_void_p, C.c_int, _dp]),
+    "casl_set_scalar": (C.c_int, [C.c_void_p, C.c_int, C.c_double]),
+    "casl_ptospc": (C.c_int, [C.c_void_p, _dp, _dp]),
+    "casl_spctop": (C.c_int, [C.c_void_p, _dp, _dp]),
+    "casl_con2grid": (C.c_int, [C.c_void_p, _dp, _ip]),
+    "casl_velint": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
+    "casl_main_invert": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
+    "casl_gradient": (C.c_int, [C.c_void_p, _dp, _dp, _dp]),
+    "casl_inversion": (C.c_int, [C.c_void_p]),
+    "casl_advance": (C.c_int, [C.c_void_p]),
+    "casl_surgery": (C.c_int, [C.c_void_p]),
+    "casl_renode": (C.c_int, [C.c_void_p, _dp, _dp, C.c_int, _dp, _dp, C.c_int, _ip]),
+    "casl_recontour": (C.c_int, [C.c_void_p, _dp]),
+    "casl_initialise": (C.c_int, [C.c_void_p, _dp]),
+    "casl_step": (C.c_int, [C.c_void_p, C.c_int]),
+    "casl_diagnostics": (C.c_int, [C.c_void_p, _dp]),
+}
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libhydra_casl.so (raises OSError if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(path):
+            raise OSError(f"hydra_b200: CUDA library not built ({path}); run hydra_b200/build.py")
+        lib = C.CDLL(path)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp) if a is not None else None
+
+
+def _i(a):
+    return a.ctypes.data_as(_ip) if a is not None else None
+
+
+def _f64(a, shape=None):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if shape is not None and a.shape != shape:
+        raise ValueError(f"expected shape {shape}, got {a.shape}")
+    return a
+
+
+class CaslGPU:
+    """One contour-advection simulation resident on one GPU."""
+
+    def __init__(self, nx, ncontq=40, ellx=2 * np.pi, elly=None, kd=0.0, beta=0.0, rtherm=0.0,
+                 rekman=0.0, cdamp=2.0, nnu=3.0, npm=None, nm=0, nlevm=2000, fixed_dt=0.0,
+                 dtmax=0.05, force_surgery=0, nregmax=20, twistmax=2.5, device=0):
+        self.lib = load_library()
+        elly = ellx if elly is None else elly
+        if npm is None:
+            npm = 60 * nx * nx
+        self.p = CaslParams(nx, nx, ncontq, ellx, elly, kd, beta, rtherm, rekman, cdamp, nnu,
+                            int(npm), int(nm), nlevm, fixed_dt, dtmax, force_surgery, nregmax,
+                            twistmax)
+        h = C.c_void_p()
+        self._check(self.lib.casl_create(C.byref(self.p), device, C.byref(h)), "casl_create")
+        self.h = h
+        self.nx = self.ny = nx
+
+    def _check(self, rc, where):
+        if rc != CASL_OK:
+            msg = self.lib.casl_error_string(rc).decode()
+            raise CaslError(rc, where, msg)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.casl_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # --- state ------------------------------------------------------------------
+    def field(self, name):
+        shape = (self.nx, self.ny)
+        out = np.empty(shape)
+        self._check(self.lib.casl_get_field(self.h, FIELDS[name], _d(out)), "casl_get_field")
+        return out
+
+    def set_field(self, name, arr):
+        a = _f64(arr, (self.nx, self.ny))
+        self._check(self.lib.casl_set_field(self.h, FIELDS[name], _d(a)), "casl_set_field")
+
+    def scalar(self, name):
+        v = C.c_double()
+        self._check(self.lib.casl_get_scalar(self.h, SCALARS[name], C.byref(v)), "casl_get_scalar")
+        return v.value
+
+    def set_scalar(self, name, value):
+        self._check(self.lib.casl_set_scalar(self.h, SCALARS[name], float(value)), "casl_set_scalar")
+
+    def counts(self):
+        nq, npt, qj = C.c_int(), C.c_int(), C.c_double()
+        self._check(self.lib.casl_get_counts(self.h, C.byref(nq), C.byref(npt), C.byref(qj)),
+                    "casl_get_counts")
+        return nq.value, npt.value, qj.value
+
+    def contours(self):
+        nq, npt, qj = self.counts()
+        xq = np.zeros(npt); yq = np.zeros(npt); nextq = np.zeros(npt, np.int32)
+        indq = np.zeros(nq, np.int32); npq = np.zeros(nq, np.int32)
+        i1q = np.zeros(nq, np.int32); i2q = np.zeros(nq, np.int32)
+        self._check(self.lib.casl_get_contours(self.h, _d(xq), _d(yq), _i(nextq), _i(indq), _i(npq),
+                                               _i(i1q), _i(i2q)), "casl_get_contours")
+        return dict(nq=nq, nptq=npt, qjump=qj, xq=xq, yq=yq, nextq=nextq, indq=indq, npq=npq,
+                    i1q=i1q, i2q=i2q)
+
+    def set_contours(self, c):
+        xq = _f64(c["xq"]); yq = _f64(c["yq"])
+        nextq = np.ascontiguousarray(c["nextq"], np.int32)
+        indq = np.ascontiguousarray(c["indq"], np.int32); npq = np.ascontiguousarray(c["npq"], np.int32)
+        i1q = np.ascontiguousarray(c["i1q"], np.int32); i2q = np.ascontiguousarray(c["i2q"], np.int32)
+        self._check(self.lib.casl_set_contours(self.h, len(indq), len(xq), float(c["qjump"]), _d(xq),
+                                               _d(yq), _i(nextq), _i(indq), _i(npq), _i(i1q), _i(i2q)),
+                    "casl_set_contours")
+
+    # --- module procedures ------------------------------------------------------------
+    def ptospc(self, q):
+        a = _f64(q, (self.nx, self.ny)); out = np.empty((self.ny, self.nx))
+        self._check(self.lib.casl_ptospc(self.h, _d(a), _d(out)), "casl_ptospc")
+        return out
+
+    def spctop(self, s):
+        a = _f64(s, (self.ny, self.nx)); out = np.empty((self.nx, self.ny))
+        self._check(self.lib.casl_spctop(self.h, _d(a), _d(out)), "casl_spctop")
+        return out
+
+    def con2grid(self, levels=False):
+        qc = np.empty((self.nx, self.ny))
+        lv = np.empty((4 * self.nx, 4 * self.ny), np.int32) if levels else None
+        self._check(self.lib.casl_con2grid(self.h, _d(qc), _i(lv)), "casl_con2grid")
+        return (qc, lv) if levels else qc
+
+    def velint(self, uu, vv):
+        _, npt, _ = self.counts()
+        uu = _f64(uu, (self.nx, self.ny)); vv = _f64(vv, (self.nx, self.ny))
+        uq = np.empty(npt); vq = np.empty(npt)
+        self._check(self.lib.casl_velint(self.h, _d(uu), _d(vv), _d(uq), _d(vq)), "casl_velint")
+        return uq, vq
+
+    def main_invert(self, qq):
+        qq = _f64(qq, (self.ny, self.nx))
+        uu = np.empty((self.nx, self.ny)); vv = np.empty((self.nx, self.ny)); pp = np.empty((self.ny, self.nx))
+        self._check(self.lib.casl_main_invert(self.h, _d(qq), _d(uu), _d(vv), _d(pp)), "casl_main_invert")
+        return uu, vv, pp
+
+    def gradient(self, ff):
+        ff = _f64(ff, (self.ny, self.nx))
+        fx = np.empty((self.nx, self.ny)); fy = np.empty((self.nx, self.ny))
+        self._check(self.lib.casl_gradient(self.h, _d(ff), _d(fx), _d(fy)), "casl_gradient")
+        return fx, fy
+
+    def inversion(self):
+        self._check(self.lib.casl_inversion(self.h), "casl_inversion")
+
+    def advance(self):
+        self._check(self.lib.casl_advance(self.h), "casl_advance")
+
+    def surgery(self):
+        self._check(self.lib.casl_surgery(self.h), "casl_surgery")
+
+    def renode(self, xd, yd):
+        xd = _f64(xd); yd = _f64(yd)
+        cap = 8 * len(xd) + 64
+        xr = np.empty(cap); yr = np.empty(cap); npr = C.c_int()
+        self._check(self.lib.casl_renode(self.h, _d(xd), _d(yd), len(xd), _d(xr), _d(yr), cap,
+                                         C.byref(npr)), "casl_renode")
+        return xr[:npr.value], yr[:npr.value]
+
+    def recontour(self, qq):
+        qq = _f64(qq, (self.nx, self.ny))
+        self._check(self.lib.casl_recontour(self.h, _d(qq)), "casl_recontour")
+
+    def initialise(self, q0):
+        q0 = _f64(q0, (self.nx, self.ny))
+        self._check(self.lib.casl_initialise(self.h, _d(q0)), "casl_initialise")
+
+    def step(self, nsteps=1):
+        self._check(self.lib.casl_step(self.h, int(nsteps)), "casl_step")
+
+    def synchronize(self):
+        self._check(self.lib.casl_synchronize(self.h), "casl_synchronize")
+
+    def diagnostics(self):
+        out = np.zeros(4)
+        self._check(self.lib.casl_diagnostics(self.h, _d(out)), "casl_diagnostics")
+        return dict(ekin=out[0], epot=out[1], enstrophy=out[2], circulation=out[3])

@@ -1,0 +1,1584 @@
+// B200 contour-advection time step: handle, tables, transforms, con2grid,
+// node advection, spectral source terms, adapt and the RK4 advance.
+//
+// Reference: basic_hydra/ca/plane/qg/caps (Fortran 90).  File:line citations
+// name the reference procedure each piece restates.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+#include "common.cuh"
+#include "fft.cuh"
+#include "state.cuh"
+
+using namespace casl;
+
+namespace casl {
+
+int set_cuda_error(casl_handle *h, cudaError_t e) {
+  if (h) h->last_cuda = (int)e;
+  cudaGetLastError();  // clear sticky non-fatal error state
+  if (e == cudaErrorMemoryAllocation) return CASL_ENOMEM;
+  return CASL_ECUDA;
+}
+
+int check_launch(casl_handle *h) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_cuda_error(h, e);
+  return CASL_OK;
+}
+
+static int ilog2(int n) {
+  int l = 0;
+  while ((1 << l) < n) l++;
+  return l;
+}
+
+// ---------------------------------------------------------------------------
+// Transform launches
+// ---------------------------------------------------------------------------
+template <int V, bool FWD, bool LVF, bool SVF, class LD, class ST>
+static int launch_rfft(casl_handle *h, LD ld, ST st, int batch) {
+  int n = h->n;
+  size_t sm = rfft_smem_bytes(V, n);
+  auto kern = k_rfft<V, FWD, LVF, SVF, LD, ST>;
+  static bool configured = false;  // one per template instance
+  if (!configured) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    configured = true;
+  }
+  dim3 grid(n / V, batch);
+  kern<<<grid, 256, sm, h->stream>>>(ld, st, h->tw, n, ilog2(n / 2));
+  return check_launch(h);
+}
+
+// Vectors per CTA: keep >= ~2 CTAs per SM at every size while the shared
+// tile (2 buffers) stays well inside 227 KB.
+#define RFFT_DISPATCH(FWD, LVF, SVF, ld, st, batch)                        \
+  (h->n >= 2048 ? launch_rfft<2, FWD, LVF, SVF>(h, ld, st, batch)          \
+                : launch_rfft<4, FWD, LVF, SVF>(h, ld, st, batch))
+
+int ptospc_dev(casl_handle *h, const double *phys, double *spec) {
+  long long n = h->n, nn = n * n;
+  // pass A: along ix for each iy; phys[ix*n+iy] -> spec[iy*n+kx] (transposed)
+  int rc = RFFT_DISPATCH(true, true, false, (LoadStrided{phys, nn, 1, n}),
+                         (StoreStrided{spec, nn, n, 1}), 1);
+  if (rc) return rc;
+  // pass B: along iy for each kx, in place: spec[j*n + kx]
+  return RFFT_DISPATCH(true, true, true, (LoadStrided{spec, nn, 1, n}),
+                       (StoreStrided{spec, nn, 1, n}), 1);
+}
+
+int spctop_dev(casl_handle *h, const double *spec, double *phys, double *tmp) {
+  long long n = h->n, nn = n * n;
+  int rc = RFFT_DISPATCH(false, true, true, (LoadStrided{spec, nn, 1, n}),
+                         (StoreStrided{tmp, nn, 1, n}), 1);
+  if (rc) return rc;
+  return RFFT_DISPATCH(false, false, true, (LoadStrided{tmp, nn, n, 1}),
+                       (StoreStrided{phys, nn, 1, n}), 1);
+}
+
+// ---------------------------------------------------------------------------
+// Fused load / store functors
+// ---------------------------------------------------------------------------
+
+// Element (v = kx-1, j = ky-1) of xderiv / yderiv (sta2dfft.f90:169-245) of
+// a spectral field, optionally of green*field (main_invert, spectral.f90:321).
+// Batch index b selects field and direction.
+struct LoadDeriv {
+  const double *f[4];
+  int dir[4];  // 0: d/dx, 1: d/dy
+  const double *green;
+  const double *hrkx, *hrky;
+  int n;
+  __device__ __forceinline__ double base(int b, int kx0, int ky0) const {
+    long long k = (long long)ky0 * n + kx0;
+    double v = f[b][k];
+    return green ? green[k] * v : v;
+  }
+  __device__ __forceinline__ double operator()(int b, int v, int j) const {
+    const int nw = n >> 1;
+    if (dir[b] == 0) {
+      if (v == 0 || v == nw) return 0.0;
+      if (v < nw) return -hrkx[2 * v - 1] * base(b, n - v, j);
+      return hrkx[2 * (n - v) - 1] * base(b, n - v, j);
+    } else {
+      if (j == 0 || j == nw) return 0.0;
+      if (j < nw) return -hrky[2 * j - 1] * base(b, v, n - j);
+      return hrky[2 * (n - j) - 1] * base(b, v, n - j);
+    }
+  }
+};
+
+// qa(iy,ix) of con2grid from the exact integer coarse cells:
+// qc = qjump*(C*n^2 - S)/(256 n^2) (+ beta field), phys layout [ix][iy].
+struct LoadQC {
+  const int *C;
+  const Scalars *s;
+  const double *betac;  // nullable
+  long long nn;
+  double inv;           // 1/(256 n^2)
+  int n;
+  __device__ __forceinline__ double operator()(int b, int v /*iy*/, int j /*ix*/) const {
+    long long k = (long long)j * n + v;
+    long long num = (long long)C[k] * nn - s->csum;
+    double q = s->qjump * ((double)num * inv);
+    if (betac) q = q + betac[v];
+    return q;
+  }
+};
+
+// Advection product -u*fx - v*(fy [+ beta]) of evolution.f90:449,456-461,
+// read from physical arrays ([ix][iy]); b = 0 for qd, 1 for qs.
+struct LoadAdvect {
+  const double *uu, *vv;
+  const double *fx[2], *fy[2];
+  double betab[2];  // beta added to fy for the qs term when beffect
+  int n;
+  __device__ __forceinline__ double operator()(int b, int v /*iy*/, int j /*ix*/) const {
+    long long k = (long long)j * n + v;
+    double gx = fx[b][k], gy = fy[b][k];
+    if (betab[b] != 0.0) gy = gy + betab[b];
+    return -uu[k] * gx - vv[k] * gy;
+  }
+};
+
+// Store of the source terms after ptospc pass B (evolution.f90:466-487):
+// b = 0 -> sqd with damping and the integrating factor, b = 1 -> sqs.
+struct StoreSource {
+  double *sqd, *sqs;
+  const double *qq, *pp, *epq;
+  double rekman, kdsq, therm;
+  int heating, friction, lev, n;
+  __device__ __forceinline__ void operator()(int b, int v /*kx*/, int k /*ky*/, double x) const {
+    long long idx = (long long)k * n + v;
+    if (b == 1) {
+      sqs[idx] = x;
+      return;
+    }
+    double t;
+    if (heating) {
+      if (friction)
+        t = x + therm * (pp[idx] - 0.0) - rekman * (qq[idx] + kdsq * pp[idx]);
+      else
+        t = x + therm * (pp[idx] - 0.0);
+    } else {
+      t = x - rekman * (qq[idx] + kdsq * pp[idx]);
+    }
+    if (lev == 1)
+      t = epq[idx] * t;
+    else if (lev == 2)
+      t = epq[idx] * epq[idx] * t;
+    sqd[idx] = t;
+  }
+};
+
+struct StoreScaled {
+  double *p[4];
+  double scale[4];
+  int n;
+  __device__ __forceinline__ void operator()(int b, int v, int k, double x) const {
+    p[b][(long long)k * n + v] = scale[b] == 1.0 ? x : scale[b] * x;
+  }
+};
+struct LoadBatch {
+  const double *p[4];
+  long long vs, es;
+  __device__ __forceinline__ double operator()(int b, int v, int j) const {
+    return p[b][(long long)v * vs + (long long)j * es];
+  }
+};
+// Load qq + kdsq*pp (adapt, evolution.f90:541-547).
+struct LoadVort {
+  const double *qq, *pp;
+  double kdsq;
+  int btropic, n;
+  __device__ __forceinline__ double operator()(int b, int v, int j) const {
+    long long k = (long long)j * n + v;
+    return btropic ? qq[k] : qq[k] + kdsq * pp[k];
+  }
+};
+
+// ---------------------------------------------------------------------------
+// con2grid (contours.f90:173-346)
+// ---------------------------------------------------------------------------
+// Per segment (i, nextq(i)): x fine-grid-line crossings and the crossing of
+// y = ymin, counted as +-1 PV jumps.  The FP64 expressions are the
+// reference's, evaluated in its order without FMA, so every crossing lands
+// in the same fine cell.
+__global__ void k_c2g_scatter(const double *__restrict__ xq, const double *__restrict__ yq,
+                              const int *__restrict__ nextq, const Scalars *__restrict__ s,
+                              int *__restrict__ J, int *__restrict__ ljx, Consts c,
+                              int *__restrict__ err) {
+  int npt = s->nptq;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npt; i += gridDim.x * blockDim.x) {
+    int ia = nextq[i];
+    if (ia < 0 || ia >= npt) { atomicExch(err, CASL_EINVAL); continue; }
+    double xi = xq[i], yi = yq[i], xa = xq[ia], ya = yq[ia];
+    if (!(xi >= c.xmin && xi < c.xmax && yi >= c.ymin && yi < c.ymax)) {
+      atomicExch(err, CASL_EDOMAIN);
+      continue;
+    }
+    int ixci = 1 + f_int(c.glxfi * (xi - c.xmin));
+    int ixca = 1 + f_int(c.glxfi * (xa - c.xmin));
+    double xx = xa - xi;
+    double dx = xx - c.ellx * f_dint(xx * c.hlxi);
+    double yy = ya - yi;
+    double dy = yy - c.elly * f_dint(yy * c.hlyi);
+    int ixdif = ixca - ixci;
+    int nxc = ixdif - c.nxf * ((2 * ixdif) / c.nxf);
+    if (fabs(yy) > c.hly) {
+      double cc = f_sign1(dy);
+      double p = -(yi - c.hly * cc) / (dy + c.small);
+      int ix = 1 + f_int(c.glxfi * fmod(c.ellx + c.hlx + xi + p * dx, c.ellx));
+      ix = ix < 1 ? 1 : (ix > c.nxf ? c.nxf : ix);
+      atomicAdd(&ljx[ix - 1], -(int)cc);
+    }
+    if (nxc != 0 && nxc >= -c.nxf && nxc <= c.nxf) {
+      int jump = f_isign1(nxc);
+      int ixbeg = ixci + (jump - 1) / 2 + c.nxf;
+      int sgn = (int)f_sign1(dx);
+      for (int ncr = 0; ncr != nxc; ncr += jump) {
+        int m = (ixbeg + ncr) % c.nxf;
+        if (m < 0) m += c.nxf;
+        int ix = 1 + m;
+        double xgf = c.xmin + c.glxf * (double)(ix - 1);
+        double x2 = xgf - xi;
+        double px0 = (x2 - c.ellx * f_dint(x2 * c.hlxi)) / dx;
+        double y2 = yi + px0 * dy;
+        int iy = 2 + f_int(c.glyfi * (y2 - c.elly * f_dint(y2 * c.hlyi) - c.ymin));
+        if (iy >= 2 && iy <= c.nyf) atomicAdd(&J[(long long)(ix - 1) * c.nyf + (iy - 1)], sgn);
+      }
+    }
+  }
+}
+
+// qbot: exclusive prefix of the bottom jumps along x -> row 0 of each column.
+__global__ void k_c2g_lbot(const int *__restrict__ ljx, int *__restrict__ J, int nxf, int nyf) {
+  __shared__ int warp_tot[32];
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int base = 0; base < nxf; base += blockDim.x) {
+    int i = base + threadIdx.x;
+    int v = i < nxf ? ljx[i] : 0;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_tot[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+      int t = lane < nw ? warp_tot[lane] : 0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, t, o);
+        if (lane >= o) t += y;
+      }
+      if (lane < nw) warp_tot[lane] = t;
+    }
+    __syncthreads();
+    int incl = x + (wid > 0 ? warp_tot[wid - 1] : 0) + carry;
+    if (i < nxf) J[(long long)i * nyf] = incl - v;  // exclusive: lbot(ix)
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) carry = incl;
+    __syncthreads();
+  }
+}
+
+// Inclusive scan down every fine column (contours.f90:272-277), in place:
+// J(row, col) -> level L(iy = row+1, ix = col+1).  One warp per column.
+__global__ void k_c2g_colscan(int *__restrict__ J, int nxf, int nyf) {
+  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (warp >= nxf) return;
+  int *col = J + (long long)warp * nyf;
+  int carry = 0;
+  for (int base = 0; base < nyf; base += 32) {
+    int x = col[base + lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    x += carry;
+    col[base + lane] = x;
+    carry = __shfl_sync(0xffffffffu, x, 31);
+  }
+}
+
+// Two nine-point 2:1 averagings (contours.f90:290-327) compose to a 7x7
+// stencil with weights [1,2,3,4,3,2,1]^2/256 on fine rows/columns
+// 4i-6..4i (1-based, periodic).  Levels are integers, so the coarse cell is
+// the exact integer C; the mean is removed exactly from the integer sum.
+__global__ void k_c2g_coarsen(const int *__restrict__ L, int *__restrict__ C,
+                              unsigned long long *__restrict__ csum, int n, int nf) {
+  const int w7[7] = {1, 2, 3, 4, 3, 2, 1};
+  long long local = 0;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)n * n;
+       t += (long long)gridDim.x * blockDim.x) {
+    int iy = (int)(t % n) + 1, ix = (int)(t / n) + 1;
+    int acc = 0;
+#pragma unroll
+    for (int b = 0; b < 7; b++) {
+      int fx = 4 * ix - 6 + b;
+      if (fx <= 0) fx += nf;
+      const int *col = L + (long long)(fx - 1) * nf;
+      int accy = 0;
+#pragma unroll
+      for (int a = 0; a < 7; a++) {
+        int fy = 4 * iy - 6 + a;
+        if (fy <= 0) fy += nf;
+        accy += w7[a] * col[fy - 1];
+      }
+      acc += w7[b] * accy;
+    }
+    C[t] = acc;
+    local += acc;
+  }
+  // block reduction of the integer sum (order-independent: exact)
+  __shared__ long long red[32];
+  for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xffffffffu, local, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = local;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    long long v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (threadIdx.x == 0) atomicAdd(csum, (unsigned long long)v);
+  }
+}
+
+__global__ void k_zero_csum(Scalars *s) { s->csum = 0; }
+
+__global__ void k_c2g_final(const int *__restrict__ C, const Scalars *__restrict__ s,
+                            const double *__restrict__ betac, double *__restrict__ qc, int n) {
+  LoadQC ld{C, s, betac, (long long)n * n, 1.0 / (256.0 * (double)n * (double)n), n};
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)n * n;
+       t += (long long)gridDim.x * blockDim.x) {
+    int iy = (int)(t % n), ix = (int)(t / n);
+    qc[t] = ld(0, iy, ix);
+  }
+}
+
+static int grid_for(long long work, int block = 256) {
+  long long g = (work + block - 1) / block;
+  if (g < 1) g = 1;
+  if (g > 148 * 16) g = 148 * 16;
+  return (int)g;
+}
+
+int con2grid_dev(casl_handle *h) {
+  const Consts &c = h->c;
+  size_t fine = (size_t)c.nxf * c.nyf;
+  CASL_CUDA_TRY(cudaMemsetAsync(h->fineJ, 0, fine * sizeof(int), h->stream));
+  CASL_CUDA_TRY(cudaMemsetAsync(h->ljx, 0, (size_t)c.nxf * sizeof(int), h->stream));
+  k_zero_csum<<<1, 1, 0, h->stream>>>(h->scal);
+  int *err = &h->scal->error;
+  if (h->nptq > 0)
+    k_c2g_scatter<<<grid_for(h->nptq), 256, 0, h->stream>>>(h->xq, h->yq, h->nextq, h->scal,
+                                                              h->fineJ, h->ljx, c, err);
+  k_c2g_lbot<<<1, 1024, 0, h->stream>>>(h->ljx, h->fineJ, c.nxf, c.nyf);
+  k_c2g_colscan<<<(c.nxf * 32 + 255) / 256, 256, 0, h->stream>>>(h->fineJ, c.nxf, c.nyf);
+  k_c2g_coarsen<<<grid_for((long long)h->n * h->n), 256, 0, h->stream>>>(
+      h->fineJ, h->coarseC, (unsigned long long *)&h->scal->csum, h->n, c.nxf);
+  return check_launch(h);
+}
+
+int con2grid_to_spec(casl_handle *h, double *spec) {
+  long long n = h->n, nn = n * n;
+  if (h->nptq == 0) {
+    CASL_CUDA_TRY(cudaMemsetAsync(spec, 0, nn * sizeof(double), h->stream));
+    return CASL_OK;
+  }
+  int rc = con2grid_dev(h);
+  if (rc) return rc;
+  LoadQC ld{h->coarseC, h->scal, h->c.beffect ? h->betac : nullptr, nn,
+            1.0 / (256.0 * (double)n * (double)n), (int)n};
+  rc = RFFT_DISPATCH(true, true, false, ld, (StoreStrided{spec, nn, n, 1}), 1);
+  if (rc) return rc;
+  return RFFT_DISPATCH(true, true, true, (LoadStrided{spec, nn, 1, n}),
+                       (StoreStrided{spec, nn, 1, n}), 1);
+}
+
+int con2grid_to_phys(casl_handle *h, double *phys) {
+  long long nn = (long long)h->n * h->n;
+  if (h->nptq == 0) {
+    CASL_CUDA_TRY(cudaMemsetAsync(phys, 0, nn * sizeof(double), h->stream));
+    return CASL_OK;
+  }
+  int rc = con2grid_dev(h);
+  if (rc) return rc;
+  k_c2g_final<<<grid_for(nn), 256, 0, h->stream>>>(h->coarseC, h->scal,
+                                                   h->c.beffect ? h->betac : nullptr, phys, h->n);
+  return check_launch(h);
+}
+
+// ---------------------------------------------------------------------------
+// velint (contours.f90:136-169) and the RK4 node updates (evolution.f90:212-311)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void velint1(double x, double y, const double *__restrict__ uu,
+                                        const double *__restrict__ vv, const Consts &c,
+                                        double &uq, double &vq) {
+  double xx = c.glxi * (x - c.xmin);
+  int ix0 = 1 + f_int(xx);
+  double pxc = (double)ix0 - xx;
+  double px = 1.0 - pxc;
+  double yy = c.glyi * (y - c.ymin);
+  int iy0 = 1 + f_int(yy);
+  double pyc = (double)iy0 - yy;
+  double py = 1.0 - pyc;
+  // ixp/iyp (contours.f90:58-66); indices clamped so that no input can read
+  // outside the field (valid nodes never need the clamp).
+  ix0 = ix0 < 1 ? 1 : (ix0 > c.nx ? c.nx : ix0);
+  iy0 = iy0 < 1 ? 1 : (iy0 > c.ny ? c.ny : iy0);
+  int ix1 = ix0 == c.nx ? 1 : ix0 + 1;
+  int iy1 = iy0 == c.ny ? 1 : iy0 + 1;
+  long long a00 = (long long)(ix0 - 1) * c.ny + (iy0 - 1);
+  long long a01 = (long long)(ix1 - 1) * c.ny + (iy0 - 1);
+  long long a10 = (long long)(ix0 - 1) * c.ny + (iy1 - 1);
+  long long a11 = (long long)(ix1 - 1) * c.ny + (iy1 - 1);
+  uq = pyc * (pxc * __ldg(&uu[a00]) + px * __ldg(&uu[a01])) +
+       py * (pxc * __ldg(&uu[a10]) + px * __ldg(&uu[a11]));
+  vq = pyc * (pxc * __ldg(&vv[a00]) + px * __ldg(&vv[a01])) +
+       py * (pxc * __ldg(&vv[a10]) + px * __ldg(&vv[a11]));
+}
+
+__global__ void k_velint(const double *__restrict__ xq, const double *__restrict__ yq, int npt,
+                         const double *__restrict__ uu, const double *__restrict__ vv,
+                         double *__restrict__ uq, double *__restrict__ vq, Consts c) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npt; i += gridDim.x * blockDim.x) {
+    double u, v;
+    velint1(xq[i], yq[i], uu, vv, c, u, v);
+    uq[i] = u;
+    vq[i] = v;
+  }
+}
+
+template <int STAGE>
+__global__ void k_nodes_rk(double *__restrict__ xq, double *__restrict__ yq,
+                           double *__restrict__ xqi, double *__restrict__ yqi,
+                           double *__restrict__ xqf, double *__restrict__ yqf,
+                           const double *__restrict__ uu, const double *__restrict__ vv,
+                           const Scalars *__restrict__ s, Consts c) {
+  const int npt = s->nptq;
+  const double dt = s->dt, dt2 = s->dt2, dt3 = s->dt3, dt6 = s->dt6;
+  const double ex = c.ellx, ey = c.elly, hx = c.hlxi, hy = c.hlyi, oms = c.oms;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npt; i += gridDim.x * blockDim.x) {
+    double uq, vq;
+    velint1(xq[i], yq[i], uu, vv, c, uq, vq);
+    if (STAGE == 1) {
+      double x0 = xq[i], y0 = yq[i];
+      xqi[i] = x0;
+      yqi[i] = y0;
+      xq[i] = wrapp(x0 + dt2 * uq, ex, hx, oms);
+      yq[i] = wrapp(y0 + dt2 * vq, ey, hy, oms);
+      xqf[i] = wrapp(x0 + dt6 * uq, ex, hx, oms);
+      yqf[i] = wrapp(y0 + dt6 * vq, ey, hy, oms);
+    } else if (STAGE == 2) {
+      xq[i] = wrapp(xqi[i] + dt2 * uq, ex, hx, oms);
+      yq[i] = wrapp(yqi[i] + dt2 * vq, ey, hy, oms);
+      xqf[i] = wrapp(xqf[i] + dt3 * uq, ex, hx, oms);
+      yqf[i] = wrapp(yqf[i] + dt3 * vq, ey, hy, oms);
+    } else if (STAGE == 3) {
+      xq[i] = wrapp(xqi[i] + dt * uq, ex, hx, oms);
+      yq[i] = wrapp(yqi[i] + dt * vq, ey, hy, oms);
+      xqf[i] = wrapp(xqf[i] + dt3 * uq, ex, hx, oms);
+      yqf[i] = wrapp(yqf[i] + dt3 * vq, ey, hy, oms);
+    } else {
+      xq[i] = wrapp(xqf[i] + dt6 * uq, ex, hx, oms);
+      yq[i] = wrapp(yqf[i] + dt6 * vq, ey, hy, oms);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Spectral pointwise kernels
+// ---------------------------------------------------------------------------
+// inversion's qq = flo*(qs-qc)+qc+qd and pp = green*qq (evolution.f90:514,
+// spectral.f90:321); with reset (evolution.f90:199-200) also qs <- qq and
+// qd <- fhi*(qs-qc).
+template <bool RESET>
+__global__ void k_combine(double *__restrict__ qs, double *__restrict__ qd,
+                          const double *__restrict__ qc, double *__restrict__ qq,
+                          double *__restrict__ pp, const double *__restrict__ flo,
+                          const double *__restrict__ fhi, const double *__restrict__ green,
+                          long long nn) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nn;
+       k += (long long)gridDim.x * blockDim.x) {
+    double s = qs[k], c = qc[k], d = qd[k];
+    double q = flo[k] * (s - c) + c + d;
+    qq[k] = q;
+    pp[k] = green[k] * q;
+    if (RESET) {
+      qs[k] = q;
+      qd[k] = fhi[k] * (q - c);
+    }
+  }
+}
+
+template <int STAGE>
+__global__ void k_spec_rk(double *__restrict__ qs, double *__restrict__ qd,
+                          double *__restrict__ qsi, double *__restrict__ qsf,
+                          double *__restrict__ qdi, double *__restrict__ qdf,
+                          const double *__restrict__ sqs, const double *__restrict__ sqd,
+                          double *__restrict__ emq, const Scalars *__restrict__ s, long long nn) {
+  const double dt = s->dt, dt2 = s->dt2, dt3 = s->dt3, dt6 = s->dt6;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nn;
+       k += (long long)gridDim.x * blockDim.x) {
+    double a = sqs[k], b = sqd[k];
+    if (STAGE == 1) {
+      double si = qs[k], di = qd[k];
+      qsi[k] = si;
+      qs[k] = si + dt2 * a;
+      qsf[k] = si + dt6 * a;
+      qdi[k] = di;
+      qd[k] = emq[k] * (di + dt2 * b);
+      qdf[k] = di + dt6 * b;
+    } else if (STAGE == 2) {
+      qs[k] = qsi[k] + dt2 * a;
+      qsf[k] = qsf[k] + dt3 * a;
+      qd[k] = emq[k] * (qdi[k] + dt2 * b);
+      qdf[k] = qdf[k] + dt3 * b;
+    } else if (STAGE == 3) {
+      qs[k] = qsi[k] + dt * a;
+      qsf[k] = qsf[k] + dt3 * a;
+      double e = emq[k];
+      e = e * e;
+      emq[k] = e;
+      qd[k] = e * (qdi[k] + dt * b);
+      qdf[k] = qdf[k] + dt3 * b;
+    } else {
+      qs[k] = qsf[k] + dt6 * a;
+      qd[k] = emq[k] * (qdf[k] + dt6 * b);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// adapt (evolution.f90:524-608): deterministic two-level reductions
+// ---------------------------------------------------------------------------
+#define RED_BLOCKS 296
+__global__ void k_reduce_adapt(const double *__restrict__ zz, const double *__restrict__ uu,
+                               const double *__restrict__ vv, double *__restrict__ part,
+                               long long nn) {
+  double sum = 0.0, zmax = 0.0, umax = 0.0;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nn;
+       k += (long long)gridDim.x * blockDim.x) {
+    double z = zz[k];
+    z = z * z;
+    sum += z;
+    zmax = fmax(zmax, z);
+    double w = uu[k] * uu[k] + vv[k] * vv[k];
+    umax = fmax(umax, w);
+  }
+  __shared__ double s0[256], s1[256], s2[256];
+  s0[threadIdx.x] = sum;
+  s1[threadIdx.x] = zmax;
+  s2[threadIdx.x] = umax;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      s0[threadIdx.x] += s0[threadIdx.x + o];
+      s1[threadIdx.x] = fmax(s1[threadIdx.x], s1[threadIdx.x + o]);
+      s2[threadIdx.x] = fmax(s2[threadIdx.x], s2[threadIdx.x + o]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[3 * blockIdx.x + 0] = s0[0];
+    part[3 * blockIdx.x + 1] = s1[0];
+    part[3 * blockIdx.x + 2] = s2[0];
+  }
+}
+
+__global__ void k_adapt_final(const double *__restrict__ part, int nparts, Scalars *s, Consts c,
+                              double fixed_dt) {
+  __shared__ double s0[256], s1[256], s2[256];
+  double a = 0.0, b = 0.0, d = 0.0;
+  for (int i = threadIdx.x; i < nparts; i += blockDim.x) {
+    a += part[3 * i];
+    b = fmax(b, part[3 * i + 1]);
+    d = fmax(d, part[3 * i + 2]);
+  }
+  s0[threadIdx.x] = a;
+  s1[threadIdx.x] = b;
+  s2[threadIdx.x] = d;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      s0[threadIdx.x] += s0[threadIdx.x + o];
+      s1[threadIdx.x] = fmax(s1[threadIdx.x], s1[threadIdx.x + o]);
+      s2[threadIdx.x] = fmax(s2[threadIdx.x], s2[threadIdx.x + o]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double dtfac = c.pi / 10.0, cflmax = 0.7;
+    double zzrms = sqrt(c.dsumi * s0[0]);
+    double zzmax = sqrt(s1[0]) + c.small;
+    double uumax = sqrt(s2[0]) + c.small;
+    double t1 = c.glx * cflmax / uumax;
+    double t2 = dtfac / fmax(zzmax, c.srwfm);
+    double dtacc = fmin(t1, t2);
+    double dt;
+    if (fixed_dt > 0.0)
+      dt = fixed_dt;
+    else
+      dt = fmin(dtacc, s->dtmax);
+    s->dt = dt;
+    s->dt2 = dt * 0.5;
+    s->dt3 = dt * (1.0 / 3.0);
+    s->dt6 = dt * (1.0 / 6.0);
+    s->twist = s->twist + dt * zzmax;
+    s->zzrms = zzrms;
+    s->zzmax = zzmax;
+    s->uumax = uumax;
+  }
+}
+
+__global__ void k_epq(const double *__restrict__ qdiss, double *__restrict__ epq,
+                      double *__restrict__ emq, const Scalars *__restrict__ s, long long nn) {
+  const double dfac = s->dt2 * s->zzrms;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nn;
+       k += (long long)gridDim.x * blockDim.x) {
+    double e = exp(dfac * qdiss[k]);
+    epq[k] = e;
+    emq[k] = 1.0 / e;
+  }
+}
+
+__global__ void k_advance_time(Scalars *s) { s->t = s->t + s->dt2; }
+__global__ void k_twist_sub(Scalars *s, double twistmax) { s->twist = s->twist - twistmax; }
+__global__ void k_twist_zero(Scalars *s) { s->twist = 0.0; }
+
+// ---------------------------------------------------------------------------
+// Stages
+// ---------------------------------------------------------------------------
+static int inversion_dev(casl_handle *h, bool reset) {
+  long long nn = (long long)h->n * h->n;
+  int rc = con2grid_to_spec(h, h->qc);
+  if (rc) return rc;
+  if (reset)
+    k_combine<true><<<grid_for(nn), 256, 0, h->stream>>>(h->qs, h->qd, h->qc, h->qq, h->pp,
+                                                          h->flo, h->fhi, h->green, nn);
+  else
+    k_combine<false><<<grid_for(nn), 256, 0, h->stream>>>(h->qs, h->qd, h->qc, h->qq, h->pp,
+                                                           h->flo, h->fhi, h->green, nn);
+  rc = check_launch(h);
+  if (rc) return rc;
+  // main_invert: vv = spctop(xderiv(green*qq)), uu = -spctop(yderiv(green*qq))
+  LoadDeriv ld{};
+  ld.f[0] = h->qq; ld.f[1] = h->qq;
+  ld.dir[0] = 0; ld.dir[1] = 1;
+  ld.green = h->green; ld.hrkx = h->hrkx; ld.hrky = h->hrky; ld.n = h->n;
+  long long n = h->n;
+  rc = RFFT_DISPATCH(false, true, true, ld, (StoreStrided{h->w[0], nn, 1, n}), 2);
+  if (rc) return rc;
+  StoreScaled st{};
+  st.p[0] = h->vv; st.p[1] = h->uu;
+  st.scale[0] = 1.0; st.scale[1] = -1.0; st.n = h->n;
+  // pass B reads tmp (v = iy, j = kx contiguous) and writes phys [ix][iy]
+  LoadBatch lb{};
+  lb.p[0] = h->w[0]; lb.p[1] = h->w[0] + nn; lb.vs = n; lb.es = 1;
+  return RFFT_DISPATCH(false, false, true, lb, st, 2);
+}
+
+static int adapt_dev(casl_handle *h) {
+  long long nn = (long long)h->n * h->n, n = h->n;
+  LoadVort lv{h->qq, h->pp, h->c.kdsq, h->c.btropic, h->n};
+  int rc = RFFT_DISPATCH(false, true, true, lv, (StoreStrided{h->w[0], nn, 1, n}), 1);
+  if (rc) return rc;
+  rc = RFFT_DISPATCH(false, false, true, (LoadStrided{h->w[0], nn, n, 1}),
+                     (StoreStrided{h->w[1], nn, 1, n}), 1);
+  if (rc) return rc;
+  k_reduce_adapt<<<RED_BLOCKS, 256, 0, h->stream>>>(h->w[1], h->uu, h->vv, h->part, nn);
+  k_adapt_final<<<1, 256, 0, h->stream>>>(h->part, RED_BLOCKS, h->scal, h->c, h->p.fixed_dt);
+  k_epq<<<grid_for(nn), 256, 0, h->stream>>>(h->qdiss, h->epq, h->emq, h->scal, nn);
+  return check_launch(h);
+}
+
+// source (evolution.f90:432-490): gradients of qd and qs (4 spctop in one
+// batched pair of launches), the advection products fused into ptospc's
+// first pass, damping and integrating factor fused into its last store.
+static int source_dev(casl_handle *h, int lev) {
+  long long nn = (long long)h->n * h->n, n = h->n;
+  LoadDeriv ld{};
+  ld.f[0] = h->qd; ld.f[1] = h->qd; ld.f[2] = h->qs; ld.f[3] = h->qs;
+  ld.dir[0] = 0; ld.dir[1] = 1; ld.dir[2] = 0; ld.dir[3] = 1;
+  ld.green = nullptr; ld.hrkx = h->hrkx; ld.hrky = h->hrky; ld.n = h->n;
+  // tmp for 4 transforms: w[0..3]; outputs gx_qd, gy_qd, gx_qs, gy_qs in w[4], w[5], sqs, sqd
+  // (sqs/sqd are free until the products are formed).
+  double *tmp = h->w[0];  // w[0..3] contiguous
+  int rc = RFFT_DISPATCH(false, true, true, ld, (StoreStrided{tmp, nn, 1, n}), 4);
+  if (rc) return rc;
+  LoadBatch lb{};
+  for (int b = 0; b < 4; b++) lb.p[b] = tmp + b * nn;
+  lb.vs = n; lb.es = 1;
+  StoreScaled st{};
+  st.p[0] = h->w[4]; st.p[1] = h->w[5]; st.p[2] = h->sqs; st.p[3] = h->sqd;
+  for (int b = 0; b < 4; b++) st.scale[b] = 1.0;
+  st.n = h->n;
+  rc = RFFT_DISPATCH(false, false, true, lb, st, 4);
+  if (rc) return rc;
+  // products -> ptospc pass A into tmp (transposed), pass B with the source store
+  LoadAdvect la{};
+  la.uu = h->uu; la.vv = h->vv;
+  la.fx[0] = h->w[4]; la.fy[0] = h->w[5];
+  la.fx[1] = h->sqs; la.fy[1] = h->sqd;
+  la.betab[0] = 0.0; la.betab[1] = h->c.beffect ? h->c.beta : 0.0;
+  la.n = h->n;
+  rc = RFFT_DISPATCH(true, true, false, la, (StoreStrided{tmp, nn, n, 1}), 2);
+  if (rc) return rc;
+  StoreSource ss{};
+  ss.sqd = h->sqd; ss.sqs = h->sqs; ss.qq = h->qq; ss.pp = h->pp; ss.epq = h->epq;
+  ss.rekman = h->p.rekman; ss.kdsq = h->c.kdsq; ss.therm = h->c.therm;
+  ss.heating = h->c.heating; ss.friction = h->c.friction; ss.lev = lev; ss.n = h->n;
+  return RFFT_DISPATCH(true, true, true, (LoadStrided{tmp, nn, 1, n}), ss, 2);
+}
+
+}  // namespace casl
+
+// advance (evolution.f90:166-326)
+static int advance_dev(casl_handle *h) {
+  long long nn = (long long)h->n * h->n;
+  int g = grid_for(nn);
+  int gn = grid_for(h->nptq > 0 ? h->nptq : 1);
+  int rc;
+  // stage 1
+  if ((rc = inversion_dev(h, true))) return rc;
+  if ((rc = adapt_dev(h))) return rc;
+  if ((rc = source_dev(h, 0))) return rc;
+  if (h->contex)
+    k_nodes_rk<1><<<gn, 256, 0, h->stream>>>(h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, h->uu,
+                                             h->vv, h->scal, h->c);
+  k_spec_rk<1><<<g, 256, 0, h->stream>>>(h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs,
+                                         h->sqd, h->emq, h->scal, nn);
+  if ((rc = check_launch(h))) return rc;
+  // stage 2
+  k_advance_time<<<1, 1, 0, h->stream>>>(h->scal);
+  if ((rc = inversion_dev(h, false))) return rc;
+  if ((rc = source_dev(h, 1))) return rc;
+  if (h->contex)
+    k_nodes_rk<2><<<gn, 256, 0, h->stream>>>(h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, h->uu,
+                                             h->vv, h->scal, h->c);
+  k_spec_rk<2><<<g, 256, 0, h->stream>>>(h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs,
+                                         h->sqd, h->emq, h->scal, nn);
+  if ((rc = check_launch(h))) return rc;
+  // stage 3
+  if ((rc = inversion_dev(h, false))) return rc;
+  if ((rc = source_dev(h, 1))) return rc;
+  if (h->contex)
+    k_nodes_rk<3><<<gn, 256, 0, h->stream>>>(h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, h->uu,
+                                             h->vv, h->scal, h->c);
+  k_spec_rk<3><<<g, 256, 0, h->stream>>>(h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs,
+                                         h->sqd, h->emq, h->scal, nn);
+  if ((rc = check_launch(h))) return rc;
+  // stage 4
+  k_advance_time<<<1, 1, 0, h->stream>>>(h->scal);
+  if ((rc = inversion_dev(h, false))) return rc;
+  if ((rc = source_dev(h, 2))) return rc;
+  if (h->contex)
+    k_nodes_rk<4><<<gn, 256, 0, h->stream>>>(h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, h->uu,
+                                             h->vv, h->scal, h->c);
+  k_spec_rk<4><<<g, 256, 0, h->stream>>>(h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs,
+                                         h->sqd, h->emq, h->scal, nn);
+  return check_launch(h);
+}
+
+// ---------------------------------------------------------------------------
+// Host-side set-up: constants.f90, spectral.f90:42-158 (same operations and
+// order as the reference; computed once and uploaded)
+// ---------------------------------------------------------------------------
+static double pow_cr(double x, int k) {
+#ifdef __SIZEOF_FLOAT128__
+  __float128 r = 1, b = x;
+  for (int i = 0; i < k; i++) r *= b;
+  return (double)r;
+#else
+  long double r = 1;
+  for (int i = 0; i < k; i++) r *= x;
+  return (double)r;
+#endif
+}
+
+static void make_consts(const casl_params &p, Consts &c) {
+  memset(&c, 0, sizeof(c));
+  c.nx = p.nx; c.ny = p.ny;
+  c.nxf = 4 * p.nx; c.nyf = 4 * p.ny;
+  c.nxu = 16 * p.nx; c.nyu = 16 * p.ny;
+  c.nwx = p.nx / 2; c.nwy = p.ny / 2;
+  c.ellx = p.ellx; c.elly = p.elly;
+  c.pi = 3.141592653589793238462643383279502884197169399375105820974944592307816;
+  c.twopi = 2.0 * c.pi;
+  c.small = 1.0e-12;
+  c.small3 = c.small * c.small * c.small;
+  c.oms = 1.0 - c.small;
+  c.hlx = 0.5 * p.ellx; c.hlxi = 1.0 / c.hlx; c.xmin = -c.hlx; c.xmax = c.hlx;
+  c.hly = 0.5 * p.elly; c.hlyi = 1.0 / c.hly; c.ymin = -c.hly; c.ymax = c.hly;
+  c.kdsq = pow_cr(p.kd, 2);
+  c.srwfm = p.beta * p.kd / (1.0 + c.kdsq);
+  c.therm = p.rtherm * c.kdsq;
+  c.rekman = p.rekman;
+  c.beta = p.beta;
+  c.aspect = p.ellx / p.elly;
+  c.glx = p.ellx / (double)p.nx; c.glxi = (double)p.nx / p.ellx;
+  c.gly = p.elly / (double)p.ny; c.glyi = (double)p.ny / p.elly;
+  c.garea = c.glx * c.gly;
+  c.dsumi = 1.0 / (double)(p.nx * p.ny);
+  c.glxf = p.ellx / (double)c.nxf; c.glxfi = (double)c.nxf / p.ellx;
+  c.glyf = p.elly / (double)c.nyf; c.glyfi = (double)c.nyf / p.elly;
+  c.glxu = p.ellx / (double)c.nxu; c.glxui = (double)c.nxu / p.ellx;
+  c.glyu = p.elly / (double)c.nyu; c.glyui = (double)c.nyu / p.elly;
+  c.amu = 0.2;
+  c.ell = 6.25 * c.glx;
+  c.dm = pow_cr(c.amu, 2) * c.ell / 4.0;
+  c.dm2 = pow_cr(c.dm, 2);
+  c.d4small = c.small * pow_cr(c.glx, 4);
+  c.dmsq = 4.0 * c.dm2;
+  c.dmi = 2.0 / c.dm;
+  c.elf = 1.0 / pow_cr(c.ell, 2);
+  c.densf = 1.0 / (c.amu * sqrt(c.ell));
+  c.beffect = p.beta != 0.0;
+  c.btropic = p.kd == 0.0;
+  c.heating = p.rtherm > 0.0;
+  c.friction = p.rekman > 0.0;
+}
+
+struct HostTables {
+  std::vector<double> green, flo, fhi, qdiss, hrkx, hrky, bety, betac;
+  std::vector<double2> tw;
+};
+
+static void make_tables(const casl_params &p, const Consts &c, HostTables &t) {
+  int nx = p.nx, ny = p.ny, nwx = nx / 2, nwy = ny / 2;
+  size_t nn = (size_t)nx * ny;
+  std::vector<double> rkx(nx), rky(ny), rkxf(nx), rkyf(ny);
+  t.hrkx.resize(nx); t.hrky.resize(ny);
+  double sc = c.pi / p.ellx;
+  for (int k = 1; k <= nx; k++) t.hrkx[k - 1] = sc * (double)k;
+  sc = c.pi / p.elly;
+  for (int k = 1; k <= ny; k++) t.hrky[k - 1] = sc * (double)k;
+  rkx[0] = 0.0;
+  for (int kx = 1; kx <= nwx - 1; kx++) {
+    rkx[kx] = t.hrkx[2 * kx - 1];
+    rkx[nx - kx] = t.hrkx[2 * kx - 1];
+  }
+  rkx[nwx] = t.hrkx[nx - 1];
+  double rkxmax = (c.twopi / p.ellx) * (double)nwx;
+  for (int kx = 0; kx < nx; kx++) {
+    rkxf[kx] = rkx[kx] * exp(-36.0 * pow(rkx[kx] / rkxmax, 36.0));
+    t.hrkx[kx] = t.hrkx[kx] * exp(-36.0 * pow(t.hrkx[kx] / rkxmax, 36.0));
+  }
+  rky[0] = 0.0;
+  for (int ky = 1; ky <= nwy - 1; ky++) {
+    rky[ky] = t.hrky[2 * ky - 1];
+    rky[ny - ky] = t.hrky[2 * ky - 1];
+  }
+  rky[nwy] = t.hrky[ny - 1];
+  double rkymax = (c.twopi / p.elly) * (double)nwy;
+  for (int ky = 0; ky < ny; ky++) {
+    rkyf[ky] = rky[ky] * exp(-36.0 * pow(rky[ky] / rkymax, 36.0));
+    t.hrky[ky] = t.hrky[ky] * exp(-36.0 * pow(t.hrky[ky] / rkymax, 36.0));
+  }
+  double fac = 36.0 / (double)(nx * ny);
+  double a2 = rkxmax * rkxmax, b2 = rkymax * rkymax;
+  double rkmsi = 1.0 / (a2 > b2 ? a2 : b2);
+  t.green.assign(nn, 0.0); t.flo.assign(nn, 0.0); t.fhi.assign(nn, 0.0); t.qdiss.assign(nn, 0.0);
+  for (int ky = 1; ky <= ny; ky++)
+    for (int kx = 1; kx <= nx; kx++) {
+      double rksqu = rkx[kx - 1] * rkx[kx - 1] + rky[ky - 1] * rky[ky - 1];
+      size_t k = (size_t)(ky - 1) * nx + (kx - 1);
+      t.qdiss[k] = p.cdamp * pow(rkmsi * rksqu, p.nnu);
+      double f = fac * rksqu;
+      t.flo[k] = 1.0 / (1.0 + f * f);
+      t.fhi[k] = 1.0 - t.flo[k];
+    }
+  t.green[0] = 0.0;
+  for (int kx = 2; kx <= nx; kx++) t.green[kx - 1] = -1.0 / (rkx[kx - 1] * rkx[kx - 1] + c.kdsq);
+  for (int ky = 2; ky <= ny; ky++)
+    t.green[(size_t)(ky - 1) * nx] = -1.0 / (rky[ky - 1] * rky[ky - 1] + c.kdsq);
+  for (int ky = 2; ky <= ny; ky++)
+    for (int kx = 2; kx <= nx; kx++)
+      t.green[(size_t)(ky - 1) * nx + (kx - 1)] =
+          -1.0 / (rkx[kx - 1] * rkx[kx - 1] + rky[ky - 1] * rky[ky - 1] + c.kdsq);
+  t.bety.resize(ny);
+  for (int iy = 1; iy <= ny; iy++) t.bety[iy - 1] = p.beta * (c.gly * (double)(iy - 1) + c.ymin);
+  // con2grid's beta term: the fine-grid -beta*y coarsened by the 7x7 stencil
+  // (rows only; columns sum to 16) with its mean removed.
+  t.betac.assign(ny, 0.0);
+  if (p.beta != 0.0) {
+    int nf = c.nyf;
+    const int w7[7] = {1, 2, 3, 4, 3, 2, 1};
+    double mean = 0.0;
+    for (int iy = 1; iy <= ny; iy++) {
+      double acc = 0.0;
+      for (int a = 0; a < 7; a++) {
+        int fy = 4 * iy - 6 + a;
+        if (fy <= 0) fy += nf;
+        double ygf = c.ymin + c.glyf * (double)(fy - 1);
+        acc += w7[a] * (-p.beta * ygf);
+      }
+      t.betac[iy - 1] = acc / 16.0;
+      mean += t.betac[iy - 1];
+    }
+    mean /= (double)ny;
+    for (int iy = 0; iy < ny; iy++) t.betac[iy] -= mean;
+  }
+  t.tw.resize(nx);
+  for (int k = 0; k < nx; k++) {
+    double a = c.twopi * (double)k / (double)nx;
+    t.tw[k] = make_double2(cos(a), -sin(a));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+namespace casl {
+int sync_counts(casl_handle *h) {
+  CASL_CUDA_TRY(cudaMemcpyAsync(h->hscal, h->scal, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
+  CASL_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  h->nq = h->hscal->nq;
+  h->nptq = h->hscal->nptq;
+  h->contex = h->nptq > 0;
+  if (h->hscal->error) {
+    int e = h->hscal->error;
+    return e;
+  }
+  return CASL_OK;
+}
+
+int ensure_scratch(casl_handle *h, size_t bytes) {
+  if (h->sx_bytes >= bytes) return CASL_OK;
+  if (h->sx) cudaFree(h->sx);
+  h->sx = nullptr;
+  h->sx_bytes = 0;
+  CASL_CUDA_TRY(cudaMalloc(&h->sx, bytes));
+  h->sx_bytes = bytes;
+  return CASL_OK;
+}
+}  // namespace casl
+
+extern "C" {
+
+const char *casl_error_string(int code) {
+  switch (code) {
+    case CASL_OK: return "ok";
+    case CASL_EINVAL: return "invalid argument";
+    case CASL_ECAPACITY: return "capacity exceeded";
+    case CASL_ECUDA: return "CUDA error";
+    case CASL_ENOMEM: return "device out of memory";
+    case CASL_EDOMAIN: return "node outside the domain or non-finite";
+    case CASL_ETIMEOUT: return "bounded device wait timed out";
+    case CASL_EUNSUPPORTED: return "unsupported";
+  }
+  return "unknown error";
+}
+
+int casl_last_cuda_error(casl_handle *h) { return h ? h->last_cuda : 0; }
+
+static int alloc_all(casl_handle *h) {
+  long long n = h->n, nn = n * n;
+  long long npm = h->npm, nm = h->nm;
+  double **nodes[] = {&h->xq, &h->yq, &h->xqi, &h->yqi, &h->xqf, &h->yqf, &h->uq, &h->vq};
+  for (auto pp : nodes) CASL_CUDA_TRY(cudaMalloc(pp, (size_t)npm * sizeof(double)));
+  CASL_CUDA_TRY(cudaMalloc(&h->nextq, (size_t)npm * sizeof(int)));
+  int **cont[] = {&h->i1q, &h->i2q, &h->npq, &h->indq};
+  for (auto pp : cont) CASL_CUDA_TRY(cudaMalloc(pp, (size_t)nm * sizeof(int)));
+  double **fields[] = {&h->qr, &h->qs, &h->qd, &h->qc, &h->qq, &h->pp, &h->uu, &h->vv, &h->emq,
+                       &h->epq, &h->qspre, &h->sqs, &h->sqd, &h->qsi, &h->qsf, &h->qdi, &h->qdf,
+                       &h->green, &h->flo, &h->fhi, &h->qdiss};
+  for (auto pp : fields) {
+    CASL_CUDA_TRY(cudaMalloc(pp, (size_t)nn * sizeof(double)));
+    CASL_CUDA_TRY(cudaMemset(*pp, 0, (size_t)nn * sizeof(double)));
+  }
+  // work fields: w[0..3] contiguous (batched transforms), w[4], w[5]
+  double *wk;
+  CASL_CUDA_TRY(cudaMalloc(&wk, (size_t)6 * nn * sizeof(double)));
+  for (int i = 0; i < 6; i++) h->w[i] = wk + i * nn;
+  CASL_CUDA_TRY(cudaMalloc(&h->hrkx, n * sizeof(double)));
+  CASL_CUDA_TRY(cudaMalloc(&h->hrky, n * sizeof(double)));
+  CASL_CUDA_TRY(cudaMalloc(&h->bety, n * sizeof(double)));
+  CASL_CUDA_TRY(cudaMalloc(&h->betac, n * sizeof(double)));
+  CASL_CUDA_TRY(cudaMalloc(&h->tw, n * sizeof(double2)));
+  size_t fine = (size_t)h->c.nxf * h->c.nyf;
+  CASL_CUDA_TRY(cudaMalloc(&h->fineJ, fine * sizeof(int)));
+  CASL_CUDA_TRY(cudaMalloc(&h->ljx, (size_t)h->c.nxf * sizeof(int)));
+  CASL_CUDA_TRY(cudaMalloc(&h->coarseC, (size_t)nn * sizeof(int)));
+  CASL_CUDA_TRY(cudaMalloc(&h->part, 3 * RED_BLOCKS * sizeof(double)));
+  CASL_CUDA_TRY(cudaMalloc(&h->scal, sizeof(Scalars)));
+  CASL_CUDA_TRY(cudaMemset(h->scal, 0, sizeof(Scalars)));
+  CASL_CUDA_TRY(cudaMallocHost(&h->hscal, sizeof(Scalars)));
+  memset(h->hscal, 0, sizeof(Scalars));
+  return CASL_OK;
+}
+
+static void free_all(casl_handle *h) {
+  void *ptrs[] = {h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, h->uq, h->vq, h->nextq, h->i1q,
+                  h->i2q, h->npq, h->indq, h->qr, h->qs, h->qd, h->qc, h->qq, h->pp, h->uu,
+                  h->vv, h->emq, h->epq, h->qspre, h->sqs, h->sqd, h->qsi, h->qsf, h->qdi,
+                  h->qdf, h->green, h->flo, h->fhi, h->qdiss, h->w[0], h->hrkx, h->hrky,
+                  h->bety, h->betac, h->tw, h->fineJ, h->ljx, h->coarseC, h->part, h->scal,
+                  h->sx};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (h->hscal) cudaFreeHost(h->hscal);
+}
+
+int casl_create(const casl_params *p, int device, casl_handle **out) {
+  if (!p || !out) return CASL_EINVAL;
+  *out = nullptr;
+  int n = p->nx;
+  if (p->nx != p->ny || n < 32 || n > 2048 || (n & (n - 1)) || p->ellx <= 0 || p->elly <= 0 ||
+      p->ncontq <= 0)
+    return CASL_EINVAL;
+  casl_handle *h = (casl_handle *)calloc(1, sizeof(casl_handle));
+  if (!h) return CASL_ENOMEM;
+  h->p = *p;
+  if (h->p.nlevm <= 0) h->p.nlevm = 2000;
+  if (h->p.npm <= 0) h->p.npm = 500LL * n * n;
+  if (h->p.nm <= 0) h->p.nm = h->p.npm / 20 + h->p.npm / 200;
+  if (h->p.nregmax <= 0) h->p.nregmax = 20;
+  if (h->p.twistmax <= 0) h->p.twistmax = 2.5;
+  h->n = n;
+  h->npm = h->p.npm;
+  h->nm = h->p.nm;
+  h->device = device;
+  make_consts(h->p, h->c);
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) {
+    free(h);
+    return CASL_ECUDA;
+  }
+  e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    free(h);
+    return CASL_ECUDA;
+  }
+  int rc = alloc_all(h);
+  if (rc) {
+    free_all(h);
+    cudaStreamDestroy(h->stream);
+    free(h);
+    return rc;
+  }
+  HostTables t;
+  make_tables(h->p, h->c, t);
+  size_t nn = (size_t)n * n;
+  cudaMemcpy(h->green, t.green.data(), nn * sizeof(double), cudaMemcpyHostToDevice);
+  cudaMemcpy(h->flo, t.flo.data(), nn * sizeof(double), cudaMemcpyHostToDevice);
+  cudaMemcpy(h->fhi, t.fhi.data(), nn * sizeof(double), cudaMemcpyHostToDevice);
+  cudaMemcpy(h->qdiss, t.qdiss.data(), nn * sizeof(double), cudaMemcpyHostToDevice);
+  cudaMemcpy(h->hrkx, t.hrkx.data(), n * sizeof(double), cudaMemcpyHostToDevice);
+  cudaMemcpy(h->hrky, t.hrky.data(), n * sizeof(double), cudaMemcpyHostToDevice);
+  cudaMemcpy(h->bety, t.bety.data(), n * sizeof(double), cudaMemcpyHostToDevice);
+  cudaMemcpy(h->betac, t.betac.data(), n * sizeof(double), cudaMemcpyHostToDevice);
+  e = cudaMemcpy(h->tw, t.tw.data(), n * sizeof(double2), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    free_all(h);
+    cudaStreamDestroy(h->stream);
+    free(h);
+    return CASL_ECUDA;
+  }
+  h->hscal->dtmax = h->p.dtmax > 0 ? h->p.dtmax : 1.0e30;
+  cudaMemcpy(h->scal, h->hscal, sizeof(Scalars), cudaMemcpyHostToDevice);
+  *out = h;
+  return CASL_OK;
+}
+
+void casl_destroy(casl_handle *h) {
+  if (!h) return;
+  cudaSetDevice(h->device);
+  cudaStreamSynchronize(h->stream);
+  free_all(h);
+  cudaStreamDestroy(h->stream);
+  free(h);
+}
+
+int casl_synchronize(casl_handle *h) {
+  if (!h) return CASL_EINVAL;
+  CASL_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return CASL_OK;
+}
+
+static int put_scalars(casl_handle *h) {
+  CASL_CUDA_TRY(cudaMemcpyAsync(h->scal, h->hscal, sizeof(Scalars), cudaMemcpyHostToDevice, h->stream));
+  CASL_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return CASL_OK;
+}
+static int get_scalars(casl_handle *h) {
+  CASL_CUDA_TRY(cudaMemcpyAsync(h->hscal, h->scal, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
+  CASL_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return CASL_OK;
+}
+
+__global__ void k_to0(int *a, long long m, int off) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m;
+       i += (long long)gridDim.x * blockDim.x)
+    a[i] += off;
+}
+
+int casl_set_contours(casl_handle *h, int nq, int nptq, double qjump, const double *xq,
+                      const double *yq, const int *nextq, const int *indq, const int *npq,
+                      const int *i1q, const int *i2q) {
+  if (!h || nq < 0 || nptq < 0) return CASL_EINVAL;
+  if (nptq > h->npm || nq > h->nm) return CASL_ECAPACITY;
+  if (nptq > 0 && (!xq || !yq || !nextq)) return CASL_EINVAL;
+  if (nq > 0 && (!indq || !npq || !i1q || !i2q)) return CASL_EINVAL;
+  cudaStream_t s = h->stream;
+  if (nptq) {
+    CASL_CUDA_TRY(cudaMemcpyAsync(h->xq, xq, nptq * sizeof(double), cudaMemcpyHostToDevice, s));
+    CASL_CUDA_TRY(cudaMemcpyAsync(h->yq, yq, nptq * sizeof(double), cudaMemcpyHostToDevice, s));
+    CASL_CUDA_TRY(cudaMemcpyAsync(h->nextq, nextq, nptq * sizeof(int), cudaMemcpyHostToDevice, s));
+    k_to0<<<grid_for(nptq), 256, 0, s>>>(h->nextq, nptq, -1);
+  }
+  if (nq) {
+    CASL_CUDA_TRY(cudaMemcpyAsync(h->indq, indq, nq * sizeof(int), cudaMemcpyHostToDevice, s));
+    CASL_CUDA_TRY(cudaMemcpyAsync(h->npq, npq, nq * sizeof(int), cudaMemcpyHostToDevice, s));
+    CASL_CUDA_TRY(cudaMemcpyAsync(h->i1q, i1q, nq * sizeof(int), cudaMemcpyHostToDevice, s));
+    CASL_CUDA_TRY(cudaMemcpyAsync(h->i2q, i2q, nq * sizeof(int), cudaMemcpyHostToDevice, s));
+    k_to0<<<grid_for(nq), 256, 0, s>>>(h->i1q, nq, -1);
+    k_to0<<<grid_for(nq), 256, 0, s>>>(h->i2q, nq, -1);
+  }
+  int rc = get_scalars(h);
+  if (rc) return rc;
+  h->hscal->nq = nq;
+  h->hscal->nptq = nptq;
+  h->hscal->qjump = qjump;
+  h->nq = nq;
+  h->nptq = nptq;
+  h->qjump = qjump;
+  h->contex = nptq > 0;
+  return put_scalars(h);
+}
+
+int casl_get_counts(casl_handle *h, int *nq, int *nptq, double *qjump) {
+  if (!h) return CASL_EINVAL;
+  int rc = get_scalars(h);
+  if (rc) return rc;
+  if (nq) *nq = h->hscal->nq;
+  if (nptq) *nptq = h->hscal->nptq;
+  if (qjump) *qjump = h->hscal->qjump;
+  return CASL_OK;
+}
+
+int casl_get_contours(casl_handle *h, double *xq, double *yq, int *nextq, int *indq, int *npq,
+                      int *i1q, int *i2q) {
+  if (!h) return CASL_EINVAL;
+  int rc = sync_counts(h);
+  if (rc) return rc;
+  cudaStream_t s = h->stream;
+  int npt = h->nptq, nq = h->nq;
+  if (npt) {
+    k_to0<<<grid_for(npt), 256, 0, s>>>(h->nextq, npt, 1);
+    if (xq) CASL_CUDA_TRY(cudaMemcpyAsync(xq, h->xq, npt * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (yq) CASL_CUDA_TRY(cudaMemcpyAsync(yq, h->yq, npt * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (nextq) CASL_CUDA_TRY(cudaMemcpyAsync(nextq, h->nextq, npt * sizeof(int), cudaMemcpyDeviceToHost, s));
+    k_to0<<<grid_for(npt), 256, 0, s>>>(h->nextq, npt, -1);
+  }
+  if (nq) {
+    k_to0<<<grid_for(nq), 256, 0, s>>>(h->i1q, nq, 1);
+    k_to0<<<grid_for(nq), 256, 0, s>>>(h->i2q, nq, 1);
+    if (indq) CASL_CUDA_TRY(cudaMemcpyAsync(indq, h->indq, nq * sizeof(int), cudaMemcpyDeviceToHost, s));
+    if (npq) CASL_CUDA_TRY(cudaMemcpyAsync(npq, h->npq, nq * sizeof(int), cudaMemcpyDeviceToHost, s));
+    if (i1q) CASL_CUDA_TRY(cudaMemcpyAsync(i1q, h->i1q, nq * sizeof(int), cudaMemcpyDeviceToHost, s));
+    if (i2q) CASL_CUDA_TRY(cudaMemcpyAsync(i2q, h->i2q, nq * sizeof(int), cudaMemcpyDeviceToHost, s));
+    k_to0<<<grid_for(nq), 256, 0, s>>>(h->i1q, nq, -1);
+    k_to0<<<grid_for(nq), 256, 0, s>>>(h->i2q, nq, -1);
+  }
+  CASL_CUDA_TRY(cudaStreamSynchronize(s));
+  return check_launch(h);
+}
+
+static double *field_ptr(casl_handle *h, int which) {
+  switch (which) {
+    case CASL_QS: return h->qs;
+    case CASL_QD: return h->qd;
+    case CASL_QC: return h->qc;
+    case CASL_QQ: return h->qq;
+    case CASL_PP: return h->pp;
+    case CASL_QSPRE: return h->qspre;
+    case CASL_EMQ: return h->emq;
+    case CASL_EPQ: return h->epq;
+    case CASL_UU: return h->uu;
+    case CASL_VV: return h->vv;
+    case CASL_QR: return h->qr;
+  }
+  return nullptr;
+}
+
+int casl_set_field(casl_handle *h, int which, const double *host) {
+  if (!h || !host) return CASL_EINVAL;
+  double *d = field_ptr(h, which);
+  if (!d) return CASL_EINVAL;
+  size_t nn = (size_t)h->n * h->n;
+  CASL_CUDA_TRY(cudaMemcpyAsync(d, host, nn * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CASL_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return CASL_OK;
+}
+
+int casl_get_field(casl_handle *h, int which, double *host) {
+  if (!h || !host) return CASL_EINVAL;
+  double *d = field_ptr(h, which);
+  if (!d) return CASL_EINVAL;
+  size_t nn = (size_t)h->n * h->n;
+  CASL_CUDA_TRY(cudaMemcpyAsync(host, d, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CASL_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return CASL_OK;
+}
+
+int casl_get_scalar(casl_handle *h, int which, double *value) {
+  if (!h || !value) return CASL_EINVAL;
+  int rc = get_scalars(h);
+  if (rc) return rc;
+  Scalars &s = *h->hscal;
+  switch (which) {
+    case CASL_T: *value = s.t; break;
+    case CASL_DT: *value = s.dt; break;
+    case CASL_TWIST: *value = s.twist; break;
+    case CASL_IREG: *value = h->ireg; break;
+    case CASL_ZZRMS: *value = s.zzrms; break;
+    case CASL_ZZMAX: *value = s.zzmax; break;
+    case CASL_UUMAX: *value = s.uumax; break;
+    case CASL_QJUMP: *value = s.qjump; break;
+    default: return CASL_EINVAL;
+  }
+  return CASL_OK;
+}
+
+int casl_set_scalar(casl_handle *h, int which, double value) {
+  if (!h) return CASL_EINVAL;
+  int rc = get_scalars(h);
+  if (rc) return rc;
+  Scalars &s = *h->hscal;
+  switch (which) {
+    case CASL_T: s.t = value; break;
+    case CASL_DT:
+      s.dt = value; s.dt2 = value * 0.5; s.dt3 = value * (1.0 / 3.0); s.dt6 = value * (1.0 / 6.0);
+      break;
+    case CASL_TWIST: s.twist = value; break;
+    case CASL_IREG: h->ireg = (int)value; break;
+    case CASL_QJUMP: s.qjump = value; h->qjump = value; break;
+    default: return CASL_EINVAL;
+  }
+  return put_scalars(h);
+}
+
+int casl_ptospc(casl_handle *h, const double *rvar, double *svar) {
+  if (!h || !rvar || !svar) return CASL_EINVAL;
+  size_t nn = (size_t)h->n * h->n;
+  CASL_CUDA_TRY(cudaMemcpyAsync(h->w[4], rvar, nn * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  int rc = ptospc_dev(h, h->w[4], h->w[5]);
+  if (rc) return rc;
+  CASL_CUDA_TRY(cudaMemcpyAsync(svar, h->w[5], nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CASL_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return check_launch(h);
+}
+
+int casl_spctop(casl_handle *h, const double *svar, double *rvar) {
+  if (!h || !rvar || !svar) return CASL_EINVAL;
+  size_t nn = (size_t)h->n * h->n;
+  CASL_CUDA_TRY(cudaMemcpyAsync(h->w[4], svar, nn * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  int rc = spctop_dev(h, h->w[4], h->w[5], h->w[0]);
+  if (rc) return rc;
+  CASL_CUDA_TRY(cudaMemcpyAsync(rvar, h->w[5], nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CASL_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return check_launch(h);
+}
+
+int casl_con2grid(casl_handle *h, double *qc, int *levels) {
+  if (!h) return CASL_EINVAL;
+  size_t nn = (size_t)h->n * h->n;
+  int rc = con2grid_to_phys(h, h->w[5]);
+  if (rc) return rc;
+  if (qc) CASL_CUDA_TRY(cudaMemcpyAsync(qc, h->w[5], nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  if (levels) {
+    size_t fine = (size_t)h->c.nxf * h->c.nyf;
+    if (h->nptq == 0)
+      memset(levels, 0, fine * sizeof(int));
+    else
+      CASL_CUDA_TRY(cudaMemcpyAsync(levels, h->fineJ, fine * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  }
+  CASL_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  rc = get_scalars(h);
+  if (rc) return rc;
+  if (h->hscal->error) {
+    int e = h->hscal->error;
+    h->hscal->error = 0;
+    put_scalars(h);
+    return e;
+  }
+  return CASL_OK;
+}
+
+int casl_velint(casl_handle *h, const double *uu, const double *vv, double *uq, double *vq) {
+  if (!h || !uu || !vv || !uq || !vq) return CASL_EINVAL;
+  size_t nn = (size_t)h->n * h->n;
+  cudaStream_t s = h->stream;
+  CASL_CUDA_TRY(cudaMemcpyAsync(h->w[4], uu, nn * sizeof(double), cudaMemcpyHostToDevice, s));
+  CASL_CUDA_TRY(cudaMemcpyAsync(h->w[5], vv, nn * sizeof(double), cudaMemcpyHostToDevice, s));
+  int npt = h->nptq;
+  if (npt > 0) {
+    k_velint<<<grid_for(npt), 256, 0, s>>>(h->xq, h->yq, npt, h->w[4], h->w[5], h->uq, h->vq, h->c);
+    CASL_CUDA_TRY(cudaMemcpyAsync(uq, h->uq, npt * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CASL_CUDA_TRY(cudaMemcpyAsync(vq, h->vq, npt * sizeof(double), cudaMemcpyDeviceToHost, s));
+  }
+  CASL_CUDA_TRY(cudaStreamSynchronize(s));
+  return check_launch(h);
+}
+
+int casl_main_invert(casl_handle *h, const double *qq, double *uu, double *vv, double *pp) {
+  if (!h || !qq) return CASL_EINVAL;
+  size_t nn = (size_t)h->n * h->n;
+  cudaStream_t s = h->stream;
+  // Runs on scratch copies so that the simulation state is untouched.
+  double *q = h->w[4], *p = h->w[5];
+  CASL_CUDA_TRY(cudaMemcpyAsync(q, qq, nn * sizeof(double), cudaMemcpyHostToDevice, s));
+  long long n = h->n;
+  LoadDeriv ld{};
+  ld.f[0] = q; ld.f[1] = q; ld.dir[0] = 0; ld.dir[1] = 1;
+  ld.green = h->green; ld.hrkx = h->hrkx; ld.hrky = h->hrky; ld.n = h->n;
+  int rc = RFFT_DISPATCH(false, true, true, ld, (StoreStrided{h->w[0], (long long)nn, 1, n}), 2);
+  if (rc) return rc;
+  StoreScaled st{};
+  st.p[0] = h->w[2]; st.p[1] = h->w[3]; st.scale[0] = 1.0; st.scale[1] = -1.0; st.n = h->n;
+  LoadBatch lb{};
+  lb.p[0] = h->w[0]; lb.p[1] = h->w[1]; lb.vs = n; lb.es = 1;
+  rc = RFFT_DISPATCH(false, false, true, lb, st, 2);
+  if (rc) return rc;
+  if (uu) CASL_CUDA_TRY(cudaMemcpyAsync(uu, h->w[3], nn * sizeof(double), cudaMemcpyDeviceToHost, s));
+  if (vv) CASL_CUDA_TRY(cudaMemcpyAsync(vv, h->w[2], nn * sizeof(double), cudaMemcpyDeviceToHost, s));
+  if (pp) {
+    // pp = green*qq on the host copy is exact elementwise; done on device
+    // through the combine kernel's formula.
+    CASL_CUDA_TRY(cudaMemcpyAsync(p, h->green, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    CASL_CUDA_TRY(cudaStreamSynchronize(s));
+    std::vector<double> g(nn);
+    CASL_CUDA_TRY(cudaMemcpy(g.data(), p, nn * sizeof(double), cudaMemcpyDeviceToHost));
+    for (size_t k = 0; k < nn; k++) pp[k] = g[k] * qq[k];
+  }
+  CASL_CUDA_TRY(cudaStreamSynchronize(s));
+  return check_launch(h);
+}
+
+int casl_gradient(casl_handle *h, const double *ff, double *ffx, double *ffy) {
+  if (!h || !ff) return CASL_EINVAL;
+  size_t nn = (size_t)h->n * h->n;
+  cudaStream_t s = h->stream;
+  double *f = h->w[4];
+  CASL_CUDA_TRY(cudaMemcpyAsync(f, ff, nn * sizeof(double), cudaMemcpyHostToDevice, s));
+  long long n = h->n;
+  LoadDeriv ld{};
+  ld.f[0] = f; ld.f[1] = f; ld.dir[0] = 0; ld.dir[1] = 1;
+  ld.green = nullptr; ld.hrkx = h->hrkx; ld.hrky = h->hrky; ld.n = h->n;
+  int rc = RFFT_DISPATCH(false, true, true, ld, (StoreStrided{h->w[0], (long long)nn, 1, n}), 2);
+  if (rc) return rc;
+  StoreScaled st{};
+  st.p[0] = h->w[2]; st.p[1] = h->w[3]; st.scale[0] = 1.0; st.scale[1] = 1.0; st.n = h->n;
+  LoadBatch lb{};
+  lb.p[0] = h->w[0]; lb.p[1] = h->w[1]; lb.vs = n; lb.es = 1;
+  rc = RFFT_DISPATCH(false, false, true, lb, st, 2);
+  if (rc) return rc;
+  if (ffx) CASL_CUDA_TRY(cudaMemcpyAsync(ffx, h->w[2], nn * sizeof(double), cudaMemcpyDeviceToHost, s));
+  if (ffy) CASL_CUDA_TRY(cudaMemcpyAsync(ffy, h->w[3], nn * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CASL_CUDA_TRY(cudaStreamSynchronize(s));
+  return check_launch(h);
+}
+
+int casl_inversion(casl_handle *h) {
+  if (!h) return CASL_EINVAL;
+  int rc = inversion_dev(h, false);
+  if (rc) return rc;
+  CASL_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return sync_counts(h);
+}
+
+int casl_advance(casl_handle *h) {
+  if (!h) return CASL_EINVAL;
+  int rc = advance_dev(h);
+  if (rc) return rc;
+  return sync_counts(h);
+}
+
+int casl_surgery(casl_handle *h) {
+  if (!h) return CASL_EINVAL;
+  int rc = surgery_dev(h);
+  if (rc) return rc;
+  return sync_counts(h);
+}
+
+int casl_renode(casl_handle *h, const double *xd, const double *yd, int npd, double *xr,
+                double *yr, int cap, int *npr) {
+  if (!h || !xd || !yd || !xr || !yr || !npr || npd < 1 || cap < 0) return CASL_EINVAL;
+  return renode_host(h, xd, yd, npd, xr, yr, cap, npr);
+}
+
+int casl_recontour(casl_handle *h, const double *qq) {
+  if (!h || !qq) return CASL_EINVAL;
+  size_t nn = (size_t)h->n * h->n;
+  CASL_CUDA_TRY(cudaMemcpyAsync(h->qr, qq, nn * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  int rc = recontour_dev(h, h->qr);
+  if (rc) return rc;
+  return sync_counts(h);
+}
+
+// init (evolution.f90:96-131)
+__global__ void k_evo_init(double *qd, double *qspre, const double *qs, const double *qc,
+                           const double *fhi, long long nn) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nn;
+       k += (long long)gridDim.x * blockDim.x) {
+    qd[k] = fhi[k] * (qs[k] - qc[k]);
+    qspre[k] = qs[k];
+  }
+}
+// prepare (evolution.f90:135-162), spectral part
+__global__ void k_prepare(double *qs, double *qd, const double *qc, const double *flo,
+                          long long nn) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nn;
+       k += (long long)gridDim.x * blockDim.x) {
+    double s = flo[k] * (qs[k] - qc[k]) + qc[k] + qd[k];
+    qs[k] = s;
+    qd[k] = s - qc[k];
+  }
+}
+
+static int evo_init(casl_handle *h) {
+  long long nn = (long long)h->n * h->n;
+  h->contex = h->nptq > 0;
+  int rc = con2grid_to_spec(h, h->qc);
+  if (rc) return rc;
+  k_evo_init<<<grid_for(nn), 256, 0, h->stream>>>(h->qd, h->qspre, h->qs, h->qc, h->fhi, nn);
+  return check_launch(h);
+}
+
+static int evo_prepare(casl_handle *h) {
+  long long nn = (long long)h->n * h->n;
+  int rc = con2grid_to_spec(h, h->qc);
+  if (rc) return rc;
+  k_prepare<<<grid_for(nn), 256, 0, h->stream>>>(h->qs, h->qd, h->qc, h->flo, nn);
+  if ((rc = check_launch(h))) return rc;
+  return spctop_dev(h, h->qd, h->qr, h->w[0]);
+}
+
+__global__ void k_sub_bety(double *q, const double *bety, int n) {
+  long long nn = (long long)n * n;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nn;
+       k += (long long)gridDim.x * blockDim.x)
+    q[k] -= bety[k % n];
+}
+
+__global__ void k_minmax(const double *q, long long nn, double *part) {
+  double mx = -1e308, mn = 1e308;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nn;
+       k += (long long)gridDim.x * blockDim.x) {
+    mx = fmax(mx, q[k]);
+    mn = fmin(mn, q[k]);
+  }
+  __shared__ double a[256], b[256];
+  a[threadIdx.x] = mx;
+  b[threadIdx.x] = mn;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      a[threadIdx.x] = fmax(a[threadIdx.x], a[threadIdx.x + o]);
+      b[threadIdx.x] = fmin(b[threadIdx.x], b[threadIdx.x + o]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = a[0];
+    part[2 * blockIdx.x + 1] = b[0];
+  }
+}
+
+int casl_initialise(casl_handle *h, const double *qq_init) {
+  if (!h || !qq_init) return CASL_EINVAL;
+  long long nn = (long long)h->n * h->n;
+  cudaStream_t s = h->stream;
+  int rc = get_scalars(h);
+  if (rc) return rc;
+  CASL_CUDA_TRY(cudaMemcpyAsync(h->qr, qq_init, nn * sizeof(double), cudaMemcpyHostToDevice, s));
+  double qjump;
+  if (h->c.beffect) {
+    k_sub_bety<<<grid_for(nn), 256, 0, s>>>(h->qr, h->bety, h->n);
+    qjump = h->p.beta * h->p.elly / (double)h->p.ncontq;
+  } else {
+    // contint (generic.f90:216-229)
+    k_minmax<<<RED_BLOCKS, 256, 0, s>>>(h->qr, nn, h->part);
+    std::vector<double> part(2 * RED_BLOCKS);
+    CASL_CUDA_TRY(cudaMemcpyAsync(part.data(), h->part, part.size() * sizeof(double),
+                                  cudaMemcpyDeviceToHost, s));
+    CASL_CUDA_TRY(cudaStreamSynchronize(s));
+    double mx = part[0], mn = part[1];
+    for (int i = 1; i < RED_BLOCKS; i++) {
+      mx = fmax(mx, part[2 * i]);
+      mn = fmin(mn, part[2 * i + 1]);
+    }
+    qjump = (mx - mn) / (double)h->p.ncontq;
+  }
+  rc = ptospc_dev(h, h->qr, h->qs);
+  if (rc) return rc;
+  Scalars &sc = *h->hscal;
+  sc.t = 0.0; sc.dt = 0.0; sc.twist = 0.0; sc.qjump = qjump; sc.nq = 0; sc.nptq = 0;
+  sc.error = 0;
+  sc.dtmax = h->p.dtmax > 0 ? h->p.dtmax : 1.0e30;
+  h->qjump = qjump;
+  h->nq = 0;
+  h->nptq = 0;
+  if ((rc = put_scalars(h))) return rc;
+  if ((rc = recontour_dev(h, h->qr))) return rc;
+  if ((rc = sync_counts(h))) return rc;
+  if ((rc = evo_init(h))) return rc;
+  h->ireg = 0;
+  return sync_counts(h);
+}
+
+int casl_step(casl_handle *h, int nsteps) {
+  if (!h || nsteps < 0) return CASL_EINVAL;
+  int rc;
+  for (int it = 0; it < nsteps; it++) {
+    bool force = h->p.force_surgery != 0;
+    bool reg = force;
+    if (!force) {
+      if ((rc = get_scalars(h))) return rc;
+      reg = h->hscal->twist > h->p.twistmax;
+    }
+    if (reg) {
+      h->ireg++;
+      if (h->ireg == h->p.nregmax) {
+        // prepare + recontour + init (evolution.f90:62-66; caps.f90:83-91)
+        if ((rc = evo_prepare(h))) return rc;
+        if ((rc = recontour_dev(h, h->qr))) return rc;
+        if ((rc = sync_counts(h))) return rc;
+        if ((rc = evo_init(h))) return rc;
+        k_twist_zero<<<1, 1, 0, h->stream>>>(h->scal);
+        h->ireg = 0;
+        if (force) {
+          h->ireg = 1;
+          if ((rc = surgery_dev(h))) return rc;
+          k_twist_sub<<<1, 1, 0, h->stream>>>(h->scal, h->p.twistmax);
+        }
+      } else {
+        if ((rc = surgery_dev(h))) return rc;
+        k_twist_sub<<<1, 1, 0, h->stream>>>(h->scal, h->p.twistmax);
+      }
+    }
+    if ((rc = advance_dev(h))) return rc;
+  }
+  return sync_counts(h);
+}
+
+int casl_diagnostics(casl_handle *h, double out[4]) {
+  if (!h || !out) return CASL_EINVAL;
+  (void)out;
+  return CASL_EUNSUPPORTED;
+}
+
+}  // extern "C"

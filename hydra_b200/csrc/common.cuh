@@ -1,0 +1,63 @@
+// Shared definitions of the B200 contour-advection library.
+//
+// Every translation unit is compiled with -fmad=false: the node arithmetic,
+// the grid-line crossing tests and the surgery distance tests must round each
+// product and sum separately, exactly as the Fortran reference does on x86-64
+// (gfortran without -march flags never contracts to FMA), so that integer
+// outcomes (crossing cells, box indices, surgery decisions) are reproduced.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace casl {
+
+// Constants of constants.f90 and contours.f90:17-42, computed once on the
+// host by the same operations as the reference's PARAMETER expressions.
+struct Consts {
+  int nx, ny, nxf, nyf, nxu, nyu, nwx, nwy;
+  double ellx, elly, pi, twopi, small, small3, oms;
+  double hlx, hlxi, xmin, xmax, hly, hlyi, ymin, ymax;
+  double kdsq, srwfm, therm, rekman, beta, aspect;
+  double glx, glxi, gly, glyi, garea, dsumi;
+  double glxf, glxfi, glyf, glyfi, glxu, glxui, glyu, glyui;
+  double amu, ell, dm, dm2, d4small, dmsq, dmi, elf, densf;
+  int beffect, btropic, heating, friction;
+};
+
+// Fortran intrinsics with the reference's semantics.
+__host__ __device__ __forceinline__ double f_dint(double x) { return (double)(long long)x; }
+__host__ __device__ __forceinline__ int f_int(double x) { return (int)x; }
+__host__ __device__ __forceinline__ double f_sign1(double b) { return copysign(1.0, b); }
+__host__ __device__ __forceinline__ int f_isign1(int b) { return b >= 0 ? 1 : -1; }
+
+// Periodic wrap of a displacement: xx - ellx*dble(int(xx*hlxi)).
+__host__ __device__ __forceinline__ double wrapd(double xx, double ell, double hli) {
+  return xx - ell * f_dint(xx * hli);
+}
+// Node position wrap: oms*(xx - ellx*dble(int(xx*hlxi))) (evolution.f90:219).
+__host__ __device__ __forceinline__ double wrapp(double xx, double ell, double hli, double oms) {
+  return oms * (xx - ell * f_dint(xx * hli));
+}
+
+// Device-resident scalars of one simulation (variables.f90 and adapt()).
+struct Scalars {
+  double t, dt, dt2, dt3, dt6, twist;
+  double zzrms, zzmax, uumax, dtmax;
+  double qjump;
+  unsigned long long zz2_bits;   // max of zz^2 as ordered bits (non-negative doubles)
+  unsigned long long uu2_bits;   // max of u^2+v^2
+  double zz2_sum;                // sum of zz^2 (deterministic two-level reduction)
+  long long csum;                // con2grid: sum of coarse integer cells
+  int nq, nptq;                  // current counts (device copy)
+  int error;                     // sticky device-side error code
+  int pad;
+};
+
+}  // namespace casl
+
+#define CASL_CUDA_TRY(expr)                               \
+  do {                                                    \
+    cudaError_t _e = (expr);                              \
+    if (_e != cudaSuccess) return ::casl::set_cuda_error(h, _e); \
+  } while (0)

@@ -1,0 +1,257 @@
+// Device-wide scans and a bump allocator over the handle's scratch arena.
+//
+// Scans are three-phase (per-block scan, scan of block totals in one block,
+// carry add), deterministic, with 4096 elements per block.  Integer scans
+// are exact; the segmented double scan sums in a fixed order (the same on
+// every run), restarting at every head flag.
+#pragma once
+
+#include "common.cuh"
+#include "state.cuh"
+
+namespace casl {
+
+// Bump allocator over one device buffer (256-byte aligned pieces).
+struct Arena {
+  char *base;
+  size_t cap, off;
+  template <class T>
+  T *get(size_t count) {
+    size_t bytes = (count * sizeof(T) + 255) & ~(size_t)255;
+    if (off + bytes > cap) return nullptr;
+    T *p = reinterpret_cast<T *>(base + off);
+    off += bytes;
+    return p;
+  }
+};
+
+constexpr int SCAN_BLOCK = 1024;
+constexpr int SCAN_ITEMS = 4;
+constexpr int SCAN_TILE = SCAN_BLOCK * SCAN_ITEMS;
+
+template <class T>
+__device__ __forceinline__ T warp_incl_scan(T x) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    T y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  return x;
+}
+
+// Block-wide exclusive scan of one value per thread; returns the block total
+// through *total.  blockDim.x must be SCAN_BLOCK.
+template <class T>
+__device__ T block_excl_scan(T v, T *total) {
+  __shared__ T wsum[32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  T incl = warp_incl_scan(v);
+  if (lane == 31) wsum[wid] = incl;
+  __syncthreads();
+  if (wid == 0) {
+    T w = wsum[lane];
+    T wi = warp_incl_scan(w);
+    wsum[lane] = wi - w;
+    if (lane == 31) *total = wi;
+  }
+  __syncthreads();
+  T r = incl - v + wsum[wid];
+  __syncthreads();
+  return r;
+}
+
+template <class T>
+__global__ void __launch_bounds__(SCAN_BLOCK) k_scan_tiles(const T *__restrict__ in,
+                                                           T *__restrict__ out,
+                                                           T *__restrict__ tile_tot, long long n) {
+  __shared__ T tot;
+  long long base = (long long)blockIdx.x * SCAN_TILE + (long long)threadIdx.x * SCAN_ITEMS;
+  T v[SCAN_ITEMS];
+  T s = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; k++) {
+    v[k] = (base + k < n) ? in[base + k] : T(0);
+    s += v[k];
+  }
+  T ex = block_excl_scan<T>(s, &tot);
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; k++) {
+    if (base + k < n) out[base + k] = ex;
+    ex += v[k];
+  }
+  if (threadIdx.x == 0) tile_tot[blockIdx.x] = tot;
+}
+
+// Exclusive scan of the tile totals in one block; writes the grand total.
+template <class T>
+__global__ void __launch_bounds__(SCAN_BLOCK) k_scan_totals(T *__restrict__ tot, int ntiles,
+                                                            T *__restrict__ grand) {
+  __shared__ T t;
+  __shared__ T carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < ntiles; base += SCAN_BLOCK) {
+    int i = base + threadIdx.x;
+    T v = i < ntiles ? tot[i] : T(0);
+    T ex = block_excl_scan<T>(v, &t);
+    if (i < ntiles) tot[i] = ex + carry;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += t;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0 && grand) *grand = carry;
+}
+
+template <class T>
+__global__ void k_scan_add(T *__restrict__ out, const T *__restrict__ tot, long long n) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] += tot[i / SCAN_TILE];
+}
+
+// out[i] = sum_{j<i} in[j]; *grand (device, optional) = sum of all.
+// in and out may alias.  tmp needs ceil(n/SCAN_TILE) elements.
+template <class T>
+int exclusive_scan(cudaStream_t st, const T *in, T *out, long long n, T *tmp, T *grand) {
+  if (n <= 0) {
+    if (grand) cudaMemsetAsync(grand, 0, sizeof(T), st);
+    return 0;
+  }
+  int tiles = (int)((n + SCAN_TILE - 1) / SCAN_TILE);
+  k_scan_tiles<T><<<tiles, SCAN_BLOCK, 0, st>>>(in, out, tmp, n);
+  k_scan_totals<T><<<1, SCAN_BLOCK, 0, st>>>(tmp, tiles, grand);
+  k_scan_add<T><<<(int)((n + 255) / 256), 256, 0, st>>>(out, tmp, n);
+  return (int)cudaGetLastError();
+}
+
+inline long long scan_tmp_elems(long long n) { return (n + SCAN_TILE - 1) / SCAN_TILE + 1; }
+
+
+// ---------------------------------------------------------------------------
+// Segmented inclusive scan of doubles: out[i] = sum of in[j] for j from the
+// last head at or before i through i.  head[i] != 0 starts a segment.
+// ---------------------------------------------------------------------------
+struct SegPair {
+  double v;
+  int f;
+};
+__device__ __forceinline__ SegPair seg_op(SegPair a, SegPair b) {
+  SegPair r;
+  r.f = a.f | b.f;
+  r.v = b.f ? b.v : a.v + b.v;
+  return r;
+}
+__device__ __forceinline__ SegPair warp_seg_incl(SegPair x) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    SegPair y;
+    y.v = __shfl_up_sync(0xffffffffu, x.v, o);
+    y.f = __shfl_up_sync(0xffffffffu, x.f, o);
+    if (lane >= o) x = seg_op(y, x);
+  }
+  return x;
+}
+// Exclusive (prefix before this thread) segmented scan across the block.
+__device__ SegPair block_seg_excl(SegPair x, SegPair *total) {
+  __shared__ double wv[32];
+  __shared__ int wf[32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  SegPair incl = warp_seg_incl(x);
+  SegPair ex;
+  ex.v = __shfl_up_sync(0xffffffffu, incl.v, 1);
+  ex.f = __shfl_up_sync(0xffffffffu, incl.f, 1);
+  if (lane == 0) { ex.v = 0.0; ex.f = 0; }
+  if (lane == 31) { wv[wid] = incl.v; wf[wid] = incl.f; }
+  __syncthreads();
+  if (wid == 0) {
+    SegPair w{wv[lane], wf[lane]};
+    SegPair wi = warp_seg_incl(w);
+    SegPair we;
+    we.v = __shfl_up_sync(0xffffffffu, wi.v, 1);
+    we.f = __shfl_up_sync(0xffffffffu, wi.f, 1);
+    if (lane == 0) { we.v = 0.0; we.f = 0; }
+    wv[lane] = we.v;
+    wf[lane] = we.f;
+    if (lane == 31) *total = wi;
+  }
+  __syncthreads();
+  SegPair pre{wv[wid], wf[wid]};
+  SegPair r = seg_op(pre, ex);
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(SCAN_BLOCK) k_segscan_tiles(const double *__restrict__ in,
+                                                              const int *__restrict__ head,
+                                                              double *__restrict__ out,
+                                                              SegPair *__restrict__ tile_tot,
+                                                              long long n) {
+  __shared__ SegPair tot;
+  long long base = (long long)blockIdx.x * SCAN_TILE + (long long)threadIdx.x * SCAN_ITEMS;
+  SegPair loc[SCAN_ITEMS];
+  SegPair acc{0.0, 0};
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; k++) {
+    bool ok = base + k < n;
+    loc[k].v = ok ? in[base + k] : 0.0;
+    loc[k].f = ok ? (head[base + k] != 0) : 0;
+    acc = seg_op(acc, loc[k]);
+  }
+  SegPair ex = block_seg_excl(acc, &tot);
+  SegPair run = ex;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; k++) {
+    run = seg_op(run, loc[k]);
+    if (base + k < n) out[base + k] = run.v;
+  }
+  if (threadIdx.x == 0) tile_tot[blockIdx.x] = tot;
+}
+
+// Exclusive segmented scan of tile totals (one block): carry into each tile.
+__global__ void __launch_bounds__(SCAN_BLOCK) k_segscan_totals(SegPair *__restrict__ tot,
+                                                               int ntiles) {
+  __shared__ SegPair t;
+  __shared__ SegPair carry;
+  if (threadIdx.x == 0) { carry.v = 0.0; carry.f = 0; }
+  __syncthreads();
+  for (int base = 0; base < ntiles; base += SCAN_BLOCK) {
+    int i = base + threadIdx.x;
+    SegPair v = i < ntiles ? tot[i] : SegPair{0.0, 0};
+    SegPair ex = block_seg_excl(v, &t);
+    SegPair c = carry;
+    if (i < ntiles) tot[i] = seg_op(c, ex);
+    __syncthreads();
+    if (threadIdx.x == 0) carry = seg_op(carry, t);
+    __syncthreads();
+  }
+}
+
+// Add each tile's incoming carry to its elements before the tile's first head.
+__global__ void k_segscan_add(double *__restrict__ out, const int *__restrict__ head,
+                              const SegPair *__restrict__ tot, long long n) {
+  long long tile = blockIdx.x;
+  long long beg = tile * SCAN_TILE, end = beg + SCAN_TILE < n ? beg + SCAN_TILE : n;
+  double c = tot[tile].v;
+  if (tile == 0) return;
+  // elements up to (excluding) the first head of the tile receive the carry
+  __shared__ long long first;
+  if (threadIdx.x == 0) first = end;
+  __syncthreads();
+  for (long long i = beg + threadIdx.x; i < end; i += blockDim.x)
+    if (head[i]) atomicMin((unsigned long long *)&first, (unsigned long long)i);
+  __syncthreads();
+  for (long long i = beg + threadIdx.x; i < first; i += blockDim.x) out[i] += c;
+}
+
+inline int segmented_scan(cudaStream_t st, const double *in, const int *head, double *out,
+                          long long n, SegPair *tmp) {
+  if (n <= 0) return 0;
+  int tiles = (int)((n + SCAN_TILE - 1) / SCAN_TILE);
+  k_segscan_tiles<<<tiles, SCAN_BLOCK, 0, st>>>(in, head, out, tmp, n);
+  k_segscan_totals<<<1, SCAN_BLOCK, 0, st>>>(tmp, tiles);
+  k_segscan_add<<<tiles, 256, 0, st>>>(out, head, tmp, n);
+  return (int)cudaGetLastError();
+}
+
+}  // namespace casl

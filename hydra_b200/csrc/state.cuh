@@ -1,0 +1,77 @@
+// Device state of one simulation handle and internal entry points shared
+// between the translation units of the library.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "../../include/hydra_casl.h"
+#include "common.cuh"
+
+struct casl_handle {
+  casl_params p;
+  casl::Consts c;
+  int device;
+  cudaStream_t stream;
+  int last_cuda;
+  int n;                 // nx == ny
+  long long npm, nm;     // capacities
+  double qjump;          // host copy
+  int nq, nptq;          // host copies of the counts
+  int ireg;              // regularisations since the last recontouring
+  int contex;
+
+  // nodes (structure of arrays; nextq 0-based internally)
+  double *xq, *yq;
+  int *nextq;
+  double *xqi, *yqi, *xqf, *yqf, *uq, *vq;
+  // contours (0-based i1q, i2q internally)
+  int *i1q, *i2q, *npq, *indq;
+
+  // fields, n*n doubles each
+  double *qr, *qs, *qd, *qc, *qq, *pp, *uu, *vv, *emq, *epq, *qspre;
+  double *sqs, *sqd, *qsi, *qsf, *qdi, *qdf;
+  double *w[6];          // work fields
+  // tables
+  double *green, *flo, *fhi, *qdiss, *hrkx, *hrky, *bety, *betac;
+  double2 *tw;           // exp(-2 pi i k / n), k < n
+
+  // con2grid scratch
+  int *fineJ;            // (nyf, nxf): row 0 = bottom level, rows 1.. = jump counts
+  int *ljx;              // (nxf)
+  int *coarseC;          // (n*n) coarse integer cells
+  // reductions
+  double *part;          // per-block partials
+  casl::Scalars *scal;   // device scalars
+  casl::Scalars *hscal;  // pinned host mirror
+
+  // surgery / renode / recontour scratch (allocated on first use)
+  void *sx;
+  size_t sx_bytes;
+};
+
+namespace casl {
+
+int set_cuda_error(casl_handle *h, cudaError_t e);
+int check_launch(casl_handle *h);
+
+// Spectral transforms on device buffers (in/out may alias only where noted).
+// ptospc: phys (n*n, [ix][iy]) -> spec ([ky][kx]); spec must not alias phys.
+int ptospc_dev(casl_handle *h, const double *phys, double *spec);
+// spctop: spec -> phys using tmp (n*n); spec is preserved.
+int spctop_dev(casl_handle *h, const double *spec, double *phys, double *tmp);
+
+int con2grid_dev(casl_handle *h);                   // -> coarseC, scal->csum
+int con2grid_to_spec(casl_handle *h, double *spec); // con2grid + ptospc fused load
+int con2grid_to_phys(casl_handle *h, double *phys); // con2grid + finalize to qc(ny,nx)
+
+int surgery_dev(casl_handle *h);
+int recontour_dev(casl_handle *h, const double *qq_dev);
+int renode_host(casl_handle *h, const double *xd, const double *yd, int npd, double *xr,
+                double *yr, int cap, int *npr);
+
+int sync_counts(casl_handle *h);    // device counts -> host copies
+int ensure_scratch(casl_handle *h, size_t bytes);
+
+}  // namespace casl

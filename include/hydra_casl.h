@@ -1,0 +1,169 @@
+/*
+ * hydra_casl.h -- C ABI of the B200 contour-advection (CLAM / "caps") time
+ * step for the doubly periodic plane.
+ *
+ * Drop-in boundary for the module procedures of Hydra's
+ * basic_hydra/ca/plane/qg/caps Fortran program.  Each entry point below
+ * names the reference procedure (file:line) whose body it replaces.  The
+ * reference keeps its state in module globals (contours.f90:12-15,
+ * evolution.f90:10-16, common.f90:12-16); here that state lives on one GPU
+ * behind an opaque handle, and the Fortran host passes its arrays by pointer
+ * (iso_c_binding) when it needs to move them in or out.
+ *
+ * Conventions
+ *   - Plain C types only; every pointer argument is HOST memory unless the
+ *     name says "_dev".
+ *   - Physical fields are Fortran (ny,nx) column-major double arrays
+ *     (iy fastest); spectral fields are Fortran (nx,ny) (kx fastest), in
+ *     stafft's "Hermitian" layout (lib/stafft/stafft.f90:55-58).
+ *   - Contour index arrays are 1-based exactly as in the reference:
+ *     nextq(i) in 1..nptq, i1q/i2q in 1..nptq.
+ *   - Every function returns 0 on success or a CASL_E* code; nothing aborts
+ *     the host process, and no device wait is unbounded.
+ *   - One handle is used by one host thread at a time; all work is ordered
+ *     on the handle's own CUDA stream.
+ */
+#ifndef HYDRA_CASL_H
+#define HYDRA_CASL_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define CASL_OK 0
+#define CASL_EINVAL 1      /* bad argument (size, null pointer, parameter) */
+#define CASL_ECAPACITY 2   /* node / contour / crossing capacity exceeded */
+#define CASL_ECUDA 3       /* CUDA runtime error (see casl_last_cuda_error) */
+#define CASL_ENOMEM 4      /* device allocation failed */
+#define CASL_EDOMAIN 5     /* a node left the domain or became non-finite */
+#define CASL_ETIMEOUT 6    /* a bounded device-side wait gave up */
+#define CASL_EUNSUPPORTED 7
+
+/* ---- parameters (parameters.f90 / constants.f90 of QG caps) ------------- */
+typedef struct casl_params {
+  int nx, ny;            /* inversion grid; nx == ny, a power of two 32..2048 */
+  int ncontq;            /* number of PV jumps used to set qjump (N_CONTQ) */
+  double ellx, elly;     /* domain lengths (L_X, L_Y), domain centred on 0 */
+  double kd, beta;       /* deformation wavenumber (K_D), PV gradient (PV_GRAD) */
+  double rtherm, rekman; /* thermal / Ekman damping rates */
+  double cdamp, nnu;     /* hyperdiffusion coefficient (C_DAMP) and power */
+  long long npm;         /* node capacity (reference: 500*nx*ny) */
+  long long nm;          /* contour capacity (reference: npm/20+npm/200) */
+  int nlevm;             /* level offset used by recontouring (2000) */
+  double fixed_dt;       /* > 0: use this dt instead of adapt's choice */
+  double dtmax;          /* adapt's cap on dt (0.2*min(tgsave,tcsave)) */
+  int force_surgery;     /* 1: regularise every step (else when twist > twistmax) */
+  int nregmax;           /* regularisations between recontourings (20) */
+  double twistmax;       /* 2.5 */
+} casl_params;
+
+typedef struct casl_handle casl_handle;
+
+/* Field selectors for casl_get_field / casl_set_field. */
+#define CASL_QS 0   /* spectral (nx,ny): q_s, evolved PV anomaly   (common.f90:15) */
+#define CASL_QD 1   /* spectral: q_d, residual PV                  (evolution.f90:14) */
+#define CASL_QC 2   /* spectral: contour PV                         (evolution.f90:14) */
+#define CASL_QQ 3   /* spectral: full PV anomaly                    (evolution.f90:14) */
+#define CASL_PP 4   /* spectral: streamfunction                     (evolution.f90:14) */
+#define CASL_QSPRE 5
+#define CASL_EMQ 6
+#define CASL_EPQ 7
+#define CASL_UU 8   /* physical (ny,nx): velocity u                 (evolution.f90:11) */
+#define CASL_VV 9   /* physical: velocity v */
+#define CASL_QR 10  /* physical: residual PV for recontouring       (common.f90:12) */
+
+/* Scalar selectors for casl_get_scalar / casl_set_scalar. */
+#define CASL_T 0
+#define CASL_DT 1
+#define CASL_TWIST 2
+#define CASL_IREG 3
+#define CASL_ZZRMS 4
+#define CASL_ZZMAX 5
+#define CASL_UUMAX 6
+#define CASL_QJUMP 7
+
+/* ---- lifetime ------------------------------------------------------------ */
+/* init_spectral + init_contours (spectral.f90:42-158, contours.f90:48-132):
+ * builds wavenumber, filter and Green-function tables and allocates the
+ * device state for the given capacities. */
+int casl_create(const casl_params *p, int device, casl_handle **out);
+void casl_destroy(casl_handle *h);
+const char *casl_error_string(int code);
+int casl_last_cuda_error(casl_handle *h);   /* cudaError_t of the last failure */
+int casl_synchronize(casl_handle *h);
+
+/* ---- state transfer (host <-> device) ------------------------------------ */
+/* Replaces the module state xq,yq,nextq,indq,npq,i1q,i2q,nq,nptq,qjump
+ * (contours.f90:12-15).  Arrays are 1-based in content (nextq values). */
+int casl_set_contours(casl_handle *h, int nq, int nptq, double qjump,
+                      const double *xq, const double *yq, const int *nextq,
+                      const int *indq, const int *npq, const int *i1q, const int *i2q);
+int casl_get_counts(casl_handle *h, int *nq, int *nptq, double *qjump);
+int casl_get_contours(casl_handle *h, double *xq, double *yq, int *nextq,
+                      int *indq, int *npq, int *i1q, int *i2q);
+int casl_set_field(casl_handle *h, int which, const double *host);
+int casl_get_field(casl_handle *h, int which, double *host);
+int casl_get_scalar(casl_handle *h, int which, double *value);
+int casl_set_scalar(casl_handle *h, int which, double value);
+
+/* ---- module procedures ---------------------------------------------------- */
+/* ptospc / spctop (lib/stafft/sta2dfft.f90:103-165): rvar(ny,nx) <-> svar(nx,ny).
+ * Unlike the reference the input is not destroyed. */
+int casl_ptospc(casl_handle *h, const double *rvar, double *svar);
+int casl_spctop(casl_handle *h, const double *svar, double *rvar);
+
+/* con2grid (contours.f90:173-346) on the current contours.  qc(ny,nx) may be
+ * NULL.  levels (optional, (4ny,4nx) ints, iy fastest) receives the fine-grid
+ * PV level index whose qjump multiples the reference's fine grid holds. */
+int casl_con2grid(casl_handle *h, double *qc, int *levels);
+
+/* velint (contours.f90:136-169): bilinear interpolation of uu,vv (ny,nx) to
+ * the current nodes; uq, vq have nptq entries. */
+int casl_velint(casl_handle *h, const double *uu, const double *vv, double *uq, double *vq);
+
+/* main_invert (spectral.f90:304-342): qq (nx,ny) spectral -> uu,vv (ny,nx)
+ * physical, pp (nx,ny) spectral.  Any output may be NULL. */
+int casl_main_invert(casl_handle *h, const double *qq, double *uu, double *vv, double *pp);
+
+/* gradient (spectral.f90:345-366): ff spectral -> ffx, ffy physical. */
+int casl_gradient(casl_handle *h, const double *ff, double *ffx, double *ffy);
+
+/* inversion (evolution.f90:494-520) on the device state. */
+int casl_inversion(casl_handle *h);
+
+/* advance (evolution.f90:166-326): one RK4 step of nodes, qs and qd. */
+int casl_advance(casl_handle *h);
+
+/* surgery (contours.f90:350-683), including renode of every contour. */
+int casl_surgery(casl_handle *h);
+
+/* renode (contours.f90:687-933) of one closed contour given on the host;
+ * xr, yr must hold cap entries; *npr receives the new node count (0 = the
+ * contour is too small and is dropped). */
+int casl_renode(casl_handle *h, const double *xd, const double *yd, int npd,
+                double *xr, double *yr, int cap, int *npr);
+
+/* recontour (congen.f90:24-128): new contours from the current contours plus
+ * the residual qq (ny,nx); with no contours, qq is the full field. */
+int casl_recontour(casl_handle *h, const double *qq);
+
+/* ---- driver (caps.f90 / evolution.f90:advect) ------------------------------ */
+/* initialise (caps.f90:106-361, loopinit = 0) from the initial PV q(ny,nx),
+ * then recont (caps.f90:380-395) and the evolution init
+ * (evolution.f90:96-131). */
+int casl_initialise(casl_handle *h, const double *qq_init);
+
+/* nsteps passes of the advect loop body (evolution.f90:55-79): regularise
+ * (surgery; or prepare + recontour + init every nregmax) then advance. */
+int casl_step(casl_handle *h, int nsteps);
+
+/* Diagnostics: out[0] kinetic energy, out[1] potential energy
+ * (evolution.f90:612-644), out[2] integral of (q - beta y)^2 (generic.f90:48),
+ * out[3] contour circulation qjump * sum of signed contour areas. */
+int casl_diagnostics(casl_handle *h, double out[4]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
