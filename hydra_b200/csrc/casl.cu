@@ -964,6 +964,16 @@ int ensure_scratch(casl_handle *h, size_t bytes) {
   h->sx_bytes = bytes;
   return CASL_OK;
 }
+
+int ensure_scratch2(casl_handle *h, size_t bytes) {
+  if (h->sx2_bytes >= bytes) return CASL_OK;
+  if (h->sx2) cudaFree(h->sx2);
+  h->sx2 = nullptr;
+  h->sx2_bytes = 0;
+  CASL_CUDA_TRY(cudaMalloc(&h->sx2, bytes));
+  h->sx2_bytes = bytes;
+  return CASL_OK;
+}
 }  // namespace casl
 
 extern "C" {
@@ -1026,7 +1036,7 @@ static void free_all(casl_handle *h) {
                   h->vv, h->emq, h->epq, h->qspre, h->sqs, h->sqd, h->qsi, h->qsf, h->qdi,
                   h->qdf, h->green, h->flo, h->fhi, h->qdiss, h->w[0], h->hrkx, h->hrky,
                   h->bety, h->betac, h->tw, h->fineJ, h->ljx, h->coarseC, h->part, h->scal,
-                  h->sx};
+                  h->sx, h->sx2};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (h->hscal) cudaFreeHost(h->hscal);

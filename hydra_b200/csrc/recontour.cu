@@ -1,6 +1,962 @@
-// Recontouring (congen.f90:24-441).
+// Recontouring (congen.f90:24-441) on the GPU.
+//
+// 1. Ultra-fine field (16x): contour PV from integer jump counts
+//    (con2ugrid, congen.f90:338-441) plus the bilinear residual
+//    (congen.f90:45-61), or the bilinear field alone when there are no
+//    contours (congen.f90:63-95).
+// 2. Every grid-line crossing of every level is enumerated in the
+//    reference's numbering order (x lines: ix outer / iy inner, then y lines:
+//    iy outer / ix inner, congen.f90:200-254), then stably sorted by level.
+// 3. The per-box crossing tables (noctab/icrtab) become a hash on
+//    (level, box).  A crossing's successor is the out-crossing of the box it
+//    enters; only boxes with two out-crossings (saddles) depend on the order
+//    of the reference's traversal, so those few are resolved by a short
+//    exact simulation of that traversal over chains.
+// 4. Each contour starts at its lowest-numbered crossing (the reference's
+//    `free` loop); contours are ordered by level then by that crossing,
+//    gathered into walk order and renoded three times (congen.f90:295-310).
+#include <cub/device/device_radix_sort.cuh>
+#include <math.h>
+#include <stdio.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "renode.cuh"
+#include "scan.cuh"
 #include "state.cuh"
 
 namespace casl {
-int recontour_dev(casl_handle *h, const double *) { (void)h; return CASL_EUNSUPPORTED; }
+
+// ---------------------------------------------------------------------------
+// Ultra-fine field
+// ---------------------------------------------------------------------------
+__global__ void k_u_scatter(const double *__restrict__ xq, const double *__restrict__ yq,
+                            const int *__restrict__ nextq, int npt, double qjump,
+                            int *__restrict__ J, int *__restrict__ ljx, Consts c,
+                            int *__restrict__ err) {
+  const int nxu = c.nxu, nyu = c.nyu;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npt; i += gridDim.x * blockDim.x) {
+    int ia = nextq[i];
+    if (ia < 0 || ia >= npt) { atomicExch(err, CASL_EINVAL); continue; }
+    double xi = xq[i], yi = yq[i], xa = xq[ia], ya = yq[ia];
+    if (!(xi >= c.xmin && xi < c.xmax && yi >= c.ymin && yi < c.ymax)) {
+      atomicExch(err, CASL_EDOMAIN);
+      continue;
+    }
+    int ixci = f_int(c.glxui * (xi - c.xmin));
+    int ixca = f_int(c.glxui * (xa - c.xmin));
+    double xx = xa - xi;
+    double dx = xx - c.ellx * f_dint(xx * c.hlxi);
+    double yy = ya - yi;
+    double dy = yy - c.elly * f_dint(yy * c.hlyi);
+    int ixdif = ixca - ixci;
+    int nxc = ixdif - nxu * ((2 * ixdif) / nxu);
+    if (fabs(yy) > c.hly) {
+      double cc = f_sign1(dy);
+      double p = -(yi - c.hly * cc) / (dy + c.small);
+      int ix = 1 + f_int(c.glxui * fmod(c.ellx + c.hlx + xi + p * dx, c.ellx));
+      ix = ix < 1 ? 1 : (ix > nxu ? nxu : ix);
+      atomicAdd(&ljx[ix - 1], -(int)cc);
+    }
+    if (nxc != 0 && nxc >= -nxu && nxc <= nxu) {
+      int jump = f_isign1(nxc);
+      int ixbeg = ixci + (1 + jump) / 2 + nxu;
+      for (int ncr = 0; ncr != nxc; ncr += jump) {
+        int m = (ixbeg + ncr) % nxu;
+        if (m < 0) m += nxu;
+        int ix = 1 + m;
+        double xgu = c.xmin + c.glxu * (double)(ix - 1);
+        double x2 = xgu - xi;
+        double px0 = (x2 - c.ellx * f_dint(x2 * c.hlxi)) / dx;
+        double y2 = yi + px0 * dy;
+        int iy = 2 + f_int(c.glyui * (y2 - c.elly * f_dint(y2 * c.hlyi) - c.ymin));
+        if (iy >= 2 && iy <= nyu) atomicAdd(&J[(long long)(ix - 1) * nyu + (iy - 1)], jump);
+      }
+    }
+  }
+}
+
+__global__ void k_u_lbot(const int *__restrict__ ljx, int *__restrict__ J, int nxu, int nyu) {
+  __shared__ int warp_tot[32];
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int base = 0; base < nxu; base += blockDim.x) {
+    int i = base + threadIdx.x;
+    int v = i < nxu ? ljx[i] : 0;
+    int x = warp_incl_scan(v);
+    if (lane == 31) warp_tot[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+      int t = lane < nw ? warp_tot[lane] : 0;
+      t = warp_incl_scan(t);
+      if (lane < nw) warp_tot[lane] = t;
+    }
+    __syncthreads();
+    int incl = x + (wid > 0 ? warp_tot[wid - 1] : 0) + carry;
+    if (i < nxu) J[(long long)i * nyu] = incl - v;
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) carry = incl;
+    __syncthreads();
+  }
+}
+
+// column sweep (congen.f90:419-423) with the column sums for the mean
+__global__ void k_u_colscan(int *__restrict__ J, int nxu, int nyu,
+                            unsigned long long *__restrict__ total) {
+  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (warp >= nxu) return;
+  int *col = J + (long long)warp * nyu;
+  int carry = 0;
+  long long s = 0;
+  for (int base = 0; base < nyu; base += 32) {
+    int x = warp_incl_scan(col[base + lane]) + carry;
+    col[base + lane] = x;
+    s += x;
+    carry = __shfl_sync(0xffffffffu, x, 31);
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (lane == 0) atomicAdd(total, (unsigned long long)s);
+}
+
+// qa = (L*qjump - qavg) + bilinear residual, or the bilinear field alone.
+__global__ void k_u_field(const int *__restrict__ L, const unsigned long long *__restrict__ lsum,
+                          const double *__restrict__ qq, double qjump, int have_contours,
+                          double *__restrict__ qa, double *__restrict__ part, Consts c) {
+  const int nxu = c.nxu, nyu = c.nyu, n = c.nx;
+  const long long nu = (long long)nxu * nyu;
+  double qavg = 0.0;
+  if (have_contours) qavg = qjump * ((double)(long long)(*lsum) / ((double)nxu * (double)nyu));
+  const double fac = 1.0 / 16.0;
+  double mx = -1.0e308, mn = 1.0e308;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nu;
+       t += (long long)gridDim.x * blockDim.x) {
+    int iy = (int)(t % nyu) + 1, ix = (int)(t / nyu) + 1;
+    int ixx = (ix - 1) / 16, iyy = (iy - 1) / 16;
+    int ix0 = 1 + ixx, ix1 = 2 + ixx - n * (ix0 / n), ixf = ix - 16 * ixx;
+    int iy0 = 1 + iyy, iy1 = 2 + iyy - n * (iy0 / n), iyf = iy - 16 * iyy;
+    double pxf = fac * (double)(ixf - 1), pxc = 1.0 - pxf;
+    double pyf = fac * (double)(iyf - 1), pyc = 1.0 - pyf;
+    double w00 = pyc * pxc, w10 = pyf * pxc, w01 = pyc * pxf, w11 = pyf * pxf;
+    double q00 = qq[(long long)(ix0 - 1) * n + iy0 - 1], q10 = qq[(long long)(ix0 - 1) * n + iy1 - 1];
+    double q01 = qq[(long long)(ix1 - 1) * n + iy0 - 1], q11 = qq[(long long)(ix1 - 1) * n + iy1 - 1];
+    double v;
+    if (have_contours) {
+      v = (double)L[t] * qjump - qavg;
+      v = v + w00 * q00 + w10 * q10 + w01 * q01 + w11 * q11;
+    } else {
+      v = w00 * q00 + w10 * q10 + w01 * q01 + w11 * q11;
+    }
+    qa[t] = v;
+    mx = fmax(mx, v);
+    mn = fmin(mn, v);
+  }
+  __shared__ double a[256], b[256];
+  a[threadIdx.x] = mx;
+  b[threadIdx.x] = mn;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      a[threadIdx.x] = fmax(a[threadIdx.x], a[threadIdx.x + o]);
+      b[threadIdx.x] = fmin(b[threadIdx.x], b[threadIdx.x + o]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = a[0];
+    part[2 * blockIdx.x + 1] = b[0];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Crossings
+// ---------------------------------------------------------------------------
+struct LevInfo {
+  int levbeg, levend;
+  double qjump, qoff, qjumpi;
+};
+
+__device__ __forceinline__ double qtmp_of(int lev, const LevInfo &li) {
+  return ((double)lev - 0.5) * li.qjump - li.qoff;
+}
+
+// Levels whose contour value q_lev satisfies lo < q_lev <= hi, i.e. where the
+// reference's sign(qa - qtmp) differs at the two ends (congen.f90:205-212).
+__device__ __forceinline__ void crossed_levels(double a, double b, const LevInfo &li, int &l1,
+                                               int &l2) {
+  double lo = fmin(a, b), hi = fmax(a, b);
+  int g1 = (int)floor((lo + li.qoff) * li.qjumpi + 0.5) - 1;
+  int g2 = (int)floor((hi + li.qoff) * li.qjumpi + 0.5) + 2;
+  g1 = max(g1, li.levbeg);
+  g2 = min(g2, li.levend);
+  while (g1 <= g2 && !(qtmp_of(g1, li) > lo)) g1++;
+  while (g2 >= g1 && !(qtmp_of(g2, li) <= hi)) g2--;
+  l1 = g1;
+  l2 = g2;
+}
+
+__device__ __forceinline__ void edge_values(const double *__restrict__ qa, long long e, int nxu,
+                                            int nyu, double &a, double &b) {
+  const long long NE = (long long)nxu * nyu;
+  if (e < NE) {
+    int ix = (int)(e / nyu), iy = (int)(e % nyu);
+    a = qa[(long long)ix * nyu + iy];
+    b = qa[(long long)ix * nyu + (iy + 1 == nyu ? 0 : iy + 1)];
+  } else {
+    long long f = e - NE;
+    int iy = (int)(f / nxu), ix = (int)(f % nxu);
+    a = qa[(long long)ix * nyu + iy];
+    b = qa[(long long)(ix + 1 == nxu ? 0 : ix + 1) * nyu + iy];
+  }
+}
+
+constexpr int EDGES_PER_THREAD = 16;
+
+__global__ void k_cr_count(const double *__restrict__ qa, LevInfo li, int nxu, int nyu,
+                           long long nchunks, int *__restrict__ cnt) {
+  const long long NE2 = 2LL * nxu * nyu;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nchunks;
+       t += (long long)gridDim.x * blockDim.x) {
+    int s = 0;
+    for (int q = 0; q < EDGES_PER_THREAD; q++) {
+      long long e = t * EDGES_PER_THREAD + q;
+      if (e >= NE2) break;
+      double a, b;
+      edge_values(qa, e, nxu, nyu, a, b);
+      if (a == b) continue;
+      int l1, l2;
+      crossed_levels(a, b, li, l1, l2);
+      if (l2 >= l1) s += l2 - l1 + 1;
+    }
+    cnt[t] = s;
+  }
+}
+
+__global__ void k_cr_emit(const double *__restrict__ qa, LevInfo li, int nxu, int nyu,
+                          long long nchunks, const int *__restrict__ off,
+                          unsigned long long *__restrict__ redge, int *__restrict__ rlev) {
+  const long long NE2 = 2LL * nxu * nyu;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nchunks;
+       t += (long long)gridDim.x * blockDim.x) {
+    int o = off[t];
+    for (int q = 0; q < EDGES_PER_THREAD; q++) {
+      long long e = t * EDGES_PER_THREAD + q;
+      if (e >= NE2) break;
+      double a, b;
+      edge_values(qa, e, nxu, nyu, a, b);
+      if (a == b) continue;
+      int l1, l2;
+      crossed_levels(a, b, li, l1, l2);
+      for (int l = l1; l <= l2; l++) {
+        redge[o] = (unsigned long long)e;
+        rlev[o] = l - li.levbeg;
+        o++;
+      }
+    }
+  }
+}
+
+// Position and box transitions of every crossing (congen.f90:211-252).
+__global__ void k_cr_geom(const double *__restrict__ qa, const unsigned long long *__restrict__ redge,
+                          const int *__restrict__ rlev, long long ncr, LevInfo li, Consts c,
+                          double *__restrict__ xcr, double *__restrict__ ycr,
+                          unsigned int *__restrict__ kib, unsigned int *__restrict__ kob) {
+  const int nxu = c.nxu, nyu = c.nyu;
+  const long long NE = (long long)nxu * nyu;
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
+       r += (long long)gridDim.x * blockDim.x) {
+    long long e = (long long)redge[r];
+    double qtmp = qtmp_of(rlev[r] + li.levbeg, li);
+    if (e < NE) {
+      int ix = (int)(e / nyu) + 1, iy = (int)(e % nyu) + 1;
+      double q0 = qa[(long long)(ix - 1) * nyu + iy - 1] - qtmp;
+      double q1 = qa[(long long)(ix - 1) * nyu + (iy == nyu ? 0 : iy)] - qtmp;
+      int isy = (int)f_sign1(q0);
+      int inc = (1 - isy) / 2;
+      long long kaa = (long long)(iy - 1) * nxu + 1;
+      int j1 = ix + inc, j2 = ix + 1 - inc;
+      long long bx1 = j1 == 1 ? nxu - 1 : j1 - 2, bx2 = j2 == 1 ? nxu - 1 : j2 - 2;
+      kib[r] = (unsigned int)(kaa + bx1);
+      kob[r] = (unsigned int)(kaa + bx2);
+      xcr[r] = c.xmin + c.glxu * (double)(ix - 1);
+      double ygu = c.ymin + c.glyu * (double)(iy - 1);
+      double yy = ygu - c.glyu * q0 / (q1 - q0);
+      ycr[r] = c.oms * (yy - c.elly * f_dint(yy * c.hlyi));
+    } else {
+      long long f = e - NE;
+      int iy = (int)(f / nxu) + 1, ix = (int)(f % nxu) + 1;
+      double q0 = qa[(long long)(ix - 1) * nyu + iy - 1] - qtmp;
+      double q1 = qa[(long long)(ix == nxu ? 0 : ix) * nyu + iy - 1] - qtmp;
+      int isx = (int)f_sign1(q0);
+      int inc = (1 - isx) / 2;
+      int j1 = iy + 1 - inc, j2 = iy + inc;
+      long long by1 = j1 == 1 ? nyu - 1 : j1 - 2, by2 = j2 == 1 ? nyu - 1 : j2 - 2;
+      kib[r] = (unsigned int)((long long)nxu * by1 + ix);
+      kob[r] = (unsigned int)((long long)nxu * by2 + ix);
+      ycr[r] = c.ymin + c.glyu * (double)(iy - 1);
+      double xgu = c.xmin + c.glxu * (double)(ix - 1);
+      double xx = xgu - c.glxu * q0 / (q1 - q0);
+      xcr[r] = c.oms * (xx - c.ellx * f_dint(xx * c.hlxi));
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// (level, box) -> out-crossings hash (the reference's noctab/icrtab)
+// ---------------------------------------------------------------------------
+constexpr unsigned long long HEMPTY = ~0ull;
+
+__device__ __forceinline__ unsigned long long hkey(int lev, unsigned int box) {
+  return ((unsigned long long)(unsigned int)lev << 32) | box;
+}
+__device__ __forceinline__ unsigned long long hmix(unsigned long long k) {
+  k ^= k >> 33;
+  k *= 0xff51afd7ed558ccdULL;
+  k ^= k >> 33;
+  k *= 0xc4ceb9fe1a85ec53ULL;
+  k ^= k >> 33;
+  return k;
+}
+
+__global__ void k_h_insert(const int *__restrict__ rlev, const unsigned int *__restrict__ kob,
+                           long long ncr, unsigned long long *__restrict__ keys,
+                           int *__restrict__ slots, unsigned long long mask, int *__restrict__ err) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
+       r += (long long)gridDim.x * blockDim.x) {
+    unsigned long long k = hkey(rlev[r], kob[r]);
+    unsigned long long p = hmix(k) & mask;
+    for (unsigned long long probe = 0; probe <= mask; probe++) {
+      unsigned long long prev = atomicCAS(&keys[p], HEMPTY, k);
+      if (prev == HEMPTY || prev == k) {
+        if (atomicCAS(&slots[2 * p], -1, (int)r) != -1)
+          if (atomicCAS(&slots[2 * p + 1], -1, (int)r) != -1) atomicExch(err, CASL_ECAPACITY);
+        break;
+      }
+      p = (p + 1) & mask;
+    }
+  }
+}
+
+__global__ void k_h_order(const unsigned long long *__restrict__ keys, int *__restrict__ slots,
+                          unsigned long long cap) {
+  for (unsigned long long p = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; p < cap;
+       p += (unsigned long long)gridDim.x * blockDim.x) {
+    if (keys[p] == HEMPTY) continue;
+    int a = slots[2 * p], b = slots[2 * p + 1];
+    if (b >= 0 && b < a) {
+      slots[2 * p] = b;
+      slots[2 * p + 1] = a;
+    }
+  }
+}
+
+__device__ __forceinline__ long long h_find(const unsigned long long *__restrict__ keys,
+                                            unsigned long long mask, unsigned long long k) {
+  unsigned long long p = hmix(k) & mask;
+  for (unsigned long long probe = 0; probe <= mask; probe++) {
+    unsigned long long v = keys[p];
+    if (v == k) return (long long)p;
+    if (v == HEMPTY) return -1;
+    p = (p + 1) & mask;
+  }
+  return -1;
+}
+
+// successor of each crossing; -1 where it enters a saddle box (2 out-crossings)
+__global__ void k_h_succ(const int *__restrict__ rlev, const unsigned int *__restrict__ kib,
+                         long long ncr, const unsigned long long *__restrict__ keys,
+                         const int *__restrict__ slots, unsigned long long mask,
+                         int *__restrict__ succ, long long *__restrict__ sadslot,
+                         int *__restrict__ err) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
+       r += (long long)gridDim.x * blockDim.x) {
+    long long p = h_find(keys, mask, hkey(rlev[r], kib[r]));
+    if (p < 0) {
+      atomicExch(err, CASL_EINVAL);
+      succ[r] = -1;
+      sadslot[r] = -1;
+      continue;
+    }
+    if (slots[2 * p + 1] < 0) {
+      succ[r] = slots[2 * p];
+      sadslot[r] = -1;
+    } else {
+      succ[r] = -1;
+      sadslot[r] = p;
+    }
+  }
+}
+
+// pointer jumping: minimum index along the path and list length to the end
+__global__ void k_pj_init(const int *__restrict__ succ, long long ncr, int *__restrict__ nx,
+                          int *__restrict__ lab, int *__restrict__ term) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
+       r += (long long)gridDim.x * blockDim.x) {
+    int s = succ[r];
+    nx[r] = s < 0 ? (int)r : s;
+    lab[r] = (int)r;
+    term[r] = s < 0;
+  }
+}
+
+__global__ void k_pj_min(const int *__restrict__ nx, const int *__restrict__ lab,
+                         const int *__restrict__ term, long long ncr, int *__restrict__ nx2,
+                         int *__restrict__ lab2, int *__restrict__ term2) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
+       r += (long long)gridDim.x * blockDim.x) {
+    int n = nx[r];
+    lab2[r] = min(lab[r], lab[n]);
+    term2[r] = term[r] | term[n];
+    nx2[r] = nx[n];
+  }
+}
+
+// list for ranking: cycles cut before their minimum, chains end at their end
+__global__ void k_pj_listinit(const int *__restrict__ succ, const int *__restrict__ lab,
+                              const int *__restrict__ term, long long ncr, int *__restrict__ nx,
+                              int *__restrict__ val) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
+       r += (long long)gridDim.x * blockDim.x) {
+    int s = succ[r];
+    if (term[r])
+      nx[r] = s;
+    else
+      nx[r] = (s == lab[r]) ? -1 : s;
+    val[r] = 1;
+  }
+}
+
+__global__ void k_pj_rank(const int *__restrict__ nx, const int *__restrict__ val, long long ncr,
+                          int *__restrict__ nx2, int *__restrict__ val2) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
+       r += (long long)gridDim.x * blockDim.x) {
+    int n = nx[r];
+    val2[r] = val[r] + (n >= 0 ? val[n] : 0);
+    nx2[r] = n >= 0 ? nx[n] : -1;
+  }
+}
+
+// chain end of each chain crossing (endp) via a second jump over succ
+__global__ void k_pj_endinit(const int *__restrict__ succ, long long ncr, int *__restrict__ ep) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
+       r += (long long)gridDim.x * blockDim.x)
+    ep[r] = succ[r] < 0 ? (int)r : succ[r];
+}
+__global__ void k_pj_end(const int *__restrict__ ep, long long ncr, int *__restrict__ ep2) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
+       r += (long long)gridDim.x * blockDim.x)
+    ep2[r] = ep[ep[r]];
+}
+
+// contour start flags and lengths for plain cycles (start = cycle minimum)
+__global__ void k_ct_plain(const int *__restrict__ lab, const int *__restrict__ term,
+                           const int *__restrict__ val, long long ncr, int *__restrict__ startf,
+                           int *__restrict__ clenr) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
+       r += (long long)gridDim.x * blockDim.x) {
+    bool st = !term[r] && lab[r] == (int)r;
+    startf[r] = st;
+    clenr[r] = st ? val[r] : 0;
+  }
+}
+
+// positions of plain-cycle crossings in walk layout
+__global__ void k_ct_gather_plain(const int *__restrict__ lab, const int *__restrict__ term,
+                                  const int *__restrict__ val, const int *__restrict__ cidx,
+                                  const int *__restrict__ coff, const int *__restrict__ clen,
+                                  const double *__restrict__ xcr, const double *__restrict__ ycr,
+                                  long long ncr, double *__restrict__ xw, double *__restrict__ yw) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
+       r += (long long)gridDim.x * blockDim.x) {
+    if (term[r]) continue;
+    int s = lab[r];
+    int c = cidx[s];
+    long long pos = (long long)coff[c] + (clen[c] - val[r]);
+    xw[pos] = xcr[r];
+    yw[pos] = ycr[r];
+  }
+}
+
+// chain crossings: position from the per-chain placement of the simulation
+__global__ void k_ct_gather_chain(const int *__restrict__ term, const int *__restrict__ ep,
+                                  const int *__restrict__ val, const int *__restrict__ chain_of_end,
+                                  const long long *__restrict__ chpos, const int *__restrict__ chlen,
+                                  const int *__restrict__ chrot, const int *__restrict__ chclen,
+                                  const double *__restrict__ xcr, const double *__restrict__ ycr,
+                                  long long ncr, double *__restrict__ xw, double *__restrict__ yw) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
+       r += (long long)gridDim.x * blockDim.x) {
+    if (!term[r]) continue;
+    int ch = chain_of_end[ep[r]];
+    if (ch < 0) continue;
+    int local = chlen[ch] - val[r];          // position from the chain start
+    long long pos;
+    int rot = chrot[ch];
+    if (rot < 0) {
+      pos = chpos[ch] + local;
+    } else {
+      // first chain of a contour started mid-chain at local index rot
+      int L = chclen[ch];
+      int rel = local >= rot ? local - rot : L - rot + local;
+      pos = chpos[ch] + rel;
+    }
+    xw[pos] = xcr[r];
+    yw[pos] = ycr[r];
+  }
+}
+
+__global__ void k_lev_of_contour(const int *__restrict__ startf, const int *__restrict__ rlev,
+                                 const int *__restrict__ cidx, long long ncr, LevInfo li,
+                                 int nlevm, int *__restrict__ clevt) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
+       r += (long long)gridDim.x * blockDim.x) {
+    if (!startf[r]) continue;
+    int lev = rlev[r] + li.levbeg;
+    clevt[cidx[r]] = lev - nlevm + (lev - 1) / nlevm - 1;
+  }
+}
+
+__global__ void k_set_counts2(Scalars *s, const int *cnt) {
+  s->nq = cnt[0];
+  s->nptq = cnt[1];
+}
+__global__ void k_out_contours(const int *__restrict__ ocs, const int *__restrict__ olen,
+                               const int *__restrict__ olev, int nq, int *__restrict__ i1q,
+                               int *__restrict__ i2q, int *__restrict__ npq,
+                               int *__restrict__ indq) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nq; j += gridDim.x * blockDim.x) {
+    i1q[j] = ocs[j];
+    i2q[j] = ocs[j] + olen[j] - 1;
+    npq[j] = olen[j];
+    indq[j] = olev[j];
+  }
+}
+__global__ void k_out_links(const int *__restrict__ ocs, const int *__restrict__ olen, int nq,
+                            int npt, int *__restrict__ nextq) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npt; i += gridDim.x * blockDim.x) {
+    int j = contour_of(ocs, nq, i);
+    nextq[i] = i + 1 < ocs[j] + olen[j] ? i + 1 : ocs[j];
+  }
+}
+
+static inline int gsz(long long work) {
+  long long g = (work + 255) / 256;
+  if (g < 1) g = 1;
+  if (g > 148 * 32) g = 148 * 32;
+  return (int)g;
+}
+
+#define RC_TRY(x)        \
+  do {                   \
+    int _r = (x);        \
+    if (_r) return _r;   \
+  } while (0)
+
+static int fetch_err(casl_handle *h) {
+  int e = 0;
+  cudaMemcpyAsync(&e, &h->scal->error, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+  cudaError_t ce = cudaStreamSynchronize(h->stream);
+  if (ce != cudaSuccess) return set_cuda_error(h, ce);
+  return e;
+}
+
+int recontour_dev(casl_handle *h, const double *qq) {
+  cudaStream_t st = h->stream;
+  const Consts &c = h->c;
+  if (c.beffect) return CASL_EUNSUPPORTED;  // beta != 0 uses econgen.f90
+  const int nxu = c.nxu, nyu = c.nyu;
+  const long long NU = (long long)nxu * nyu;
+  const double qjump = h->qjump;
+  const int have = h->nptq > 0 && h->nq > 0;
+  cudaMemsetAsync(&h->scal->error, 0, sizeof(int), st);
+
+  // --- 1. ultra-fine field ---------------------------------------------------
+  if (!have) {
+    // l1norm (generic.f90:180-194) of the full field: nothing to contour if ~0
+    std::vector<double> hq((size_t)c.nx * c.ny);
+    CASL_CUDA_TRY(cudaMemcpyAsync(hq.data(), qq, hq.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CASL_CUDA_TRY(cudaStreamSynchronize(st));
+    double l1 = 0.0;
+    for (double v : hq) l1 += fabs(v);
+    if (c.garea * l1 < c.small) {
+      h->nq = h->nptq = 0;
+      h->hscal->nq = h->hscal->nptq = 0;
+      int z[2] = {0, 0};
+      int *dz = &h->scal->nq;
+      CASL_CUDA_TRY(cudaMemcpyAsync(dz, z, 2 * sizeof(int), cudaMemcpyHostToDevice, st));
+      CASL_CUDA_TRY(cudaStreamSynchronize(st));
+      return CASL_OK;
+    }
+  }
+  // Field memory: qa (double) + integer levels; kept for the whole call.
+  size_t need_field = (size_t)NU * 12 + ((size_t)64 << 20);
+  RC_TRY(ensure_scratch(h, need_field));
+  Arena ar{(char *)h->sx, h->sx_bytes, 0};
+  double *qa = ar.get<double>(NU);
+  int *Lu = ar.get<int>(NU);
+  int *ljx = ar.get<int>(nxu);
+  unsigned long long *lsum = ar.get<unsigned long long>(4);
+  double *part = ar.get<double>(2 * 4096);
+  if (!part) return CASL_ENOMEM;
+  if (have) {
+    CASL_CUDA_TRY(cudaMemsetAsync(Lu, 0, (size_t)NU * sizeof(int), st));
+    CASL_CUDA_TRY(cudaMemsetAsync(ljx, 0, (size_t)nxu * sizeof(int), st));
+    CASL_CUDA_TRY(cudaMemsetAsync(lsum, 0, sizeof(unsigned long long), st));
+    k_u_scatter<<<gsz(h->nptq), 256, 0, st>>>(h->xq, h->yq, h->nextq, h->nptq, qjump, Lu, ljx, c,
+                                              &h->scal->error);
+    k_u_lbot<<<1, 1024, 0, st>>>(ljx, Lu, nxu, nyu);
+    k_u_colscan<<<(nxu * 32 + 255) / 256, 256, 0, st>>>(Lu, nxu, nyu, lsum);
+  }
+  const int fb = 4096;
+  k_u_field<<<fb, 256, 0, st>>>(Lu, lsum, qq, qjump, have, qa, part, c);
+  RC_TRY(check_launch(h));
+  RC_TRY(fetch_err(h));
+  std::vector<double> hp(2 * fb);
+  CASL_CUDA_TRY(cudaMemcpyAsync(hp.data(), part, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CASL_CUDA_TRY(cudaStreamSynchronize(st));
+  double qamax = hp[0], qamin = hp[1];
+  for (int b = 1; b < fb; b++) {
+    qamax = std::max(qamax, hp[2 * b]);
+    qamin = std::min(qamin, hp[2 * b + 1]);
+  }
+  // --- 2. levels (congen.f90:156-173) ----------------------------------------
+  LevInfo li;
+  li.qjump = qjump;
+  li.qjumpi = 1.0 / qjump;
+  li.qoff = qjump * (double)h->p.nlevm;
+  li.levbeg = (int)((li.qoff + qamin) * li.qjumpi + 0.5) + 1;
+  li.levend = (int)((li.qoff + qamax) * li.qjumpi + 0.5);
+  auto set_empty = [&]() -> int {
+    h->nq = h->nptq = 0;
+    int z[2] = {0, 0};
+    CASL_CUDA_TRY(cudaMemcpyAsync(&h->scal->nq, z, 2 * sizeof(int), cudaMemcpyHostToDevice, st));
+    CASL_CUDA_TRY(cudaStreamSynchronize(st));
+    return CASL_OK;
+  };
+  if (li.levbeg > li.levend) return set_empty();
+  const int nlev = li.levend - li.levbeg + 1;
+
+  // --- 3. crossings in reference order, stably sorted by level ----------------
+  const long long NE2 = 2 * NU;
+  const long long nchunks = (NE2 + EDGES_PER_THREAD - 1) / EDGES_PER_THREAD;
+  int *ccnt = ar.get<int>(nchunks), *coffs = ar.get<int>(nchunks);
+  int *tmpi = ar.get<int>(scan_tmp_elems(nchunks) + 4);
+  int *dtot = ar.get<int>(16);
+  if (!dtot) return CASL_ENOMEM;
+  k_cr_count<<<gsz(nchunks), 256, 0, st>>>(qa, li, nxu, nyu, nchunks, ccnt);
+  exclusive_scan<int>(st, ccnt, coffs, nchunks, tmpi, dtot);
+  int ncr_i = 0;
+  CASL_CUDA_TRY(cudaMemcpyAsync(&ncr_i, dtot, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CASL_CUDA_TRY(cudaStreamSynchronize(st));
+  const long long ncr = ncr_i;
+  if (ncr == 0) return set_empty();
+  // Per-crossing storage lives in a second arena sized from the count, so
+  // that the ultra-fine field in the first one is kept.
+  int endbit = 1;
+  while ((1 << endbit) < nlev + 1) endbit++;
+  size_t sort_bytes = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, (int *)nullptr, (int *)nullptr,
+                                  (unsigned long long *)nullptr, (unsigned long long *)nullptr,
+                                  (int)ncr, 0, endbit, st);
+  {
+    unsigned long long capb = 1;
+    while (capb < (unsigned long long)(2 * ncr)) capb <<= 1;
+    long long capn = std::max<long long>(ncr * 2, h->npm);
+    size_t need2 = (size_t)ncr * 460 + (size_t)capb * 16 + (size_t)capn * 32 + sort_bytes +
+                   ((size_t)64 << 20);
+    RC_TRY(ensure_scratch2(h, need2));
+  }
+  Arena ar2{(char *)h->sx2, h->sx2_bytes, 0};
+  unsigned long long *redge = ar2.get<unsigned long long>(ncr), *redge2 = ar2.get<unsigned long long>(ncr);
+  int *rlev = ar2.get<int>(ncr), *rlev2 = ar2.get<int>(ncr);
+  int *tmpi2 = ar2.get<int>(scan_tmp_elems(ncr) + 4);
+  void *sort_tmp = ar2.get<char>(sort_bytes + 16);
+  if (!sort_tmp) return CASL_ENOMEM;
+  k_cr_emit<<<gsz(nchunks), 256, 0, st>>>(qa, li, nxu, nyu, nchunks, coffs, redge, rlev);
+  CASL_CUDA_TRY(cub::DeviceRadixSort::SortPairs(sort_tmp, sort_bytes, rlev, rlev2, redge, redge2,
+                                                (int)ncr, 0, endbit, st));
+  std::swap(rlev, rlev2);
+  std::swap(redge, redge2);
+  double *xcr = ar2.get<double>(ncr), *ycr = ar2.get<double>(ncr);
+  unsigned int *kib = ar2.get<unsigned int>(ncr), *kob = ar2.get<unsigned int>(ncr);
+  if (!kob) return CASL_ENOMEM;
+  k_cr_geom<<<gsz(ncr), 256, 0, st>>>(qa, redge, rlev, ncr, li, c, xcr, ycr, kib, kob);
+  RC_TRY(check_launch(h));
+
+  // --- 4. box tables: hash (level, box) -> two out-crossing slots ------------
+  unsigned long long cap = 1;
+  while (cap < (unsigned long long)(2 * ncr)) cap <<= 1;
+  unsigned long long *keys = ar2.get<unsigned long long>(cap);
+  int *slots = ar2.get<int>(2 * cap);
+  int *succ = ar2.get<int>(ncr);
+  long long *sadslot = ar2.get<long long>(ncr);
+  if (!sadslot) return CASL_ENOMEM;
+  CASL_CUDA_TRY(cudaMemsetAsync(keys, 0xff, cap * sizeof(unsigned long long), st));
+  CASL_CUDA_TRY(cudaMemsetAsync(slots, 0xff, 2 * cap * sizeof(int), st));
+  k_h_insert<<<gsz(ncr), 256, 0, st>>>(rlev, kob, ncr, keys, slots, cap - 1, &h->scal->error);
+  k_h_order<<<gsz(cap), 256, 0, st>>>(keys, slots, cap);
+  k_h_succ<<<gsz(ncr), 256, 0, st>>>(rlev, kib, ncr, keys, slots, cap - 1, succ, sadslot,
+                                     &h->scal->error);
+  RC_TRY(check_launch(h));
+  RC_TRY(fetch_err(h));
+
+  // --- 5. pointer jumping over crossings --------------------------------------
+  int *nx = ar2.get<int>(ncr), *nx2 = ar2.get<int>(ncr), *lab = ar2.get<int>(ncr),
+      *lab2 = ar2.get<int>(ncr), *term = ar2.get<int>(ncr), *term2 = ar2.get<int>(ncr),
+      *val = ar2.get<int>(ncr), *val2 = ar2.get<int>(ncr), *ep = ar2.get<int>(ncr),
+      *ep2 = ar2.get<int>(ncr);
+  if (!ep2) return CASL_ENOMEM;
+  int rounds = 1;
+  while ((1LL << rounds) < ncr) rounds++;
+  rounds++;
+  int g = gsz(ncr);
+  k_pj_init<<<g, 256, 0, st>>>(succ, ncr, nx, lab, term);
+  for (int it = 0; it < rounds; it++) {
+    k_pj_min<<<g, 256, 0, st>>>(nx, lab, term, ncr, nx2, lab2, term2);
+    std::swap(nx, nx2); std::swap(lab, lab2); std::swap(term, term2);
+  }
+  k_pj_listinit<<<g, 256, 0, st>>>(succ, lab, term, ncr, nx, val);
+  for (int it = 0; it < rounds; it++) {
+    k_pj_rank<<<g, 256, 0, st>>>(nx, val, ncr, nx2, val2);
+    std::swap(nx, nx2); std::swap(val, val2);
+  }
+  k_pj_endinit<<<g, 256, 0, st>>>(succ, ncr, ep);
+  for (int it = 0; it < rounds; it++) {
+    k_pj_end<<<g, 256, 0, st>>>(ep, ncr, ep2);
+    std::swap(ep, ep2);
+  }
+  RC_TRY(check_launch(h));
+
+  // --- 6. saddle chains: exact simulation of the reference traversal ----------
+  // chain starts are the out-crossings of saddle boxes
+  std::vector<long long> hsad(ncr);
+  std::vector<int> hsucc_neg;  // crossing indices entering saddles
+  {
+    std::vector<int> hsucc(ncr);
+    CASL_CUDA_TRY(cudaMemcpyAsync(hsucc.data(), succ, ncr * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CASL_CUDA_TRY(cudaMemcpyAsync(hsad.data(), sadslot, ncr * sizeof(long long), cudaMemcpyDeviceToHost, st));
+    CASL_CUDA_TRY(cudaStreamSynchronize(st));
+    for (long long r = 0; r < ncr; r++)
+      if (hsucc[r] < 0) hsucc_neg.push_back((int)r);
+  }
+  const int nends = (int)hsucc_neg.size();
+  int nsad_contours = 0;
+  std::vector<int> sad_start;      // start crossing of each saddle contour
+  std::vector<int> sad_len;        // its length
+  std::vector<int> ch_end, ch_len, ch_rot, ch_clen, ch_cont;
+  std::vector<long long> ch_pos;   // position relative to the contour start (set later)
+  if (nends > 0) {
+    // gather per-saddle slots and per-chain data on the host (few entries)
+    std::vector<long long> sad_p;
+    for (int r : hsucc_neg) sad_p.push_back(hsad[r]);
+    std::sort(sad_p.begin(), sad_p.end());
+    sad_p.erase(std::unique(sad_p.begin(), sad_p.end()), sad_p.end());
+    int nsb = (int)sad_p.size();
+    std::vector<int> slot2(2 * nsb);
+    for (int b = 0; b < nsb; b++)
+      CASL_CUDA_TRY(cudaMemcpyAsync(&slot2[2 * b], slots + 2 * sad_p[b], 2 * sizeof(int),
+                                    cudaMemcpyDeviceToHost, st));
+    // chain starts and their ends, lengths, minima
+    int nch = 2 * nsb;
+    std::vector<int> cstart(nch), cend(nch), clen(nch), cmin(nch), clev(nch);
+    std::vector<int> h_ep(ncr), h_val(ncr), h_lab(ncr), h_lev(ncr);
+    CASL_CUDA_TRY(cudaMemcpyAsync(h_ep.data(), ep, ncr * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CASL_CUDA_TRY(cudaMemcpyAsync(h_val.data(), val, ncr * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CASL_CUDA_TRY(cudaMemcpyAsync(h_lab.data(), lab, ncr * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CASL_CUDA_TRY(cudaMemcpyAsync(h_lev.data(), rlev, ncr * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CASL_CUDA_TRY(cudaStreamSynchronize(st));
+    std::vector<std::pair<int, int>> start2ch;
+    for (int b = 0; b < nsb; b++)
+      for (int q = 0; q < 2; q++) {
+        int ch = 2 * b + q;
+        int s = slot2[2 * b + q];
+        cstart[ch] = s;
+        cend[ch] = h_ep[s];
+        clen[ch] = h_val[s];
+        cmin[ch] = h_lab[s];
+        clev[ch] = h_lev[s];
+        start2ch.push_back({s, ch});
+      }
+    std::sort(start2ch.begin(), start2ch.end());
+    auto chain_starting_at = [&](int s) -> int {
+      auto it = std::lower_bound(start2ch.begin(), start2ch.end(), std::make_pair(s, -1));
+      return (it != start2ch.end() && it->first == s) ? it->second : -1;
+    };
+    // saddle box entered by each chain end
+    std::vector<int> box_of_end(nch);
+    for (int ch = 0; ch < nch; ch++) {
+      long long p = hsad[cend[ch]];
+      box_of_end[ch] = (int)(std::lower_bound(sad_p.begin(), sad_p.end(), p) - sad_p.begin());
+    }
+    std::vector<int> noc(nsb, 2);
+    std::vector<char> used(nch, 0);
+    ch_end = cend;
+    ch_len = clen;
+    ch_rot.assign(nch, -1);
+    ch_clen.assign(nch, 0);
+    ch_cont.assign(nch, -1);
+    ch_pos.assign(nch, 0);
+    // chains in order of their smallest crossing: contour starts
+    std::vector<int> order(nch);
+    for (int k = 0; k < nch; k++) order[k] = k;
+    std::sort(order.begin(), order.end(), [&](int a, int b) { return cmin[a] < cmin[b]; });
+    for (int oc : order) {
+      if (used[oc]) continue;
+      int icr = cmin[oc];            // the contour's first crossing
+      std::vector<int> seq;          // chains in traversal order
+      int ch = oc;
+      used[ch] = 1;
+      seq.push_back(ch);
+      int guard = 0;
+      while (true) {
+        int b = box_of_end[ch];
+        int k = noc[b];
+        if (k < 1 || k > 2) return CASL_EINVAL;
+        int icrn = slot2[2 * b + k - 1];
+        if (icrn == icr) break;      // closes at the start (no decrement)
+        noc[b] = k - 1;
+        int nxt = chain_starting_at(icrn);
+        if (nxt < 0) return CASL_EINVAL;
+        if (nxt == oc) break;        // back into the first chain, which holds icr
+        if (used[nxt]) return CASL_EINVAL;
+        used[nxt] = 1;
+        seq.push_back(nxt);
+        ch = nxt;
+        if (++guard > nch + 2) return CASL_EINVAL;
+      }
+      // lay out: first chain rotated to start at icr, then the others
+      int L = 0;
+      for (int q : seq) L += clen[q];
+      int cont = nsad_contours++;
+      sad_start.push_back(icr);
+      sad_len.push_back(L);
+      int first = seq[0];
+      int rot = clen[first] - h_val[icr];  // local index of icr in its chain
+      ch_rot[first] = rot;
+      ch_clen[first] = clen[first];
+      ch_cont[first] = cont;
+      ch_pos[first] = 0;
+      long long off = clen[first] - rot;   // crossings from icr to the chain end
+      for (size_t q = 1; q < seq.size(); q++) {
+        ch_cont[seq[q]] = cont;
+        ch_pos[seq[q]] = off;
+        off += clen[seq[q]];
+      }
+    }
+  }
+
+  // --- 7. contour order and walk layout ---------------------------------------
+  int *startf = ar2.get<int>(ncr), *clenr = ar2.get<int>(ncr), *cidx = ar2.get<int>(ncr);
+  if (!cidx) return CASL_ENOMEM;
+  k_ct_plain<<<g, 256, 0, st>>>(lab, term, val, ncr, startf, clenr);
+  for (int k = 0; k < nsad_contours; k++) {
+    int one = 1;
+    CASL_CUDA_TRY(cudaMemcpyAsync(startf + sad_start[k], &one, sizeof(int), cudaMemcpyHostToDevice, st));
+    CASL_CUDA_TRY(cudaMemcpyAsync(clenr + sad_start[k], &sad_len[k], sizeof(int), cudaMemcpyHostToDevice, st));
+  }
+  exclusive_scan<int>(st, startf, cidx, ncr, tmpi2, dtot + 1);
+  int C = 0;
+  CASL_CUDA_TRY(cudaMemcpyAsync(&C, dtot + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CASL_CUDA_TRY(cudaStreamSynchronize(st));
+  if (C == 0) return set_empty();
+  int *clen = ar2.get<int>(C), *coff = ar2.get<int>(C), *clevt = ar2.get<int>(C);
+  double *xw = ar2.get<double>(ncr), *yw = ar2.get<double>(ncr);
+  if (!yw) return CASL_ENOMEM;
+  {
+    // contour lengths and offsets in contour order (host: one pass over ncr)
+    std::vector<int> h_start(ncr), h_clenr(ncr), h_cidx(ncr);
+    CASL_CUDA_TRY(cudaMemcpyAsync(h_start.data(), startf, ncr * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CASL_CUDA_TRY(cudaMemcpyAsync(h_clenr.data(), clenr, ncr * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CASL_CUDA_TRY(cudaMemcpyAsync(h_cidx.data(), cidx, ncr * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CASL_CUDA_TRY(cudaStreamSynchronize(st));
+    std::vector<int> hl(C), ho(C);
+    for (long long r = 0; r < ncr; r++)
+      if (h_start[r]) hl[h_cidx[r]] = h_clenr[r];
+    long long acc = 0;
+    for (int k = 0; k < C; k++) {
+      ho[k] = (int)acc;
+      acc += hl[k];
+    }
+    if (acc != ncr) return CASL_EINVAL;
+    CASL_CUDA_TRY(cudaMemcpyAsync(clen, hl.data(), C * sizeof(int), cudaMemcpyHostToDevice, st));
+    CASL_CUDA_TRY(cudaMemcpyAsync(coff, ho.data(), C * sizeof(int), cudaMemcpyHostToDevice, st));
+    k_ct_gather_plain<<<g, 256, 0, st>>>(lab, term, val, cidx, coff, clen, xcr, ycr, ncr, xw, yw);
+    int nch = (int)ch_end.size();
+    if (nch > 0) {
+      // absolute position of every chain; the first chain of a contour is
+      // rotated to begin at the contour's first crossing, its head wrapping
+      // to the end of the contour
+      std::vector<long long> abs_pos(nch);
+      std::vector<int> rotlen(nch, 0);
+      std::vector<int> hcoe(ncr, -1);
+      for (int ch = 0; ch < nch; ch++) {
+        int cont = ch_cont[ch];
+        if (cont < 0) return CASL_EINVAL;
+        abs_pos[ch] = ho[h_cidx[sad_start[cont]]] + ch_pos[ch];
+        if (ch_rot[ch] >= 0) rotlen[ch] = sad_len[cont];
+        hcoe[ch_end[ch]] = ch;
+      }
+      long long *d_pos = ar2.get<long long>(nch);
+      int *d_len = ar2.get<int>(nch), *d_rot = ar2.get<int>(nch), *d_cl = ar2.get<int>(nch);
+      int *chain_of_end = ar2.get<int>(ncr);
+      if (!chain_of_end) return CASL_ENOMEM;
+      CASL_CUDA_TRY(cudaMemcpyAsync(d_pos, abs_pos.data(), nch * sizeof(long long), cudaMemcpyHostToDevice, st));
+      CASL_CUDA_TRY(cudaMemcpyAsync(d_len, ch_len.data(), nch * sizeof(int), cudaMemcpyHostToDevice, st));
+      CASL_CUDA_TRY(cudaMemcpyAsync(d_rot, ch_rot.data(), nch * sizeof(int), cudaMemcpyHostToDevice, st));
+      CASL_CUDA_TRY(cudaMemcpyAsync(d_cl, rotlen.data(), nch * sizeof(int), cudaMemcpyHostToDevice, st));
+      CASL_CUDA_TRY(cudaMemcpyAsync(chain_of_end, hcoe.data(), ncr * sizeof(int), cudaMemcpyHostToDevice, st));
+      k_ct_gather_chain<<<g, 256, 0, st>>>(term, ep, val, chain_of_end, d_pos, d_len, d_rot, d_cl,
+                                           xcr, ycr, ncr, xw, yw);
+      CASL_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+  }
+  k_lev_of_contour<<<g, 256, 0, st>>>(startf, rlev, cidx, ncr, li, h->p.nlevm, clevt);
+  RC_TRY(check_launch(h));
+
+  // --- 8. renode three times (congen.f90:295-310) -----------------------------
+  RenodeIn cur{xw, yw, coff, clen, clevt, C, ncr};
+  long long capn = std::max<long long>(ncr * 2, h->npm);
+  double *xa = ar2.get<double>(capn), *ya = ar2.get<double>(capn);
+  double *xb = ar2.get<double>(capn), *yb = ar2.get<double>(capn);
+  int *ocs[2], *olen[2], *olev[2];
+  for (int q = 0; q < 2; q++) {
+    ocs[q] = ar2.get<int>(C); olen[q] = ar2.get<int>(C); olev[q] = ar2.get<int>(C);
+  }
+  int *cnt = ar2.get<int>(4);
+  if (!cnt) return CASL_ENOMEM;
+  double *ox[3] = {xa, xb, xa}, *oy[3] = {ya, yb, ya};
+  int hc[3] = {0, 0, 0};
+  for (int pass = 0; pass < 3; pass++) {
+    RenodeOut out{};
+    out.xo = ox[pass]; out.yo = oy[pass];
+    out.ocs = ocs[pass & 1]; out.olen = olen[pass & 1]; out.olev = olev[pass & 1];
+    out.cap = capn;
+    out.d_counts = cnt;
+    size_t mark = ar2.off;
+    RC_TRY(renode_batch(h, ar2, cur, out, RENODE_PLAIN));
+    ar2.off = mark;
+    CASL_CUDA_TRY(cudaMemcpyAsync(hc, cnt, 3 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CASL_CUDA_TRY(cudaStreamSynchronize(st));
+    if (hc[2]) return CASL_ECAPACITY;
+    if (hc[0] == 0) return set_empty();
+    cur = RenodeIn{out.xo, out.yo, out.ocs, out.olen, out.olev, hc[0], hc[1]};
+  }
+  int nq = hc[0], npt = hc[1];
+  if (npt > h->npm || nq > h->nm) return CASL_ECAPACITY;
+  CASL_CUDA_TRY(cudaMemcpyAsync(h->xq, cur.xw, (size_t)npt * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  CASL_CUDA_TRY(cudaMemcpyAsync(h->yq, cur.yw, (size_t)npt * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  k_out_contours<<<gsz(nq), 256, 0, st>>>(cur.cs, cur.len, cur.levt, nq, h->i1q, h->i2q, h->npq,
+                                          h->indq);
+  k_out_links<<<gsz(npt), 256, 0, st>>>(cur.cs, cur.len, nq, npt, h->nextq);
+  k_set_counts2<<<1, 1, 0, st>>>(h->scal, cnt);
+  RC_TRY(check_launch(h));
+  h->nq = nq;
+  h->nptq = npt;
+  h->contex = npt > 0;
+  return CASL_OK;
+}
+
 }  // namespace casl

@@ -1,0 +1,322 @@
+// Parallel renode of many contours (contours.f90:687-933); see renode.cuh.
+#include <math.h>
+
+#include "renode.cuh"
+
+namespace casl {
+
+__device__ __forceinline__ long long wnext(long long w, long long cs, long long L) {
+  return w + 1 < cs + L ? w + 1 : cs;
+}
+__device__ __forceinline__ long long wprev(long long w, long long cs, long long L) {
+  return w > cs ? w - 1 : cs + L - 1;
+}
+
+__global__ void k_rn_cid(const int *__restrict__ cs, int C, long long N, int *__restrict__ cid,
+                         int *__restrict__ head) {
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < N;
+       w += (long long)gridDim.x * blockDim.x) {
+    int c = contour_of(cs, C, w);
+    cid[w] = c;
+    head[w] = (w == cs[c]);
+  }
+}
+
+// dx, dy to the next node; v = |d|^2, e = |d|  (contours.f90:718-730)
+__global__ void k_rn1(RenodeIn in, RenodeScratch s, Consts c) {
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < in.N;
+       w += (long long)gridDim.x * blockDim.x) {
+    int k = s.cid[w];
+    long long cs = in.cs[k], L = in.len[k];
+    long long a = wnext(w, cs, L);
+    double xx = in.xw[a] - in.xw[w];
+    double dx = xx - c.ellx * f_dint(xx * c.hlxi);
+    double yy = in.yw[a] - in.yw[w];
+    double dy = yy - c.elly * f_dint(yy * c.hlyi);
+    s.dx[w] = dx;
+    s.dy[w] = dy;
+    double v = dx * dx + dy * dy;
+    s.v[w] = v;
+    s.e[w] = sqrt(v);
+  }
+}
+
+// corners and curvature b (contours.f90:732-752)
+__global__ void k_rn2(RenodeIn in, RenodeScratch s, Consts c) {
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < in.N;
+       w += (long long)gridDim.x * blockDim.x) {
+    int k = s.cid[w];
+    long long cs = in.cs[k], L = in.len[k];
+    long long p = wprev(w, cs, L);
+    double u = s.v[p], a = -s.dx[p], cc = -s.dy[p];
+    double dx = s.dx[w], dy = s.dy[w], v = s.v[w];
+    int corner = dx * a + dy * cc > 0.0;
+    s.corner[w] = corner;
+    if (corner) {
+      s.b[w] = 0.0;
+      atomicAdd(&s.ccnt[k], 1);
+    } else {
+      double t1 = a * v - dx * u, t2 = cc * v - dy * u;
+      s.b[w] = (dx * cc - a * dy) / sqrt(t1 * t1 + t2 * t2 + c.small3);
+    }
+  }
+}
+
+// cubic coefficients and the spherical-curvature densities (contours.f90:754-774)
+__global__ void k_rn3(RenodeIn in, RenodeScratch s, Consts c) {
+  const double f12 = 0.5, f13 = 1.0 / 3.0, f16 = 1.0 / 6.0;
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < in.N;
+       w += (long long)gridDim.x * blockDim.x) {
+    int k = s.cid[w];
+    long long cs = in.cs[k], L = in.len[k];
+    long long a = wnext(w, cs, L);
+    double e = s.e[w], bi = s.b[w], ba = s.b[a];
+    double u = e * (ba + bi);
+    double cc = e * (ba - bi);
+    s.A[w] = f16 * cc - f12 * u;
+    s.B[w] = f12 * (u - cc);
+    s.Cc[w] = f13 * cc;
+    double v = s.v[w];
+    double ww = 1.0 / (v + c.dmsq);
+    s.u2[w] = ww * sqrt(c.elf * v + u * u);
+    s.v2[w] = ww * e;
+  }
+}
+
+// node curvature as a weighted average (contours.f90:780-783)
+__global__ void k_rn4(RenodeIn in, RenodeScratch s, Consts c) {
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < in.N;
+       w += (long long)gridDim.x * blockDim.x) {
+    int k = s.cid[w];
+    long long cs = in.cs[k], L = in.len[k];
+    long long p = wprev(w, cs, L);
+    s.d[w] = (s.u2[p] + s.u2[w]) / (s.v2[p] + s.v2[w] + c.small);
+  }
+}
+
+// fractional node count per interval (contours.f90:787-796)
+__global__ void k_rn5(RenodeIn in, RenodeScratch s, Consts c) {
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < in.N;
+       w += (long long)gridDim.x * blockDim.x) {
+    int k = s.cid[w];
+    long long cs = in.cs[k], L = in.len[k];
+    long long a = wnext(w, cs, L);
+    double u = 0.5 * (s.d[w] + s.d[a]);
+    double t = c.densf * sqrt(u) + u;
+    s.e[w] = s.e[w] * fmin(c.dmi, t);
+  }
+}
+
+__global__ void k_rn_cornerpos(const int *__restrict__ corner, const int *__restrict__ crank,
+                               int *__restrict__ pos, long long N) {
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < N;
+       w += (long long)gridDim.x * blockDim.x)
+    if (corner[w]) pos[crank[w]] = (int)w;
+}
+
+// Sum of e over `m` nodes of contour [cs, cs+L) starting at walk index st.
+__device__ __forceinline__ double sumrange(const double *__restrict__ S, long long cs,
+                                           long long L, long long st, long long m) {
+  long long a = st - cs, b = a + m;
+  auto pre = [&](long long k) -> double { return k == 0 ? 0.0 : S[cs + k - 1]; };
+  if (b <= L) return pre(b) - pre(a);
+  return (pre(L) - pre(a)) + pre(b - L);
+}
+
+__device__ __forceinline__ int nint_d(double x) { return (int)llround(x); }
+
+// Per contour: node count, pieces (contours.f90:799-809, 813-930).
+__global__ void k_rn_count(RenodeIn in, RenodeScratch s, Consts c, int mode) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < in.C; k += gridDim.x * blockDim.x) {
+    long long cs = in.cs[k], L = in.len[k];
+    double total = s.S[cs + L - 1];
+    s.ctot[k] = total;
+    int np = 0;
+    if (!(mode == RENODE_SURGERY && L <= 3)) {
+      int npr0 = nint_d(total) + 1;
+      if (npr0 >= 3) np = s.ccnt[k] > 1 ? s.ccnt[k] : 1;
+    }
+    s.npiece[k] = np;
+  }
+}
+
+__global__ void k_rn_fill(RenodeIn in, RenodeScratch s, Consts c, int mode) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < in.C; k += gridDim.x * blockDim.x) {
+    long long cs = in.cs[k], L = in.len[k];
+    int np = s.npiece[k];
+    int npr = 0;
+    double total = s.ctot[k];
+    int nc = s.ccnt[k];
+    int cfirst = s.crank[cs];
+    for (int q = 0; q < np; q++) {
+      int p = s.poff[k] + q;
+      long long st, pl;
+      double sum;
+      int n;
+      if (nc <= 1) {
+        st = nc == 0 ? cs : s.cornerpos[cfirst];
+        pl = L;
+        sum = total;
+        n = nint_d(total) + 1;
+      } else {
+        st = s.cornerpos[cfirst + q];
+        long long en = s.cornerpos[cfirst + (q + 1) % nc];
+        pl = (en - st + L) % L;
+        sum = sumrange(s.S, cs, L, st, pl);
+        n = sum > c.small ? nint_d(sum) + 1 : 0;
+      }
+      s.pc[p] = k;
+      s.pstart[p] = (int)st;
+      s.plen[p] = (int)pl;
+      s.psum[p] = sum;
+      s.pn[p] = n;
+      s.pfac[p] = n > 0 ? (double)n / sum : 0.0;
+      npr += n;
+    }
+    int keep = mode == RENODE_SURGERY ? npr > 3 : npr > 0;
+    s.ckeep[k] = keep;
+    s.cnpr[k] = keep ? npr : 0;
+  }
+}
+
+__global__ void k_rn_pout(RenodeIn in, RenodeScratch s, RenodeOut out) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < in.C; k += gridDim.x * blockDim.x) {
+    if (!s.ckeep[k]) continue;
+    int base = s.cout[k];
+    for (int q = 0; q < s.npiece[k]; q++) {
+      int p = s.poff[k] + q;
+      s.pout[p] = base;
+      base += s.pn[p];
+    }
+    int j = s.ckidx[k];
+    out.ocs[j] = s.cout[k];
+    out.olen[j] = s.cnpr[k];
+    out.olev[j] = in.levt ? in.levt[k] : 0;
+  }
+}
+
+__global__ void k_rn_place(RenodeIn in, RenodeScratch s, RenodeOut out, Consts c) {
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < in.N;
+       w += (long long)gridDim.x * blockDim.x) {
+    int k = s.cid[w];
+    if (!s.ckeep[k]) continue;
+    long long cs = in.cs[k], L = in.len[k];
+    int nc = s.ccnt[k];
+    int q = 0;
+    if (nc >= 2) {
+      int inc = s.crank[w] - s.crank[cs] + s.corner[w];
+      q = inc - 1;
+      if (q < 0) q = nc - 1;
+    }
+    int p = s.poff[k] + q;
+    int n = s.pn[p];
+    if (n == 0) continue;
+    long long st = s.pstart[p];
+    long long rel = (w - st + L) % L;
+    if (rel >= s.plen[p]) continue;
+    long long o = s.pout[p];
+    if (rel == 0) {
+      out.xo[o] = in.xw[w];
+      out.yo[o] = in.yw[w];
+    }
+    double fac = s.pfac[p];
+    double Ep = fac * sumrange(s.S, cs, L, st, rel);
+    double Ec = fac * sumrange(s.S, cs, L, st, rel + 1);
+    long long t0 = (long long)floor(Ep) + 1;
+    long long t1 = (long long)floor(Ec);
+    if (t1 > n - 1) t1 = n - 1;
+    if (t0 < 1) t0 = 1;
+    if (t1 < t0) continue;
+    double ew = fac * s.e[w];
+    double xd = in.xw[w], yd = in.yw[w], dx = s.dx[w], dy = s.dy[w];
+    double A = s.A[w], B = s.B[w], Cc = s.Cc[w];
+    for (long long t = t0; t <= t1; t++) {
+      double acc = Ec - (double)t;
+      double pp = 1.0 - acc / ew;
+      double eta = pp * (A + pp * (B + pp * Cc));
+      double xx = xd + pp * dx - eta * dy;
+      double yy = yd + pp * dy + eta * dx;
+      out.xo[o + t] = wrapp(xx, c.ellx, c.hlxi, c.oms);
+      out.yo[o + t] = wrapp(yy, c.elly, c.hlyi, c.oms);
+    }
+  }
+}
+
+__global__ void k_rn_finish(int *counts_dev, const int *ntot, const int *ctot, long long cap) {
+  counts_dev[0] = *ctot;
+  counts_dev[1] = *ntot;
+  counts_dev[2] = (long long)*ntot > cap;
+}
+
+static inline int gsz(long long work) {
+  long long g = (work + 255) / 256;
+  if (g < 1) g = 1;
+  if (g > 148 * 16) g = 148 * 16;
+  return (int)g;
+}
+
+int renode_batch(casl_handle *h, Arena &ar, const RenodeIn &in, RenodeOut &out, int mode) {
+  cudaStream_t st = h->stream;
+  const Consts &c = h->c;
+  long long N = in.N;
+  int C = in.C;
+  if (C == 0 || N == 0) {
+    cudaMemsetAsync(out.d_counts, 0, 3 * sizeof(int), st);
+    return CASL_OK;
+  }
+  RenodeScratch s{};
+  s.cid = ar.get<int>(N);
+  s.dx = ar.get<double>(N); s.dy = ar.get<double>(N); s.v = ar.get<double>(N);
+  s.e = ar.get<double>(N); s.b = ar.get<double>(N); s.A = ar.get<double>(N);
+  s.B = ar.get<double>(N); s.Cc = ar.get<double>(N); s.u2 = ar.get<double>(N);
+  s.v2 = ar.get<double>(N); s.d = ar.get<double>(N); s.S = ar.get<double>(N);
+  s.corner = ar.get<int>(N); s.crank = ar.get<int>(N); s.head = ar.get<int>(N);
+  s.cornerpos = ar.get<int>(N + 1);
+  s.ccnt = ar.get<int>(C); s.ctot = ar.get<double>(C);
+  s.npiece = ar.get<int>(C); s.poff = ar.get<int>(C);
+  s.cnpr = ar.get<int>(C); s.cout = ar.get<int>(C); s.ckeep = ar.get<int>(C);
+  s.ckidx = ar.get<int>(C);
+  long long tmpn = scan_tmp_elems(N > C ? N : C) + 4;
+  s.tmpi = ar.get<int>(tmpn);
+  s.tmps = ar.get<SegPair>(tmpn);
+  s.d_tot = ar.get<int>(8);
+  if (!s.d_tot) return CASL_ENOMEM;
+  cudaMemsetAsync(s.ccnt, 0, C * sizeof(int), st);
+  int g = gsz(N);
+  k_rn_cid<<<g, 256, 0, st>>>(in.cs, C, N, s.cid, s.head);
+  k_rn1<<<g, 256, 0, st>>>(in, s, c);
+  k_rn2<<<g, 256, 0, st>>>(in, s, c);
+  k_rn3<<<g, 256, 0, st>>>(in, s, c);
+  k_rn4<<<g, 256, 0, st>>>(in, s, c);
+  k_rn5<<<g, 256, 0, st>>>(in, s, c);
+  segmented_scan(st, s.e, s.head, s.S, N, s.tmps);
+  exclusive_scan<int>(st, s.corner, s.crank, N, s.tmpi, s.d_tot + 0);
+  k_rn_cornerpos<<<g, 256, 0, st>>>(s.corner, s.crank, s.cornerpos, N);
+  int gc = gsz(C);
+  k_rn_count<<<gc, 256, 0, st>>>(in, s, c, mode);
+  exclusive_scan<int>(st, s.npiece, s.poff, C, s.tmpi, s.d_tot + 1);
+  // pieces: at most one per corner, or one per contour
+  int hp = 0;
+  cudaMemcpyAsync(&hp, s.d_tot + 1, sizeof(int), cudaMemcpyDeviceToHost, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return set_cuda_error(h, e);
+  long long P = hp > 0 ? hp : 1;
+  s.pc = ar.get<int>(P); s.pstart = ar.get<int>(P); s.plen = ar.get<int>(P);
+  s.pn = ar.get<int>(P); s.pout = ar.get<int>(P);
+  s.psum = ar.get<double>(P); s.pfac = ar.get<double>(P);
+  if (!s.pfac) return CASL_ENOMEM;
+  k_rn_fill<<<gc, 256, 0, st>>>(in, s, c, mode);
+  exclusive_scan<int>(st, s.cnpr, s.cout, C, s.tmpi, s.d_tot + 2);
+  exclusive_scan<int>(st, s.ckeep, s.ckidx, C, s.tmpi, s.d_tot + 3);
+  k_rn_finish<<<1, 1, 0, st>>>(out.d_counts, s.d_tot + 2, s.d_tot + 3, out.cap);
+  int hc[3];
+  cudaMemcpyAsync(hc, out.d_counts, 3 * sizeof(int), cudaMemcpyDeviceToHost, st);
+  e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return set_cuda_error(h, e);
+  if (hc[2]) return CASL_ECAPACITY;
+  k_rn_pout<<<gc, 256, 0, st>>>(in, s, out);
+  k_rn_place<<<g, 256, 0, st>>>(in, s, out, c);
+  return check_launch(h);
+}
+
+}  // namespace casl

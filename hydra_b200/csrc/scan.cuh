@@ -153,7 +153,7 @@ __device__ __forceinline__ SegPair warp_seg_incl(SegPair x) {
   return x;
 }
 // Exclusive (prefix before this thread) segmented scan across the block.
-__device__ SegPair block_seg_excl(SegPair x, SegPair *total) {
+static __device__ SegPair block_seg_excl(SegPair x, SegPair *total) {
   __shared__ double wv[32];
   __shared__ int wf[32];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -182,7 +182,7 @@ __device__ SegPair block_seg_excl(SegPair x, SegPair *total) {
   return r;
 }
 
-__global__ void __launch_bounds__(SCAN_BLOCK) k_segscan_tiles(const double *__restrict__ in,
+static __global__ void __launch_bounds__(SCAN_BLOCK) k_segscan_tiles(const double *__restrict__ in,
                                                               const int *__restrict__ head,
                                                               double *__restrict__ out,
                                                               SegPair *__restrict__ tile_tot,
@@ -209,7 +209,7 @@ __global__ void __launch_bounds__(SCAN_BLOCK) k_segscan_tiles(const double *__re
 }
 
 // Exclusive segmented scan of tile totals (one block): carry into each tile.
-__global__ void __launch_bounds__(SCAN_BLOCK) k_segscan_totals(SegPair *__restrict__ tot,
+static __global__ void __launch_bounds__(SCAN_BLOCK) k_segscan_totals(SegPair *__restrict__ tot,
                                                                int ntiles) {
   __shared__ SegPair t;
   __shared__ SegPair carry;
@@ -228,7 +228,7 @@ __global__ void __launch_bounds__(SCAN_BLOCK) k_segscan_totals(SegPair *__restri
 }
 
 // Add each tile's incoming carry to its elements before the tile's first head.
-__global__ void k_segscan_add(double *__restrict__ out, const int *__restrict__ head,
+static __global__ void k_segscan_add(double *__restrict__ out, const int *__restrict__ head,
                               const SegPair *__restrict__ tot, long long n) {
   long long tile = blockIdx.x;
   long long beg = tile * SCAN_TILE, end = beg + SCAN_TILE < n ? beg + SCAN_TILE : n;

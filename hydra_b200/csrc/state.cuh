@@ -49,6 +49,8 @@ struct casl_handle {
   // surgery / renode / recontour scratch (allocated on first use)
   void *sx;
   size_t sx_bytes;
+  void *sx2;             // second arena (recontouring's per-crossing data)
+  size_t sx2_bytes;
 };
 
 namespace casl {
@@ -73,5 +75,6 @@ int renode_host(casl_handle *h, const double *xd, const double *yd, int npd, dou
 
 int sync_counts(casl_handle *h);    // device counts -> host copies
 int ensure_scratch(casl_handle *h, size_t bytes);
+int ensure_scratch2(casl_handle *h, size_t bytes);
 
 }  // namespace casl
