@@ -1,0 +1,393 @@
+#!/usr/bin/env python
+"""Benchmark of the contour-advection time step (Hydra ca/plane/qg/caps) on B200.
+
+Metric: node-steps/s -- the sum over steps of the contour nodes advanced,
+divided by the device time of those steps.  A step is one pass of the
+reference's advect loop body (evolution.f90:55-79): a regularisation (surgery
++ renode every step; prepare + recontour + init every 20th) followed by one
+RK4 advance (4 inversions, 37 real 2-D FFTs, 4 con2grid, 4 velint).
+
+Workload (the plain-CASL-at-scale configuration): doubly periodic
+[-pi, pi)^2, 1024^2 inversion grid, random-phase PV with amplitude
+k^3 exp(-(k/16)^2) normalised to rms 4 pi, 80 contour levels (about two
+million FP64 nodes), surgery every step, recontouring every 20
+regularisations, the reference's adaptive dt (dtmax 0.05).  Seeded synthetic
+input; working set well above the 126 MB L2 (no flush needed).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+For N > 1 (torchrun), every rank advances an independent ensemble member
+(seed + rank): replicas, weak scaling, no collective on the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "node-steps/s on 1 B200, chosen vs plain form at <=1e-3 rel node-velocity err"
+UNIT = "node-steps/s"
+
+
+def workload_args(a):
+    return dict(n=a.n, k0=a.k0, levels=a.levels, dtmax=a.dtmax)
+
+
+def config_dict(a, nodes):
+    return {
+        "workload": f"plain CASL 2D Euler, {a.n}^2 grid, k0={a.k0:g}, {a.levels} levels, "
+                    "surgery every step, recontour every 20 regularisations, adaptive dt",
+        "n": a.n, "levels": a.levels, "k0": a.k0, "seed": a.seed, "dtmax": a.dtmax,
+        "nodes_mean": nodes, "precision": "FP64 nodes and FP64 inversion",
+        "l2": "working set > 126 MB L2 (fields + 4x fine grid + nodes); no flush",
+        "parallelism": "replicas" if a.gpus > 1 else "single",
+    }
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per launch of the profiled transform pass, from the committed
+    ncu summary (profiles/rfft_pass_1024.md, line 'traffic_bytes_per_launch: X')."""
+    p = os.path.join(ROOT, "profiles", "rfft_pass_1024.md")
+    try:
+        for ln in open(p):
+            if ln.startswith("traffic_bytes_per_launch:"):
+                return float(ln.split(":")[1])
+    except Exception:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------------------
+# CPU legs (the oracle; test infrastructure, never the measured product)
+# ---------------------------------------------------------------------------
+def cpu_oracle_steps(state, a, budget_s, max_steps):
+    """Time oracle steps on the given state (contours + fields); 1 core."""
+    from oracle.oracle import Oracle
+    c = state["contours"]
+    o = Oracle(a.n, ncontq=a.levels, force_surgery=1, dtmax=a.dtmax,
+               npm=max(4 * c["nptq"], 1 << 20), nm=max(4 * c["nq"], 1 << 16))
+    o.set_contours(c)
+    for f in ("qs", "qd", "qr"):
+        o.set_field(f, state[f])
+    o.set_scalar("t", state["t"])
+    o.set_scalar("twist", 0.0)
+    o.set_scalar("ireg", 0)
+    node_steps, steps = 0, 0
+    t0 = time.perf_counter()
+    while steps < max_steps:
+        node_steps += o.counts()[1]
+        o.step()
+        steps += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    o.close()
+    return node_steps / dt, steps, dt
+
+
+def run_reference(a):
+    """--impl reference: the reference's CPU path (the oracle port; the Fortran
+    reference cannot be compiled on these machines), serial as the reference
+    is, on the same workload."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle.oracle import Oracle
+    from hydra_b200.synthetic import random_pv
+    q0 = random_pv(a.n, a.k0, a.seed)
+    o = Oracle(a.n, ncontq=a.levels, force_surgery=1, dtmax=a.dtmax,
+               npm=16_000_000, nm=1_000_000)
+    t_init = time.perf_counter()
+    o.initialise(q0)
+    t_init = time.perf_counter() - t_init
+    for _ in range(min(a.warmup, 1)):
+        o.step()
+    budget = a.cpu_seconds
+    node_steps, steps = 0, 0
+    t0 = time.perf_counter()
+    while steps < a.steps:
+        node_steps += o.counts()[1]
+        o.step()
+        steps += 1
+        if time.perf_counter() - t0 > budget:
+            break
+    dt = time.perf_counter() - t0
+    v = node_steps / dt
+    nodes = node_steps / max(steps, 1)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus,
+        "steps": steps, "warmup": min(a.warmup, 1), "ms_per_step": 1000.0 * dt / max(steps, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": config_dict(a, nodes),
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
+                         "sample": f"{steps} steps of the workload after a 1-step warm-up "
+                                   f"(initialise {t_init:.0f} s untimed); the reference path is "
+                                   "serial Fortran, restated in C (no Fortran compiler here)"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def run_gpu(a):
+    import torch
+    import torch.distributed as dist
+
+    from hydra_b200.casl import CaslGPU, load_library
+    from hydra_b200.synthetic import random_pv
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    load_library()
+
+    q0 = random_pv(a.n, a.k0, a.seed + rank)
+    g = CaslGPU(a.n, ncontq=a.levels, force_surgery=1, dtmax=a.dtmax,
+                npm=16_000_000, nm=1_000_000, device=local)
+    g.initialise(q0)
+    for _ in range(a.warmup):
+        g.step(1)
+    stream = torch.cuda.ExternalStream(g.stream_ptr(), device=local)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- resident-data timed region ------------------------------------------------
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    ns0 = g.scalar("node_steps")
+    l0 = g.launch_count()
+    g.profile(1)  # the transform passes
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(a.steps):
+        g.step(1)
+    ev1.record(stream)
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    launches = g.launch_count() - l0
+    fft_ms, fft_n, fft_bytes = g.profile_read()
+    g.profile(0)
+    node_steps = g.scalar("node_steps") - ns0
+    clk = clocks.stop()
+
+    # ---- end to end through the C-ABI with host buffers -----------------------------
+    e2e = run_e2e(g, a, stream, torch)
+
+    # CPU baseline on this host (rank 0, N = 1 only): the oracle on the same state
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu:
+        state = {"contours": g.contours(), "qs": g.field("qs"), "qd": g.field("qd"),
+                 "qr": g.field("qr"), "t": g.scalar("t")}
+        v, steps, dt = cpu_oracle_steps(state, a, a.cpu_seconds, 8)
+        cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"{steps} oracle steps ({dt:.1f} s) from the GPU run's state after "
+                         "its timed steps (surgery + advance; no recontouring in the sample)"}
+
+    # ---- reduce over ranks ---------------------------------------------------------------
+    t = torch.tensor([ms, node_steps, e2e["ms"], e2e["node_steps"]], dtype=torch.float64,
+                     device=f"cuda:{local}")
+    if world > 1:
+        mx = t.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        sm = t.clone()
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        ms_max, ns_sum = mx[0].item(), sm[1].item()
+        e2e_ms, e2e_ns = mx[2].item(), sm[3].item()
+    else:
+        ms_max, ns_sum, e2e_ms, e2e_ns = ms, node_steps, e2e["ms"], e2e["node_steps"]
+    if rank == 0:
+        peak, peak_kind = measured_peak()
+        ach = fft_bytes / (fft_ms * 1e-3) / 1e9 if fft_ms > 0 else 0.0
+        traffic = profiled_traffic()
+        line = {
+            "metric": METRIC,
+            "value": ns_sum / (ms_max * 1e-3),
+            "unit": UNIT,
+            "n_gpus": world,
+            "steps": a.steps,
+            "warmup": a.warmup,
+            "ms_per_step": ms_max / a.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64",
+            "data": "synthetic",
+            "config": config_dict(a, node_steps / a.steps),
+            "e2e": {"value": e2e_ns / (e2e_ms * 1e-3), "unit": UNIT,
+                    "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"],
+                    "steps": e2e["steps"]},
+            "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                         "frac": ach / peak if peak else None, "traffic": traffic,
+                         "kernel": "k_rfft (batched real-FFT pass, all variants)",
+                         "launches": fft_n, "kernel_ms_per_step": fft_ms / a.steps,
+                         "peak_source": f"{peak_kind} hbm_gbs"},
+            "cpu_baseline": cpu,
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    g.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def run_e2e(g, a, stream, torch):
+    """node-steps/s through the public C-ABI with the state in pinned host
+    memory: every step uploads contours + spectral fields, steps, downloads."""
+    import ctypes as C
+    lib = g.lib
+    n = a.n
+    cap_n, cap_c = 16_000_000, 1_000_000
+
+    def pinned(shape, dtype):
+        t = torch.empty(shape, dtype=dtype, pin_memory=True)
+        return t.numpy()
+
+    xq = pinned(cap_n, torch.float64); yq = pinned(cap_n, torch.float64)
+    nextq = pinned(cap_n, torch.int32)
+    indq = pinned(cap_c, torch.int32); npq = pinned(cap_c, torch.int32)
+    i1q = pinned(cap_c, torch.int32); i2q = pinned(cap_c, torch.int32)
+    qs = pinned((n, n), torch.float64); qd = pinned((n, n), torch.float64)
+    dp, ip = C.POINTER(C.c_double), C.POINTER(C.c_int)
+    D = lambda x: x.ctypes.data_as(dp)
+    I = lambda x: x.ctypes.data_as(ip)
+
+    def download():
+        nq, npt, qj = g.counts()
+        g._check(lib.casl_get_contours(g.h, D(xq), D(yq), I(nextq), I(indq), I(npq), I(i1q), I(i2q)),
+                 "casl_get_contours")
+        g._check(lib.casl_get_field(g.h, 0, D(qs)), "casl_get_field")
+        g._check(lib.casl_get_field(g.h, 1, D(qd)), "casl_get_field")
+        return nq, npt, qj
+
+    nq, npt, qj = download()
+    steps = max(1, a.steps)   # same steps as the timed region (recontourings included)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ns0 = g.scalar("node_steps")
+    h2d = d2h = 0
+    ev0.record(stream)
+    for _ in range(steps):
+        g._check(lib.casl_set_contours(g.h, nq, npt, qj, D(xq), D(yq), I(nextq), I(indq), I(npq),
+                                       I(i1q), I(i2q)), "casl_set_contours")
+        g._check(lib.casl_set_field(g.h, 0, D(qs)), "casl_set_field")
+        g._check(lib.casl_set_field(g.h, 1, D(qd)), "casl_set_field")
+        h2d += npt * 20 + nq * 16 + 2 * n * n * 8
+        g.step(1)
+        nq, npt, qj = download()
+        d2h += npt * 20 + nq * 16 + 2 * n * n * 8
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    return {"ms": ev0.elapsed_time(ev1), "node_steps": g.scalar("node_steps") - ns0,
+            "h2d": h2d // steps, "d2h": d2h // steps, "steps": steps}
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["hydra", "reference"], default="hydra")
+    ap.add_argument("--n", type=int, default=1024)
+    ap.add_argument("--k0", type=float, default=16.0)
+    ap.add_argument("--levels", type=int, default=80)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--dtmax", type=float, default=0.05)
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    a = ap.parse_args()
+    if a.warmup < 3 and a.impl == "hydra":
+        print("bench: at least 3 warm-up steps are required", file=sys.stderr)
+        return 2
+    if a.impl == "reference":
+        return run_reference(a)
+    return run_gpu(a)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -27,7 +27,8 @@ CASL_OK, CASL_EINVAL, CASL_ECAPACITY, CASL_ECUDA, CASL_ENOMEM, CASL_EDOMAIN, CAS
 
 FIELDS = {"qs": 0, "qd": 1, "qc": 2, "qq": 3, "pp": 4, "qspre": 5, "emq": 6, "epq": 7,
           "uu": 8, "vv": 9, "qr": 10}
-SCALARS = {"t": 0, "dt": 1, "twist": 2, "ireg": 3, "zzrms": 4, "zzmax": 5, "uumax": 6, "qjump": 7}
+SCALARS = {"t": 0, "dt": 1, "twist": 2, "ireg": 3, "zzrms": 4, "zzmax": 5, "uumax": 6, "qjump": 7,
+           "node_steps": 8}
 
 
 class CaslError(RuntimeError):
@@ -79,6 +80,10 @@ SIGNATURES = {
     "casl_initialise": (C.c_int, [C.c_void_p, _dp]),
     "casl_step": (C.c_int, [C.c_void_p, C.c_int]),
     "casl_diagnostics": (C.c_int, [C.c_void_p, _dp]),
+    "casl_get_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "casl_launch_count": (C.c_int, [C.POINTER(C.c_longlong)]),
+    "casl_profile": (C.c_int, [C.c_void_p, C.c_int]),
+    "casl_profile_read": (C.c_int, [C.c_void_p, _dp, C.POINTER(C.c_longlong), _dp]),
 }
 
 
@@ -256,6 +261,26 @@ class CaslGPU:
 
     def synchronize(self):
         self._check(self.lib.casl_synchronize(self.h), "casl_synchronize")
+
+    # --- benchmarking hooks --------------------------------------------------------
+    def stream_ptr(self) -> int:
+        p = C.c_void_p()
+        self._check(self.lib.casl_get_stream(self.h, C.byref(p)), "casl_get_stream")
+        return p.value or 0
+
+    def launch_count(self) -> int:
+        v = C.c_longlong()
+        self._check(self.lib.casl_launch_count(C.byref(v)), "casl_launch_count")
+        return v.value
+
+    def profile(self, kernel_class: int):
+        self._check(self.lib.casl_profile(self.h, kernel_class), "casl_profile")
+
+    def profile_read(self):
+        ms, n, b = C.c_double(), C.c_longlong(), C.c_double()
+        self._check(self.lib.casl_profile_read(self.h, C.byref(ms), C.byref(n), C.byref(b)),
+                    "casl_profile_read")
+        return ms.value, n.value, b.value
 
     def diagnostics(self):
         out = np.zeros(4)

@@ -19,6 +19,8 @@ using namespace casl;
 
 namespace casl {
 
+unsigned long long g_launches = 0;
+
 int set_cuda_error(casl_handle *h, cudaError_t e) {
   if (h) h->last_cuda = (int)e;
   cudaGetLastError();  // clear sticky non-fatal error state
@@ -52,7 +54,15 @@ static int launch_rfft(casl_handle *h, LD ld, ST st, int batch) {
     configured = true;
   }
   dim3 grid(n / V, batch);
-  kern<<<grid, 256, sm, h->stream>>>(ld, st, h->tw, n, ilog2(n / 2));
+  const bool prof = h->prof_class == CASL_PROF_FFT && h->prof_ev && h->prof_n < CASL_PROF_MAX;
+  if (prof) cudaEventRecord(h->prof_ev[2 * h->prof_n], h->stream);
+  CASL_K(kern, grid, 256, sm, h->stream)(ld, st, h->tw, n, ilog2(n / 2));
+  if (prof) {
+    cudaEventRecord(h->prof_ev[2 * h->prof_n + 1], h->stream);
+    h->prof_n++;
+    // algorithmic bytes: every element of every vector read once and written once
+    h->prof_bytes += (double)batch * (double)n * (double)n * (ld.bytes() + st.bytes());
+  }
   return check_launch(h);
 }
 
@@ -90,6 +100,7 @@ int spctop_dev(casl_handle *h, const double *spec, double *phys, double *tmp) {
 // a spectral field, optionally of green*field (main_invert, spectral.f90:321).
 // Batch index b selects field and direction.
 struct LoadDeriv {
+  __host__ double bytes() const { return green ? 16.0 : 8.0; }
   const double *f[4];
   int dir[4];  // 0: d/dx, 1: d/dy
   const double *green;
@@ -117,6 +128,7 @@ struct LoadDeriv {
 // qa(iy,ix) of con2grid from the exact integer coarse cells:
 // qc = qjump*(C*n^2 - S)/(256 n^2) (+ beta field), phys layout [ix][iy].
 struct LoadQC {
+  __host__ double bytes() const { return 4.0; }
   const int *C;
   const Scalars *s;
   const double *betac;  // nullable
@@ -135,6 +147,7 @@ struct LoadQC {
 // Advection product -u*fx - v*(fy [+ beta]) of evolution.f90:449,456-461,
 // read from physical arrays ([ix][iy]); b = 0 for qd, 1 for qs.
 struct LoadAdvect {
+  __host__ double bytes() const { return 32.0; }
   const double *uu, *vv;
   const double *fx[2], *fy[2];
   double betab[2];  // beta added to fy for the qs term when beffect
@@ -150,6 +163,7 @@ struct LoadAdvect {
 // Store of the source terms after ptospc pass B (evolution.f90:466-487):
 // b = 0 -> sqd with damping and the integrating factor, b = 1 -> sqs.
 struct StoreSource {
+  __host__ double bytes() const { return 8.0 + 0.5 * 24.0; }  // sqd reads qq, pp, epq
   double *sqd, *sqs;
   const double *qq, *pp, *epq;
   double rekman, kdsq, therm;
@@ -178,6 +192,7 @@ struct StoreSource {
 };
 
 struct StoreScaled {
+  __host__ double bytes() const { return 8.0; }
   double *p[4];
   double scale[4];
   int n;
@@ -186,6 +201,7 @@ struct StoreScaled {
   }
 };
 struct LoadBatch {
+  __host__ double bytes() const { return 8.0; }
   const double *p[4];
   long long vs, es;
   __device__ __forceinline__ double operator()(int b, int v, int j) const {
@@ -194,6 +210,7 @@ struct LoadBatch {
 };
 // Load qq + kdsq*pp (adapt, evolution.f90:541-547).
 struct LoadVort {
+  __host__ double bytes() const { return btropic ? 8.0 : 16.0; }
   const double *qq, *pp;
   double kdsq;
   int btropic, n;
@@ -379,14 +396,14 @@ int con2grid_dev(casl_handle *h) {
   size_t fine = (size_t)c.nxf * c.nyf;
   CASL_CUDA_TRY(cudaMemsetAsync(h->fineJ, 0, fine * sizeof(int), h->stream));
   CASL_CUDA_TRY(cudaMemsetAsync(h->ljx, 0, (size_t)c.nxf * sizeof(int), h->stream));
-  k_zero_csum<<<1, 1, 0, h->stream>>>(h->scal);
+  CASL_K(k_zero_csum, 1, 1, 0, h->stream)(h->scal);
   int *err = &h->scal->error;
   if (h->nptq > 0)
-    k_c2g_scatter<<<grid_for(h->nptq), 256, 0, h->stream>>>(h->xq, h->yq, h->nextq, h->scal,
+    CASL_K(k_c2g_scatter, grid_for(h->nptq), 256, 0, h->stream)(h->xq, h->yq, h->nextq, h->scal,
                                                               h->fineJ, h->ljx, c, err);
-  k_c2g_lbot<<<1, 1024, 0, h->stream>>>(h->ljx, h->fineJ, c.nxf, c.nyf);
-  k_c2g_colscan<<<(c.nxf * 32 + 255) / 256, 256, 0, h->stream>>>(h->fineJ, c.nxf, c.nyf);
-  k_c2g_coarsen<<<grid_for((long long)h->n * h->n), 256, 0, h->stream>>>(
+  CASL_K(k_c2g_lbot, 1, 1024, 0, h->stream)(h->ljx, h->fineJ, c.nxf, c.nyf);
+  CASL_K(k_c2g_colscan, (c.nxf * 32 + 255) / 256, 256, 0, h->stream)(h->fineJ, c.nxf, c.nyf);
+  CASL_K(k_c2g_coarsen, grid_for((long long)h->n * h->n), 256, 0, h->stream)(
       h->fineJ, h->coarseC, (unsigned long long *)&h->scal->csum, h->n, c.nxf);
   return check_launch(h);
 }
@@ -415,7 +432,7 @@ int con2grid_to_phys(casl_handle *h, double *phys) {
   }
   int rc = con2grid_dev(h);
   if (rc) return rc;
-  k_c2g_final<<<grid_for(nn), 256, 0, h->stream>>>(h->coarseC, h->scal,
+  CASL_K(k_c2g_final, grid_for(nn), 256, 0, h->stream)(h->coarseC, h->scal,
                                                    h->c.beffect ? h->betac : nullptr, phys, h->n);
   return check_launch(h);
 }
@@ -666,10 +683,10 @@ static int inversion_dev(casl_handle *h, bool reset) {
   int rc = con2grid_to_spec(h, h->qc);
   if (rc) return rc;
   if (reset)
-    k_combine<true><<<grid_for(nn), 256, 0, h->stream>>>(h->qs, h->qd, h->qc, h->qq, h->pp,
+    CASL_K(k_combine<true>, grid_for(nn), 256, 0, h->stream)(h->qs, h->qd, h->qc, h->qq, h->pp,
                                                           h->flo, h->fhi, h->green, nn);
   else
-    k_combine<false><<<grid_for(nn), 256, 0, h->stream>>>(h->qs, h->qd, h->qc, h->qq, h->pp,
+    CASL_K(k_combine<false>, grid_for(nn), 256, 0, h->stream)(h->qs, h->qd, h->qc, h->qq, h->pp,
                                                            h->flo, h->fhi, h->green, nn);
   rc = check_launch(h);
   if (rc) return rc;
@@ -698,9 +715,9 @@ static int adapt_dev(casl_handle *h) {
   rc = RFFT_DISPATCH(false, false, true, (LoadStrided{h->w[0], nn, n, 1}),
                      (StoreStrided{h->w[1], nn, 1, n}), 1);
   if (rc) return rc;
-  k_reduce_adapt<<<RED_BLOCKS, 256, 0, h->stream>>>(h->w[1], h->uu, h->vv, h->part, nn);
-  k_adapt_final<<<1, 256, 0, h->stream>>>(h->part, RED_BLOCKS, h->scal, h->c, h->p.fixed_dt);
-  k_epq<<<grid_for(nn), 256, 0, h->stream>>>(h->qdiss, h->epq, h->emq, h->scal, nn);
+  CASL_K(k_reduce_adapt, RED_BLOCKS, 256, 0, h->stream)(h->w[1], h->uu, h->vv, h->part, nn);
+  CASL_K(k_adapt_final, 1, 256, 0, h->stream)(h->part, RED_BLOCKS, h->scal, h->c, h->p.fixed_dt);
+  CASL_K(k_epq, grid_for(nn), 256, 0, h->stream)(h->qdiss, h->epq, h->emq, h->scal, nn);
   return check_launch(h);
 }
 
@@ -756,38 +773,38 @@ static int advance_dev(casl_handle *h) {
   if ((rc = adapt_dev(h))) return rc;
   if ((rc = source_dev(h, 0))) return rc;
   if (h->contex)
-    k_nodes_rk<1><<<gn, 256, 0, h->stream>>>(h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, h->uu,
+    CASL_K(k_nodes_rk<1>, gn, 256, 0, h->stream)(h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, h->uu,
                                              h->vv, h->scal, h->c);
-  k_spec_rk<1><<<g, 256, 0, h->stream>>>(h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs,
+  CASL_K(k_spec_rk<1>, g, 256, 0, h->stream)(h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs,
                                          h->sqd, h->emq, h->scal, nn);
   if ((rc = check_launch(h))) return rc;
   // stage 2
-  k_advance_time<<<1, 1, 0, h->stream>>>(h->scal);
+  CASL_K(k_advance_time, 1, 1, 0, h->stream)(h->scal);
   if ((rc = inversion_dev(h, false))) return rc;
   if ((rc = source_dev(h, 1))) return rc;
   if (h->contex)
-    k_nodes_rk<2><<<gn, 256, 0, h->stream>>>(h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, h->uu,
+    CASL_K(k_nodes_rk<2>, gn, 256, 0, h->stream)(h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, h->uu,
                                              h->vv, h->scal, h->c);
-  k_spec_rk<2><<<g, 256, 0, h->stream>>>(h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs,
+  CASL_K(k_spec_rk<2>, g, 256, 0, h->stream)(h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs,
                                          h->sqd, h->emq, h->scal, nn);
   if ((rc = check_launch(h))) return rc;
   // stage 3
   if ((rc = inversion_dev(h, false))) return rc;
   if ((rc = source_dev(h, 1))) return rc;
   if (h->contex)
-    k_nodes_rk<3><<<gn, 256, 0, h->stream>>>(h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, h->uu,
+    CASL_K(k_nodes_rk<3>, gn, 256, 0, h->stream)(h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, h->uu,
                                              h->vv, h->scal, h->c);
-  k_spec_rk<3><<<g, 256, 0, h->stream>>>(h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs,
+  CASL_K(k_spec_rk<3>, g, 256, 0, h->stream)(h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs,
                                          h->sqd, h->emq, h->scal, nn);
   if ((rc = check_launch(h))) return rc;
   // stage 4
-  k_advance_time<<<1, 1, 0, h->stream>>>(h->scal);
+  CASL_K(k_advance_time, 1, 1, 0, h->stream)(h->scal);
   if ((rc = inversion_dev(h, false))) return rc;
   if ((rc = source_dev(h, 2))) return rc;
   if (h->contex)
-    k_nodes_rk<4><<<gn, 256, 0, h->stream>>>(h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, h->uu,
+    CASL_K(k_nodes_rk<4>, gn, 256, 0, h->stream)(h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, h->uu,
                                              h->vv, h->scal, h->c);
-  k_spec_rk<4><<<g, 256, 0, h->stream>>>(h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs,
+  CASL_K(k_spec_rk<4>, g, 256, 0, h->stream)(h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs,
                                          h->sqd, h->emq, h->scal, nn);
   return check_launch(h);
 }
@@ -1108,6 +1125,10 @@ void casl_destroy(casl_handle *h) {
   cudaSetDevice(h->device);
   cudaStreamSynchronize(h->stream);
   free_all(h);
+  if (h->prof_ev) {
+    for (int i = 0; i < 2 * CASL_PROF_MAX; i++) cudaEventDestroy(h->prof_ev[i]);
+    free(h->prof_ev);
+  }
   cudaStreamDestroy(h->stream);
   free(h);
 }
@@ -1147,15 +1168,15 @@ int casl_set_contours(casl_handle *h, int nq, int nptq, double qjump, const doub
     CASL_CUDA_TRY(cudaMemcpyAsync(h->xq, xq, nptq * sizeof(double), cudaMemcpyHostToDevice, s));
     CASL_CUDA_TRY(cudaMemcpyAsync(h->yq, yq, nptq * sizeof(double), cudaMemcpyHostToDevice, s));
     CASL_CUDA_TRY(cudaMemcpyAsync(h->nextq, nextq, nptq * sizeof(int), cudaMemcpyHostToDevice, s));
-    k_to0<<<grid_for(nptq), 256, 0, s>>>(h->nextq, nptq, -1);
+    CASL_K(k_to0, grid_for(nptq), 256, 0, s)(h->nextq, nptq, -1);
   }
   if (nq) {
     CASL_CUDA_TRY(cudaMemcpyAsync(h->indq, indq, nq * sizeof(int), cudaMemcpyHostToDevice, s));
     CASL_CUDA_TRY(cudaMemcpyAsync(h->npq, npq, nq * sizeof(int), cudaMemcpyHostToDevice, s));
     CASL_CUDA_TRY(cudaMemcpyAsync(h->i1q, i1q, nq * sizeof(int), cudaMemcpyHostToDevice, s));
     CASL_CUDA_TRY(cudaMemcpyAsync(h->i2q, i2q, nq * sizeof(int), cudaMemcpyHostToDevice, s));
-    k_to0<<<grid_for(nq), 256, 0, s>>>(h->i1q, nq, -1);
-    k_to0<<<grid_for(nq), 256, 0, s>>>(h->i2q, nq, -1);
+    CASL_K(k_to0, grid_for(nq), 256, 0, s)(h->i1q, nq, -1);
+    CASL_K(k_to0, grid_for(nq), 256, 0, s)(h->i2q, nq, -1);
   }
   int rc = get_scalars(h);
   if (rc) return rc;
@@ -1187,21 +1208,21 @@ int casl_get_contours(casl_handle *h, double *xq, double *yq, int *nextq, int *i
   cudaStream_t s = h->stream;
   int npt = h->nptq, nq = h->nq;
   if (npt) {
-    k_to0<<<grid_for(npt), 256, 0, s>>>(h->nextq, npt, 1);
+    CASL_K(k_to0, grid_for(npt), 256, 0, s)(h->nextq, npt, 1);
     if (xq) CASL_CUDA_TRY(cudaMemcpyAsync(xq, h->xq, npt * sizeof(double), cudaMemcpyDeviceToHost, s));
     if (yq) CASL_CUDA_TRY(cudaMemcpyAsync(yq, h->yq, npt * sizeof(double), cudaMemcpyDeviceToHost, s));
     if (nextq) CASL_CUDA_TRY(cudaMemcpyAsync(nextq, h->nextq, npt * sizeof(int), cudaMemcpyDeviceToHost, s));
-    k_to0<<<grid_for(npt), 256, 0, s>>>(h->nextq, npt, -1);
+    CASL_K(k_to0, grid_for(npt), 256, 0, s)(h->nextq, npt, -1);
   }
   if (nq) {
-    k_to0<<<grid_for(nq), 256, 0, s>>>(h->i1q, nq, 1);
-    k_to0<<<grid_for(nq), 256, 0, s>>>(h->i2q, nq, 1);
+    CASL_K(k_to0, grid_for(nq), 256, 0, s)(h->i1q, nq, 1);
+    CASL_K(k_to0, grid_for(nq), 256, 0, s)(h->i2q, nq, 1);
     if (indq) CASL_CUDA_TRY(cudaMemcpyAsync(indq, h->indq, nq * sizeof(int), cudaMemcpyDeviceToHost, s));
     if (npq) CASL_CUDA_TRY(cudaMemcpyAsync(npq, h->npq, nq * sizeof(int), cudaMemcpyDeviceToHost, s));
     if (i1q) CASL_CUDA_TRY(cudaMemcpyAsync(i1q, h->i1q, nq * sizeof(int), cudaMemcpyDeviceToHost, s));
     if (i2q) CASL_CUDA_TRY(cudaMemcpyAsync(i2q, h->i2q, nq * sizeof(int), cudaMemcpyDeviceToHost, s));
-    k_to0<<<grid_for(nq), 256, 0, s>>>(h->i1q, nq, -1);
-    k_to0<<<grid_for(nq), 256, 0, s>>>(h->i2q, nq, -1);
+    CASL_K(k_to0, grid_for(nq), 256, 0, s)(h->i1q, nq, -1);
+    CASL_K(k_to0, grid_for(nq), 256, 0, s)(h->i2q, nq, -1);
   }
   CASL_CUDA_TRY(cudaStreamSynchronize(s));
   return check_launch(h);
@@ -1258,6 +1279,7 @@ int casl_get_scalar(casl_handle *h, int which, double *value) {
     case CASL_ZZMAX: *value = s.zzmax; break;
     case CASL_UUMAX: *value = s.uumax; break;
     case CASL_QJUMP: *value = s.qjump; break;
+    case CASL_NODESTEPS: *value = h->node_steps; break;
     default: return CASL_EINVAL;
   }
   return CASL_OK;
@@ -1276,6 +1298,7 @@ int casl_set_scalar(casl_handle *h, int which, double value) {
     case CASL_TWIST: s.twist = value; break;
     case CASL_IREG: h->ireg = (int)value; break;
     case CASL_QJUMP: s.qjump = value; h->qjump = value; break;
+    case CASL_NODESTEPS: h->node_steps = value; return CASL_OK;
     default: return CASL_EINVAL;
   }
   return put_scalars(h);
@@ -1336,7 +1359,7 @@ int casl_velint(casl_handle *h, const double *uu, const double *vv, double *uq, 
   CASL_CUDA_TRY(cudaMemcpyAsync(h->w[5], vv, nn * sizeof(double), cudaMemcpyHostToDevice, s));
   int npt = h->nptq;
   if (npt > 0) {
-    k_velint<<<grid_for(npt), 256, 0, s>>>(h->xq, h->yq, npt, h->w[4], h->w[5], h->uq, h->vq, h->c);
+    CASL_K(k_velint, grid_for(npt), 256, 0, s)(h->xq, h->yq, npt, h->w[4], h->w[5], h->uq, h->vq, h->c);
     CASL_CUDA_TRY(cudaMemcpyAsync(uq, h->uq, npt * sizeof(double), cudaMemcpyDeviceToHost, s));
     CASL_CUDA_TRY(cudaMemcpyAsync(vq, h->vq, npt * sizeof(double), cudaMemcpyDeviceToHost, s));
   }
@@ -1464,7 +1487,7 @@ static int evo_init(casl_handle *h) {
   h->contex = h->nptq > 0;
   int rc = con2grid_to_spec(h, h->qc);
   if (rc) return rc;
-  k_evo_init<<<grid_for(nn), 256, 0, h->stream>>>(h->qd, h->qspre, h->qs, h->qc, h->fhi, nn);
+  CASL_K(k_evo_init, grid_for(nn), 256, 0, h->stream)(h->qd, h->qspre, h->qs, h->qc, h->fhi, nn);
   return check_launch(h);
 }
 
@@ -1472,7 +1495,7 @@ static int evo_prepare(casl_handle *h) {
   long long nn = (long long)h->n * h->n;
   int rc = con2grid_to_spec(h, h->qc);
   if (rc) return rc;
-  k_prepare<<<grid_for(nn), 256, 0, h->stream>>>(h->qs, h->qd, h->qc, h->flo, nn);
+  CASL_K(k_prepare, grid_for(nn), 256, 0, h->stream)(h->qs, h->qd, h->qc, h->flo, nn);
   if ((rc = check_launch(h))) return rc;
   return spctop_dev(h, h->qd, h->qr, h->w[0]);
 }
@@ -1517,11 +1540,11 @@ int casl_initialise(casl_handle *h, const double *qq_init) {
   CASL_CUDA_TRY(cudaMemcpyAsync(h->qr, qq_init, nn * sizeof(double), cudaMemcpyHostToDevice, s));
   double qjump;
   if (h->c.beffect) {
-    k_sub_bety<<<grid_for(nn), 256, 0, s>>>(h->qr, h->bety, h->n);
+    CASL_K(k_sub_bety, grid_for(nn), 256, 0, s)(h->qr, h->bety, h->n);
     qjump = h->p.beta * h->p.elly / (double)h->p.ncontq;
   } else {
     // contint (generic.f90:216-229)
-    k_minmax<<<RED_BLOCKS, 256, 0, s>>>(h->qr, nn, h->part);
+    CASL_K(k_minmax, RED_BLOCKS, 256, 0, s)(h->qr, nn, h->part);
     std::vector<double> part(2 * RED_BLOCKS);
     CASL_CUDA_TRY(cudaMemcpyAsync(part.data(), h->part, part.size() * sizeof(double),
                                   cudaMemcpyDeviceToHost, s));
@@ -1568,21 +1591,64 @@ int casl_step(casl_handle *h, int nsteps) {
         if ((rc = recontour_dev(h, h->qr))) return rc;
         if ((rc = sync_counts(h))) return rc;
         if ((rc = evo_init(h))) return rc;
-        k_twist_zero<<<1, 1, 0, h->stream>>>(h->scal);
+        CASL_K(k_twist_zero, 1, 1, 0, h->stream)(h->scal);
         h->ireg = 0;
         if (force) {
           h->ireg = 1;
           if ((rc = surgery_dev(h))) return rc;
-          k_twist_sub<<<1, 1, 0, h->stream>>>(h->scal, h->p.twistmax);
+          CASL_K(k_twist_sub, 1, 1, 0, h->stream)(h->scal, h->p.twistmax);
         }
       } else {
         if ((rc = surgery_dev(h))) return rc;
-        k_twist_sub<<<1, 1, 0, h->stream>>>(h->scal, h->p.twistmax);
+        CASL_K(k_twist_sub, 1, 1, 0, h->stream)(h->scal, h->p.twistmax);
       }
     }
+    h->node_steps += (double)h->nptq;
     if ((rc = advance_dev(h))) return rc;
   }
   return sync_counts(h);
+}
+
+int casl_get_stream(casl_handle *h, void **stream) {
+  if (!h || !stream) return CASL_EINVAL;
+  *stream = (void *)h->stream;
+  return CASL_OK;
+}
+
+int casl_launch_count(long long *count) {
+  if (!count) return CASL_EINVAL;
+  *count = (long long)casl::g_launches;
+  return CASL_OK;
+}
+
+int casl_profile(casl_handle *h, int kernel_class) {
+  if (!h || kernel_class < 0 || kernel_class > CASL_PROF_FFT) return CASL_EINVAL;
+  if (!h->prof_ev && kernel_class) {
+    h->prof_ev = (cudaEvent_t *)calloc(2 * CASL_PROF_MAX, sizeof(cudaEvent_t));
+    if (!h->prof_ev) return CASL_ENOMEM;
+    for (int i = 0; i < 2 * CASL_PROF_MAX; i++) CASL_CUDA_TRY(cudaEventCreate(&h->prof_ev[i]));
+  }
+  h->prof_class = kernel_class;
+  h->prof_n = 0;
+  h->prof_bytes = 0.0;
+  return CASL_OK;
+}
+
+int casl_profile_read(casl_handle *h, double *total_ms, long long *launches, double *bytes) {
+  if (!h || !total_ms || !launches || !bytes) return CASL_EINVAL;
+  CASL_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  double tot = 0.0;
+  for (int i = 0; i < h->prof_n; i++) {
+    float ms = 0.f;
+    CASL_CUDA_TRY(cudaEventElapsedTime(&ms, h->prof_ev[2 * i], h->prof_ev[2 * i + 1]));
+    tot += ms;
+  }
+  *total_ms = tot;
+  *launches = h->prof_n;
+  *bytes = h->prof_bytes;
+  h->prof_n = 0;
+  h->prof_bytes = 0.0;
+  return CASL_OK;
 }
 
 int casl_diagnostics(casl_handle *h, double out[4]) {

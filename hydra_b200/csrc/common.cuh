@@ -12,6 +12,16 @@
 
 namespace casl {
 
+// Process-wide count of kernel launches issued by this library.
+extern unsigned long long g_launches;
+
+// Every kernel launch goes through CASL_K(kernel, grid, block, smem, stream)(args);
+// it counts the launch.  The for-statement form keeps it a single statement
+// that is safe inside an unbraced if/else.
+#define CASL_K(name, ...)                                                          \
+  for (bool casl_once_ = (++::casl::g_launches, true); casl_once_; casl_once_ = false) \
+  name<<<__VA_ARGS__>>>
+
 // Constants of constants.f90 and contours.f90:17-42, computed once on the
 // host by the same operations as the reference's PARAMETER expressions.
 struct Consts {

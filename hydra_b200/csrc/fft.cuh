@@ -135,6 +135,7 @@ __device__ double2 *complex_fft(double2 *a, double2 *b, int V, int h, int ldc, i
 
 // Plain strided load / store functors: element (b, v, j) at p[b*bs + v*vs + j*es].
 struct LoadStrided {
+  __host__ double bytes() const { return 8.0; }
   const double *p;
   long long bs, vs, es;
   __device__ __forceinline__ double operator()(int b, int v, int j) const {
@@ -142,6 +143,7 @@ struct LoadStrided {
   }
 };
 struct StoreStrided {
+  __host__ double bytes() const { return 8.0; }
   double *p;
   long long bs, vs, es;
   __device__ __forceinline__ void operator()(int b, int v, int k, double x) const {

@@ -591,8 +591,11 @@ int recontour_dev(casl_handle *h, const double *qq) {
       return CASL_OK;
     }
   }
-  // Field memory: qa (double) + integer levels; kept for the whole call.
-  size_t need_field = (size_t)NU * 12 + ((size_t)64 << 20);
+  // Field memory: qa (double) + integer levels + per-chunk crossing counts;
+  // kept for the whole call.
+  const long long nchunks_f = (2 * NU + EDGES_PER_THREAD - 1) / EDGES_PER_THREAD;
+  size_t need_field = (size_t)NU * 12 + (size_t)nchunks_f * 8 + (size_t)nxu * 4 +
+                      ((size_t)64 << 20);
   RC_TRY(ensure_scratch(h, need_field));
   Arena ar{(char *)h->sx, h->sx_bytes, 0};
   double *qa = ar.get<double>(NU);
@@ -600,18 +603,18 @@ int recontour_dev(casl_handle *h, const double *qq) {
   int *ljx = ar.get<int>(nxu);
   unsigned long long *lsum = ar.get<unsigned long long>(4);
   double *part = ar.get<double>(2 * 4096);
-  if (!part) return CASL_ENOMEM;
+  if (ar.failed) return CASL_ENOMEM;
   if (have) {
     CASL_CUDA_TRY(cudaMemsetAsync(Lu, 0, (size_t)NU * sizeof(int), st));
     CASL_CUDA_TRY(cudaMemsetAsync(ljx, 0, (size_t)nxu * sizeof(int), st));
     CASL_CUDA_TRY(cudaMemsetAsync(lsum, 0, sizeof(unsigned long long), st));
-    k_u_scatter<<<gsz(h->nptq), 256, 0, st>>>(h->xq, h->yq, h->nextq, h->nptq, qjump, Lu, ljx, c,
+    CASL_K(k_u_scatter, gsz(h->nptq), 256, 0, st)(h->xq, h->yq, h->nextq, h->nptq, qjump, Lu, ljx, c,
                                               &h->scal->error);
-    k_u_lbot<<<1, 1024, 0, st>>>(ljx, Lu, nxu, nyu);
-    k_u_colscan<<<(nxu * 32 + 255) / 256, 256, 0, st>>>(Lu, nxu, nyu, lsum);
+    CASL_K(k_u_lbot, 1, 1024, 0, st)(ljx, Lu, nxu, nyu);
+    CASL_K(k_u_colscan, (nxu * 32 + 255) / 256, 256, 0, st)(Lu, nxu, nyu, lsum);
   }
   const int fb = 4096;
-  k_u_field<<<fb, 256, 0, st>>>(Lu, lsum, qq, qjump, have, qa, part, c);
+  CASL_K(k_u_field, fb, 256, 0, st)(Lu, lsum, qq, qjump, have, qa, part, c);
   RC_TRY(check_launch(h));
   RC_TRY(fetch_err(h));
   std::vector<double> hp(2 * fb);
@@ -645,8 +648,8 @@ int recontour_dev(casl_handle *h, const double *qq) {
   int *ccnt = ar.get<int>(nchunks), *coffs = ar.get<int>(nchunks);
   int *tmpi = ar.get<int>(scan_tmp_elems(nchunks) + 4);
   int *dtot = ar.get<int>(16);
-  if (!dtot) return CASL_ENOMEM;
-  k_cr_count<<<gsz(nchunks), 256, 0, st>>>(qa, li, nxu, nyu, nchunks, ccnt);
+  if (ar.failed) return CASL_ENOMEM;
+  CASL_K(k_cr_count, gsz(nchunks), 256, 0, st)(qa, li, nxu, nyu, nchunks, ccnt);
   exclusive_scan<int>(st, ccnt, coffs, nchunks, tmpi, dtot);
   int ncr_i = 0;
   CASL_CUDA_TRY(cudaMemcpyAsync(&ncr_i, dtot, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -674,16 +677,16 @@ int recontour_dev(casl_handle *h, const double *qq) {
   int *rlev = ar2.get<int>(ncr), *rlev2 = ar2.get<int>(ncr);
   int *tmpi2 = ar2.get<int>(scan_tmp_elems(ncr) + 4);
   void *sort_tmp = ar2.get<char>(sort_bytes + 16);
-  if (!sort_tmp) return CASL_ENOMEM;
-  k_cr_emit<<<gsz(nchunks), 256, 0, st>>>(qa, li, nxu, nyu, nchunks, coffs, redge, rlev);
+  if (ar2.failed) return CASL_ENOMEM;
+  CASL_K(k_cr_emit, gsz(nchunks), 256, 0, st)(qa, li, nxu, nyu, nchunks, coffs, redge, rlev);
   CASL_CUDA_TRY(cub::DeviceRadixSort::SortPairs(sort_tmp, sort_bytes, rlev, rlev2, redge, redge2,
                                                 (int)ncr, 0, endbit, st));
   std::swap(rlev, rlev2);
   std::swap(redge, redge2);
   double *xcr = ar2.get<double>(ncr), *ycr = ar2.get<double>(ncr);
   unsigned int *kib = ar2.get<unsigned int>(ncr), *kob = ar2.get<unsigned int>(ncr);
-  if (!kob) return CASL_ENOMEM;
-  k_cr_geom<<<gsz(ncr), 256, 0, st>>>(qa, redge, rlev, ncr, li, c, xcr, ycr, kib, kob);
+  if (ar2.failed) return CASL_ENOMEM;
+  CASL_K(k_cr_geom, gsz(ncr), 256, 0, st)(qa, redge, rlev, ncr, li, c, xcr, ycr, kib, kob);
   RC_TRY(check_launch(h));
 
   // --- 4. box tables: hash (level, box) -> two out-crossing slots ------------
@@ -693,12 +696,12 @@ int recontour_dev(casl_handle *h, const double *qq) {
   int *slots = ar2.get<int>(2 * cap);
   int *succ = ar2.get<int>(ncr);
   long long *sadslot = ar2.get<long long>(ncr);
-  if (!sadslot) return CASL_ENOMEM;
+  if (ar2.failed) return CASL_ENOMEM;
   CASL_CUDA_TRY(cudaMemsetAsync(keys, 0xff, cap * sizeof(unsigned long long), st));
   CASL_CUDA_TRY(cudaMemsetAsync(slots, 0xff, 2 * cap * sizeof(int), st));
-  k_h_insert<<<gsz(ncr), 256, 0, st>>>(rlev, kob, ncr, keys, slots, cap - 1, &h->scal->error);
-  k_h_order<<<gsz(cap), 256, 0, st>>>(keys, slots, cap);
-  k_h_succ<<<gsz(ncr), 256, 0, st>>>(rlev, kib, ncr, keys, slots, cap - 1, succ, sadslot,
+  CASL_K(k_h_insert, gsz(ncr), 256, 0, st)(rlev, kob, ncr, keys, slots, cap - 1, &h->scal->error);
+  CASL_K(k_h_order, gsz(cap), 256, 0, st)(keys, slots, cap);
+  CASL_K(k_h_succ, gsz(ncr), 256, 0, st)(rlev, kib, ncr, keys, slots, cap - 1, succ, sadslot,
                                      &h->scal->error);
   RC_TRY(check_launch(h));
   RC_TRY(fetch_err(h));
@@ -708,24 +711,24 @@ int recontour_dev(casl_handle *h, const double *qq) {
       *lab2 = ar2.get<int>(ncr), *term = ar2.get<int>(ncr), *term2 = ar2.get<int>(ncr),
       *val = ar2.get<int>(ncr), *val2 = ar2.get<int>(ncr), *ep = ar2.get<int>(ncr),
       *ep2 = ar2.get<int>(ncr);
-  if (!ep2) return CASL_ENOMEM;
+  if (ar2.failed) return CASL_ENOMEM;
   int rounds = 1;
   while ((1LL << rounds) < ncr) rounds++;
   rounds++;
   int g = gsz(ncr);
-  k_pj_init<<<g, 256, 0, st>>>(succ, ncr, nx, lab, term);
+  CASL_K(k_pj_init, g, 256, 0, st)(succ, ncr, nx, lab, term);
   for (int it = 0; it < rounds; it++) {
-    k_pj_min<<<g, 256, 0, st>>>(nx, lab, term, ncr, nx2, lab2, term2);
+    CASL_K(k_pj_min, g, 256, 0, st)(nx, lab, term, ncr, nx2, lab2, term2);
     std::swap(nx, nx2); std::swap(lab, lab2); std::swap(term, term2);
   }
-  k_pj_listinit<<<g, 256, 0, st>>>(succ, lab, term, ncr, nx, val);
+  CASL_K(k_pj_listinit, g, 256, 0, st)(succ, lab, term, ncr, nx, val);
   for (int it = 0; it < rounds; it++) {
-    k_pj_rank<<<g, 256, 0, st>>>(nx, val, ncr, nx2, val2);
+    CASL_K(k_pj_rank, g, 256, 0, st)(nx, val, ncr, nx2, val2);
     std::swap(nx, nx2); std::swap(val, val2);
   }
-  k_pj_endinit<<<g, 256, 0, st>>>(succ, ncr, ep);
+  CASL_K(k_pj_endinit, g, 256, 0, st)(succ, ncr, ep);
   for (int it = 0; it < rounds; it++) {
-    k_pj_end<<<g, 256, 0, st>>>(ep, ncr, ep2);
+    CASL_K(k_pj_end, g, 256, 0, st)(ep, ncr, ep2);
     std::swap(ep, ep2);
   }
   RC_TRY(check_launch(h));
@@ -850,8 +853,8 @@ int recontour_dev(casl_handle *h, const double *qq) {
 
   // --- 7. contour order and walk layout ---------------------------------------
   int *startf = ar2.get<int>(ncr), *clenr = ar2.get<int>(ncr), *cidx = ar2.get<int>(ncr);
-  if (!cidx) return CASL_ENOMEM;
-  k_ct_plain<<<g, 256, 0, st>>>(lab, term, val, ncr, startf, clenr);
+  if (ar2.failed) return CASL_ENOMEM;
+  CASL_K(k_ct_plain, g, 256, 0, st)(lab, term, val, ncr, startf, clenr);
   for (int k = 0; k < nsad_contours; k++) {
     int one = 1;
     CASL_CUDA_TRY(cudaMemcpyAsync(startf + sad_start[k], &one, sizeof(int), cudaMemcpyHostToDevice, st));
@@ -864,7 +867,7 @@ int recontour_dev(casl_handle *h, const double *qq) {
   if (C == 0) return set_empty();
   int *clen = ar2.get<int>(C), *coff = ar2.get<int>(C), *clevt = ar2.get<int>(C);
   double *xw = ar2.get<double>(ncr), *yw = ar2.get<double>(ncr);
-  if (!yw) return CASL_ENOMEM;
+  if (ar2.failed) return CASL_ENOMEM;
   {
     // contour lengths and offsets in contour order (host: one pass over ncr)
     std::vector<int> h_start(ncr), h_clenr(ncr), h_cidx(ncr);
@@ -883,7 +886,7 @@ int recontour_dev(casl_handle *h, const double *qq) {
     if (acc != ncr) return CASL_EINVAL;
     CASL_CUDA_TRY(cudaMemcpyAsync(clen, hl.data(), C * sizeof(int), cudaMemcpyHostToDevice, st));
     CASL_CUDA_TRY(cudaMemcpyAsync(coff, ho.data(), C * sizeof(int), cudaMemcpyHostToDevice, st));
-    k_ct_gather_plain<<<g, 256, 0, st>>>(lab, term, val, cidx, coff, clen, xcr, ycr, ncr, xw, yw);
+    CASL_K(k_ct_gather_plain, g, 256, 0, st)(lab, term, val, cidx, coff, clen, xcr, ycr, ncr, xw, yw);
     int nch = (int)ch_end.size();
     if (nch > 0) {
       // absolute position of every chain; the first chain of a contour is
@@ -902,18 +905,18 @@ int recontour_dev(casl_handle *h, const double *qq) {
       long long *d_pos = ar2.get<long long>(nch);
       int *d_len = ar2.get<int>(nch), *d_rot = ar2.get<int>(nch), *d_cl = ar2.get<int>(nch);
       int *chain_of_end = ar2.get<int>(ncr);
-      if (!chain_of_end) return CASL_ENOMEM;
+      if (ar2.failed) return CASL_ENOMEM;
       CASL_CUDA_TRY(cudaMemcpyAsync(d_pos, abs_pos.data(), nch * sizeof(long long), cudaMemcpyHostToDevice, st));
       CASL_CUDA_TRY(cudaMemcpyAsync(d_len, ch_len.data(), nch * sizeof(int), cudaMemcpyHostToDevice, st));
       CASL_CUDA_TRY(cudaMemcpyAsync(d_rot, ch_rot.data(), nch * sizeof(int), cudaMemcpyHostToDevice, st));
       CASL_CUDA_TRY(cudaMemcpyAsync(d_cl, rotlen.data(), nch * sizeof(int), cudaMemcpyHostToDevice, st));
       CASL_CUDA_TRY(cudaMemcpyAsync(chain_of_end, hcoe.data(), ncr * sizeof(int), cudaMemcpyHostToDevice, st));
-      k_ct_gather_chain<<<g, 256, 0, st>>>(term, ep, val, chain_of_end, d_pos, d_len, d_rot, d_cl,
+      CASL_K(k_ct_gather_chain, g, 256, 0, st)(term, ep, val, chain_of_end, d_pos, d_len, d_rot, d_cl,
                                            xcr, ycr, ncr, xw, yw);
       CASL_CUDA_TRY(cudaStreamSynchronize(st));
     }
   }
-  k_lev_of_contour<<<g, 256, 0, st>>>(startf, rlev, cidx, ncr, li, h->p.nlevm, clevt);
+  CASL_K(k_lev_of_contour, g, 256, 0, st)(startf, rlev, cidx, ncr, li, h->p.nlevm, clevt);
   RC_TRY(check_launch(h));
 
   // --- 8. renode three times (congen.f90:295-310) -----------------------------
@@ -926,7 +929,7 @@ int recontour_dev(casl_handle *h, const double *qq) {
     ocs[q] = ar2.get<int>(C); olen[q] = ar2.get<int>(C); olev[q] = ar2.get<int>(C);
   }
   int *cnt = ar2.get<int>(4);
-  if (!cnt) return CASL_ENOMEM;
+  if (ar2.failed) return CASL_ENOMEM;
   double *ox[3] = {xa, xb, xa}, *oy[3] = {ya, yb, ya};
   int hc[3] = {0, 0, 0};
   for (int pass = 0; pass < 3; pass++) {
@@ -948,10 +951,10 @@ int recontour_dev(casl_handle *h, const double *qq) {
   if (npt > h->npm || nq > h->nm) return CASL_ECAPACITY;
   CASL_CUDA_TRY(cudaMemcpyAsync(h->xq, cur.xw, (size_t)npt * sizeof(double), cudaMemcpyDeviceToDevice, st));
   CASL_CUDA_TRY(cudaMemcpyAsync(h->yq, cur.yw, (size_t)npt * sizeof(double), cudaMemcpyDeviceToDevice, st));
-  k_out_contours<<<gsz(nq), 256, 0, st>>>(cur.cs, cur.len, cur.levt, nq, h->i1q, h->i2q, h->npq,
+  CASL_K(k_out_contours, gsz(nq), 256, 0, st)(cur.cs, cur.len, cur.levt, nq, h->i1q, h->i2q, h->npq,
                                           h->indq);
-  k_out_links<<<gsz(npt), 256, 0, st>>>(cur.cs, cur.len, nq, npt, h->nextq);
-  k_set_counts2<<<1, 1, 0, st>>>(h->scal, cnt);
+  CASL_K(k_out_links, gsz(npt), 256, 0, st)(cur.cs, cur.len, nq, npt, h->nextq);
+  CASL_K(k_set_counts2, 1, 1, 0, st)(h->scal, cnt);
   RC_TRY(check_launch(h));
   h->nq = nq;
   h->nptq = npt;

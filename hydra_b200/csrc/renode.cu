@@ -280,20 +280,20 @@ int renode_batch(casl_handle *h, Arena &ar, const RenodeIn &in, RenodeOut &out, 
   s.tmpi = ar.get<int>(tmpn);
   s.tmps = ar.get<SegPair>(tmpn);
   s.d_tot = ar.get<int>(8);
-  if (!s.d_tot) return CASL_ENOMEM;
+  if (ar.failed) return CASL_ENOMEM;
   cudaMemsetAsync(s.ccnt, 0, C * sizeof(int), st);
   int g = gsz(N);
-  k_rn_cid<<<g, 256, 0, st>>>(in.cs, C, N, s.cid, s.head);
-  k_rn1<<<g, 256, 0, st>>>(in, s, c);
-  k_rn2<<<g, 256, 0, st>>>(in, s, c);
-  k_rn3<<<g, 256, 0, st>>>(in, s, c);
-  k_rn4<<<g, 256, 0, st>>>(in, s, c);
-  k_rn5<<<g, 256, 0, st>>>(in, s, c);
+  CASL_K(k_rn_cid, g, 256, 0, st)(in.cs, C, N, s.cid, s.head);
+  CASL_K(k_rn1, g, 256, 0, st)(in, s, c);
+  CASL_K(k_rn2, g, 256, 0, st)(in, s, c);
+  CASL_K(k_rn3, g, 256, 0, st)(in, s, c);
+  CASL_K(k_rn4, g, 256, 0, st)(in, s, c);
+  CASL_K(k_rn5, g, 256, 0, st)(in, s, c);
   segmented_scan(st, s.e, s.head, s.S, N, s.tmps);
   exclusive_scan<int>(st, s.corner, s.crank, N, s.tmpi, s.d_tot + 0);
-  k_rn_cornerpos<<<g, 256, 0, st>>>(s.corner, s.crank, s.cornerpos, N);
+  CASL_K(k_rn_cornerpos, g, 256, 0, st)(s.corner, s.crank, s.cornerpos, N);
   int gc = gsz(C);
-  k_rn_count<<<gc, 256, 0, st>>>(in, s, c, mode);
+  CASL_K(k_rn_count, gc, 256, 0, st)(in, s, c, mode);
   exclusive_scan<int>(st, s.npiece, s.poff, C, s.tmpi, s.d_tot + 1);
   // pieces: at most one per corner, or one per contour
   int hp = 0;
@@ -304,18 +304,18 @@ int renode_batch(casl_handle *h, Arena &ar, const RenodeIn &in, RenodeOut &out, 
   s.pc = ar.get<int>(P); s.pstart = ar.get<int>(P); s.plen = ar.get<int>(P);
   s.pn = ar.get<int>(P); s.pout = ar.get<int>(P);
   s.psum = ar.get<double>(P); s.pfac = ar.get<double>(P);
-  if (!s.pfac) return CASL_ENOMEM;
-  k_rn_fill<<<gc, 256, 0, st>>>(in, s, c, mode);
+  if (ar.failed) return CASL_ENOMEM;
+  CASL_K(k_rn_fill, gc, 256, 0, st)(in, s, c, mode);
   exclusive_scan<int>(st, s.cnpr, s.cout, C, s.tmpi, s.d_tot + 2);
   exclusive_scan<int>(st, s.ckeep, s.ckidx, C, s.tmpi, s.d_tot + 3);
-  k_rn_finish<<<1, 1, 0, st>>>(out.d_counts, s.d_tot + 2, s.d_tot + 3, out.cap);
+  CASL_K(k_rn_finish, 1, 1, 0, st)(out.d_counts, s.d_tot + 2, s.d_tot + 3, out.cap);
   int hc[3];
   cudaMemcpyAsync(hc, out.d_counts, 3 * sizeof(int), cudaMemcpyDeviceToHost, st);
   e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return set_cuda_error(h, e);
   if (hc[2]) return CASL_ECAPACITY;
-  k_rn_pout<<<gc, 256, 0, st>>>(in, s, out);
-  k_rn_place<<<g, 256, 0, st>>>(in, s, out, c);
+  CASL_K(k_rn_pout, gc, 256, 0, st)(in, s, out);
+  CASL_K(k_rn_place, g, 256, 0, st)(in, s, out, c);
   return check_launch(h);
 }
 

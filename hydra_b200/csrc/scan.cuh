@@ -11,14 +11,20 @@
 
 namespace casl {
 
-// Bump allocator over one device buffer (256-byte aligned pieces).
+// Bump allocator over one device buffer (256-byte aligned pieces).  Once a
+// request does not fit, every later request fails too, so checking the last
+// pointer of a group of requests checks them all.
 struct Arena {
   char *base;
   size_t cap, off;
+  bool failed = false;
   template <class T>
   T *get(size_t count) {
     size_t bytes = (count * sizeof(T) + 255) & ~(size_t)255;
-    if (off + bytes > cap) return nullptr;
+    if (failed || base == nullptr || off + bytes > cap) {
+      failed = true;
+      return nullptr;
+    }
     T *p = reinterpret_cast<T *>(base + off);
     off += bytes;
     return p;
@@ -118,9 +124,9 @@ int exclusive_scan(cudaStream_t st, const T *in, T *out, long long n, T *tmp, T 
     return 0;
   }
   int tiles = (int)((n + SCAN_TILE - 1) / SCAN_TILE);
-  k_scan_tiles<T><<<tiles, SCAN_BLOCK, 0, st>>>(in, out, tmp, n);
-  k_scan_totals<T><<<1, SCAN_BLOCK, 0, st>>>(tmp, tiles, grand);
-  k_scan_add<T><<<(int)((n + 255) / 256), 256, 0, st>>>(out, tmp, n);
+  CASL_K(k_scan_tiles<T>, tiles, SCAN_BLOCK, 0, st)(in, out, tmp, n);
+  CASL_K(k_scan_totals<T>, 1, SCAN_BLOCK, 0, st)(tmp, tiles, grand);
+  CASL_K(k_scan_add<T>, (int)((n + 255) / 256), 256, 0, st)(out, tmp, n);
   return (int)cudaGetLastError();
 }
 
@@ -248,9 +254,9 @@ inline int segmented_scan(cudaStream_t st, const double *in, const int *head, do
                           long long n, SegPair *tmp) {
   if (n <= 0) return 0;
   int tiles = (int)((n + SCAN_TILE - 1) / SCAN_TILE);
-  k_segscan_tiles<<<tiles, SCAN_BLOCK, 0, st>>>(in, head, out, tmp, n);
-  k_segscan_totals<<<1, SCAN_BLOCK, 0, st>>>(tmp, tiles);
-  k_segscan_add<<<tiles, 256, 0, st>>>(out, head, tmp, n);
+  CASL_K(k_segscan_tiles, tiles, SCAN_BLOCK, 0, st)(in, head, out, tmp, n);
+  CASL_K(k_segscan_totals, 1, SCAN_BLOCK, 0, st)(tmp, tiles);
+  CASL_K(k_segscan_add, tiles, 256, 0, st)(out, head, tmp, n);
   return (int)cudaGetLastError();
 }
 

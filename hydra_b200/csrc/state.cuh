@@ -21,6 +21,7 @@ struct casl_handle {
   int nq, nptq;          // host copies of the counts
   int ireg;              // regularisations since the last recontouring
   int contex;
+  double node_steps;     // sum of nptq over advanced steps (casl_step)
 
   // nodes (structure of arrays; nextq 0-based internally)
   double *xq, *yq;
@@ -51,7 +52,15 @@ struct casl_handle {
   size_t sx_bytes;
   void *sx2;             // second arena (recontouring's per-crossing data)
   size_t sx2_bytes;
+
+  // kernel-class timing for benchmarks (events on the handle's stream)
+  int prof_class;
+  int prof_n;
+  double prof_bytes;
+  cudaEvent_t *prof_ev;  // 2 * CASL_PROF_MAX events, created on first use
 };
+
+#define CASL_PROF_MAX 8192
 
 namespace casl {
 

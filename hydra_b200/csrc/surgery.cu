@@ -494,9 +494,9 @@ static int rebuild_and_renode(casl_handle *h, Arena &ar, const int *lvl, const L
   int *stf = ar.get<int>(npt), *brk = ar.get<int>(npt), *sx = ar.get<int>(npt);
   int *rid = ar.get<int>(npt), *tmpi = ar.get<int>(scan_tmp_elems(npt) + 4);
   int *dtot = ar.get<int>(8);
-  if (!dtot) return CASL_ENOMEM;
+  if (ar.failed) return CASL_ENOMEM;
   int g = gs(npt);
-  k_rb_flags<<<g, 256, 0, st>>>(h->nextq, npt, stf, brk);
+  CASL_K(k_rb_flags, g, 256, 0, st)(h->nextq, npt, stf, brk);
   exclusive_scan<int>(st, stf, sx, npt, tmpi, dtot);
   int R = 0;
   cudaMemcpyAsync(&R, dtot, sizeof(int), cudaMemcpyDeviceToHost, st);
@@ -507,21 +507,21 @@ static int rebuild_and_renode(casl_handle *h, Arena &ar, const int *lvl, const L
   int *succ = ar.get<int>(R), *succ2 = ar.get<int>(R), *ishead = ar.get<int>(R);
   int *cidx = ar.get<int>(R);
   long long *val = ar.get<long long>(R), *val2 = ar.get<long long>(R);
-  if (!val2) return CASL_ENOMEM;
-  k_rb_runs<<<g, 256, 0, st>>>(stf, brk, sx, npt, rid, rs, re);
+  if (ar.failed) return CASL_ENOMEM;
+  CASL_K(k_rb_runs, g, 256, 0, st)(stf, brk, sx, npt, rid, rs, re);
   int gr = gs(R);
-  k_rb_runinit<<<gr, 256, 0, st>>>(h->nextq, rid, rs, re, R, nr, lab, nrj);
+  CASL_K(k_rb_runinit, gr, 256, 0, st)(h->nextq, rid, rs, re, R, nr, lab, nrj);
   int rounds = 1;
   while ((1 << rounds) < R) rounds++;
   rounds++;
   for (int it = 0; it < rounds; it++) {
-    k_rb_minjump<<<gr, 256, 0, st>>>(lab, nrj, R, lab2, nrj2);
+    CASL_K(k_rb_minjump, gr, 256, 0, st)(lab, nrj, R, lab2, nrj2);
     std::swap(lab, lab2);
     std::swap(nrj, nrj2);
   }
-  k_rb_succ<<<gr, 256, 0, st>>>(lab, rid, nr, rs, re, R, hr, succ, val, ishead);
+  CASL_K(k_rb_succ, gr, 256, 0, st)(lab, rid, nr, rs, re, R, hr, succ, val, ishead);
   for (int it = 0; it < rounds; it++) {
-    k_rb_sumjump<<<gr, 256, 0, st>>>(val, succ, R, val2, succ2);
+    CASL_K(k_rb_sumjump, gr, 256, 0, st)(val, succ, R, val2, succ2);
     std::swap(val, val2);
     std::swap(succ, succ2);
   }
@@ -532,10 +532,10 @@ static int rebuild_and_renode(casl_handle *h, Arena &ar, const int *lvl, const L
   if (e != cudaSuccess) return set_cuda_error(h, e);
   int *clen = ar.get<int>(C), *clev = ar.get<int>(C), *cst = ar.get<int>(C);
   double *xw = ar.get<double>(npt), *yw = ar.get<double>(npt);
-  if (!yw) return CASL_ENOMEM;
-  k_rb_cycles<<<gr, 256, 0, st>>>(ishead, cidx, val, rs, lvl, dlev, R, clen, clev);
+  if (ar.failed) return CASL_ENOMEM;
+  CASL_K(k_rb_cycles, gr, 256, 0, st)(ishead, cidx, val, rs, lvl, dlev, R, clen, clev);
   exclusive_scan<int>(st, clen, cst, C, tmpi, dtot + 2);
-  k_rb_gather<<<g, 256, 0, st>>>(h->xq, h->yq, npt, rid, rs, hr, cidx, val, cst, clen, xw, yw);
+  CASL_K(k_rb_gather, g, 256, 0, st)(h->xq, h->yq, npt, rid, rs, hr, cidx, val, cst, clen, xw, yw);
   int rc = check_launch(h);
   if (rc) return rc;
   // renode every cycle; write straight into the node arrays
@@ -546,7 +546,7 @@ static int rebuild_and_renode(casl_handle *h, Arena &ar, const int *lvl, const L
   out.ocs = ar.get<int>(C); out.olen = ar.get<int>(C); out.olev = ar.get<int>(C);
   out.cap = h->npm;
   out.d_counts = ar.get<int>(4);
-  if (!out.d_counts) return CASL_ENOMEM;
+  if (ar.failed) return CASL_ENOMEM;
   rc = renode_batch(h, ar, in, out, RENODE_SURGERY);
   if (rc) return rc;
   int hc[3];
@@ -560,11 +560,11 @@ static int rebuild_and_renode(casl_handle *h, Arena &ar, const int *lvl, const L
     cudaMemcpyAsync(h->yq, out.yo, (size_t)nptn * sizeof(double), cudaMemcpyDeviceToDevice, st);
   }
   if (nq > 0) {
-    k_rb_contours<<<gs(nq), 256, 0, st>>>(out.ocs, out.olen, out.olev, nq, h->i1q, h->i2q, h->npq,
+    CASL_K(k_rb_contours, gs(nq), 256, 0, st)(out.ocs, out.olen, out.olev, nq, h->i1q, h->i2q, h->npq,
                                           h->indq);
-    k_rb_links<<<gs(nptn), 256, 0, st>>>(out.ocs, out.olen, nq, nptn, h->nextq);
+    CASL_K(k_rb_links, gs(nptn), 256, 0, st)(out.ocs, out.olen, nq, nptn, h->nextq);
   }
-  k_set_counts<<<1, 1, 0, st>>>(h->scal, out.d_counts);
+  CASL_K(k_set_counts, 1, 1, 0, st)(h->scal, out.d_counts);
   rc = check_launch(h);
   if (rc) return rc;
   h->nq = nq;
@@ -625,7 +625,7 @@ int surgery_dev(casl_handle *h) {
   }
   int nlev = (int)lev.size();
   // scratch
-  size_t need = (size_t)npt * 420 + (size_t)nbox * 40 + (size_t)nq * 256 + ((size_t)64 << 20);
+  size_t need = (size_t)npt * 560 + (size_t)nbox * 40 + (size_t)nq * 256 + ((size_t)64 << 20);
   int rc = ensure_scratch(h, need);
   if (rc) return rc;
   Arena ar{(char *)h->sx, h->sx_bytes, 0};
@@ -641,22 +641,22 @@ int surgery_dev(casl_handle *h) {
   int *nbcnt = ar.get<int>(nbox), *nb1 = ar.get<int>(nbox), *nbnode = ar.get<int>(npt);
   int *tmpi = ar.get<int>(scan_tmp_elems(std::max<long long>(npt, nbox)) + 4);
   int *dtot = ar.get<int>(8);
-  if (!dtot) return CASL_ENOMEM;
+  if (ar.failed) return CASL_ENOMEM;
   cudaMemcpyAsync(dlev, lev.data(), nlev * sizeof(LevelDesc), cudaMemcpyHostToDevice, st);
   cudaMemsetAsync(endnext, 0xff, (size_t)npt * sizeof(int), st);
   cudaMemsetAsync(bcnt, 0, (size_t)nbox * sizeof(int), st);
   cudaMemsetAsync(nbcnt, 0, (size_t)nbox * sizeof(int), st);
   cudaMemsetAsync(&h->scal->error, 0, sizeof(int), st);
   int g = gs(npt);
-  k_sg_endnext<<<gs(nq), 256, 0, st>>>(h->i1q, h->i2q, nq, endnext);
-  k_sg_level_of<<<g, 256, 0, st>>>(dlev, nlev, npt, lvl);
-  k_sg_init<<<g, 256, 0, st>>>(h->xq, h->yq, h->nextq, endnext, npt, dx, dy, dsq, x0, y0, dx0, dy0,
+  CASL_K(k_sg_endnext, gs(nq), 256, 0, st)(h->i1q, h->i2q, nq, endnext);
+  CASL_K(k_sg_level_of, g, 256, 0, st)(dlev, nlev, npt, lvl);
+  CASL_K(k_sg_init, g, 256, 0, st)(h->xq, h->yq, h->nextq, endnext, npt, dx, dy, dsq, x0, y0, dx0, dy0,
                                nq0, prev0, pending, c, &h->scal->error);
   SurgState S{};
   S.xq = h->xq; S.yq = h->yq; S.dx = dx; S.dy = dy; S.dsq = dsq; S.nextq = h->nextq;
   S.x0 = x0; S.y0 = y0; S.dx0 = dx0; S.dy0 = dy0; S.nq0 = nq0; S.prev0 = prev0; S.lvl = lvl;
   S.pending = pending;
-  k_sg_count_entries<<<g, 256, 0, st>>>(S, dlev, npt, ecount, nbox_of, nbcnt, c);
+  CASL_K(k_sg_count_entries, g, 256, 0, st)(S, dlev, npt, ecount, nbox_of, nbcnt, c);
   exclusive_scan<int>(st, ecount, eoff, npt, tmpi, dtot);
   int ne = 0;
   cudaMemcpyAsync(&ne, dtot, sizeof(int), cudaMemcpyDeviceToHost, st);
@@ -666,20 +666,20 @@ int surgery_dev(casl_handle *h) {
   if (e != cudaSuccess) return set_cuda_error(h, e);
   if (herr) return herr;
   int *ebox = ar.get<int>(ne), *eib = ar.get<int>(ne), *bnode = ar.get<int>(ne);
-  if (!bnode) return CASL_ENOMEM;
-  k_sg_emit<<<g, 256, 0, st>>>(S, dlev, npt, eoff, ebox, eib, bcnt, c);
+  if (ar.failed) return CASL_ENOMEM;
+  CASL_K(k_sg_emit, g, 256, 0, st)(S, dlev, npt, eoff, ebox, eib, bcnt, c);
   exclusive_scan<int>(st, bcnt, kb1, nbox, tmpi, dtot + 1);
   cudaMemsetAsync(cursor, 0, (size_t)nbox * sizeof(int), st);
-  k_sg_place<<<gs(ne), 256, 0, st>>>(ebox, eib, ne, kb1, cursor, bnode);
-  k_sg_sort_boxes<<<gs(nbox), 256, 0, st>>>(kb1, bcnt, (int)nbox, bnode);
+  CASL_K(k_sg_place, gs(ne), 256, 0, st)(ebox, eib, ne, kb1, cursor, bnode);
+  CASL_K(k_sg_sort_boxes, gs(nbox), 256, 0, st)(kb1, bcnt, (int)nbox, bnode);
   exclusive_scan<int>(st, nbcnt, nb1, nbox, tmpi, dtot + 2);
   cudaMemsetAsync(cursor, 0, (size_t)nbox * sizeof(int), st);
-  k_sg_place_nodes<<<g, 256, 0, st>>>(nbox_of, npt, nb1, cursor, nbnode);
+  CASL_K(k_sg_place_nodes, g, 256, 0, st)(nbox_of, npt, nb1, cursor, nbnode);
   S.kb1 = kb1; S.bcnt = bcnt; S.bnode = bnode; S.nb1 = nb1; S.nbcnt = nbcnt; S.nbnode = nbnode;
-  k_sg_candidates<<<g, 256, 0, st>>>(S, dlev, npt, nbox_of, c);
+  CASL_K(k_sg_candidates, g, 256, 0, st)(S, dlev, npt, nbox_of, c);
   int *nsurg = dtot + 4;
   cudaMemsetAsync(nsurg, 0, sizeof(int), st);
-  k_sg_replay<<<(nlev * 32 + 127) / 128, 128, 0, st>>>(S, dlev, nlev, c, nsurg);
+  CASL_K(k_sg_replay, (nlev * 32 + 127) / 128, 128, 0, st)(S, dlev, nlev, c, nsurg);
   rc = check_launch(h);
   if (rc) return rc;
   return rebuild_and_renode(h, ar, lvl, dlev);
@@ -701,7 +701,7 @@ int renode_host(casl_handle *h, const double *xd, const double *yd, int npd, dou
   out.ocs = ar.get<int>(1); out.olen = ar.get<int>(1); out.olev = ar.get<int>(1);
   out.cap = cap;
   out.d_counts = ar.get<int>(4);
-  if (!out.d_counts) return CASL_ENOMEM;
+  if (ar.failed) return CASL_ENOMEM;
   int z = 0;
   CASL_CUDA_TRY(cudaMemcpyAsync(xw, xd, npd * sizeof(double), cudaMemcpyHostToDevice, st));
   CASL_CUDA_TRY(cudaMemcpyAsync(yw, yd, npd * sizeof(double), cudaMemcpyHostToDevice, st));

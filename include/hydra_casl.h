@@ -82,6 +82,7 @@ typedef struct casl_handle casl_handle;
 #define CASL_ZZMAX 5
 #define CASL_UUMAX 6
 #define CASL_QJUMP 7
+#define CASL_NODESTEPS 8  /* sum over casl_step passes of the node count advanced */
 
 /* ---- lifetime ------------------------------------------------------------ */
 /* init_spectral + init_contours (spectral.f90:42-158, contours.f90:48-132):
@@ -162,6 +163,22 @@ int casl_step(casl_handle *h, int nsteps);
  * (evolution.f90:612-644), out[2] integral of (q - beta y)^2 (generic.f90:48),
  * out[3] contour circulation qjump * sum of signed contour areas. */
 int casl_diagnostics(casl_handle *h, double out[4]);
+
+/* ---- benchmarking hooks (no counterpart in the reference) ---------------- */
+/* The cudaStream_t (as void*) on which all of the handle's work is ordered,
+ * so a caller can bracket work with its own CUDA events. */
+int casl_get_stream(casl_handle *h, void **stream);
+/* Kernel launches issued by this library in this process so far. */
+int casl_launch_count(long long *count);
+/* Kernel-class timing: while a class is selected, each launch of that class
+ * is bracketed by CUDA events on the handle's stream; casl_profile_read
+ * returns the summed device time, the number of launches and their
+ * algorithmic bytes (each input read once, each output written once), then
+ * resets the tally.  Classes: */
+#define CASL_PROF_OFF 0
+#define CASL_PROF_FFT 1   /* the batched real-FFT passes (ptospc/spctop halves) */
+int casl_profile(casl_handle *h, int kernel_class);
+int casl_profile_read(casl_handle *h, double *total_ms, long long *launches, double *bytes);
 
 #ifdef __cplusplus
 }

@@ -1564,11 +1564,68 @@ static int ugrid2con(o_state *s, ugrid *g) {
     }
   int levbeg = f_int((qoff + qamin) * qjumpi + F12) + 1;
   int levend = f_int((qoff + qamax) * qjumpi + F12);
+  /* One pass over every grid-line edge in the reference's numbering order
+   * (x lines: ix outer, iy inner; then y lines: iy outer, ix inner;
+   * congen.f90:200-254), bucketing each crossing by level.  Each level's
+   * bucket then lists exactly the crossings, in exactly the order, that the
+   * reference's per-level scan of the whole grid finds; only the work of
+   * rescanning the grid for every level is saved. */
+  const long long NE = (long long)nxu * nyu;
+  int nlv = levend >= levbeg ? levend - levbeg + 1 : 0;
+  long long *lstart = xcalloc((size_t)nlv + 2, sizeof(long long));
+  long long *ledge = NULL;
+#define EDGE_VALUES(e, a, b)                                                      \
+  do {                                                                            \
+    if ((e) < NE) {                                                               \
+      int ix_ = (int)((e) / nyu) + 1, iy_ = (int)((e) % nyu) + 1;                 \
+      a = UQA(g, iy_, ix_);                                                       \
+      b = UQA(g, iy_ == nyu ? 1 : iy_ + 1, ix_);                                  \
+    } else {                                                                      \
+      long long f_ = (e) - NE;                                                    \
+      int iy_ = (int)(f_ / nxu) + 1, ix_ = (int)(f_ % nxu) + 1;                   \
+      a = UQA(g, iy_, ix_);                                                       \
+      b = UQA(g, iy_, ix_ == nxu ? 1 : ix_ + 1);                                  \
+    }                                                                             \
+  } while (0)
+  /* levels l with lo < qtmp(l) <= hi: sign(qa - qtmp) differs at the ends */
+#define QTMP(l) (((double)(l)-F12) * qjump - qoff)
+#define LEVEL_RANGE(a, b, l1, l2)                                                 \
+  do {                                                                            \
+    double lo_ = (a) < (b) ? (a) : (b), hi_ = (a) < (b) ? (b) : (a);              \
+    l1 = (int)floor((lo_ + qoff) * qjumpi + F12) - 1;                             \
+    l2 = (int)floor((hi_ + qoff) * qjumpi + F12) + 2;                             \
+    if (l1 < levbeg) l1 = levbeg;                                                 \
+    if (l2 > levend) l2 = levend;                                                 \
+    while (l1 <= l2 && !(QTMP(l1) > lo_)) l1++;                                   \
+    while (l2 >= l1 && !(QTMP(l2) <= hi_)) l2--;                                  \
+  } while (0)
+  if (nlv > 0) {
+    for (long long e = 0; e < 2 * NE; e++) {
+      double a, b;
+      int l1, l2;
+      EDGE_VALUES(e, a, b);
+      if (a == b) continue;
+      LEVEL_RANGE(a, b, l1, l2);
+      for (int l = l1; l <= l2; l++) lstart[l - levbeg + 1]++;
+    }
+    for (int l = 0; l < nlv; l++) lstart[l + 1] += lstart[l];
+    ledge = xcalloc((size_t)lstart[nlv] + 1, sizeof(long long));
+    long long *cur = xcalloc((size_t)nlv + 1, sizeof(long long));
+    for (long long e = 0; e < 2 * NE; e++) {
+      double a, b;
+      int l1, l2;
+      EDGE_VALUES(e, a, b);
+      if (a == b) continue;
+      LEVEL_RANGE(a, b, l1, l2);
+      for (int l = l1; l <= l2; l++) ledge[lstart[l - levbeg] + cur[l - levbeg]++] = e;
+    }
+    free(cur);
+  }
   for (int lev = levbeg; lev <= levend && !err; lev++) {
     int levt = lev - nlevm + (lev - 1) / nlevm - 1;
     long ncr = 0;
     double qtmp = ((double)lev - F12) * qjump - qoff;
-    memset(noctab, 0, (size_t)nxny + 1);
+    long long b0 = lstart[lev - levbeg], b1 = lstart[lev - levbeg + 1];
 #define ADDCR()                                                           \
   do {                                                                    \
     if ((size_t)ncr + 1 > crcap) {                                        \
@@ -1580,49 +1637,38 @@ static int ugrid2con(o_state *s, ugrid *g) {
     }                                                                     \
     ncr = ncr + 1;                                                        \
   } while (0)
-    for (int ix = 1; ix <= nxu; ix++) {
-      double xgt = s->xgu[ix];
-      for (int iy = 1; iy <= nyu; iy++) {
-        qdy[iy] = UQA(g, iy, ix) - qtmp;
-        isy[iy] = (int)f_sign1(qdy[iy]);
-      }
-      qdy[nyu + 1] = qdy[1];
-      isy[nyu + 1] = isy[1];
-      for (int iy = 1; iy <= nyu; iy++) {
-        if (isy[iy] != isy[iy + 1]) {
-          ADDCR();
-          int inc = (1 - isy[iy]) / 2;
-          long long kaa = (long long)(iy - 1) * nxu + 1;
-          kib[ncr] = kaa + s->ibx[ix + inc];
-          long long kob = kaa + s->ibx[ix + 1 - inc];
-          noctab[kob] = noctab[kob] + 1;
-          ICR(kob, noctab[kob]) = (int)ncr;
-          xcr[ncr] = xgt;
-          double yy = s->ygu[iy] - glyu * qdy[iy] / (qdy[iy + 1] - qdy[iy]);
-          ycr[ncr] = oms * (yy - elly * f_dint(yy * hlyi));
-        }
-      }
-    }
-    for (int iy = 1; iy <= nyu; iy++) {
-      double ygt = s->ygu[iy];
-      for (int ix = 1; ix <= nxu; ix++) {
-        qdx[ix] = UQA(g, iy, ix) - qtmp;
-        isx[ix] = (int)f_sign1(qdx[ix]);
-      }
-      qdx[nxu + 1] = qdx[1];
-      isx[nxu + 1] = isx[1];
-      for (int ix = 1; ix <= nxu; ix++) {
-        if (isx[ix] != isx[ix + 1]) {
-          ADDCR();
-          int inc = (1 - isx[ix]) / 2;
-          kib[ncr] = (long long)nxu * s->iby[iy + 1 - inc] + ix;
-          long long kob = (long long)nxu * s->iby[iy + inc] + ix;
-          noctab[kob] = noctab[kob] + 1;
-          ICR(kob, noctab[kob]) = (int)ncr;
-          ycr[ncr] = ygt;
-          double xx = s->xgu[ix] - glxu * qdx[ix] / (qdx[ix + 1] - qdx[ix]);
-          xcr[ncr] = oms * (xx - ellx * f_dint(xx * hlxi));
-        }
+    for (long long q = b0; q < b1; q++) {
+      long long e = ledge[q];
+      if (e < NE) {
+        int ix = (int)(e / nyu) + 1, iy = (int)(e % nyu) + 1;
+        double qd0 = UQA(g, iy, ix) - qtmp;
+        double qd1 = UQA(g, iy == nyu ? 1 : iy + 1, ix) - qtmp;
+        int is0 = (int)f_sign1(qd0);
+        ADDCR();
+        int inc = (1 - is0) / 2;
+        long long kaa = (long long)(iy - 1) * nxu + 1;
+        kib[ncr] = kaa + s->ibx[ix + inc];
+        long long kob = kaa + s->ibx[ix + 1 - inc];
+        noctab[kob] = noctab[kob] + 1;
+        ICR(kob, noctab[kob]) = (int)ncr;
+        xcr[ncr] = s->xgu[ix];
+        double yy = s->ygu[iy] - glyu * qd0 / (qd1 - qd0);
+        ycr[ncr] = oms * (yy - elly * f_dint(yy * hlyi));
+      } else {
+        long long f = e - NE;
+        int iy = (int)(f / nxu) + 1, ix = (int)(f % nxu) + 1;
+        double qd0 = UQA(g, iy, ix) - qtmp;
+        double qd1 = UQA(g, iy, ix == nxu ? 1 : ix + 1) - qtmp;
+        int is0 = (int)f_sign1(qd0);
+        ADDCR();
+        int inc = (1 - is0) / 2;
+        kib[ncr] = (long long)nxu * s->iby[iy + 1 - inc] + ix;
+        long long kob = (long long)nxu * s->iby[iy + inc] + ix;
+        noctab[kob] = noctab[kob] + 1;
+        ICR(kob, noctab[kob]) = (int)ncr;
+        ycr[ncr] = s->ygu[iy];
+        double xx = s->xgu[ix] - glxu * qd0 / (qd1 - qd0);
+        xcr[ncr] = oms * (xx - ellx * f_dint(xx * hlxi));
       }
     }
 #undef ADDCR
@@ -1680,7 +1726,16 @@ static int ugrid2con(o_state *s, ugrid *g) {
       }
       freec[icr] = 0;
     }
+    /* clear this level's box counts (the reference clears every box): each
+     * box holding an out-crossing is also entered by one, so clearing the
+     * boxes entered clears them all */
+    for (long icr = 1; icr <= ncr; icr++) noctab[kib[icr]] = 0;
   }
+  free(lstart);
+  free(ledge);
+#undef EDGE_VALUES
+#undef QTMP
+#undef LEVEL_RANGE
 #undef ICR
   for (int i = 1; i <= npta; i++) {
     s->xq[i] = xa[i];
