@@ -80,6 +80,8 @@ SIGNATURES = {
     "casl_initialise": (C.c_int, [C.c_void_p, _dp]),
     "casl_step": (C.c_int, [C.c_void_p, C.c_int]),
     "casl_diagnostics": (C.c_int, [C.c_void_p, _dp]),
+    "casl_con2grid_noalloc": (C.c_int, [C.c_int, C.c_double, C.c_double, C.c_int, C.c_double,
+                                         C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "casl_get_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "casl_launch_count": (C.c_int, [C.POINTER(C.c_longlong)]),
     "casl_profile": (C.c_int, [C.c_void_p, C.c_int]),

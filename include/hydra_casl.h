@@ -164,6 +164,27 @@ int casl_step(casl_handle *h, int nsteps);
  * out[3] contour circulation qjump * sum of signed contour areas. */
 int casl_diagnostics(casl_handle *h, double out[4]);
 
+/* ---- con2grid without device allocation ---------------------------------- */
+/* No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * -- their GPU memory is handed out by their own pool or another framework,
+ * they must not hit cudaMalloc's implicit device synchronisation inside a
+ * time-critical loop, or they hold no casl handle -- this runs con2grid
+ * (contours.f90:173-346, beta = 0) on device arrays the caller owns:
+ * xq_dev, yq_dev (nptq doubles), nextq_dev (nptq ints, 1-based successors as
+ * in the reference) and qc_dev (n*n doubles, Fortran (ny,nx) order).  It
+ * allocates nothing: its scratch is one fixed file-scope device array of
+ * 4.3 MB, so n is limited to 32..256 (a power of two; larger n returns
+ * CASL_EINVAL), and every GPU that loads the library holds that array until
+ * the process exits.  The first call on a device looks the array's address
+ * up (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls on a device share the array and it keeps the last call's
+ * contents (the call clears what must start at zero), so calls that overlap
+ * on the GPU (e.g. on two streams at once) race.  `stream` is a cudaStream_t
+ * (NULL = default stream); the call synchronises it before returning. */
+int casl_con2grid_noalloc(int n, double ellx, double elly, int nptq, double qjump,
+                          const double *xq_dev, const double *yq_dev, const int *nextq_dev,
+                          double *qc_dev, void *stream);
+
 /* ---- benchmarking hooks (no counterpart in the reference) ---------------- */
 /* The cudaStream_t (as void*) on which all of the handle's work is ordered,
  * so a caller can bracket work with its own CUDA events. */
