@@ -13,6 +13,7 @@
 
 #include "common.cuh"
 #include "fft.cuh"
+#include "scan.cuh"
 #include "state.cuh"
 
 using namespace casl;
@@ -993,6 +994,76 @@ int ensure_scratch2(casl_handle *h, size_t bytes) {
 }
 }  // namespace casl
 
+// ---------------------------------------------------------------------------
+// Diagnostics kernels (deterministic two-level sums)
+// ---------------------------------------------------------------------------
+__global__ void k_diag_sumsq2(const double *__restrict__ a, const double *__restrict__ b,
+                              double *__restrict__ part, long long nn) {
+  double s = 0.0;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nn;
+       k += (long long)gridDim.x * blockDim.x) {
+    double v = a[k] * a[k];
+    if (b) v = v + b[k] * b[k];
+    s += v;
+  }
+  __shared__ double sh[256];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+__global__ void k_diag_final(const double *__restrict__ part, int np, double *__restrict__ out) {
+  __shared__ double sh[256];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < np; i += blockDim.x) s += part[i];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = sh[0];
+}
+__global__ void k_diag_incr(const double *__restrict__ xq, const double *__restrict__ yq,
+                            const int *__restrict__ nextq, int npt, double *__restrict__ dx,
+                            double *__restrict__ dy, int *__restrict__ head, Consts c) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npt; i += gridDim.x * blockDim.x) {
+    int a = nextq[i];
+    double xx = xq[a] - xq[i];
+    dx[i] = xx - c.ellx * f_dint(xx * c.hlxi);
+    double yy = yq[a] - yq[i];
+    dy[i] = yy - c.elly * f_dint(yy * c.hlyi);
+    head[i] = 0;
+  }
+}
+__global__ void k_diag_heads(const int *__restrict__ i1q, int nq, int *__restrict__ head) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nq; j += gridDim.x * blockDim.x)
+    head[i1q[j]] = 1;
+}
+// term_i = X_i dy_i - Y_i dx_i with (X_i, Y_i) the exclusive prefix of the
+// increments from the contour's first node
+__global__ void k_diag_shoelace(const double *__restrict__ dx, const double *__restrict__ dy,
+                                const double *__restrict__ X, const double *__restrict__ Y,
+                                int npt, double *__restrict__ part) {
+  double s = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npt; i += gridDim.x * blockDim.x) {
+    double xe = X[i] - dx[i], ye = Y[i] - dy[i];
+    s += xe * dy[i] - ye * dx[i];
+  }
+  __shared__ double sh[256];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+
 extern "C" {
 
 const char *casl_error_string(int code) {
@@ -1653,8 +1724,60 @@ int casl_profile_read(casl_handle *h, double *total_ms, long long *launches, dou
 
 int casl_diagnostics(casl_handle *h, double out[4]) {
   if (!h || !out) return CASL_EINVAL;
-  (void)out;
-  return CASL_EUNSUPPORTED;
+  cudaStream_t st = h->stream;
+  const long long nn = (long long)h->n * h->n;
+  // ekin = 1/2 garea sum(u^2+v^2) (evolution.f90:628-629)
+  CASL_K(k_diag_sumsq2, RED_BLOCKS, 256, 0, st)(h->uu, h->vv, h->part, nn);
+  CASL_K(k_diag_final, 1, 256, 0, st)(h->part, RED_BLOCKS, h->part + 2 * RED_BLOCKS);
+  // epot = 1/2 garea kd^2 sum(psi^2) (evolution.f90:636-640)
+  if (!h->c.btropic) {
+    int rc = spctop_dev(h, h->pp, h->w[5], h->w[0]);
+    if (rc) return rc;
+    CASL_K(k_diag_sumsq2, RED_BLOCKS, 256, 0, st)(h->w[5], nullptr, h->part, nn);
+    CASL_K(k_diag_final, 1, 256, 0, st)(h->part, RED_BLOCKS, h->part + 2 * RED_BLOCKS + 1);
+  }
+  // integral of (q - beta y)^2 (generic.f90:198-212 on spctop(qq))
+  int rc = spctop_dev(h, h->qq, h->w[5], h->w[0]);
+  if (rc) return rc;
+  CASL_K(k_diag_sumsq2, RED_BLOCKS, 256, 0, st)(h->w[5], nullptr, h->part, nn);
+  CASL_K(k_diag_final, 1, 256, 0, st)(h->part, RED_BLOCKS, h->part + 2 * RED_BLOCKS + 2);
+  // contour circulation: qjump * sum of signed areas (shoelace on unwrapped
+  // increments along each contour)
+  double hs[3] = {0, 0, 0}, circ = 0.0;
+  int npt = h->nptq;
+  if (npt > 0) {
+    size_t need = (size_t)npt * 48 + ((size_t)16 << 20);
+    rc = ensure_scratch(h, need);
+    if (rc) return rc;
+    Arena ar{(char *)h->sx, h->sx_bytes, 0};
+    double *dx = ar.get<double>(npt), *dy = ar.get<double>(npt);
+    double *X = ar.get<double>(npt), *Y = ar.get<double>(npt);
+    int *head = ar.get<int>(npt);
+    SegPair *tmps = ar.get<SegPair>(scan_tmp_elems(npt) + 4);
+    double *cpart = ar.get<double>(RED_BLOCKS + 4);
+    if (ar.failed) return CASL_ENOMEM;
+    CASL_K(k_diag_incr, grid_for(npt), 256, 0, st)(h->xq, h->yq, h->nextq, npt, dx, dy, head, h->c);
+    CASL_K(k_diag_heads, grid_for(h->nq), 256, 0, st)(h->i1q, h->nq, head);
+    segmented_scan(st, dx, head, X, npt, tmps);
+    segmented_scan(st, dy, head, Y, npt, tmps);
+    CASL_K(k_diag_shoelace, RED_BLOCKS, 256, 0, st)(dx, dy, X, Y, npt, cpart);
+    CASL_K(k_diag_final, 1, 256, 0, st)(cpart, RED_BLOCKS, cpart + RED_BLOCKS);
+    CASL_CUDA_TRY(cudaMemcpyAsync(&circ, cpart + RED_BLOCKS, sizeof(double), cudaMemcpyDeviceToHost, st));
+  }
+  CASL_CUDA_TRY(cudaMemcpyAsync(hs, h->part + 2 * RED_BLOCKS, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CASL_CUDA_TRY(cudaStreamSynchronize(st));
+  rc = check_launch(h);
+  if (rc) return rc;
+  out[0] = 0.5 * h->c.garea * hs[0];
+  out[1] = h->c.btropic ? 0.0 : 0.5 * h->c.garea * h->c.kdsq * hs[1];
+  out[2] = h->c.garea * hs[2];
+  out[3] = h->hscal->qjump * (0.5 * circ);
+  if (npt > 0) {
+    rc = get_scalars(h);
+    if (rc) return rc;
+    out[3] = h->hscal->qjump * (0.5 * circ);
+  }
+  return CASL_OK;
 }
 
 }  // extern "C"

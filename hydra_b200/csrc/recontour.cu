@@ -215,11 +215,24 @@ __device__ __forceinline__ void edge_values(const double *__restrict__ qa, long 
 
 constexpr int EDGES_PER_THREAD = 16;
 
+
+// Chunk of 16 consecutive edges (in the reference's numbering) handled by
+// thread t.  x-line chunks go in order; y-line chunks are remapped so that
+// neighbouring threads take neighbouring rows iy and read qa coalesced.
+__device__ __forceinline__ long long chunk_of_thread(long long t, int nxu, int nyu) {
+  const long long ncx = (long long)nxu * nyu / EDGES_PER_THREAD;
+  if (t < ncx) return t;
+  long long u = t - ncx;
+  long long iy = u % nyu, ixb = u / nyu;
+  return ncx + iy * (nxu / EDGES_PER_THREAD) + ixb;
+}
+
 __global__ void k_cr_count(const double *__restrict__ qa, LevInfo li, int nxu, int nyu,
                            long long nchunks, int *__restrict__ cnt) {
   const long long NE2 = 2LL * nxu * nyu;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nchunks;
-       t += (long long)gridDim.x * blockDim.x) {
+  for (long long tt = blockIdx.x * (long long)blockDim.x + threadIdx.x; tt < nchunks;
+       tt += (long long)gridDim.x * blockDim.x) {
+    const long long t = chunk_of_thread(tt, nxu, nyu);
     int s = 0;
     for (int q = 0; q < EDGES_PER_THREAD; q++) {
       long long e = t * EDGES_PER_THREAD + q;
@@ -239,8 +252,9 @@ __global__ void k_cr_emit(const double *__restrict__ qa, LevInfo li, int nxu, in
                           long long nchunks, const int *__restrict__ off,
                           unsigned long long *__restrict__ redge, int *__restrict__ rlev) {
   const long long NE2 = 2LL * nxu * nyu;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nchunks;
-       t += (long long)gridDim.x * blockDim.x) {
+  for (long long tt = blockIdx.x * (long long)blockDim.x + threadIdx.x; tt < nchunks;
+       tt += (long long)gridDim.x * blockDim.x) {
+    const long long t = chunk_of_thread(tt, nxu, nyu);
     int o = off[t];
     for (int q = 0; q < EDGES_PER_THREAD; q++) {
       long long e = t * EDGES_PER_THREAD + q;
@@ -542,6 +556,53 @@ __global__ void k_out_links(const int *__restrict__ ocs, const int *__restrict__
   }
 }
 
+
+// --- small device helpers for the saddle bookkeeping ------------------------
+__global__ void k_sd_endflag(const int *__restrict__ succ, long long ncr, int *__restrict__ flag) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
+       r += (long long)gridDim.x * blockDim.x)
+    flag[r] = succ[r] < 0;
+}
+__global__ void k_sd_compact(const int *__restrict__ flag, const int *__restrict__ pos,
+                             const long long *__restrict__ sadslot, long long ncr,
+                             int *__restrict__ oidx, long long *__restrict__ oslot) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
+       r += (long long)gridDim.x * blockDim.x)
+    if (flag[r]) {
+      oidx[pos[r]] = (int)r;
+      oslot[pos[r]] = sadslot[r];
+    }
+}
+__global__ void k_gather_i(const int *__restrict__ src, const int *__restrict__ idx, int m,
+                           int *__restrict__ dst) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x)
+    dst[k] = src[idx[k]];
+}
+__global__ void k_gather_slots(const int *__restrict__ slots, const long long *__restrict__ sadp,
+                               int nsb, int *__restrict__ out) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nsb; b += gridDim.x * blockDim.x) {
+    out[2 * b] = slots[2 * sadp[b]];
+    out[2 * b + 1] = slots[2 * sadp[b] + 1];
+  }
+}
+__global__ void k_ct_len(const int *__restrict__ startf, const int *__restrict__ clenr,
+                         const int *__restrict__ cidx, long long ncr, int *__restrict__ clen) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
+       r += (long long)gridDim.x * blockDim.x)
+    if (startf[r]) clen[cidx[r]] = clenr[r];
+}
+__global__ void k_chain_of_end(const int *__restrict__ ends, int nch, int *__restrict__ coe) {
+  for (int ch = blockIdx.x * blockDim.x + threadIdx.x; ch < nch; ch += gridDim.x * blockDim.x)
+    coe[ends[ch]] = ch;
+}
+__global__ void k_set_starts(const int *__restrict__ st_idx, const int *__restrict__ st_len, int m,
+                             int *__restrict__ startf, int *__restrict__ clenr) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
+    startf[st_idx[k]] = 1;
+    clenr[st_idx[k]] = st_len[k];
+  }
+}
+
 static inline int gsz(long long work) {
   long long g = (work + 255) / 256;
   if (g < 1) g = 1;
@@ -734,65 +795,87 @@ int recontour_dev(casl_handle *h, const double *qq) {
   RC_TRY(check_launch(h));
 
   // --- 6. saddle chains: exact simulation of the reference traversal ----------
-  // chain starts are the out-crossings of saddle boxes
-  std::vector<long long> hsad(ncr);
-  std::vector<int> hsucc_neg;  // crossing indices entering saddles
-  {
-    std::vector<int> hsucc(ncr);
-    CASL_CUDA_TRY(cudaMemcpyAsync(hsucc.data(), succ, ncr * sizeof(int), cudaMemcpyDeviceToHost, st));
-    CASL_CUDA_TRY(cudaMemcpyAsync(hsad.data(), sadslot, ncr * sizeof(long long), cudaMemcpyDeviceToHost, st));
+  // Only the crossings entering saddle boxes and the chain starts come to the
+  // host; everything of size ncr stays on the device.
+  int *endflag = ar2.get<int>(ncr), *endpos = ar2.get<int>(ncr);
+  if (ar2.failed) return CASL_ENOMEM;
+  CASL_K(k_sd_endflag, g, 256, 0, st)(succ, ncr, endflag);
+  exclusive_scan<int>(st, endflag, endpos, ncr, tmpi2, dtot + 3);
+  int nends = 0;
+  CASL_CUDA_TRY(cudaMemcpyAsync(&nends, dtot + 3, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CASL_CUDA_TRY(cudaStreamSynchronize(st));
+  // gather src[idx[k]] for a host index list
+  int *gidx = nullptr, *gout = nullptr;
+  long long gcap = 0;
+  auto gather = [&](const int *src, const std::vector<int> &idx, std::vector<int> &out) -> int {
+    int m = (int)idx.size();
+    out.assign(m, 0);
+    if (m == 0) return CASL_OK;
+    if (m > gcap) {
+      gidx = ar2.get<int>(m);
+      gout = ar2.get<int>(m);
+      gcap = m;
+      if (ar2.failed) return CASL_ENOMEM;
+    }
+    CASL_CUDA_TRY(cudaMemcpyAsync(gidx, idx.data(), m * sizeof(int), cudaMemcpyHostToDevice, st));
+    CASL_K(k_gather_i, gsz(m), 256, 0, st)(src, gidx, m, gout);
+    CASL_CUDA_TRY(cudaMemcpyAsync(out.data(), gout, m * sizeof(int), cudaMemcpyDeviceToHost, st));
     CASL_CUDA_TRY(cudaStreamSynchronize(st));
-    for (long long r = 0; r < ncr; r++)
-      if (hsucc[r] < 0) hsucc_neg.push_back((int)r);
-  }
-  const int nends = (int)hsucc_neg.size();
+    return CASL_OK;
+  };
   int nsad_contours = 0;
   std::vector<int> sad_start;      // start crossing of each saddle contour
   std::vector<int> sad_len;        // its length
   std::vector<int> ch_end, ch_len, ch_rot, ch_clen, ch_cont;
   std::vector<long long> ch_pos;   // position relative to the contour start (set later)
   if (nends > 0) {
-    // gather per-saddle slots and per-chain data on the host (few entries)
-    std::vector<long long> sad_p;
-    for (int r : hsucc_neg) sad_p.push_back(hsad[r]);
+    int *d_eidx = ar2.get<int>(nends);
+    long long *d_eslot = ar2.get<long long>(nends);
+    if (ar2.failed) return CASL_ENOMEM;
+    CASL_K(k_sd_compact, g, 256, 0, st)(endflag, endpos, sadslot, ncr, d_eidx, d_eslot);
+    std::vector<int> eidx(nends);
+    std::vector<long long> eslot(nends);
+    CASL_CUDA_TRY(cudaMemcpyAsync(eidx.data(), d_eidx, nends * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CASL_CUDA_TRY(cudaMemcpyAsync(eslot.data(), d_eslot, nends * sizeof(long long), cudaMemcpyDeviceToHost, st));
+    CASL_CUDA_TRY(cudaStreamSynchronize(st));
+    std::vector<long long> sad_p(eslot);
     std::sort(sad_p.begin(), sad_p.end());
     sad_p.erase(std::unique(sad_p.begin(), sad_p.end()), sad_p.end());
     int nsb = (int)sad_p.size();
     std::vector<int> slot2(2 * nsb);
-    for (int b = 0; b < nsb; b++)
-      CASL_CUDA_TRY(cudaMemcpyAsync(&slot2[2 * b], slots + 2 * sad_p[b], 2 * sizeof(int),
-                                    cudaMemcpyDeviceToHost, st));
-    // chain starts and their ends, lengths, minima
+    {
+      long long *d_sadp = ar2.get<long long>(nsb);
+      int *d_slot2 = ar2.get<int>(2 * nsb);
+      if (ar2.failed) return CASL_ENOMEM;
+      CASL_CUDA_TRY(cudaMemcpyAsync(d_sadp, sad_p.data(), nsb * sizeof(long long), cudaMemcpyHostToDevice, st));
+      CASL_K(k_gather_slots, gsz(nsb), 256, 0, st)(slots, d_sadp, nsb, d_slot2);
+      CASL_CUDA_TRY(cudaMemcpyAsync(slot2.data(), d_slot2, 2 * nsb * sizeof(int), cudaMemcpyDeviceToHost, st));
+      CASL_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    // chain starts (the saddle out-crossings) and their ends, lengths, minima
     int nch = 2 * nsb;
-    std::vector<int> cstart(nch), cend(nch), clen(nch), cmin(nch), clev(nch);
-    std::vector<int> h_ep(ncr), h_val(ncr), h_lab(ncr), h_lev(ncr);
-    CASL_CUDA_TRY(cudaMemcpyAsync(h_ep.data(), ep, ncr * sizeof(int), cudaMemcpyDeviceToHost, st));
-    CASL_CUDA_TRY(cudaMemcpyAsync(h_val.data(), val, ncr * sizeof(int), cudaMemcpyDeviceToHost, st));
-    CASL_CUDA_TRY(cudaMemcpyAsync(h_lab.data(), lab, ncr * sizeof(int), cudaMemcpyDeviceToHost, st));
-    CASL_CUDA_TRY(cudaMemcpyAsync(h_lev.data(), rlev, ncr * sizeof(int), cudaMemcpyDeviceToHost, st));
-    CASL_CUDA_TRY(cudaStreamSynchronize(st));
+    std::vector<int> cstart(slot2), cend, clen, cmin;
+    RC_TRY(gather(ep, cstart, cend));
+    RC_TRY(gather(val, cstart, clen));
+    RC_TRY(gather(lab, cstart, cmin));
+    std::vector<int> val_at_min;
+    RC_TRY(gather(val, cmin, val_at_min));
     std::vector<std::pair<int, int>> start2ch;
-    for (int b = 0; b < nsb; b++)
-      for (int q = 0; q < 2; q++) {
-        int ch = 2 * b + q;
-        int s = slot2[2 * b + q];
-        cstart[ch] = s;
-        cend[ch] = h_ep[s];
-        clen[ch] = h_val[s];
-        cmin[ch] = h_lab[s];
-        clev[ch] = h_lev[s];
-        start2ch.push_back({s, ch});
-      }
+    for (int ch = 0; ch < nch; ch++) start2ch.push_back({cstart[ch], ch});
     std::sort(start2ch.begin(), start2ch.end());
     auto chain_starting_at = [&](int s) -> int {
       auto it = std::lower_bound(start2ch.begin(), start2ch.end(), std::make_pair(s, -1));
       return (it != start2ch.end() && it->first == s) ? it->second : -1;
     };
     // saddle box entered by each chain end
+    std::vector<std::pair<int, long long>> end_slot(nends);
+    for (int k = 0; k < nends; k++) end_slot[k] = {eidx[k], eslot[k]};
+    std::sort(end_slot.begin(), end_slot.end());
     std::vector<int> box_of_end(nch);
     for (int ch = 0; ch < nch; ch++) {
-      long long p = hsad[cend[ch]];
-      box_of_end[ch] = (int)(std::lower_bound(sad_p.begin(), sad_p.end(), p) - sad_p.begin());
+      auto it = std::lower_bound(end_slot.begin(), end_slot.end(), std::make_pair(cend[ch], -1LL));
+      if (it == end_slot.end() || it->first != cend[ch]) return CASL_EINVAL;
+      box_of_end[ch] = (int)(std::lower_bound(sad_p.begin(), sad_p.end(), it->second) - sad_p.begin());
     }
     std::vector<int> noc(nsb, 2);
     std::vector<char> used(nch, 0);
@@ -837,7 +920,7 @@ int recontour_dev(casl_handle *h, const double *qq) {
       sad_start.push_back(icr);
       sad_len.push_back(L);
       int first = seq[0];
-      int rot = clen[first] - h_val[icr];  // local index of icr in its chain
+      int rot = clen[first] - val_at_min[oc];  // local index of icr in its chain
       ch_rot[first] = rot;
       ch_clen[first] = clen[first];
       ch_cont[first] = cont;
@@ -855,10 +938,12 @@ int recontour_dev(casl_handle *h, const double *qq) {
   int *startf = ar2.get<int>(ncr), *clenr = ar2.get<int>(ncr), *cidx = ar2.get<int>(ncr);
   if (ar2.failed) return CASL_ENOMEM;
   CASL_K(k_ct_plain, g, 256, 0, st)(lab, term, val, ncr, startf, clenr);
-  for (int k = 0; k < nsad_contours; k++) {
-    int one = 1;
-    CASL_CUDA_TRY(cudaMemcpyAsync(startf + sad_start[k], &one, sizeof(int), cudaMemcpyHostToDevice, st));
-    CASL_CUDA_TRY(cudaMemcpyAsync(clenr + sad_start[k], &sad_len[k], sizeof(int), cudaMemcpyHostToDevice, st));
+  if (nsad_contours > 0) {
+    int *d_si = ar2.get<int>(nsad_contours), *d_sl = ar2.get<int>(nsad_contours);
+    if (ar2.failed) return CASL_ENOMEM;
+    CASL_CUDA_TRY(cudaMemcpyAsync(d_si, sad_start.data(), nsad_contours * sizeof(int), cudaMemcpyHostToDevice, st));
+    CASL_CUDA_TRY(cudaMemcpyAsync(d_sl, sad_len.data(), nsad_contours * sizeof(int), cudaMemcpyHostToDevice, st));
+    CASL_K(k_set_starts, gsz(nsad_contours), 256, 0, st)(d_si, d_sl, nsad_contours, startf, clenr);
   }
   exclusive_scan<int>(st, startf, cidx, ncr, tmpi2, dtot + 1);
   int C = 0;
@@ -868,53 +953,40 @@ int recontour_dev(casl_handle *h, const double *qq) {
   int *clen = ar2.get<int>(C), *coff = ar2.get<int>(C), *clevt = ar2.get<int>(C);
   double *xw = ar2.get<double>(ncr), *yw = ar2.get<double>(ncr);
   if (ar2.failed) return CASL_ENOMEM;
-  {
-    // contour lengths and offsets in contour order (host: one pass over ncr)
-    std::vector<int> h_start(ncr), h_clenr(ncr), h_cidx(ncr);
-    CASL_CUDA_TRY(cudaMemcpyAsync(h_start.data(), startf, ncr * sizeof(int), cudaMemcpyDeviceToHost, st));
-    CASL_CUDA_TRY(cudaMemcpyAsync(h_clenr.data(), clenr, ncr * sizeof(int), cudaMemcpyDeviceToHost, st));
-    CASL_CUDA_TRY(cudaMemcpyAsync(h_cidx.data(), cidx, ncr * sizeof(int), cudaMemcpyDeviceToHost, st));
-    CASL_CUDA_TRY(cudaStreamSynchronize(st));
-    std::vector<int> hl(C), ho(C);
-    for (long long r = 0; r < ncr; r++)
-      if (h_start[r]) hl[h_cidx[r]] = h_clenr[r];
-    long long acc = 0;
-    for (int k = 0; k < C; k++) {
-      ho[k] = (int)acc;
-      acc += hl[k];
+  // contour lengths in contour order, and their offsets
+  CASL_K(k_ct_len, g, 256, 0, st)(startf, clenr, cidx, ncr, clen);
+  exclusive_scan<int>(st, clen, coff, C, tmpi2, dtot + 2);
+  CASL_K(k_ct_gather_plain, g, 256, 0, st)(lab, term, val, cidx, coff, clen, xcr, ycr, ncr, xw, yw);
+  int nch = (int)ch_end.size();
+  if (nch > 0) {
+    // absolute position of every chain; the first chain of a contour is
+    // rotated to begin at the contour's first crossing, its head wrapping
+    // to the end of the contour
+    std::vector<int> sad_cidx, sad_off;
+    RC_TRY(gather(cidx, sad_start, sad_cidx));
+    RC_TRY(gather(coff, sad_cidx, sad_off));
+    std::vector<long long> abs_pos(nch);
+    std::vector<int> rotlen(nch, 0);
+    for (int ch = 0; ch < nch; ch++) {
+      int cont = ch_cont[ch];
+      if (cont < 0) return CASL_EINVAL;
+      abs_pos[ch] = sad_off[cont] + ch_pos[ch];
+      if (ch_rot[ch] >= 0) rotlen[ch] = sad_len[cont];
     }
-    if (acc != ncr) return CASL_EINVAL;
-    CASL_CUDA_TRY(cudaMemcpyAsync(clen, hl.data(), C * sizeof(int), cudaMemcpyHostToDevice, st));
-    CASL_CUDA_TRY(cudaMemcpyAsync(coff, ho.data(), C * sizeof(int), cudaMemcpyHostToDevice, st));
-    CASL_K(k_ct_gather_plain, g, 256, 0, st)(lab, term, val, cidx, coff, clen, xcr, ycr, ncr, xw, yw);
-    int nch = (int)ch_end.size();
-    if (nch > 0) {
-      // absolute position of every chain; the first chain of a contour is
-      // rotated to begin at the contour's first crossing, its head wrapping
-      // to the end of the contour
-      std::vector<long long> abs_pos(nch);
-      std::vector<int> rotlen(nch, 0);
-      std::vector<int> hcoe(ncr, -1);
-      for (int ch = 0; ch < nch; ch++) {
-        int cont = ch_cont[ch];
-        if (cont < 0) return CASL_EINVAL;
-        abs_pos[ch] = ho[h_cidx[sad_start[cont]]] + ch_pos[ch];
-        if (ch_rot[ch] >= 0) rotlen[ch] = sad_len[cont];
-        hcoe[ch_end[ch]] = ch;
-      }
-      long long *d_pos = ar2.get<long long>(nch);
-      int *d_len = ar2.get<int>(nch), *d_rot = ar2.get<int>(nch), *d_cl = ar2.get<int>(nch);
-      int *chain_of_end = ar2.get<int>(ncr);
-      if (ar2.failed) return CASL_ENOMEM;
-      CASL_CUDA_TRY(cudaMemcpyAsync(d_pos, abs_pos.data(), nch * sizeof(long long), cudaMemcpyHostToDevice, st));
-      CASL_CUDA_TRY(cudaMemcpyAsync(d_len, ch_len.data(), nch * sizeof(int), cudaMemcpyHostToDevice, st));
-      CASL_CUDA_TRY(cudaMemcpyAsync(d_rot, ch_rot.data(), nch * sizeof(int), cudaMemcpyHostToDevice, st));
-      CASL_CUDA_TRY(cudaMemcpyAsync(d_cl, rotlen.data(), nch * sizeof(int), cudaMemcpyHostToDevice, st));
-      CASL_CUDA_TRY(cudaMemcpyAsync(chain_of_end, hcoe.data(), ncr * sizeof(int), cudaMemcpyHostToDevice, st));
-      CASL_K(k_ct_gather_chain, g, 256, 0, st)(term, ep, val, chain_of_end, d_pos, d_len, d_rot, d_cl,
-                                           xcr, ycr, ncr, xw, yw);
-      CASL_CUDA_TRY(cudaStreamSynchronize(st));
-    }
+    long long *d_pos = ar2.get<long long>(nch);
+    int *d_len = ar2.get<int>(nch), *d_rot = ar2.get<int>(nch), *d_cl = ar2.get<int>(nch);
+    int *d_ends = ar2.get<int>(nch);
+    int *chain_of_end = ar2.get<int>(ncr);
+    if (ar2.failed) return CASL_ENOMEM;
+    CASL_CUDA_TRY(cudaMemcpyAsync(d_pos, abs_pos.data(), nch * sizeof(long long), cudaMemcpyHostToDevice, st));
+    CASL_CUDA_TRY(cudaMemcpyAsync(d_len, ch_len.data(), nch * sizeof(int), cudaMemcpyHostToDevice, st));
+    CASL_CUDA_TRY(cudaMemcpyAsync(d_rot, ch_rot.data(), nch * sizeof(int), cudaMemcpyHostToDevice, st));
+    CASL_CUDA_TRY(cudaMemcpyAsync(d_cl, rotlen.data(), nch * sizeof(int), cudaMemcpyHostToDevice, st));
+    CASL_CUDA_TRY(cudaMemcpyAsync(d_ends, ch_end.data(), nch * sizeof(int), cudaMemcpyHostToDevice, st));
+    CASL_CUDA_TRY(cudaMemsetAsync(chain_of_end, 0xff, ncr * sizeof(int), st));
+    CASL_K(k_chain_of_end, gsz(nch), 256, 0, st)(d_ends, nch, chain_of_end);
+    CASL_K(k_ct_gather_chain, g, 256, 0, st)(term, ep, val, chain_of_end, d_pos, d_len, d_rot, d_cl,
+                                             xcr, ycr, ncr, xw, yw);
   }
   CASL_K(k_lev_of_contour, g, 256, 0, st)(startf, rlev, cidx, ncr, li, h->p.nlevm, clevt);
   RC_TRY(check_launch(h));

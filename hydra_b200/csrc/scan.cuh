@@ -115,6 +115,37 @@ __global__ void k_scan_add(T *__restrict__ out, const T *__restrict__ tot, long 
   if (i < n) out[i] += tot[i / SCAN_TILE];
 }
 
+// One block scans a small array tile by tile (one launch instead of three).
+template <class T>
+__global__ void __launch_bounds__(SCAN_BLOCK) k_scan_small(const T *__restrict__ in,
+                                                           T *__restrict__ out, long long n,
+                                                           T *__restrict__ grand) {
+  __shared__ T tot;
+  __shared__ T carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (long long tile = 0; tile * SCAN_TILE < n; tile++) {
+    long long base = tile * SCAN_TILE + (long long)threadIdx.x * SCAN_ITEMS;
+    T v[SCAN_ITEMS];
+    T s = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; k++) {
+      v[k] = (base + k < n) ? in[base + k] : T(0);
+      s += v[k];
+    }
+    T ex = block_excl_scan<T>(s, &tot) + carry;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; k++) {
+      if (base + k < n) out[base + k] = ex;
+      ex += v[k];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) carry += tot;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0 && grand) *grand = carry;
+}
+
 // out[i] = sum_{j<i} in[j]; *grand (device, optional) = sum of all.
 // in and out may alias.  tmp needs ceil(n/SCAN_TILE) elements.
 template <class T>
@@ -122,6 +153,10 @@ int exclusive_scan(cudaStream_t st, const T *in, T *out, long long n, T *tmp, T 
   if (n <= 0) {
     if (grand) cudaMemsetAsync(grand, 0, sizeof(T), st);
     return 0;
+  }
+  if (n <= 16 * SCAN_TILE) {
+    CASL_K(k_scan_small<T>, 1, SCAN_BLOCK, 0, st)(in, out, n, grand);
+    return (int)cudaGetLastError();
   }
   int tiles = (int)((n + SCAN_TILE - 1) / SCAN_TILE);
   CASL_K(k_scan_tiles<T>, tiles, SCAN_BLOCK, 0, st)(in, out, tmp, n);

@@ -83,4 +83,9 @@ def test_driver_steps_through_recontour(oracle_mod, gpu_lib):
     same_topology(co, cg)
     close_nodes(co, cg, 1e-8)
     assert abs(g.scalar("t") - o.scalar("t")) < 1e-12
+    # energy, enstrophy and circulation track the oracle within 1e-6 relative
+    do, dg = o.diagnostics(), g.diagnostics()
+    for k in ("ekin", "enstrophy", "circulation"):
+        assert abs(dg[k] - do[k]) <= 1e-6 * abs(do[k]), (k, dg[k], do[k])
+    assert dg["epot"] == 0.0 and do["epot"] == 0.0
     g.close()
