@@ -983,6 +983,41 @@ int ensure_scratch(casl_handle *h, size_t bytes) {
   return CASL_OK;
 }
 
+void Trace::begin(cudaStream_t s, const char *what) {
+  static int enabled = -1;
+  if (enabled < 0) {
+    const char *e = getenv("CASL_TRACE");
+    enabled = e && e[0] == '1';
+  }
+  on = enabled == 1;
+  n = 0;
+  st = s;
+  if (on) point(what);
+}
+
+void Trace::point(const char *what) {
+  if (!on || n >= 64) return;
+  cudaEventCreate(&ev[n]);
+  cudaEventRecord(ev[n], st);
+  name[n++] = what;
+}
+
+void Trace::flush(const char *title) {
+  if (!on) return;
+  cudaStreamSynchronize(st);
+  fprintf(stderr, "[casl trace] %s:", title);
+  for (int i = 1; i < n; i++) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev[i - 1], ev[i]);
+    fprintf(stderr, " %s %.3f", name[i], ms);
+  }
+  float tot = 0.f;
+  if (n > 1) cudaEventElapsedTime(&tot, ev[0], ev[n - 1]);
+  fprintf(stderr, " | total %.3f ms\n", tot);
+  for (int i = 0; i < n; i++) cudaEventDestroy(ev[i]);
+  n = 0;
+}
+
 int ensure_scratch2(casl_handle *h, size_t bytes) {
   if (h->sx2_bytes >= bytes) return CASL_OK;
   if (h->sx2) cudaFree(h->sx2);
@@ -1648,6 +1683,8 @@ int casl_step(casl_handle *h, int nsteps) {
   if (!h || nsteps < 0) return CASL_EINVAL;
   int rc;
   for (int it = 0; it < nsteps; it++) {
+    // exact counts for this step's regularisation (one small copy per step)
+    if ((rc = sync_counts(h))) return rc;
     bool force = h->p.force_surgery != 0;
     bool reg = force;
     if (!force) {

@@ -167,10 +167,25 @@ __global__ void __launch_bounds__(256) k_rfft(LD ld, ST st, const double2 *__res
   const int v0 = blockIdx.x * V;
   const int b = blockIdx.y;
 
-  for (int idx = threadIdx.x; idx < V * n; idx += blockDim.x) {
-    int v, j;
-    if (LVF) { v = idx % V; j = idx / V; } else { v = idx / n; j = idx - (idx / n) * n; }
-    rA[v * ldr + j] = ld(b, v0 + v, j);
+  // Global -> shared, four independent loads in flight per thread.
+  constexpr int U = 4;
+  for (int base = threadIdx.x; base < V * n; base += U * blockDim.x) {
+    double r[U];
+    int off[U];
+#pragma unroll
+    for (int q = 0; q < U; q++) {
+      int idx = base + q * blockDim.x;
+      off[q] = -1;
+      if (idx < V * n) {
+        int v, j;
+        if (LVF) { v = idx % V; j = idx / V; } else { v = idx / n; j = idx - (idx / n) * n; }
+        r[q] = ld(b, v0 + v, j);
+        off[q] = v * ldr + j;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < U; q++)
+      if (off[q] >= 0) rA[off[q]] = r[q];
   }
   __syncthreads();
 

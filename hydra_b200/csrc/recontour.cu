@@ -404,67 +404,6 @@ __global__ void k_h_succ(const int *__restrict__ rlev, const unsigned int *__res
   }
 }
 
-// pointer jumping: minimum index along the path and list length to the end
-__global__ void k_pj_init(const int *__restrict__ succ, long long ncr, int *__restrict__ nx,
-                          int *__restrict__ lab, int *__restrict__ term) {
-  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
-       r += (long long)gridDim.x * blockDim.x) {
-    int s = succ[r];
-    nx[r] = s < 0 ? (int)r : s;
-    lab[r] = (int)r;
-    term[r] = s < 0;
-  }
-}
-
-__global__ void k_pj_min(const int *__restrict__ nx, const int *__restrict__ lab,
-                         const int *__restrict__ term, long long ncr, int *__restrict__ nx2,
-                         int *__restrict__ lab2, int *__restrict__ term2) {
-  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
-       r += (long long)gridDim.x * blockDim.x) {
-    int n = nx[r];
-    lab2[r] = min(lab[r], lab[n]);
-    term2[r] = term[r] | term[n];
-    nx2[r] = nx[n];
-  }
-}
-
-// list for ranking: cycles cut before their minimum, chains end at their end
-__global__ void k_pj_listinit(const int *__restrict__ succ, const int *__restrict__ lab,
-                              const int *__restrict__ term, long long ncr, int *__restrict__ nx,
-                              int *__restrict__ val) {
-  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
-       r += (long long)gridDim.x * blockDim.x) {
-    int s = succ[r];
-    if (term[r])
-      nx[r] = s;
-    else
-      nx[r] = (s == lab[r]) ? -1 : s;
-    val[r] = 1;
-  }
-}
-
-__global__ void k_pj_rank(const int *__restrict__ nx, const int *__restrict__ val, long long ncr,
-                          int *__restrict__ nx2, int *__restrict__ val2) {
-  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
-       r += (long long)gridDim.x * blockDim.x) {
-    int n = nx[r];
-    val2[r] = val[r] + (n >= 0 ? val[n] : 0);
-    nx2[r] = n >= 0 ? nx[n] : -1;
-  }
-}
-
-// chain end of each chain crossing (endp) via a second jump over succ
-__global__ void k_pj_endinit(const int *__restrict__ succ, long long ncr, int *__restrict__ ep) {
-  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
-       r += (long long)gridDim.x * blockDim.x)
-    ep[r] = succ[r] < 0 ? (int)r : succ[r];
-}
-__global__ void k_pj_end(const int *__restrict__ ep, long long ncr, int *__restrict__ ep2) {
-  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
-       r += (long long)gridDim.x * blockDim.x)
-    ep2[r] = ep[ep[r]];
-}
-
 // contour start flags and lengths for plain cycles (start = cycle minimum)
 __global__ void k_ct_plain(const int *__restrict__ lab, const int *__restrict__ term,
                            const int *__restrict__ val, long long ncr, int *__restrict__ startf,
@@ -557,6 +496,159 @@ __global__ void k_out_links(const int *__restrict__ ocs, const int *__restrict__
 }
 
 
+// ---------------------------------------------------------------------------
+// List ranking of the crossing successor graph with splitters.
+// Splitters: every K-th crossing and every chain start (a crossing no one
+// points to); each walks its segment up to the next splitter.  Cycles that
+// hold no sampled crossing get every crossing as a splitter in a second
+// round.  Pointer jumping then runs on the (few) splitters only, and the
+// result expands back to: term (on a chain), lab (cycle minimum / chain
+// minimum at chain starts), val (cycles: crossings from here to the end of
+// the walk that starts at the cycle minimum; chains: to the chain end,
+// inclusive) and ep (chain end).
+// ---------------------------------------------------------------------------
+__global__ void k_sp_pred(const int *__restrict__ succ, long long N, int *__restrict__ pred) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < N;
+       r += (long long)gridDim.x * blockDim.x) {
+    int s = succ[r];
+    if (s >= 0) pred[s] = (int)r;
+  }
+}
+__global__ void k_sp_flag(const int *__restrict__ pred, long long N, int K, int *__restrict__ isspl,
+                          int *__restrict__ owner) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < N;
+       r += (long long)gridDim.x * blockDim.x) {
+    isspl[r] = (r % K == 0) || pred[r] < 0;
+    owner[r] = -1;
+  }
+}
+__global__ void k_sp_walk(const int *__restrict__ succ, const int *__restrict__ isspl, long long N,
+                          int *__restrict__ owner, int *__restrict__ off, int *__restrict__ nexts_c,
+                          int *__restrict__ seglen_c, int *__restrict__ segmin_c,
+                          int *__restrict__ segend_c, int *__restrict__ err) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < N;
+       r += (long long)gridDim.x * blockDim.x) {
+    if (!isspl[r] || owner[r] >= 0) continue;
+    int s = (int)r, v = s, k = 0, mn = s, nx = -1;
+    owner[s] = s;
+    off[s] = 0;
+    for (long long guard = 0; guard < N; guard++) {
+      int n = succ[v];
+      if (n < 0) { nx = -1; break; }
+      if (isspl[n]) { nx = n; break; }
+      v = n;
+      k++;
+      owner[v] = s;
+      off[v] = k;
+      mn = min(mn, v);
+      if (guard == N - 1) atomicExch(err, CASL_EINVAL);
+    }
+    nexts_c[s] = nx;
+    seglen_c[s] = k + 1;
+    segmin_c[s] = mn;
+    segend_c[s] = v;
+  }
+}
+__global__ void k_sp_unowned(long long N, const int *__restrict__ owner, int *__restrict__ isspl) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < N;
+       r += (long long)gridDim.x * blockDim.x)
+    if (owner[r] < 0) isspl[r] = 1;
+}
+__global__ void k_sp_compact(const int *__restrict__ isspl, const int *__restrict__ srank, long long N,
+                             const int *__restrict__ nexts_c, const int *__restrict__ seglen_c,
+                             const int *__restrict__ segmin_c, const int *__restrict__ segend_c,
+                             int *__restrict__ nexts, int *__restrict__ seglen,
+                             int *__restrict__ segmin, int *__restrict__ segend) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < N;
+       r += (long long)gridDim.x * blockDim.x) {
+    if (!isspl[r]) continue;
+    int k = srank[r];
+    int nx = nexts_c[r];
+    nexts[k] = nx < 0 ? -1 : srank[nx];
+    seglen[k] = seglen_c[r];
+    segmin[k] = segmin_c[r];
+    segend[k] = segend_c[r];
+  }
+}
+__global__ void k_sp_init(const int *__restrict__ nexts, const int *__restrict__ segmin, int S,
+                          int *__restrict__ nx, int *__restrict__ mn, int *__restrict__ tm,
+                          int *__restrict__ lastp) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < S; k += gridDim.x * blockDim.x) {
+    int n = nexts[k];
+    nx[k] = n < 0 ? k : n;
+    mn[k] = segmin[k];
+    tm[k] = n < 0;
+    lastp[k] = n < 0 ? k : n;
+  }
+}
+__global__ void k_sp_jump1(const int *__restrict__ nx, const int *__restrict__ mn,
+                           const int *__restrict__ tm, const int *__restrict__ lastp, int S,
+                           int *__restrict__ nx2, int *__restrict__ mn2, int *__restrict__ tm2,
+                           int *__restrict__ lastp2) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < S; k += gridDim.x * blockDim.x) {
+    int n = nx[k];
+    mn2[k] = min(mn[k], mn[n]);
+    tm2[k] = tm[k] | tm[n];
+    nx2[k] = nx[n];
+    lastp2[k] = lastp[lastp[k]];
+  }
+}
+// list for suffix sums: cycles are cut before the splitter holding the cycle
+// minimum; chains end at their last splitter
+__global__ void k_sp_list(const int *__restrict__ nexts, const int *__restrict__ mn,
+                          const int *__restrict__ tm, const int *__restrict__ owner,
+                          const int *__restrict__ srank, const int *__restrict__ seglen, int S,
+                          int *__restrict__ sl, long long *__restrict__ suf,
+                          int *__restrict__ head) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < S; k += gridDim.x * blockDim.x) {
+    int n = nexts[k];
+    if (tm[k]) {
+      sl[k] = n;
+      head[k] = -1;
+    } else {
+      int h = srank[owner[mn[k]]];
+      head[k] = h;
+      sl[k] = n == h ? -1 : n;
+    }
+    suf[k] = seglen[k];
+  }
+}
+__global__ void k_sp_jump2(const int *__restrict__ sl, const long long *__restrict__ suf, int S,
+                           int *__restrict__ sl2, long long *__restrict__ suf2) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < S; k += gridDim.x * blockDim.x) {
+    int n = sl[k];
+    suf2[k] = suf[k] + (n >= 0 ? suf[n] : 0);
+    sl2[k] = n >= 0 ? sl[n] : -1;
+  }
+}
+__global__ void k_sp_expand(long long N, const int *__restrict__ owner, const int *__restrict__ off,
+                            const int *__restrict__ srank, const int *__restrict__ tm,
+                            const int *__restrict__ mn, const long long *__restrict__ suf,
+                            const int *__restrict__ head, const int *__restrict__ lastp,
+                            const int *__restrict__ segend, int *__restrict__ term,
+                            int *__restrict__ lab, int *__restrict__ val, int *__restrict__ ep) {
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < N;
+       c += (long long)gridDim.x * blockDim.x) {
+    int k = srank[owner[c]];
+    int o = off[c];
+    if (tm[k]) {
+      term[c] = 1;
+      val[c] = (int)(suf[k] - o);
+      ep[c] = segend[lastp[k]];
+      lab[c] = o == 0 ? mn[k] : (int)c;
+    } else {
+      int m = mn[k];
+      long long L = suf[head[k]];
+      long long pos = (L - suf[k]) + o - off[m];
+      if (pos < 0) pos += L;
+      term[c] = 0;
+      val[c] = (int)(L - pos);
+      lab[c] = m;
+      ep[c] = (int)c;
+    }
+  }
+}
+
 // --- small device helpers for the saddle bookkeeping ------------------------
 __global__ void k_sd_endflag(const int *__restrict__ succ, long long ncr, int *__restrict__ flag) {
   for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
@@ -633,6 +725,12 @@ int recontour_dev(casl_handle *h, const double *qq) {
   const double qjump = h->qjump;
   const int have = h->nptq > 0 && h->nq > 0;
   cudaMemsetAsync(&h->scal->error, 0, sizeof(int), st);
+  Trace tr;
+  tr.begin(st, "start");
+  struct Flush {
+    Trace &t;
+    ~Flush() { t.flush("recontour"); }
+  } flush_at_exit{tr};
 
   // --- 1. ultra-fine field ---------------------------------------------------
   if (!have) {
@@ -686,6 +784,7 @@ int recontour_dev(casl_handle *h, const double *qq) {
     qamax = std::max(qamax, hp[2 * b]);
     qamin = std::min(qamin, hp[2 * b + 1]);
   }
+  tr.point("field");
   // --- 2. levels (congen.f90:156-173) ----------------------------------------
   LevInfo li;
   li.qjump = qjump;
@@ -703,6 +802,7 @@ int recontour_dev(casl_handle *h, const double *qq) {
   if (li.levbeg > li.levend) return set_empty();
   const int nlev = li.levend - li.levbeg + 1;
 
+  tr.point("levels");
   // --- 3. crossings in reference order, stably sorted by level ----------------
   const long long NE2 = 2 * NU;
   const long long nchunks = (NE2 + EDGES_PER_THREAD - 1) / EDGES_PER_THREAD;
@@ -729,7 +829,7 @@ int recontour_dev(casl_handle *h, const double *qq) {
     unsigned long long capb = 1;
     while (capb < (unsigned long long)(2 * ncr)) capb <<= 1;
     long long capn = std::max<long long>(ncr * 2, h->npm);
-    size_t need2 = (size_t)ncr * 460 + (size_t)capb * 16 + (size_t)capn * 32 + sort_bytes +
+    size_t need2 = (size_t)ncr * 600 + (size_t)capb * 16 + (size_t)capn * 32 + sort_bytes +
                    ((size_t)64 << 20);
     RC_TRY(ensure_scratch2(h, need2));
   }
@@ -750,6 +850,7 @@ int recontour_dev(casl_handle *h, const double *qq) {
   CASL_K(k_cr_geom, gsz(ncr), 256, 0, st)(qa, redge, rlev, ncr, li, c, xcr, ycr, kib, kob);
   RC_TRY(check_launch(h));
 
+  tr.point("crossings");
   // --- 4. box tables: hash (level, box) -> two out-crossing slots ------------
   unsigned long long cap = 1;
   while (cap < (unsigned long long)(2 * ncr)) cap <<= 1;
@@ -767,33 +868,58 @@ int recontour_dev(casl_handle *h, const double *qq) {
   RC_TRY(check_launch(h));
   RC_TRY(fetch_err(h));
 
-  // --- 5. pointer jumping over crossings --------------------------------------
-  int *nx = ar2.get<int>(ncr), *nx2 = ar2.get<int>(ncr), *lab = ar2.get<int>(ncr),
-      *lab2 = ar2.get<int>(ncr), *term = ar2.get<int>(ncr), *term2 = ar2.get<int>(ncr),
-      *val = ar2.get<int>(ncr), *val2 = ar2.get<int>(ncr), *ep = ar2.get<int>(ncr),
-      *ep2 = ar2.get<int>(ncr);
+  tr.point("hash");
+  // --- 5. list ranking over crossings (splitters) ------------------------------
+  int *lab = ar2.get<int>(ncr), *term = ar2.get<int>(ncr), *val = ar2.get<int>(ncr),
+      *ep = ar2.get<int>(ncr);
+  int *pred = ar2.get<int>(ncr), *isspl = ar2.get<int>(ncr), *owner = ar2.get<int>(ncr),
+      *offc = ar2.get<int>(ncr), *srank = ar2.get<int>(ncr);
+  int *nexts_c = ar2.get<int>(ncr), *seglen_c = ar2.get<int>(ncr), *segmin_c = ar2.get<int>(ncr),
+      *segend_c = ar2.get<int>(ncr);
   if (ar2.failed) return CASL_ENOMEM;
-  int rounds = 1;
-  while ((1LL << rounds) < ncr) rounds++;
-  rounds++;
   int g = gsz(ncr);
-  CASL_K(k_pj_init, g, 256, 0, st)(succ, ncr, nx, lab, term);
+  CASL_CUDA_TRY(cudaMemsetAsync(pred, 0xff, ncr * sizeof(int), st));
+  CASL_K(k_sp_pred, g, 256, 0, st)(succ, ncr, pred);
+  CASL_K(k_sp_flag, g, 256, 0, st)(pred, ncr, 32, isspl, owner);
+  CASL_K(k_sp_walk, g, 256, 0, st)(succ, isspl, ncr, owner, offc, nexts_c, seglen_c, segmin_c,
+                                   segend_c, &h->scal->error);
+  CASL_K(k_sp_unowned, g, 256, 0, st)(ncr, owner, isspl);
+  CASL_K(k_sp_walk, g, 256, 0, st)(succ, isspl, ncr, owner, offc, nexts_c, seglen_c, segmin_c,
+                                   segend_c, &h->scal->error);
+  exclusive_scan<int>(st, isspl, srank, ncr, tmpi2, dtot + 6);
+  int S = 0;
+  CASL_CUDA_TRY(cudaMemcpyAsync(&S, dtot + 6, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CASL_CUDA_TRY(cudaStreamSynchronize(st));
+  if (S <= 0) return CASL_EINVAL;
+  int *nexts = ar2.get<int>(S), *seglen = ar2.get<int>(S), *segmin = ar2.get<int>(S),
+      *segend = ar2.get<int>(S);
+  int *snx = ar2.get<int>(S), *snx2 = ar2.get<int>(S), *smn = ar2.get<int>(S),
+      *smn2 = ar2.get<int>(S), *stm = ar2.get<int>(S), *stm2 = ar2.get<int>(S),
+      *slp = ar2.get<int>(S), *slp2 = ar2.get<int>(S), *ssl = ar2.get<int>(S),
+      *ssl2 = ar2.get<int>(S), *shead = ar2.get<int>(S);
+  long long *ssuf = ar2.get<long long>(S), *ssuf2 = ar2.get<long long>(S);
+  if (ar2.failed) return CASL_ENOMEM;
+  CASL_K(k_sp_compact, g, 256, 0, st)(isspl, srank, ncr, nexts_c, seglen_c, segmin_c, segend_c,
+                                      nexts, seglen, segmin, segend);
+  int gsS = gsz(S);
+  int rounds = 1;
+  while ((1LL << rounds) < S) rounds++;
+  rounds++;
+  CASL_K(k_sp_init, gsS, 256, 0, st)(nexts, segmin, S, snx, smn, stm, slp);
   for (int it = 0; it < rounds; it++) {
-    CASL_K(k_pj_min, g, 256, 0, st)(nx, lab, term, ncr, nx2, lab2, term2);
-    std::swap(nx, nx2); std::swap(lab, lab2); std::swap(term, term2);
+    CASL_K(k_sp_jump1, gsS, 256, 0, st)(snx, smn, stm, slp, S, snx2, smn2, stm2, slp2);
+    std::swap(snx, snx2); std::swap(smn, smn2); std::swap(stm, stm2); std::swap(slp, slp2);
   }
-  CASL_K(k_pj_listinit, g, 256, 0, st)(succ, lab, term, ncr, nx, val);
+  CASL_K(k_sp_list, gsS, 256, 0, st)(nexts, smn, stm, owner, srank, seglen, S, ssl, ssuf, shead);
   for (int it = 0; it < rounds; it++) {
-    CASL_K(k_pj_rank, g, 256, 0, st)(nx, val, ncr, nx2, val2);
-    std::swap(nx, nx2); std::swap(val, val2);
+    CASL_K(k_sp_jump2, gsS, 256, 0, st)(ssl, ssuf, S, ssl2, ssuf2);
+    std::swap(ssl, ssl2); std::swap(ssuf, ssuf2);
   }
-  CASL_K(k_pj_endinit, g, 256, 0, st)(succ, ncr, ep);
-  for (int it = 0; it < rounds; it++) {
-    CASL_K(k_pj_end, g, 256, 0, st)(ep, ncr, ep2);
-    std::swap(ep, ep2);
-  }
+  CASL_K(k_sp_expand, g, 256, 0, st)(ncr, owner, offc, srank, stm, smn, ssuf, shead, slp, segend,
+                                     term, lab, val, ep);
   RC_TRY(check_launch(h));
 
+  tr.point("ranking");
   // --- 6. saddle chains: exact simulation of the reference traversal ----------
   // Only the crossings entering saddle boxes and the chain starts come to the
   // host; everything of size ncr stays on the device.
@@ -934,6 +1060,7 @@ int recontour_dev(casl_handle *h, const double *qq) {
     }
   }
 
+  tr.point("saddles");
   // --- 7. contour order and walk layout ---------------------------------------
   int *startf = ar2.get<int>(ncr), *clenr = ar2.get<int>(ncr), *cidx = ar2.get<int>(ncr);
   if (ar2.failed) return CASL_ENOMEM;
@@ -991,6 +1118,7 @@ int recontour_dev(casl_handle *h, const double *qq) {
   CASL_K(k_lev_of_contour, g, 256, 0, st)(startf, rlev, cidx, ncr, li, h->p.nlevm, clevt);
   RC_TRY(check_launch(h));
 
+  tr.point("layout");
   // --- 8. renode three times (congen.f90:295-310) -----------------------------
   RenodeIn cur{xw, yw, coff, clen, clevt, C, ncr};
   long long capn = std::max<long long>(ncr * 2, h->npm);
@@ -1018,6 +1146,7 @@ int recontour_dev(casl_handle *h, const double *qq) {
     if (hc[2]) return CASL_ECAPACITY;
     if (hc[0] == 0) return set_empty();
     cur = RenodeIn{out.xo, out.yo, out.ocs, out.olen, out.olev, hc[0], hc[1]};
+    tr.point(pass == 0 ? "renode1" : (pass == 1 ? "renode2" : "renode3"));
   }
   int nq = hc[0], npt = hc[1];
   if (npt > h->npm || nq > h->nm) return CASL_ECAPACITY;

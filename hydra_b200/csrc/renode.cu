@@ -12,8 +12,9 @@ __device__ __forceinline__ long long wprev(long long w, long long cs, long long 
   return w > cs ? w - 1 : cs + L - 1;
 }
 
-__global__ void k_rn_cid(const int *__restrict__ cs, int C, long long N, int *__restrict__ cid,
-                         int *__restrict__ head) {
+__global__ void k_rn_cid(RenodeIn in, long long N, int *__restrict__ cid, int *__restrict__ head) {
+  const int C = contours_in(in);
+  const int *cs = in.cs;
   for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < N;
        w += (long long)gridDim.x * blockDim.x) {
     int c = contour_of(cs, C, w);
@@ -127,7 +128,14 @@ __device__ __forceinline__ int nint_d(double x) { return (int)llround(x); }
 
 // Per contour: node count, pieces (contours.f90:799-809, 813-930).
 __global__ void k_rn_count(RenodeIn in, RenodeScratch s, Consts c, int mode) {
+  const int Ce = contours_in(in);
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < in.C; k += gridDim.x * blockDim.x) {
+    if (k >= Ce) {
+      s.npiece[k] = 0;
+      s.cnpr[k] = 0;
+      s.ckeep[k] = 0;
+      continue;
+    }
     long long cs = in.cs[k], L = in.len[k];
     double total = s.S[cs + L - 1];
     s.ctot[k] = total;
@@ -141,7 +149,8 @@ __global__ void k_rn_count(RenodeIn in, RenodeScratch s, Consts c, int mode) {
 }
 
 __global__ void k_rn_fill(RenodeIn in, RenodeScratch s, Consts c, int mode) {
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < in.C; k += gridDim.x * blockDim.x) {
+  const int Ce = contours_in(in);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < Ce; k += gridDim.x * blockDim.x) {
     long long cs = in.cs[k], L = in.len[k];
     int np = s.npiece[k];
     int npr = 0;
@@ -180,7 +189,9 @@ __global__ void k_rn_fill(RenodeIn in, RenodeScratch s, Consts c, int mode) {
 }
 
 __global__ void k_rn_pout(RenodeIn in, RenodeScratch s, RenodeOut out) {
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < in.C; k += gridDim.x * blockDim.x) {
+  if (out.d_counts[2]) return;  // overflow: the caller reports it
+  const int Ce = contours_in(in);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < Ce; k += gridDim.x * blockDim.x) {
     if (!s.ckeep[k]) continue;
     int base = s.cout[k];
     for (int q = 0; q < s.npiece[k]; q++) {
@@ -196,6 +207,7 @@ __global__ void k_rn_pout(RenodeIn in, RenodeScratch s, RenodeOut out) {
 }
 
 __global__ void k_rn_place(RenodeIn in, RenodeScratch s, RenodeOut out, Consts c) {
+  if (out.d_counts[2]) return;  // overflow: the caller reports it
   for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < in.N;
        w += (long long)gridDim.x * blockDim.x) {
     int k = s.cid[w];
@@ -259,7 +271,7 @@ int renode_batch(casl_handle *h, Arena &ar, const RenodeIn &in, RenodeOut &out, 
   cudaStream_t st = h->stream;
   const Consts &c = h->c;
   long long N = in.N;
-  int C = in.C;
+  int C = in.C;  // capacity when in.Cdev is set
   if (C == 0 || N == 0) {
     cudaMemsetAsync(out.d_counts, 0, 3 * sizeof(int), st);
     return CASL_OK;
@@ -280,10 +292,16 @@ int renode_batch(casl_handle *h, Arena &ar, const RenodeIn &in, RenodeOut &out, 
   s.tmpi = ar.get<int>(tmpn);
   s.tmps = ar.get<SegPair>(tmpn);
   s.d_tot = ar.get<int>(8);
+  // pieces: one per corner of a contour with >= 2 corners, else one per
+  // contour, so at most N + C
+  long long P = N + C;
+  s.pc = ar.get<int>(P); s.pstart = ar.get<int>(P); s.plen = ar.get<int>(P);
+  s.pn = ar.get<int>(P); s.pout = ar.get<int>(P);
+  s.psum = ar.get<double>(P); s.pfac = ar.get<double>(P);
   if (ar.failed) return CASL_ENOMEM;
   cudaMemsetAsync(s.ccnt, 0, C * sizeof(int), st);
   int g = gsz(N);
-  CASL_K(k_rn_cid, g, 256, 0, st)(in.cs, C, N, s.cid, s.head);
+  CASL_K(k_rn_cid, g, 256, 0, st)(in, N, s.cid, s.head);
   CASL_K(k_rn1, g, 256, 0, st)(in, s, c);
   CASL_K(k_rn2, g, 256, 0, st)(in, s, c);
   CASL_K(k_rn3, g, 256, 0, st)(in, s, c);
@@ -295,25 +313,10 @@ int renode_batch(casl_handle *h, Arena &ar, const RenodeIn &in, RenodeOut &out, 
   int gc = gsz(C);
   CASL_K(k_rn_count, gc, 256, 0, st)(in, s, c, mode);
   exclusive_scan<int>(st, s.npiece, s.poff, C, s.tmpi, s.d_tot + 1);
-  // pieces: at most one per corner, or one per contour
-  int hp = 0;
-  cudaMemcpyAsync(&hp, s.d_tot + 1, sizeof(int), cudaMemcpyDeviceToHost, st);
-  cudaError_t e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) return set_cuda_error(h, e);
-  long long P = hp > 0 ? hp : 1;
-  s.pc = ar.get<int>(P); s.pstart = ar.get<int>(P); s.plen = ar.get<int>(P);
-  s.pn = ar.get<int>(P); s.pout = ar.get<int>(P);
-  s.psum = ar.get<double>(P); s.pfac = ar.get<double>(P);
-  if (ar.failed) return CASL_ENOMEM;
   CASL_K(k_rn_fill, gc, 256, 0, st)(in, s, c, mode);
   exclusive_scan<int>(st, s.cnpr, s.cout, C, s.tmpi, s.d_tot + 2);
   exclusive_scan<int>(st, s.ckeep, s.ckidx, C, s.tmpi, s.d_tot + 3);
   CASL_K(k_rn_finish, 1, 1, 0, st)(out.d_counts, s.d_tot + 2, s.d_tot + 3, out.cap);
-  int hc[3];
-  cudaMemcpyAsync(hc, out.d_counts, 3 * sizeof(int), cudaMemcpyDeviceToHost, st);
-  e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) return set_cuda_error(h, e);
-  if (hc[2]) return CASL_ECAPACITY;
   CASL_K(k_rn_pout, gc, 256, 0, st)(in, s, out);
   CASL_K(k_rn_place, g, 256, 0, st)(in, s, out, c);
   return check_launch(h);

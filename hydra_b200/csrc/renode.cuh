@@ -23,9 +23,12 @@ struct RenodeIn {
   const double *xw, *yw;  // walk layout, N nodes
   const int *cs, *len;    // per contour
   const int *levt;        // per contour level index (copied to the output)
-  int C;                  // contours
+  int C;                  // contours (an upper bound when Cdev is given)
   long long N;            // nodes
+  const int *Cdev;        // optional: the contour count in device memory
 };
+
+__device__ __forceinline__ int contours_in(const RenodeIn &in) { return in.Cdev ? *in.Cdev : in.C; }
 
 struct RenodeOut {
   double *xo, *yo;        // output nodes (capacity cap)
@@ -60,6 +63,10 @@ struct RenodeScratch {
   long long maxpieces;
 };
 
+// Renodes every contour; issues no host synchronisation.  out.d_counts
+// receives [kept contours, kept nodes, overflow flag]; on overflow (kept
+// nodes > out.cap) nothing is written to the output arrays and the caller
+// reports CASL_ECAPACITY when it reads the counts.
 int renode_batch(casl_handle *h, Arena &ar, const RenodeIn &in, RenodeOut &out, int mode);
 
 }  // namespace casl

@@ -83,6 +83,20 @@ int renode_host(casl_handle *h, const double *xd, const double *yd, int npd, dou
                 double *yr, int cap, int *npr);
 
 int sync_counts(casl_handle *h);    // device counts -> host copies
+
+// Opt-in phase trace (environment variable CASL_TRACE=1): records CUDA
+// events at named points on the handle's stream and prints the device time
+// between consecutive points to stderr when flushed.
+struct Trace {
+  bool on = false;
+  int n = 0;
+  cudaEvent_t ev[64];
+  const char *name[64];
+  cudaStream_t st;
+  void begin(cudaStream_t s, const char *what);
+  void point(const char *what);
+  void flush(const char *title);
+};
 int ensure_scratch(casl_handle *h, size_t bytes);
 int ensure_scratch2(casl_handle *h, size_t bytes);
 

@@ -83,14 +83,78 @@ __device__ __forceinline__ int node_box(double x, double y, const LevelDesc &L, 
   return L.boxbase + L.nby * bx + by;
 }
 
+
+// --- levels (contours.f90:374-394) and box counts (contours.f90:429-454) ----
+// A new level starts where indq increases; contours arrive sorted by level.
+__global__ void k_lv_flags(const int *__restrict__ indq, int nq, int *__restrict__ flag,
+                           int *__restrict__ err) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nq; j += gridDim.x * blockDim.x) {
+    flag[j] = j == 0 || indq[j] > indq[j - 1];
+    if (j > 0 && indq[j] < indq[j - 1]) atomicExch(err, CASL_EINVAL);
+  }
+}
+
+__global__ void k_lv_desc(const int *__restrict__ i1q, const int *__restrict__ i2q,
+                          const int *__restrict__ indq, const int *__restrict__ flag,
+                          const int *__restrict__ lex, int nq, LevelDesc *__restrict__ lev) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nq; j += gridDim.x * blockDim.x) {
+    int L = lex[j] + flag[j] - 1;
+    if (flag[j]) {
+      lev[L].ibeg = i1q[j];
+      lev[L].levt = indq[j];
+    }
+    if (j == nq - 1 || flag[j + 1]) lev[L].iend = i2q[j];
+  }
+}
+
+__global__ void k_lv_boxes(LevelDesc *__restrict__ lev, const int *__restrict__ nlev_dev, int nq,
+                           int npt, Consts c, int *__restrict__ nbox_l, int *__restrict__ err) {
+  const int nlev = *nlev_dev;
+  for (int L = blockIdx.x * blockDim.x + threadIdx.x; L < nq; L += gridDim.x * blockDim.x) {
+    if (L >= nlev) {
+      nbox_l[L] = 0;
+      continue;
+    }
+    LevelDesc d = lev[L];
+    if (d.ibeg < 0 || d.iend >= npt || d.iend < d.ibeg) {
+      atomicExch(err, CASL_EINVAL);
+      nbox_l[L] = 0;
+      continue;
+    }
+    double fnq = (double)(d.iend - d.ibeg + 1);
+    double fnbx = 1.2 * sqrt(fnq * c.aspect);
+    double fnby = fnbx / c.aspect;
+    int nbx = (int)llround(fnbx);
+    nbx = max(min(nbx, c.nx), 1);
+    int nby = (int)llround(fnby);
+    nby = max(min(nby, c.ny), 1);
+    d.nbx = nbx;
+    d.nby = nby;
+    d.bwxi = c.oms * (double)nbx / c.ellx;
+    d.bwyi = c.oms * (double)nby / c.elly;
+    lev[L] = d;
+    nbox_l[L] = nbx * nby;
+  }
+}
+
+__global__ void k_lv_base(LevelDesc *__restrict__ lev, const int *__restrict__ nlev_dev,
+                          const int *__restrict__ boxbase, const int *__restrict__ nbox_dev,
+                          long long nbox_cap, int *__restrict__ err) {
+  const int nlev = *nlev_dev;
+  for (int L = blockIdx.x * blockDim.x + threadIdx.x; L < nlev; L += gridDim.x * blockDim.x)
+    lev[L].boxbase = boxbase[L];
+  if (blockIdx.x == 0 && threadIdx.x == 0 && *nbox_dev > nbox_cap) atomicExch(err, CASL_ECAPACITY);
+}
+
 __global__ void k_sg_endnext(const int *__restrict__ i1q, const int *__restrict__ i2q, int nq,
                              int *__restrict__ endnext) {
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nq; j += gridDim.x * blockDim.x)
     endnext[i2q[j]] = i1q[j];
 }
 
-__global__ void k_sg_level_of(const LevelDesc *__restrict__ lev, int nlev, int npt,
-                              int *__restrict__ lvl) {
+__global__ void k_sg_level_of(const LevelDesc *__restrict__ lev, const int *__restrict__ nlev_dev,
+                              int npt, int *__restrict__ lvl) {
+  const int nlev = *nlev_dev;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npt; i += gridDim.x * blockDim.x) {
     int lo = 0, hi = nlev - 1;
     while (lo < hi) {
@@ -143,14 +207,19 @@ __global__ void k_sg_count_entries(SurgState S, const LevelDesc *__restrict__ le
 }
 
 __global__ void k_sg_emit(SurgState S, const LevelDesc *__restrict__ lev, int npt,
-                          const int *__restrict__ eoff, int *__restrict__ ebox,
-                          int *__restrict__ eib, int *__restrict__ bcnt, Consts c) {
+                          const int *__restrict__ eoff, const int *__restrict__ ecount,
+                          long long ne_cap, int *__restrict__ ebox, int *__restrict__ eib,
+                          int *__restrict__ bcnt, Consts c, int *__restrict__ err) {
   for (int ib = blockIdx.x * blockDim.x + threadIdx.x; ib < npt; ib += gridDim.x * blockDim.x) {
     LevelDesc L = lev[S.lvl[ib]];
     int i = S.nq0[ib];
     int mbx1, mbx2, mby1, mby2;
     seg_boxes(S.x0[i], S.y0[i], S.dx0[i], S.dy0[i], L, c, mbx1, mbx2, mby1, mby2);
     int e = eoff[ib];
+    if ((long long)e + ecount[ib] > ne_cap) {
+      atomicExch(err, CASL_ECAPACITY);
+      continue;
+    }
     for (int mbx = mbx1; mbx <= mbx2; mbx++) {
       int mmbx = mbx % L.nbx;
       for (int mby = mby1; mby <= mby2; mby++) {
@@ -164,9 +233,10 @@ __global__ void k_sg_emit(SurgState S, const LevelDesc *__restrict__ lev, int np
   }
 }
 
-__global__ void k_sg_place(const int *__restrict__ ebox, const int *__restrict__ eib, long long ne,
-                           const int *__restrict__ kb1, int *__restrict__ cursor,
-                           int *__restrict__ bnode) {
+__global__ void k_sg_place(const int *__restrict__ ebox, const int *__restrict__ eib,
+                           const int *__restrict__ ne_dev, const int *__restrict__ kb1,
+                           int *__restrict__ cursor, int *__restrict__ bnode) {
+  const long long ne = *ne_dev;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ne;
        e += (long long)gridDim.x * blockDim.x) {
     int gb = ebox[e];
@@ -186,7 +256,8 @@ __global__ void k_sg_place_nodes(const int *__restrict__ nbox_of, int npt,
 
 // Restore the reference's per-box order (ascending node before the segment).
 __global__ void k_sg_sort_boxes(const int *__restrict__ kb1, const int *__restrict__ bcnt,
-                                int nbox, int *__restrict__ bnode) {
+                                const int *__restrict__ nbox_dev, int *__restrict__ bnode) {
+  const int nbox = *nbox_dev;
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nbox; b += gridDim.x * blockDim.x) {
     int s = kb1[b], n = bcnt[b];
     for (int a = 1; a < n; a++) {
@@ -237,7 +308,7 @@ __global__ void k_sg_candidates(SurgState S, const LevelDesc *__restrict__ lev, 
 }
 
 __device__ __forceinline__ void mark(SurgState &S, int x, int ib, int iend) {
-  if (x > ib && x <= iend) S.pending[x] = 1;
+  if (x > ib && x <= iend) ((volatile unsigned char *)S.pending)[x] = 1;
 }
 
 // Mark every later node whose tests may read node j's changed data.
@@ -262,11 +333,11 @@ __device__ void mark_affected(SurgState &S, const LevelDesc &L, int j, int ib, c
 }
 
 // One warp per level replays contours.f90:528-613 at pending nodes.
-__global__ void k_sg_replay(SurgState S, const LevelDesc *__restrict__ lev, int nlev, Consts c,
-                            int *nsurg) {
+__global__ void k_sg_replay(SurgState S, const LevelDesc *__restrict__ lev,
+                            const int *__restrict__ nlev_dev, Consts c, int *nsurg) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (warp >= nlev) return;
+  if (warp >= *nlev_dev) return;
   const LevelDesc L = lev[warp];
   volatile unsigned char *pend = S.pending;
   volatile double *xq = S.xq, *yq = S.yq, *dx = S.dx, *dy = S.dy, *dsq = S.dsq;
@@ -275,14 +346,37 @@ __global__ void k_sg_replay(SurgState S, const LevelDesc *__restrict__ lev, int 
   int count = 0;
   long long pos = L.ibeg;
   while (pos <= L.iend) {
-    long long idx = pos + lane;
-    bool f = idx <= L.iend && pend[idx];
-    unsigned b = __ballot_sync(0xffffffffu, f);
-    if (!b) {
-      pos += 32;
-      continue;
+    int ib;
+    if ((pos & 15) == 0 && pos + 512 <= (long long)L.iend + 1) {
+      // 512 flags per step: one 16-byte uncached load per lane
+      uint4 v = __ldcv(reinterpret_cast<const uint4 *>(S.pending + pos) + lane);
+      unsigned b = __ballot_sync(0xffffffffu, (v.x | v.y | v.z | v.w) != 0u);
+      if (!b) {
+        pos += 512;
+        continue;
+      }
+      const int f = __ffs(b) - 1;
+      int off = 0;
+      if (lane == f) {
+        unsigned w[4] = {v.x, v.y, v.z, v.w};
+        for (int q = 0; q < 4; q++)
+          if (w[q]) {
+            off = 4 * q + (__ffs(w[q]) - 1) / 8;
+            break;
+          }
+      }
+      off = __shfl_sync(0xffffffffu, off, f);
+      ib = (int)(pos + 16 * f + off);
+    } else {
+      long long idx = pos + lane;
+      bool fl = idx <= L.iend && pend[idx];
+      unsigned b = __ballot_sync(0xffffffffu, fl);
+      if (!b) {
+        pos += 32;
+        continue;
+      }
+      ib = (int)(pos + __ffs(b) - 1);
     }
-    const int ib = (int)(pos + __ffs(b) - 1);
     __syncwarp();
     int i = nextq[ib];
     double xi = xq[i], yi = yq[i];
@@ -346,8 +440,8 @@ __global__ void k_sg_replay(SurgState S, const LevelDesc *__restrict__ lev, int 
         for (int q = 0; q < 4; q++) mark_affected(S, L, touched[q], ib, c);
         inew = is;
         count++;
+        __threadfence();  // marks and moved nodes visible to the uncached reloads
       }
-      __threadfence_block();
       __syncwarp();
       i = __shfl_sync(0xffffffffu, inew, 0);
       xi = xq[i];
@@ -382,53 +476,73 @@ __global__ void k_rb_runs(const int *__restrict__ st, const int *__restrict__ br
   }
 }
 
-__global__ void k_rb_runinit(const int *__restrict__ nextq, const int *__restrict__ rid,
-                             const int *__restrict__ rs, const int *__restrict__ re, int R,
-                             int *__restrict__ nr, int *__restrict__ lab, int *__restrict__ nrj) {
-  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < R; r += gridDim.x * blockDim.x) {
+
+
+
+
+
+
+
+
+
+
+// All run-level cycle work in one block: min-label and list-ranking pointer
+// jumping over the R runs (R is small: contours plus a few per
+// reconnection), rounds separated by block barriers.
+__global__ void __launch_bounds__(1024) k_rb_cycles_block(
+    const int *__restrict__ nextq, const int *__restrict__ rid, const int *__restrict__ rs,
+    const int *__restrict__ re, const int *__restrict__ R_dev, int *__restrict__ nr,
+    int *lab, int *lab2, int *nrj, int *nrj2, int *__restrict__ hr, int *succ, int *succ2,
+    long long *val, long long *val2, int *__restrict__ ishead, long long **valout) {
+  const int R = *R_dev;
+  for (int r = threadIdx.x; r < R; r += blockDim.x) {
     int t = rid[nextq[re[r]]];
     nr[r] = t;
     nrj[r] = t;
     lab[r] = rs[r];
   }
-}
-
-__global__ void k_rb_minjump(const int *__restrict__ lab, const int *__restrict__ nrj, int R,
-                             int *__restrict__ lab2, int *__restrict__ nrj2) {
-  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < R; r += gridDim.x * blockDim.x) {
-    int n = nrj[r];
-    lab2[r] = min(lab[r], lab[n]);
-    nrj2[r] = nrj[n];
+  __syncthreads();
+  int rounds = 1;
+  while ((1 << rounds) < R) rounds++;
+  rounds++;
+  for (int it = 0; it < rounds; it++) {
+    for (int r = threadIdx.x; r < R; r += blockDim.x) {
+      int n = nrj[r];
+      lab2[r] = min(lab[r], lab[n]);
+      nrj2[r] = nrj[n];
+    }
+    __syncthreads();
+    int *t1 = lab; lab = lab2; lab2 = t1;
+    int *t2 = nrj; nrj = nrj2; nrj2 = t2;
   }
-}
-
-__global__ void k_rb_succ(const int *__restrict__ lab, const int *__restrict__ rid,
-                          const int *__restrict__ nr, const int *__restrict__ rs,
-                          const int *__restrict__ re, int R, int *__restrict__ hr,
-                          int *__restrict__ succ, long long *__restrict__ val,
-                          int *__restrict__ ishead) {
-  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < R; r += gridDim.x * blockDim.x) {
+  for (int r = threadIdx.x; r < R; r += blockDim.x) {
     int h = rid[lab[r]];
     hr[r] = h;
-    succ[r] = nr[r] == h ? -1 : nr[r];  // the cycle's last run ends the list
+    succ[r] = nr[r] == h ? -1 : nr[r];
     val[r] = re[r] - rs[r] + 1;
     ishead[r] = h == r;
   }
-}
-
-__global__ void k_rb_sumjump(const long long *__restrict__ val, const int *__restrict__ succ, int R,
-                             long long *__restrict__ val2, int *__restrict__ succ2) {
-  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < R; r += gridDim.x * blockDim.x) {
-    int s = succ[r];
-    val2[r] = val[r] + (s >= 0 ? val[s] : 0);
-    succ2[r] = s >= 0 ? succ[s] : -1;
+  __syncthreads();
+  for (int it = 0; it < rounds; it++) {
+    for (int r = threadIdx.x; r < R; r += blockDim.x) {
+      int sc = succ[r];
+      val2[r] = val[r] + (sc >= 0 ? val[sc] : 0);
+      succ2[r] = sc >= 0 ? succ[sc] : -1;
+    }
+    __syncthreads();
+    long long *t3 = val; val = val2; val2 = t3;
+    int *t4 = succ; succ = succ2; succ2 = t4;
   }
+  if (threadIdx.x == 0) *valout = val;  // whichever buffer holds the result
 }
 
-__global__ void k_rb_cycles(const int *__restrict__ ishead, const int *__restrict__ cidx,
-                            const long long *__restrict__ val, const int *__restrict__ rs,
-                            const int *__restrict__ lvl, const LevelDesc *__restrict__ lev, int R,
-                            int *__restrict__ clen, int *__restrict__ clev) {
+__global__ void k_rb_cycles2(const int *__restrict__ ishead, const int *__restrict__ cidx,
+                             long long *const *__restrict__ valp, const int *__restrict__ rs,
+                             const int *__restrict__ lvl, const LevelDesc *__restrict__ lev,
+                             const int *__restrict__ R_dev, int *__restrict__ clen,
+                             int *__restrict__ clev) {
+  const int R = *R_dev;
+  const long long *val = *valp;
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < R; r += gridDim.x * blockDim.x) {
     if (!ishead[r]) continue;
     int c = cidx[r];
@@ -437,12 +551,13 @@ __global__ void k_rb_cycles(const int *__restrict__ ishead, const int *__restric
   }
 }
 
-__global__ void k_rb_gather(const double *__restrict__ xq, const double *__restrict__ yq, int npt,
-                            const int *__restrict__ rid, const int *__restrict__ rs,
-                            const int *__restrict__ hr, const int *__restrict__ cidx,
-                            const long long *__restrict__ val, const int *__restrict__ cst,
-                            const int *__restrict__ clen, double *__restrict__ xw,
-                            double *__restrict__ yw) {
+__global__ void k_rb_gather2(const double *__restrict__ xq, const double *__restrict__ yq, int npt,
+                             const int *__restrict__ rid, const int *__restrict__ rs,
+                             const int *__restrict__ hr, const int *__restrict__ cidx,
+                             long long *const *__restrict__ valp, const int *__restrict__ cst,
+                             const int *__restrict__ clen, double *__restrict__ xw,
+                             double *__restrict__ yw) {
+  const long long *val = *valp;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npt; i += gridDim.x * blockDim.x) {
     int r = rid[i];
     int c = cidx[hr[r]];
@@ -453,30 +568,37 @@ __global__ void k_rb_gather(const double *__restrict__ xq, const double *__restr
   }
 }
 
-// Final contour arrays and canonical links (contours.f90:645-680).
-__global__ void k_rb_contours(const int *__restrict__ ocs, const int *__restrict__ olen,
-                              const int *__restrict__ olev, int nq, int *__restrict__ i1q,
-                              int *__restrict__ i2q, int *__restrict__ npq,
-                              int *__restrict__ indq) {
+// Write the renoded contours back into the node and contour arrays
+// (contours.f90:645-680) using the counts left in device memory.
+__global__ void k_rb_writeback(const int *__restrict__ cnt, long long npm, long long nm,
+                               const int *__restrict__ ocs, const int *__restrict__ olen,
+                               const int *__restrict__ olev, const double *__restrict__ xo,
+                               const double *__restrict__ yo, double *__restrict__ xq,
+                               double *__restrict__ yq, int *__restrict__ nextq,
+                               int *__restrict__ i1q, int *__restrict__ i2q,
+                               int *__restrict__ npq, int *__restrict__ indq,
+                               Scalars *__restrict__ s) {
+  const int nq = cnt[0], npt = cnt[1];
+  if (cnt[2] || npt > npm || nq > nm) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(&s->error, CASL_ECAPACITY);
+    return;
+  }
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nq; j += gridDim.x * blockDim.x) {
     i1q[j] = ocs[j];
     i2q[j] = ocs[j] + olen[j] - 1;
     npq[j] = olen[j];
     indq[j] = olev[j];
   }
-}
-
-__global__ void k_rb_links(const int *__restrict__ ocs, const int *__restrict__ olen, int nq,
-                           int npt, int *__restrict__ nextq) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npt; i += gridDim.x * blockDim.x) {
+    xq[i] = xo[i];
+    yq[i] = yo[i];
     int j = contour_of(ocs, nq, i);
     nextq[i] = i + 1 < ocs[j] + olen[j] ? i + 1 : ocs[j];
   }
-}
-
-__global__ void k_set_counts(Scalars *s, const int *cnt) {
-  s->nq = cnt[0];
-  s->nptq = cnt[1];
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    s->nq = nq;
+    s->nptq = npt;
+  }
 }
 
 static inline int gs(long long work) {
@@ -487,202 +609,131 @@ static inline int gs(long long work) {
 }
 
 // Walk-ordered contours of the current link array + renode + write back.
-// Used by surgery; lvl/lev give each node's level.
-static int rebuild_and_renode(casl_handle *h, Arena &ar, const int *lvl, const LevelDesc *dlev) {
+// Issues no host synchronisation: every count stays in device memory and
+// every buffer is sized from the node count npt.
+static int rebuild_and_renode(casl_handle *h, Arena &ar, int npt, const int *lvl,
+                              const LevelDesc *dlev) {
   cudaStream_t st = h->stream;
-  int npt = h->nptq;
   int *stf = ar.get<int>(npt), *brk = ar.get<int>(npt), *sx = ar.get<int>(npt);
   int *rid = ar.get<int>(npt), *tmpi = ar.get<int>(scan_tmp_elems(npt) + 4);
   int *dtot = ar.get<int>(8);
-  if (ar.failed) return CASL_ENOMEM;
-  int g = gs(npt);
-  CASL_K(k_rb_flags, g, 256, 0, st)(h->nextq, npt, stf, brk);
-  exclusive_scan<int>(st, stf, sx, npt, tmpi, dtot);
-  int R = 0;
-  cudaMemcpyAsync(&R, dtot, sizeof(int), cudaMemcpyDeviceToHost, st);
-  cudaError_t e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) return set_cuda_error(h, e);
-  int *rs = ar.get<int>(R), *re = ar.get<int>(R), *nr = ar.get<int>(R), *lab = ar.get<int>(R);
-  int *lab2 = ar.get<int>(R), *nrj = ar.get<int>(R), *nrj2 = ar.get<int>(R), *hr = ar.get<int>(R);
-  int *succ = ar.get<int>(R), *succ2 = ar.get<int>(R), *ishead = ar.get<int>(R);
-  int *cidx = ar.get<int>(R);
-  long long *val = ar.get<long long>(R), *val2 = ar.get<long long>(R);
-  if (ar.failed) return CASL_ENOMEM;
-  CASL_K(k_rb_runs, g, 256, 0, st)(stf, brk, sx, npt, rid, rs, re);
-  int gr = gs(R);
-  CASL_K(k_rb_runinit, gr, 256, 0, st)(h->nextq, rid, rs, re, R, nr, lab, nrj);
-  int rounds = 1;
-  while ((1 << rounds) < R) rounds++;
-  rounds++;
-  for (int it = 0; it < rounds; it++) {
-    CASL_K(k_rb_minjump, gr, 256, 0, st)(lab, nrj, R, lab2, nrj2);
-    std::swap(lab, lab2);
-    std::swap(nrj, nrj2);
-  }
-  CASL_K(k_rb_succ, gr, 256, 0, st)(lab, rid, nr, rs, re, R, hr, succ, val, ishead);
-  for (int it = 0; it < rounds; it++) {
-    CASL_K(k_rb_sumjump, gr, 256, 0, st)(val, succ, R, val2, succ2);
-    std::swap(val, val2);
-    std::swap(succ, succ2);
-  }
-  exclusive_scan<int>(st, ishead, cidx, R, tmpi, dtot + 1);
-  int C = 0;
-  cudaMemcpyAsync(&C, dtot + 1, sizeof(int), cudaMemcpyDeviceToHost, st);
-  e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) return set_cuda_error(h, e);
-  int *clen = ar.get<int>(C), *clev = ar.get<int>(C), *cst = ar.get<int>(C);
+  // run arrays (R <= npt)
+  int *rs = ar.get<int>(npt), *re = ar.get<int>(npt), *nr = ar.get<int>(npt);
+  int *lab = ar.get<int>(npt), *lab2 = ar.get<int>(npt), *nrj = ar.get<int>(npt);
+  int *nrj2 = ar.get<int>(npt), *hr = ar.get<int>(npt), *succ = ar.get<int>(npt);
+  int *succ2 = ar.get<int>(npt), *ishead = ar.get<int>(npt), *cidx = ar.get<int>(npt);
+  long long *val = ar.get<long long>(npt), *val2 = ar.get<long long>(npt);
+  long long **valp = ar.get<long long *>(1);
+  // cycles (C <= R <= npt)
+  int *clen = ar.get<int>(npt), *clev = ar.get<int>(npt), *cst = ar.get<int>(npt);
   double *xw = ar.get<double>(npt), *yw = ar.get<double>(npt);
+  int *ocs = ar.get<int>(npt), *olen = ar.get<int>(npt), *olev = ar.get<int>(npt);
+  int *cnt = ar.get<int>(4);
   if (ar.failed) return CASL_ENOMEM;
-  CASL_K(k_rb_cycles, gr, 256, 0, st)(ishead, cidx, val, rs, lvl, dlev, R, clen, clev);
-  exclusive_scan<int>(st, clen, cst, C, tmpi, dtot + 2);
-  CASL_K(k_rb_gather, g, 256, 0, st)(h->xq, h->yq, npt, rid, rs, hr, cidx, val, cst, clen, xw, yw);
+  const int g = gs(npt);
+  CASL_K(k_rb_flags, g, 256, 0, st)(h->nextq, npt, stf, brk);
+  exclusive_scan<int>(st, stf, sx, npt, tmpi, dtot);           // dtot[0] = R
+  CASL_K(k_rb_runs, g, 256, 0, st)(stf, brk, sx, npt, rid, rs, re);
+  CASL_CUDA_TRY(cudaMemsetAsync(ishead, 0, (size_t)npt * sizeof(int), st));
+  CASL_CUDA_TRY(cudaMemsetAsync(clen, 0, (size_t)npt * sizeof(int), st));
+  CASL_K(k_rb_cycles_block, 1, 1024, 0, st)(h->nextq, rid, rs, re, dtot, nr, lab, lab2, nrj, nrj2,
+                                            hr, succ, succ2, val, val2, ishead, valp);
+  exclusive_scan<int>(st, ishead, cidx, npt, tmpi, dtot + 1);  // dtot[1] = C
+  CASL_K(k_rb_cycles2, g, 256, 0, st)(ishead, cidx, valp, rs, lvl, dlev, dtot, clen, clev);
+  exclusive_scan<int>(st, clen, cst, npt, tmpi, dtot + 2);
+  CASL_K(k_rb_gather2, g, 256, 0, st)(h->xq, h->yq, npt, rid, rs, hr, cidx, valp, cst, clen, xw, yw);
   int rc = check_launch(h);
   if (rc) return rc;
-  // renode every cycle; write straight into the node arrays
-  RenodeIn in{xw, yw, cst, clen, clev, C, npt};
+  RenodeIn in{xw, yw, cst, clen, clev, npt, npt, dtot + 1};
   RenodeOut out{};
   out.xo = h->xqi;  // node-sized scratch of the RK step, free between steps
   out.yo = h->yqi;
-  out.ocs = ar.get<int>(C); out.olen = ar.get<int>(C); out.olev = ar.get<int>(C);
+  out.ocs = ocs; out.olen = olen; out.olev = olev;
   out.cap = h->npm;
-  out.d_counts = ar.get<int>(4);
-  if (ar.failed) return CASL_ENOMEM;
+  out.d_counts = cnt;
   rc = renode_batch(h, ar, in, out, RENODE_SURGERY);
   if (rc) return rc;
-  int hc[3];
-  cudaMemcpyAsync(hc, out.d_counts, 3 * sizeof(int), cudaMemcpyDeviceToHost, st);
-  e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) return set_cuda_error(h, e);
-  int nq = hc[0], nptn = hc[1];
-  if (nq > h->nm || nptn > h->npm) return CASL_ECAPACITY;
-  if (nptn > 0) {
-    cudaMemcpyAsync(h->xq, out.xo, (size_t)nptn * sizeof(double), cudaMemcpyDeviceToDevice, st);
-    cudaMemcpyAsync(h->yq, out.yo, (size_t)nptn * sizeof(double), cudaMemcpyDeviceToDevice, st);
-  }
-  if (nq > 0) {
-    CASL_K(k_rb_contours, gs(nq), 256, 0, st)(out.ocs, out.olen, out.olev, nq, h->i1q, h->i2q, h->npq,
-                                          h->indq);
-    CASL_K(k_rb_links, gs(nptn), 256, 0, st)(out.ocs, out.olen, nq, nptn, h->nextq);
-  }
-  CASL_K(k_set_counts, 1, 1, 0, st)(h->scal, out.d_counts);
-  rc = check_launch(h);
-  if (rc) return rc;
-  h->nq = nq;
-  h->nptq = nptn;
-  h->contex = nptn > 0;
-  return CASL_OK;
+  CASL_K(k_rb_writeback, gs(h->npm < (1 << 24) ? h->npm : (1 << 24)), 256, 0, st)(
+      cnt, h->npm, h->nm, ocs, olen, olev, h->xqi, h->yqi, h->xq, h->yq, h->nextq, h->i1q,
+      h->i2q, h->npq, h->indq, h->scal);
+  return check_launch(h);
 }
 
 int surgery_dev(casl_handle *h) {
   if (h->nq == 0 || h->nptq == 0) return CASL_OK;
   cudaStream_t st = h->stream;
   const Consts &c = h->c;
-  int nq = h->nq, npt = h->nptq;
-  // Levels (contours.f90:374-394) and box dimensions (contours.f90:429-454),
-  // on the host from the contour table.
-  std::vector<int> indq(nq), i1q(nq), i2q(nq);
-  cudaMemcpyAsync(indq.data(), h->indq, nq * sizeof(int), cudaMemcpyDeviceToHost, st);
-  cudaMemcpyAsync(i1q.data(), h->i1q, nq * sizeof(int), cudaMemcpyDeviceToHost, st);
-  cudaMemcpyAsync(i2q.data(), h->i2q, nq * sizeof(int), cudaMemcpyDeviceToHost, st);
-  cudaError_t e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) return set_cuda_error(h, e);
-  std::vector<LevelDesc> lev;
-  {
-    int levp = indq[0], jq1 = 0;
-    auto push = [&](int j1, int j2, int levt) {
-      LevelDesc L{};
-      L.ibeg = i1q[j1];
-      L.iend = i2q[j2];
-      L.levt = levt;
-      lev.push_back(L);
-    };
-    for (int j = 1; j < nq; j++) {
-      if (indq[j] > levp) {
-        push(jq1, j - 1, levp);
-        jq1 = j;
-        levp = indq[j];
-      }
-    }
-    push(jq1, nq - 1, levp);
-  }
-  long long nbox = 0;
-  for (auto &L : lev) {
-    if (L.ibeg < 0 || L.iend >= npt || L.iend < L.ibeg) return CASL_EINVAL;
-    int nptlev = L.iend - L.ibeg + 1;
-    double fnq = (double)nptlev;
-    double fnbx = 1.2 * sqrt(fnq * c.aspect);
-    double fnby = fnbx / c.aspect;
-    int nbx = (int)llround(fnbx);
-    nbx = std::max(std::min(nbx, c.nx), 1);
-    int nby = (int)llround(fnby);
-    nby = std::max(std::min(nby, c.ny), 1);
-    L.nbx = nbx;
-    L.nby = nby;
-    L.bwxi = c.oms * (double)nbx / c.ellx;
-    L.bwyi = c.oms * (double)nby / c.elly;
-    L.boxbase = (int)nbox;
-    nbox += (long long)nbx * nby;
-  }
-  int nlev = (int)lev.size();
-  // scratch
-  size_t need = (size_t)npt * 560 + (size_t)nbox * 40 + (size_t)nq * 256 + ((size_t)64 << 20);
+  const int nq = h->nq, npt = h->nptq;
+  const long long nbox_cap = 2LL * npt + nq + 64;
+  const long long ne_cap = 16LL * npt + 64;
+  size_t need = (size_t)npt * 760 + (size_t)nq * 96 + (size_t)nbox_cap * 24 +
+                (size_t)ne_cap * 12 + ((size_t)64 << 20);
   int rc = ensure_scratch(h, need);
   if (rc) return rc;
   Arena ar{(char *)h->sx, h->sx_bytes, 0};
-  LevelDesc *dlev = ar.get<LevelDesc>(nlev);
+  int *err = &h->scal->error;
+  Trace tr;
+  tr.begin(st, "start");
+  // levels and boxes, on the device
+  int *lflag = ar.get<int>(nq), *lex = ar.get<int>(nq), *nbox_l = ar.get<int>(nq);
+  int *boxbase = ar.get<int>(nq);
+  LevelDesc *dlev = ar.get<LevelDesc>(nq);
+  int *tmpi = ar.get<int>(scan_tmp_elems(std::max<long long>(std::max<long long>(npt, nbox_cap), ne_cap)) + 4);
+  int *dtot = ar.get<int>(16);  // [0] nlev, [1] nbox, [2] ne, [3] nsurg
   int *endnext = ar.get<int>(npt), *lvl = ar.get<int>(npt);
   double *dx = ar.get<double>(npt), *dy = ar.get<double>(npt), *dsq = ar.get<double>(npt);
   double *x0 = ar.get<double>(npt), *y0 = ar.get<double>(npt);
   double *dx0 = ar.get<double>(npt), *dy0 = ar.get<double>(npt);
   int *nq0 = ar.get<int>(npt), *prev0 = ar.get<int>(npt);
-  unsigned char *pending = ar.get<unsigned char>(npt);
+  unsigned char *pending = ar.get<unsigned char>(npt + 16);
   int *ecount = ar.get<int>(npt), *eoff = ar.get<int>(npt), *nbox_of = ar.get<int>(npt);
-  int *bcnt = ar.get<int>(nbox), *kb1 = ar.get<int>(nbox), *cursor = ar.get<int>(nbox);
-  int *nbcnt = ar.get<int>(nbox), *nb1 = ar.get<int>(nbox), *nbnode = ar.get<int>(npt);
-  int *tmpi = ar.get<int>(scan_tmp_elems(std::max<long long>(npt, nbox)) + 4);
-  int *dtot = ar.get<int>(8);
+  int *bcnt = ar.get<int>(nbox_cap), *kb1 = ar.get<int>(nbox_cap), *cursor = ar.get<int>(nbox_cap);
+  int *nbcnt = ar.get<int>(nbox_cap), *nb1 = ar.get<int>(nbox_cap), *nbnode = ar.get<int>(npt);
+  int *ebox = ar.get<int>(ne_cap), *eib = ar.get<int>(ne_cap), *bnode = ar.get<int>(ne_cap);
   if (ar.failed) return CASL_ENOMEM;
-  cudaMemcpyAsync(dlev, lev.data(), nlev * sizeof(LevelDesc), cudaMemcpyHostToDevice, st);
-  cudaMemsetAsync(endnext, 0xff, (size_t)npt * sizeof(int), st);
-  cudaMemsetAsync(bcnt, 0, (size_t)nbox * sizeof(int), st);
-  cudaMemsetAsync(nbcnt, 0, (size_t)nbox * sizeof(int), st);
-  cudaMemsetAsync(&h->scal->error, 0, sizeof(int), st);
-  int g = gs(npt);
-  CASL_K(k_sg_endnext, gs(nq), 256, 0, st)(h->i1q, h->i2q, nq, endnext);
-  CASL_K(k_sg_level_of, g, 256, 0, st)(dlev, nlev, npt, lvl);
-  CASL_K(k_sg_init, g, 256, 0, st)(h->xq, h->yq, h->nextq, endnext, npt, dx, dy, dsq, x0, y0, dx0, dy0,
-                               nq0, prev0, pending, c, &h->scal->error);
+  const int g = gs(npt), gq = gs(nq), gb = gs(nbox_cap);
+  CASL_K(k_lv_flags, gq, 256, 0, st)(h->indq, nq, lflag, err);
+  exclusive_scan<int>(st, lflag, lex, nq, tmpi, dtot + 0);
+  CASL_K(k_lv_desc, gq, 256, 0, st)(h->i1q, h->i2q, h->indq, lflag, lex, nq, dlev);
+  CASL_K(k_lv_boxes, gq, 256, 0, st)(dlev, dtot + 0, nq, npt, c, nbox_l, err);
+  exclusive_scan<int>(st, nbox_l, boxbase, nq, tmpi, dtot + 1);
+  CASL_K(k_lv_base, gq, 256, 0, st)(dlev, dtot + 0, boxbase, dtot + 1, nbox_cap, err);
+  CASL_CUDA_TRY(cudaMemsetAsync(endnext, 0xff, (size_t)npt * sizeof(int), st));
+  CASL_CUDA_TRY(cudaMemsetAsync(bcnt, 0, (size_t)nbox_cap * sizeof(int), st));
+  CASL_CUDA_TRY(cudaMemsetAsync(nbcnt, 0, (size_t)nbox_cap * sizeof(int), st));
+  CASL_K(k_sg_endnext, gq, 256, 0, st)(h->i1q, h->i2q, nq, endnext);
+  CASL_K(k_sg_level_of, g, 256, 0, st)(dlev, dtot + 0, npt, lvl);
+  CASL_K(k_sg_init, g, 256, 0, st)(h->xq, h->yq, h->nextq, endnext, npt, dx, dy, dsq, x0, y0, dx0,
+                                   dy0, nq0, prev0, pending, c, err);
   SurgState S{};
   S.xq = h->xq; S.yq = h->yq; S.dx = dx; S.dy = dy; S.dsq = dsq; S.nextq = h->nextq;
   S.x0 = x0; S.y0 = y0; S.dx0 = dx0; S.dy0 = dy0; S.nq0 = nq0; S.prev0 = prev0; S.lvl = lvl;
   S.pending = pending;
   CASL_K(k_sg_count_entries, g, 256, 0, st)(S, dlev, npt, ecount, nbox_of, nbcnt, c);
-  exclusive_scan<int>(st, ecount, eoff, npt, tmpi, dtot);
-  int ne = 0;
-  cudaMemcpyAsync(&ne, dtot, sizeof(int), cudaMemcpyDeviceToHost, st);
-  int herr = 0;
-  cudaMemcpyAsync(&herr, &h->scal->error, sizeof(int), cudaMemcpyDeviceToHost, st);
-  e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) return set_cuda_error(h, e);
-  if (herr) return herr;
-  int *ebox = ar.get<int>(ne), *eib = ar.get<int>(ne), *bnode = ar.get<int>(ne);
-  if (ar.failed) return CASL_ENOMEM;
-  CASL_K(k_sg_emit, g, 256, 0, st)(S, dlev, npt, eoff, ebox, eib, bcnt, c);
-  exclusive_scan<int>(st, bcnt, kb1, nbox, tmpi, dtot + 1);
-  cudaMemsetAsync(cursor, 0, (size_t)nbox * sizeof(int), st);
-  CASL_K(k_sg_place, gs(ne), 256, 0, st)(ebox, eib, ne, kb1, cursor, bnode);
-  CASL_K(k_sg_sort_boxes, gs(nbox), 256, 0, st)(kb1, bcnt, (int)nbox, bnode);
-  exclusive_scan<int>(st, nbcnt, nb1, nbox, tmpi, dtot + 2);
-  cudaMemsetAsync(cursor, 0, (size_t)nbox * sizeof(int), st);
+  exclusive_scan<int>(st, ecount, eoff, npt, tmpi, dtot + 2);
+  CASL_K(k_sg_emit, g, 256, 0, st)(S, dlev, npt, eoff, ecount, ne_cap, ebox, eib, bcnt, c, err);
+  exclusive_scan<int>(st, bcnt, kb1, nbox_cap, tmpi, dtot + 4);
+  CASL_CUDA_TRY(cudaMemsetAsync(cursor, 0, (size_t)nbox_cap * sizeof(int), st));
+  CASL_K(k_sg_place, gs(ne_cap), 256, 0, st)(ebox, eib, dtot + 2, kb1, cursor, bnode);
+  CASL_K(k_sg_sort_boxes, gb, 256, 0, st)(kb1, bcnt, dtot + 1, bnode);
+  exclusive_scan<int>(st, nbcnt, nb1, nbox_cap, tmpi, dtot + 5);
+  CASL_CUDA_TRY(cudaMemsetAsync(cursor, 0, (size_t)nbox_cap * sizeof(int), st));
   CASL_K(k_sg_place_nodes, g, 256, 0, st)(nbox_of, npt, nb1, cursor, nbnode);
   S.kb1 = kb1; S.bcnt = bcnt; S.bnode = bnode; S.nb1 = nb1; S.nbcnt = nbcnt; S.nbnode = nbnode;
+  tr.point("binning");
   CASL_K(k_sg_candidates, g, 256, 0, st)(S, dlev, npt, nbox_of, c);
-  int *nsurg = dtot + 4;
-  cudaMemsetAsync(nsurg, 0, sizeof(int), st);
-  CASL_K(k_sg_replay, (nlev * 32 + 127) / 128, 128, 0, st)(S, dlev, nlev, c, nsurg);
+  tr.point("candidates");
+  CASL_CUDA_TRY(cudaMemsetAsync(dtot + 3, 0, sizeof(int), st));
+  CASL_K(k_sg_replay, (nq * 32 + 127) / 128, 128, 0, st)(S, dlev, dtot + 0, c, dtot + 3);
   rc = check_launch(h);
   if (rc) return rc;
-  return rebuild_and_renode(h, ar, lvl, dlev);
+  tr.point("replay");
+  rc = rebuild_and_renode(h, ar, npt, lvl, dlev);
+  if (rc) return rc;
+  tr.point("rebuild+renode");
+  tr.flush("surgery");
+  // the host copies of the counts are refreshed at the next synchronisation
+  return CASL_OK;
 }
 
 // Renode of one contour supplied by the host (casl_renode).
@@ -713,6 +764,7 @@ int renode_host(casl_handle *h, const double *xd, const double *yd, int npd, dou
   int hc[3];
   CASL_CUDA_TRY(cudaMemcpyAsync(hc, out.d_counts, 3 * sizeof(int), cudaMemcpyDeviceToHost, st));
   CASL_CUDA_TRY(cudaStreamSynchronize(st));
+  if (hc[2]) return CASL_ECAPACITY;
   *npr = hc[1];
   if (hc[1] > 0) {
     CASL_CUDA_TRY(cudaMemcpyAsync(xr, xo, hc[1] * sizeof(double), cudaMemcpyDeviceToHost, st));
