@@ -35,43 +35,48 @@ int check_launch(casl_handle *h) {
   return CASL_OK;
 }
 
-static int ilog2(int n) {
-  int l = 0;
-  while ((1 << l) < n) l++;
-  return l;
-}
 
 // ---------------------------------------------------------------------------
 // Transform launches
 // ---------------------------------------------------------------------------
-template <int V, bool FWD, bool LVF, bool SVF, class LD, class ST>
+// One batched transform pass (all vectors of `batch` fields along one axis).
+template <int LOGH, bool FWD, bool LVF, bool SVF, class LD, class ST>
 static int launch_rfft(casl_handle *h, LD ld, ST st, int batch) {
-  int n = h->n;
-  size_t sm = rfft_smem_bytes(V, n);
-  auto kern = k_rfft<V, FWD, LVF, SVF, LD, ST>;
-  static bool configured = false;  // one per template instance
-  if (!configured) {
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    configured = true;
-  }
-  dim3 grid(n / V, batch);
+  using Sh = RfftShape<LOGH>;
+  dim3 grid(Sh::N / Sh::V, batch);
   const bool prof = h->prof_class == CASL_PROF_FFT && h->prof_ev && h->prof_n < CASL_PROF_MAX;
   if (prof) cudaEventRecord(h->prof_ev[2 * h->prof_n], h->stream);
-  CASL_K(kern, grid, 256, sm, h->stream)(ld, st, h->tw, n, ilog2(n / 2));
+  auto kern = k_rfft_r<LOGH, FWD, LVF, SVF, LD, ST>;
+  const size_t sm = Sh::smem(FWD && SVF);
+  static bool configured = false;  // one per template instance
+  if (!configured) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    configured = true;
+  }
+  CASL_K(kern, grid, Sh::NT, sm, h->stream)(ld, st, h->tw);
   if (prof) {
     cudaEventRecord(h->prof_ev[2 * h->prof_n + 1], h->stream);
     h->prof_n++;
     // algorithmic bytes: every element of every vector read once and written once
-    h->prof_bytes += (double)batch * (double)n * (double)n * (ld.bytes() + st.bytes());
+    h->prof_bytes += (double)batch * (double)Sh::N * (double)Sh::N * (ld.bytes() + st.bytes());
   }
   return check_launch(h);
 }
 
-// Vectors per CTA: keep >= ~2 CTAs per SM at every size while the shared
-// tile (2 buffers) stays well inside 227 KB.
-#define RFFT_DISPATCH(FWD, LVF, SVF, ld, st, batch)                        \
-  (h->n >= 2048 ? launch_rfft<2, FWD, LVF, SVF>(h, ld, st, batch)          \
-                : launch_rfft<4, FWD, LVF, SVF>(h, ld, st, batch))
+template <bool FWD, bool LVF, bool SVF, class LD, class ST>
+static int rfft_dispatch(casl_handle *h, LD ld, ST st, int batch) {
+  switch (h->n) {
+    case 32: return launch_rfft<4, FWD, LVF, SVF>(h, ld, st, batch);
+    case 64: return launch_rfft<5, FWD, LVF, SVF>(h, ld, st, batch);
+    case 128: return launch_rfft<6, FWD, LVF, SVF>(h, ld, st, batch);
+    case 256: return launch_rfft<7, FWD, LVF, SVF>(h, ld, st, batch);
+    case 512: return launch_rfft<8, FWD, LVF, SVF>(h, ld, st, batch);
+    case 1024: return launch_rfft<9, FWD, LVF, SVF>(h, ld, st, batch);
+    case 2048: return launch_rfft<10, FWD, LVF, SVF>(h, ld, st, batch);
+    default: return CASL_EINVAL;
+  }
+}
+#define RFFT_DISPATCH(FWD, LVF, SVF, ld, st, batch) rfft_dispatch<FWD, LVF, SVF>(h, ld, st, batch)
 
 int ptospc_dev(casl_handle *h, const double *phys, double *spec) {
   long long n = h->n, nn = n * n;
@@ -373,6 +378,115 @@ __global__ void k_c2g_coarsen(const int *__restrict__ L, int *__restrict__ C,
   }
 }
 
+
+// Column scan + 7x7 coarsening in one pass (the two kernels above, fused;
+// the fine grid is only read, the level grid never goes to memory).  A CTA
+// owns CW = 7 coarse columns and scans the 4*CW+3 = 31 fine columns they
+// need, one warp per column, RPS = 32U fine rows per step with the next
+// step's rows already in flight (register prefetch).  The level rows go to
+// a shared ring of RPS+8 rows; each step then forms its RPS/4 coarse rows as
+// 7-tap vertical sums per fine column (all threads, conflict-free) followed
+// by 7-tap horizontal sums.  Coarse row 1 needs the last fine rows (periodic
+// wrap), so it is formed after the last step from the saved first rows.
+// Requires nf % RPS == 0.
+#define C2G_CW 7
+#define C2G_FC (4 * C2G_CW + 3)
+template <int U>
+__global__ void __launch_bounds__(1024) k_c2g_fused(const int *__restrict__ J, int *__restrict__ C,
+                                                    unsigned long long *__restrict__ csum, int n,
+                                                    int nf) {
+  constexpr int RPS = 32 * U, RING = RPS + 8, CR = RPS / 4;
+  __shared__ int ring[RING][C2G_FC];
+  __shared__ int first[4][C2G_FC];
+  __shared__ int vsum[CR][C2G_FC];
+  __shared__ long long red[32];
+  const int w7[7] = {1, 2, 3, 4, 3, 2, 1};
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int cx0 = blockIdx.x * C2G_CW;  // first coarse column (0-based)
+  int col = 4 * cx0 - 3 + warp;         // this warp's fine column (0-based), wrapped
+  if (col < 0) col += nf;
+  if (col >= nf) col -= nf;
+  const int *cp = J + (long long)col * nf + lane;
+  const int nsteps = nf / RPS;
+  int v[U];
+  if (warp < C2G_FC) {
+#pragma unroll
+    for (int u = 0; u < U; u++) v[u] = __ldcs(cp + u * 32);
+  }
+  int carry = 0;
+  long long local = 0;
+  for (int s = 0; s < nsteps; s++) {
+    if (warp < C2G_FC) {
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        int x = warp_incl_scan(v[u]) + carry;
+        carry = __shfl_sync(0xffffffffu, x, 31);
+        int r = s * RPS + u * 32 + lane;  // 0-based fine row
+        ring[r % RING][warp] = x;
+        if (r < 4) first[r][warp] = x;
+      }
+      if (s + 1 < nsteps) {
+#pragma unroll
+        for (int u = 0; u < U; u++) v[u] = __ldcs(cp + (s + 1) * RPS + u * 32);
+      }
+    }
+    __syncthreads();
+    // vertical: coarse row iy (1-based) uses fine rows 4iy-7..4iy-1 (0-based)
+    for (int t = threadIdx.x; t < CR * 32; t += blockDim.x) {
+      int iyl = t >> 5, fc = t & 31;
+      int iy = s * CR + iyl + 1;
+      if (fc < C2G_FC && iy > 1) {
+        int acc = 0;
+#pragma unroll
+        for (int a = 0; a < 7; a++) acc += w7[a] * ring[(4 * iy - 7 + a) % RING][fc];
+        vsum[iyl][fc] = acc;
+      }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < C2G_CW * CR; t += blockDim.x) {
+      int cxl = t / CR, iyl = t % CR;
+      int cx = cx0 + cxl, iy = s * CR + iyl + 1;
+      if (cx < n && iy > 1) {
+        int acc = 0;
+#pragma unroll
+        for (int b = 0; b < 7; b++) acc += w7[b] * vsum[iyl][4 * cxl + b];
+        C[(long long)cx * n + (iy - 1)] = acc;
+        local += acc;
+      }
+    }
+  }
+  __syncthreads();
+  // coarse row 1: fine rows nf-3..nf-1 and 0..3 (0-based)
+  if (threadIdx.x < C2G_FC) {
+    int fc = threadIdx.x, acc = 0;
+#pragma unroll
+    for (int a = 0; a < 7; a++) {
+      int r = a - 3;
+      acc += w7[a] * (r < 0 ? ring[(r + nf) % RING][fc] : first[r][fc]);
+    }
+    vsum[0][fc] = acc;
+  }
+  __syncthreads();
+  if (threadIdx.x < C2G_CW) {
+    int cx = cx0 + threadIdx.x;
+    if (cx < n) {
+      int acc = 0;
+#pragma unroll
+      for (int b = 0; b < 7; b++) acc += w7[b] * vsum[0][4 * threadIdx.x + b];
+      C[(long long)cx * n] = acc;
+      local += acc;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xffffffffu, local, o);
+  if (lane == 0) red[warp] = local;
+  __syncthreads();
+  if (warp == 0) {
+    long long x = red[lane];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) atomicAdd(csum, (unsigned long long)x);
+  }
+}
+
 __global__ void k_zero_csum(Scalars *s) { s->csum = 0; }
 
 __global__ void k_c2g_final(const int *__restrict__ C, const Scalars *__restrict__ s,
@@ -392,7 +506,7 @@ static int grid_for(long long work, int block = 256) {
   return (int)g;
 }
 
-int con2grid_dev(casl_handle *h) {
+int con2grid_dev(casl_handle *h, bool want_levels) {
   const Consts &c = h->c;
   size_t fine = (size_t)c.nxf * c.nyf;
   CASL_CUDA_TRY(cudaMemsetAsync(h->fineJ, 0, fine * sizeof(int), h->stream));
@@ -403,9 +517,18 @@ int con2grid_dev(casl_handle *h) {
     CASL_K(k_c2g_scatter, grid_for(h->nptq), 256, 0, h->stream)(h->xq, h->yq, h->nextq, h->scal,
                                                               h->fineJ, h->ljx, c, err);
   CASL_K(k_c2g_lbot, 1, 1024, 0, h->stream)(h->ljx, h->fineJ, c.nxf, c.nyf);
-  CASL_K(k_c2g_colscan, (c.nxf * 32 + 255) / 256, 256, 0, h->stream)(h->fineJ, c.nxf, c.nyf);
-  CASL_K(k_c2g_coarsen, grid_for((long long)h->n * h->n), 256, 0, h->stream)(
-      h->fineJ, h->coarseC, (unsigned long long *)&h->scal->csum, h->n, c.nxf);
+  unsigned long long *csum = (unsigned long long *)&h->scal->csum;
+  int nblk = (h->n + C2G_CW - 1) / C2G_CW;
+  if (!want_levels && c.nxf == c.nyf && c.nxf % 256 == 0) {
+    CASL_K(k_c2g_fused<8>, nblk, 1024, 0, h->stream)(h->fineJ, h->coarseC, csum, h->n, c.nxf);
+  } else if (!want_levels && c.nxf == c.nyf && c.nxf % 128 == 0) {
+    CASL_K(k_c2g_fused<4>, nblk, 1024, 0, h->stream)(h->fineJ, h->coarseC, csum, h->n, c.nxf);
+  } else {
+    // the fine-grid levels themselves are wanted: scan in place, then coarsen
+    CASL_K(k_c2g_colscan, (c.nxf * 32 + 255) / 256, 256, 0, h->stream)(h->fineJ, c.nxf, c.nyf);
+    CASL_K(k_c2g_coarsen, grid_for((long long)h->n * h->n), 256, 0, h->stream)(
+        h->fineJ, h->coarseC, csum, h->n, c.nxf);
+  }
   return check_launch(h);
 }
 
@@ -415,7 +538,7 @@ int con2grid_to_spec(casl_handle *h, double *spec) {
     CASL_CUDA_TRY(cudaMemsetAsync(spec, 0, nn * sizeof(double), h->stream));
     return CASL_OK;
   }
-  int rc = con2grid_dev(h);
+  int rc = con2grid_dev(h, false);
   if (rc) return rc;
   LoadQC ld{h->coarseC, h->scal, h->c.beffect ? h->betac : nullptr, nn,
             1.0 / (256.0 * (double)n * (double)n), (int)n};
@@ -425,13 +548,13 @@ int con2grid_to_spec(casl_handle *h, double *spec) {
                        (StoreStrided{spec, nn, 1, n}), 1);
 }
 
-int con2grid_to_phys(casl_handle *h, double *phys) {
+int con2grid_to_phys(casl_handle *h, double *phys, bool want_levels) {
   long long nn = (long long)h->n * h->n;
   if (h->nptq == 0) {
     CASL_CUDA_TRY(cudaMemsetAsync(phys, 0, nn * sizeof(double), h->stream));
     return CASL_OK;
   }
-  int rc = con2grid_dev(h);
+  int rc = con2grid_dev(h, want_levels);
   if (rc) return rc;
   CASL_K(k_c2g_final, grid_for(nn), 256, 0, h->stream)(h->coarseC, h->scal,
                                                    h->c.beffect ? h->betac : nullptr, phys, h->n);
@@ -973,11 +1096,15 @@ int sync_counts(casl_handle *h) {
   return CASL_OK;
 }
 
+// Scratch arenas grow with 50% headroom: their sizes follow node and
+// crossing counts, which drift from step to step, and re-allocating several
+// GB costs far more than the spare memory.
 int ensure_scratch(casl_handle *h, size_t bytes) {
   if (h->sx_bytes >= bytes) return CASL_OK;
   if (h->sx) cudaFree(h->sx);
   h->sx = nullptr;
   h->sx_bytes = 0;
+  bytes += bytes / 2;
   CASL_CUDA_TRY(cudaMalloc(&h->sx, bytes));
   h->sx_bytes = bytes;
   return CASL_OK;
@@ -1023,6 +1150,7 @@ int ensure_scratch2(casl_handle *h, size_t bytes) {
   if (h->sx2) cudaFree(h->sx2);
   h->sx2 = nullptr;
   h->sx2_bytes = 0;
+  bytes += bytes / 2;
   CASL_CUDA_TRY(cudaMalloc(&h->sx2, bytes));
   h->sx2_bytes = bytes;
   return CASL_OK;
@@ -1435,7 +1563,7 @@ int casl_spctop(casl_handle *h, const double *svar, double *rvar) {
 int casl_con2grid(casl_handle *h, double *qc, int *levels) {
   if (!h) return CASL_EINVAL;
   size_t nn = (size_t)h->n * h->n;
-  int rc = con2grid_to_phys(h, h->w[5]);
+  int rc = con2grid_to_phys(h, h->w[5], levels != nullptr);
   if (rc) return rc;
   if (qc) CASL_CUDA_TRY(cudaMemcpyAsync(qc, h->w[5], nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   if (levels) {

@@ -7,13 +7,15 @@
 // A 2-D ptospc/spctop (sta2dfft.f90:103-165) is two launches of this kernel,
 // one per axis, with the transpose folded into the store/load addressing.
 //
-// B200 design: one CTA transforms V vectors of one field entirely in shared
-// memory.  The real length-n transform runs as a complex length-n/2 Stockham
-// FFT (radix 8, then 4 or 2) between two shared-memory buffers, bracketed by
-// the even/odd untangling step.  Global traffic is exactly one read and one
-// write of every element per axis; the load and store are functors so that
-// pointwise spectral work (Green function, derivatives, filters, products)
-// fuses into the transform instead of costing extra HBM passes.
+// B200 design: one CTA transforms V vectors of one field on chip.  The real
+// length-n transform runs as a complex length-n/2 Stockham FFT (radix 8,
+// then 4 or 2) bracketed by the even/odd untangling step.  Global traffic is
+// exactly one read and one write of every element per axis; the load and
+// store are functors so that pointwise spectral work (Green function,
+// derivatives, filters, products) fuses into the transform instead of
+// costing extra HBM passes.  LVF / SVF: whether consecutive vectors (true)
+// or consecutive elements (false) are adjacent in global memory for the load
+// / the store, which sets the thread mapping for coalescing.
 #pragma once
 
 #include "common.cuh"
@@ -72,67 +74,6 @@ __device__ __forceinline__ void dft8(double2 *v) {
   v[7] = csub(e3, t3);
 }
 
-// One Stockham pass of radix R over V complex vectors of length h held in
-// `src` (vector stride ldc complex), writing `dst`.
-template <int R, bool FWD>
-__device__ __forceinline__ void stockham_pass(const double2 *src, double2 *dst, int V, int h, int ldc,
-                                              int Ns, const double2 *__restrict__ tw, int n) {
-  const int q = h / R;
-  const int L = Ns * R;
-  const int tstride = n / L;
-  for (int w = threadIdx.x; w < V * q; w += blockDim.x) {
-    int v = w / q, j = w - v * q;
-    const double2 *s = src + v * ldc;
-    double2 *d = dst + v * ldc;
-    int k = j % Ns;
-    double2 x[R];
-#pragma unroll
-    for (int r = 0; r < R; r++) x[r] = s[j + r * q];
-    if (k) {
-#pragma unroll
-      for (int r = 1; r < R; r++) {
-        double2 t = __ldg(&tw[r * k * tstride]);
-        x[r] = cmul(x[r], FWD ? t : cconj(t));
-      }
-    }
-    if (R == 8) dft8<FWD>(x);
-    if (R == 4) dft4<FWD>(x[0], x[1], x[2], x[3]);
-    if (R == 2) dft2<FWD>(x);
-    int idxD = (j / Ns) * L + k;
-#pragma unroll
-    for (int r = 0; r < R; r++) d[idxD + r * Ns] = x[r];
-  }
-}
-
-// Complex FFT of length h = 2^logh on V vectors, ping-ponging a <-> b.
-// Returns the buffer holding the result.
-template <bool FWD>
-__device__ double2 *complex_fft(double2 *a, double2 *b, int V, int h, int ldc, int logh,
-                                const double2 *__restrict__ tw, int n) {
-  int Ns = 1;
-  int rem = logh;
-  while (rem > 0) {
-    if (rem >= 3) {
-      stockham_pass<8, FWD>(a, b, V, h, ldc, Ns, tw, n);
-      Ns *= 8;
-      rem -= 3;
-    } else if (rem == 2) {
-      stockham_pass<4, FWD>(a, b, V, h, ldc, Ns, tw, n);
-      Ns *= 4;
-      rem -= 2;
-    } else {
-      stockham_pass<2, FWD>(a, b, V, h, ldc, Ns, tw, n);
-      Ns *= 2;
-      rem -= 1;
-    }
-    __syncthreads();
-    double2 *t = a;
-    a = b;
-    b = t;
-  }
-  return a;
-}
-
 // Plain strided load / store functors: element (b, v, j) at p[b*bs + v*vs + j*es].
 struct LoadStrided {
   __host__ double bytes() const { return 8.0; }
@@ -151,113 +92,261 @@ struct StoreStrided {
   }
 };
 
-// The kernel: grid (nvec / V, batch).  LVF / SVF: whether consecutive vectors
-// (true) or consecutive elements (false) are adjacent in global memory for
-// the load / the store, which sets the thread mapping for coalescing.
-template <int V, bool FWD, bool LVF, bool SVF, class LD, class ST>
-__global__ void __launch_bounds__(256) k_rfft(LD ld, ST st, const double2 *__restrict__ tw, int n,
-                                              int logh) {
-  extern __shared__ double2 smem[];
-  const int h = n >> 1;
-  const int ldc = h + 1;           // padded vector stride (complex units)
-  const int ldr = 2 * ldc;         // same stride in doubles
-  double2 *bufA = smem;
-  double2 *bufB = smem + V * ldc;
-  double *rA = reinterpret_cast<double *>(bufA);
-  const int v0 = blockIdx.x * V;
-  const int b = blockIdx.y;
+// ---------------------------------------------------------------------------
+// Register-resident transform.  Each vector of complex length H = 2^LOGH is
+// handled by H/8 threads holding 8 complex values each; a radix-8 (or the
+// final radix-4/2) butterfly runs in registers and only the exchange between
+// passes goes through one shared slot per vector, so shared traffic is a
+// single write + read per pass instead of a ping-pong of whole buffers.
+// Where global memory is element-contiguous (LVF / SVF false) the loads and
+// stores go straight between registers and HBM, coalesced across the
+// vector's threads; vector-fastest layouts are staged through shared memory
+// with lanes running over vectors.
+//
+// Register convention: before and after every pass thread t holds
+// x[m] = Z[t + m*TPV], m = 0..7 (TPV = H/8).  A radix-R pass applies 8/R
+// butterflies j = t + m*TPV on x[m + r*(8/R)], r = 0..R-1, which are exactly
+// the Stockham inputs j + r*H/R; for the last pass (Ns*R = H) the outputs
+// j + r*Ns land back in the same slots, so only earlier passes scatter.
+// Padded position of complex element i within a slot: one spare element per
+// eight keeps the stride-8 scatter of the first pass conflict-free.
+__device__ __forceinline__ int cpad(int i) { return i + (i >> 3); }
+__device__ __forceinline__ int dpos(int j) { return 2 * cpad(j >> 1) + (j & 1); }
 
-  // Global -> shared, four independent loads in flight per thread.
-  constexpr int U = 4;
-  for (int base = threadIdx.x; base < V * n; base += U * blockDim.x) {
-    double r[U];
-    int off[U];
+template <int LOGH>
+struct RfftShape {
+  static constexpr int H = 1 << LOGH;
+  static constexpr int N = 2 * H;
+  static constexpr int TPV = H / 8;
+  static constexpr int VS = H + H / 8 + 1;  // complex stride between slots
+  static constexpr int V = (256 / TPV) < N ? (256 / TPV) : N;  // vectors per CTA
+  static constexpr int NT = V * TPV;        // threads per CTA
+  static constexpr int P8 = LOGH / 3;       // radix-8 passes
+  static constexpr int REM = LOGH % 3;      // final radix-4 (2) or radix-2 (1) pass
+  // forward transforms with a vector-fastest store stage their output in a
+  // second region, so the untangle can emit while other threads still read Z
+  static constexpr size_t smem(bool fwd_svf) {
+    return (size_t)(fwd_svf ? 2 : 1) * V * VS * sizeof(double2);
+  }
+};
+
+template <int R, bool FWD, int TPV>
+__device__ __forceinline__ void rf_butterflies(double2 (&x)[8], int t, int Ns,
+                                               const double2 *__restrict__ tw, int n) {
+  constexpr int NB = 8 / R;
 #pragma unroll
-    for (int q = 0; q < U; q++) {
-      int idx = base + q * blockDim.x;
-      off[q] = -1;
-      if (idx < V * n) {
-        int v, j;
-        if (LVF) { v = idx % V; j = idx / V; } else { v = idx / n; j = idx - (idx / n) * n; }
-        r[q] = ld(b, v0 + v, j);
-        off[q] = v * ldr + j;
+  for (int m = 0; m < NB; m++) {
+    double2 y[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) y[r] = x[m + r * NB];
+    const int j = t + m * TPV;
+    const int k = j & (Ns - 1);
+    if (k) {
+      const int ts = n / (Ns * R);
+#pragma unroll
+      for (int r = 1; r < R; r++) {
+        double2 w = __ldg(&tw[r * k * ts]);
+        y[r] = cmul(y[r], FWD ? w : cconj(w));
       }
     }
+    if (R == 8) dft8<FWD>(y);
+    if (R == 4) dft4<FWD>(y[0], y[1], y[2], y[3]);
+    if (R == 2) dft2<FWD>(y);
 #pragma unroll
-    for (int q = 0; q < U; q++)
-      if (off[q] >= 0) rA[off[q]] = r[q];
+    for (int r = 0; r < R; r++) x[m + r * NB] = y[r];
   }
-  __syncthreads();
+}
 
-  if (FWD) {
-    double2 *Z = complex_fft<true>(bufA, bufB, V, h, ldc, logh, tw, n);
-    double *out = reinterpret_cast<double *>(Z == bufA ? bufB : bufA);
-    const double s = 1.0 / sqrt((double)n);
-    const int hh = h / 2;
-    for (int w = threadIdx.x; w < V * (hh + 1); w += blockDim.x) {
-      int v = w / (hh + 1), k = w - v * (hh + 1);
-      const double2 *z = Z + v * ldc;
-      double *o = out + v * ldr;
-      if (k == 0) {
-        double2 z0 = z[0];
-        o[0] = (z0.x + z0.y) * s;
-        o[h] = (z0.x - z0.y) * s;
-      } else {
-        // pair (k, h-k)
-        for (int pass = 0; pass < 2; pass++) {
-          int kk = pass == 0 ? k : h - k;
-          if (pass == 1 && kk == k) break;
-          double2 zk = z[kk], zc = cconj(z[h - kk]);
-          double2 e = make_double2(0.5 * (zk.x + zc.x), 0.5 * (zk.y + zc.y));
-          double2 d = csub(zk, zc);
-          double2 od = make_double2(0.5 * d.y, -0.5 * d.x);  // (Z - conj Zc)/(2i)
-          double2 f = cadd(e, cmul(__ldg(&tw[kk]), od));
-          o[kk] = f.x * s;
-          o[n - kk] = f.y * s;
-        }
+// All passes of the complex FFT; x holds Z[t + m*TPV] on entry and on exit.
+// S is this vector's slot; the caller has synchronised after its last read
+// of shared memory.
+template <int LOGH, bool FWD>
+__device__ __forceinline__ void rf_complex(double2 (&x)[8], double2 *S, int t,
+                                           const double2 *__restrict__ tw, int n) {
+  using Sh = RfftShape<LOGH>;
+  int Ns = 1;
+#pragma unroll
+  for (int p = 0; p < Sh::P8; p++) {
+    rf_butterflies<8, FWD, Sh::TPV>(x, t, Ns, tw, n);
+    if (p < Sh::P8 - 1 || Sh::REM != 0) {
+      const int base = (t / Ns) * Ns * 8 + (t & (Ns - 1));
+#pragma unroll
+      for (int r = 0; r < 8; r++) S[cpad(base + r * Ns)] = x[r];
+      __syncthreads();
+#pragma unroll
+      for (int m = 0; m < 8; m++) x[m] = S[cpad(t + m * Sh::TPV)];
+      __syncthreads();
+    }
+    Ns *= 8;
+  }
+  if (Sh::REM == 2) rf_butterflies<4, FWD, Sh::TPV>(x, t, Ns, tw, n);
+  if (Sh::REM == 1) rf_butterflies<2, FWD, Sh::TPV>(x, t, Ns, tw, n);
+}
+
+template <int LOGH, bool FWD, bool LVF, bool SVF, class LD, class ST>
+__global__ void __launch_bounds__(RfftShape<LOGH>::NT, 3) k_rfft_r(LD ld, ST st,
+                                                                const double2 *__restrict__ tw) {
+  using Sh = RfftShape<LOGH>;
+  constexpr int H = Sh::H, N = Sh::N, TPV = Sh::TPV, V = Sh::V, NT = Sh::NT, VS = Sh::VS;
+  extern __shared__ double2 smem[];
+  double *Sd = reinterpret_cast<double *>(smem);
+  const int vl = threadIdx.x / TPV, t = threadIdx.x - vl * TPV;
+  const int v0 = blockIdx.x * V, vg = v0 + vl;
+  const int b = blockIdx.y;
+  double2 *S = smem + vl * VS;
+  double *SdV = Sd + 2 * vl * VS;
+  double2 x[8];
+
+  // Vector-fastest input: stage V vectors, lanes over vectors (16 values per
+  // thread, loaded 8 at a time).
+  if (LVF) {
+    constexpr int Q = (V * N) / NT;
+#pragma unroll
+    for (int q0 = 0; q0 < Q; q0 += 8) {
+      double r[8];
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        int idx = threadIdx.x + (q0 + q) * NT;
+        r[q] = ld(b, v0 + (idx % V), idx / V);
+      }
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        int idx = threadIdx.x + (q0 + q) * NT;
+        Sd[2 * (idx % V) * VS + dpos(idx / V)] = r[q];
       }
     }
     __syncthreads();
-    for (int idx = threadIdx.x; idx < V * n; idx += blockDim.x) {
-      int v, k;
-      if (SVF) { v = idx % V; k = idx / V; } else { v = idx / n; k = idx - (idx / n) * n; }
-      st(b, v0 + v, k, out[v * ldr + k]);
+  }
+
+  if (FWD) {
+    if (LVF) {
+#pragma unroll
+      for (int m = 0; m < 8; m++) x[m] = S[cpad(t + m * TPV)];
+      __syncthreads();
+    } else {
+#pragma unroll
+      for (int m = 0; m < 8; m++) {
+        int e = t + m * TPV;
+        x[m] = make_double2(ld(b, vg, 2 * e), ld(b, vg, 2 * e + 1));
+      }
+    }
+    rf_complex<LOGH, true>(x, S, t, tw, N);
+    // untangle: pairs (k, H-k) live in threads t and TPV-t, so exchange once
+#pragma unroll
+    for (int m = 0; m < 8; m++) S[cpad(t + m * TPV)] = x[m];
+    __syncthreads();
+    const double s = 1.0 / sqrt((double)N);
+    double *Out = Sd + 2 * V * VS + 2 * vl * VS;  // forward + SVF staging region
+    auto emit = [&](int k, double val) {
+      if (SVF) Out[dpos(k)] = val; else st(b, vg, k, val);
+    };
+    auto pair_out = [&](int kk) {
+      double2 zk = S[cpad(kk)], zc = cconj(S[cpad(H - kk)]);
+      double2 e = make_double2(0.5 * (zk.x + zc.x), 0.5 * (zk.y + zc.y));
+      double2 d = csub(zk, zc);
+      double2 od = make_double2(0.5 * d.y, -0.5 * d.x);  // (Z - conj Zc)/(2i)
+      double2 f = cadd(e, cmul(__ldg(&tw[kk]), od));
+      emit(kk, f.x * s);
+      emit(N - kk, f.y * s);
+    };
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+      const int k = t + m * TPV;
+      if (k == 0) {
+        double2 z0 = S[0];
+        emit(0, (z0.x + z0.y) * s);
+        emit(H, (z0.x - z0.y) * s);
+      } else {
+        pair_out(k);
+        pair_out(H - k);
+      }
+    }
+    if (t == 0) pair_out(H / 2);  // k = H/2 pairs with itself
+    if (SVF) {
+      __syncthreads();
+      constexpr int Q = (V * N) / NT;
+      const double *O = Sd + 2 * V * VS;
+#pragma unroll
+      for (int q = 0; q < Q; q++) {
+        int idx = threadIdx.x + q * NT;
+        int vv = idx % V, k = idx / V;
+        st(b, v0 + vv, k, O[2 * vv * VS + dpos(k)]);
+      }
     }
   } else {
-    // Hermitian -> Z (even/odd packing), then inverse complex FFT.
-    const int hh = h / 2;
-    for (int w = threadIdx.x; w < V * (hh + 1); w += blockDim.x) {
-      int v = w / (hh + 1), k = w - v * (hh + 1);
-      const double *x = rA + v * ldr;
-      double2 *z = bufB + v * ldc;
+    // Hermitian -> Z (even/odd packing): thread t forms Z at k and H-k for
+    // k = t + m*TPV (m < 4), thread 0 also k = H/2.
+    auto X = [&](int j) -> double { return LVF ? SdV[dpos(j)] : ld(b, vg, j); };
+    double2 zp[9];
+    int zk[9];
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+      const int k = t + m * TPV;
       if (k == 0) {
-        double F0 = x[0], Fh = x[h];
-        z[0] = make_double2(0.5 * (F0 + Fh), 0.5 * (F0 - Fh));
+        double F0 = X(0), Fh = X(H);
+        zp[2 * m] = make_double2(0.5 * (F0 + Fh), 0.5 * (F0 - Fh));
+        zk[2 * m] = 0;
+        zk[2 * m + 1] = -1;
+        zp[2 * m + 1] = make_double2(0.0, 0.0);
       } else {
+        const double a = X(k), bq = X(N - k), c = X(H - k), dq = X(N - (H - k));
+#pragma unroll
         for (int pass = 0; pass < 2; pass++) {
-          int kk = pass == 0 ? k : h - k;
-          if (pass == 1 && kk == k) break;
-          double2 F = make_double2(x[kk], x[n - kk]);
-          double2 G = make_double2(x[h - kk], -x[n - (h - kk)]);  // conj F(h-kk)
+          const int kk = pass == 0 ? k : H - k;
+          double2 F = pass == 0 ? make_double2(a, bq) : make_double2(c, dq);
+          double2 G = pass == 0 ? make_double2(c, -dq) : make_double2(a, -bq);  // conj F(H-kk)
           double2 e = make_double2(0.5 * (F.x + G.x), 0.5 * (F.y + G.y));
           double2 d = make_double2(0.5 * (F.x - G.x), 0.5 * (F.y - G.y));
           double2 o = cmul(d, cconj(__ldg(&tw[kk])));
-          z[kk] = make_double2(e.x - o.y, e.y + o.x);
+          zp[2 * m + pass] = make_double2(e.x - o.y, e.y + o.x);
+          zk[2 * m + pass] = kk;
         }
       }
     }
+    if (t == 0) {
+      const int kk = H / 2;
+      double2 F = make_double2(X(kk), X(N - kk));
+      double2 G = make_double2(X(H - kk), -X(N - (H - kk)));
+      double2 e = make_double2(0.5 * (F.x + G.x), 0.5 * (F.y + G.y));
+      double2 d = make_double2(0.5 * (F.x - G.x), 0.5 * (F.y - G.y));
+      double2 o = cmul(d, cconj(__ldg(&tw[kk])));
+      zp[8] = make_double2(e.x - o.y, e.y + o.x);
+      zk[8] = kk;
+    } else {
+      zk[8] = -1;
+      zp[8] = make_double2(0.0, 0.0);
+    }
+    if (LVF) __syncthreads();  // staged input fully read before Z overwrites it
+#pragma unroll
+    for (int q = 0; q < 9; q++)
+      if (zk[q] >= 0) S[cpad(zk[q])] = zp[q];
     __syncthreads();
-    double2 *Z = complex_fft<false>(bufB, bufA, V, h, ldc, logh, tw, n);
-    const double *out = reinterpret_cast<const double *>(Z);
-    const double s = 2.0 / sqrt((double)n);
-    for (int idx = threadIdx.x; idx < V * n; idx += blockDim.x) {
-      int v, k;
-      if (SVF) { v = idx % V; k = idx / V; } else { v = idx / n; k = idx - (idx / n) * n; }
-      st(b, v0 + v, k, out[v * ldr + k] * s);
+#pragma unroll
+    for (int m = 0; m < 8; m++) x[m] = S[cpad(t + m * TPV)];
+    __syncthreads();
+    rf_complex<LOGH, false>(x, S, t, tw, N);
+    const double s = 2.0 / sqrt((double)N);
+    if (!SVF) {
+#pragma unroll
+      for (int m = 0; m < 8; m++) {
+        int e = t + m * TPV;
+        st(b, vg, 2 * e, x[m].x * s);
+        st(b, vg, 2 * e + 1, x[m].y * s);
+      }
+    } else {
+#pragma unroll
+      for (int m = 0; m < 8; m++) S[cpad(t + m * TPV)] = x[m];
+      __syncthreads();
+      constexpr int Q = (V * N) / NT;
+#pragma unroll
+      for (int q = 0; q < Q; q++) {
+        int idx = threadIdx.x + q * NT;
+        int vv = idx % V, k = idx / V;
+        st(b, v0 + vv, k, Sd[2 * vv * VS + dpos(k)] * s);
+      }
     }
   }
 }
 
-inline size_t rfft_smem_bytes(int V, int n) { return (size_t)2 * V * (n / 2 + 1) * sizeof(double2); }
 
 }  // namespace casl

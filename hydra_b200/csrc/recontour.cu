@@ -811,6 +811,7 @@ int recontour_dev(casl_handle *h, const double *qq) {
   int *dtot = ar.get<int>(16);
   if (ar.failed) return CASL_ENOMEM;
   CASL_K(k_cr_count, gsz(nchunks), 256, 0, st)(qa, li, nxu, nyu, nchunks, ccnt);
+  tr.point("cr_count");
   exclusive_scan<int>(st, ccnt, coffs, nchunks, tmpi, dtot);
   int ncr_i = 0;
   CASL_CUDA_TRY(cudaMemcpyAsync(&ncr_i, dtot, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -839,11 +840,14 @@ int recontour_dev(casl_handle *h, const double *qq) {
   int *tmpi2 = ar2.get<int>(scan_tmp_elems(ncr) + 4);
   void *sort_tmp = ar2.get<char>(sort_bytes + 16);
   if (ar2.failed) return CASL_ENOMEM;
+  tr.point("cr_alloc");
   CASL_K(k_cr_emit, gsz(nchunks), 256, 0, st)(qa, li, nxu, nyu, nchunks, coffs, redge, rlev);
+  tr.point("cr_emit");
   CASL_CUDA_TRY(cub::DeviceRadixSort::SortPairs(sort_tmp, sort_bytes, rlev, rlev2, redge, redge2,
                                                 (int)ncr, 0, endbit, st));
   std::swap(rlev, rlev2);
   std::swap(redge, redge2);
+  tr.point("cr_sort");
   double *xcr = ar2.get<double>(ncr), *ycr = ar2.get<double>(ncr);
   unsigned int *kib = ar2.get<unsigned int>(ncr), *kob = ar2.get<unsigned int>(ncr);
   if (ar2.failed) return CASL_ENOMEM;

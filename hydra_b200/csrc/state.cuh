@@ -73,9 +73,9 @@ int ptospc_dev(casl_handle *h, const double *phys, double *spec);
 // spctop: spec -> phys using tmp (n*n); spec is preserved.
 int spctop_dev(casl_handle *h, const double *spec, double *phys, double *tmp);
 
-int con2grid_dev(casl_handle *h);                   // -> coarseC, scal->csum
+int con2grid_dev(casl_handle *h, bool want_levels);  // -> coarseC, scal->csum
 int con2grid_to_spec(casl_handle *h, double *spec); // con2grid + ptospc fused load
-int con2grid_to_phys(casl_handle *h, double *phys); // con2grid + finalize to qc(ny,nx)
+int con2grid_to_phys(casl_handle *h, double *phys, bool want_levels);  // -> qc(ny,nx)
 
 int surgery_dev(casl_handle *h);
 int recontour_dev(casl_handle *h, const double *qq_dev);

@@ -486,36 +486,58 @@ __global__ void k_rb_runs(const int *__restrict__ st, const int *__restrict__ br
 
 
 
-// All run-level cycle work in one block: min-label and list-ranking pointer
-// jumping over the R runs (R is small: contours plus a few per
-// reconnection), rounds separated by block barriers.
+// All run-level cycle work in one block.  A contour no reconnection touched
+// is a single run that points to itself and is finished at once; pointer
+// jumping (min label, then list ranking) runs over the few remaining runs
+// only, rounds separated by block barriers.
 __global__ void __launch_bounds__(1024) k_rb_cycles_block(
     const int *__restrict__ nextq, const int *__restrict__ rid, const int *__restrict__ rs,
     const int *__restrict__ re, const int *__restrict__ R_dev, int *__restrict__ nr,
     int *lab, int *lab2, int *nrj, int *nrj2, int *__restrict__ hr, int *succ, int *succ2,
-    long long *val, long long *val2, int *__restrict__ ishead, long long **valout) {
+    long long *val, long long *val2, int *__restrict__ ishead, int *__restrict__ multi,
+    long long **valout) {
+  __shared__ int nmulti;
   const int R = *R_dev;
+  if (threadIdx.x == 0) nmulti = 0;
+  __syncthreads();
   for (int r = threadIdx.x; r < R; r += blockDim.x) {
     int t = rid[nextq[re[r]]];
     nr[r] = t;
-    nrj[r] = t;
-    lab[r] = rs[r];
+    long long len = re[r] - rs[r] + 1;
+    if (t == r) {  // a whole contour
+      lab[r] = rs[r];
+      hr[r] = r;
+      ishead[r] = 1;
+      val[r] = len;
+      val2[r] = len;
+    } else {
+      nrj[r] = t;
+      lab[r] = rs[r];
+      multi[atomicAdd(&nmulti, 1)] = r;
+    }
   }
   __syncthreads();
+  const int M = nmulti;
   int rounds = 1;
-  while ((1 << rounds) < R) rounds++;
+  while ((1 << rounds) < M) rounds++;
   rounds++;
-  for (int it = 0; it < rounds; it++) {
-    for (int r = threadIdx.x; r < R; r += blockDim.x) {
+  for (int it = 0; it < rounds && M > 0; it++) {
+    for (int q = threadIdx.x; q < M; q += blockDim.x) {
+      int r = multi[q];
       int n = nrj[r];
       lab2[r] = min(lab[r], lab[n]);
       nrj2[r] = nrj[n];
     }
     __syncthreads();
-    int *t1 = lab; lab = lab2; lab2 = t1;
-    int *t2 = nrj; nrj = nrj2; nrj2 = t2;
+    for (int q = threadIdx.x; q < M; q += blockDim.x) {
+      int r = multi[q];
+      lab[r] = lab2[r];
+      nrj[r] = nrj2[r];
+    }
+    __syncthreads();
   }
-  for (int r = threadIdx.x; r < R; r += blockDim.x) {
+  for (int q = threadIdx.x; q < M; q += blockDim.x) {
+    int r = multi[q];
     int h = rid[lab[r]];
     hr[r] = h;
     succ[r] = nr[r] == h ? -1 : nr[r];
@@ -523,17 +545,22 @@ __global__ void __launch_bounds__(1024) k_rb_cycles_block(
     ishead[r] = h == r;
   }
   __syncthreads();
-  for (int it = 0; it < rounds; it++) {
-    for (int r = threadIdx.x; r < R; r += blockDim.x) {
+  for (int it = 0; it < rounds && M > 0; it++) {
+    for (int q = threadIdx.x; q < M; q += blockDim.x) {
+      int r = multi[q];
       int sc = succ[r];
       val2[r] = val[r] + (sc >= 0 ? val[sc] : 0);
       succ2[r] = sc >= 0 ? succ[sc] : -1;
     }
     __syncthreads();
-    long long *t3 = val; val = val2; val2 = t3;
-    int *t4 = succ; succ = succ2; succ2 = t4;
+    for (int q = threadIdx.x; q < M; q += blockDim.x) {
+      int r = multi[q];
+      val[r] = val2[r];
+      succ[r] = succ2[r];
+    }
+    __syncthreads();
   }
-  if (threadIdx.x == 0) *valout = val;  // whichever buffer holds the result
+  if (threadIdx.x == 0) *valout = val;
 }
 
 __global__ void k_rb_cycles2(const int *__restrict__ ishead, const int *__restrict__ cidx,
@@ -624,6 +651,7 @@ static int rebuild_and_renode(casl_handle *h, Arena &ar, int npt, const int *lvl
   int *succ2 = ar.get<int>(npt), *ishead = ar.get<int>(npt), *cidx = ar.get<int>(npt);
   long long *val = ar.get<long long>(npt), *val2 = ar.get<long long>(npt);
   long long **valp = ar.get<long long *>(1);
+  int *multi = ar.get<int>(npt);
   // cycles (C <= R <= npt)
   int *clen = ar.get<int>(npt), *clev = ar.get<int>(npt), *cst = ar.get<int>(npt);
   double *xw = ar.get<double>(npt), *yw = ar.get<double>(npt);
@@ -637,7 +665,7 @@ static int rebuild_and_renode(casl_handle *h, Arena &ar, int npt, const int *lvl
   CASL_CUDA_TRY(cudaMemsetAsync(ishead, 0, (size_t)npt * sizeof(int), st));
   CASL_CUDA_TRY(cudaMemsetAsync(clen, 0, (size_t)npt * sizeof(int), st));
   CASL_K(k_rb_cycles_block, 1, 1024, 0, st)(h->nextq, rid, rs, re, dtot, nr, lab, lab2, nrj, nrj2,
-                                            hr, succ, succ2, val, val2, ishead, valp);
+                                            hr, succ, succ2, val, val2, ishead, multi, valp);
   exclusive_scan<int>(st, ishead, cidx, npt, tmpi, dtot + 1);  // dtot[1] = C
   CASL_K(k_rb_cycles2, g, 256, 0, st)(ishead, cidx, valp, rs, lvl, dlev, dtot, clen, clev);
   exclusive_scan<int>(st, clen, cst, npt, tmpi, dtot + 2);
