@@ -80,6 +80,8 @@ SIGNATURES = {
     "casl_initialise": (C.c_int, [C.c_void_p, _dp]),
     "casl_step": (C.c_int, [C.c_void_p, C.c_int]),
     "casl_diagnostics": (C.c_int, [C.c_void_p, _dp]),
+    "casl_spec1d": (C.c_int, [C.c_void_p, _dp, _dp, C.c_int]),
+    "casl_spec_tables": (C.c_int, [C.c_void_p, _ip, _ip, _dp, _dp]),
     "casl_con2grid_noalloc": (C.c_int, [C.c_int, C.c_double, C.c_double, C.c_int, C.c_double,
                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "casl_get_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
@@ -288,3 +290,19 @@ class CaslGPU:
         out = np.zeros(4)
         self._check(self.lib.casl_diagnostics(self.h, _d(out)), "casl_diagnostics")
         return dict(ekin=out[0], epot=out[1], enstrophy=out[2], circulation=out[3])
+
+    def spec1d(self, ss, iopt=0):
+        """spec1d (spectral.f90:370-424) of the spectral field ss(nx,ny), given
+        as an (ny, nx) array; returns (spec[0..n], ss after the call)."""
+        a = np.ascontiguousarray(ss, dtype=np.float64).copy()
+        spec = np.zeros(self.nx + 1)
+        self._check(self.lib.casl_spec1d(self.h, _d(a), _d(spec), int(iopt)), "casl_spec1d")
+        return spec, a
+
+    def spec_tables(self):
+        """kmax, kmaxred, spmf, alk of init_spectral (spectral.f90:109-134)."""
+        kmax, kred = C.c_int(), C.c_int()
+        spmf, alk = np.zeros(self.nx + 1), np.zeros(self.nx + 1)
+        self._check(self.lib.casl_spec_tables(self.h, C.byref(kmax), C.byref(kred), _d(spmf), _d(alk)),
+                    "casl_spec_tables")
+        return dict(kmax=kmax.value, kmaxred=kred.value, spmf=spmf, alk=alk)

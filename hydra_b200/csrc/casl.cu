@@ -42,7 +42,7 @@ int check_launch(casl_handle *h) {
 // One batched transform pass (all vectors of `batch` fields along one axis).
 template <int LOGH, bool FWD, bool LVF, bool SVF, class LD, class ST>
 static int launch_rfft(casl_handle *h, LD ld, ST st, int batch) {
-  using Sh = RfftShape<LOGH>;
+  using Sh = RfftShape<LOGH, LVF || SVF>;
   dim3 grid(Sh::N / Sh::V, batch);
   const bool prof = h->prof_class == CASL_PROF_FFT && h->prof_ev && h->prof_n < CASL_PROF_MAX;
   if (prof) cudaEventRecord(h->prof_ev[2 * h->prof_n], h->stream);
@@ -78,24 +78,32 @@ static int rfft_dispatch(casl_handle *h, LD ld, ST st, int batch) {
 }
 #define RFFT_DISPATCH(FWD, LVF, SVF, ld, st, batch) rfft_dispatch<FWD, LVF, SVF>(h, ld, st, batch)
 
+// A 2-D transform is separable, so each one takes the axis whose vectors are
+// contiguous first: forward transforms run along iy (phys columns, vector v =
+// ix) and then along ix (rows of the intermediate, v = ky); inverse ones run
+// along kx (spectral rows, v = ky) and then along ky (v = ix).  Only one of
+// the four global sides is vector-fastest.  The intermediate of both is
+// T[ky*n + ix].  The order of the axes changes results by rounding only.
 int ptospc_dev(casl_handle *h, const double *phys, double *spec) {
   long long n = h->n, nn = n * n;
-  // pass A: along ix for each iy; phys[ix*n+iy] -> spec[iy*n+kx] (transposed)
-  int rc = RFFT_DISPATCH(true, true, false, (LoadStrided{phys, nn, 1, n}),
-                         (StoreStrided{spec, nn, n, 1}), 1);
+  // along iy for each ix: phys[ix*n+iy] -> spec[ky*n+ix] (spec != phys)
+  int rc = RFFT_DISPATCH(true, false, true, (LoadStrided{phys, nn, n, 1}),
+                         (StoreStrided{spec, nn, 1, n}), 1);
   if (rc) return rc;
-  // pass B: along iy for each kx, in place: spec[j*n + kx]
-  return RFFT_DISPATCH(true, true, true, (LoadStrided{spec, nn, 1, n}),
-                       (StoreStrided{spec, nn, 1, n}), 1);
+  // along ix for each ky, in place by rows: spec[ky*n + kx]
+  return RFFT_DISPATCH(true, false, false, (LoadStrided{spec, nn, n, 1}),
+                       (StoreStrided{spec, nn, n, 1}), 1);
 }
 
 int spctop_dev(casl_handle *h, const double *spec, double *phys, double *tmp) {
   long long n = h->n, nn = n * n;
-  int rc = RFFT_DISPATCH(false, true, true, (LoadStrided{spec, nn, 1, n}),
-                         (StoreStrided{tmp, nn, 1, n}), 1);
+  // along kx for each ky: spec[ky*n+kx] -> tmp[ky*n+ix]
+  int rc = RFFT_DISPATCH(false, false, false, (LoadStrided{spec, nn, n, 1}),
+                         (StoreStrided{tmp, nn, n, 1}), 1);
   if (rc) return rc;
-  return RFFT_DISPATCH(false, false, true, (LoadStrided{tmp, nn, n, 1}),
-                       (StoreStrided{phys, nn, 1, n}), 1);
+  // along ky for each ix: tmp[ky*n+ix] -> phys[ix*n+iy]
+  return RFFT_DISPATCH(false, true, false, (LoadStrided{tmp, nn, 1, n}),
+                       (StoreStrided{phys, nn, n, 1}), 1);
 }
 
 // ---------------------------------------------------------------------------
@@ -117,16 +125,17 @@ struct LoadDeriv {
     double v = f[b][k];
     return green ? green[k] * v : v;
   }
+  // first pass of an inverse transform: vector v = ky, element j = kx
   __device__ __forceinline__ double operator()(int b, int v, int j) const {
-    const int nw = n >> 1;
+    const int nw = n >> 1, kx = j, ky = v;
     if (dir[b] == 0) {
-      if (v == 0 || v == nw) return 0.0;
-      if (v < nw) return -hrkx[2 * v - 1] * base(b, n - v, j);
-      return hrkx[2 * (n - v) - 1] * base(b, n - v, j);
+      if (kx == 0 || kx == nw) return 0.0;
+      if (kx < nw) return -hrkx[2 * kx - 1] * base(b, n - kx, ky);
+      return hrkx[2 * (n - kx) - 1] * base(b, n - kx, ky);
     } else {
-      if (j == 0 || j == nw) return 0.0;
-      if (j < nw) return -hrky[2 * j - 1] * base(b, v, n - j);
-      return hrky[2 * (n - j) - 1] * base(b, v, n - j);
+      if (ky == 0 || ky == nw) return 0.0;
+      if (ky < nw) return -hrky[2 * ky - 1] * base(b, kx, n - ky);
+      return hrky[2 * (n - ky) - 1] * base(b, kx, n - ky);
     }
   }
 };
@@ -141,11 +150,11 @@ struct LoadQC {
   long long nn;
   double inv;           // 1/(256 n^2)
   int n;
-  __device__ __forceinline__ double operator()(int b, int v /*iy*/, int j /*ix*/) const {
-    long long k = (long long)j * n + v;
+  __device__ __forceinline__ double operator()(int b, int v /*ix*/, int j /*iy*/) const {
+    long long k = (long long)v * n + j;
     long long num = (long long)C[k] * nn - s->csum;
     double q = s->qjump * ((double)num * inv);
-    if (betac) q = q + betac[v];
+    if (betac) q = q + betac[j];
     return q;
   }
 };
@@ -158,8 +167,8 @@ struct LoadAdvect {
   const double *fx[2], *fy[2];
   double betab[2];  // beta added to fy for the qs term when beffect
   int n;
-  __device__ __forceinline__ double operator()(int b, int v /*iy*/, int j /*ix*/) const {
-    long long k = (long long)j * n + v;
+  __device__ __forceinline__ double operator()(int b, int v /*ix*/, int j /*iy*/) const {
+    long long k = (long long)v * n + j;
     double gx = fx[b][k], gy = fy[b][k];
     if (betab[b] != 0.0) gy = gy + betab[b];
     return -uu[k] * gx - vv[k] * gy;
@@ -174,8 +183,8 @@ struct StoreSource {
   const double *qq, *pp, *epq;
   double rekman, kdsq, therm;
   int heating, friction, lev, n;
-  __device__ __forceinline__ void operator()(int b, int v /*kx*/, int k /*ky*/, double x) const {
-    long long idx = (long long)k * n + v;
+  __device__ __forceinline__ void operator()(int b, int v /*ky*/, int k /*kx*/, double x) const {
+    long long idx = (long long)v * n + k;
     if (b == 1) {
       sqs[idx] = x;
       return;
@@ -202,8 +211,9 @@ struct StoreScaled {
   double *p[4];
   double scale[4];
   int n;
+  // last pass of an inverse transform: vector v = ix, element k = iy
   __device__ __forceinline__ void operator()(int b, int v, int k, double x) const {
-    p[b][(long long)k * n + v] = scale[b] == 1.0 ? x : scale[b] * x;
+    p[b][(long long)v * n + k] = scale[b] == 1.0 ? x : scale[b] * x;
   }
 };
 struct LoadBatch {
@@ -220,8 +230,9 @@ struct LoadVort {
   const double *qq, *pp;
   double kdsq;
   int btropic, n;
+  // first pass of an inverse transform: vector v = ky, element j = kx
   __device__ __forceinline__ double operator()(int b, int v, int j) const {
-    long long k = (long long)j * n + v;
+    long long k = (long long)v * n + j;
     return btropic ? qq[k] : qq[k] + kdsq * pp[k];
   }
 };
@@ -489,13 +500,21 @@ __global__ void __launch_bounds__(1024) k_c2g_fused(const int *__restrict__ J, i
 
 __global__ void k_zero_csum(Scalars *s) { s->csum = 0; }
 
+// c = a * b elementwise
+__global__ void k_mul2(const double *__restrict__ a, const double *__restrict__ b,
+                       double *__restrict__ c, long long nn) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nn;
+       k += (long long)gridDim.x * blockDim.x)
+    c[k] = a[k] * b[k];
+}
+
 __global__ void k_c2g_final(const int *__restrict__ C, const Scalars *__restrict__ s,
                             const double *__restrict__ betac, double *__restrict__ qc, int n) {
   LoadQC ld{C, s, betac, (long long)n * n, 1.0 / (256.0 * (double)n * (double)n), n};
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)n * n;
        t += (long long)gridDim.x * blockDim.x) {
     int iy = (int)(t % n), ix = (int)(t / n);
-    qc[t] = ld(0, iy, ix);
+    qc[t] = ld(0, ix, iy);
   }
 }
 
@@ -542,10 +561,10 @@ int con2grid_to_spec(casl_handle *h, double *spec) {
   if (rc) return rc;
   LoadQC ld{h->coarseC, h->scal, h->c.beffect ? h->betac : nullptr, nn,
             1.0 / (256.0 * (double)n * (double)n), (int)n};
-  rc = RFFT_DISPATCH(true, true, false, ld, (StoreStrided{spec, nn, n, 1}), 1);
+  rc = RFFT_DISPATCH(true, false, true, ld, (StoreStrided{spec, nn, 1, n}), 1);
   if (rc) return rc;
-  return RFFT_DISPATCH(true, true, true, (LoadStrided{spec, nn, 1, n}),
-                       (StoreStrided{spec, nn, 1, n}), 1);
+  return RFFT_DISPATCH(true, false, false, (LoadStrided{spec, nn, n, 1}),
+                       (StoreStrided{spec, nn, n, 1}), 1);
 }
 
 int con2grid_to_phys(casl_handle *h, double *phys, bool want_levels) {
@@ -820,24 +839,24 @@ static int inversion_dev(casl_handle *h, bool reset) {
   ld.dir[0] = 0; ld.dir[1] = 1;
   ld.green = h->green; ld.hrkx = h->hrkx; ld.hrky = h->hrky; ld.n = h->n;
   long long n = h->n;
-  rc = RFFT_DISPATCH(false, true, true, ld, (StoreStrided{h->w[0], nn, 1, n}), 2);
+  rc = RFFT_DISPATCH(false, false, false, ld, (StoreStrided{h->w[0], nn, n, 1}), 2);
   if (rc) return rc;
   StoreScaled st{};
   st.p[0] = h->vv; st.p[1] = h->uu;
   st.scale[0] = 1.0; st.scale[1] = -1.0; st.n = h->n;
-  // pass B reads tmp (v = iy, j = kx contiguous) and writes phys [ix][iy]
+  // second pass reads tmp[ky*n + ix] (v = ix fastest, j = ky) and writes phys [ix][iy]
   LoadBatch lb{};
-  lb.p[0] = h->w[0]; lb.p[1] = h->w[0] + nn; lb.vs = n; lb.es = 1;
-  return RFFT_DISPATCH(false, false, true, lb, st, 2);
+  lb.p[0] = h->w[0]; lb.p[1] = h->w[0] + nn; lb.vs = 1; lb.es = n;
+  return RFFT_DISPATCH(false, true, false, lb, st, 2);
 }
 
 static int adapt_dev(casl_handle *h) {
   long long nn = (long long)h->n * h->n, n = h->n;
   LoadVort lv{h->qq, h->pp, h->c.kdsq, h->c.btropic, h->n};
-  int rc = RFFT_DISPATCH(false, true, true, lv, (StoreStrided{h->w[0], nn, 1, n}), 1);
+  int rc = RFFT_DISPATCH(false, false, false, lv, (StoreStrided{h->w[0], nn, n, 1}), 1);
   if (rc) return rc;
-  rc = RFFT_DISPATCH(false, false, true, (LoadStrided{h->w[0], nn, n, 1}),
-                     (StoreStrided{h->w[1], nn, 1, n}), 1);
+  rc = RFFT_DISPATCH(false, true, false, (LoadStrided{h->w[0], nn, 1, n}),
+                     (StoreStrided{h->w[1], nn, n, 1}), 1);
   if (rc) return rc;
   CASL_K(k_reduce_adapt, RED_BLOCKS, 256, 0, h->stream)(h->w[1], h->uu, h->vv, h->part, nn);
   CASL_K(k_adapt_final, 1, 256, 0, h->stream)(h->part, RED_BLOCKS, h->scal, h->c, h->p.fixed_dt);
@@ -857,31 +876,31 @@ static int source_dev(casl_handle *h, int lev) {
   // tmp for 4 transforms: w[0..3]; outputs gx_qd, gy_qd, gx_qs, gy_qs in w[4], w[5], sqs, sqd
   // (sqs/sqd are free until the products are formed).
   double *tmp = h->w[0];  // w[0..3] contiguous
-  int rc = RFFT_DISPATCH(false, true, true, ld, (StoreStrided{tmp, nn, 1, n}), 4);
+  int rc = RFFT_DISPATCH(false, false, false, ld, (StoreStrided{tmp, nn, n, 1}), 4);
   if (rc) return rc;
   LoadBatch lb{};
   for (int b = 0; b < 4; b++) lb.p[b] = tmp + b * nn;
-  lb.vs = n; lb.es = 1;
+  lb.vs = 1; lb.es = n;
   StoreScaled st{};
   st.p[0] = h->w[4]; st.p[1] = h->w[5]; st.p[2] = h->sqs; st.p[3] = h->sqd;
   for (int b = 0; b < 4; b++) st.scale[b] = 1.0;
   st.n = h->n;
-  rc = RFFT_DISPATCH(false, false, true, lb, st, 4);
+  rc = RFFT_DISPATCH(false, true, false, lb, st, 4);
   if (rc) return rc;
-  // products -> ptospc pass A into tmp (transposed), pass B with the source store
+  // products -> ptospc's first pass into tmp, its second pass with the source store
   LoadAdvect la{};
   la.uu = h->uu; la.vv = h->vv;
   la.fx[0] = h->w[4]; la.fy[0] = h->w[5];
   la.fx[1] = h->sqs; la.fy[1] = h->sqd;
   la.betab[0] = 0.0; la.betab[1] = h->c.beffect ? h->c.beta : 0.0;
   la.n = h->n;
-  rc = RFFT_DISPATCH(true, true, false, la, (StoreStrided{tmp, nn, n, 1}), 2);
+  rc = RFFT_DISPATCH(true, false, true, la, (StoreStrided{tmp, nn, 1, n}), 2);
   if (rc) return rc;
   StoreSource ss{};
   ss.sqd = h->sqd; ss.sqs = h->sqs; ss.qq = h->qq; ss.pp = h->pp; ss.epq = h->epq;
   ss.rekman = h->p.rekman; ss.kdsq = h->c.kdsq; ss.therm = h->c.therm;
   ss.heating = h->c.heating; ss.friction = h->c.friction; ss.lev = lev; ss.n = h->n;
-  return RFFT_DISPATCH(true, true, true, (LoadStrided{tmp, nn, 1, n}), ss, 2);
+  return RFFT_DISPATCH(true, false, false, (LoadStrided{tmp, nn, n, 1}), ss, 2);
 }
 
 }  // namespace casl
@@ -993,8 +1012,10 @@ static void make_consts(const casl_params &p, Consts &c) {
 }
 
 struct HostTables {
-  std::vector<double> green, flo, fhi, qdiss, hrkx, hrky, bety, betac;
+  std::vector<double> green, flo, fhi, qdiss, hrkx, hrky, bety, betac, rkxf, rkyf, spmf, alk;
   std::vector<double2> tw;
+  std::vector<int> shell_off, shell_idx;
+  int kmax = 0, kmaxred = 0;
 };
 
 static void make_tables(const casl_params &p, const Consts &c, HostTables &t) {
@@ -1071,6 +1092,39 @@ static void make_tables(const casl_params &p, const Consts &c, HostTables &t) {
     }
     mean /= (double)ny;
     for (int iy = 0; iy < ny; iy++) t.betac[iy] -= mean;
+  }
+  // 1-D spectrum tables (spectral.f90:109-134): shell of every mode, shell
+  // population factor spmf, log10 wavenumber alk, the indices of each shell
+  {
+    double scx = c.twopi / p.ellx, scy = c.twopi / p.elly;
+    double delk = sqrt(scx * scx + scy * scy), delki = 1.0 / delk;
+    t.kmax = (int)lround(sqrt(rkxmax * rkxmax + rkymax * rkymax) * delki);
+    int mx = nx > ny ? nx : ny;
+    t.spmf.assign(mx + 1, 0.0);
+    t.alk.assign(mx + 1, 0.0);
+    std::vector<int> kmag(nn);
+    std::vector<int> cnt(t.kmax + 2, 0);
+    for (int ky = 0; ky < ny; ky++)
+      for (int kx = 0; kx < nx; kx++) {
+        int k = (int)lround(sqrt(rkx[kx] * rkx[kx] + rky[ky] * rky[ky]) * delki);
+        kmag[(size_t)ky * nx + kx] = k;
+        t.spmf[k] = t.spmf[k] + 1.0;
+        cnt[k + 1]++;
+      }
+    double snorm = 4.0 * c.pi / (double)(nx * ny);
+    t.spmf[0] = 0.0;
+    for (int k = 1; k <= t.kmax; k++) {
+      t.spmf[k] = snorm * (double)k / t.spmf[k];
+      t.alk[k] = log10(delk * (double)k);
+    }
+    t.kmaxred = (int)lround(sqrt((rkxmax * rkxmax + rkymax * rkymax) / 2.0) * delki);
+    t.shell_off.assign(t.kmax + 2, 0);
+    for (int k = 0; k <= t.kmax; k++) t.shell_off[k + 1] = t.shell_off[k] + cnt[k + 1];
+    t.shell_idx.resize(nn);
+    std::vector<int> pos(t.shell_off.begin(), t.shell_off.end() - 1);
+    for (size_t i = 0; i < nn; i++) t.shell_idx[pos[kmag[i]]++] = (int)i;
+    t.rkxf = rkxf;
+    t.rkyf = rkyf;
   }
   t.tw.resize(nx);
   for (int k = 0; k < nx; k++) {
@@ -1208,6 +1262,34 @@ __global__ void k_diag_heads(const int *__restrict__ i1q, int nq, int *__restric
 }
 // term_i = X_i dy_i - Y_i dx_i with (X_i, Y_i) the exclusive prefix of the
 // increments from the contour's first node
+// spec1d (spectral.f90:370-424): one warp per shell sums w*ss^2 over the
+// shell's modes (lane-strided, then a fixed shuffle tree: deterministic);
+// w = 1/4 for the mean, 1/2 for the kx = 0 and ky = 0 modes.
+__global__ void k_spec1d(const double *__restrict__ ss, const int *__restrict__ off,
+                         const int *__restrict__ idx, int nx, int kmax, double *__restrict__ spec) {
+  const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (k > kmax) return;
+  double acc = 0.0;
+  for (int i = off[k] + lane; i < off[k + 1]; i += 32) {
+    int m = idx[i], kx = m % nx, ky = m / nx;
+    double v = ss[m];
+    double w = (kx == 0 && ky == 0) ? 0.25 : ((kx == 0 || ky == 0) ? 0.5 : 1.0);
+    acc += w * (v * v);
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if (lane == 0) spec[k] = acc;
+}
+
+// ss <- ss * (rkxf^2 + rkyf^2), the filtered K^2 of spec1d's iopt = 1
+__global__ void k_mul_rksq(double *__restrict__ ss, const double *__restrict__ rkxf,
+                           const double *__restrict__ rkyf, int nx, long long nn) {
+  for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < nn;
+       m += (long long)gridDim.x * blockDim.x) {
+    int kx = (int)(m % nx), ky = (int)(m / nx);
+    ss[m] = ss[m] * (rkxf[kx] * rkxf[kx] + rkyf[ky] * rkyf[ky]);
+  }
+}
+
 __global__ void k_diag_shoelace(const double *__restrict__ dx, const double *__restrict__ dy,
                                 const double *__restrict__ X, const double *__restrict__ Y,
                                 int npt, double *__restrict__ part) {
@@ -1269,6 +1351,10 @@ static int alloc_all(casl_handle *h) {
   CASL_CUDA_TRY(cudaMalloc(&h->bety, n * sizeof(double)));
   CASL_CUDA_TRY(cudaMalloc(&h->betac, n * sizeof(double)));
   CASL_CUDA_TRY(cudaMalloc(&h->tw, n * sizeof(double2)));
+  CASL_CUDA_TRY(cudaMalloc(&h->shell_idx, (size_t)nn * sizeof(int)));
+  CASL_CUDA_TRY(cudaMalloc(&h->shell_off, (size_t)(2 * n + 2) * sizeof(int)));
+  CASL_CUDA_TRY(cudaMalloc(&h->rkxf, n * sizeof(double)));
+  CASL_CUDA_TRY(cudaMalloc(&h->rkyf, n * sizeof(double)));
   size_t fine = (size_t)h->c.nxf * h->c.nyf;
   CASL_CUDA_TRY(cudaMalloc(&h->fineJ, fine * sizeof(int)));
   CASL_CUDA_TRY(cudaMalloc(&h->ljx, (size_t)h->c.nxf * sizeof(int)));
@@ -1287,9 +1373,11 @@ static void free_all(casl_handle *h) {
                   h->vv, h->emq, h->epq, h->qspre, h->sqs, h->sqd, h->qsi, h->qsf, h->qdi,
                   h->qdf, h->green, h->flo, h->fhi, h->qdiss, h->w[0], h->hrkx, h->hrky,
                   h->bety, h->betac, h->tw, h->fineJ, h->ljx, h->coarseC, h->part, h->scal,
-                  h->sx, h->sx2};
+                  h->sx, h->sx2, h->shell_idx, h->shell_off, h->rkxf, h->rkyf};
   for (void *p : ptrs)
     if (p) cudaFree(p);
+  free(h->spmf_h);
+  free(h->alk_h);
   if (h->hscal) cudaFreeHost(h->hscal);
 }
 
@@ -1341,8 +1429,20 @@ int casl_create(const casl_params *p, int device, casl_handle **out) {
   cudaMemcpy(h->hrky, t.hrky.data(), n * sizeof(double), cudaMemcpyHostToDevice);
   cudaMemcpy(h->bety, t.bety.data(), n * sizeof(double), cudaMemcpyHostToDevice);
   cudaMemcpy(h->betac, t.betac.data(), n * sizeof(double), cudaMemcpyHostToDevice);
+  cudaMemcpy(h->shell_idx, t.shell_idx.data(), nn * sizeof(int), cudaMemcpyHostToDevice);
+  cudaMemcpy(h->shell_off, t.shell_off.data(), t.shell_off.size() * sizeof(int), cudaMemcpyHostToDevice);
+  cudaMemcpy(h->rkxf, t.rkxf.data(), n * sizeof(double), cudaMemcpyHostToDevice);
+  cudaMemcpy(h->rkyf, t.rkyf.data(), n * sizeof(double), cudaMemcpyHostToDevice);
+  h->kmax = t.kmax;
+  h->kmaxred = t.kmaxred;
+  h->spmf_h = (double *)malloc((n + 1) * sizeof(double));
+  h->alk_h = (double *)malloc((n + 1) * sizeof(double));
+  if (h->spmf_h && h->alk_h) {
+    memcpy(h->spmf_h, t.spmf.data(), (n + 1) * sizeof(double));
+    memcpy(h->alk_h, t.alk.data(), (n + 1) * sizeof(double));
+  }
   e = cudaMemcpy(h->tw, t.tw.data(), n * sizeof(double2), cudaMemcpyHostToDevice);
-  if (e != cudaSuccess) {
+  if (e != cudaSuccess || !h->spmf_h || !h->alk_h) {
     free_all(h);
     cudaStreamDestroy(h->stream);
     free(h);
@@ -1612,24 +1712,20 @@ int casl_main_invert(casl_handle *h, const double *qq, double *uu, double *vv, d
   LoadDeriv ld{};
   ld.f[0] = q; ld.f[1] = q; ld.dir[0] = 0; ld.dir[1] = 1;
   ld.green = h->green; ld.hrkx = h->hrkx; ld.hrky = h->hrky; ld.n = h->n;
-  int rc = RFFT_DISPATCH(false, true, true, ld, (StoreStrided{h->w[0], (long long)nn, 1, n}), 2);
+  int rc = RFFT_DISPATCH(false, false, false, ld, (StoreStrided{h->w[0], (long long)nn, n, 1}), 2);
   if (rc) return rc;
   StoreScaled st{};
   st.p[0] = h->w[2]; st.p[1] = h->w[3]; st.scale[0] = 1.0; st.scale[1] = -1.0; st.n = h->n;
   LoadBatch lb{};
-  lb.p[0] = h->w[0]; lb.p[1] = h->w[1]; lb.vs = n; lb.es = 1;
-  rc = RFFT_DISPATCH(false, false, true, lb, st, 2);
+  lb.p[0] = h->w[0]; lb.p[1] = h->w[1]; lb.vs = 1; lb.es = n;
+  rc = RFFT_DISPATCH(false, true, false, lb, st, 2);
   if (rc) return rc;
   if (uu) CASL_CUDA_TRY(cudaMemcpyAsync(uu, h->w[3], nn * sizeof(double), cudaMemcpyDeviceToHost, s));
   if (vv) CASL_CUDA_TRY(cudaMemcpyAsync(vv, h->w[2], nn * sizeof(double), cudaMemcpyDeviceToHost, s));
   if (pp) {
-    // pp = green*qq on the host copy is exact elementwise; done on device
-    // through the combine kernel's formula.
-    CASL_CUDA_TRY(cudaMemcpyAsync(p, h->green, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    CASL_CUDA_TRY(cudaStreamSynchronize(s));
-    std::vector<double> g(nn);
-    CASL_CUDA_TRY(cudaMemcpy(g.data(), p, nn * sizeof(double), cudaMemcpyDeviceToHost));
-    for (size_t k = 0; k < nn; k++) pp[k] = g[k] * qq[k];
+    // pp = green*qq (spectral.f90:321)
+    CASL_K(k_mul2, grid_for((long long)nn), 256, 0, s)(h->green, q, p, (long long)nn);
+    CASL_CUDA_TRY(cudaMemcpyAsync(pp, p, nn * sizeof(double), cudaMemcpyDeviceToHost, s));
   }
   CASL_CUDA_TRY(cudaStreamSynchronize(s));
   return check_launch(h);
@@ -1645,13 +1741,13 @@ int casl_gradient(casl_handle *h, const double *ff, double *ffx, double *ffy) {
   LoadDeriv ld{};
   ld.f[0] = f; ld.f[1] = f; ld.dir[0] = 0; ld.dir[1] = 1;
   ld.green = nullptr; ld.hrkx = h->hrkx; ld.hrky = h->hrky; ld.n = h->n;
-  int rc = RFFT_DISPATCH(false, true, true, ld, (StoreStrided{h->w[0], (long long)nn, 1, n}), 2);
+  int rc = RFFT_DISPATCH(false, false, false, ld, (StoreStrided{h->w[0], (long long)nn, n, 1}), 2);
   if (rc) return rc;
   StoreScaled st{};
   st.p[0] = h->w[2]; st.p[1] = h->w[3]; st.scale[0] = 1.0; st.scale[1] = 1.0; st.n = h->n;
   LoadBatch lb{};
-  lb.p[0] = h->w[0]; lb.p[1] = h->w[1]; lb.vs = n; lb.es = 1;
-  rc = RFFT_DISPATCH(false, false, true, lb, st, 2);
+  lb.p[0] = h->w[0]; lb.p[1] = h->w[1]; lb.vs = 1; lb.es = n;
+  rc = RFFT_DISPATCH(false, true, false, lb, st, 2);
   if (rc) return rc;
   if (ffx) CASL_CUDA_TRY(cudaMemcpyAsync(ffx, h->w[2], nn * sizeof(double), cudaMemcpyDeviceToHost, s));
   if (ffy) CASL_CUDA_TRY(cudaMemcpyAsync(ffy, h->w[3], nn * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -1942,6 +2038,33 @@ int casl_diagnostics(casl_handle *h, double out[4]) {
     if (rc) return rc;
     out[3] = h->hscal->qjump * (0.5 * circ);
   }
+  return CASL_OK;
+}
+
+int casl_spec1d(casl_handle *h, double *ss, double *spec, int iopt) {
+  if (!h || !ss || !spec || (iopt != 0 && iopt != 1)) return CASL_EINVAL;
+  cudaStream_t st = h->stream;
+  const long long nn = (long long)h->n * h->n;
+  double *d = h->w[5], *dspec = h->w[4];
+  CASL_CUDA_TRY(cudaMemcpyAsync(d, ss, nn * sizeof(double), cudaMemcpyHostToDevice, st));
+  if (iopt == 1)
+    CASL_K(k_mul_rksq, grid_for(nn), 256, 0, st)(d, h->rkxf, h->rkyf, h->n, nn);
+  CASL_CUDA_TRY(cudaMemsetAsync(dspec, 0, (h->n + 1) * sizeof(double), st));
+  CASL_K(k_spec1d, (32 * (h->kmax + 1) + 255) / 256, 256, 0, st)(d, h->shell_off, h->shell_idx, h->n,
+                                                               h->kmax, dspec);
+  CASL_CUDA_TRY(cudaMemcpyAsync(spec, dspec, (h->n + 1) * sizeof(double), cudaMemcpyDeviceToHost, st));
+  if (iopt == 1)
+    CASL_CUDA_TRY(cudaMemcpyAsync(ss, d, nn * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CASL_CUDA_TRY(cudaStreamSynchronize(st));
+  return check_launch(h);
+}
+
+int casl_spec_tables(casl_handle *h, int *kmax, int *kmaxred, double *spmf, double *alk) {
+  if (!h || !kmax || !kmaxred) return CASL_EINVAL;
+  *kmax = h->kmax;
+  *kmaxred = h->kmaxred;
+  if (spmf) memcpy(spmf, h->spmf_h, (h->n + 1) * sizeof(double));
+  if (alk) memcpy(alk, h->alk_h, (h->n + 1) * sizeof(double));
   return CASL_OK;
 }
 

@@ -113,14 +113,20 @@ struct StoreStrided {
 __device__ __forceinline__ int cpad(int i) { return i + (i >> 3); }
 __device__ __forceinline__ int dpos(int j) { return 2 * cpad(j >> 1) + (j & 1); }
 
-template <int LOGH>
+// VF: a side of the pass is vector-fastest and is staged through shared
+// memory with lanes over vectors, which wants several vectors per CTA (V*8
+// contiguous bytes per row); contiguous-only passes take small CTAs so that
+// one transform spreads evenly over all SMs.
+template <int LOGH, bool VF>
 struct RfftShape {
   static constexpr int H = 1 << LOGH;
   static constexpr int N = 2 * H;
   static constexpr int TPV = H / 8;
   static constexpr int VS = H + H / 8 + 1;  // complex stride between slots
-  static constexpr int V = (256 / TPV) < N ? (256 / TPV) : N;  // vectors per CTA
+  static constexpr int VW = VF ? 256 / TPV : 64 / TPV;
+  static constexpr int V = VW < 1 ? 1 : (VW < N ? VW : N);  // vectors per CTA
   static constexpr int NT = V * TPV;        // threads per CTA
+  static constexpr int MINB = 768 / NT > 0 ? 768 / NT : 1;  // CTAs per SM to fit
   static constexpr int P8 = LOGH / 3;       // radix-8 passes
   static constexpr int REM = LOGH % 3;      // final radix-4 (2) or radix-2 (1) pass
   // forward transforms with a vector-fastest store stage their output in a
@@ -163,7 +169,7 @@ __device__ __forceinline__ void rf_butterflies(double2 (&x)[8], int t, int Ns,
 template <int LOGH, bool FWD>
 __device__ __forceinline__ void rf_complex(double2 (&x)[8], double2 *S, int t,
                                            const double2 *__restrict__ tw, int n) {
-  using Sh = RfftShape<LOGH>;
+  using Sh = RfftShape<LOGH, false>;  // only H, TPV and the pass plan are used
   int Ns = 1;
 #pragma unroll
   for (int p = 0; p < Sh::P8; p++) {
@@ -184,9 +190,9 @@ __device__ __forceinline__ void rf_complex(double2 (&x)[8], double2 *S, int t,
 }
 
 template <int LOGH, bool FWD, bool LVF, bool SVF, class LD, class ST>
-__global__ void __launch_bounds__(RfftShape<LOGH>::NT, 3) k_rfft_r(LD ld, ST st,
-                                                                const double2 *__restrict__ tw) {
-  using Sh = RfftShape<LOGH>;
+__global__ void __launch_bounds__(RfftShape<LOGH, LVF || SVF>::NT, RfftShape<LOGH, LVF || SVF>::MINB)
+    k_rfft_r(LD ld, ST st, const double2 *__restrict__ tw) {
+  using Sh = RfftShape<LOGH, LVF || SVF>;
   constexpr int H = Sh::H, N = Sh::N, TPV = Sh::TPV, V = Sh::V, NT = Sh::NT, VS = Sh::VS;
   extern __shared__ double2 smem[];
   double *Sd = reinterpret_cast<double *>(smem);

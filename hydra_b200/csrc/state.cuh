@@ -37,6 +37,11 @@ struct casl_handle {
   // tables
   double *green, *flo, *fhi, *qdiss, *hrkx, *hrky, *bety, *betac;
   double2 *tw;           // exp(-2 pi i k / n), k < n
+  // 1-D spectrum (spectral.f90:109-134): spectral indices grouped by shell
+  int *shell_off, *shell_idx;  // kmax+2 offsets; n*n indices kx + nx*ky
+  double *rkxf, *rkyf;         // filtered wavenumbers for K^2 (spec1d iopt = 1)
+  int kmax, kmaxred;
+  double *spmf_h, *alk_h;      // host, n+1 entries each
 
   // con2grid scratch
   int *fineJ;            // (nyf, nxf): row 0 = bottom level, rows 1.. = jump counts

@@ -308,15 +308,18 @@ __global__ void k_sg_candidates(SurgState S, const LevelDesc *__restrict__ lev, 
 }
 
 __device__ __forceinline__ void mark(SurgState &S, int x, int ib, int iend) {
-  if (x > ib && x <= iend) ((volatile unsigned char *)S.pending)[x] = 1;
+  if (x > ib && x <= iend) S.pending[x] = 1;
 }
 
-// Mark every later node whose tests may read node j's changed data.
-__device__ void mark_affected(SurgState &S, const LevelDesc &L, int j, int ib, const Consts &c) {
+// Mark every later node whose tests may read node j's changed data.  Called
+// by all 32 lanes of the level's warp with the same j: the loops over boxes
+// are uniform and the entries of each box are split across the lanes.
+__device__ void mark_affected(SurgState &S, const LevelDesc &L, int j, int ib, const Consts &c,
+                              int lane) {
   int cand[2] = {j, S.prev0[j]};
   for (int q = 0; q < 2; q++) {
     int e = cand[q];
-    mark(S, e, ib, L.iend);
+    if (lane == 0) mark(S, e, ib, L.iend);
     // boxes listing the segment whose list entry is e
     int i = S.nq0[e];
     int mbx1, mbx2, mby1, mby2;
@@ -326,7 +329,7 @@ __device__ void mark_affected(SurgState &S, const LevelDesc &L, int j, int ib, c
       for (int mby = mby1; mby <= mby2; mby++) {
         int gb = L.boxbase + L.nby * mmbx + mby % L.nby;
         int s = S.nb1[gb], n = S.nbcnt[gb];
-        for (int k = 0; k < n; k++) mark(S, S.nbnode[s + k], ib, L.iend);
+        for (int k = lane; k < n; k += 32) mark(S, S.nbnode[s + k], ib, L.iend);
       }
     }
   }
@@ -339,17 +342,21 @@ __global__ void k_sg_replay(SurgState S, const LevelDesc *__restrict__ lev,
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (warp >= *nlev_dev) return;
   const LevelDesc L = lev[warp];
-  volatile unsigned char *pend = S.pending;
-  volatile double *xq = S.xq, *yq = S.yq, *dx = S.dx, *dy = S.dy, *dsq = S.dsq;
-  volatile int *nextq = S.nextq;
+  // Every node, flag and box entry this warp reads or writes belongs to its
+  // own level, so no other warp touches them: lane 0's updates reach the
+  // other lanes through this SM's L1 after __syncwarp(), and plain cached
+  // loads are coherent here.
+  const unsigned char *pend = S.pending;
+  double *xq = S.xq, *yq = S.yq, *dx = S.dx, *dy = S.dy, *dsq = S.dsq;
+  int *nextq = S.nextq;
   const double f12 = 0.5;
   int count = 0;
   long long pos = L.ibeg;
   while (pos <= L.iend) {
     int ib;
     if ((pos & 15) == 0 && pos + 512 <= (long long)L.iend + 1) {
-      // 512 flags per step: one 16-byte uncached load per lane
-      uint4 v = __ldcv(reinterpret_cast<const uint4 *>(S.pending + pos) + lane);
+      // 512 flags per step: one 16-byte load per lane
+      uint4 v = reinterpret_cast<const uint4 *>(pend + pos)[lane];
       unsigned b = __ballot_sync(0xffffffffu, (v.x | v.y | v.z | v.w) != 0u);
       if (!b) {
         pos += 512;
@@ -397,7 +404,7 @@ __global__ void k_sg_replay(SurgState S, const LevelDesc *__restrict__ lev,
         continue;
       }
       kk = k + __ffs(pb) - 1;
-      int inew = 0;
+      int inew = 0, tsb = 0;
       if (lane == 0) {
         int isb = S.bnode[kk];
         int is = nextq[isb];
@@ -436,14 +443,19 @@ __global__ void k_sg_replay(SurgState S, const LevelDesc *__restrict__ lev,
         dx[ib] = dx[ib] + dxa;
         dy[ib] = dy[ib] + dya;
         dsq[ib] = dx[ib] * dx[ib] + dy[ib] * dy[ib];
-        int touched[4] = {i, is, isb, ib};
-        for (int q = 0; q < 4; q++) mark_affected(S, L, touched[q], ib, c);
+        tsb = isb;
         inew = is;
         count++;
-        __threadfence();  // marks and moved nodes visible to the uncached reloads
       }
-      __syncwarp();
-      i = __shfl_sync(0xffffffffu, inew, 0);
+      __syncwarp();  // lane 0's moves are visible to the whole warp
+      const int is_new = __shfl_sync(0xffffffffu, inew, 0);
+      const int isb_new = __shfl_sync(0xffffffffu, tsb, 0);
+      {
+        const int touched[4] = {i, is_new, isb_new, ib};
+        for (int q = 0; q < 4; q++) mark_affected(S, L, touched[q], ib, c, lane);
+      }
+      __syncwarp();  // marks visible before the next flag scan
+      i = is_new;
       xi = xq[i];
       yi = yq[i];
       if (i == ib) break;

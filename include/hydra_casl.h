@@ -164,6 +164,17 @@ int casl_step(casl_handle *h, int nsteps);
  * out[3] contour circulation qjump * sum of signed contour areas. */
 int casl_diagnostics(casl_handle *h, double out[4]);
 
+/* spec1d (spectral.f90:370-424): 1-D spectrum of the spectral field
+ * ss(nx,ny) (host array); spec receives max(nx,ny)+1 shell sums, zero above
+ * kmax.  iopt = 1 multiplies ss by the filtered K^2 first and returns it so
+ * modified, as the reference does; iopt = 0 leaves ss untouched. */
+int casl_spec1d(casl_handle *h, double *ss, double *spec, int iopt);
+
+/* The spectrum tables of init_spectral (spectral.f90:109-134): kmax, kmaxred
+ * and, when non-NULL, spmf and alk (max(nx,ny)+1 entries each) as savegrid
+ * (evolution.f90:683-719) uses them. */
+int casl_spec_tables(casl_handle *h, int *kmax, int *kmaxred, double *spmf, double *alk);
+
 /* ---- con2grid without device allocation ---------------------------------- */
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc
  * -- their GPU memory is handed out by their own pool or another framework,

@@ -72,6 +72,9 @@ struct o_state {
   /* spectral tables */
   double *rkx, *hrkx, *rky, *hrky, *bety;
   double *rksq, *qdiss, *green, *flo, *fhi, *rk;
+  /* 1-D spectrum tables (spectral.f90:109-134) */
+  int *kmag, kmax, kmaxred;
+  double *spmf, *alk;
   fftplan px, py;
   double *fwork;
   /* contours */
@@ -485,8 +488,68 @@ static void init_spectral(o_state *s) {
       s->green[SPC(s, kx, ky)] =
           -ONE / (s->rkx[kx - 1] * s->rkx[kx - 1] + s->rky[ky - 1] * s->rky[ky - 1] + s->kdsq);
   for (int iy = 1; iy <= ny; iy++) s->bety[iy - 1] = p->beta * (s->gly * (double)(iy - 1) + s->ymin);
+  /* Shell index, shell-population factor and log wavenumber of the 1-D
+   * spectrum (spectral.f90:109-134). */
+  {
+    double delk = sqrt(scx * scx + scy * scy), delki = ONE / delk;
+    s->kmax = f_nint(sqrt(rkxmax * rkxmax + rkymax * rkymax) * delki);
+    int mx = nx > ny ? nx : ny;
+    s->spmf = xcalloc((size_t)mx + 1, sizeof(double));
+    s->alk = xcalloc((size_t)mx + 1, sizeof(double));
+    s->kmag = xcalloc((size_t)nx * ny, sizeof(int));
+    for (int ky = 1; ky <= ny; ky++)
+      for (int kx = 1; kx <= nx; kx++) {
+        int k = f_nint(sqrt(s->rkx[kx - 1] * s->rkx[kx - 1] + s->rky[ky - 1] * s->rky[ky - 1]) * delki);
+        s->kmag[SPC(s, kx, ky)] = k;
+        s->spmf[k] = s->spmf[k] + ONE;
+      }
+    double snorm = 4.0 * s->pi / (double)(nx * ny);
+    s->spmf[0] = 0.0;
+    for (int k = 1; k <= s->kmax; k++) {
+      s->spmf[k] = snorm * (double)k / s->spmf[k];
+      s->alk[k] = log10(delk * (double)k);
+    }
+    s->kmaxred = f_nint(sqrt((rkxmax * rkxmax + rkymax * rkymax) / 2.0) * delki);
+  }
   free(rkxf);
   free(rkyf);
+}
+
+/* spec1d (spectral.f90:370-424): shell sums of ss^2 with weight 1/4 for the
+ * mean, 1/2 for the x- and y-independent modes.  iopt = 1 multiplies ss by
+ * the filtered K^2 first and leaves it modified.  spec has max(nx,ny)+1
+ * entries; those above kmax are zero. */
+void o_spec1d(o_state *s, double *ss, double *spec, int iopt) {
+  int nx = s->nx, ny = s->ny, mx = nx > ny ? nx : ny;
+  if (iopt == 1)
+    for (int ky = 1; ky <= ny; ky++)
+      for (int kx = 1; kx <= nx; kx++) ss[SPC(s, kx, ky)] = ss[SPC(s, kx, ky)] * s->rksq[SPC(s, kx, ky)];
+  for (int k = 0; k <= mx; k++) spec[k] = 0.0;
+  int k = s->kmag[SPC(s, 1, 1)];
+  spec[k] = spec[k] + F14 * (ss[SPC(s, 1, 1)] * ss[SPC(s, 1, 1)]);
+  for (int kx = 2; kx <= nx; kx++) {
+    k = s->kmag[SPC(s, kx, 1)];
+    spec[k] = spec[k] + F12 * (ss[SPC(s, kx, 1)] * ss[SPC(s, kx, 1)]);
+  }
+  for (int ky = 2; ky <= ny; ky++) {
+    k = s->kmag[SPC(s, 1, ky)];
+    spec[k] = spec[k] + F12 * (ss[SPC(s, 1, ky)] * ss[SPC(s, 1, ky)]);
+  }
+  for (int ky = 2; ky <= ny; ky++)
+    for (int kx = 2; kx <= nx; kx++) {
+      k = s->kmag[SPC(s, kx, ky)];
+      spec[k] = spec[k] + ss[SPC(s, kx, ky)] * ss[SPC(s, kx, ky)];
+    }
+}
+
+void o_spec_tables(o_state *s, int *kmax, int *kmaxred, double *spmf, double *alk) {
+  int mx = s->nx > s->ny ? s->nx : s->ny;
+  *kmax = s->kmax;
+  *kmaxred = s->kmaxred;
+  for (int k = 0; k <= mx; k++) {
+    spmf[k] = s->spmf[k];
+    alk[k] = s->alk[k];
+  }
 }
 
 o_state *o_create(const o_params *p) {
@@ -532,7 +595,8 @@ void o_destroy(o_state *s) {
                   s->ix0w, s->ix1w, s->iyfw, s->iy0w, s->iy1w, s->rkx, s->hrkx, s->rky, s->hrky,
                   s->bety, s->rksq, s->qdiss, s->green, s->flo, s->fhi, s->rk, s->fwork, s->qr,
                   s->qs, s->uu, s->vv, s->pp, s->qq, s->qc, s->qd, s->qspre, s->emq, s->epq,
-                  s->xq, s->yq, s->nextq, s->indq, s->npq, s->i1q, s->i2q};
+                  s->xq, s->yq, s->nextq, s->indq, s->npq, s->i1q, s->i2q, s->kmag, s->spmf,
+                  s->alk};
   for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); i++) free(ptrs[i]);
   plan_free(&s->px);
   plan_free(&s->py);

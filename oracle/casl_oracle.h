@@ -114,6 +114,10 @@ void o_set_scalar(o_state *s, int which, double v);
 /* diagnostics: ekin, epot (evolution.f90:612-644), enstrophy-like l2 norm of
  * q - beta*y (generic.f90:48-62), circulation sum over contours */
 void o_diagnostics(o_state *s, double *out4);
+/* 1-D spectrum of a spectral field (spectral.f90:370-424) and its tables
+ * (spectral.f90:109-134); arrays of max(nx,ny)+1 entries. */
+void o_spec1d(o_state *s, double *ss, double *spec, int iopt);
+void o_spec_tables(o_state *s, int *kmax, int *kmaxred, double *spmf, double *alk);
 
 #ifdef __cplusplus
 }

@@ -84,6 +84,8 @@ def lib():
         L.o_scalar.argtypes = [C.c_void_p, C.c_int]
         L.o_set_scalar.argtypes = [C.c_void_p, C.c_int, C.c_double]
         L.o_diagnostics.argtypes = [C.c_void_p, dp]
+        L.o_spec1d.argtypes = [C.c_void_p, dp, dp, C.c_int]
+        L.o_spec_tables.argtypes = [C.c_void_p, ip, ip, dp, dp]
     return _lib
 
 
@@ -275,3 +277,20 @@ class Oracle:
         out = np.zeros(4)
         lib().o_diagnostics(self.h, _dp(out))
         return dict(ekin=out[0], epot=out[1], enstrophy=out[2], circulation=out[3])
+
+    def spec1d(self, ss, iopt=0):
+        """spec1d (spectral.f90:370-424) of a spectral field ss(nx,ny) given as
+        an (ny, nx) array; returns (spec[0..max(nx,ny)], ss after the call)."""
+        a = np.ascontiguousarray(ss, dtype=np.float64).copy()
+        spec = np.zeros(max(self.nx, self.nx) + 1)
+        lib().o_spec1d(self.h, _dp(a), _dp(spec), int(iopt))
+        return spec, a
+
+    def spec_tables(self):
+        """kmax, kmaxred, spmf, alk of init_spectral (spectral.f90:109-134)."""
+        kmax = C.c_int(0)
+        kred = C.c_int(0)
+        spmf = np.zeros(self.nx + 1)
+        alk = np.zeros(self.nx + 1)
+        lib().o_spec_tables(self.h, C.byref(kmax), C.byref(kred), _dp(spmf), _dp(alk))
+        return dict(kmax=kmax.value, kmaxred=kred.value, spmf=spmf, alk=alk)

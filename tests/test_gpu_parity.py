@@ -63,6 +63,26 @@ def test_fft_sizes(gpu_lib, n):
     g.close()
 
 
+@pytest.mark.parametrize("n", [64, 256])
+def test_spec1d(oracle_mod, gpu_lib, n):
+    """spec1d (spectral.f90:370-424) and init_spectral's spectrum tables."""
+    from hydra_b200.casl import CaslGPU
+    o = oracle_mod.Oracle(n)
+    g = CaslGPU(n, ncontq=10, npm=1000)
+    tg, to = g.spec_tables(), o.spec_tables()
+    assert (tg["kmax"], tg["kmaxred"]) == (to["kmax"], to["kmaxred"])
+    assert np.array_equal(tg["spmf"], to["spmf"]) and np.array_equal(tg["alk"], to["alk"])
+    rng = np.random.default_rng(7)
+    ss = o.ptospc(rng.standard_normal((n, n)))
+    for iopt in (0, 1):
+        sg, ag = g.spec1d(ss, iopt)
+        so, ao = o.spec1d(ss, iopt)
+        assert np.array_equal(ag, ao)  # iopt = 1: the same K^2 product, bit for bit
+        # shell sums in a different order: rounding only
+        assert np.abs(sg - so).max() <= 1e-13 * np.abs(so).max()
+    g.close()
+
+
 def test_con2grid_levels_bit_exact(pair):
     o, g = pair
     qc_o, lv_o = o.con2grid(levels=True)
