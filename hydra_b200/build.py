@@ -13,7 +13,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libhydra_casl.so")
-SOURCES = ["casl.cu", "surgery.cu", "renode.cu", "recontour.cu", "noalloc.cu"]
+SOURCES = ["casl.cu", "surgery.cu", "renode.cu", "recontour.cu", "noalloc.cu", "io.cu"]
 HEADERS = ["common.cuh", "fft.cuh", "state.cuh", "scan.cuh", "renode.cuh"]
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 

@@ -88,6 +88,26 @@ SIGNATURES = {
     "casl_launch_count": (C.c_int, [C.POINTER(C.c_longlong)]),
     "casl_profile": (C.c_int, [C.c_void_p, C.c_int]),
     "casl_profile_read": (C.c_int, [C.c_void_p, _dp, C.POINTER(C.c_longlong), _dp]),
+    "casl_io_append_synopsis": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_double, C.c_double]),
+    "casl_io_append_ene": (C.c_int, [C.c_char_p, C.c_double, C.c_double, C.c_double]),
+    "casl_io_append_norms": (C.c_int, [C.c_char_p, C.c_double, C.c_double]),
+    "casl_io_append_spectrum": (C.c_int, [C.c_char_p, C.c_double, C.c_double, C.c_double, C.c_int,
+                                          _dp, _dp]),
+    "casl_io_append_monitor": (C.c_int, [C.c_char_p] + [C.c_double] * 6),
+    "casl_io_append_complexity": (C.c_int, [C.c_char_p, C.c_double, C.c_int, C.c_int]),
+    "casl_io_write_index": (C.c_int, [C.c_char_p, C.c_int, _ip, _ip, _ip]),
+    "casl_io_read_index": (C.c_int, [C.c_char_p, C.c_int, _ip, _ip, _ip]),
+    "casl_io_write_nodes": (C.c_int, [C.c_char_p, C.c_int, _dp, _dp]),
+    "casl_io_read_nodes": (C.c_int, [C.c_char_p, C.c_int, _dp, _dp]),
+    "casl_io_write_r4": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_float,
+                                   C.POINTER(C.c_float)]),
+    "casl_io_read_r4": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_float),
+                                  C.POINTER(C.c_float)]),
+    "casl_io_read_synopsis": (C.c_int, [C.c_char_p, C.c_int, _ip, _ip, _dp, _dp]),
+    "casl_savecont": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int]),
+    "casl_savegrid": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int]),
+    "casl_io_wait": (C.c_int, [C.c_void_p]),
+    "casl_readcont": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int]),
 }
 
 
@@ -290,6 +310,22 @@ class CaslGPU:
         out = np.zeros(4)
         self._check(self.lib.casl_diagnostics(self.h, _d(out)), "casl_diagnostics")
         return dict(ekin=out[0], epot=out[1], enstrophy=out[2], circulation=out[3])
+
+    def savecont(self, rundir, icrec):
+        """savecont (evolution.f90:731-774) into rundir/cont; the files are
+        written by a background thread (see io_wait)."""
+        self._check(self.lib.casl_savecont(self.h, os.fsencode(rundir), int(icrec)), "casl_savecont")
+
+    def savegrid(self, rundir, irec):
+        """savegrid (evolution.f90:648-727) at the current time."""
+        self._check(self.lib.casl_savegrid(self.h, os.fsencode(rundir), int(irec)), "casl_savegrid")
+
+    def io_wait(self):
+        self._check(self.lib.casl_io_wait(self.h), "casl_io_wait")
+
+    def readcont(self, rundir, iind):
+        """readcont (common.f90:30-100) + init: restart from save iind."""
+        self._check(self.lib.casl_readcont(self.h, os.fsencode(rundir), int(iind)), "casl_readcont")
 
     def spec1d(self, ss, iopt=0):
         """spec1d (spectral.f90:370-424) of the spectral field ss(nx,ny), given

@@ -125,18 +125,20 @@ struct LoadDeriv {
     double v = f[b][k];
     return green ? green[k] * v : v;
   }
-  // first pass of an inverse transform: vector v = ky, element j = kx
+  // first pass of an inverse transform: vector v = ky, element j = kx.
+  // Branch-free, so that a thread's loads are issued together: the factor
+  // is 0 at k = 0 and k = n/2, -hrk(2k-1) below n/2 and +hrk(2(n-k)-1) above,
+  // and the reflected index (n-k) mod n is always a valid element.
   __device__ __forceinline__ double operator()(int b, int v, int j) const {
     const int nw = n >> 1, kx = j, ky = v;
-    if (dir[b] == 0) {
-      if (kx == 0 || kx == nw) return 0.0;
-      if (kx < nw) return -hrkx[2 * kx - 1] * base(b, n - kx, ky);
-      return hrkx[2 * (n - kx) - 1] * base(b, n - kx, ky);
-    } else {
-      if (ky == 0 || ky == nw) return 0.0;
-      if (ky < nw) return -hrky[2 * ky - 1] * base(b, kx, n - ky);
-      return hrky[2 * (n - ky) - 1] * base(b, kx, n - ky);
-    }
+    const bool dx = dir[b] == 0;
+    const int k = dx ? kx : ky;
+    const int kr = (n - k) & (n - 1);
+    const int hi = k < nw ? 2 * k - 1 : 2 * (n - k) - 1;
+    const double *hrk = dx ? hrkx : hrky;
+    const double h = hrk[hi < 0 ? 0 : hi];
+    const double fac = (k == 0 || k == nw) ? 0.0 : (k < nw ? -h : h);
+    return fac * (dx ? base(b, kr, ky) : base(b, kx, kr));
   }
 };
 
@@ -157,6 +159,19 @@ struct LoadQC {
     if (betac) q = q + betac[j];
     return q;
   }
+  __device__ __forceinline__ double2 pair(int b, int v, int j) const {
+    long long k = (long long)v * n + j;
+    const int2 c = *reinterpret_cast<const int2 *>(C + k);
+    const long long S = s->csum;
+    const double qj = s->qjump;
+    double q0 = qj * ((double)((long long)c.x * nn - S) * inv);
+    double q1 = qj * ((double)((long long)c.y * nn - S) * inv);
+    if (betac) {
+      q0 = q0 + betac[j];
+      q1 = q1 + betac[j + 1];
+    }
+    return make_double2(q0, q1);
+  }
 };
 
 // Advection product -u*fx - v*(fy [+ beta]) of evolution.f90:449,456-461,
@@ -172,6 +187,18 @@ struct LoadAdvect {
     double gx = fx[b][k], gy = fy[b][k];
     if (betab[b] != 0.0) gy = gy + betab[b];
     return -uu[k] * gx - vv[k] * gy;
+  }
+  __device__ __forceinline__ double2 pair(int b, int v, int j) const {
+    long long k = (long long)v * n + j;
+    const double2 gx = *reinterpret_cast<const double2 *>(fx[b] + k);
+    double2 gy = *reinterpret_cast<const double2 *>(fy[b] + k);
+    const double2 u = *reinterpret_cast<const double2 *>(uu + k);
+    const double2 w = *reinterpret_cast<const double2 *>(vv + k);
+    if (betab[b] != 0.0) {
+      gy.x = gy.x + betab[b];
+      gy.y = gy.y + betab[b];
+    }
+    return make_double2(-u.x * gx.x - w.x * gy.x, -u.y * gx.y - w.y * gy.y);
   }
 };
 
@@ -214,6 +241,11 @@ struct StoreScaled {
   // last pass of an inverse transform: vector v = ix, element k = iy
   __device__ __forceinline__ void operator()(int b, int v, int k, double x) const {
     p[b][(long long)v * n + k] = scale[b] == 1.0 ? x : scale[b] * x;
+  }
+  __device__ __forceinline__ void pair(int b, int v, int k, double2 x) const {
+    const double sc = scale[b];
+    if (sc != 1.0) x = make_double2(sc * x.x, sc * x.y);
+    *reinterpret_cast<double2 *>(p[b] + (long long)v * n + k) = x;
   }
 };
 struct LoadBatch {
@@ -821,7 +853,8 @@ __global__ void k_twist_zero(Scalars *s) { s->twist = 0.0; }
 // ---------------------------------------------------------------------------
 // Stages
 // ---------------------------------------------------------------------------
-static int inversion_dev(casl_handle *h, bool reset) {
+// con2grid + the filter combination that forms qq and pp (evolution.f90:507-514)
+static int inversion_qq(casl_handle *h, bool reset) {
   long long nn = (long long)h->n * h->n;
   int rc = con2grid_to_spec(h, h->qc);
   if (rc) return rc;
@@ -831,9 +864,14 @@ static int inversion_dev(casl_handle *h, bool reset) {
   else
     CASL_K(k_combine<false>, grid_for(nn), 256, 0, h->stream)(h->qs, h->qd, h->qc, h->qq, h->pp,
                                                            h->flo, h->fhi, h->green, nn);
-  rc = check_launch(h);
-  if (rc) return rc;
-  // main_invert: vv = spctop(xderiv(green*qq)), uu = -spctop(yderiv(green*qq))
+  return check_launch(h);
+}
+
+// main_invert (spectral.f90:304-342): vv = spctop(xderiv(green*qq)),
+// uu = -spctop(yderiv(green*qq))
+static int main_invert_dev(casl_handle *h) {
+  long long nn = (long long)h->n * h->n;
+  int rc;
   LoadDeriv ld{};
   ld.f[0] = h->qq; ld.f[1] = h->qq;
   ld.dir[0] = 0; ld.dir[1] = 1;
@@ -848,6 +886,12 @@ static int inversion_dev(casl_handle *h, bool reset) {
   LoadBatch lb{};
   lb.p[0] = h->w[0]; lb.p[1] = h->w[0] + nn; lb.vs = 1; lb.es = n;
   return RFFT_DISPATCH(false, true, false, lb, st, 2);
+}
+
+int inversion_dev(casl_handle *h, bool reset) {
+  int rc = inversion_qq(h, reset);
+  if (rc) return rc;
+  return main_invert_dev(h);
 }
 
 static int adapt_dev(casl_handle *h) {
@@ -867,15 +911,16 @@ static int adapt_dev(casl_handle *h) {
 // source (evolution.f90:432-490): gradients of qd and qs (4 spctop in one
 // batched pair of launches), the advection products fused into ptospc's
 // first pass, damping and integrating factor fused into its last store.
-static int source_dev(casl_handle *h, int lev) {
+// The gradients of qd and qs (4 spctop in one batched pair of launches) into
+// w[4], w[5], sqs, sqd; they read only qd and qs, so advance runs them on the
+// second stream beside the inversion.  Scratch: gtmp (4 fields).
+static int source_grad(casl_handle *h) {
   long long nn = (long long)h->n * h->n, n = h->n;
   LoadDeriv ld{};
   ld.f[0] = h->qd; ld.f[1] = h->qd; ld.f[2] = h->qs; ld.f[3] = h->qs;
   ld.dir[0] = 0; ld.dir[1] = 1; ld.dir[2] = 0; ld.dir[3] = 1;
   ld.green = nullptr; ld.hrkx = h->hrkx; ld.hrky = h->hrky; ld.n = h->n;
-  // tmp for 4 transforms: w[0..3]; outputs gx_qd, gy_qd, gx_qs, gy_qs in w[4], w[5], sqs, sqd
-  // (sqs/sqd are free until the products are formed).
-  double *tmp = h->w[0];  // w[0..3] contiguous
+  double *tmp = h->gtmp;  // 4 contiguous fields
   int rc = RFFT_DISPATCH(false, false, false, ld, (StoreStrided{tmp, nn, n, 1}), 4);
   if (rc) return rc;
   LoadBatch lb{};
@@ -885,8 +930,15 @@ static int source_dev(casl_handle *h, int lev) {
   st.p[0] = h->w[4]; st.p[1] = h->w[5]; st.p[2] = h->sqs; st.p[3] = h->sqd;
   for (int b = 0; b < 4; b++) st.scale[b] = 1.0;
   st.n = h->n;
-  rc = RFFT_DISPATCH(false, true, false, lb, st, 4);
-  if (rc) return rc;
+  return RFFT_DISPATCH(false, true, false, lb, st, 4);
+}
+
+// The rest of source (evolution.f90:432-490): the advection products fused
+// into ptospc's first pass, damping and integrating factor into its store.
+static int source_prod(casl_handle *h, int lev) {
+  long long nn = (long long)h->n * h->n, n = h->n;
+  double *tmp = h->w[0];  // w[0..1]
+  int rc;
   // products -> ptospc's first pass into tmp, its second pass with the source store
   LoadAdvect la{};
   la.uu = h->uu; la.vv = h->vv;
@@ -906,15 +958,38 @@ static int source_dev(casl_handle *h, int lev) {
 }  // namespace casl
 
 // advance (evolution.f90:166-326)
+// The gradient transforms of source run on the handle's second stream: fork
+// after the last writer of qs/qd, join before the products need them.
+static int grad_fork(casl_handle *h) {
+  CASL_CUDA_TRY(cudaEventRecord(h->ev_fork, h->stream));
+  CASL_CUDA_TRY(cudaStreamWaitEvent(h->stream2, h->ev_fork, 0));
+  cudaStream_t a = h->stream;
+  h->stream = h->stream2;
+  int rc = source_grad(h);
+  h->stream = a;
+  if (rc) return rc;
+  CASL_CUDA_TRY(cudaEventRecord(h->ev_join, h->stream2));
+  return CASL_OK;
+}
+
+static int grad_join(casl_handle *h) {
+  CASL_CUDA_TRY(cudaStreamWaitEvent(h->stream, h->ev_join, 0));
+  return CASL_OK;
+}
+
 static int advance_dev(casl_handle *h) {
   long long nn = (long long)h->n * h->n;
   int g = grid_for(nn);
   int gn = grid_for(h->nptq > 0 ? h->nptq : 1);
   int rc;
-  // stage 1
-  if ((rc = inversion_dev(h, true))) return rc;
+  // stage 1: the reset in the combination rewrites qs and qd, so the
+  // gradients start after it
+  if ((rc = inversion_qq(h, true))) return rc;
+  if ((rc = grad_fork(h))) return rc;
+  if ((rc = main_invert_dev(h))) return rc;
   if ((rc = adapt_dev(h))) return rc;
-  if ((rc = source_dev(h, 0))) return rc;
+  if ((rc = grad_join(h))) return rc;
+  if ((rc = source_prod(h, 0))) return rc;
   if (h->contex)
     CASL_K(k_nodes_rk<1>, gn, 256, 0, h->stream)(h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, h->uu,
                                              h->vv, h->scal, h->c);
@@ -922,9 +997,11 @@ static int advance_dev(casl_handle *h) {
                                          h->sqd, h->emq, h->scal, nn);
   if ((rc = check_launch(h))) return rc;
   // stage 2
+  if ((rc = grad_fork(h))) return rc;
   CASL_K(k_advance_time, 1, 1, 0, h->stream)(h->scal);
   if ((rc = inversion_dev(h, false))) return rc;
-  if ((rc = source_dev(h, 1))) return rc;
+  if ((rc = grad_join(h))) return rc;
+  if ((rc = source_prod(h, 1))) return rc;
   if (h->contex)
     CASL_K(k_nodes_rk<2>, gn, 256, 0, h->stream)(h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, h->uu,
                                              h->vv, h->scal, h->c);
@@ -932,8 +1009,10 @@ static int advance_dev(casl_handle *h) {
                                          h->sqd, h->emq, h->scal, nn);
   if ((rc = check_launch(h))) return rc;
   // stage 3
+  if ((rc = grad_fork(h))) return rc;
   if ((rc = inversion_dev(h, false))) return rc;
-  if ((rc = source_dev(h, 1))) return rc;
+  if ((rc = grad_join(h))) return rc;
+  if ((rc = source_prod(h, 1))) return rc;
   if (h->contex)
     CASL_K(k_nodes_rk<3>, gn, 256, 0, h->stream)(h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, h->uu,
                                              h->vv, h->scal, h->c);
@@ -941,9 +1020,11 @@ static int advance_dev(casl_handle *h) {
                                          h->sqd, h->emq, h->scal, nn);
   if ((rc = check_launch(h))) return rc;
   // stage 4
+  if ((rc = grad_fork(h))) return rc;
   CASL_K(k_advance_time, 1, 1, 0, h->stream)(h->scal);
   if ((rc = inversion_dev(h, false))) return rc;
-  if ((rc = source_dev(h, 2))) return rc;
+  if ((rc = grad_join(h))) return rc;
+  if ((rc = source_prod(h, 2))) return rc;
   if (h->contex)
     CASL_K(k_nodes_rk<4>, gn, 256, 0, h->stream)(h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, h->uu,
                                              h->vv, h->scal, h->c);
@@ -1321,6 +1402,7 @@ const char *casl_error_string(int code) {
     case CASL_EDOMAIN: return "node outside the domain or non-finite";
     case CASL_ETIMEOUT: return "bounded device wait timed out";
     case CASL_EUNSUPPORTED: return "unsupported";
+    case CASL_EIO: return "file input/output error";
   }
   return "unknown error";
 }
@@ -1351,6 +1433,10 @@ static int alloc_all(casl_handle *h) {
   CASL_CUDA_TRY(cudaMalloc(&h->bety, n * sizeof(double)));
   CASL_CUDA_TRY(cudaMalloc(&h->betac, n * sizeof(double)));
   CASL_CUDA_TRY(cudaMalloc(&h->tw, n * sizeof(double2)));
+  CASL_CUDA_TRY(cudaMalloc(&h->gtmp, (size_t)4 * nn * sizeof(double)));
+  CASL_CUDA_TRY(cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking));
+  CASL_CUDA_TRY(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
+  CASL_CUDA_TRY(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
   CASL_CUDA_TRY(cudaMalloc(&h->shell_idx, (size_t)nn * sizeof(int)));
   CASL_CUDA_TRY(cudaMalloc(&h->shell_off, (size_t)(2 * n + 2) * sizeof(int)));
   CASL_CUDA_TRY(cudaMalloc(&h->rkxf, n * sizeof(double)));
@@ -1373,7 +1459,13 @@ static void free_all(casl_handle *h) {
                   h->vv, h->emq, h->epq, h->qspre, h->sqs, h->sqd, h->qsi, h->qsf, h->qdi,
                   h->qdf, h->green, h->flo, h->fhi, h->qdiss, h->w[0], h->hrkx, h->hrky,
                   h->bety, h->betac, h->tw, h->fineJ, h->ljx, h->coarseC, h->part, h->scal,
-                  h->sx, h->sx2, h->shell_idx, h->shell_off, h->rkxf, h->rkyf};
+                  h->sx, h->sx2, h->shell_idx, h->shell_off, h->rkxf, h->rkyf, h->gtmp};
+  if (h->stream2) {
+    cudaStreamSynchronize(h->stream2);
+    cudaStreamDestroy(h->stream2);
+  }
+  if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+  if (h->ev_join) cudaEventDestroy(h->ev_join);
   for (void *p : ptrs)
     if (p) cudaFree(p);
   free(h->spmf_h);
@@ -1457,6 +1549,7 @@ int casl_create(const casl_params *p, int device, casl_handle **out) {
 void casl_destroy(casl_handle *h) {
   if (!h) return;
   cudaSetDevice(h->device);
+  io_release(h);
   cudaStreamSynchronize(h->stream);
   free_all(h);
   if (h->prof_ev) {
@@ -1473,16 +1566,28 @@ int casl_synchronize(casl_handle *h) {
   return CASL_OK;
 }
 
-static int put_scalars(casl_handle *h) {
+}  // extern "C"
+
+namespace casl {
+int put_scalars(casl_handle *h) {
   CASL_CUDA_TRY(cudaMemcpyAsync(h->scal, h->hscal, sizeof(Scalars), cudaMemcpyHostToDevice, h->stream));
   CASL_CUDA_TRY(cudaStreamSynchronize(h->stream));
   return CASL_OK;
 }
-static int get_scalars(casl_handle *h) {
+}  // namespace casl
+
+extern "C" {
+}  // extern "C"
+
+namespace casl {
+int get_scalars(casl_handle *h) {
   CASL_CUDA_TRY(cudaMemcpyAsync(h->hscal, h->scal, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
   CASL_CUDA_TRY(cudaStreamSynchronize(h->stream));
   return CASL_OK;
 }
+}  // namespace casl
+
+extern "C" {
 
 __global__ void k_to0(int *a, long long m, int off) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m;
@@ -1812,7 +1917,10 @@ __global__ void k_prepare(double *qs, double *qd, const double *qc, const double
   }
 }
 
-static int evo_init(casl_handle *h) {
+}  // extern "C"
+
+namespace casl {
+int evo_init(casl_handle *h) {
   long long nn = (long long)h->n * h->n;
   h->contex = h->nptq > 0;
   int rc = con2grid_to_spec(h, h->qc);
@@ -1820,6 +1928,9 @@ static int evo_init(casl_handle *h) {
   CASL_K(k_evo_init, grid_for(nn), 256, 0, h->stream)(h->qd, h->qspre, h->qs, h->qc, h->fhi, nn);
   return check_launch(h);
 }
+}  // namespace casl
+
+extern "C" {
 
 static int evo_prepare(casl_handle *h) {
   long long nn = (long long)h->n * h->n;
@@ -2041,6 +2152,19 @@ int casl_diagnostics(casl_handle *h, double out[4]) {
   return CASL_OK;
 }
 
+}  // extern "C"
+
+namespace casl {
+// Shell sums of the spectral field ss (device) into dspec[0..n] (device).
+int spec1d_dev(casl_handle *h, const double *ss, double *dspec) {
+  CASL_CUDA_TRY(cudaMemsetAsync(dspec, 0, (h->n + 1) * sizeof(double), h->stream));
+  CASL_K(k_spec1d, (32 * (h->kmax + 1) + 255) / 256, 256, 0, h->stream)(
+      ss, h->shell_off, h->shell_idx, h->n, h->kmax, dspec);
+  return check_launch(h);
+}
+}  // namespace casl
+
+extern "C" {
 int casl_spec1d(casl_handle *h, double *ss, double *spec, int iopt) {
   if (!h || !ss || !spec || (iopt != 0 && iopt != 1)) return CASL_EINVAL;
   cudaStream_t st = h->stream;
@@ -2049,9 +2173,8 @@ int casl_spec1d(casl_handle *h, double *ss, double *spec, int iopt) {
   CASL_CUDA_TRY(cudaMemcpyAsync(d, ss, nn * sizeof(double), cudaMemcpyHostToDevice, st));
   if (iopt == 1)
     CASL_K(k_mul_rksq, grid_for(nn), 256, 0, st)(d, h->rkxf, h->rkyf, h->n, nn);
-  CASL_CUDA_TRY(cudaMemsetAsync(dspec, 0, (h->n + 1) * sizeof(double), st));
-  CASL_K(k_spec1d, (32 * (h->kmax + 1) + 255) / 256, 256, 0, st)(d, h->shell_off, h->shell_idx, h->n,
-                                                               h->kmax, dspec);
+  int rc = spec1d_dev(h, d, dspec);
+  if (rc) return rc;
   CASL_CUDA_TRY(cudaMemcpyAsync(spec, dspec, (h->n + 1) * sizeof(double), cudaMemcpyDeviceToHost, st));
   if (iopt == 1)
     CASL_CUDA_TRY(cudaMemcpyAsync(ss, d, nn * sizeof(double), cudaMemcpyDeviceToHost, st));

@@ -18,14 +18,18 @@
 // / the store, which sets the thread mapping for coalescing.
 #pragma once
 
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace casl {
 
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+// Complex product with fused multiply-adds (transform outputs are compared
+// to the oracle within a tolerance, not bit for bit).
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+  return make_double2(__fma_rn(a.x, b.x, -(a.y * b.y)), __fma_rn(a.x, b.y, a.y * b.x));
 }
 __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
 // multiply by -i (FWD) or +i (inverse)
@@ -74,6 +78,14 @@ __device__ __forceinline__ void dft8(double2 *v) {
   v[7] = csub(e3, t3);
 }
 
+// A load functor may also provide pair(b, v, j) -> elements (j, j+1) for
+// even j, and a store functor pair(b, v, k, x) for (k, k+1): one 16-byte
+// access instead of two 8-byte ones where the elements are adjacent.
+template <class T, class = void>
+struct has_pair : std::false_type {};
+template <class T>
+struct has_pair<T, std::void_t<decltype(&T::pair)>> : std::true_type {};
+
 // Plain strided load / store functors: element (b, v, j) at p[b*bs + v*vs + j*es].
 struct LoadStrided {
   __host__ double bytes() const { return 8.0; }
@@ -82,6 +94,11 @@ struct LoadStrided {
   __device__ __forceinline__ double operator()(int b, int v, int j) const {
     return p[b * bs + (long long)v * vs + (long long)j * es];
   }
+  __device__ __forceinline__ double2 pair(int b, int v, int j) const {
+    const long long o = b * bs + (long long)v * vs + (long long)j * es;
+    if (es == 1) return *reinterpret_cast<const double2 *>(p + o);
+    return make_double2(p[o], p[o + es]);
+  }
 };
 struct StoreStrided {
   __host__ double bytes() const { return 8.0; }
@@ -89,6 +106,15 @@ struct StoreStrided {
   long long bs, vs, es;
   __device__ __forceinline__ void operator()(int b, int v, int k, double x) const {
     p[b * bs + (long long)v * vs + (long long)k * es] = x;
+  }
+  __device__ __forceinline__ void pair(int b, int v, int k, double2 x) const {
+    const long long o = b * bs + (long long)v * vs + (long long)k * es;
+    if (es == 1) {
+      *reinterpret_cast<double2 *>(p + o) = x;
+    } else {
+      p[o] = x.x;
+      p[o + es] = x.y;
+    }
   }
 };
 
@@ -233,7 +259,10 @@ __global__ void __launch_bounds__(RfftShape<LOGH, LVF || SVF>::NT, RfftShape<LOG
 #pragma unroll
       for (int m = 0; m < 8; m++) {
         int e = t + m * TPV;
-        x[m] = make_double2(ld(b, vg, 2 * e), ld(b, vg, 2 * e + 1));
+        if constexpr (has_pair<LD>::value)
+          x[m] = ld.pair(b, vg, 2 * e);
+        else
+          x[m] = make_double2(ld(b, vg, 2 * e), ld(b, vg, 2 * e + 1));
       }
     }
     rf_complex<LOGH, true>(x, S, t, tw, N);
@@ -336,8 +365,12 @@ __global__ void __launch_bounds__(RfftShape<LOGH, LVF || SVF>::NT, RfftShape<LOG
 #pragma unroll
       for (int m = 0; m < 8; m++) {
         int e = t + m * TPV;
-        st(b, vg, 2 * e, x[m].x * s);
-        st(b, vg, 2 * e + 1, x[m].y * s);
+        if constexpr (has_pair<ST>::value) {
+          st.pair(b, vg, 2 * e, make_double2(x[m].x * s, x[m].y * s));
+        } else {
+          st(b, vg, 2 * e, x[m].x * s);
+          st(b, vg, 2 * e + 1, x[m].y * s);
+        }
       }
     } else {
 #pragma unroll

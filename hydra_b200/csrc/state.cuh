@@ -14,6 +14,9 @@ struct casl_handle {
   casl::Consts c;
   int device;
   cudaStream_t stream;
+  cudaStream_t stream2;          // side stream of advance (source gradients)
+  cudaEvent_t ev_fork, ev_join;  // fork/join between the two
+  double *gtmp;                  // 4 fields of scratch for the side stream
   int last_cuda;
   int n;                 // nx == ny
   long long npm, nm;     // capacities
@@ -42,6 +45,7 @@ struct casl_handle {
   double *rkxf, *rkyf;         // filtered wavenumbers for K^2 (spec1d iopt = 1)
   int kmax, kmaxred;
   double *spmf_h, *alk_h;      // host, n+1 entries each
+  void *io;                    // output writer (thread + pinned staging), see io.cu
 
   // con2grid scratch
   int *fineJ;            // (nyf, nxf): row 0 = bottom level, rows 1.. = jump counts
@@ -88,6 +92,12 @@ int renode_host(casl_handle *h, const double *xd, const double *yd, int npd, dou
                 double *yr, int cap, int *npr);
 
 int sync_counts(casl_handle *h);    // device counts -> host copies
+int get_scalars(casl_handle *h);    // device scalars -> hscal
+int put_scalars(casl_handle *h);    // hscal -> device scalars
+int inversion_dev(casl_handle *h, bool reset);  // evolution.f90:494-520
+int evo_init(casl_handle *h);       // evolution.f90:96-131 (qc, qd, qspre)
+int spec1d_dev(casl_handle *h, const double *ss, double *dspec);
+void io_release(casl_handle *h);    // joins the output writer, frees its staging
 
 // Opt-in phase trace (environment variable CASL_TRACE=1): records CUDA
 // events at named points on the handle's stream and prints the device time

@@ -39,6 +39,7 @@ extern "C" {
 #define CASL_EDOMAIN 5     /* a node left the domain or became non-finite */
 #define CASL_ETIMEOUT 6    /* a bounded device-side wait gave up */
 #define CASL_EUNSUPPORTED 7
+#define CASL_EIO 8         /* a file could not be opened, read or written */
 
 /* ---- parameters (parameters.f90 / constants.f90 of QG caps) ------------- */
 typedef struct casl_params {
@@ -174,6 +175,45 @@ int casl_spec1d(casl_handle *h, double *ss, double *spec, int iopt);
  * and, when non-NULL, spmf and alk (max(nx,ny)+1 entries each) as savegrid
  * (evolution.f90:683-719) uses them. */
 int casl_spec_tables(casl_handle *h, int *kmax, int *kmaxred, double *spmf, double *alk);
+
+/* ---- output files and restart (row f1) ----------------------------------- */
+/* The caps output files, byte-compatible with the reference's gfortran I/O
+ * (evolution.f90:582-583, 648-774; caps.f90:233-248; common.f90:30-100).
+ * Paths are files; `dir` arguments are the run directory holding cont/.
+ * ASCII writers append one formatted line (spectrum: header + kmaxred lines)
+ * with the reference's edit descriptors; sequential records carry 4-byte
+ * length markers; r4 files are direct access with recl = 4*(nx*ny+1). */
+int casl_io_append_synopsis(const char *path, int nq, int nptq, double t, double qjump);
+int casl_io_append_ene(const char *path, double tgrid, double ekin, double epot);
+int casl_io_append_norms(const char *path, double tgrid, double qql2);
+int casl_io_append_spectrum(const char *path, double tgrid, double sumqspec, double qql2,
+                            int kmaxred, const double *alk, const double *qspec);
+int casl_io_append_monitor(const char *path, double t, double cfl, double zzrms, double zzmax,
+                           double uumax, double twist);
+int casl_io_append_complexity(const char *path, double t, int nq, int nptq);
+int casl_io_write_index(const char *path, int nq, const int *npq, const int *i1q, const int *indq);
+int casl_io_read_index(const char *path, int nq, int *npq, int *i1q, int *indq);
+int casl_io_write_nodes(const char *path, int nptq, const double *xq, const double *yq);
+int casl_io_read_nodes(const char *path, int nptq, double *xq, double *yq);
+int casl_io_write_r4(const char *path, int irec, int nx, int ny, float t, const float *a);
+int casl_io_read_r4(const char *path, int irec, int nx, int ny, float *t, float *a);
+int casl_io_read_synopsis(const char *path, int iind, int *nq, int *nptq, double *t,
+                          double *qjump);
+
+/* savecont (evolution.f90:731-774) of the current state into dir/cont/
+ * (record icrec, 1..999).  The device work and copies are enqueued on the
+ * handle's stream and a host thread writes the files; the call returns
+ * without waiting for them.  casl_io_wait joins the writer and returns its
+ * status; the next save, readcont and casl_destroy join it too. */
+int casl_savecont(casl_handle *h, const char *dir, int icrec);
+/* savegrid (evolution.f90:648-727) at the current time (no interpolation
+ * between steps): ene.asc, norms.asc, spectra.asc and record irec of qq.r4,
+ * written by the same host thread. */
+int casl_savegrid(casl_handle *h, const char *dir, int irec);
+int casl_io_wait(casl_handle *h);
+/* readcont (common.f90:30-100) followed by init (evolution.f90:96-131):
+ * contours, residual and time of save iind; qs = ptospc(con2grid + qr). */
+int casl_readcont(casl_handle *h, const char *dir, int iind);
 
 /* ---- con2grid without device allocation ---------------------------------- */
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc
