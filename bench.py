@@ -64,13 +64,14 @@ class ClockSampler:
     def __init__(self, device):
         self.device = device
         self.proc = None
-        self.lines = []
+        self.lines = []  # (arrival time, csv line)
+        self.window = None
 
     def start(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -79,7 +80,13 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
+
+    def mark(self, t0, t1):
+        """The timed region in wall-clock seconds; only samples that arrive
+        inside it are kept (the sampler runs from before the warm-up so that
+        its start-up does not fall into the region)."""
+        self.window = (t0, t1)
 
     def stop(self):
         if not self.proc:
@@ -91,7 +98,10 @@ class ClockSampler:
             self.proc.kill()
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        lines = self.lines
+        if self.window:
+            lines = [l for l in lines if self.window[0] <= l[0] <= self.window[1]]
+        for _, ln in lines:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
                 continue
@@ -224,6 +234,8 @@ def run_gpu(a):
     g = CaslGPU(a.n, ncontq=a.levels, force_surgery=1, dtmax=a.dtmax,
                 npm=16_000_000, nm=1_000_000, device=local)
     g.initialise(q0)
+    clocks = ClockSampler(local)
+    clocks.start()
     for _ in range(a.warmup):
         g.step(1)
     stream = torch.cuda.ExternalStream(g.stream_ptr(), device=local)
@@ -234,9 +246,8 @@ def run_gpu(a):
         torch.cuda.synchronize()
 
     # ---- resident-data timed region ------------------------------------------------
-    clocks = ClockSampler(local)
-    clocks.start()
     barrier()
+    wall0 = time.time()
     ns0 = g.scalar("node_steps")
     l0 = g.launch_count()
     g.profile(1)  # the transform passes
@@ -246,6 +257,7 @@ def run_gpu(a):
         g.step(1)
     ev1.record(stream)
     barrier()
+    clocks.mark(wall0, time.time())
     ms = ev0.elapsed_time(ev1)
     launches = g.launch_count() - l0
     fft_ms, fft_n, fft_bytes = g.profile_read()
@@ -370,7 +382,7 @@ def run_e2e(g, a, stream, torch):
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["hydra", "reference"], default="hydra")
     ap.add_argument("--n", type=int, default=1024)

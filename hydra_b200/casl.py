@@ -108,6 +108,8 @@ SIGNATURES = {
     "casl_savegrid": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int]),
     "casl_io_wait": (C.c_int, [C.c_void_p]),
     "casl_readcont": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int]),
+    "casl_genfg": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                             C.POINTER(C.c_float)]),
 }
 
 
@@ -326,6 +328,17 @@ class CaslGPU:
     def readcont(self, rundir, iind):
         """readcont (common.f90:30-100) + init: restart from save iind."""
         self._check(self.lib.casl_readcont(self.h, os.fsencode(rundir), int(iind)), "casl_readcont")
+
+    def genfg(self, ix1v=1, nxv=None, iy1v=1, nyv=None, stride=1):
+        """genfg (post/genfg.f90:79-194): ultra-fine PV of the contours plus the
+        residual qr, float32 (nxv, nyv) array (iy fastest), 1-based starts."""
+        nu = 16 * self.nx
+        nxv = nxv or (nu - ix1v) // stride + 1
+        nyv = nyv or (nu - iy1v) // stride + 1
+        out = np.zeros((nxv, nyv), np.float32)
+        self._check(self.lib.casl_genfg(self.h, ix1v, nxv, iy1v, nyv, stride,
+                                        out.ctypes.data_as(C.POINTER(C.c_float))), "casl_genfg")
+        return out
 
     def spec1d(self, ss, iopt=0):
         """spec1d (spectral.f90:370-424) of the spectral field ss(nx,ny), given

@@ -1168,3 +1168,66 @@ int recontour_dev(casl_handle *h, const double *qq) {
 }
 
 }  // namespace casl
+
+// ---------------------------------------------------------------------------
+// genfg (post/genfg.f90:79-194): the PV on the ultra-fine grid as an image
+// ---------------------------------------------------------------------------
+namespace casl {
+
+// out(iy, ix) = real(qa(iy1 + iy*stride, ix1 + ix*stride)), periodic, 0-based
+// starts, out column-major (nyv, nxv)
+__global__ void k_gf_gather(const double *__restrict__ qa, int nxu, int nyu, int ix1, int nxv,
+                            int iy1, int nyv, int stride, float *__restrict__ out) {
+  const long long m = (long long)nxv * nyv;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < m;
+       t += (long long)gridDim.x * blockDim.x) {
+    int iy = (int)(t % nyv), ix = (int)(t / nyv);
+    long long sx = ((long long)ix1 + (long long)ix * stride) % nxu;
+    long long sy = ((long long)iy1 + (long long)iy * stride) % nyu;
+    out[t] = (float)qa[sx * nyu + sy];
+  }
+}
+
+}  // namespace casl
+
+using namespace casl;
+
+extern "C" int casl_genfg(casl_handle *h, int ix1v, int nxv, int iy1v, int nyv, int stride,
+                          float *out) {
+  if (!h || !out) return CASL_EINVAL;
+  const Consts &c = h->c;
+  const int nxu = c.nxu, nyu = c.nyu;
+  if (ix1v < 1 || ix1v > nxu || iy1v < 1 || iy1v > nyu || nxv < 1 || nyv < 1 || stride < 1 ||
+      (long long)(nxv - 1) * stride >= nxu || (long long)(nyv - 1) * stride >= nyu)
+    return CASL_EINVAL;
+  int rc = sync_counts(h);
+  if (rc) return rc;
+  cudaStream_t st = h->stream;
+  const long long NU = (long long)nxu * nyu, m = (long long)nxv * nyv;
+  size_t need = (size_t)NU * 12 + (size_t)nxu * 4 + (size_t)m * 4 + ((size_t)64 << 20);
+  RC_TRY(ensure_scratch(h, need));
+  Arena ar{(char *)h->sx, h->sx_bytes, 0};
+  double *qa = ar.get<double>(NU);
+  int *Lu = ar.get<int>(NU);
+  int *ljx = ar.get<int>(nxu);
+  unsigned long long *lsum = ar.get<unsigned long long>(4);
+  double *part = ar.get<double>(2 * 4096);
+  float *img = ar.get<float>(m);
+  if (ar.failed) return CASL_ENOMEM;
+  // con2ugrid (congen.f90:338-441), always called by genfg, then the
+  // bilinear residual qr (genfg.f90:95-109)
+  CASL_CUDA_TRY(cudaMemsetAsync(Lu, 0, (size_t)NU * sizeof(int), st));
+  CASL_CUDA_TRY(cudaMemsetAsync(ljx, 0, (size_t)nxu * sizeof(int), st));
+  CASL_CUDA_TRY(cudaMemsetAsync(lsum, 0, sizeof(unsigned long long), st));
+  if (h->nptq > 0)
+    CASL_K(k_u_scatter, gsz(h->nptq), 256, 0, st)(h->xq, h->yq, h->nextq, h->nptq, h->qjump, Lu,
+                                              ljx, c, &h->scal->error);
+  CASL_K(k_u_lbot, 1, 1024, 0, st)(ljx, Lu, nxu, nyu);
+  CASL_K(k_u_colscan, (nxu * 32 + 255) / 256, 256, 0, st)(Lu, nxu, nyu, lsum);
+  CASL_K(k_u_field, 4096, 256, 0, st)(Lu, lsum, h->qr, h->qjump, 1, qa, part, c);
+  CASL_K(k_gf_gather, gsz(m), 256, 0, st)(qa, nxu, nyu, ix1v - 1, nxv, iy1v - 1, nyv, stride, img);
+  RC_TRY(check_launch(h));
+  CASL_CUDA_TRY(cudaMemcpyAsync(out, img, (size_t)m * sizeof(float), cudaMemcpyDeviceToHost, st));
+  CASL_CUDA_TRY(cudaStreamSynchronize(st));
+  return fetch_err(h);
+}

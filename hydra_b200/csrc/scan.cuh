@@ -146,6 +146,82 @@ __global__ void __launch_bounds__(SCAN_BLOCK) k_scan_small(const T *__restrict__
   if (threadIdx.x == 0 && grand) *grand = carry;
 }
 
+// Two-pass scan for mid-size arrays: per-tile sums, then each tile adds the
+// sum of the tiles before it (read by the tile's own block, so no third
+// kernel) and scans itself.  VEC: items move as one 16-byte access per
+// thread (in/out 16-byte aligned, 4-byte T).
+template <class T, bool VEC>
+__device__ __forceinline__ void scan_load(const T *__restrict__ in, long long base, long long n,
+                                          T (&v)[SCAN_ITEMS]) {
+  if (VEC && base + SCAN_ITEMS <= n) {
+    int4 q = *reinterpret_cast<const int4 *>(in + base);
+    v[0] = (T)q.x; v[1] = (T)q.y; v[2] = (T)q.z; v[3] = (T)q.w;
+  } else {
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; k++) v[k] = (base + k < n) ? in[base + k] : T(0);
+  }
+}
+
+template <class T, bool VEC>
+__global__ void __launch_bounds__(SCAN_BLOCK) k_scan_tilesum(const T *__restrict__ in,
+                                                             T *__restrict__ tile_tot, long long n) {
+  __shared__ T part[32];
+  long long base = (long long)blockIdx.x * SCAN_TILE + (long long)threadIdx.x * SCAN_ITEMS;
+  T v[SCAN_ITEMS];
+  scan_load<T, VEC>(in, base, n, v);
+  T s = v[0] + v[1] + v[2] + v[3];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    T w = part[threadIdx.x];
+    for (int o = 16; o > 0; o >>= 1) w += __shfl_down_sync(0xffffffffu, w, o);
+    if (threadIdx.x == 0) tile_tot[blockIdx.x] = w;
+  }
+}
+
+template <class T, bool VEC>
+__global__ void __launch_bounds__(SCAN_BLOCK) k_scan_apply(const T *in, T *out,
+                                                           const T *__restrict__ tile_tot,
+                                                           long long n, T *__restrict__ grand) {
+  __shared__ T part[32];
+  __shared__ T tot;
+  // offset of this tile: sum of the earlier tiles' totals (fixed order)
+  T o = 0;
+  for (int i = threadIdx.x; i < (int)blockIdx.x; i += SCAN_BLOCK) o += tile_tot[i];
+  for (int d = 16; d > 0; d >>= 1) o += __shfl_down_sync(0xffffffffu, o, d);
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = o;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    T w = part[threadIdx.x];
+    for (int d = 16; d > 0; d >>= 1) w += __shfl_down_sync(0xffffffffu, w, d);
+    if (threadIdx.x == 0) part[0] = w;
+  }
+  __syncthreads();
+  const T off = part[0];
+  __syncthreads();
+  long long base = (long long)blockIdx.x * SCAN_TILE + (long long)threadIdx.x * SCAN_ITEMS;
+  T v[SCAN_ITEMS];
+  scan_load<T, VEC>(in, base, n, v);
+  T ex = block_excl_scan<T>(v[0] + v[1] + v[2] + v[3], &tot) + off;
+  T r[SCAN_ITEMS];
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; k++) {
+    r[k] = ex;
+    ex += v[k];
+  }
+  if (VEC && base + SCAN_ITEMS <= n) {
+    *reinterpret_cast<int4 *>(out + base) = make_int4((int)r[0], (int)r[1], (int)r[2], (int)r[3]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; k++)
+      if (base + k < n) out[base + k] = r[k];
+  }
+  if (grand && blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) *grand = off + tot;
+}
+
+constexpr int SCAN_TWO_PASS_MAX_TILES = 2048;
+
 // out[i] = sum_{j<i} in[j]; *grand (device, optional) = sum of all.
 // in and out may alias.  tmp needs ceil(n/SCAN_TILE) elements.
 template <class T>
@@ -156,6 +232,18 @@ int exclusive_scan(cudaStream_t st, const T *in, T *out, long long n, T *tmp, T 
   }
   if (n <= 16 * SCAN_TILE) {
     CASL_K(k_scan_small<T>, 1, SCAN_BLOCK, 0, st)(in, out, n, grand);
+    return (int)cudaGetLastError();
+  }
+  if ((n + SCAN_TILE - 1) / SCAN_TILE <= SCAN_TWO_PASS_MAX_TILES) {
+    const int tiles = (int)((n + SCAN_TILE - 1) / SCAN_TILE);
+    const bool vec = sizeof(T) == 4 && (((uintptr_t)in | (uintptr_t)out) & 15) == 0;
+    if (vec) {
+      CASL_K((k_scan_tilesum<T, true>), tiles, SCAN_BLOCK, 0, st)(in, tmp, n);
+      CASL_K((k_scan_apply<T, true>), tiles, SCAN_BLOCK, 0, st)(in, out, tmp, n, grand);
+    } else {
+      CASL_K((k_scan_tilesum<T, false>), tiles, SCAN_BLOCK, 0, st)(in, tmp, n);
+      CASL_K((k_scan_apply<T, false>), tiles, SCAN_BLOCK, 0, st)(in, out, tmp, n, grand);
+    }
     return (int)cudaGetLastError();
   }
   int tiles = (int)((n + SCAN_TILE - 1) / SCAN_TILE);

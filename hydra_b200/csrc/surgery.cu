@@ -18,6 +18,7 @@
 //      its lowest node index (the reference's avail() walk); they are found
 //      by pointer jumping over runs of consecutive nodes, gathered into walk
 //      order and renoded in parallel (renode.cu).
+#include <limits.h>
 #include <math.h>
 #include <stdio.h>
 
@@ -255,22 +256,6 @@ __global__ void k_sg_place_nodes(const int *__restrict__ nbox_of, int npt,
 }
 
 // Restore the reference's per-box order (ascending node before the segment).
-__global__ void k_sg_sort_boxes(const int *__restrict__ kb1, const int *__restrict__ bcnt,
-                                const int *__restrict__ nbox_dev, int *__restrict__ bnode) {
-  const int nbox = *nbox_dev;
-  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nbox; b += gridDim.x * blockDim.x) {
-    int s = kb1[b], n = bcnt[b];
-    for (int a = 1; a < n; a++) {
-      int v = bnode[s + a], k = a - 1;
-      while (k >= 0 && bnode[s + k] > v) {
-        bnode[s + k + 1] = bnode[s + k];
-        k--;
-      }
-      bnode[s + k + 1] = v;
-    }
-  }
-}
-
 // The two tests of contours.f90:542-563.
 __device__ __forceinline__ bool surg_test(double xi, double yi, double xs, double ys, double dxs,
                                           double dys, double dsqs, const Consts &c) {
@@ -388,25 +373,28 @@ __global__ void k_sg_replay(SurgState S, const LevelDesc *__restrict__ lev,
     int i = nextq[ib];
     double xi = xq[i], yi = yq[i];
     int mb = node_box(xi, yi, L, c);
-    int k = S.kb1[mb];
-    const int kend = k + S.bcnt[mb];
-    while (k < kend) {
-      int kk = k + lane;
-      bool pass = false;
-      if (kk < kend) {
+    const int kbeg = S.kb1[mb];
+    const int kend = kbeg + S.bcnt[mb];
+    // The reference walks the box's segments in list order and continues
+    // after each reconnection with the moved node.  The box list is stored
+    // unordered, so each round takes the passing segment with the smallest
+    // list index above the last one taken.
+    int thr = -1;
+    while (true) {
+      int best = INT_MAX;
+      for (int kk = kbeg + lane; kk < kend; kk += 32) {
         int isb = S.bnode[kk];
-        int is = nextq[isb];
-        if (!(is == ib || is == i)) pass = surg_test(xi, yi, xq[is], yq[is], dx[is], dy[is], dsq[is], c);
+        if (isb > thr && isb < best) {
+          int is = nextq[isb];
+          if (!(is == ib || is == i) && surg_test(xi, yi, xq[is], yq[is], dx[is], dy[is], dsq[is], c))
+            best = isb;
+        }
       }
-      unsigned pb = __ballot_sync(0xffffffffu, pass);
-      if (!pb) {
-        k += 32;
-        continue;
-      }
-      kk = k + __ffs(pb) - 1;
+      for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
+      if (best == INT_MAX) break;
       int inew = 0, tsb = 0;
       if (lane == 0) {
-        int isb = S.bnode[kk];
+        int isb = best;
         int is = nextq[isb];
         double xx = xq[is] - xq[i];
         double delx = xx - c.ellx * f_dint(xx * c.hlxi);
@@ -459,7 +447,7 @@ __global__ void k_sg_replay(SurgState S, const LevelDesc *__restrict__ lev,
       xi = xq[i];
       yi = yq[i];
       if (i == ib) break;
-      k = kk + 1;
+      thr = best;
     }
     pos = ib + 1;
   }
@@ -755,7 +743,6 @@ int surgery_dev(casl_handle *h) {
   exclusive_scan<int>(st, bcnt, kb1, nbox_cap, tmpi, dtot + 4);
   CASL_CUDA_TRY(cudaMemsetAsync(cursor, 0, (size_t)nbox_cap * sizeof(int), st));
   CASL_K(k_sg_place, gs(ne_cap), 256, 0, st)(ebox, eib, dtot + 2, kb1, cursor, bnode);
-  CASL_K(k_sg_sort_boxes, gb, 256, 0, st)(kb1, bcnt, dtot + 1, bnode);
   exclusive_scan<int>(st, nbcnt, nb1, nbox_cap, tmpi, dtot + 5);
   CASL_CUDA_TRY(cudaMemsetAsync(cursor, 0, (size_t)nbox_cap * sizeof(int), st));
   CASL_K(k_sg_place_nodes, g, 256, 0, st)(nbox_of, npt, nb1, cursor, nbnode);

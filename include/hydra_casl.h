@@ -215,6 +215,14 @@ int casl_io_wait(casl_handle *h);
  * contours, residual and time of save iind; qs = ptospc(con2grid + qr). */
 int casl_readcont(casl_handle *h, const char *dir, int iind);
 
+/* genfg (post/genfg.f90:79-194): the PV on the ultra-fine (16n)^2 grid,
+ * con2ugrid of the current contours plus the bilinear interpolation of the
+ * residual field qr (CASL_QR, e.g. as casl_readcont leaves it), as float32.
+ * out is (nyv, nxv) column-major with out(iy, ix) = qa(iy1v + (iy-1)*stride,
+ * ix1v + (ix-1)*stride), 1-based and periodic: stride 1 over the whole grid
+ * is genfg's option 1, stride n its option 2, a wrapped window option 3. */
+int casl_genfg(casl_handle *h, int ix1v, int nxv, int iy1v, int nyv, int stride, float *out);
+
 /* ---- con2grid without device allocation ---------------------------------- */
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc
  * -- their GPU memory is handed out by their own pool or another framework,

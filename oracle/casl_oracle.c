@@ -1813,6 +1813,28 @@ static int ugrid2con(o_state *s, ugrid *g) {
 }
 
 /* recontour (congen.f90:24-128); qq(ny,nx) is the residual (or full) field. */
+/* genfg's ugridsave (post/genfg.f90:79-113): con2ugrid of the contours
+ * plus the bilinear interpolation of the residual qq, as float32 in the
+ * (nyu, nxu) column-major layout of rqa. */
+void o_genfg(o_state *s, const double *qq, float *out) {
+  int nxu = s->nxu, nyu = s->nyu;
+  ugrid g;
+  g.ldq = (size_t)nyu + 1;
+  g.qa = xcalloc(g.ldq * nxu, sizeof(double));
+  con2ugrid(s, &g);
+  for (int ix = 1; ix <= nxu; ix++) {
+    int ixf = s->ixfw[ix], ix0 = s->ix0w[ix], ix1 = s->ix1w[ix];
+    for (int iy = 1; iy <= nyu; iy++) {
+      int iyf = s->iyfw[iy], iy0 = s->iy0w[iy], iy1 = s->iy1w[iy];
+      int w = (ixf - 1) * 16 + (iyf - 1);
+      double v = UQA(&g, iy, ix) + s->w00[w] * qq[PHY(s, iy0, ix0)] + s->w10[w] * qq[PHY(s, iy1, ix0)] +
+                 s->w01[w] * qq[PHY(s, iy0, ix1)] + s->w11[w] * qq[PHY(s, iy1, ix1)];
+      out[(size_t)(ix - 1) * nyu + (iy - 1)] = (float)v;
+    }
+  }
+  free(g.qa);
+}
+
 int o_recontour(o_state *s, double *qq) {
   int nx = s->nx, ny = s->ny, nxu = s->nxu, nyu = s->nyu;
   ugrid g;

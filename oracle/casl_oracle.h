@@ -118,6 +118,8 @@ void o_diagnostics(o_state *s, double *out4);
  * (spectral.f90:109-134); arrays of max(nx,ny)+1 entries. */
 void o_spec1d(o_state *s, double *ss, double *spec, int iopt);
 void o_spec_tables(o_state *s, int *kmax, int *kmaxred, double *spmf, double *alk);
+/* genfg's ultra-fine PV (post/genfg.f90:79-113): float32 (nyu, nxu). */
+void o_genfg(o_state *s, const double *qq, float *out);
 
 #ifdef __cplusplus
 }

@@ -86,6 +86,7 @@ def lib():
         L.o_diagnostics.argtypes = [C.c_void_p, dp]
         L.o_spec1d.argtypes = [C.c_void_p, dp, dp, C.c_int]
         L.o_spec_tables.argtypes = [C.c_void_p, ip, ip, dp, dp]
+        L.o_genfg.argtypes = [C.c_void_p, dp, C.POINTER(C.c_float)]
     return _lib
 
 
@@ -285,6 +286,14 @@ class Oracle:
         spec = np.zeros(max(self.nx, self.nx) + 1)
         lib().o_spec1d(self.h, _dp(a), _dp(spec), int(iopt))
         return spec, a
+
+    def genfg(self, qq):
+        """genfg's ultra-fine PV (post/genfg.f90:79-113) of the current contours
+        plus the residual qq (physical, (nx, ny) array), float32 (nxu, nyu)."""
+        r = np.ascontiguousarray(qq, np.float64)
+        out = np.zeros((16 * self.nx, 16 * self.nx), np.float32)
+        lib().o_genfg(self.h, _dp(r), out.ctypes.data_as(C.POINTER(C.c_float)))
+        return out
 
     def spec_tables(self):
         """kmax, kmaxred, spmf, alk of init_spectral (spectral.f90:109-134)."""

@@ -90,3 +90,32 @@ def test_savegrid_matches_oracle(oracle_mod, gpu_lib, tmp_path):
     ref = o.spctop(o.field("qq"))
     assert np.abs(q4 - ref).max() <= 1e-6 * np.abs(ref).max()
     g.close()
+
+
+def test_genfg_matches_oracle(oracle_mod, gpu_lib):
+    """genfg's ultra-fine PV (post/genfg.f90:79-194): con2ugrid of the
+    contours plus the bilinear residual, as float32; strided and wrapped
+    window views are slices of the full image."""
+    from hydra_b200.casl import CaslGPU
+
+    n = 32
+    o = oracle_mod.Oracle(n, ncontq=10, force_surgery=1, dtmax=0.05)
+    o.initialise(random_pv(n, 4.0, 5))
+    o.step()
+    g = CaslGPU(n, ncontq=10, force_surgery=1, dtmax=0.05)
+    g.set_contours(o.contours())
+    rng = np.random.default_rng(6)
+    qr = 0.3 * rng.standard_normal((n, n))
+    g.set_field("qr", qr)
+    ref = o.genfg(qr)
+    full = g.genfg()
+    assert full.shape == ref.shape == (16 * n, 16 * n)
+    # integer-exact contour part; the residual terms agree to FP64 rounding
+    assert np.abs(full - ref).max() <= 1e-6 * np.abs(ref).max()
+    assert np.array_equal(g.genfg(stride=4), full[::4, ::4])
+    nu = 16 * n
+    win = g.genfg(ix1v=nu - 40 + 1, nxv=100, iy1v=7, nyv=nu)  # wraps in x and y
+    cols = [(nu - 40 + i) % nu for i in range(100)]
+    rows = [(6 + i) % nu for i in range(nu)]
+    assert np.array_equal(win, full[np.ix_(cols, rows)])
+    g.close()

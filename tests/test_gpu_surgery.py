@@ -91,3 +91,21 @@ def test_surgery_matches_oracle(oracle_mod, gpu64, seed, steps):
     o.surgery()
     gpu64.surgery()
     compare_contours(o.contours(), gpu64.contours())
+
+
+def test_surgery_matches_oracle_large(oracle_mod, gpu_lib):
+    """~120k nodes at 256^2: the binning, rebuild and renode scans run their
+    multi-tile paths (more than 16 tiles of 4096)."""
+    from hydra_b200.casl import CaslGPU
+    n = 256
+    o = oracle_mod.Oracle(n, ncontq=40, force_surgery=1, dtmax=0.05)
+    o.initialise(random_pv(n, 8.0, 4))
+    o.step()
+    c0 = o.contours()
+    assert c0["nptq"] > 16 * 4096
+    g = CaslGPU(n, ncontq=40, force_surgery=1, dtmax=0.05)
+    g.set_contours(c0)
+    o.surgery()
+    g.surgery()
+    compare_contours(o.contours(), g.contours())
+    g.close()
