@@ -322,7 +322,8 @@ __device__ void mark_affected(SurgState &S, const LevelDesc &L, int j, int ib, c
 
 // One warp per level replays contours.f90:528-613 at pending nodes.
 __global__ void k_sg_replay(SurgState S, const LevelDesc *__restrict__ lev,
-                            const int *__restrict__ nlev_dev, Consts c, int *nsurg) {
+                            const int *__restrict__ nlev_dev, Consts c, int *nsurg,
+                            int *__restrict__ stats) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (warp >= *nlev_dev) return;
@@ -335,16 +336,31 @@ __global__ void k_sg_replay(SurgState S, const LevelDesc *__restrict__ lev,
   double *xq = S.xq, *yq = S.yq, *dx = S.dx, *dy = S.dy, *dsq = S.dsq;
   int *nextq = S.nextq;
   const double f12 = 0.5;
-  int count = 0;
+  int count = 0, npend = 0;
   long long pos = L.ibeg;
   while (pos <= L.iend) {
     int ib;
-    if ((pos & 15) == 0 && pos + 512 <= (long long)L.iend + 1) {
+    // Windows start at the 16-aligned position at or below pos, so the wide
+    // path is taken whatever the level's first node; flags below pos (already
+    // visited, or another level's) are masked out.
+    const long long base = pos & ~15LL;
+    if (base + 512 <= (long long)L.iend + 1) {
       // 512 flags per step: one 16-byte load per lane
-      uint4 v = reinterpret_cast<const uint4 *>(pend + pos)[lane];
+      uint4 v = reinterpret_cast<const uint4 *>(pend + base)[lane];
+      if (lane == 0 && pos > base) {
+        const int sh = (int)(pos - base);  // 1..15 leading bytes to drop
+        unsigned w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const int drop = sh - 4 * q;  // bytes of word q below pos
+          if (drop >= 4) w[q] = 0u;
+          else if (drop > 0) w[q] &= ~0u << (8 * drop);
+        }
+        v = make_uint4(w[0], w[1], w[2], w[3]);
+      }
       unsigned b = __ballot_sync(0xffffffffu, (v.x | v.y | v.z | v.w) != 0u);
       if (!b) {
-        pos += 512;
+        pos = base + 512;
         continue;
       }
       const int f = __ffs(b) - 1;
@@ -358,18 +374,19 @@ __global__ void k_sg_replay(SurgState S, const LevelDesc *__restrict__ lev,
           }
       }
       off = __shfl_sync(0xffffffffu, off, f);
-      ib = (int)(pos + 16 * f + off);
+      ib = (int)(base + 16 * f + off);
     } else {
-      long long idx = pos + lane;
-      bool fl = idx <= L.iend && pend[idx];
+      long long idx = base + lane;
+      bool fl = idx >= pos && idx <= L.iend && pend[idx];
       unsigned b = __ballot_sync(0xffffffffu, fl);
       if (!b) {
-        pos += 32;
+        pos = base + 32;
         continue;
       }
-      ib = (int)(pos + __ffs(b) - 1);
+      ib = (int)(base + __ffs(b) - 1);
     }
     __syncwarp();
+    npend++;
     int i = nextq[ib];
     double xi = xq[i], yi = yq[i];
     int mb = node_box(xi, yi, L, c);
@@ -452,6 +469,10 @@ __global__ void k_sg_replay(SurgState S, const LevelDesc *__restrict__ lev,
     pos = ib + 1;
   }
   if (lane == 0 && count) atomicAdd(nsurg, count);
+  if (stats && lane == 0) {  // trace only: pending nodes visited, surgeries
+    stats[2 * warp] = npend;
+    stats[2 * warp + 1] = count;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -751,10 +772,29 @@ int surgery_dev(casl_handle *h) {
   CASL_K(k_sg_candidates, g, 256, 0, st)(S, dlev, npt, nbox_of, c);
   tr.point("candidates");
   CASL_CUDA_TRY(cudaMemsetAsync(dtot + 3, 0, sizeof(int), st));
-  CASL_K(k_sg_replay, (nq * 32 + 127) / 128, 128, 0, st)(S, dlev, dtot + 0, c, dtot + 3);
+  int *stats = tr.on ? ar.get<int>(2 * (size_t)nq) : nullptr;
+  if (stats) CASL_CUDA_TRY(cudaMemsetAsync(stats, 0, 2 * (size_t)nq * sizeof(int), st));
+  CASL_K(k_sg_replay, (nq * 32 + 127) / 128, 128, 0, st)(S, dlev, dtot + 0, c, dtot + 3, stats);
   rc = check_launch(h);
   if (rc) return rc;
   tr.point("replay");
+  if (stats) {
+    std::vector<int> hs(2 * (size_t)nq);
+    int nlev = 0;
+    CASL_CUDA_TRY(cudaMemcpyAsync(hs.data(), stats, hs.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CASL_CUDA_TRY(cudaMemcpyAsync(&nlev, dtot, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CASL_CUDA_TRY(cudaStreamSynchronize(st));
+    long long sp = 0, ss = 0;
+    int mp = 0, ms = 0, wl = 0;
+    for (int l = 0; l < nlev; l++) {
+      sp += hs[2 * l];
+      ss += hs[2 * l + 1];
+      if (hs[2 * l] > mp) { mp = hs[2 * l]; wl = l; }
+      ms = std::max(ms, hs[2 * l + 1]);
+    }
+    fprintf(stderr, "[casl trace] replay: %d levels, pending %lld (max %d at level %d, %d surgeries there), surgeries %lld (max %d)\n",
+            nlev, sp, mp, wl, hs[2 * wl + 1], ss, ms);
+  }
   rc = rebuild_and_renode(h, ar, npt, lvl, dlev);
   if (rc) return rc;
   tr.point("rebuild+renode");
