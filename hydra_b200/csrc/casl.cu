@@ -958,79 +958,83 @@ static int source_prod(casl_handle *h, int lev) {
 }  // namespace casl
 
 // advance (evolution.f90:166-326)
-// The gradient transforms of source run on the handle's second stream: fork
-// after the last writer of qs/qd, join before the products need them.
-static int grad_fork(casl_handle *h) {
+// advance on two streams.  The side stream runs the four gradient
+// transforms of source (they read only qs and qd) beside con2grid and the
+// inversion, which are latency-bound.  Events: ev_fork marks a point of the
+// main stream the side stream waits for, ev_grad the gradients' end.
+static int side_after_main(casl_handle *h) {
   CASL_CUDA_TRY(cudaEventRecord(h->ev_fork, h->stream));
   CASL_CUDA_TRY(cudaStreamWaitEvent(h->stream2, h->ev_fork, 0));
-  cudaStream_t a = h->stream;
-  h->stream = h->stream2;
-  int rc = source_grad(h);
-  h->stream = a;
-  if (rc) return rc;
-  CASL_CUDA_TRY(cudaEventRecord(h->ev_join, h->stream2));
   return CASL_OK;
 }
 
-static int grad_join(casl_handle *h) {
-  CASL_CUDA_TRY(cudaStreamWaitEvent(h->stream, h->ev_join, 0));
+static int on_side(casl_handle *h, int (*fn)(casl_handle *, int), int arg, cudaEvent_t done) {
+  cudaStream_t a = h->stream;
+  h->stream = h->stream2;
+  int rc = fn(h, arg);
+  h->stream = a;
+  if (rc) return rc;
+  CASL_CUDA_TRY(cudaEventRecord(done, h->stream2));
   return CASL_OK;
+}
+
+static int main_after(casl_handle *h, cudaEvent_t ev) {
+  CASL_CUDA_TRY(cudaStreamWaitEvent(h->stream, ev, 0));
+  return CASL_OK;
+}
+
+static int grad_task(casl_handle *h, int) { return source_grad(h); }
+
+static int nodes_task(casl_handle *h, int stage) {
+  if (!h->contex) return CASL_OK;
+  int gn = grid_for(h->nptq > 0 ? h->nptq : 1);
+  cudaStream_t st = h->stream;
+  switch (stage) {
+    case 1: CASL_K(k_nodes_rk<1>, gn, 256, 0, st)(h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, h->uu, h->vv, h->scal, h->c); break;
+    case 2: CASL_K(k_nodes_rk<2>, gn, 256, 0, st)(h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, h->uu, h->vv, h->scal, h->c); break;
+    case 3: CASL_K(k_nodes_rk<3>, gn, 256, 0, st)(h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, h->uu, h->vv, h->scal, h->c); break;
+    default: CASL_K(k_nodes_rk<4>, gn, 256, 0, st)(h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, h->uu, h->vv, h->scal, h->c); break;
+  }
+  return check_launch(h);
+}
+
+static int spec_update(casl_handle *h, int stage) {
+  long long nn = (long long)h->n * h->n;
+  int g = grid_for(nn);
+  cudaStream_t st = h->stream;
+  switch (stage) {
+    case 1: CASL_K(k_spec_rk<1>, g, 256, 0, st)(h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs, h->sqd, h->emq, h->scal, nn); break;
+    case 2: CASL_K(k_spec_rk<2>, g, 256, 0, st)(h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs, h->sqd, h->emq, h->scal, nn); break;
+    case 3: CASL_K(k_spec_rk<3>, g, 256, 0, st)(h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs, h->sqd, h->emq, h->scal, nn); break;
+    default: CASL_K(k_spec_rk<4>, g, 256, 0, st)(h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs, h->sqd, h->emq, h->scal, nn); break;
+  }
+  return check_launch(h);
 }
 
 static int advance_dev(casl_handle *h) {
-  long long nn = (long long)h->n * h->n;
-  int g = grid_for(nn);
-  int gn = grid_for(h->nptq > 0 ? h->nptq : 1);
   int rc;
-  // stage 1: the reset in the combination rewrites qs and qd, so the
-  // gradients start after it
-  if ((rc = inversion_qq(h, true))) return rc;
-  if ((rc = grad_fork(h))) return rc;
-  if ((rc = main_invert_dev(h))) return rc;
-  if ((rc = adapt_dev(h))) return rc;
-  if ((rc = grad_join(h))) return rc;
-  if ((rc = source_prod(h, 0))) return rc;
-  if (h->contex)
-    CASL_K(k_nodes_rk<1>, gn, 256, 0, h->stream)(h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, h->uu,
-                                             h->vv, h->scal, h->c);
-  CASL_K(k_spec_rk<1>, g, 256, 0, h->stream)(h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs,
-                                         h->sqd, h->emq, h->scal, nn);
-  if ((rc = check_launch(h))) return rc;
-  // stage 2
-  if ((rc = grad_fork(h))) return rc;
-  CASL_K(k_advance_time, 1, 1, 0, h->stream)(h->scal);
-  if ((rc = inversion_dev(h, false))) return rc;
-  if ((rc = grad_join(h))) return rc;
-  if ((rc = source_prod(h, 1))) return rc;
-  if (h->contex)
-    CASL_K(k_nodes_rk<2>, gn, 256, 0, h->stream)(h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, h->uu,
-                                             h->vv, h->scal, h->c);
-  CASL_K(k_spec_rk<2>, g, 256, 0, h->stream)(h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs,
-                                         h->sqd, h->emq, h->scal, nn);
-  if ((rc = check_launch(h))) return rc;
-  // stage 3
-  if ((rc = grad_fork(h))) return rc;
-  if ((rc = inversion_dev(h, false))) return rc;
-  if ((rc = grad_join(h))) return rc;
-  if ((rc = source_prod(h, 1))) return rc;
-  if (h->contex)
-    CASL_K(k_nodes_rk<3>, gn, 256, 0, h->stream)(h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, h->uu,
-                                             h->vv, h->scal, h->c);
-  CASL_K(k_spec_rk<3>, g, 256, 0, h->stream)(h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs,
-                                         h->sqd, h->emq, h->scal, nn);
-  if ((rc = check_launch(h))) return rc;
-  // stage 4
-  if ((rc = grad_fork(h))) return rc;
-  CASL_K(k_advance_time, 1, 1, 0, h->stream)(h->scal);
-  if ((rc = inversion_dev(h, false))) return rc;
-  if ((rc = grad_join(h))) return rc;
-  if ((rc = source_prod(h, 2))) return rc;
-  if (h->contex)
-    CASL_K(k_nodes_rk<4>, gn, 256, 0, h->stream)(h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, h->uu,
-                                             h->vv, h->scal, h->c);
-  CASL_K(k_spec_rk<4>, g, 256, 0, h->stream)(h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs,
-                                         h->sqd, h->emq, h->scal, nn);
-  return check_launch(h);
+  for (int stage = 1; stage <= 4; stage++) {
+    if (stage == 1) {
+      // the reset inside the filter combination rewrites qs and qd, so the
+      // gradients start after it
+      if ((rc = inversion_qq(h, true))) return rc;
+      if ((rc = side_after_main(h))) return rc;
+      if ((rc = on_side(h, grad_task, 0, h->ev_grad))) return rc;
+    } else {
+      // gradients as soon as the previous spectral update is done
+      if ((rc = side_after_main(h))) return rc;
+      if ((rc = on_side(h, grad_task, 0, h->ev_grad))) return rc;
+      if (stage == 2 || stage == 4) CASL_K(k_advance_time, 1, 1, 0, h->stream)(h->scal);
+      if ((rc = inversion_qq(h, false))) return rc;
+    }
+    if ((rc = main_invert_dev(h))) return rc;
+    if (stage == 1 && (rc = adapt_dev(h))) return rc;
+    if ((rc = main_after(h, h->ev_grad))) return rc;
+    if ((rc = source_prod(h, stage == 1 ? 0 : (stage == 4 ? 2 : 1)))) return rc;
+    if ((rc = nodes_task(h, stage))) return rc;
+    if ((rc = spec_update(h, stage))) return rc;
+  }
+  return CASL_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -1436,7 +1440,7 @@ static int alloc_all(casl_handle *h) {
   CASL_CUDA_TRY(cudaMalloc(&h->gtmp, (size_t)4 * nn * sizeof(double)));
   CASL_CUDA_TRY(cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking));
   CASL_CUDA_TRY(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
-  CASL_CUDA_TRY(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
+  CASL_CUDA_TRY(cudaEventCreateWithFlags(&h->ev_grad, cudaEventDisableTiming));
   CASL_CUDA_TRY(cudaMalloc(&h->shell_idx, (size_t)nn * sizeof(int)));
   CASL_CUDA_TRY(cudaMalloc(&h->shell_off, (size_t)(2 * n + 2) * sizeof(int)));
   CASL_CUDA_TRY(cudaMalloc(&h->rkxf, n * sizeof(double)));
@@ -1465,7 +1469,7 @@ static void free_all(casl_handle *h) {
     cudaStreamDestroy(h->stream2);
   }
   if (h->ev_fork) cudaEventDestroy(h->ev_fork);
-  if (h->ev_join) cudaEventDestroy(h->ev_join);
+  if (h->ev_grad) cudaEventDestroy(h->ev_grad);
   for (void *p : ptrs)
     if (p) cudaFree(p);
   free(h->spmf_h);

@@ -123,36 +123,60 @@ __global__ void k_u_colscan(int *__restrict__ J, int nxu, int nyu,
 }
 
 // qa = (L*qjump - qavg) + bilinear residual, or the bilinear field alone.
+// One thread per run of 16 rows of a column: the run lies in one coarse cell
+// in y, so the four coarse values are gathered once; the levels come in and
+// qa goes out as 16-byte vectors.  Per element the expression and its order
+// are the reference's (congen.f90:45-61 on con2ugrid's field).
 __global__ void k_u_field(const int *__restrict__ L, const unsigned long long *__restrict__ lsum,
                           const double *__restrict__ qq, double qjump, int have_contours,
                           double *__restrict__ qa, double *__restrict__ part, Consts c) {
   const int nxu = c.nxu, nyu = c.nyu, n = c.nx;
-  const long long nu = (long long)nxu * nyu;
+  const long long nruns = (long long)nxu * (nyu / 16);
   double qavg = 0.0;
   if (have_contours) qavg = qjump * ((double)(long long)(*lsum) / ((double)nxu * (double)nyu));
   const double fac = 1.0 / 16.0;
   double mx = -1.0e308, mn = 1.0e308;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nu;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nruns;
        t += (long long)gridDim.x * blockDim.x) {
-    int iy = (int)(t % nyu) + 1, ix = (int)(t / nyu) + 1;
-    int ixx = (ix - 1) / 16, iyy = (iy - 1) / 16;
-    int ix0 = 1 + ixx, ix1 = 2 + ixx - n * (ix0 / n), ixf = ix - 16 * ixx;
-    int iy0 = 1 + iyy, iy1 = 2 + iyy - n * (iy0 / n), iyf = iy - 16 * iyy;
-    double pxf = fac * (double)(ixf - 1), pxc = 1.0 - pxf;
-    double pyf = fac * (double)(iyf - 1), pyc = 1.0 - pyf;
-    double w00 = pyc * pxc, w10 = pyf * pxc, w01 = pyc * pxf, w11 = pyf * pxf;
-    double q00 = qq[(long long)(ix0 - 1) * n + iy0 - 1], q10 = qq[(long long)(ix0 - 1) * n + iy1 - 1];
-    double q01 = qq[(long long)(ix1 - 1) * n + iy0 - 1], q11 = qq[(long long)(ix1 - 1) * n + iy1 - 1];
-    double v;
+    const int iyy = (int)(t % (nyu / 16)), ix = (int)(t / (nyu / 16)) + 1;
+    const int ixx = (ix - 1) / 16;
+    const int ix0 = 1 + ixx, ix1 = 2 + ixx - n * (ix0 / n), ixf = ix - 16 * ixx;
+    const int iy0 = 1 + iyy, iy1 = 2 + iyy - n * (iy0 / n);
+    const double pxf = fac * (double)(ixf - 1), pxc = 1.0 - pxf;
+    const double q00 = qq[(long long)(ix0 - 1) * n + iy0 - 1], q10 = qq[(long long)(ix0 - 1) * n + iy1 - 1];
+    const double q01 = qq[(long long)(ix1 - 1) * n + iy0 - 1], q11 = qq[(long long)(ix1 - 1) * n + iy1 - 1];
+    const long long base = (long long)(ix - 1) * nyu + 16LL * iyy;
+    int lv[16];
     if (have_contours) {
-      v = (double)L[t] * qjump - qavg;
-      v = v + w00 * q00 + w10 * q10 + w01 * q01 + w11 * q11;
-    } else {
-      v = w00 * q00 + w10 * q10 + w01 * q01 + w11 * q11;
+      const int4 *l4 = reinterpret_cast<const int4 *>(L + base);
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        int4 q = l4[k];
+        lv[4 * k] = q.x; lv[4 * k + 1] = q.y; lv[4 * k + 2] = q.z; lv[4 * k + 3] = q.w;
+      }
     }
-    qa[t] = v;
-    mx = fmax(mx, v);
-    mn = fmin(mn, v);
+    double2 *o2 = reinterpret_cast<double2 *>(qa + base);
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      double out[2];
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int iyf = 2 * k + h + 1;
+        const double pyf = fac * (double)(iyf - 1), pyc = 1.0 - pyf;
+        const double w00 = pyc * pxc, w10 = pyf * pxc, w01 = pyc * pxf, w11 = pyf * pxf;
+        double v;
+        if (have_contours) {
+          v = (double)lv[2 * k + h] * qjump - qavg;
+          v = v + w00 * q00 + w10 * q10 + w01 * q01 + w11 * q11;
+        } else {
+          v = w00 * q00 + w10 * q10 + w01 * q01 + w11 * q11;
+        }
+        out[h] = v;
+        mx = fmax(mx, v);
+        mn = fmin(mn, v);
+      }
+      o2[k] = make_double2(out[0], out[1]);
+    }
   }
   __shared__ double a[256], b[256];
   a[threadIdx.x] = mx;
@@ -183,91 +207,97 @@ __device__ __forceinline__ double qtmp_of(int lev, const LevInfo &li) {
   return ((double)lev - 0.5) * li.qjump - li.qoff;
 }
 
-// Levels whose contour value q_lev satisfies lo < q_lev <= hi, i.e. where the
-// reference's sign(qa - qtmp) differs at the two ends (congen.f90:205-212).
-__device__ __forceinline__ void crossed_levels(double a, double b, const LevInfo &li, int &l1,
-                                               int &l2) {
-  double lo = fmin(a, b), hi = fmax(a, b);
-  int g1 = (int)floor((lo + li.qoff) * li.qjumpi + 0.5) - 1;
-  int g2 = (int)floor((hi + li.qoff) * li.qjumpi + 0.5) + 2;
-  g1 = max(g1, li.levbeg);
-  g2 = min(g2, li.levend);
-  while (g1 <= g2 && !(qtmp_of(g1, li) > lo)) g1++;
-  while (g2 >= g1 && !(qtmp_of(g2, li) <= hi)) g2--;
-  l1 = g1;
-  l2 = g2;
-}
-
-__device__ __forceinline__ void edge_values(const double *__restrict__ qa, long long e, int nxu,
-                                            int nyu, double &a, double &b) {
-  const long long NE = (long long)nxu * nyu;
-  if (e < NE) {
-    int ix = (int)(e / nyu), iy = (int)(e % nyu);
-    a = qa[(long long)ix * nyu + iy];
-    b = qa[(long long)ix * nyu + (iy + 1 == nyu ? 0 : iy + 1)];
-  } else {
-    long long f = e - NE;
-    int iy = (int)(f / nxu), ix = (int)(f % nxu);
-    a = qa[(long long)ix * nyu + iy];
-    b = qa[(long long)(ix + 1 == nxu ? 0 : ix + 1) * nyu + iy];
-  }
+// Largest level l whose contour value qtmp(l) = (l - 1/2) qjump - qoff is
+// <= v.  qtmp is increasing in l (also as rounded), so an edge with end
+// values lo < hi crosses exactly the levels c(lo) < l <= c(hi): those where
+// the reference's sign(qa - qtmp) differs at the two ends (congen.f90:205-212).
+__device__ __forceinline__ int level_index(double v, const LevInfo &li) {
+  int l = (int)floor((v + li.qoff) * li.qjumpi + 0.5);
+  while (qtmp_of(l + 1, li) <= v) l++;
+  while (qtmp_of(l, li) > v) l--;
+  return l;
 }
 
 constexpr int EDGES_PER_THREAD = 16;
 
+// Crossings are counted and emitted per chunk of 16 consecutive edges in the
+// reference's numbering: x-line edges (ix, iy)-(ix, iy+1) are numbered
+// e = ix*nyu + iy, y-line edges (ix, iy)-(ix+1, iy) e = NE + iy*nxu + ix.
+// One CTA takes a tile of CB = 16 columns x RB = 64 rows of the field, staged
+// in shared memory with the next row and column (periodic), so the field is
+// read once, coalesced, by independent CTAs.  Each half-warp handles one
+// chunk: 16 rows of a column (x-line edges) or 16 columns of a row (y-line
+// edges).  COUNT writes the chunk's number of crossings; EMIT writes its
+// crossings (edge, level) from the chunk's offset on, edge by edge and level
+// by level, which is the reference's order within a chunk.
+constexpr int CR_CB = 16, CR_RB = 64;
 
-// Chunk of 16 consecutive edges (in the reference's numbering) handled by
-// thread t.  x-line chunks go in order; y-line chunks are remapped so that
-// neighbouring threads take neighbouring rows iy and read qa coalesced.
-__device__ __forceinline__ long long chunk_of_thread(long long t, int nxu, int nyu) {
-  const long long ncx = (long long)nxu * nyu / EDGES_PER_THREAD;
-  if (t < ncx) return t;
-  long long u = t - ncx;
-  long long iy = u % nyu, ixb = u / nyu;
-  return ncx + iy * (nxu / EDGES_PER_THREAD) + ixb;
-}
-
-__global__ void k_cr_count(const double *__restrict__ qa, LevInfo li, int nxu, int nyu,
-                           long long nchunks, int *__restrict__ cnt) {
-  const long long NE2 = 2LL * nxu * nyu;
-  for (long long tt = blockIdx.x * (long long)blockDim.x + threadIdx.x; tt < nchunks;
-       tt += (long long)gridDim.x * blockDim.x) {
-    const long long t = chunk_of_thread(tt, nxu, nyu);
-    int s = 0;
-    for (int q = 0; q < EDGES_PER_THREAD; q++) {
-      long long e = t * EDGES_PER_THREAD + q;
-      if (e >= NE2) break;
-      double a, b;
-      edge_values(qa, e, nxu, nyu, a, b);
-      if (a == b) continue;
-      int l1, l2;
-      crossed_levels(a, b, li, l1, l2);
-      if (l2 >= l1) s += l2 - l1 + 1;
-    }
-    cnt[t] = s;
+template <bool EMIT>
+__global__ void __launch_bounds__(256) k_cr_tile(const double *__restrict__ qa, LevInfo li, int nxu,
+                                                 int nyu, int *__restrict__ cnt,
+                                                 const int *__restrict__ off,
+                                                 unsigned long long *__restrict__ redge,
+                                                 int *__restrict__ rlev) {
+  __shared__ double S[CR_CB + 1][CR_RB + 1];  // row length 65: conflict-free both ways
+  __shared__ int Cl[CR_CB + 1][CR_RB + 1];    // level index of every staged value
+  const int ix0 = blockIdx.x * CR_CB, iy0 = blockIdx.y * CR_RB;
+  for (int idx = threadIdx.x; idx < (CR_CB + 1) * (CR_RB + 1); idx += blockDim.x) {
+    const int cc = idx / (CR_RB + 1), r = idx - cc * (CR_RB + 1);
+    int ix = ix0 + cc, iy = iy0 + r;
+    if (ix >= nxu) ix -= nxu;
+    if (iy >= nyu) iy -= nyu;
+    const double v = qa[(long long)ix * nyu + iy];
+    S[cc][r] = v;
+    Cl[cc][r] = level_index(v, li);
   }
-}
-
-__global__ void k_cr_emit(const double *__restrict__ qa, LevInfo li, int nxu, int nyu,
-                          long long nchunks, const int *__restrict__ off,
-                          unsigned long long *__restrict__ redge, int *__restrict__ rlev) {
-  const long long NE2 = 2LL * nxu * nyu;
-  for (long long tt = blockIdx.x * (long long)blockDim.x + threadIdx.x; tt < nchunks;
-       tt += (long long)gridDim.x * blockDim.x) {
-    const long long t = chunk_of_thread(tt, nxu, nyu);
-    int o = off[t];
-    for (int q = 0; q < EDGES_PER_THREAD; q++) {
-      long long e = t * EDGES_PER_THREAD + q;
-      if (e >= NE2) break;
-      double a, b;
-      edge_values(qa, e, nxu, nyu, a, b);
-      if (a == b) continue;
-      int l1, l2;
-      crossed_levels(a, b, li, l1, l2);
+  __syncthreads();
+  const long long NE = (long long)nxu * nyu;
+  const int lane = threadIdx.x & 31, sub = lane & 15, hw = threadIdx.x >> 4;
+  // 64 x-line chunks (16 columns x 4 groups of 16 rows), then 64 y-line
+  // chunks (one per row): 16 half-warps take one chunk each per round
+  for (int round = 0; round < 8; round++) {
+    int cc, r, nxt_c, nxt_r;
+    long long e;
+    if (round < 4) {
+      const int chunk = round * 16 + hw;  // 0..63
+      cc = chunk >> 2;                    // column 0..15
+      r = (chunk & 3) * 16 + sub;
+      nxt_c = cc;
+      nxt_r = r + 1;
+      e = (long long)(ix0 + cc) * nyu + (iy0 + r);
+    } else {
+      r = (round - 4) * 16 + hw;  // row 0..63
+      cc = sub;
+      nxt_c = cc + 1;
+      nxt_r = r;
+      e = NE + (long long)(iy0 + r) * nxu + (ix0 + cc);
+    }
+    const double a = S[cc][r], b = S[nxt_c][nxt_r];
+    const int ca = Cl[cc][r], cb = Cl[nxt_c][nxt_r];
+    int l1 = 0, l2 = -1;
+    if (a != b) {
+      l1 = max((a < b ? ca : cb) + 1, li.levbeg);
+      l2 = min(a < b ? cb : ca, li.levend);
+    }
+    const int k = l2 >= l1 ? l2 - l1 + 1 : 0;
+    const long long chunk_id = e / EDGES_PER_THREAD;
+    if (!EMIT) {
+      int t = k;
+#pragma unroll
+      for (int o = 8; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o, 16);
+      if (sub == 0) cnt[chunk_id] = t;
+    } else {
+      int incl = k;
+#pragma unroll
+      for (int o = 1; o < 16; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, incl, o, 16);
+        if (sub >= o) incl += y;
+      }
+      int pos = off[chunk_id] + incl - k;
       for (int l = l1; l <= l2; l++) {
-        redge[o] = (unsigned long long)e;
-        rlev[o] = l - li.levbeg;
-        o++;
+        redge[pos] = (unsigned long long)e;
+        rlev[pos] = l - li.levbeg;
+        pos++;
       }
     }
   }
@@ -335,18 +365,26 @@ __device__ __forceinline__ unsigned long long hmix(unsigned long long k) {
   return k;
 }
 
+// One bucket per (level, box) key: the key and its (at most two) out-
+// crossings share 16 bytes, so a probe touches one sector.  The two slots
+// are filled in arrival order; readers that need them ordered take min/max.
+struct __align__(16) HBucket {
+  unsigned long long key;
+  int s0, s1;
+};
+
 __global__ void k_h_insert(const int *__restrict__ rlev, const unsigned int *__restrict__ kob,
-                           long long ncr, unsigned long long *__restrict__ keys,
-                           int *__restrict__ slots, unsigned long long mask, int *__restrict__ err) {
+                           long long ncr, HBucket *__restrict__ hb, unsigned long long mask,
+                           int *__restrict__ err) {
   for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
        r += (long long)gridDim.x * blockDim.x) {
     unsigned long long k = hkey(rlev[r], kob[r]);
     unsigned long long p = hmix(k) & mask;
     for (unsigned long long probe = 0; probe <= mask; probe++) {
-      unsigned long long prev = atomicCAS(&keys[p], HEMPTY, k);
+      unsigned long long prev = atomicCAS(&hb[p].key, HEMPTY, k);
       if (prev == HEMPTY || prev == k) {
-        if (atomicCAS(&slots[2 * p], -1, (int)r) != -1)
-          if (atomicCAS(&slots[2 * p + 1], -1, (int)r) != -1) atomicExch(err, CASL_ECAPACITY);
+        if (atomicCAS(&hb[p].s0, -1, (int)r) != -1)
+          if (atomicCAS(&hb[p].s1, -1, (int)r) != -1) atomicExch(err, CASL_ECAPACITY);
         break;
       }
       p = (p + 1) & mask;
@@ -354,52 +392,38 @@ __global__ void k_h_insert(const int *__restrict__ rlev, const unsigned int *__r
   }
 }
 
-__global__ void k_h_order(const unsigned long long *__restrict__ keys, int *__restrict__ slots,
-                          unsigned long long cap) {
-  for (unsigned long long p = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; p < cap;
-       p += (unsigned long long)gridDim.x * blockDim.x) {
-    if (keys[p] == HEMPTY) continue;
-    int a = slots[2 * p], b = slots[2 * p + 1];
-    if (b >= 0 && b < a) {
-      slots[2 * p] = b;
-      slots[2 * p + 1] = a;
-    }
-  }
-}
-
-__device__ __forceinline__ long long h_find(const unsigned long long *__restrict__ keys,
-                                            unsigned long long mask, unsigned long long k) {
-  unsigned long long p = hmix(k) & mask;
-  for (unsigned long long probe = 0; probe <= mask; probe++) {
-    unsigned long long v = keys[p];
-    if (v == k) return (long long)p;
-    if (v == HEMPTY) return -1;
-    p = (p + 1) & mask;
-  }
-  return -1;
-}
-
 // successor of each crossing; -1 where it enters a saddle box (2 out-crossings)
 __global__ void k_h_succ(const int *__restrict__ rlev, const unsigned int *__restrict__ kib,
-                         long long ncr, const unsigned long long *__restrict__ keys,
-                         const int *__restrict__ slots, unsigned long long mask,
+                         long long ncr, const HBucket *__restrict__ hb, unsigned long long mask,
                          int *__restrict__ succ, long long *__restrict__ sadslot,
                          int *__restrict__ err) {
   for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
        r += (long long)gridDim.x * blockDim.x) {
-    long long p = h_find(keys, mask, hkey(rlev[r], kib[r]));
-    if (p < 0) {
+    const unsigned long long k = hkey(rlev[r], kib[r]);
+    unsigned long long p = hmix(k) & mask;
+    long long found = -1;
+    HBucket v;
+    for (unsigned long long probe = 0; probe <= mask; probe++) {
+      v = hb[p];
+      if (v.key == k) {
+        found = (long long)p;
+        break;
+      }
+      if (v.key == HEMPTY) break;
+      p = (p + 1) & mask;
+    }
+    if (found < 0) {
       atomicExch(err, CASL_EINVAL);
       succ[r] = -1;
       sadslot[r] = -1;
       continue;
     }
-    if (slots[2 * p + 1] < 0) {
-      succ[r] = slots[2 * p];
+    if (v.s1 < 0) {
+      succ[r] = v.s0;
       sadslot[r] = -1;
     } else {
       succ[r] = -1;
-      sadslot[r] = p;
+      sadslot[r] = found;
     }
   }
 }
@@ -670,11 +694,13 @@ __global__ void k_gather_i(const int *__restrict__ src, const int *__restrict__ 
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x)
     dst[k] = src[idx[k]];
 }
-__global__ void k_gather_slots(const int *__restrict__ slots, const long long *__restrict__ sadp,
+// the two out-crossings of each saddle bucket, lower index first
+__global__ void k_gather_slots(const HBucket *__restrict__ hb, const long long *__restrict__ sadp,
                                int nsb, int *__restrict__ out) {
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nsb; b += gridDim.x * blockDim.x) {
-    out[2 * b] = slots[2 * sadp[b]];
-    out[2 * b + 1] = slots[2 * sadp[b] + 1];
+    const HBucket v = hb[sadp[b]];
+    out[2 * b] = min(v.s0, v.s1);
+    out[2 * b + 1] = max(v.s0, v.s1);
   }
 }
 __global__ void k_ct_len(const int *__restrict__ startf, const int *__restrict__ clenr,
@@ -767,10 +793,13 @@ int recontour_dev(casl_handle *h, const double *qq) {
     CASL_CUDA_TRY(cudaMemsetAsync(Lu, 0, (size_t)NU * sizeof(int), st));
     CASL_CUDA_TRY(cudaMemsetAsync(ljx, 0, (size_t)nxu * sizeof(int), st));
     CASL_CUDA_TRY(cudaMemsetAsync(lsum, 0, sizeof(unsigned long long), st));
+    tr.point("u_memset");
     CASL_K(k_u_scatter, gsz(h->nptq), 256, 0, st)(h->xq, h->yq, h->nextq, h->nptq, qjump, Lu, ljx, c,
                                               &h->scal->error);
+    tr.point("u_scatter");
     CASL_K(k_u_lbot, 1, 1024, 0, st)(ljx, Lu, nxu, nyu);
     CASL_K(k_u_colscan, (nxu * 32 + 255) / 256, 256, 0, st)(Lu, nxu, nyu, lsum);
+    tr.point("u_colscan");
   }
   const int fb = 4096;
   CASL_K(k_u_field, fb, 256, 0, st)(Lu, lsum, qq, qjump, have, qa, part, c);
@@ -810,13 +839,15 @@ int recontour_dev(casl_handle *h, const double *qq) {
   int *tmpi = ar.get<int>(scan_tmp_elems(nchunks) + 4);
   int *dtot = ar.get<int>(16);
   if (ar.failed) return CASL_ENOMEM;
-  CASL_K(k_cr_count, gsz(nchunks), 256, 0, st)(qa, li, nxu, nyu, nchunks, ccnt);
+  const dim3 tgrid(nxu / CR_CB, nyu / CR_RB);
+  CASL_K(k_cr_tile<false>, tgrid, 256, 0, st)(qa, li, nxu, nyu, ccnt, nullptr, nullptr, nullptr);
   tr.point("cr_count");
   exclusive_scan<int>(st, ccnt, coffs, nchunks, tmpi, dtot);
   int ncr_i = 0;
   CASL_CUDA_TRY(cudaMemcpyAsync(&ncr_i, dtot, sizeof(int), cudaMemcpyDeviceToHost, st));
   CASL_CUDA_TRY(cudaStreamSynchronize(st));
   const long long ncr = ncr_i;
+  if (tr.on) fprintf(stderr, "[casl trace] recontour: %lld crossings on %d levels\n", ncr, nlev);
   if (ncr == 0) return set_empty();
   // Per-crossing storage lives in a second arena sized from the count, so
   // that the ultra-fine field in the first one is kept.
@@ -841,7 +872,7 @@ int recontour_dev(casl_handle *h, const double *qq) {
   void *sort_tmp = ar2.get<char>(sort_bytes + 16);
   if (ar2.failed) return CASL_ENOMEM;
   tr.point("cr_alloc");
-  CASL_K(k_cr_emit, gsz(nchunks), 256, 0, st)(qa, li, nxu, nyu, nchunks, coffs, redge, rlev);
+  CASL_K(k_cr_tile<true>, tgrid, 256, 0, st)(qa, li, nxu, nyu, nullptr, coffs, redge, rlev);
   tr.point("cr_emit");
   CASL_CUDA_TRY(cub::DeviceRadixSort::SortPairs(sort_tmp, sort_bytes, rlev, rlev2, redge, redge2,
                                                 (int)ncr, 0, endbit, st));
@@ -858,16 +889,13 @@ int recontour_dev(casl_handle *h, const double *qq) {
   // --- 4. box tables: hash (level, box) -> two out-crossing slots ------------
   unsigned long long cap = 1;
   while (cap < (unsigned long long)(2 * ncr)) cap <<= 1;
-  unsigned long long *keys = ar2.get<unsigned long long>(cap);
-  int *slots = ar2.get<int>(2 * cap);
+  HBucket *hb = ar2.get<HBucket>(cap);
   int *succ = ar2.get<int>(ncr);
   long long *sadslot = ar2.get<long long>(ncr);
   if (ar2.failed) return CASL_ENOMEM;
-  CASL_CUDA_TRY(cudaMemsetAsync(keys, 0xff, cap * sizeof(unsigned long long), st));
-  CASL_CUDA_TRY(cudaMemsetAsync(slots, 0xff, 2 * cap * sizeof(int), st));
-  CASL_K(k_h_insert, gsz(ncr), 256, 0, st)(rlev, kob, ncr, keys, slots, cap - 1, &h->scal->error);
-  CASL_K(k_h_order, gsz(cap), 256, 0, st)(keys, slots, cap);
-  CASL_K(k_h_succ, gsz(ncr), 256, 0, st)(rlev, kib, ncr, keys, slots, cap - 1, succ, sadslot,
+  CASL_CUDA_TRY(cudaMemsetAsync(hb, 0xff, cap * sizeof(HBucket), st));  // empty key, slots -1
+  CASL_K(k_h_insert, gsz(ncr), 256, 0, st)(rlev, kob, ncr, hb, cap - 1, &h->scal->error);
+  CASL_K(k_h_succ, gsz(ncr), 256, 0, st)(rlev, kib, ncr, hb, cap - 1, succ, sadslot,
                                      &h->scal->error);
   RC_TRY(check_launch(h));
   RC_TRY(fetch_err(h));
@@ -903,6 +931,7 @@ int recontour_dev(casl_handle *h, const double *qq) {
       *ssl2 = ar2.get<int>(S), *shead = ar2.get<int>(S);
   long long *ssuf = ar2.get<long long>(S), *ssuf2 = ar2.get<long long>(S);
   if (ar2.failed) return CASL_ENOMEM;
+  tr.point("rk_walk");
   CASL_K(k_sp_compact, g, 256, 0, st)(isspl, srank, ncr, nexts_c, seglen_c, segmin_c, segend_c,
                                       nexts, seglen, segmin, segend);
   int gsS = gsz(S);
@@ -919,11 +948,13 @@ int recontour_dev(casl_handle *h, const double *qq) {
     CASL_K(k_sp_jump2, gsS, 256, 0, st)(ssl, ssuf, S, ssl2, ssuf2);
     std::swap(ssl, ssl2); std::swap(ssuf, ssuf2);
   }
+  tr.point("rk_jump");
   CASL_K(k_sp_expand, g, 256, 0, st)(ncr, owner, offc, srank, stm, smn, ssuf, shead, slp, segend,
                                      term, lab, val, ep);
   RC_TRY(check_launch(h));
+  if (tr.on) fprintf(stderr, "[casl trace] ranking: %d splitters, %d jump rounds\n", S, rounds);
 
-  tr.point("ranking");
+  tr.point("rk_expand");
   // --- 6. saddle chains: exact simulation of the reference traversal ----------
   // Only the crossings entering saddle boxes and the chain starts come to the
   // host; everything of size ncr stays on the device.
@@ -978,7 +1009,7 @@ int recontour_dev(casl_handle *h, const double *qq) {
       int *d_slot2 = ar2.get<int>(2 * nsb);
       if (ar2.failed) return CASL_ENOMEM;
       CASL_CUDA_TRY(cudaMemcpyAsync(d_sadp, sad_p.data(), nsb * sizeof(long long), cudaMemcpyHostToDevice, st));
-      CASL_K(k_gather_slots, gsz(nsb), 256, 0, st)(slots, d_sadp, nsb, d_slot2);
+      CASL_K(k_gather_slots, gsz(nsb), 256, 0, st)(hb, d_sadp, nsb, d_slot2);
       CASL_CUDA_TRY(cudaMemcpyAsync(slot2.data(), d_slot2, 2 * nsb * sizeof(int), cudaMemcpyDeviceToHost, st));
       CASL_CUDA_TRY(cudaStreamSynchronize(st));
     }

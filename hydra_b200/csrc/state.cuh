@@ -15,7 +15,7 @@ struct casl_handle {
   int device;
   cudaStream_t stream;
   cudaStream_t stream2;          // side stream of advance (source gradients)
-  cudaEvent_t ev_fork, ev_join;  // fork/join between the two
+  cudaEvent_t ev_fork, ev_grad;  // synchronisation between the two
   double *gtmp;                  // 4 fields of scratch for the side stream
   int last_cuda;
   int n;                 // nx == ny
