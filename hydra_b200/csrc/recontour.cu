@@ -556,11 +556,15 @@ __global__ void k_sp_walk(const int *__restrict__ succ, const int *__restrict__ 
     int s = (int)r, v = s, k = 0, mn = s, nx = -1;
     owner[s] = s;
     off[s] = 0;
+    // the next node's flag and successor are loaded together, so a step
+    // costs one dependent memory latency
+    int n = succ[v];
     for (long long guard = 0; guard < N; guard++) {
-      int n = succ[v];
       if (n < 0) { nx = -1; break; }
-      if (isspl[n]) { nx = n; break; }
+      const int spl = isspl[n], nn = succ[n];
+      if (spl) { nx = n; break; }
       v = n;
+      n = nn;
       k++;
       owner[v] = s;
       off[v] = k;
@@ -912,7 +916,7 @@ int recontour_dev(casl_handle *h, const double *qq) {
   int g = gsz(ncr);
   CASL_CUDA_TRY(cudaMemsetAsync(pred, 0xff, ncr * sizeof(int), st));
   CASL_K(k_sp_pred, g, 256, 0, st)(succ, ncr, pred);
-  CASL_K(k_sp_flag, g, 256, 0, st)(pred, ncr, 32, isspl, owner);
+  CASL_K(k_sp_flag, g, 256, 0, st)(pred, ncr, 16, isspl, owner);
   CASL_K(k_sp_walk, g, 256, 0, st)(succ, isspl, ncr, owner, offc, nexts_c, seglen_c, segmin_c,
                                    segend_c, &h->scal->error);
   CASL_K(k_sp_unowned, g, 256, 0, st)(ncr, owner, isspl);

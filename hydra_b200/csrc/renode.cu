@@ -23,88 +23,86 @@ __global__ void k_rn_cid(RenodeIn in, long long N, int *__restrict__ cid, int *_
   }
 }
 
-// dx, dy to the next node; v = |d|^2, e = |d|  (contours.f90:718-730)
-__global__ void k_rn1(RenodeIn in, RenodeScratch s, Consts c) {
-  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < in.N;
-       w += (long long)gridDim.x * blockDim.x) {
-    int k = s.cid[w];
-    long long cs = in.cs[k], L = in.len[k];
-    long long a = wnext(w, cs, L);
-    double xx = in.xw[a] - in.xw[w];
-    double dx = xx - c.ellx * f_dint(xx * c.hlxi);
-    double yy = in.yw[a] - in.yw[w];
-    double dy = yy - c.elly * f_dint(yy * c.hlyi);
-    s.dx[w] = dx;
-    s.dy[w] = dy;
-    double v = dx * dx + dy * dy;
-    s.v[w] = v;
-    s.e[w] = sqrt(v);
-  }
-}
-
-// corners and curvature b (contours.f90:732-752)
-__global__ void k_rn2(RenodeIn in, RenodeScratch s, Consts c) {
-  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < in.N;
-       w += (long long)gridDim.x * blockDim.x) {
-    int k = s.cid[w];
-    long long cs = in.cs[k], L = in.len[k];
-    long long p = wprev(w, cs, L);
-    double u = s.v[p], a = -s.dx[p], cc = -s.dy[p];
-    double dx = s.dx[w], dy = s.dy[w], v = s.v[w];
-    int corner = dx * a + dy * cc > 0.0;
-    s.corner[w] = corner;
-    if (corner) {
-      s.b[w] = 0.0;
-      atomicAdd(&s.ccnt[k], 1);
-    } else {
-      double t1 = a * v - dx * u, t2 = cc * v - dy * u;
-      s.b[w] = (dx * cc - a * dy) / sqrt(t1 * t1 + t2 * t2 + c.small3);
-    }
-  }
-}
-
-// cubic coefficients and the spherical-curvature densities (contours.f90:754-774)
-__global__ void k_rn3(RenodeIn in, RenodeScratch s, Consts c) {
+// The node densities of renode (contours.f90:718-796) for node w in one
+// pass: dx, dy, |d| to the next node; corners and curvature b; the cubic
+// coefficients and spherical-curvature densities; node curvature as a
+// weighted average; the fractional node count.  Every quantity node w needs is
+// recomputed from the coordinates of nodes w-2..w+3 (cyclic in the contour)
+// with the same expressions in the same order, so only the results the
+// placement reads (dx, dy, the final e, A, B, Cc, corner) go to memory.
+__global__ void k_rn_stencil(RenodeIn in, RenodeScratch s, Consts c) {
   const double f12 = 0.5, f13 = 1.0 / 3.0, f16 = 1.0 / 6.0;
   for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < in.N;
        w += (long long)gridDim.x * blockDim.x) {
-    int k = s.cid[w];
-    long long cs = in.cs[k], L = in.len[k];
-    long long a = wnext(w, cs, L);
-    double e = s.e[w], bi = s.b[w], ba = s.b[a];
-    double u = e * (ba + bi);
-    double cc = e * (ba - bi);
-    s.A[w] = f16 * cc - f12 * u;
-    s.B[w] = f12 * (u - cc);
-    s.Cc[w] = f13 * cc;
-    double v = s.v[w];
-    double ww = 1.0 / (v + c.dmsq);
-    s.u2[w] = ww * sqrt(c.elf * v + u * u);
-    s.v2[w] = ww * e;
-  }
-}
-
-// node curvature as a weighted average (contours.f90:780-783)
-__global__ void k_rn4(RenodeIn in, RenodeScratch s, Consts c) {
-  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < in.N;
-       w += (long long)gridDim.x * blockDim.x) {
-    int k = s.cid[w];
-    long long cs = in.cs[k], L = in.len[k];
-    long long p = wprev(w, cs, L);
-    s.d[w] = (s.u2[p] + s.u2[w]) / (s.v2[p] + s.v2[w] + c.small);
-  }
-}
-
-// fractional node count per interval (contours.f90:787-796)
-__global__ void k_rn5(RenodeIn in, RenodeScratch s, Consts c) {
-  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < in.N;
-       w += (long long)gridDim.x * blockDim.x) {
-    int k = s.cid[w];
-    long long cs = in.cs[k], L = in.len[k];
-    long long a = wnext(w, cs, L);
-    double u = 0.5 * (s.d[w] + s.d[a]);
-    double t = c.densf * sqrt(u) + u;
-    s.e[w] = s.e[w] * fmin(c.dmi, t);
+    const int k = s.cid[w];
+    const long long cs = in.cs[k], L = in.len[k];
+    long long j[6];
+    j[2] = w;
+    j[1] = wprev(w, cs, L);
+    j[0] = wprev(j[1], cs, L);
+    j[3] = wnext(w, cs, L);
+    j[4] = wnext(j[3], cs, L);
+    j[5] = wnext(j[4], cs, L);
+    double X[6], Y[6];
+#pragma unroll
+    for (int m = 0; m < 6; m++) {
+      X[m] = in.xw[j[m]];
+      Y[m] = in.yw[j[m]];
+    }
+    // rn1 at nodes m = 0..4
+    double dx[5], dy[5], v[5], e1[5];
+#pragma unroll
+    for (int m = 0; m < 5; m++) {
+      double xx = X[m + 1] - X[m];
+      dx[m] = xx - c.ellx * f_dint(xx * c.hlxi);
+      double yy = Y[m + 1] - Y[m];
+      dy[m] = yy - c.elly * f_dint(yy * c.hlyi);
+      v[m] = dx[m] * dx[m] + dy[m] * dy[m];
+      e1[m] = sqrt(v[m]);
+    }
+    // rn2 at nodes m = 1..4
+    double b[5];
+    int corner2 = 0;
+#pragma unroll
+    for (int m = 1; m < 5; m++) {
+      double u = v[m - 1], a = -dx[m - 1], cc = -dy[m - 1];
+      int corner = dx[m] * a + dy[m] * cc > 0.0;
+      if (m == 2) corner2 = corner;
+      if (corner) {
+        b[m] = 0.0;
+      } else {
+        double t1 = a * v[m] - dx[m] * u, t2 = cc * v[m] - dy[m] * u;
+        b[m] = (dx[m] * cc - a * dy[m]) / sqrt(t1 * t1 + t2 * t2 + c.small3);
+      }
+    }
+    // rn3 at nodes m = 1..3 (the cubic coefficients only at m = 2)
+    double u2[4], v2[4], A = 0.0, B = 0.0, Cc = 0.0;
+#pragma unroll
+    for (int m = 1; m < 4; m++) {
+      double u = e1[m] * (b[m + 1] + b[m]);
+      double cc = e1[m] * (b[m + 1] - b[m]);
+      if (m == 2) {
+        A = f16 * cc - f12 * u;
+        B = f12 * (u - cc);
+        Cc = f13 * cc;
+      }
+      double ww = 1.0 / (v[m] + c.dmsq);
+      u2[m] = ww * sqrt(c.elf * v[m] + u * u);
+      v2[m] = ww * e1[m];
+    }
+    // rn4 at nodes 2, 3 and rn5 at node 2
+    const double d2 = (u2[1] + u2[2]) / (v2[1] + v2[2] + c.small);
+    const double d3 = (u2[2] + u2[3]) / (v2[2] + v2[3] + c.small);
+    const double uu = 0.5 * (d2 + d3);
+    const double t = c.densf * sqrt(uu) + uu;
+    s.dx[w] = dx[2];
+    s.dy[w] = dy[2];
+    s.e[w] = e1[2] * fmin(c.dmi, t);
+    s.A[w] = A;
+    s.B[w] = B;
+    s.Cc[w] = Cc;
+    s.corner[w] = corner2;
+    if (corner2) atomicAdd(&s.ccnt[k], 1);
   }
 }
 
@@ -278,10 +276,9 @@ int renode_batch(casl_handle *h, Arena &ar, const RenodeIn &in, RenodeOut &out, 
   }
   RenodeScratch s{};
   s.cid = ar.get<int>(N);
-  s.dx = ar.get<double>(N); s.dy = ar.get<double>(N); s.v = ar.get<double>(N);
-  s.e = ar.get<double>(N); s.b = ar.get<double>(N); s.A = ar.get<double>(N);
-  s.B = ar.get<double>(N); s.Cc = ar.get<double>(N); s.u2 = ar.get<double>(N);
-  s.v2 = ar.get<double>(N); s.d = ar.get<double>(N); s.S = ar.get<double>(N);
+  s.dx = ar.get<double>(N); s.dy = ar.get<double>(N);
+  s.e = ar.get<double>(N); s.A = ar.get<double>(N);
+  s.B = ar.get<double>(N); s.Cc = ar.get<double>(N); s.S = ar.get<double>(N);
   s.corner = ar.get<int>(N); s.crank = ar.get<int>(N); s.head = ar.get<int>(N);
   s.cornerpos = ar.get<int>(N + 1);
   s.ccnt = ar.get<int>(C); s.ctot = ar.get<double>(C);
@@ -302,11 +299,7 @@ int renode_batch(casl_handle *h, Arena &ar, const RenodeIn &in, RenodeOut &out, 
   cudaMemsetAsync(s.ccnt, 0, C * sizeof(int), st);
   int g = gsz(N);
   CASL_K(k_rn_cid, g, 256, 0, st)(in, N, s.cid, s.head);
-  CASL_K(k_rn1, g, 256, 0, st)(in, s, c);
-  CASL_K(k_rn2, g, 256, 0, st)(in, s, c);
-  CASL_K(k_rn3, g, 256, 0, st)(in, s, c);
-  CASL_K(k_rn4, g, 256, 0, st)(in, s, c);
-  CASL_K(k_rn5, g, 256, 0, st)(in, s, c);
+  CASL_K(k_rn_stencil, g, 256, 0, st)(in, s, c);
   segmented_scan(st, s.e, s.head, s.S, N, s.tmps);
   exclusive_scan<int>(st, s.corner, s.crank, N, s.tmpi, s.d_tot + 0);
   CASL_K(k_rn_cornerpos, g, 256, 0, st)(s.corner, s.crank, s.cornerpos, N);

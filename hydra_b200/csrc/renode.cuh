@@ -48,7 +48,7 @@ __device__ __forceinline__ int contour_of(const int *__restrict__ cs, int C, lon
 
 struct RenodeScratch {
   int *cid;                  // contour of each walk node
-  double *dx, *dy, *v, *e, *b, *A, *B, *Cc, *u2, *v2, *d, *S;
+  double *dx, *dy, *e, *A, *B, *Cc, *S;
   int *corner, *crank, *head;
   int *ccnt;                 // corners per contour
   double *ctot;              // density sum per contour
