@@ -279,7 +279,9 @@ struct LoadVort {
 __global__ void k_c2g_scatter(const double *__restrict__ xq, const double *__restrict__ yq,
                               const int *__restrict__ nextq, const Scalars *__restrict__ s,
                               int *__restrict__ J, int *__restrict__ ljx, Consts c,
-                              int *__restrict__ err) {
+                              int *__restrict__ err, unsigned long long *__restrict__ csum) {
+  // the coarsening that follows accumulates the coarse-cell sum here
+  if (blockIdx.x == 0 && threadIdx.x == 0) *csum = 0;
   int npt = s->nptq;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npt; i += gridDim.x * blockDim.x) {
     int ia = nextq[i];
@@ -435,7 +437,9 @@ __global__ void k_c2g_coarsen(const int *__restrict__ L, int *__restrict__ C,
 #define C2G_CW 7
 #define C2G_FC (4 * C2G_CW + 3)
 template <int U>
-__global__ void __launch_bounds__(1024) k_c2g_fused(const int *__restrict__ J, int *__restrict__ C,
+__global__ void __launch_bounds__(1024) k_c2g_fused(const int *__restrict__ J,
+                                                    const int *__restrict__ ljx,
+                                                    int *__restrict__ C,
                                                     unsigned long long *__restrict__ csum, int n,
                                                     int nf) {
   constexpr int RPS = 32 * U, RING = RPS + 8, CR = RPS / 4;
@@ -456,7 +460,13 @@ __global__ void __launch_bounds__(1024) k_c2g_fused(const int *__restrict__ J, i
 #pragma unroll
     for (int u = 0; u < U; u++) v[u] = __ldcs(cp + u * 32);
   }
+  // row 0 of the column starts from the exclusive prefix of the bottom
+  // jumps along x (qbot, contours.f90:255-269), summed here by the warp
   int carry = 0;
+  if (warp < C2G_FC) {
+    for (int i = lane; i < col; i += 32) carry += ljx[i];
+    for (int o = 16; o > 0; o >>= 1) carry += __shfl_xor_sync(0xffffffffu, carry, o);
+  }
   long long local = 0;
   for (int s = 0; s < nsteps; s++) {
     if (warp < C2G_FC) {
@@ -530,7 +540,6 @@ __global__ void __launch_bounds__(1024) k_c2g_fused(const int *__restrict__ J, i
   }
 }
 
-__global__ void k_zero_csum(Scalars *s) { s->csum = 0; }
 
 // c = a * b elementwise
 __global__ void k_mul2(const double *__restrict__ a, const double *__restrict__ b,
@@ -562,20 +571,23 @@ int con2grid_dev(casl_handle *h, bool want_levels) {
   size_t fine = (size_t)c.nxf * c.nyf;
   CASL_CUDA_TRY(cudaMemsetAsync(h->fineJ, 0, fine * sizeof(int), h->stream));
   CASL_CUDA_TRY(cudaMemsetAsync(h->ljx, 0, (size_t)c.nxf * sizeof(int), h->stream));
-  CASL_K(k_zero_csum, 1, 1, 0, h->stream)(h->scal);
   int *err = &h->scal->error;
-  if (h->nptq > 0)
-    CASL_K(k_c2g_scatter, grid_for(h->nptq), 256, 0, h->stream)(h->xq, h->yq, h->nextq, h->scal,
-                                                              h->fineJ, h->ljx, c, err);
-  CASL_K(k_c2g_lbot, 1, 1024, 0, h->stream)(h->ljx, h->fineJ, c.nxf, c.nyf);
   unsigned long long *csum = (unsigned long long *)&h->scal->csum;
+  if (h->nptq > 0) {
+    CASL_K(k_c2g_scatter, grid_for(h->nptq), 256, 0, h->stream)(h->xq, h->yq, h->nextq, h->scal,
+                                                              h->fineJ, h->ljx, c, err, csum);
+  } else {
+    CASL_CUDA_TRY(cudaMemsetAsync(csum, 0, sizeof(unsigned long long), h->stream));
+  }
   int nblk = (h->n + C2G_CW - 1) / C2G_CW;
   if (!want_levels && c.nxf == c.nyf && c.nxf % 256 == 0) {
-    CASL_K(k_c2g_fused<8>, nblk, 1024, 0, h->stream)(h->fineJ, h->coarseC, csum, h->n, c.nxf);
+    CASL_K(k_c2g_fused<8>, nblk, 1024, 0, h->stream)(h->fineJ, h->ljx, h->coarseC, csum, h->n, c.nxf);
   } else if (!want_levels && c.nxf == c.nyf && c.nxf % 128 == 0) {
-    CASL_K(k_c2g_fused<4>, nblk, 1024, 0, h->stream)(h->fineJ, h->coarseC, csum, h->n, c.nxf);
+    CASL_K(k_c2g_fused<4>, nblk, 1024, 0, h->stream)(h->fineJ, h->ljx, h->coarseC, csum, h->n, c.nxf);
   } else {
-    // the fine-grid levels themselves are wanted: scan in place, then coarsen
+    // the fine-grid levels themselves are wanted: bottom row, scan in place,
+    // then coarsen
+    CASL_K(k_c2g_lbot, 1, 1024, 0, h->stream)(h->ljx, h->fineJ, c.nxf, c.nyf);
     CASL_K(k_c2g_colscan, (c.nxf * 32 + 255) / 256, 256, 0, h->stream)(h->fineJ, c.nxf, c.nyf);
     CASL_K(k_c2g_coarsen, grid_for((long long)h->n * h->n), 256, 0, h->stream)(
         h->fineJ, h->coarseC, csum, h->n, c.nxf);

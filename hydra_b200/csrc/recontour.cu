@@ -538,36 +538,40 @@ __global__ void k_sp_pred(const int *__restrict__ succ, long long N, int *__rest
     if (s >= 0) pred[s] = (int)r;
   }
 }
-__global__ void k_sp_flag(const int *__restrict__ pred, long long N, int K, int *__restrict__ isspl,
-                          int *__restrict__ owner) {
+// A walk step reads the next node's successor and splitter flag (sf, one
+// 8-byte load) and writes the node's (owner, offset) pair (own, one 8-byte
+// store): two random accesses per step.  isspl keeps the flags as a plain
+// array for the scan.
+__global__ void k_sp_flag(const int *__restrict__ pred, const int *__restrict__ succ, long long N,
+                          int K, int *__restrict__ isspl, int2 *__restrict__ sf,
+                          int2 *__restrict__ own) {
   for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < N;
        r += (long long)gridDim.x * blockDim.x) {
-    isspl[r] = (r % K == 0) || pred[r] < 0;
-    owner[r] = -1;
+    const int f = (r % K == 0) || pred[r] < 0;
+    isspl[r] = f;
+    sf[r] = make_int2(succ[r], f);
+    own[r] = make_int2(-1, 0);
   }
 }
-__global__ void k_sp_walk(const int *__restrict__ succ, const int *__restrict__ isspl, long long N,
-                          int *__restrict__ owner, int *__restrict__ off, int *__restrict__ nexts_c,
-                          int *__restrict__ seglen_c, int *__restrict__ segmin_c,
-                          int *__restrict__ segend_c, int *__restrict__ err) {
+__global__ void k_sp_walk(const int2 *__restrict__ sf, long long N, int2 *__restrict__ own,
+                          int *__restrict__ nexts_c, int *__restrict__ seglen_c,
+                          int *__restrict__ segmin_c, int *__restrict__ segend_c,
+                          int *__restrict__ err) {
   for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < N;
        r += (long long)gridDim.x * blockDim.x) {
-    if (!isspl[r] || owner[r] >= 0) continue;
+    const int2 me = sf[r];
+    if (!me.y || own[r].x >= 0) continue;
     int s = (int)r, v = s, k = 0, mn = s, nx = -1;
-    owner[s] = s;
-    off[s] = 0;
-    // the next node's flag and successor are loaded together, so a step
-    // costs one dependent memory latency
-    int n = succ[v];
+    own[s] = make_int2(s, 0);
+    int n = me.x;
     for (long long guard = 0; guard < N; guard++) {
       if (n < 0) { nx = -1; break; }
-      const int spl = isspl[n], nn = succ[n];
-      if (spl) { nx = n; break; }
+      const int2 q = sf[n];  // successor and flag of the next node
+      if (q.y) { nx = n; break; }
       v = n;
-      n = nn;
+      n = q.x;
       k++;
-      owner[v] = s;
-      off[v] = k;
+      own[v] = make_int2(s, k);
       mn = min(mn, v);
       if (guard == N - 1) atomicExch(err, CASL_EINVAL);
     }
@@ -577,10 +581,14 @@ __global__ void k_sp_walk(const int *__restrict__ succ, const int *__restrict__ 
     segend_c[s] = v;
   }
 }
-__global__ void k_sp_unowned(long long N, const int *__restrict__ owner, int *__restrict__ isspl) {
+__global__ void k_sp_unowned(long long N, const int2 *__restrict__ own, int *__restrict__ isspl,
+                             int2 *__restrict__ sf) {
   for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < N;
        r += (long long)gridDim.x * blockDim.x)
-    if (owner[r] < 0) isspl[r] = 1;
+    if (own[r].x < 0) {
+      isspl[r] = 1;
+      sf[r].y = 1;
+    }
 }
 __global__ void k_sp_compact(const int *__restrict__ isspl, const int *__restrict__ srank, long long N,
                              const int *__restrict__ nexts_c, const int *__restrict__ seglen_c,
@@ -624,7 +632,7 @@ __global__ void k_sp_jump1(const int *__restrict__ nx, const int *__restrict__ m
 // list for suffix sums: cycles are cut before the splitter holding the cycle
 // minimum; chains end at their last splitter
 __global__ void k_sp_list(const int *__restrict__ nexts, const int *__restrict__ mn,
-                          const int *__restrict__ tm, const int *__restrict__ owner,
+                          const int *__restrict__ tm, const int2 *__restrict__ own,
                           const int *__restrict__ srank, const int *__restrict__ seglen, int S,
                           int *__restrict__ sl, long long *__restrict__ suf,
                           int *__restrict__ head) {
@@ -634,7 +642,7 @@ __global__ void k_sp_list(const int *__restrict__ nexts, const int *__restrict__
       sl[k] = n;
       head[k] = -1;
     } else {
-      int h = srank[owner[mn[k]]];
+      int h = srank[own[mn[k]].x];
       head[k] = h;
       sl[k] = n == h ? -1 : n;
     }
@@ -649,7 +657,7 @@ __global__ void k_sp_jump2(const int *__restrict__ sl, const long long *__restri
     sl2[k] = n >= 0 ? sl[n] : -1;
   }
 }
-__global__ void k_sp_expand(long long N, const int *__restrict__ owner, const int *__restrict__ off,
+__global__ void k_sp_expand(long long N, const int2 *__restrict__ own,
                             const int *__restrict__ srank, const int *__restrict__ tm,
                             const int *__restrict__ mn, const long long *__restrict__ suf,
                             const int *__restrict__ head, const int *__restrict__ lastp,
@@ -657,8 +665,9 @@ __global__ void k_sp_expand(long long N, const int *__restrict__ owner, const in
                             int *__restrict__ lab, int *__restrict__ val, int *__restrict__ ep) {
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < N;
        c += (long long)gridDim.x * blockDim.x) {
-    int k = srank[owner[c]];
-    int o = off[c];
+    const int2 oc = own[c];
+    int k = srank[oc.x];
+    int o = oc.y;
     if (tm[k]) {
       term[c] = 1;
       val[c] = (int)(suf[k] - o);
@@ -667,7 +676,7 @@ __global__ void k_sp_expand(long long N, const int *__restrict__ owner, const in
     } else {
       int m = mn[k];
       long long L = suf[head[k]];
-      long long pos = (L - suf[k]) + o - off[m];
+      long long pos = (L - suf[k]) + o - own[m].y;
       if (pos < 0) pos += L;
       term[c] = 0;
       val[c] = (int)(L - pos);
@@ -908,20 +917,20 @@ int recontour_dev(casl_handle *h, const double *qq) {
   // --- 5. list ranking over crossings (splitters) ------------------------------
   int *lab = ar2.get<int>(ncr), *term = ar2.get<int>(ncr), *val = ar2.get<int>(ncr),
       *ep = ar2.get<int>(ncr);
-  int *pred = ar2.get<int>(ncr), *isspl = ar2.get<int>(ncr), *owner = ar2.get<int>(ncr),
-      *offc = ar2.get<int>(ncr), *srank = ar2.get<int>(ncr);
+  int *pred = ar2.get<int>(ncr), *isspl = ar2.get<int>(ncr), *srank = ar2.get<int>(ncr);
+  int2 *sf = ar2.get<int2>(ncr), *own = ar2.get<int2>(ncr);
   int *nexts_c = ar2.get<int>(ncr), *seglen_c = ar2.get<int>(ncr), *segmin_c = ar2.get<int>(ncr),
       *segend_c = ar2.get<int>(ncr);
   if (ar2.failed) return CASL_ENOMEM;
   int g = gsz(ncr);
   CASL_CUDA_TRY(cudaMemsetAsync(pred, 0xff, ncr * sizeof(int), st));
   CASL_K(k_sp_pred, g, 256, 0, st)(succ, ncr, pred);
-  CASL_K(k_sp_flag, g, 256, 0, st)(pred, ncr, 16, isspl, owner);
-  CASL_K(k_sp_walk, g, 256, 0, st)(succ, isspl, ncr, owner, offc, nexts_c, seglen_c, segmin_c,
-                                   segend_c, &h->scal->error);
-  CASL_K(k_sp_unowned, g, 256, 0, st)(ncr, owner, isspl);
-  CASL_K(k_sp_walk, g, 256, 0, st)(succ, isspl, ncr, owner, offc, nexts_c, seglen_c, segmin_c,
-                                   segend_c, &h->scal->error);
+  CASL_K(k_sp_flag, g, 256, 0, st)(pred, succ, ncr, 16, isspl, sf, own);
+  CASL_K(k_sp_walk, g, 256, 0, st)(sf, ncr, own, nexts_c, seglen_c, segmin_c, segend_c,
+                                   &h->scal->error);
+  CASL_K(k_sp_unowned, g, 256, 0, st)(ncr, own, isspl, sf);
+  CASL_K(k_sp_walk, g, 256, 0, st)(sf, ncr, own, nexts_c, seglen_c, segmin_c, segend_c,
+                                   &h->scal->error);
   exclusive_scan<int>(st, isspl, srank, ncr, tmpi2, dtot + 6);
   int S = 0;
   CASL_CUDA_TRY(cudaMemcpyAsync(&S, dtot + 6, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -947,13 +956,13 @@ int recontour_dev(casl_handle *h, const double *qq) {
     CASL_K(k_sp_jump1, gsS, 256, 0, st)(snx, smn, stm, slp, S, snx2, smn2, stm2, slp2);
     std::swap(snx, snx2); std::swap(smn, smn2); std::swap(stm, stm2); std::swap(slp, slp2);
   }
-  CASL_K(k_sp_list, gsS, 256, 0, st)(nexts, smn, stm, owner, srank, seglen, S, ssl, ssuf, shead);
+  CASL_K(k_sp_list, gsS, 256, 0, st)(nexts, smn, stm, own, srank, seglen, S, ssl, ssuf, shead);
   for (int it = 0; it < rounds; it++) {
     CASL_K(k_sp_jump2, gsS, 256, 0, st)(ssl, ssuf, S, ssl2, ssuf2);
     std::swap(ssl, ssl2); std::swap(ssuf, ssuf2);
   }
   tr.point("rk_jump");
-  CASL_K(k_sp_expand, g, 256, 0, st)(ncr, owner, offc, srank, stm, smn, ssuf, shead, slp, segend,
+  CASL_K(k_sp_expand, g, 256, 0, st)(ncr, own, srank, stm, smn, ssuf, shead, slp, segend,
                                      term, lab, val, ep);
   RC_TRY(check_launch(h));
   if (tr.on) fprintf(stderr, "[casl trace] ranking: %d splitters, %d jump rounds\n", S, rounds);
