@@ -174,12 +174,21 @@ __device__ __forceinline__ void rf_butterflies(double2 (&x)[8], int t, int Ns,
     const int j = t + m * TPV;
     const int k = j & (Ns - 1);
     if (k) {
+      // powers w^r of the butterfly's twiddle w (one table load): products
+      // at most three deep, so each is within a few ulps
       const int ts = n / (Ns * R);
-#pragma unroll
-      for (int r = 1; r < R; r++) {
-        double2 w = __ldg(&tw[r * k * ts]);
-        y[r] = cmul(y[r], FWD ? w : cconj(w));
+      double2 wr[8];
+      wr[1] = __ldg(&tw[k * ts]);
+      if (R >= 4) wr[2] = cmul(wr[1], wr[1]);
+      if (R == 8) wr[4] = cmul(wr[2], wr[2]);
+      if (R >= 4) wr[3] = cmul(wr[1], wr[2]);
+      if (R == 8) {
+        wr[5] = cmul(wr[1], wr[4]);
+        wr[6] = cmul(wr[2], wr[4]);
+        wr[7] = cmul(wr[3], wr[4]);
       }
+#pragma unroll
+      for (int r = 1; r < R; r++) y[r] = cmul(y[r], FWD ? wr[r] : cconj(wr[r]));
     }
     if (R == 8) dft8<FWD>(y);
     if (R == 4) dft4<FWD>(y[0], y[1], y[2], y[3]);
@@ -275,12 +284,13 @@ __global__ void __launch_bounds__(RfftShape<LOGH, LVF || SVF>::NT, RfftShape<LOG
     auto emit = [&](int k, double val) {
       if (SVF) Out[dpos(k)] = val; else st(b, vg, k, val);
     };
-    auto pair_out = [&](int kk) {
+    // tw[H-k] = -conj(tw[k]) (tw[H] = -1), so a pair needs one table load
+    auto pair_out = [&](int kk, double2 w) {
       double2 zk = S[cpad(kk)], zc = cconj(S[cpad(H - kk)]);
       double2 e = make_double2(0.5 * (zk.x + zc.x), 0.5 * (zk.y + zc.y));
       double2 d = csub(zk, zc);
       double2 od = make_double2(0.5 * d.y, -0.5 * d.x);  // (Z - conj Zc)/(2i)
-      double2 f = cadd(e, cmul(__ldg(&tw[kk]), od));
+      double2 f = cadd(e, cmul(w, od));
       emit(kk, f.x * s);
       emit(N - kk, f.y * s);
     };
@@ -292,11 +302,12 @@ __global__ void __launch_bounds__(RfftShape<LOGH, LVF || SVF>::NT, RfftShape<LOG
         emit(0, (z0.x + z0.y) * s);
         emit(H, (z0.x - z0.y) * s);
       } else {
-        pair_out(k);
-        pair_out(H - k);
+        const double2 w = __ldg(&tw[k]);
+        pair_out(k, w);
+        pair_out(H - k, make_double2(-w.x, w.y));
       }
     }
-    if (t == 0) pair_out(H / 2);  // k = H/2 pairs with itself
+    if (t == 0) pair_out(H / 2, __ldg(&tw[H / 2]));  // k = H/2 pairs with itself
     if (SVF) {
       __syncthreads();
       constexpr int Q = (V * N) / NT;
@@ -325,6 +336,7 @@ __global__ void __launch_bounds__(RfftShape<LOGH, LVF || SVF>::NT, RfftShape<LOG
         zp[2 * m + 1] = make_double2(0.0, 0.0);
       } else {
         const double a = X(k), bq = X(N - k), c = X(H - k), dq = X(N - (H - k));
+        const double2 wk = __ldg(&tw[k]);  // tw[H-k] = -conj(tw[k])
 #pragma unroll
         for (int pass = 0; pass < 2; pass++) {
           const int kk = pass == 0 ? k : H - k;
@@ -332,7 +344,8 @@ __global__ void __launch_bounds__(RfftShape<LOGH, LVF || SVF>::NT, RfftShape<LOG
           double2 G = pass == 0 ? make_double2(c, -dq) : make_double2(a, -bq);  // conj F(H-kk)
           double2 e = make_double2(0.5 * (F.x + G.x), 0.5 * (F.y + G.y));
           double2 d = make_double2(0.5 * (F.x - G.x), 0.5 * (F.y - G.y));
-          double2 o = cmul(d, cconj(__ldg(&tw[kk])));
+          const double2 w = pass == 0 ? wk : make_double2(-wk.x, wk.y);
+          double2 o = cmul(d, cconj(w));
           zp[2 * m + pass] = make_double2(e.x - o.y, e.y + o.x);
           zk[2 * m + pass] = kk;
         }

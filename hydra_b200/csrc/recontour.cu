@@ -445,7 +445,8 @@ __global__ void k_ct_gather_plain(const int *__restrict__ lab, const int *__rest
                                   const int *__restrict__ val, const int *__restrict__ cidx,
                                   const int *__restrict__ coff, const int *__restrict__ clen,
                                   const double *__restrict__ xcr, const double *__restrict__ ycr,
-                                  long long ncr, double *__restrict__ xw, double *__restrict__ yw) {
+                                  long long ncr, double *__restrict__ xw, double *__restrict__ yw,
+                                  int *__restrict__ cidw) {
   for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
        r += (long long)gridDim.x * blockDim.x) {
     if (term[r]) continue;
@@ -454,6 +455,7 @@ __global__ void k_ct_gather_plain(const int *__restrict__ lab, const int *__rest
     long long pos = (long long)coff[c] + (clen[c] - val[r]);
     xw[pos] = xcr[r];
     yw[pos] = ycr[r];
+    cidw[pos] = c;  // the contour of every walk position, for the first renode
   }
 }
 
@@ -462,8 +464,10 @@ __global__ void k_ct_gather_chain(const int *__restrict__ term, const int *__res
                                   const int *__restrict__ val, const int *__restrict__ chain_of_end,
                                   const long long *__restrict__ chpos, const int *__restrict__ chlen,
                                   const int *__restrict__ chrot, const int *__restrict__ chclen,
-                                  const double *__restrict__ xcr, const double *__restrict__ ycr,
-                                  long long ncr, double *__restrict__ xw, double *__restrict__ yw) {
+                                  const int *__restrict__ chcont, const double *__restrict__ xcr,
+                                  const double *__restrict__ ycr, long long ncr,
+                                  double *__restrict__ xw, double *__restrict__ yw,
+                                  int *__restrict__ cidw) {
   for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
        r += (long long)gridDim.x * blockDim.x) {
     if (!term[r]) continue;
@@ -482,6 +486,7 @@ __global__ void k_ct_gather_chain(const int *__restrict__ term, const int *__res
     }
     xw[pos] = xcr[r];
     yw[pos] = ycr[r];
+    cidw[pos] = chcont[ch];
   }
 }
 
@@ -1127,11 +1132,13 @@ int recontour_dev(casl_handle *h, const double *qq) {
   if (C == 0) return set_empty();
   int *clen = ar2.get<int>(C), *coff = ar2.get<int>(C), *clevt = ar2.get<int>(C);
   double *xw = ar2.get<double>(ncr), *yw = ar2.get<double>(ncr);
+  int *cidw = ar2.get<int>(ncr);
   if (ar2.failed) return CASL_ENOMEM;
   // contour lengths in contour order, and their offsets
   CASL_K(k_ct_len, g, 256, 0, st)(startf, clenr, cidx, ncr, clen);
   exclusive_scan<int>(st, clen, coff, C, tmpi2, dtot + 2);
-  CASL_K(k_ct_gather_plain, g, 256, 0, st)(lab, term, val, cidx, coff, clen, xcr, ycr, ncr, xw, yw);
+  CASL_K(k_ct_gather_plain, g, 256, 0, st)(lab, term, val, cidx, coff, clen, xcr, ycr, ncr, xw, yw,
+                                           cidw);
   int nch = (int)ch_end.size();
   if (nch > 0) {
     // absolute position of every chain; the first chain of a contour is
@@ -1141,16 +1148,17 @@ int recontour_dev(casl_handle *h, const double *qq) {
     RC_TRY(gather(cidx, sad_start, sad_cidx));
     RC_TRY(gather(coff, sad_cidx, sad_off));
     std::vector<long long> abs_pos(nch);
-    std::vector<int> rotlen(nch, 0);
+    std::vector<int> rotlen(nch, 0), chc(nch);
     for (int ch = 0; ch < nch; ch++) {
       int cont = ch_cont[ch];
       if (cont < 0) return CASL_EINVAL;
       abs_pos[ch] = sad_off[cont] + ch_pos[ch];
       if (ch_rot[ch] >= 0) rotlen[ch] = sad_len[cont];
+      chc[ch] = sad_cidx[cont];
     }
     long long *d_pos = ar2.get<long long>(nch);
     int *d_len = ar2.get<int>(nch), *d_rot = ar2.get<int>(nch), *d_cl = ar2.get<int>(nch);
-    int *d_ends = ar2.get<int>(nch);
+    int *d_ends = ar2.get<int>(nch), *d_cc = ar2.get<int>(nch);
     int *chain_of_end = ar2.get<int>(ncr);
     if (ar2.failed) return CASL_ENOMEM;
     CASL_CUDA_TRY(cudaMemcpyAsync(d_pos, abs_pos.data(), nch * sizeof(long long), cudaMemcpyHostToDevice, st));
@@ -1158,17 +1166,18 @@ int recontour_dev(casl_handle *h, const double *qq) {
     CASL_CUDA_TRY(cudaMemcpyAsync(d_rot, ch_rot.data(), nch * sizeof(int), cudaMemcpyHostToDevice, st));
     CASL_CUDA_TRY(cudaMemcpyAsync(d_cl, rotlen.data(), nch * sizeof(int), cudaMemcpyHostToDevice, st));
     CASL_CUDA_TRY(cudaMemcpyAsync(d_ends, ch_end.data(), nch * sizeof(int), cudaMemcpyHostToDevice, st));
+    CASL_CUDA_TRY(cudaMemcpyAsync(d_cc, chc.data(), nch * sizeof(int), cudaMemcpyHostToDevice, st));
     CASL_CUDA_TRY(cudaMemsetAsync(chain_of_end, 0xff, ncr * sizeof(int), st));
     CASL_K(k_chain_of_end, gsz(nch), 256, 0, st)(d_ends, nch, chain_of_end);
     CASL_K(k_ct_gather_chain, g, 256, 0, st)(term, ep, val, chain_of_end, d_pos, d_len, d_rot, d_cl,
-                                             xcr, ycr, ncr, xw, yw);
+                                             d_cc, xcr, ycr, ncr, xw, yw, cidw);
   }
   CASL_K(k_lev_of_contour, g, 256, 0, st)(startf, rlev, cidx, ncr, li, h->p.nlevm, clevt);
   RC_TRY(check_launch(h));
 
   tr.point("layout");
   // --- 8. renode three times (congen.f90:295-310) -----------------------------
-  RenodeIn cur{xw, yw, coff, clen, clevt, C, ncr};
+  RenodeIn cur{xw, yw, coff, clen, clevt, C, ncr, nullptr, cidw};
   long long capn = std::max<long long>(ncr * 2, h->npm);
   double *xa = ar2.get<double>(capn), *ya = ar2.get<double>(capn);
   double *xb = ar2.get<double>(capn), *yb = ar2.get<double>(capn);

@@ -12,15 +12,12 @@ __device__ __forceinline__ long long wprev(long long w, long long cs, long long 
   return w > cs ? w - 1 : cs + L - 1;
 }
 
-__global__ void k_rn_cid(RenodeIn in, long long N, int *__restrict__ cid, int *__restrict__ head) {
+__global__ void k_rn_cid(RenodeIn in, long long N, int *__restrict__ cid) {
   const int C = contours_in(in);
   const int *cs = in.cs;
   for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < N;
-       w += (long long)gridDim.x * blockDim.x) {
-    int c = contour_of(cs, C, w);
-    cid[w] = c;
-    head[w] = (w == cs[c]);
-  }
+       w += (long long)gridDim.x * blockDim.x)
+    cid[w] = contour_of(cs, C, w);
 }
 
 // The node densities of renode (contours.f90:718-796) for node w in one
@@ -102,6 +99,7 @@ __global__ void k_rn_stencil(RenodeIn in, RenodeScratch s, Consts c) {
     s.B[w] = B;
     s.Cc[w] = Cc;
     s.corner[w] = corner2;
+    s.head[w] = (w == cs);
     if (corner2) atomicAdd(&s.ccnt[k], 1);
   }
 }
@@ -275,7 +273,7 @@ int renode_batch(casl_handle *h, Arena &ar, const RenodeIn &in, RenodeOut &out, 
     return CASL_OK;
   }
   RenodeScratch s{};
-  s.cid = ar.get<int>(N);
+  s.cid = in.cid ? const_cast<int *>(in.cid) : ar.get<int>(N);
   s.dx = ar.get<double>(N); s.dy = ar.get<double>(N);
   s.e = ar.get<double>(N); s.A = ar.get<double>(N);
   s.B = ar.get<double>(N); s.Cc = ar.get<double>(N); s.S = ar.get<double>(N);
@@ -298,7 +296,7 @@ int renode_batch(casl_handle *h, Arena &ar, const RenodeIn &in, RenodeOut &out, 
   if (ar.failed) return CASL_ENOMEM;
   cudaMemsetAsync(s.ccnt, 0, C * sizeof(int), st);
   int g = gsz(N);
-  CASL_K(k_rn_cid, g, 256, 0, st)(in, N, s.cid, s.head);
+  if (!in.cid) CASL_K(k_rn_cid, g, 256, 0, st)(in, N, s.cid);
   CASL_K(k_rn_stencil, g, 256, 0, st)(in, s, c);
   segmented_scan(st, s.e, s.head, s.S, N, s.tmps);
   exclusive_scan<int>(st, s.corner, s.crank, N, s.tmpi, s.d_tot + 0);

@@ -26,6 +26,7 @@ struct RenodeIn {
   int C;                  // contours (an upper bound when Cdev is given)
   long long N;            // nodes
   const int *Cdev;        // optional: the contour count in device memory
+  const int *cid;         // optional: the contour of every walk node (else searched)
 };
 
 __device__ __forceinline__ int contours_in(const RenodeIn &in) { return in.Cdev ? *in.Cdev : in.C; }

@@ -604,7 +604,7 @@ __global__ void k_rb_gather2(const double *__restrict__ xq, const double *__rest
                              const int *__restrict__ hr, const int *__restrict__ cidx,
                              long long *const *__restrict__ valp, const int *__restrict__ cst,
                              const int *__restrict__ clen, double *__restrict__ xw,
-                             double *__restrict__ yw) {
+                             double *__restrict__ yw, int *__restrict__ cidw) {
   const long long *val = *valp;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npt; i += gridDim.x * blockDim.x) {
     int r = rid[i];
@@ -613,6 +613,7 @@ __global__ void k_rb_gather2(const double *__restrict__ xq, const double *__rest
     long long pos = cst[c] + off + (i - rs[r]);
     xw[pos] = xq[i];
     yw[pos] = yq[i];
+    cidw[pos] = c;
   }
 }
 
@@ -690,10 +691,13 @@ static int rebuild_and_renode(casl_handle *h, Arena &ar, int npt, const int *lvl
   exclusive_scan<int>(st, ishead, cidx, npt, tmpi, dtot + 1);  // dtot[1] = C
   CASL_K(k_rb_cycles2, g, 256, 0, st)(ishead, cidx, valp, rs, lvl, dlev, dtot, clen, clev);
   exclusive_scan<int>(st, clen, cst, npt, tmpi, dtot + 2);
-  CASL_K(k_rb_gather2, g, 256, 0, st)(h->xq, h->yq, npt, rid, rs, hr, cidx, valp, cst, clen, xw, yw);
+  int *cidw = ar.get<int>(npt);
+  if (ar.failed) return CASL_ENOMEM;
+  CASL_K(k_rb_gather2, g, 256, 0, st)(h->xq, h->yq, npt, rid, rs, hr, cidx, valp, cst, clen, xw, yw,
+                                      cidw);
   int rc = check_launch(h);
   if (rc) return rc;
-  RenodeIn in{xw, yw, cst, clen, clev, npt, npt, dtot + 1};
+  RenodeIn in{xw, yw, cst, clen, clev, npt, npt, dtot + 1, cidw};
   RenodeOut out{};
   out.xo = h->xqi;  // node-sized scratch of the RK step, free between steps
   out.yo = h->yqi;
