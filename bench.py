@@ -214,6 +214,23 @@ def run_reference(a):
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
+def reduce_over_ranks(vals, world, device):
+    """[ms, node_steps, e2e_ms, e2e_node_steps] of this rank -> the job's
+    (max ms, summed node-steps, max e2e ms, summed e2e node-steps): the time
+    of the slowest replica, the work of all of them.  The all-reduces run on
+    the process group's backend (NCCL between GPUs)."""
+    import torch
+    import torch.distributed as dist
+    if world <= 1:
+        return vals[0], vals[1], vals[2], vals[3]
+    t = torch.tensor(vals, dtype=torch.float64, device=device)
+    mx = t.clone()
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    sm = t.clone()
+    dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+    return mx[0].item(), sm[1].item(), mx[2].item(), sm[3].item()
+
+
 def run_gpu(a):
     import torch
     import torch.distributed as dist
@@ -279,17 +296,8 @@ def run_gpu(a):
                          "its timed steps (surgery + advance; no recontouring in the sample)"}
 
     # ---- reduce over ranks ---------------------------------------------------------------
-    t = torch.tensor([ms, node_steps, e2e["ms"], e2e["node_steps"]], dtype=torch.float64,
-                     device=f"cuda:{local}")
-    if world > 1:
-        mx = t.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        sm = t.clone()
-        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        ms_max, ns_sum = mx[0].item(), sm[1].item()
-        e2e_ms, e2e_ns = mx[2].item(), sm[3].item()
-    else:
-        ms_max, ns_sum, e2e_ms, e2e_ns = ms, node_steps, e2e["ms"], e2e["node_steps"]
+    ms_max, ns_sum, e2e_ms, e2e_ns = reduce_over_ranks(
+        [ms, node_steps, e2e["ms"], e2e["node_steps"]], world, f"cuda:{local}")
     if rank == 0:
         peak, peak_kind = measured_peak()
         ach = fft_bytes / (fft_ms * 1e-3) / 1e9 if fft_ms > 0 else 0.0

@@ -437,16 +437,23 @@ __global__ void k_c2g_coarsen(const int *__restrict__ L, int *__restrict__ C,
 #define C2G_CW 7
 #define C2G_FC (4 * C2G_CW + 3)
 template <int U>
+constexpr size_t c2g_fused_smem() {
+  return 32 * sizeof(long long) + (size_t)(32 * U + 8 + 4 + 8 * U) * C2G_FC * sizeof(int);
+}
+template <int U>
 __global__ void __launch_bounds__(1024) k_c2g_fused(const int *__restrict__ J,
                                                     const int *__restrict__ ljx,
                                                     int *__restrict__ C,
                                                     unsigned long long *__restrict__ csum, int n,
                                                     int nf) {
   constexpr int RPS = 32 * U, RING = RPS + 8, CR = RPS / 4;
-  __shared__ int ring[RING][C2G_FC];
-  __shared__ int first[4][C2G_FC];
-  __shared__ int vsum[CR][C2G_FC];
-  __shared__ long long red[32];
+  // dynamic shared memory (c2g_fused_smem<U>() bytes): the ring of level
+  // rows, the first rows, the vertical sums, the block reduction
+  extern __shared__ long long c2g_dyn[];
+  long long *red = c2g_dyn;
+  int (*ring)[C2G_FC] = reinterpret_cast<int (*)[C2G_FC]>(c2g_dyn + 32);
+  int (*first)[C2G_FC] = ring + RING;
+  int (*vsum)[C2G_FC] = first + 4;
   const int w7[7] = {1, 2, 3, 4, 3, 2, 1};
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int cx0 = blockIdx.x * C2G_CW;  // first coarse column (0-based)
@@ -580,10 +587,21 @@ int con2grid_dev(casl_handle *h, bool want_levels) {
     CASL_CUDA_TRY(cudaMemsetAsync(csum, 0, sizeof(unsigned long long), h->stream));
   }
   int nblk = (h->n + C2G_CW - 1) / C2G_CW;
-  if (!want_levels && c.nxf == c.nyf && c.nxf % 256 == 0) {
-    CASL_K(k_c2g_fused<8>, nblk, 1024, 0, h->stream)(h->fineJ, h->ljx, h->coarseC, csum, h->n, c.nxf);
+  if (!want_levels && c.nxf == c.nyf && c.nxf % 512 == 0) {
+    static bool attr16 = false;  // one attribute call for the >48 KB variant
+    if (!attr16) {
+      cudaFuncSetAttribute(k_c2g_fused<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)c2g_fused_smem<16>());
+      attr16 = true;
+    }
+    CASL_K(k_c2g_fused<16>, nblk, 1024, c2g_fused_smem<16>(), h->stream)(h->fineJ, h->ljx, h->coarseC,
+                                                                       csum, h->n, c.nxf);
+  } else if (!want_levels && c.nxf == c.nyf && c.nxf % 256 == 0) {
+    CASL_K(k_c2g_fused<8>, nblk, 1024, c2g_fused_smem<8>(), h->stream)(h->fineJ, h->ljx, h->coarseC,
+                                                                     csum, h->n, c.nxf);
   } else if (!want_levels && c.nxf == c.nyf && c.nxf % 128 == 0) {
-    CASL_K(k_c2g_fused<4>, nblk, 1024, 0, h->stream)(h->fineJ, h->ljx, h->coarseC, csum, h->n, c.nxf);
+    CASL_K(k_c2g_fused<4>, nblk, 1024, c2g_fused_smem<4>(), h->stream)(h->fineJ, h->ljx, h->coarseC,
+                                                                     csum, h->n, c.nxf);
   } else {
     // the fine-grid levels themselves are wanted: bottom row, scan in place,
     // then coarsen

@@ -91,6 +91,22 @@ def test_con2grid_levels_bit_exact(pair):
     assert np.abs(qc_g - qc_o).max() < 1e-12 * np.abs(qc_o).max()
 
 
+@pytest.mark.parametrize("n,k0,levels", [(64, 6.0, 20), (128, 8.0, 30), (256, 8.0, 40)])
+def test_con2grid_fused_matches_oracle(oracle_mod, gpu_lib, n, k0, levels):
+    """con2grid without the fine levels runs the fused column scan +
+    coarsening (8 or 16 chunks of 32 rows per step, by size); its integer
+    coarse cells make qc agree with the oracle to rounding."""
+    from hydra_b200.casl import CaslGPU
+    o = oracle_mod.Oracle(n, ncontq=levels, dtmax=0.05)
+    o.initialise(random_pv(n, k0, 3))
+    g = CaslGPU(n, ncontq=levels, dtmax=0.05)
+    g.set_contours(o.contours())
+    qc_o, _ = o.con2grid(levels=True)
+    qc_g = g.con2grid()
+    assert np.abs(qc_g - qc_o).max() < 1e-12 * np.abs(qc_o).max()
+    g.close()
+
+
 def test_velint_bit_exact(pair):
     o, g = pair
     rng = np.random.default_rng(9)
