@@ -122,19 +122,85 @@ __global__ void k_u_colscan(int *__restrict__ J, int nxu, int nyu,
   if (lane == 0) atomicAdd(total, (unsigned long long)s);
 }
 
-// qa = (L*qjump - qavg) + bilinear residual, or the bilinear field alone.
-// One thread per run of 16 rows of a column: the run lies in one coarse cell
-// in y, so the four coarse values are gathered once; the levels come in and
-// qa goes out as 16-byte vectors.  Per element the expression and its order
-// are the reference's (congen.f90:45-61 on con2ugrid's field).
+struct LevInfo {
+  int levbeg, levend;
+  double qjump, qoff, qjumpi;
+};
+
+__device__ __forceinline__ double qtmp_of(int lev, const LevInfo &li) {
+  return ((double)lev - 0.5) * li.qjump - li.qoff;
+}
+
+// Largest level l whose contour value qtmp(l) = (l - 1/2) qjump - qoff is
+// <= v.  qtmp is increasing in l (also as rounded), so an edge with end
+// values lo < hi crosses exactly the levels c(lo) < l <= c(hi): those where
+// the reference's sign(qa - qtmp) differs at the two ends (congen.f90:205-212).
+__device__ __forceinline__ int level_index(double v, const LevInfo &li) {
+  int l = (int)floor((v + li.qoff) * li.qjumpi + 0.5);
+  while (qtmp_of(l + 1, li) <= v) l++;
+  while (qtmp_of(l, li) > v) l--;
+  return l;
+}
+
+// One element of the ultra-fine field: (L*qjump - qavg) + bilinear residual,
+// or the bilinear residual alone; (ixf, iyf) is the point's 1-based place in
+// its coarse cell, q00..q11 the cell's corner values.  Per element the
+// expression and its order are the reference's (congen.f90:45-61 on
+// con2ugrid's field).  The field kernel and the crossing geometry both
+// evaluate the field here, so the crossing positions are computed from the
+// very values the crossings were found on.
+__device__ __forceinline__ double ufield_elem(int lv, int ixf, int iyf, double q00, double q10,
+                                              double q01, double q11, double qjump, double qavg,
+                                              int have_contours) {
+  const double fac = 1.0 / 16.0;
+  const double pxf = fac * (double)(ixf - 1), pxc = 1.0 - pxf;
+  const double pyf = fac * (double)(iyf - 1), pyc = 1.0 - pyf;
+  const double w00 = pyc * pxc, w10 = pyf * pxc, w01 = pyc * pxf, w11 = pyf * pxf;
+  if (have_contours) {
+    double v = (double)lv * qjump - qavg;
+    return v + w00 * q00 + w10 * q10 + w01 * q01 + w11 * q11;
+  }
+  return w00 * q00 + w10 * q10 + w01 * q01 + w11 * q11;
+}
+__device__ __forceinline__ double ufield_qavg(const unsigned long long *lsum, double qjump,
+                                              int have_contours, int nxu, int nyu) {
+  return have_contours ? qjump * ((double)(long long)(*lsum) / ((double)nxu * (double)nyu)) : 0.0;
+}
+// the field at the 1-based ultra-fine point (ix, iy)
+struct UField {
+  const int *L;
+  const unsigned long long *lsum;
+  const double *qq;
+  double qjump;
+  int have;
+};
+__device__ __forceinline__ double ufield_at(const UField &u, double qavg, int ix, int iy,
+                                            const Consts &c) {
+  const int n = c.nx;
+  const int ixx = (ix - 1) / 16, iyy = (iy - 1) / 16;
+  const int ix0 = 1 + ixx, ix1 = 2 + ixx - n * (ix0 / n), ixf = ix - 16 * ixx;
+  const int iy0 = 1 + iyy, iy1 = 2 + iyy - n * (iy0 / n), iyf = iy - 16 * iyy;
+  const double q00 = u.qq[(long long)(ix0 - 1) * n + iy0 - 1];
+  const double q10 = u.qq[(long long)(ix0 - 1) * n + iy1 - 1];
+  const double q01 = u.qq[(long long)(ix1 - 1) * n + iy0 - 1];
+  const double q11 = u.qq[(long long)(ix1 - 1) * n + iy1 - 1];
+  const int lv = u.have ? u.L[(long long)(ix - 1) * c.nyu + iy - 1] : 0;
+  return ufield_elem(lv, ixf, iyf, q00, q10, q01, q11, u.qjump, qavg, u.have);
+}
+
+// The ultra-fine field, one thread per run of 16 rows of a column: the run
+// lies in one coarse cell in y, so the four coarse values are gathered once;
+// the levels come in as 16-byte vectors.  Out go the field itself (qa, when
+// asked for) and/or its level code lc = level_index(v) clipped to
+// [0, 65535], with the field's extremes.  qtmp depends only on qjump and
+// nlevm, so the code is known before the level range is.
 __global__ void k_u_field(const int *__restrict__ L, const unsigned long long *__restrict__ lsum,
                           const double *__restrict__ qq, double qjump, int have_contours,
-                          double *__restrict__ qa, double *__restrict__ part, Consts c) {
+                          LevInfo lq, double *__restrict__ qa, unsigned short *__restrict__ lc,
+                          double *__restrict__ part, Consts c) {
   const int nxu = c.nxu, nyu = c.nyu, n = c.nx;
   const long long nruns = (long long)nxu * (nyu / 16);
-  double qavg = 0.0;
-  if (have_contours) qavg = qjump * ((double)(long long)(*lsum) / ((double)nxu * (double)nyu));
-  const double fac = 1.0 / 16.0;
+  const double qavg = ufield_qavg(lsum, qjump, have_contours, nxu, nyu);
   double mx = -1.0e308, mn = 1.0e308;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nruns;
        t += (long long)gridDim.x * blockDim.x) {
@@ -142,7 +208,6 @@ __global__ void k_u_field(const int *__restrict__ L, const unsigned long long *_
     const int ixx = (ix - 1) / 16;
     const int ix0 = 1 + ixx, ix1 = 2 + ixx - n * (ix0 / n), ixf = ix - 16 * ixx;
     const int iy0 = 1 + iyy, iy1 = 2 + iyy - n * (iy0 / n);
-    const double pxf = fac * (double)(ixf - 1), pxc = 1.0 - pxf;
     const double q00 = qq[(long long)(ix0 - 1) * n + iy0 - 1], q10 = qq[(long long)(ix0 - 1) * n + iy1 - 1];
     const double q01 = qq[(long long)(ix1 - 1) * n + iy0 - 1], q11 = qq[(long long)(ix1 - 1) * n + iy1 - 1];
     const long long base = (long long)(ix - 1) * nyu + 16LL * iyy;
@@ -154,28 +219,33 @@ __global__ void k_u_field(const int *__restrict__ L, const unsigned long long *_
         int4 q = l4[k];
         lv[4 * k] = q.x; lv[4 * k + 1] = q.y; lv[4 * k + 2] = q.z; lv[4 * k + 3] = q.w;
       }
+    } else {
+#pragma unroll
+      for (int k = 0; k < 16; k++) lv[k] = 0;
     }
-    double2 *o2 = reinterpret_cast<double2 *>(qa + base);
+    unsigned int code[8];
 #pragma unroll
     for (int k = 0; k < 8; k++) {
       double out[2];
 #pragma unroll
       for (int h = 0; h < 2; h++) {
-        const int iyf = 2 * k + h + 1;
-        const double pyf = fac * (double)(iyf - 1), pyc = 1.0 - pyf;
-        const double w00 = pyc * pxc, w10 = pyf * pxc, w01 = pyc * pxf, w11 = pyf * pxf;
-        double v;
-        if (have_contours) {
-          v = (double)lv[2 * k + h] * qjump - qavg;
-          v = v + w00 * q00 + w10 * q10 + w01 * q01 + w11 * q11;
-        } else {
-          v = w00 * q00 + w10 * q10 + w01 * q01 + w11 * q11;
-        }
+        const double v = ufield_elem(lv[2 * k + h], ixf, 2 * k + h + 1, q00, q10, q01, q11, qjump,
+                                     qavg, have_contours);
         out[h] = v;
         mx = fmax(mx, v);
         mn = fmin(mn, v);
       }
-      o2[k] = make_double2(out[0], out[1]);
+      if (qa) reinterpret_cast<double2 *>(qa + base)[k] = make_double2(out[0], out[1]);
+      if (lc) {
+        const unsigned int c0 = (unsigned int)min(max(level_index(out[0], lq), 0), 65535);
+        const unsigned int c1 = (unsigned int)min(max(level_index(out[1], lq), 0), 65535);
+        code[k] = c0 | (c1 << 16);
+      }
+    }
+    if (lc) {
+      uint4 *o4 = reinterpret_cast<uint4 *>(lc + base);
+      o4[0] = make_uint4(code[0], code[1], code[2], code[3]);
+      o4[1] = make_uint4(code[4], code[5], code[6], code[7]);
     }
   }
   __shared__ double a[256], b[256];
@@ -198,57 +268,52 @@ __global__ void k_u_field(const int *__restrict__ L, const unsigned long long *_
 // ---------------------------------------------------------------------------
 // Crossings
 // ---------------------------------------------------------------------------
-struct LevInfo {
-  int levbeg, levend;
-  double qjump, qoff, qjumpi;
-};
-
-__device__ __forceinline__ double qtmp_of(int lev, const LevInfo &li) {
-  return ((double)lev - 0.5) * li.qjump - li.qoff;
-}
-
-// Largest level l whose contour value qtmp(l) = (l - 1/2) qjump - qoff is
-// <= v.  qtmp is increasing in l (also as rounded), so an edge with end
-// values lo < hi crosses exactly the levels c(lo) < l <= c(hi): those where
-// the reference's sign(qa - qtmp) differs at the two ends (congen.f90:205-212).
-__device__ __forceinline__ int level_index(double v, const LevInfo &li) {
-  int l = (int)floor((v + li.qoff) * li.qjumpi + 0.5);
-  while (qtmp_of(l + 1, li) <= v) l++;
-  while (qtmp_of(l, li) > v) l--;
-  return l;
-}
-
 constexpr int EDGES_PER_THREAD = 16;
 
 // Crossings are counted and emitted per chunk of 16 consecutive edges in the
 // reference's numbering: x-line edges (ix, iy)-(ix, iy+1) are numbered
 // e = ix*nyu + iy, y-line edges (ix, iy)-(ix+1, iy) e = NE + iy*nxu + ix.
-// One CTA takes a tile of CB = 16 columns x RB = 64 rows of the field, staged
-// in shared memory with the next row and column (periodic), so the field is
-// read once, coalesced, by independent CTAs.  Each half-warp handles one
-// chunk: 16 rows of a column (x-line edges) or 16 columns of a row (y-line
-// edges).  COUNT writes the chunk's number of crossings; EMIT writes its
-// crossings (edge, level) from the chunk's offset on, edge by edge and level
-// by level, which is the reference's order within a chunk.
+// One CTA takes a tile of CB = 16 columns x RB = 64 rows of level codes,
+// staged in shared memory with the next row and column (periodic): each
+// column's 64 codes are 8 16-byte loads, so the tile with its halo is one
+// load per thread.  An edge whose ends have codes ca, cb crosses exactly the
+// levels min(ca, cb) < l <= max(ca, cb) (none when they are equal, which
+// takes in equal end values).  Each half-warp handles one chunk: 16 rows of
+// a column (x-line edges) or 16 columns of a row (y-line edges).  COUNT
+// writes the chunk's number of crossings; EMIT writes its crossings (edge,
+// level) from the chunk's offset on, edge by edge and level by level, which
+// is the reference's order within a chunk.
 constexpr int CR_CB = 16, CR_RB = 64;
 
 template <bool EMIT>
-__global__ void __launch_bounds__(256) k_cr_tile(const double *__restrict__ qa, LevInfo li, int nxu,
-                                                 int nyu, int *__restrict__ cnt,
+__global__ void __launch_bounds__(256) k_cr_tile(const unsigned short *__restrict__ lc, LevInfo li,
+                                                 int nxu, int nyu, int *__restrict__ cnt,
                                                  const int *__restrict__ off,
                                                  unsigned long long *__restrict__ redge,
                                                  int *__restrict__ rlev) {
-  __shared__ double S[CR_CB + 1][CR_RB + 1];  // row length 65: conflict-free both ways
-  __shared__ int Cl[CR_CB + 1][CR_RB + 1];    // level index of every staged value
+  __shared__ int Cl[CR_CB + 1][CR_RB + 1];  // row length 65: conflict-free both ways
   const int ix0 = blockIdx.x * CR_CB, iy0 = blockIdx.y * CR_RB;
-  for (int idx = threadIdx.x; idx < (CR_CB + 1) * (CR_RB + 1); idx += blockDim.x) {
-    const int cc = idx / (CR_RB + 1), r = idx - cc * (CR_RB + 1);
-    int ix = ix0 + cc, iy = iy0 + r;
-    if (ix >= nxu) ix -= nxu;
-    if (iy >= nyu) iy -= nyu;
-    const double v = qa[(long long)ix * nyu + iy];
-    S[cc][r] = v;
-    Cl[cc][r] = level_index(v, li);
+  {
+    const int t = threadIdx.x;
+    if (t < (CR_CB + 1) * 8) {  // 17 columns x 8 vectors of 8 codes
+      const int cc = t >> 3, part = t & 7;
+      int ix = ix0 + cc;
+      if (ix >= nxu) ix -= nxu;
+      const uint4 v =
+          *reinterpret_cast<const uint4 *>(lc + (long long)ix * nyu + iy0 + 8 * part);
+      const unsigned int w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        Cl[cc][8 * part + 2 * j] = (int)(w[j] & 0xffffu);
+        Cl[cc][8 * part + 2 * j + 1] = (int)(w[j] >> 16);
+      }
+    } else if (t < (CR_CB + 1) * 9) {  // the row after the tile, periodic
+      const int cc = t - (CR_CB + 1) * 8;
+      int ix = ix0 + cc, iy = iy0 + CR_RB;
+      if (ix >= nxu) ix -= nxu;
+      if (iy >= nyu) iy -= nyu;
+      Cl[cc][CR_RB] = lc[(long long)ix * nyu + iy];
+    }
   }
   __syncthreads();
   const long long NE = (long long)nxu * nyu;
@@ -272,13 +337,8 @@ __global__ void __launch_bounds__(256) k_cr_tile(const double *__restrict__ qa, 
       nxt_r = r;
       e = NE + (long long)(iy0 + r) * nxu + (ix0 + cc);
     }
-    const double a = S[cc][r], b = S[nxt_c][nxt_r];
     const int ca = Cl[cc][r], cb = Cl[nxt_c][nxt_r];
-    int l1 = 0, l2 = -1;
-    if (a != b) {
-      l1 = max((a < b ? ca : cb) + 1, li.levbeg);
-      l2 = min(a < b ? cb : ca, li.levend);
-    }
+    const int l1 = max(min(ca, cb) + 1, li.levbeg), l2 = min(max(ca, cb), li.levend);
     const int k = l2 >= l1 ? l2 - l1 + 1 : 0;
     const long long chunk_id = e / EDGES_PER_THREAD;
     if (!EMIT) {
@@ -304,20 +364,23 @@ __global__ void __launch_bounds__(256) k_cr_tile(const double *__restrict__ qa, 
 }
 
 // Position and box transitions of every crossing (congen.f90:211-252).
-__global__ void k_cr_geom(const double *__restrict__ qa, const unsigned long long *__restrict__ redge,
+// The end values are the ultra-fine field recomputed at the edge's two
+// points, bit for bit the values the level codes were taken from.
+__global__ void k_cr_geom(UField uf, const unsigned long long *__restrict__ redge,
                           const int *__restrict__ rlev, long long ncr, LevInfo li, Consts c,
                           double *__restrict__ xcr, double *__restrict__ ycr,
                           unsigned int *__restrict__ kib, unsigned int *__restrict__ kob) {
   const int nxu = c.nxu, nyu = c.nyu;
   const long long NE = (long long)nxu * nyu;
+  const double qavg = ufield_qavg(uf.lsum, uf.qjump, uf.have, nxu, nyu);
   for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
        r += (long long)gridDim.x * blockDim.x) {
     long long e = (long long)redge[r];
     double qtmp = qtmp_of(rlev[r] + li.levbeg, li);
     if (e < NE) {
       int ix = (int)(e / nyu) + 1, iy = (int)(e % nyu) + 1;
-      double q0 = qa[(long long)(ix - 1) * nyu + iy - 1] - qtmp;
-      double q1 = qa[(long long)(ix - 1) * nyu + (iy == nyu ? 0 : iy)] - qtmp;
+      double q0 = ufield_at(uf, qavg, ix, iy, c) - qtmp;
+      double q1 = ufield_at(uf, qavg, ix, iy == nyu ? 1 : iy + 1, c) - qtmp;
       int isy = (int)f_sign1(q0);
       int inc = (1 - isy) / 2;
       long long kaa = (long long)(iy - 1) * nxu + 1;
@@ -332,8 +395,8 @@ __global__ void k_cr_geom(const double *__restrict__ qa, const unsigned long lon
     } else {
       long long f = e - NE;
       int iy = (int)(f / nxu) + 1, ix = (int)(f % nxu) + 1;
-      double q0 = qa[(long long)(ix - 1) * nyu + iy - 1] - qtmp;
-      double q1 = qa[(long long)(ix == nxu ? 0 : ix) * nyu + iy - 1] - qtmp;
+      double q0 = ufield_at(uf, qavg, ix, iy, c) - qtmp;
+      double q1 = ufield_at(uf, qavg, ix == nxu ? 1 : ix + 1, iy, c) - qtmp;
       int isx = (int)f_sign1(q0);
       int inc = (1 - isx) / 2;
       int j1 = iy + 1 - inc, j2 = iy + inc;
@@ -373,18 +436,21 @@ struct __align__(16) HBucket {
   int s0, s1;
 };
 
+// Crossings [0, n) of a batch of consecutive levels; slots store the global
+// crossing index base + r.
 __global__ void k_h_insert(const int *__restrict__ rlev, const unsigned int *__restrict__ kob,
-                           long long ncr, HBucket *__restrict__ hb, unsigned long long mask,
-                           int *__restrict__ err) {
-  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
+                           long long n, int base, HBucket *__restrict__ hb,
+                           unsigned long long mask, int *__restrict__ err) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n;
        r += (long long)gridDim.x * blockDim.x) {
     unsigned long long k = hkey(rlev[r], kob[r]);
     unsigned long long p = hmix(k) & mask;
+    const int slot = base + (int)r;
     for (unsigned long long probe = 0; probe <= mask; probe++) {
       unsigned long long prev = atomicCAS(&hb[p].key, HEMPTY, k);
       if (prev == HEMPTY || prev == k) {
-        if (atomicCAS(&hb[p].s0, -1, (int)r) != -1)
-          if (atomicCAS(&hb[p].s1, -1, (int)r) != -1) atomicExch(err, CASL_ECAPACITY);
+        if (atomicCAS(&hb[p].s0, -1, slot) != -1)
+          if (atomicCAS(&hb[p].s1, -1, slot) != -1) atomicExch(err, CASL_ECAPACITY);
         break;
       }
       p = (p + 1) & mask;
@@ -392,27 +458,30 @@ __global__ void k_h_insert(const int *__restrict__ rlev, const unsigned int *__r
   }
 }
 
-// successor of each crossing; -1 where it enters a saddle box (2 out-crossings)
+// Successor of each crossing of the batch.  A crossing that enters a saddle
+// box (two out-crossings) gets succ = -1 and, in sadslot, the box's two
+// out-crossings packed as (lower << 32) | higher: the pair names the box
+// once the table has been reused for the next batch.  -1 elsewhere.
 __global__ void k_h_succ(const int *__restrict__ rlev, const unsigned int *__restrict__ kib,
-                         long long ncr, const HBucket *__restrict__ hb, unsigned long long mask,
+                         long long n, const HBucket *__restrict__ hb, unsigned long long mask,
                          int *__restrict__ succ, long long *__restrict__ sadslot,
                          int *__restrict__ err) {
-  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n;
        r += (long long)gridDim.x * blockDim.x) {
     const unsigned long long k = hkey(rlev[r], kib[r]);
     unsigned long long p = hmix(k) & mask;
-    long long found = -1;
+    bool found = false;
     HBucket v;
     for (unsigned long long probe = 0; probe <= mask; probe++) {
       v = hb[p];
       if (v.key == k) {
-        found = (long long)p;
+        found = true;
         break;
       }
       if (v.key == HEMPTY) break;
       p = (p + 1) & mask;
     }
-    if (found < 0) {
+    if (!found) {
       atomicExch(err, CASL_EINVAL);
       succ[r] = -1;
       sadslot[r] = -1;
@@ -423,8 +492,22 @@ __global__ void k_h_succ(const int *__restrict__ rlev, const unsigned int *__res
       sadslot[r] = -1;
     } else {
       succ[r] = -1;
-      sadslot[r] = found;
+      sadslot[r] = (long long)(((unsigned long long)min(v.s0, v.s1) << 32) |
+                               (unsigned int)max(v.s0, v.s1));
     }
+  }
+}
+
+// first crossing of each level (crossings are sorted by level); lstart[nlev] = n
+__global__ void k_lev_starts(const int *__restrict__ rlev, long long n, int nlev,
+                             long long *__restrict__ lstart) {
+  for (int l = blockIdx.x * blockDim.x + threadIdx.x; l <= nlev; l += gridDim.x * blockDim.x) {
+    long long lo = 0, hi = n;
+    while (lo < hi) {
+      const long long mid = (lo + hi) >> 1;
+      if (rlev[mid] < l) lo = mid + 1; else hi = mid;
+    }
+    lstart[l] = lo;
   }
 }
 
@@ -546,33 +629,42 @@ __global__ void k_sp_pred(const int *__restrict__ succ, long long N, int *__rest
 // A walk step reads the next node's successor and splitter flag (sf, one
 // 8-byte load) and writes the node's (owner, offset) pair (own, one 8-byte
 // store): two random accesses per step.  isspl keeps the flags as a plain
-// array for the scan.
+// array for the scan.  The walks run one thread per splitter: the sampled
+// crossings r = K*t by their index, the chain starts that are not sampled
+// from an appended list, so that no lane idles on a crossing that is not a
+// splitter.
 __global__ void k_sp_flag(const int *__restrict__ pred, const int *__restrict__ succ, long long N,
                           int K, int *__restrict__ isspl, int2 *__restrict__ sf,
-                          int2 *__restrict__ own) {
+                          int2 *__restrict__ own, int *__restrict__ xlist,
+                          int *__restrict__ nx) {
   for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < N;
        r += (long long)gridDim.x * blockDim.x) {
-    const int f = (r % K == 0) || pred[r] < 0;
+    const bool smp = r % K == 0;
+    const int f = smp || pred[r] < 0;
     isspl[r] = f;
     sf[r] = make_int2(succ[r], f);
     own[r] = make_int2(-1, 0);
+    if (f && !smp) xlist[atomicAdd(nx, 1)] = (int)r;
   }
 }
-__global__ void k_sp_walk(const int2 *__restrict__ sf, long long N, int2 *__restrict__ own,
-                          int *__restrict__ nexts_c, int *__restrict__ seglen_c,
-                          int *__restrict__ segmin_c, int *__restrict__ segend_c,
-                          int *__restrict__ err) {
-  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < N;
-       r += (long long)gridDim.x * blockDim.x) {
-    const int2 me = sf[r];
-    if (!me.y || own[r].x >= 0) continue;
-    int s = (int)r, v = s, k = 0, mn = s, nx = -1;
+// walks from splitters t < nsmp (crossing K*t) and xlist[t - nsmp] after
+// them, up to the next splitter
+__global__ void k_sp_walk(const int2 *__restrict__ sf, long long N, int K, long long nsmp,
+                          const int *__restrict__ xlist, const int *__restrict__ nx,
+                          int2 *__restrict__ own, int *__restrict__ nexts_c,
+                          int *__restrict__ seglen_c, int *__restrict__ segmin_c,
+                          int *__restrict__ segend_c, int *__restrict__ err) {
+  const long long total = nsmp + *nx;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int s = t < nsmp ? (int)(t * K) : xlist[t - nsmp];
+    int v = s, k = 0, mn = s, nxt = -1;
     own[s] = make_int2(s, 0);
-    int n = me.x;
+    int n = sf[s].x;
     for (long long guard = 0; guard < N; guard++) {
-      if (n < 0) { nx = -1; break; }
+      if (n < 0) { nxt = -1; break; }
       const int2 q = sf[n];  // successor and flag of the next node
-      if (q.y) { nx = n; break; }
+      if (q.y) { nxt = n; break; }
       v = n;
       n = q.x;
       k++;
@@ -580,19 +672,23 @@ __global__ void k_sp_walk(const int2 *__restrict__ sf, long long N, int2 *__rest
       mn = min(mn, v);
       if (guard == N - 1) atomicExch(err, CASL_EINVAL);
     }
-    nexts_c[s] = nx;
+    nexts_c[s] = nxt;
     seglen_c[s] = k + 1;
     segmin_c[s] = mn;
     segend_c[s] = v;
   }
 }
+// crossings on cycles that hold no splitter: every one becomes a splitter
+// (its walk ends at once, the successor being one too)
 __global__ void k_sp_unowned(long long N, const int2 *__restrict__ own, int *__restrict__ isspl,
-                             int2 *__restrict__ sf) {
+                             int2 *__restrict__ sf, int *__restrict__ xlist,
+                             int *__restrict__ nx) {
   for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < N;
        r += (long long)gridDim.x * blockDim.x)
     if (own[r].x < 0) {
       isspl[r] = 1;
       sf[r].y = 1;
+      xlist[atomicAdd(nx, 1)] = (int)r;
     }
 }
 __global__ void k_sp_compact(const int *__restrict__ isspl, const int *__restrict__ srank, long long N,
@@ -712,15 +808,6 @@ __global__ void k_gather_i(const int *__restrict__ src, const int *__restrict__ 
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x)
     dst[k] = src[idx[k]];
 }
-// the two out-crossings of each saddle bucket, lower index first
-__global__ void k_gather_slots(const HBucket *__restrict__ hb, const long long *__restrict__ sadp,
-                               int nsb, int *__restrict__ out) {
-  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nsb; b += gridDim.x * blockDim.x) {
-    const HBucket v = hb[sadp[b]];
-    out[2 * b] = min(v.s0, v.s1);
-    out[2 * b + 1] = max(v.s0, v.s1);
-  }
-}
 __global__ void k_ct_len(const int *__restrict__ startf, const int *__restrict__ clenr,
                          const int *__restrict__ cidx, long long ncr, int *__restrict__ clen) {
   for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
@@ -794,14 +881,14 @@ int recontour_dev(casl_handle *h, const double *qq) {
       return CASL_OK;
     }
   }
-  // Field memory: qa (double) + integer levels + per-chunk crossing counts;
+  // Field memory: level codes + integer levels + per-chunk crossing counts;
   // kept for the whole call.
   const long long nchunks_f = (2 * NU + EDGES_PER_THREAD - 1) / EDGES_PER_THREAD;
-  size_t need_field = (size_t)NU * 12 + (size_t)nchunks_f * 8 + (size_t)nxu * 4 +
+  size_t need_field = (size_t)NU * 6 + (size_t)nchunks_f * 8 + (size_t)nxu * 4 +
                       ((size_t)64 << 20);
   RC_TRY(ensure_scratch(h, need_field));
   Arena ar{(char *)h->sx, h->sx_bytes, 0};
-  double *qa = ar.get<double>(NU);
+  unsigned short *lc = ar.get<unsigned short>(NU);
   int *Lu = ar.get<int>(NU);
   int *ljx = ar.get<int>(nxu);
   unsigned long long *lsum = ar.get<unsigned long long>(4);
@@ -819,8 +906,14 @@ int recontour_dev(casl_handle *h, const double *qq) {
     CASL_K(k_u_colscan, (nxu * 32 + 255) / 256, 256, 0, st)(Lu, nxu, nyu, lsum);
     tr.point("u_colscan");
   }
+  // qtmp(l) = (l - 1/2) qjump - qoff with qoff = qjump*nlevm (congen.f90:156-173)
+  LevInfo li;
+  li.qjump = qjump;
+  li.qjumpi = 1.0 / qjump;
+  li.qoff = qjump * (double)h->p.nlevm;
+  li.levbeg = li.levend = 0;
   const int fb = 4096;
-  CASL_K(k_u_field, fb, 256, 0, st)(Lu, lsum, qq, qjump, have, qa, part, c);
+  CASL_K(k_u_field, fb, 256, 0, st)(Lu, lsum, qq, qjump, have, li, nullptr, lc, part, c);
   RC_TRY(check_launch(h));
   RC_TRY(fetch_err(h));
   std::vector<double> hp(2 * fb);
@@ -833,12 +926,10 @@ int recontour_dev(casl_handle *h, const double *qq) {
   }
   tr.point("field");
   // --- 2. levels (congen.f90:156-173) ----------------------------------------
-  LevInfo li;
-  li.qjump = qjump;
-  li.qjumpi = 1.0 / qjump;
-  li.qoff = qjump * (double)h->p.nlevm;
   li.levbeg = (int)((li.qoff + qamin) * li.qjumpi + 0.5) + 1;
   li.levend = (int)((li.qoff + qamax) * li.qjumpi + 0.5);
+  // the level codes hold 0..65535: levels must lie inside
+  if (li.levbeg <= li.levend && (li.levbeg < 1 || li.levend > 65534)) return CASL_ECAPACITY;
   auto set_empty = [&]() -> int {
     h->nq = h->nptq = 0;
     int z[2] = {0, 0};
@@ -858,7 +949,7 @@ int recontour_dev(casl_handle *h, const double *qq) {
   int *dtot = ar.get<int>(16);
   if (ar.failed) return CASL_ENOMEM;
   const dim3 tgrid(nxu / CR_CB, nyu / CR_RB);
-  CASL_K(k_cr_tile<false>, tgrid, 256, 0, st)(qa, li, nxu, nyu, ccnt, nullptr, nullptr, nullptr);
+  CASL_K(k_cr_tile<false>, tgrid, 256, 0, st)(lc, li, nxu, nyu, ccnt, nullptr, nullptr, nullptr);
   tr.point("cr_count");
   exclusive_scan<int>(st, ccnt, coffs, nchunks, tmpi, dtot);
   int ncr_i = 0;
@@ -890,7 +981,7 @@ int recontour_dev(casl_handle *h, const double *qq) {
   void *sort_tmp = ar2.get<char>(sort_bytes + 16);
   if (ar2.failed) return CASL_ENOMEM;
   tr.point("cr_alloc");
-  CASL_K(k_cr_tile<true>, tgrid, 256, 0, st)(qa, li, nxu, nyu, nullptr, coffs, redge, rlev);
+  CASL_K(k_cr_tile<true>, tgrid, 256, 0, st)(lc, li, nxu, nyu, nullptr, coffs, redge, rlev);
   tr.point("cr_emit");
   CASL_CUDA_TRY(cub::DeviceRadixSort::SortPairs(sort_tmp, sort_bytes, rlev, rlev2, redge, redge2,
                                                 (int)ncr, 0, endbit, st));
@@ -900,23 +991,55 @@ int recontour_dev(casl_handle *h, const double *qq) {
   double *xcr = ar2.get<double>(ncr), *ycr = ar2.get<double>(ncr);
   unsigned int *kib = ar2.get<unsigned int>(ncr), *kob = ar2.get<unsigned int>(ncr);
   if (ar2.failed) return CASL_ENOMEM;
-  CASL_K(k_cr_geom, gsz(ncr), 256, 0, st)(qa, redge, rlev, ncr, li, c, xcr, ycr, kib, kob);
+  const UField uf{have ? Lu : nullptr, lsum, qq, qjump, have};
+  CASL_K(k_cr_geom, gsz(ncr), 256, 0, st)(uf, redge, rlev, ncr, li, c, xcr, ycr, kib, kob);
   RC_TRY(check_launch(h));
 
   tr.point("crossings");
   // --- 4. box tables: hash (level, box) -> two out-crossing slots ------------
+  // Levels go through the table in batches of about HB_BATCH crossings, so
+  // that the table (16 bytes per bucket, load <= 1/2) stays in L2 while the
+  // batch's inserts and look-ups run; the keys carry the level, so a batch of
+  // several levels shares one table.
+  constexpr long long HB_BATCH = 1 << 20;
+  long long *lstart = ar2.get<long long>(nlev + 1);
+  if (ar2.failed) return CASL_ENOMEM;
+  std::vector<long long> hl(nlev + 1);
+  CASL_K(k_lev_starts, 1, 128, 0, st)(rlev, ncr, nlev, lstart);
+  CASL_CUDA_TRY(cudaMemcpyAsync(hl.data(), lstart, (nlev + 1) * sizeof(long long),
+                                cudaMemcpyDeviceToHost, st));
+  CASL_CUDA_TRY(cudaStreamSynchronize(st));
+  std::vector<std::pair<long long, long long>> batches;  // [r0, r1)
+  for (int l = 0; l < nlev;) {
+    int l2 = l + 1;
+    while (l2 < nlev && hl[l2 + 1] - hl[l] <= HB_BATCH) l2++;
+    batches.push_back({hl[l], hl[l2]});
+    l = l2;
+  }
+  long long bmax = 0;
+  for (auto &b : batches) bmax = std::max(bmax, b.second - b.first);
   unsigned long long cap = 1;
-  while (cap < (unsigned long long)(2 * ncr)) cap <<= 1;
+  while (cap < (unsigned long long)(2 * bmax)) cap <<= 1;
   HBucket *hb = ar2.get<HBucket>(cap);
   int *succ = ar2.get<int>(ncr);
   long long *sadslot = ar2.get<long long>(ncr);
   if (ar2.failed) return CASL_ENOMEM;
-  CASL_CUDA_TRY(cudaMemsetAsync(hb, 0xff, cap * sizeof(HBucket), st));  // empty key, slots -1
-  CASL_K(k_h_insert, gsz(ncr), 256, 0, st)(rlev, kob, ncr, hb, cap - 1, &h->scal->error);
-  CASL_K(k_h_succ, gsz(ncr), 256, 0, st)(rlev, kib, ncr, hb, cap - 1, succ, sadslot,
-                                     &h->scal->error);
+  for (auto &b : batches) {
+    const long long nb = b.second - b.first;
+    if (nb <= 0) continue;
+    unsigned long long cb = 1;
+    while (cb < (unsigned long long)(2 * nb)) cb <<= 1;
+    CASL_CUDA_TRY(cudaMemsetAsync(hb, 0xff, cb * sizeof(HBucket), st));  // empty key, slots -1
+    CASL_K(k_h_insert, gsz(nb), 256, 0, st)(rlev + b.first, kob + b.first, nb, (int)b.first, hb,
+                                           cb - 1, &h->scal->error);
+    CASL_K(k_h_succ, gsz(nb), 256, 0, st)(rlev + b.first, kib + b.first, nb, hb, cb - 1,
+                                         succ + b.first, sadslot + b.first, &h->scal->error);
+  }
   RC_TRY(check_launch(h));
   RC_TRY(fetch_err(h));
+  if (tr.on)
+    fprintf(stderr, "[casl trace] hash: %zu level batches, table %llu buckets\n", batches.size(),
+            cap);
 
   tr.point("hash");
   // --- 5. list ranking over crossings (splitters) ------------------------------
@@ -930,12 +1053,18 @@ int recontour_dev(casl_handle *h, const double *qq) {
   int g = gsz(ncr);
   CASL_CUDA_TRY(cudaMemsetAsync(pred, 0xff, ncr * sizeof(int), st));
   CASL_K(k_sp_pred, g, 256, 0, st)(succ, ncr, pred);
-  CASL_K(k_sp_flag, g, 256, 0, st)(pred, succ, ncr, 16, isspl, sf, own);
-  CASL_K(k_sp_walk, g, 256, 0, st)(sf, ncr, own, nexts_c, seglen_c, segmin_c, segend_c,
-                                   &h->scal->error);
-  CASL_K(k_sp_unowned, g, 256, 0, st)(ncr, own, isspl, sf);
-  CASL_K(k_sp_walk, g, 256, 0, st)(sf, ncr, own, nexts_c, seglen_c, segmin_c, segend_c,
-                                   &h->scal->error);
+  // term and val are written only by the expansion at the end: until then
+  // they hold the lists of splitters that are not sampled crossings
+  const int K = 16;
+  const long long nsmp = (ncr + K - 1) / K;
+  int *xl1 = term, *xl2 = val, *nx1 = dtot + 10, *nx2 = dtot + 11;
+  CASL_CUDA_TRY(cudaMemsetAsync(nx1, 0, 2 * sizeof(int), st));
+  CASL_K(k_sp_flag, g, 256, 0, st)(pred, succ, ncr, K, isspl, sf, own, xl1, nx1);
+  CASL_K(k_sp_walk, gsz(nsmp), 256, 0, st)(sf, ncr, K, nsmp, xl1, nx1, own, nexts_c, seglen_c,
+                                           segmin_c, segend_c, &h->scal->error);
+  CASL_K(k_sp_unowned, g, 256, 0, st)(ncr, own, isspl, sf, xl2, nx2);
+  CASL_K(k_sp_walk, g, 256, 0, st)(sf, ncr, K, 0, xl2, nx2, own, nexts_c, seglen_c, segmin_c,
+                                   segend_c, &h->scal->error);
   exclusive_scan<int>(st, isspl, srank, ncr, tmpi2, dtot + 6);
   int S = 0;
   CASL_CUDA_TRY(cudaMemcpyAsync(&S, dtot + 6, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -1021,15 +1150,11 @@ int recontour_dev(casl_handle *h, const double *qq) {
     std::sort(sad_p.begin(), sad_p.end());
     sad_p.erase(std::unique(sad_p.begin(), sad_p.end()), sad_p.end());
     int nsb = (int)sad_p.size();
+    // each saddle box is named by its two out-crossings, lower index first
     std::vector<int> slot2(2 * nsb);
-    {
-      long long *d_sadp = ar2.get<long long>(nsb);
-      int *d_slot2 = ar2.get<int>(2 * nsb);
-      if (ar2.failed) return CASL_ENOMEM;
-      CASL_CUDA_TRY(cudaMemcpyAsync(d_sadp, sad_p.data(), nsb * sizeof(long long), cudaMemcpyHostToDevice, st));
-      CASL_K(k_gather_slots, gsz(nsb), 256, 0, st)(hb, d_sadp, nsb, d_slot2);
-      CASL_CUDA_TRY(cudaMemcpyAsync(slot2.data(), d_slot2, 2 * nsb * sizeof(int), cudaMemcpyDeviceToHost, st));
-      CASL_CUDA_TRY(cudaStreamSynchronize(st));
+    for (int b = 0; b < nsb; b++) {
+      slot2[2 * b] = (int)((unsigned long long)sad_p[b] >> 32);
+      slot2[2 * b + 1] = (int)((unsigned long long)sad_p[b] & 0xffffffffull);
     }
     // chain starts (the saddle out-crossings) and their ends, lengths, minima
     int nch = 2 * nsb;
@@ -1277,7 +1402,8 @@ extern "C" int casl_genfg(casl_handle *h, int ix1v, int nxv, int iy1v, int nyv, 
                                               ljx, c, &h->scal->error);
   CASL_K(k_u_lbot, 1, 1024, 0, st)(ljx, Lu, nxu, nyu);
   CASL_K(k_u_colscan, (nxu * 32 + 255) / 256, 256, 0, st)(Lu, nxu, nyu, lsum);
-  CASL_K(k_u_field, 4096, 256, 0, st)(Lu, lsum, h->qr, h->qjump, 1, qa, part, c);
+  LevInfo lq{0, 0, h->qjump, 0.0, 1.0};
+  CASL_K(k_u_field, 4096, 256, 0, st)(Lu, lsum, h->qr, h->qjump, 1, lq, qa, nullptr, part, c);
   CASL_K(k_gf_gather, gsz(m), 256, 0, st)(qa, nxu, nyu, ix1v - 1, nxv, iy1v - 1, nyv, stride, img);
   RC_TRY(check_launch(h));
   CASL_CUDA_TRY(cudaMemcpyAsync(out, img, (size_t)m * sizeof(float), cudaMemcpyDeviceToHost, st));
