@@ -88,6 +88,7 @@ SIGNATURES = {
     "casl_launch_count": (C.c_int, [C.POINTER(C.c_longlong)]),
     "casl_profile": (C.c_int, [C.c_void_p, C.c_int]),
     "casl_profile_read": (C.c_int, [C.c_void_p, _dp, C.POINTER(C.c_longlong), _dp]),
+    "casl_kernel_times": (C.c_int, [C.c_int, C.c_char_p, C.c_longlong]),
     "casl_io_append_synopsis": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_double, C.c_double]),
     "casl_io_append_ene": (C.c_int, [C.c_char_p, C.c_double, C.c_double, C.c_double]),
     "casl_io_append_norms": (C.c_int, [C.c_char_p, C.c_double, C.c_double]),
@@ -307,6 +308,15 @@ class CaslGPU:
         self._check(self.lib.casl_profile_read(self.h, C.byref(ms), C.byref(n), C.byref(b)),
                     "casl_profile_read")
         return ms.value, n.value, b.value
+
+    def kernel_times(self, mode: int) -> str:
+        """Per-launch timing of every kernel (process-wide): 1 on, 0 off,
+        2 returns the report (launches, total ms, mean us per kernel) and
+        starts a new tally."""
+        buf = C.create_string_buffer(1 << 16) if mode == 2 else None
+        self._check(self.lib.casl_kernel_times(mode, buf, len(buf) if buf else 0),
+                    "casl_kernel_times")
+        return buf.value.decode() if buf else ""
 
     def diagnostics(self):
         out = np.zeros(4)

@@ -9,6 +9,9 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
+#include <map>
+#include <string>
 #include <vector>
 
 #include "common.cuh"
@@ -21,6 +24,38 @@ using namespace casl;
 namespace casl {
 
 unsigned long long g_launches = 0;
+
+// ---- per-launch timing ------------------------------------------------------
+namespace {
+constexpr int KT_MAX = 1 << 16;  // launches recorded between two reports
+struct KTime {
+  bool on = false;
+  cudaEvent_t *ev = nullptr;  // 2 * KT_MAX, created when switched on
+  const char **name = nullptr;
+  int n = 0, open = -1;
+  cudaStream_t st = 0;
+};
+KTime g_kt;
+}  // namespace
+
+bool kt_begin(const char *name, dim3, dim3, size_t, cudaStream_t st) {
+  ++g_launches;
+  if (g_kt.on && g_kt.n < KT_MAX) {
+    g_kt.open = g_kt.n;
+    g_kt.st = st;
+    g_kt.name[g_kt.n] = name;
+    cudaEventRecord(g_kt.ev[2 * g_kt.n], st);
+  }
+  return true;
+}
+bool kt_end() {
+  if (g_kt.open >= 0) {
+    cudaEventRecord(g_kt.ev[2 * g_kt.open + 1], g_kt.st);
+    g_kt.n = g_kt.open + 1;
+    g_kt.open = -1;
+  }
+  return false;
+}
 
 int set_cuda_error(casl_handle *h, cudaError_t e) {
   if (h) h->last_cuda = (int)e;
@@ -202,18 +237,37 @@ struct LoadAdvect {
   }
 };
 
-// Store of the source terms after ptospc pass B (evolution.f90:466-487):
-// b = 0 -> sqd with damping and the integrating factor, b = 1 -> sqs.
+// Store of the source terms after ptospc pass B (evolution.f90:466-487),
+// b = 0 -> sqd with damping and the integrating factor, b = 1 -> sqs, with
+// the RK4 update of the spectral fields that uses them (evolution.f90:
+// 212-311, the qs/qd halves of each stage) done in the same store: b = 1
+// updates qs, qsi, qsf from sqs; b = 0 updates qd, qdi, qdf (and emq at
+// stage 3) from sqd.  The sources themselves never go to memory.
 struct StoreSource {
-  __host__ double bytes() const { return 8.0 + 0.5 * 24.0; }  // sqd reads qq, pp, epq
-  double *sqd, *sqs;
+  __host__ double bytes() const { return 0.5 * 24.0 + 0.5 * (stage == 1 ? 40.0 : 32.0); }
   const double *qq, *pp, *epq;
+  double *qs, *qd, *qsi, *qsf, *qdi, *qdf, *emq;
+  const Scalars *sc;
   double rekman, kdsq, therm;
-  int heating, friction, lev, n;
+  int heating, friction, lev, stage, n;
   __device__ __forceinline__ void operator()(int b, int v /*ky*/, int k /*kx*/, double x) const {
     long long idx = (long long)v * n + k;
     if (b == 1) {
-      sqs[idx] = x;
+      const double a = x;
+      if (stage == 1) {
+        const double si = qs[idx];
+        qsi[idx] = si;
+        qs[idx] = si + sc->dt2 * a;
+        qsf[idx] = si + sc->dt6 * a;
+      } else if (stage == 2) {
+        qs[idx] = qsi[idx] + sc->dt2 * a;
+        qsf[idx] = qsf[idx] + sc->dt3 * a;
+      } else if (stage == 3) {
+        qs[idx] = qsi[idx] + sc->dt * a;
+        qsf[idx] = qsf[idx] + sc->dt3 * a;
+      } else {
+        qs[idx] = qsf[idx] + sc->dt6 * a;
+      }
       return;
     }
     double t;
@@ -229,7 +283,66 @@ struct StoreSource {
       t = epq[idx] * t;
     else if (lev == 2)
       t = epq[idx] * epq[idx] * t;
-    sqd[idx] = t;
+    const double bb = t;
+    if (stage == 1) {
+      const double di = qd[idx];
+      qdi[idx] = di;
+      qd[idx] = emq[idx] * (di + sc->dt2 * bb);
+      qdf[idx] = di + sc->dt6 * bb;
+    } else if (stage == 2) {
+      qd[idx] = emq[idx] * (qdi[idx] + sc->dt2 * bb);
+      qdf[idx] = qdf[idx] + sc->dt3 * bb;
+    } else if (stage == 3) {
+      double e = emq[idx];
+      e = e * e;
+      emq[idx] = e;
+      qd[idx] = e * (qdi[idx] + sc->dt * bb);
+      qdf[idx] = qdf[idx] + sc->dt3 * bb;
+    } else {
+      qd[idx] = emq[idx] * (qdf[idx] + sc->dt6 * bb);
+    }
+  }
+};
+
+// Last store of con2grid's forward transform with the filter combination
+// (evolution.f90:507-514) done in place of a separate pass: the coarse
+// spectral PV qc is kept, qq = flo*(qs - qc) + qc + qd and pp = green*qq
+// formed, and with RESET qs = qq, qd = fhi*(qq - qc).
+template <bool RESET>
+struct StoreCombine {
+  __host__ double bytes() const { return RESET ? 80.0 : 56.0; }
+  double *qs, *qd, *qc, *qq, *pp;
+  const double *flo, *fhi, *green;
+  int n;
+  __device__ __forceinline__ void one(long long i, double c) const {
+    const double s = qs[i], d = qd[i];
+    const double q = flo[i] * (s - c) + c + d;
+    qc[i] = c;
+    qq[i] = q;
+    pp[i] = green[i] * q;
+    if (RESET) {
+      qs[i] = q;
+      qd[i] = fhi[i] * (q - c);
+    }
+  }
+  __device__ __forceinline__ void operator()(int, int v, int k, double x) const {
+    one((long long)v * n + k, x);
+  }
+  __device__ __forceinline__ void pair(int, int v, int k, double2 x) const {
+    const long long i = (long long)v * n + k;
+    const double2 s = *reinterpret_cast<const double2 *>(qs + i);
+    const double2 d = *reinterpret_cast<const double2 *>(qd + i);
+    const double2 f = *reinterpret_cast<const double2 *>(flo + i);
+    const double2 g = *reinterpret_cast<const double2 *>(green + i);
+    const double q0 = f.x * (s.x - x.x) + x.x + d.x, q1 = f.y * (s.y - x.y) + x.y + d.y;
+    *reinterpret_cast<double2 *>(qc + i) = x;
+    *reinterpret_cast<double2 *>(qq + i) = make_double2(q0, q1);
+    *reinterpret_cast<double2 *>(pp + i) = make_double2(g.x * q0, g.y * q1);
+    if (RESET) {
+      const double2 h = *reinterpret_cast<const double2 *>(fhi + i);
+      *reinterpret_cast<double2 *>(qs + i) = make_double2(q0, q1);
+      *reinterpret_cast<double2 *>(qd + i) = make_double2(h.x * (q0 - x.x), h.y * (q1 - x.y));
+    }
   }
 };
 
@@ -272,14 +385,47 @@ struct LoadVort {
 // ---------------------------------------------------------------------------
 // con2grid (contours.f90:173-346)
 // ---------------------------------------------------------------------------
+// Sparse con2grid.  The coarse cell is C(cx, cy) = sum_b w_b G(4cx-3+b, cy)
+// with G(fx, cy) = sum_a w_a L(fx, 4cy-3+a) the 7-tap of fine column fx at
+// coarse row cy, L(fx, r) = lbot(fx) + sum_{r' <= r} J(fx, r') (rows and
+// columns periodic, 0-based).  A crossing s at fine row r >= 1 adds to G(fx,
+// cy) s times the weight of the stencil rows at or above r: 16 for every
+// cy >= cf = (r+6)/4 (kept as a jump 16s at cf, summed up the column
+// later), a partial tail of the weights for the (at most two) cy between,
+// and for cy = 0, whose stencil wraps to the top rows, 6 for every crossing
+// below the top seven rows (formed from the column total later) with the
+// differences at rows 1..3 and nf-6..nf-1 added here.  DP(fx, cy) holds the
+// jumps (.x) and the direct terms (.y); integer sums, so the result is the
+// dense scan's to the bit in any order.
+__device__ __forceinline__ int c2g_tail(int k) {  // w_k + ... + w_6 for k = 1..6
+  return k == 1 ? 15 : (k == 2 ? 13 : (k == 3 ? 10 : (k == 4 ? 6 : (k == 5 ? 3 : 1))));
+}
+__device__ __forceinline__ void c2g_sparse_add(int2 *__restrict__ DP, int fx, int r, int s, int n,
+                                               int nf) {
+  int2 *col = DP + (long long)fx * n;
+  const int cf = (r + 6) >> 2;
+  if (cf <= n - 1) atomicAdd(&col[cf].x, 16 * s);
+  const int lo = max(1, r >> 2), hi = min(cf - 1, n - 1);
+  for (int cy = lo; cy <= hi; cy++) atomicAdd(&col[cy].y, s * c2g_tail(r - 4 * cy + 3));
+  int w0 = 0;
+  if (r <= 3)
+    w0 = r == 1 ? 6 : (r == 2 ? 3 : 1);
+  else if (r >= nf - 6)
+    w0 = r <= nf - 3 ? 6 : (r == nf - 2 ? 5 : 3);
+  if (w0) atomicAdd(&col[0].y, s * w0);
+}
+
 // Per segment (i, nextq(i)): x fine-grid-line crossings and the crossing of
-// y = ymin, counted as +-1 PV jumps.  The FP64 expressions are the
-// reference's, evaluated in its order without FMA, so every crossing lands
-// in the same fine cell.
+// y = ymin, counted as +-1 PV jumps (contours.f90:232-270): J += sgn at
+// each (SPARSE: the coarse-row terms above into DP), ljx the bottom-boundary
+// jumps.  The FP64 expressions are the reference's, evaluated in its order
+// without FMA, so every crossing lands in the same fine cell.
+template <bool SPARSE>
 __global__ void k_c2g_scatter(const double *__restrict__ xq, const double *__restrict__ yq,
                               const int *__restrict__ nextq, const Scalars *__restrict__ s,
-                              int *__restrict__ J, int *__restrict__ ljx, Consts c,
-                              int *__restrict__ err, unsigned long long *__restrict__ csum) {
+                              int *__restrict__ J, int2 *__restrict__ DP, int *__restrict__ ljx,
+                              Consts c, int *__restrict__ err,
+                              unsigned long long *__restrict__ csum) {
   // the coarsening that follows accumulates the coarse-cell sum here
   if (blockIdx.x == 0 && threadIdx.x == 0) *csum = 0;
   int npt = s->nptq;
@@ -319,7 +465,12 @@ __global__ void k_c2g_scatter(const double *__restrict__ xq, const double *__res
         double px0 = (x2 - c.ellx * f_dint(x2 * c.hlxi)) / dx;
         double y2 = yi + px0 * dy;
         int iy = 2 + f_int(c.glyfi * (y2 - c.elly * f_dint(y2 * c.hlyi) - c.ymin));
-        if (iy >= 2 && iy <= c.nyf) atomicAdd(&J[(long long)(ix - 1) * c.nyf + (iy - 1)], sgn);
+        if (iy >= 2 && iy <= c.nyf) {
+          if (SPARSE)
+            c2g_sparse_add(DP, ix - 1, iy - 1, sgn, c.nx, c.nyf);
+          else
+            atomicAdd(&J[(long long)(ix - 1) * c.nyf + (iy - 1)], sgn);
+        }
       }
     }
   }
@@ -424,66 +575,55 @@ __global__ void k_c2g_coarsen(const int *__restrict__ L, int *__restrict__ C,
 }
 
 
-// Column scan + 7x7 coarsening in one pass (the two kernels above, fused;
-// the fine grid is only read, the level grid never goes to memory).  A CTA
-// owns CW = 7 coarse columns and scans the 4*CW+3 = 31 fine columns they
-// need, one warp per column, RPS = 32U fine rows per step with the next
-// step's rows already in flight (register prefetch).  The level rows go to
-// a shared ring of RPS+8 rows; each step then forms its RPS/4 coarse rows as
-// 7-tap vertical sums per fine column (all threads, conflict-free) followed
-// by 7-tap horizontal sums.  Coarse row 1 needs the last fine rows (periodic
-// wrap), so it is formed after the last step from the saved first rows.
-// Requires nf % RPS == 0.
+// Sparse con2grid, second half: per fine column an inclusive scan of the
+// jumps up the coarse rows plus the direct terms gives G(fx, cy) (with
+// 16*lbot(fx)); G(fx, 0) takes 6/16 of the column's jump total.  Then the
+// 7-tap along x.  A CTA owns CW = 7 coarse columns and their 4*CW+3 = 31
+// fine columns, one warp per column, RPS = 32U coarse rows per step with
+// the next step's rows in flight; the rows of G pass through shared memory.
+// Requires n % RPS == 0.
 #define C2G_CW 7
 #define C2G_FC (4 * C2G_CW + 3)
 template <int U>
-constexpr size_t c2g_fused_smem() {
-  return 32 * sizeof(long long) + (size_t)(32 * U + 8 + 4 + 8 * U) * C2G_FC * sizeof(int);
-}
-template <int U>
-__global__ void __launch_bounds__(1024) k_c2g_fused(const int *__restrict__ J,
-                                                    const int *__restrict__ ljx,
-                                                    int *__restrict__ C,
-                                                    unsigned long long *__restrict__ csum, int n,
-                                                    int nf) {
-  constexpr int RPS = 32 * U, RING = RPS + 8, CR = RPS / 4;
-  // dynamic shared memory (c2g_fused_smem<U>() bytes): the ring of level
-  // rows, the first rows, the vertical sums, the block reduction
-  extern __shared__ long long c2g_dyn[];
-  long long *red = c2g_dyn;
-  int (*ring)[C2G_FC] = reinterpret_cast<int (*)[C2G_FC]>(c2g_dyn + 32);
-  int (*first)[C2G_FC] = ring + RING;
-  int (*vsum)[C2G_FC] = first + 4;
+__global__ void __launch_bounds__(1024) k_c2g_sparse_sum(const int2 *__restrict__ DP,
+                                                         const int *__restrict__ ljx,
+                                                         int *__restrict__ C,
+                                                         unsigned long long *__restrict__ csum,
+                                                         int n, int nf) {
+  constexpr int RPS = 32 * U;
+  __shared__ int G[RPS][C2G_FC + 2];  // row length 33: conflict-free both ways
+  __shared__ int G0[C2G_FC];
+  __shared__ long long red[32];
   const int w7[7] = {1, 2, 3, 4, 3, 2, 1};
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int cx0 = blockIdx.x * C2G_CW;  // first coarse column (0-based)
-  int col = 4 * cx0 - 3 + warp;         // this warp's fine column (0-based), wrapped
+  const int cx0 = blockIdx.x * C2G_CW;
+  int col = 4 * cx0 - 3 + warp;  // this warp's fine column (0-based), wrapped
   if (col < 0) col += nf;
   if (col >= nf) col -= nf;
-  const int *cp = J + (long long)col * nf + lane;
-  const int nsteps = nf / RPS;
-  int v[U];
+  const int2 *cp = DP + (long long)col * n + lane;
+  const int nsteps = n / RPS;
+  int2 v[U];
   if (warp < C2G_FC) {
 #pragma unroll
     for (int u = 0; u < U; u++) v[u] = __ldcs(cp + u * 32);
   }
-  // row 0 of the column starts from the exclusive prefix of the bottom
-  // jumps along x (qbot, contours.f90:255-269), summed here by the warp
-  int carry = 0;
+  // 16 * lbot(col): the exclusive prefix of the bottom jumps (contours.f90:255-269)
+  int lb = 0;
   if (warp < C2G_FC) {
-    for (int i = lane; i < col; i += 32) carry += ljx[i];
-    for (int o = 16; o > 0; o >>= 1) carry += __shfl_xor_sync(0xffffffffu, carry, o);
+    for (int i = lane; i < col; i += 32) lb += ljx[i];
+    for (int o = 16; o > 0; o >>= 1) lb += __shfl_xor_sync(0xffffffffu, lb, o);
   }
+  const int lb16 = 16 * lb;
+  int carry = 0, p0 = 0;
   long long local = 0;
   for (int s = 0; s < nsteps; s++) {
     if (warp < C2G_FC) {
 #pragma unroll
       for (int u = 0; u < U; u++) {
-        int x = warp_incl_scan(v[u]) + carry;
+        const int x = warp_incl_scan(v[u].x) + carry;
         carry = __shfl_sync(0xffffffffu, x, 31);
-        int r = s * RPS + u * 32 + lane;  // 0-based fine row
-        ring[r % RING][warp] = x;
-        if (r < 4) first[r][warp] = x;
+        G[u * 32 + lane][warp] = lb16 + v[u].y + x;
+        if (s == 0 && u == 0 && lane == 0) p0 = v[0].y;
       }
       if (s + 1 < nsteps) {
 #pragma unroll
@@ -491,48 +631,28 @@ __global__ void __launch_bounds__(1024) k_c2g_fused(const int *__restrict__ J,
       }
     }
     __syncthreads();
-    // vertical: coarse row iy (1-based) uses fine rows 4iy-7..4iy-1 (0-based)
-    for (int t = threadIdx.x; t < CR * 32; t += blockDim.x) {
-      int iyl = t >> 5, fc = t & 31;
-      int iy = s * CR + iyl + 1;
-      if (fc < C2G_FC && iy > 1) {
+    for (int t = threadIdx.x; t < C2G_CW * RPS; t += blockDim.x) {
+      const int cxl = t / RPS, rl = t % RPS;
+      const int cx = cx0 + cxl, cy = s * RPS + rl;
+      if (cx < n && cy > 0) {
         int acc = 0;
 #pragma unroll
-        for (int a = 0; a < 7; a++) acc += w7[a] * ring[(4 * iy - 7 + a) % RING][fc];
-        vsum[iyl][fc] = acc;
-      }
-    }
-    __syncthreads();
-    for (int t = threadIdx.x; t < C2G_CW * CR; t += blockDim.x) {
-      int cxl = t / CR, iyl = t % CR;
-      int cx = cx0 + cxl, iy = s * CR + iyl + 1;
-      if (cx < n && iy > 1) {
-        int acc = 0;
-#pragma unroll
-        for (int b = 0; b < 7; b++) acc += w7[b] * vsum[iyl][4 * cxl + b];
-        C[(long long)cx * n + (iy - 1)] = acc;
+        for (int b = 0; b < 7; b++) acc += w7[b] * G[rl][4 * cxl + b];
+        C[(long long)cx * n + cy] = acc;
         local += acc;
       }
     }
+    __syncthreads();
   }
-  __syncthreads();
-  // coarse row 1: fine rows nf-3..nf-1 and 0..3 (0-based)
-  if (threadIdx.x < C2G_FC) {
-    int fc = threadIdx.x, acc = 0;
-#pragma unroll
-    for (int a = 0; a < 7; a++) {
-      int r = a - 3;
-      acc += w7[a] * (r < 0 ? ring[(r + nf) % RING][fc] : first[r][fc]);
-    }
-    vsum[0][fc] = acc;
-  }
+  // coarse row 0: its stencil wraps to the top rows
+  if (warp < C2G_FC && lane == 0) G0[warp] = lb16 + p0 + 6 * (carry / 16);
   __syncthreads();
   if (threadIdx.x < C2G_CW) {
-    int cx = cx0 + threadIdx.x;
+    const int cx = cx0 + threadIdx.x;
     if (cx < n) {
       int acc = 0;
 #pragma unroll
-      for (int b = 0; b < 7; b++) acc += w7[b] * vsum[0][4 * threadIdx.x + b];
+      for (int b = 0; b < 7; b++) acc += w7[b] * G0[4 * threadIdx.x + b];
       C[(long long)cx * n] = acc;
       local += acc;
     }
@@ -575,41 +695,46 @@ static int grid_for(long long work, int block = 256) {
 
 int con2grid_dev(casl_handle *h, bool want_levels) {
   const Consts &c = h->c;
+  int *err = &h->scal->error;
+  unsigned long long *csum = (unsigned long long *)&h->scal->csum;
+  const int n = h->n;
+  const int U = n % 128 == 0 ? 4 : (n % 64 == 0 ? 2 : (n % 32 == 0 ? 1 : 0));
+  if (!want_levels && c.nxf == c.nyf && U > 0) {
+    // sparse: jumps and direct terms per (fine column, coarse row), in the
+    // first half of the fine-grid buffer
+    int2 *DP = reinterpret_cast<int2 *>(h->fineJ);
+    CASL_CUDA_TRY(cudaMemsetAsync(DP, 0, (size_t)c.nxf * n * sizeof(int2), h->stream));
+    CASL_CUDA_TRY(cudaMemsetAsync(h->ljx, 0, (size_t)c.nxf * sizeof(int), h->stream));
+    if (h->nptq > 0) {
+      CASL_K(k_c2g_scatter<true>, grid_for(h->nptq), 256, 0, h->stream)(
+          h->xq, h->yq, h->nextq, h->scal, nullptr, DP, h->ljx, c, err, csum);
+    } else {
+      CASL_CUDA_TRY(cudaMemsetAsync(csum, 0, sizeof(unsigned long long), h->stream));
+    }
+    const int nblk = (n + C2G_CW - 1) / C2G_CW;
+    if (U == 4)
+      CASL_K(k_c2g_sparse_sum<4>, nblk, 1024, 0, h->stream)(DP, h->ljx, h->coarseC, csum, n, c.nxf);
+    else if (U == 2)
+      CASL_K(k_c2g_sparse_sum<2>, nblk, 1024, 0, h->stream)(DP, h->ljx, h->coarseC, csum, n, c.nxf);
+    else
+      CASL_K(k_c2g_sparse_sum<1>, nblk, 1024, 0, h->stream)(DP, h->ljx, h->coarseC, csum, n, c.nxf);
+    return check_launch(h);
+  }
+  // the fine-grid levels themselves are wanted: crossings onto the fine
+  // grid, bottom row, scan in place, then coarsen
   size_t fine = (size_t)c.nxf * c.nyf;
   CASL_CUDA_TRY(cudaMemsetAsync(h->fineJ, 0, fine * sizeof(int), h->stream));
   CASL_CUDA_TRY(cudaMemsetAsync(h->ljx, 0, (size_t)c.nxf * sizeof(int), h->stream));
-  int *err = &h->scal->error;
-  unsigned long long *csum = (unsigned long long *)&h->scal->csum;
   if (h->nptq > 0) {
-    CASL_K(k_c2g_scatter, grid_for(h->nptq), 256, 0, h->stream)(h->xq, h->yq, h->nextq, h->scal,
-                                                              h->fineJ, h->ljx, c, err, csum);
+    CASL_K(k_c2g_scatter<false>, grid_for(h->nptq), 256, 0, h->stream)(
+        h->xq, h->yq, h->nextq, h->scal, h->fineJ, nullptr, h->ljx, c, err, csum);
   } else {
     CASL_CUDA_TRY(cudaMemsetAsync(csum, 0, sizeof(unsigned long long), h->stream));
   }
-  int nblk = (h->n + C2G_CW - 1) / C2G_CW;
-  if (!want_levels && c.nxf == c.nyf && c.nxf % 512 == 0) {
-    static bool attr16 = false;  // one attribute call for the >48 KB variant
-    if (!attr16) {
-      cudaFuncSetAttribute(k_c2g_fused<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)c2g_fused_smem<16>());
-      attr16 = true;
-    }
-    CASL_K(k_c2g_fused<16>, nblk, 1024, c2g_fused_smem<16>(), h->stream)(h->fineJ, h->ljx, h->coarseC,
-                                                                       csum, h->n, c.nxf);
-  } else if (!want_levels && c.nxf == c.nyf && c.nxf % 256 == 0) {
-    CASL_K(k_c2g_fused<8>, nblk, 1024, c2g_fused_smem<8>(), h->stream)(h->fineJ, h->ljx, h->coarseC,
-                                                                     csum, h->n, c.nxf);
-  } else if (!want_levels && c.nxf == c.nyf && c.nxf % 128 == 0) {
-    CASL_K(k_c2g_fused<4>, nblk, 1024, c2g_fused_smem<4>(), h->stream)(h->fineJ, h->ljx, h->coarseC,
-                                                                     csum, h->n, c.nxf);
-  } else {
-    // the fine-grid levels themselves are wanted: bottom row, scan in place,
-    // then coarsen
-    CASL_K(k_c2g_lbot, 1, 1024, 0, h->stream)(h->ljx, h->fineJ, c.nxf, c.nyf);
-    CASL_K(k_c2g_colscan, (c.nxf * 32 + 255) / 256, 256, 0, h->stream)(h->fineJ, c.nxf, c.nyf);
-    CASL_K(k_c2g_coarsen, grid_for((long long)h->n * h->n), 256, 0, h->stream)(
-        h->fineJ, h->coarseC, csum, h->n, c.nxf);
-  }
+  CASL_K(k_c2g_lbot, 1, 1024, 0, h->stream)(h->ljx, h->fineJ, c.nxf, c.nyf);
+  CASL_K(k_c2g_colscan, (c.nxf * 32 + 255) / 256, 256, 0, h->stream)(h->fineJ, c.nxf, c.nyf);
+  CASL_K(k_c2g_coarsen, grid_for((long long)h->n * h->n), 256, 0, h->stream)(
+      h->fineJ, h->coarseC, csum, h->n, c.nxf);
   return check_launch(h);
 }
 
@@ -745,43 +870,6 @@ __global__ void k_combine(double *__restrict__ qs, double *__restrict__ qd,
   }
 }
 
-template <int STAGE>
-__global__ void k_spec_rk(double *__restrict__ qs, double *__restrict__ qd,
-                          double *__restrict__ qsi, double *__restrict__ qsf,
-                          double *__restrict__ qdi, double *__restrict__ qdf,
-                          const double *__restrict__ sqs, const double *__restrict__ sqd,
-                          double *__restrict__ emq, const Scalars *__restrict__ s, long long nn) {
-  const double dt = s->dt, dt2 = s->dt2, dt3 = s->dt3, dt6 = s->dt6;
-  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nn;
-       k += (long long)gridDim.x * blockDim.x) {
-    double a = sqs[k], b = sqd[k];
-    if (STAGE == 1) {
-      double si = qs[k], di = qd[k];
-      qsi[k] = si;
-      qs[k] = si + dt2 * a;
-      qsf[k] = si + dt6 * a;
-      qdi[k] = di;
-      qd[k] = emq[k] * (di + dt2 * b);
-      qdf[k] = di + dt6 * b;
-    } else if (STAGE == 2) {
-      qs[k] = qsi[k] + dt2 * a;
-      qsf[k] = qsf[k] + dt3 * a;
-      qd[k] = emq[k] * (qdi[k] + dt2 * b);
-      qdf[k] = qdf[k] + dt3 * b;
-    } else if (STAGE == 3) {
-      qs[k] = qsi[k] + dt * a;
-      qsf[k] = qsf[k] + dt3 * a;
-      double e = emq[k];
-      e = e * e;
-      emq[k] = e;
-      qd[k] = e * (qdi[k] + dt * b);
-      qdf[k] = qdf[k] + dt3 * b;
-    } else {
-      qs[k] = qsf[k] + dt6 * a;
-      qd[k] = emq[k] * (qdf[k] + dt6 * b);
-    }
-  }
-}
 
 // ---------------------------------------------------------------------------
 // adapt (evolution.f90:524-608): deterministic two-level reductions
@@ -886,8 +974,28 @@ __global__ void k_twist_zero(Scalars *s) { s->twist = 0.0; }
 // con2grid + the filter combination that forms qq and pp (evolution.f90:507-514)
 static int inversion_qq(casl_handle *h, bool reset) {
   long long nn = (long long)h->n * h->n;
-  int rc = con2grid_to_spec(h, h->qc);
-  if (rc) return rc;
+  if (h->nptq == 0) {
+    CASL_CUDA_TRY(cudaMemsetAsync(h->qc, 0, nn * sizeof(double), h->stream));
+  } else {
+    // con2grid, then its forward transform whose last store combines
+    int rc = con2grid_dev(h, false);
+    if (rc) return rc;
+    long long n = h->n;
+    LoadQC ld{h->coarseC, h->scal, h->c.beffect ? h->betac : nullptr, nn,
+              1.0 / (256.0 * (double)n * (double)n), (int)n};
+    rc = RFFT_DISPATCH(true, false, true, ld, (StoreStrided{h->qc, nn, 1, n}), 1);
+    if (rc) return rc;
+    const LoadStrided lq{h->qc, nn, n, 1};
+    if (reset)
+      return RFFT_DISPATCH(true, false, false, lq,
+                           (StoreCombine<true>{h->qs, h->qd, h->qc, h->qq, h->pp, h->flo, h->fhi,
+                                               h->green, (int)n}),
+                           1);
+    return RFFT_DISPATCH(true, false, false, lq,
+                         (StoreCombine<false>{h->qs, h->qd, h->qc, h->qq, h->pp, h->flo, h->fhi,
+                                              h->green, (int)n}),
+                         1);
+  }
   if (reset)
     CASL_K(k_combine<true>, grid_for(nn), 256, 0, h->stream)(h->qs, h->qd, h->qc, h->qq, h->pp,
                                                           h->flo, h->fhi, h->green, nn);
@@ -965,7 +1073,8 @@ static int source_grad(casl_handle *h) {
 
 // The rest of source (evolution.f90:432-490): the advection products fused
 // into ptospc's first pass, damping and integrating factor into its store.
-static int source_prod(casl_handle *h, int lev) {
+static int source_prod(casl_handle *h, int stage) {
+  const int lev = stage == 1 ? 0 : (stage == 4 ? 2 : 1);
   long long nn = (long long)h->n * h->n, n = h->n;
   double *tmp = h->w[0];  // w[0..1]
   int rc;
@@ -979,9 +1088,12 @@ static int source_prod(casl_handle *h, int lev) {
   rc = RFFT_DISPATCH(true, false, true, la, (StoreStrided{tmp, nn, 1, n}), 2);
   if (rc) return rc;
   StoreSource ss{};
-  ss.sqd = h->sqd; ss.sqs = h->sqs; ss.qq = h->qq; ss.pp = h->pp; ss.epq = h->epq;
+  ss.qq = h->qq; ss.pp = h->pp; ss.epq = h->epq;
+  ss.qs = h->qs; ss.qd = h->qd; ss.qsi = h->qsi; ss.qsf = h->qsf; ss.qdi = h->qdi;
+  ss.qdf = h->qdf; ss.emq = h->emq; ss.sc = h->scal;
   ss.rekman = h->p.rekman; ss.kdsq = h->c.kdsq; ss.therm = h->c.therm;
-  ss.heating = h->c.heating; ss.friction = h->c.friction; ss.lev = lev; ss.n = h->n;
+  ss.heating = h->c.heating; ss.friction = h->c.friction; ss.lev = lev; ss.stage = stage;
+  ss.n = h->n;
   return RFFT_DISPATCH(true, false, false, (LoadStrided{tmp, nn, n, 1}), ss, 2);
 }
 
@@ -1028,18 +1140,6 @@ static int nodes_task(casl_handle *h, int stage) {
   return check_launch(h);
 }
 
-static int spec_update(casl_handle *h, int stage) {
-  long long nn = (long long)h->n * h->n;
-  int g = grid_for(nn);
-  cudaStream_t st = h->stream;
-  switch (stage) {
-    case 1: CASL_K(k_spec_rk<1>, g, 256, 0, st)(h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs, h->sqd, h->emq, h->scal, nn); break;
-    case 2: CASL_K(k_spec_rk<2>, g, 256, 0, st)(h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs, h->sqd, h->emq, h->scal, nn); break;
-    case 3: CASL_K(k_spec_rk<3>, g, 256, 0, st)(h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs, h->sqd, h->emq, h->scal, nn); break;
-    default: CASL_K(k_spec_rk<4>, g, 256, 0, st)(h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs, h->sqd, h->emq, h->scal, nn); break;
-  }
-  return check_launch(h);
-}
 
 static int advance_dev(casl_handle *h) {
   int rc;
@@ -1060,9 +1160,8 @@ static int advance_dev(casl_handle *h) {
     if ((rc = main_invert_dev(h))) return rc;
     if (stage == 1 && (rc = adapt_dev(h))) return rc;
     if ((rc = main_after(h, h->ev_grad))) return rc;
-    if ((rc = source_prod(h, stage == 1 ? 0 : (stage == 4 ? 2 : 1)))) return rc;
+    if ((rc = source_prod(h, stage))) return rc;  // with the spectral RK update
     if ((rc = nodes_task(h, stage))) return rc;
-    if ((rc = spec_update(h, stage))) return rc;
   }
   return CASL_OK;
 }
@@ -2095,6 +2194,51 @@ int casl_get_stream(casl_handle *h, void **stream) {
 int casl_launch_count(long long *count) {
   if (!count) return CASL_EINVAL;
   *count = (long long)casl::g_launches;
+  return CASL_OK;
+}
+
+int casl_kernel_times(int mode, char *buf, long long cap) {
+  using namespace casl;
+  casl_handle *h = nullptr;  // process-wide: no handle records the error
+  if (mode < 0 || mode > 2) return CASL_EINVAL;
+  if (mode == 1 && !g_kt.ev) {
+    g_kt.ev = (cudaEvent_t *)calloc(2 * KT_MAX, sizeof(cudaEvent_t));
+    g_kt.name = (const char **)calloc(KT_MAX, sizeof(const char *));
+    if (!g_kt.ev || !g_kt.name) return CASL_ENOMEM;
+    for (int i = 0; i < 2 * KT_MAX; i++) CASL_CUDA_TRY(cudaEventCreate(&g_kt.ev[i]));
+  }
+  if (mode == 2) {
+    // report: per kernel name, launches / total ms / mean us, by total
+    if (!buf || cap <= 0) return CASL_EINVAL;
+    CASL_CUDA_TRY(cudaDeviceSynchronize());
+    std::vector<std::pair<std::string, std::pair<long long, double>>> rows;
+    std::map<std::string, size_t> at;
+    for (int i = 0; i < g_kt.n; i++) {
+      float ms = 0.f;
+      CASL_CUDA_TRY(cudaEventElapsedTime(&ms, g_kt.ev[2 * i], g_kt.ev[2 * i + 1]));
+      auto it = at.find(g_kt.name[i]);
+      if (it == at.end()) {
+        it = at.emplace(g_kt.name[i], rows.size()).first;
+        rows.push_back({g_kt.name[i], {0, 0.0}});
+      }
+      rows[it->second].second.first++;
+      rows[it->second].second.second += ms;
+    }
+    std::sort(rows.begin(), rows.end(),
+              [](const auto &a, const auto &b) { return a.second.second > b.second.second; });
+    std::string out;
+    char line[256];
+    for (auto &r : rows) {
+      snprintf(line, sizeof line, "%-40s %7lld %10.3f ms %9.2f us\n", r.first.c_str(),
+               r.second.first, r.second.second, 1e3 * r.second.second / r.second.first);
+      out += line;
+    }
+    snprintf(buf, (size_t)cap, "%s", out.c_str());
+    g_kt.n = 0;
+    return CASL_OK;
+  }
+  g_kt.on = mode == 1;
+  g_kt.n = 0;
   return CASL_OK;
 }
 

@@ -15,11 +15,18 @@ namespace casl {
 // Process-wide count of kernel launches issued by this library.
 extern unsigned long long g_launches;
 
+// Per-launch timing (casl_kernel_times): when switched on, every launch is
+// bracketed by a pair of CUDA events on its stream and tallied by kernel.
+bool kt_begin(const char *name, dim3 grid, dim3 block, size_t smem = 0, cudaStream_t st = 0);
+bool kt_end();
+
 // Every kernel launch goes through CASL_K(kernel, grid, block, smem, stream)(args);
-// it counts the launch.  The for-statement form keeps it a single statement
-// that is safe inside an unbraced if/else.
-#define CASL_K(name, ...)                                                          \
-  for (bool casl_once_ = (++::casl::g_launches, true); casl_once_; casl_once_ = false) \
+// it counts the launch (and times it while per-launch timing is on).  The
+// for-statement form keeps it a single statement that is safe inside an
+// unbraced if/else; its increment runs right after the launch.
+#define CASL_K(name, ...)                                                            \
+  for (bool casl_once_ = ::casl::kt_begin(#name, __VA_ARGS__); casl_once_;         \
+       casl_once_ = ::casl::kt_end())                                               \
   name<<<__VA_ARGS__>>>
 
 // Constants of constants.f90 and contours.f90:17-42, computed once on the

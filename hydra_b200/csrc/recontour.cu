@@ -1009,6 +1009,7 @@ int recontour_dev(casl_handle *h, const double *qq) {
   CASL_CUDA_TRY(cudaMemcpyAsync(hl.data(), lstart, (nlev + 1) * sizeof(long long),
                                 cudaMemcpyDeviceToHost, st));
   CASL_CUDA_TRY(cudaStreamSynchronize(st));
+  tr.point("hash_levels");
   std::vector<std::pair<long long, long long>> batches;  // [r0, r1)
   for (int l = 0; l < nlev;) {
     int l2 = l + 1;
@@ -1053,6 +1054,7 @@ int recontour_dev(casl_handle *h, const double *qq) {
   int g = gsz(ncr);
   CASL_CUDA_TRY(cudaMemsetAsync(pred, 0xff, ncr * sizeof(int), st));
   CASL_K(k_sp_pred, g, 256, 0, st)(succ, ncr, pred);
+  tr.point("rk_pred");
   // term and val are written only by the expansion at the end: until then
   // they hold the lists of splitters that are not sampled crossings
   const int K = 16;
@@ -1060,11 +1062,14 @@ int recontour_dev(casl_handle *h, const double *qq) {
   int *xl1 = term, *xl2 = val, *nx1 = dtot + 10, *nx2 = dtot + 11;
   CASL_CUDA_TRY(cudaMemsetAsync(nx1, 0, 2 * sizeof(int), st));
   CASL_K(k_sp_flag, g, 256, 0, st)(pred, succ, ncr, K, isspl, sf, own, xl1, nx1);
+  tr.point("rk_flag");
   CASL_K(k_sp_walk, gsz(nsmp), 256, 0, st)(sf, ncr, K, nsmp, xl1, nx1, own, nexts_c, seglen_c,
                                            segmin_c, segend_c, &h->scal->error);
+  tr.point("rk_walk1");
   CASL_K(k_sp_unowned, g, 256, 0, st)(ncr, own, isspl, sf, xl2, nx2);
   CASL_K(k_sp_walk, g, 256, 0, st)(sf, ncr, K, 0, xl2, nx2, own, nexts_c, seglen_c, segmin_c,
                                    segend_c, &h->scal->error);
+  tr.point("rk_walk2");
   exclusive_scan<int>(st, isspl, srank, ncr, tmpi2, dtot + 6);
   int S = 0;
   CASL_CUDA_TRY(cudaMemcpyAsync(&S, dtot + 6, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -1078,7 +1083,7 @@ int recontour_dev(casl_handle *h, const double *qq) {
       *ssl2 = ar2.get<int>(S), *shead = ar2.get<int>(S);
   long long *ssuf = ar2.get<long long>(S), *ssuf2 = ar2.get<long long>(S);
   if (ar2.failed) return CASL_ENOMEM;
-  tr.point("rk_walk");
+  tr.point("rk_scan");
   CASL_K(k_sp_compact, g, 256, 0, st)(isspl, srank, ncr, nexts_c, seglen_c, segmin_c, segend_c,
                                       nexts, seglen, segmin, segend);
   int gsS = gsz(S);

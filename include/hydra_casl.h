@@ -259,6 +259,12 @@ int casl_launch_count(long long *count);
 #define CASL_PROF_FFT 1   /* the batched real-FFT passes (ptospc/spctop halves) */
 int casl_profile(casl_handle *h, int kernel_class);
 int casl_profile_read(casl_handle *h, double *total_ms, long long *launches, double *bytes);
+/* Per-launch timing of every kernel of this library (process-wide):
+ * mode 1 switches it on (each launch bracketed by two CUDA events on its
+ * stream, up to 65536 launches), 0 switches it off, 2 writes a report into
+ * buf (one line per kernel: launches, total ms, mean us; by total) and
+ * starts a new tally.  A diagnostic, not a part of the reference interface. */
+int casl_kernel_times(int mode, char *buf, long long cap);
 
 #ifdef __cplusplus
 }
