@@ -428,48 +428,87 @@ __global__ void k_c2g_scatter(const double *__restrict__ xq, const double *__res
                               unsigned long long *__restrict__ csum) {
   // the coarsening that follows accumulates the coarse-cell sum here
   if (blockIdx.x == 0 && threadIdx.x == 0) *csum = 0;
-  int npt = s->nptq;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npt; i += gridDim.x * blockDim.x) {
-    int ia = nextq[i];
-    if (ia < 0 || ia >= npt) { atomicExch(err, CASL_EINVAL); continue; }
-    double xi = xq[i], yi = yq[i], xa = xq[ia], ya = yq[ia];
-    if (!(xi >= c.xmin && xi < c.xmax && yi >= c.ymin && yi < c.ymax)) {
-      atomicExch(err, CASL_EDOMAIN);
-      continue;
+  const unsigned FULL = 0xffffffffu;
+  const int npt = s->nptq, nf = c.nxf, lane = threadIdx.x & 31;
+  const int wstride = gridDim.x * blockDim.x;
+  // whole warps step through the nodes together, so that a segment's x-line
+  // crossings can be shared out over the warp's lanes below
+  for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < npt; base += wstride) {
+    const int i = base + lane;
+    int cnt = 0, ixbeg = 0, jump = 0, sgn = 0;
+    double xi = 0.0, yi = 0.0, dx = 1.0, dy = 0.0;
+    if (i < npt) {
+      const int ia = nextq[i];
+      if (ia < 0 || ia >= npt) {
+        atomicExch(err, CASL_EINVAL);
+      } else {
+        xi = xq[i];
+        yi = yq[i];
+        const double xa = xq[ia], ya = yq[ia];
+        if (!(xi >= c.xmin && xi < c.xmax && yi >= c.ymin && yi < c.ymax)) {
+          atomicExch(err, CASL_EDOMAIN);
+        } else {
+          const int ixci = 1 + f_int(c.glxfi * (xi - c.xmin));
+          const int ixca = 1 + f_int(c.glxfi * (xa - c.xmin));
+          const double xx = xa - xi;
+          dx = xx - c.ellx * f_dint(xx * c.hlxi);
+          const double yy = ya - yi;
+          dy = yy - c.elly * f_dint(yy * c.hlyi);
+          const int ixdif = ixca - ixci;
+          // nxc = ixdif - nf*((2*ixdif)/nf): with |2*ixdif| < 2nf the
+          // truncated quotient is -1, 0 or 1
+          const int t2 = 2 * ixdif;
+          const int nxc = ixdif - nf * (t2 >= nf ? 1 : (t2 <= -nf ? -1 : 0));
+          if (fabs(yy) > c.hly) {
+            const double cc = f_sign1(dy);
+            const double p = -(yi - c.hly * cc) / (dy + c.small);
+            int ix = 1 + f_int(c.glxfi * fmod(c.ellx + c.hlx + xi + p * dx, c.ellx));
+            ix = ix < 1 ? 1 : (ix > nf ? nf : ix);
+            atomicAdd(&ljx[ix - 1], -(int)cc);
+          }
+          if (nxc != 0) {
+            jump = f_isign1(nxc);
+            ixbeg = ixci + (jump - 1) / 2 + nf;
+            sgn = (int)f_sign1(dx);
+            cnt = nxc * jump;
+          }
+        }
+      }
     }
-    int ixci = 1 + f_int(c.glxfi * (xi - c.xmin));
-    int ixca = 1 + f_int(c.glxfi * (xa - c.xmin));
-    double xx = xa - xi;
-    double dx = xx - c.ellx * f_dint(xx * c.hlxi);
-    double yy = ya - yi;
-    double dy = yy - c.elly * f_dint(yy * c.hlyi);
-    int ixdif = ixca - ixci;
-    int nxc = ixdif - c.nxf * ((2 * ixdif) / c.nxf);
-    if (fabs(yy) > c.hly) {
-      double cc = f_sign1(dy);
-      double p = -(yi - c.hly * cc) / (dy + c.small);
-      int ix = 1 + f_int(c.glxfi * fmod(c.ellx + c.hlx + xi + p * dx, c.ellx));
-      ix = ix < 1 ? 1 : (ix > c.nxf ? c.nxf : ix);
-      atomicAdd(&ljx[ix - 1], -(int)cc);
-    }
-    if (nxc != 0 && nxc >= -c.nxf && nxc <= c.nxf) {
-      int jump = f_isign1(nxc);
-      int ixbeg = ixci + (jump - 1) / 2 + c.nxf;
-      int sgn = (int)f_sign1(dx);
-      for (int ncr = 0; ncr != nxc; ncr += jump) {
-        int m = (ixbeg + ncr) % c.nxf;
-        if (m < 0) m += c.nxf;
-        int ix = 1 + m;
-        double xgf = c.xmin + c.glxf * (double)(ix - 1);
-        double x2 = xgf - xi;
-        double px0 = (x2 - c.ellx * f_dint(x2 * c.hlxi)) / dx;
-        double y2 = yi + px0 * dy;
-        int iy = 2 + f_int(c.glyfi * (y2 - c.elly * f_dint(y2 * c.hlyi) - c.ymin));
+    // crossing q of the warp (all segments' crossings in lane order) goes
+    // to lane q % 32: its segment is the first lane whose inclusive count
+    // exceeds q
+    const int incl = warp_incl_scan(cnt);
+    const int excl = incl - cnt;
+    const int tot = __shfl_sync(FULL, incl, 31);
+    for (int b0 = 0; b0 < tot; b0 += 32) {
+      const int q = b0 + lane;
+      int o = 0;
+#pragma unroll
+      for (int st = 16; st > 0; st >>= 1)
+        if (__shfl_sync(FULL, incl, o + st - 1) <= q) o += st;
+      o = min(o, 31);
+      const int oex = __shfl_sync(FULL, excl, o), obeg = __shfl_sync(FULL, ixbeg, o);
+      const int ojump = __shfl_sync(FULL, jump, o), osgn = __shfl_sync(FULL, sgn, o);
+      const double oxi = __shfl_sync(FULL, xi, o), oyi = __shfl_sync(FULL, yi, o);
+      const double odx = __shfl_sync(FULL, dx, o), ody = __shfl_sync(FULL, dy, o);
+      if (q < tot) {
+        const int ncr = (q - oex) * ojump;
+        // (ixbeg + ncr) mod nf, the argument lying in (nf/2, 5nf/2)
+        int m = obeg + ncr;
+        m -= m >= nf ? nf : 0;
+        m -= m >= nf ? nf : 0;
+        const int ix = 1 + m;
+        const double xgf = c.xmin + c.glxf * (double)(ix - 1);
+        const double x2 = xgf - oxi;
+        const double px0 = (x2 - c.ellx * f_dint(x2 * c.hlxi)) / odx;
+        const double y2 = oyi + px0 * ody;
+        const int iy = 2 + f_int(c.glyfi * (y2 - c.elly * f_dint(y2 * c.hlyi) - c.ymin));
         if (iy >= 2 && iy <= c.nyf) {
           if (SPARSE)
-            c2g_sparse_add(DP, ix - 1, iy - 1, sgn, c.nx, c.nyf);
+            c2g_sparse_add(DP, ix - 1, iy - 1, osgn, c.nx, c.nyf);
           else
-            atomicAdd(&J[(long long)(ix - 1) * c.nyf + (iy - 1)], sgn);
+            atomicAdd(&J[(long long)(ix - 1) * c.nyf + (iy - 1)], osgn);
         }
       }
     }

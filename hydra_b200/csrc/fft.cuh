@@ -152,7 +152,10 @@ struct RfftShape {
   static constexpr int VW = VF ? 256 / TPV : 64 / TPV;
   static constexpr int V = VW < 1 ? 1 : (VW < N ? VW : N);  // vectors per CTA
   static constexpr int NT = V * TPV;        // threads per CTA
-  static constexpr int MINB = 768 / NT > 0 ? 768 / NT : 1;  // CTAs per SM to fit
+  // CTAs per SM to fit: 768 threads (<= 85 registers, no spills; a cap of
+  // 64 registers, one full wave for a batch of 2 at 1024^2, spilled and
+  // measured no faster inside the time step)
+  static constexpr int MINB = 768 / NT > 0 ? 768 / NT : 1;
   static constexpr int P8 = LOGH / 3;       // radix-8 passes
   static constexpr int REM = LOGH % 3;      // final radix-4 (2) or radix-2 (1) pass
   // forward transforms with a vector-fastest store stage their output in a

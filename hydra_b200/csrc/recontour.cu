@@ -273,16 +273,17 @@ constexpr int EDGES_PER_THREAD = 16;
 // Crossings are counted and emitted per chunk of 16 consecutive edges in the
 // reference's numbering: x-line edges (ix, iy)-(ix, iy+1) are numbered
 // e = ix*nyu + iy, y-line edges (ix, iy)-(ix+1, iy) e = NE + iy*nxu + ix.
-// One CTA takes a tile of CB = 16 columns x RB = 64 rows of level codes,
-// staged in shared memory with the next row and column (periodic): each
-// column's 64 codes are 8 16-byte loads, so the tile with its halo is one
-// load per thread.  An edge whose ends have codes ca, cb crosses exactly the
-// levels min(ca, cb) < l <= max(ca, cb) (none when they are equal, which
-// takes in equal end values).  Each half-warp handles one chunk: 16 rows of
-// a column (x-line edges) or 16 columns of a row (y-line edges).  COUNT
-// writes the chunk's number of crossings; EMIT writes its crossings (edge,
-// level) from the chunk's offset on, edge by edge and level by level, which
-// is the reference's order within a chunk.
+// One CTA takes two tiles of CB = 16 columns x RB = 64 rows of level codes,
+// each staged in shared memory with the next row and column (periodic):
+// each column's 64 codes are 8 16-byte loads, so a tile with its halo is one
+// load per thread of its half of the CTA.  An edge whose ends have codes
+// ca, cb crosses exactly the levels min(ca, cb) < l <= max(ca, cb) (none
+// when they are equal, which takes in equal end values).  Each thread owns
+// one chunk of its tile (64 chunks of 16 rows of a column, then 64 chunks of
+// 16 columns of a row) and walks its 17 codes: COUNT writes the chunk's
+// number of crossings, EMIT writes its crossings (edge, level) from the
+// chunk's offset on, edge by edge and level by level, which is the
+// reference's order within a chunk.
 constexpr int CR_CB = 16, CR_RB = 64;
 
 template <bool EMIT>
@@ -291,76 +292,63 @@ __global__ void __launch_bounds__(256) k_cr_tile(const unsigned short *__restric
                                                  const int *__restrict__ off,
                                                  unsigned long long *__restrict__ redge,
                                                  int *__restrict__ rlev) {
-  __shared__ int Cl[CR_CB + 1][CR_RB + 1];  // row length 65: conflict-free both ways
-  const int ix0 = blockIdx.x * CR_CB, iy0 = blockIdx.y * CR_RB;
-  {
-    const int t = threadIdx.x;
-    if (t < (CR_CB + 1) * 8) {  // 17 columns x 8 vectors of 8 codes
-      const int cc = t >> 3, part = t & 7;
-      int ix = ix0 + cc;
-      if (ix >= nxu) ix -= nxu;
-      const uint4 v =
-          *reinterpret_cast<const uint4 *>(lc + (long long)ix * nyu + iy0 + 8 * part);
-      const unsigned int w[4] = {v.x, v.y, v.z, v.w};
+  __shared__ int Cl[2][CR_CB + 1][CR_RB + 1];  // row length 65
+  const int half = threadIdx.x >> 7, t = threadIdx.x & 127;
+  const int ntx = nxu / CR_CB, nty = nyu / CR_RB;
+  const long long tile = 2LL * blockIdx.x + half;
+  const bool live = tile < (long long)ntx * nty;
+  const int ix0 = live ? (int)(tile % ntx) * CR_CB : 0, iy0 = live ? (int)(tile / ntx) * CR_RB : 0;
+  int(*C)[CR_RB + 1] = Cl[half];
+  if (live) {
+    for (int q = t; q < (CR_CB + 1) * 9; q += 128) {
+      if (q < (CR_CB + 1) * 8) {  // 17 columns x 8 vectors of 8 codes
+        const int cc = q >> 3, part = q & 7;
+        int ix = ix0 + cc;
+        if (ix >= nxu) ix -= nxu;
+        const uint4 v = *reinterpret_cast<const uint4 *>(lc + (long long)ix * nyu + iy0 + 8 * part);
+        const unsigned int w[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
-      for (int j = 0; j < 4; j++) {
-        Cl[cc][8 * part + 2 * j] = (int)(w[j] & 0xffffu);
-        Cl[cc][8 * part + 2 * j + 1] = (int)(w[j] >> 16);
+        for (int j = 0; j < 4; j++) {
+          C[cc][8 * part + 2 * j] = (int)(w[j] & 0xffffu);
+          C[cc][8 * part + 2 * j + 1] = (int)(w[j] >> 16);
+        }
+      } else {  // the row after the tile, periodic
+        const int cc = q - (CR_CB + 1) * 8;
+        int ix = ix0 + cc, iy = iy0 + CR_RB;
+        if (ix >= nxu) ix -= nxu;
+        if (iy >= nyu) iy -= nyu;
+        C[cc][CR_RB] = lc[(long long)ix * nyu + iy];
       }
-    } else if (t < (CR_CB + 1) * 9) {  // the row after the tile, periodic
-      const int cc = t - (CR_CB + 1) * 8;
-      int ix = ix0 + cc, iy = iy0 + CR_RB;
-      if (ix >= nxu) ix -= nxu;
-      if (iy >= nyu) iy -= nyu;
-      Cl[cc][CR_RB] = lc[(long long)ix * nyu + iy];
     }
   }
   __syncthreads();
+  if (!live) return;
   const long long NE = (long long)nxu * nyu;
-  const int lane = threadIdx.x & 31, sub = lane & 15, hw = threadIdx.x >> 4;
-  // 64 x-line chunks (16 columns x 4 groups of 16 rows), then 64 y-line
-  // chunks (one per row): 16 half-warps take one chunk each per round
-  for (int round = 0; round < 8; round++) {
-    int cc, r, nxt_c, nxt_r;
-    long long e;
-    if (round < 4) {
-      const int chunk = round * 16 + hw;  // 0..63
-      cc = chunk >> 2;                    // column 0..15
-      r = (chunk & 3) * 16 + sub;
-      nxt_c = cc;
-      nxt_r = r + 1;
-      e = (long long)(ix0 + cc) * nyu + (iy0 + r);
-    } else {
-      r = (round - 4) * 16 + hw;  // row 0..63
-      cc = sub;
-      nxt_c = cc + 1;
-      nxt_r = r;
-      e = NE + (long long)(iy0 + r) * nxu + (ix0 + cc);
-    }
-    const int ca = Cl[cc][r], cb = Cl[nxt_c][nxt_r];
+  // chunk t: x-line chunks 0..63 (column t>>2, rows 16*(t&3)...), then
+  // y-line chunks 64..127 (row t-64, columns 0..15)
+  const bool xl = t < 64;
+  const int cc0 = xl ? t >> 2 : 0, r0 = xl ? 16 * (t & 3) : t - 64;
+  const long long e0 = xl ? (long long)(ix0 + cc0) * nyu + (iy0 + r0)
+                          : NE + (long long)(iy0 + r0) * nxu + ix0;
+  const long long chunk_id = e0 / EDGES_PER_THREAD;
+  int pos = EMIT ? off[chunk_id] : 0, total = 0;
+  int ca = xl ? C[cc0][r0] : C[0][r0];
+#pragma unroll 4
+  for (int i = 0; i < 16; i++) {
+    const int cb = xl ? C[cc0][r0 + i + 1] : C[i + 1][r0];
     const int l1 = max(min(ca, cb) + 1, li.levbeg), l2 = min(max(ca, cb), li.levend);
-    const int k = l2 >= l1 ? l2 - l1 + 1 : 0;
-    const long long chunk_id = e / EDGES_PER_THREAD;
     if (!EMIT) {
-      int t = k;
-#pragma unroll
-      for (int o = 8; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o, 16);
-      if (sub == 0) cnt[chunk_id] = t;
+      total += l2 >= l1 ? l2 - l1 + 1 : 0;
     } else {
-      int incl = k;
-#pragma unroll
-      for (int o = 1; o < 16; o <<= 1) {
-        int y = __shfl_up_sync(0xffffffffu, incl, o, 16);
-        if (sub >= o) incl += y;
-      }
-      int pos = off[chunk_id] + incl - k;
       for (int l = l1; l <= l2; l++) {
-        redge[pos] = (unsigned long long)e;
+        redge[pos] = (unsigned long long)(e0 + i);
         rlev[pos] = l - li.levbeg;
         pos++;
       }
     }
+    ca = cb;
   }
+  if (!EMIT) cnt[chunk_id] = total;
 }
 
 // Position and box transitions of every crossing (congen.f90:211-252).
@@ -629,35 +617,71 @@ __global__ void k_sp_pred(const int *__restrict__ succ, long long N, int *__rest
 // A walk step reads the next node's successor and splitter flag (sf, one
 // 8-byte load) and writes the node's (owner, offset) pair (own, one 8-byte
 // store): two random accesses per step.  isspl keeps the flags as a plain
-// array for the scan.  The walks run one thread per splitter: the sampled
-// crossings r = K*t by their index, the chain starts that are not sampled
-// from an appended list, so that no lane idles on a crossing that is not a
-// splitter.
+// array for the scan.  The sampled crossings are those whose index hashes
+// to 0 mod K, not every K-th index: along a contour the indices often step
+// by a constant (parallel contours put the same number of crossings in
+// every row), and an arithmetic sample can then miss a whole contour.  All
+// splitters (sampled ones and chain starts) are appended to xlist, so the
+// walks run one thread per splitter with no idle lanes.
+__device__ __forceinline__ unsigned int sp_hash(unsigned int x) {
+  x ^= x >> 16;
+  x *= 0x7feb352dU;
+  x ^= x >> 15;
+  x *= 0x846ca68bU;
+  x ^= x >> 16;
+  return x;
+}
+// Appends go through one atomic per block and tile of the crossings: the
+// block's flags are counted by ballots, so the list keeps index order within
+// a block.
+__device__ __forceinline__ void sp_append(bool f, int r, int *__restrict__ xlist,
+                                          int *__restrict__ nx, int *wtot, int *wbase) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const unsigned m = __ballot_sync(0xffffffffu, f);
+  if (lane == 0) wtot[w] = __popc(m);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int i = 0; i < nw; i++) {
+      const int c = wtot[i];
+      wtot[i] = t;
+      t += c;
+    }
+    *wbase = t ? atomicAdd(nx, t) : 0;
+  }
+  __syncthreads();
+  if (f) xlist[*wbase + wtot[w] + __popc(m & ((1u << lane) - 1))] = r;
+  __syncthreads();
+}
 __global__ void k_sp_flag(const int *__restrict__ pred, const int *__restrict__ succ, long long N,
                           int K, int *__restrict__ isspl, int2 *__restrict__ sf,
                           int2 *__restrict__ own, int *__restrict__ xlist,
                           int *__restrict__ nx) {
-  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < N;
-       r += (long long)gridDim.x * blockDim.x) {
-    const bool smp = r % K == 0;
-    const int f = smp || pred[r] < 0;
-    isspl[r] = f;
-    sf[r] = make_int2(succ[r], f);
-    own[r] = make_int2(-1, 0);
-    if (f && !smp) xlist[atomicAdd(nx, 1)] = (int)r;
+  __shared__ int wtot[32], wbase;
+  for (long long b0 = blockIdx.x * (long long)blockDim.x; b0 < N;
+       b0 += (long long)gridDim.x * blockDim.x) {
+    const long long r = b0 + threadIdx.x;
+    int f = 0;
+    if (r < N) {
+      f = sp_hash((unsigned int)r) % (unsigned int)K == 0 || pred[r] < 0;
+      isspl[r] = f;
+      sf[r] = make_int2(succ[r], f);
+      own[r] = make_int2(-1, 0);
+    }
+    sp_append(f != 0, (int)r, xlist, nx, wtot, &wbase);
   }
 }
-// walks from splitters t < nsmp (crossing K*t) and xlist[t - nsmp] after
-// them, up to the next splitter
-__global__ void k_sp_walk(const int2 *__restrict__ sf, long long N, int K, long long nsmp,
-                          const int *__restrict__ xlist, const int *__restrict__ nx,
-                          int2 *__restrict__ own, int *__restrict__ nexts_c,
-                          int *__restrict__ seglen_c, int *__restrict__ segmin_c,
-                          int *__restrict__ segend_c, int *__restrict__ err) {
-  const long long total = nsmp + *nx;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-       t += (long long)gridDim.x * blockDim.x) {
-    const int s = t < nsmp ? (int)(t * K) : xlist[t - nsmp];
+// Walks from the splitters xlist[0 .. *nx) up to the next splitter, one
+// thread per splitter.  A walk longer than N steps (impossible for a
+// successor graph) sets err and ends.
+__global__ void k_sp_walk(const int2 *__restrict__ sf, long long N, const int *__restrict__ xlist,
+                          const int *__restrict__ nx, int2 *__restrict__ own,
+                          int *__restrict__ nexts_c, int *__restrict__ seglen_c,
+                          int *__restrict__ segmin_c, int *__restrict__ segend_c,
+                          int *__restrict__ err) {
+  const int total = *nx;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const int s = xlist[t];
     int v = s, k = 0, mn = s, nxt = -1;
     own[s] = make_int2(s, 0);
     int n = sf[s].x;
@@ -683,13 +707,18 @@ __global__ void k_sp_walk(const int2 *__restrict__ sf, long long N, int K, long 
 __global__ void k_sp_unowned(long long N, const int2 *__restrict__ own, int *__restrict__ isspl,
                              int2 *__restrict__ sf, int *__restrict__ xlist,
                              int *__restrict__ nx) {
-  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < N;
-       r += (long long)gridDim.x * blockDim.x)
-    if (own[r].x < 0) {
+  __shared__ int wtot[32], wbase;
+  for (long long b0 = blockIdx.x * (long long)blockDim.x; b0 < N;
+       b0 += (long long)gridDim.x * blockDim.x) {
+    const long long r = b0 + threadIdx.x;
+    bool f = false;
+    if (r < N && own[r].x < 0) {
+      f = true;
       isspl[r] = 1;
       sf[r].y = 1;
-      xlist[atomicAdd(nx, 1)] = (int)r;
     }
+    sp_append(f, (int)r, xlist, nx, wtot, &wbase);
+  }
 }
 __global__ void k_sp_compact(const int *__restrict__ isspl, const int *__restrict__ srank, long long N,
                              const int *__restrict__ nexts_c, const int *__restrict__ seglen_c,
@@ -948,7 +977,8 @@ int recontour_dev(casl_handle *h, const double *qq) {
   int *tmpi = ar.get<int>(scan_tmp_elems(nchunks) + 4);
   int *dtot = ar.get<int>(16);
   if (ar.failed) return CASL_ENOMEM;
-  const dim3 tgrid(nxu / CR_CB, nyu / CR_RB);
+  const long long ntile = (long long)(nxu / CR_CB) * (nyu / CR_RB);
+  const int tgrid = (int)((ntile + 1) / 2);
   CASL_K(k_cr_tile<false>, tgrid, 256, 0, st)(lc, li, nxu, nyu, ccnt, nullptr, nullptr, nullptr);
   tr.point("cr_count");
   exclusive_scan<int>(st, ccnt, coffs, nchunks, tmpi, dtot);
@@ -1056,18 +1086,17 @@ int recontour_dev(casl_handle *h, const double *qq) {
   CASL_K(k_sp_pred, g, 256, 0, st)(succ, ncr, pred);
   tr.point("rk_pred");
   // term and val are written only by the expansion at the end: until then
-  // they hold the lists of splitters that are not sampled crossings
+  // they hold the lists of splitters
   const int K = 16;
-  const long long nsmp = (ncr + K - 1) / K;
   int *xl1 = term, *xl2 = val, *nx1 = dtot + 10, *nx2 = dtot + 11;
   CASL_CUDA_TRY(cudaMemsetAsync(nx1, 0, 2 * sizeof(int), st));
   CASL_K(k_sp_flag, g, 256, 0, st)(pred, succ, ncr, K, isspl, sf, own, xl1, nx1);
   tr.point("rk_flag");
-  CASL_K(k_sp_walk, gsz(nsmp), 256, 0, st)(sf, ncr, K, nsmp, xl1, nx1, own, nexts_c, seglen_c,
-                                           segmin_c, segend_c, &h->scal->error);
+  CASL_K(k_sp_walk, gsz(ncr / K + 1), 256, 0, st)(sf, ncr, xl1, nx1, own, nexts_c, seglen_c,
+                                                  segmin_c, segend_c, &h->scal->error);
   tr.point("rk_walk1");
   CASL_K(k_sp_unowned, g, 256, 0, st)(ncr, own, isspl, sf, xl2, nx2);
-  CASL_K(k_sp_walk, g, 256, 0, st)(sf, ncr, K, 0, xl2, nx2, own, nexts_c, seglen_c, segmin_c,
+  CASL_K(k_sp_walk, g, 256, 0, st)(sf, ncr, xl2, nx2, own, nexts_c, seglen_c, segmin_c,
                                    segend_c, &h->scal->error);
   tr.point("rk_walk2");
   exclusive_scan<int>(st, isspl, srank, ncr, tmpi2, dtot + 6);
@@ -1104,7 +1133,19 @@ int recontour_dev(casl_handle *h, const double *qq) {
   CASL_K(k_sp_expand, g, 256, 0, st)(ncr, own, srank, stm, smn, ssuf, shead, slp, segend,
                                      term, lab, val, ep);
   RC_TRY(check_launch(h));
-  if (tr.on) fprintf(stderr, "[casl trace] ranking: %d splitters, %d jump rounds\n", S, rounds);
+  if (tr.on) {
+    std::vector<int> sl(S);
+    CASL_CUDA_TRY(cudaMemcpyAsync(sl.data(), seglen, S * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CASL_CUDA_TRY(cudaStreamSynchronize(st));
+    long long tot = 0;
+    int mx = 0;
+    for (int x : sl) {
+      tot += x;
+      mx = std::max(mx, x);
+    }
+    fprintf(stderr, "[casl trace] ranking: %d splitters, %d jump rounds; segment length mean %.2f, max %d\n",
+            S, rounds, (double)tot / S, mx);
+  }
 
   tr.point("rk_expand");
   // --- 6. saddle chains: exact simulation of the reference traversal ----------
