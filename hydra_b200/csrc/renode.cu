@@ -20,87 +20,184 @@ __global__ void k_rn_cid(RenodeIn in, long long N, int *__restrict__ cid) {
     cid[w] = contour_of(cs, C, w);
 }
 
-// The node densities of renode (contours.f90:718-796) for node w in one
-// pass: dx, dy, |d| to the next node; corners and curvature b; the cubic
-// coefficients and spherical-curvature densities; node curvature as a
-// weighted average; the fractional node count.  Every quantity node w needs is
-// recomputed from the coordinates of nodes w-2..w+3 (cyclic in the contour)
-// with the same expressions in the same order, so only the results the
-// placement reads (dx, dy, the final e, A, B, Cc, corner) go to memory.
+// The node densities of renode (contours.f90:718-796) for node w: dx, dy,
+// |d| to the next node; corners and curvature b; the cubic coefficients and
+// spherical-curvature densities; node curvature as a weighted average; the
+// fractional node count.  Only the results the placement reads (dx, dy, the
+// final e, A, B, Cc, corner) go to memory.  rn_node recomputes every
+// quantity node w needs from the coordinates of nodes w-2..w+3 (cyclic in
+// the contour); k_rn_stencil computes each quantity once per node and passes
+// it to the neighbouring lanes, with rn_node for the warps whose nodes come
+// near a contour's end.  Both use the same expressions in the same order.
+__device__ __forceinline__ void rn_node(const RenodeIn &in, const RenodeScratch &s, const Consts &c,
+                                        long long w) {
+  const double f12 = 0.5, f13 = 1.0 / 3.0, f16 = 1.0 / 6.0;
+  const int k = s.cid[w];
+  const long long cs = in.cs[k], L = in.len[k];
+  long long j[6];
+  j[2] = w;
+  j[1] = wprev(w, cs, L);
+  j[0] = wprev(j[1], cs, L);
+  j[3] = wnext(w, cs, L);
+  j[4] = wnext(j[3], cs, L);
+  j[5] = wnext(j[4], cs, L);
+  double X[6], Y[6];
+#pragma unroll
+  for (int m = 0; m < 6; m++) {
+    X[m] = in.xw[j[m]];
+    Y[m] = in.yw[j[m]];
+  }
+  // rn1 at nodes m = 0..4
+  double dx[5], dy[5], v[5], e1[5];
+#pragma unroll
+  for (int m = 0; m < 5; m++) {
+    double xx = X[m + 1] - X[m];
+    dx[m] = xx - c.ellx * f_dint(xx * c.hlxi);
+    double yy = Y[m + 1] - Y[m];
+    dy[m] = yy - c.elly * f_dint(yy * c.hlyi);
+    v[m] = dx[m] * dx[m] + dy[m] * dy[m];
+    e1[m] = sqrt(v[m]);
+  }
+  // rn2 at nodes m = 1..4
+  double b[5];
+  int corner2 = 0;
+#pragma unroll
+  for (int m = 1; m < 5; m++) {
+    double u = v[m - 1], a = -dx[m - 1], cc = -dy[m - 1];
+    int corner = dx[m] * a + dy[m] * cc > 0.0;
+    if (m == 2) corner2 = corner;
+    if (corner) {
+      b[m] = 0.0;
+    } else {
+      double t1 = a * v[m] - dx[m] * u, t2 = cc * v[m] - dy[m] * u;
+      b[m] = (dx[m] * cc - a * dy[m]) / sqrt(t1 * t1 + t2 * t2 + c.small3);
+    }
+  }
+  // rn3 at nodes m = 1..3 (the cubic coefficients only at m = 2)
+  double u2[4], v2[4], A = 0.0, B = 0.0, Cc = 0.0;
+#pragma unroll
+  for (int m = 1; m < 4; m++) {
+    double u = e1[m] * (b[m + 1] + b[m]);
+    double cc = e1[m] * (b[m + 1] - b[m]);
+    if (m == 2) {
+      A = f16 * cc - f12 * u;
+      B = f12 * (u - cc);
+      Cc = f13 * cc;
+    }
+    double ww = 1.0 / (v[m] + c.dmsq);
+    u2[m] = ww * sqrt(c.elf * v[m] + u * u);
+    v2[m] = ww * e1[m];
+  }
+  // rn4 at nodes 2, 3 and rn5 at node 2
+  const double d2 = (u2[1] + u2[2]) / (v2[1] + v2[2] + c.small);
+  const double d3 = (u2[2] + u2[3]) / (v2[2] + v2[3] + c.small);
+  const double uu = 0.5 * (d2 + d3);
+  const double t = c.densf * sqrt(uu) + uu;
+  s.dx[w] = dx[2];
+  s.dy[w] = dy[2];
+  s.e[w] = e1[2] * fmin(c.dmi, t);
+  s.A[w] = A;
+  s.B[w] = B;
+  s.Cc[w] = Cc;
+  s.corner[w] = corner2;
+  s.head[w] = (w == cs);
+  if (corner2) atomicAdd(&s.ccnt[k], 1);
+}
+
+// One warp covers nodes base-2 .. base+29 (lane L holds node base-2+L) and
+// writes nodes base .. base+27 (lanes 2..29): the segment quantities (rn1)
+// of lane L, its curvature (rn2), its cubic and density terms (rn3) and its
+// rn4 average each take the lower neighbour's value from lane L-1 and the
+// upper neighbour's from lane L+1.  Valid while every written node's
+// stencil w-2..w+3 lies inside its contour without wrapping; otherwise the
+// warp takes rn_node.
+constexpr int RN_OUT = 28;
 __global__ void k_rn_stencil(RenodeIn in, RenodeScratch s, Consts c) {
   const double f12 = 0.5, f13 = 1.0 / 3.0, f16 = 1.0 / 6.0;
-  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < in.N;
-       w += (long long)gridDim.x * blockDim.x) {
-    const int k = s.cid[w];
-    const long long cs = in.cs[k], L = in.len[k];
-    long long j[6];
-    j[2] = w;
-    j[1] = wprev(w, cs, L);
-    j[0] = wprev(j[1], cs, L);
-    j[3] = wnext(w, cs, L);
-    j[4] = wnext(j[3], cs, L);
-    j[5] = wnext(j[4], cs, L);
-    double X[6], Y[6];
-#pragma unroll
-    for (int m = 0; m < 6; m++) {
-      X[m] = in.xw[j[m]];
-      Y[m] = in.yw[j[m]];
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const long long N = in.N;
+  const long long nwin = (N + RN_OUT - 1) / RN_OUT;
+  const long long wstride = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long wi = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); wi < nwin;
+       wi += wstride) {
+    const long long base = wi * RN_OUT;
+    const long long o = base - 2 + lane;  // this lane's node
+    const bool out = lane >= 2 && lane < 2 + RN_OUT && o < N;
+    int k = 0;
+    long long cs = 0, L = 0;
+    bool lin = true;
+    if (out) {
+      k = s.cid[o];
+      cs = in.cs[k];
+      L = in.len[k];
+      lin = o - 2 >= cs && o + 3 <= cs + L - 1;
     }
-    // rn1 at nodes m = 0..4
-    double dx[5], dy[5], v[5], e1[5];
-#pragma unroll
-    for (int m = 0; m < 5; m++) {
-      double xx = X[m + 1] - X[m];
-      dx[m] = xx - c.ellx * f_dint(xx * c.hlxi);
-      double yy = Y[m + 1] - Y[m];
-      dy[m] = yy - c.elly * f_dint(yy * c.hlyi);
-      v[m] = dx[m] * dx[m] + dy[m] * dy[m];
-      e1[m] = sqrt(v[m]);
+    if (!__all_sync(FULL, lin)) {
+      if (out) rn_node(in, s, c, o);
+      continue;
     }
-    // rn2 at nodes m = 1..4
-    double b[5];
-    int corner2 = 0;
-#pragma unroll
-    for (int m = 1; m < 5; m++) {
-      double u = v[m - 1], a = -dx[m - 1], cc = -dy[m - 1];
-      int corner = dx[m] * a + dy[m] * cc > 0.0;
-      if (m == 2) corner2 = corner;
-      if (corner) {
-        b[m] = 0.0;
-      } else {
-        double t1 = a * v[m] - dx[m] * u, t2 = cc * v[m] - dy[m] * u;
-        b[m] = (dx[m] * cc - a * dy[m]) / sqrt(t1 * t1 + t2 * t2 + c.small3);
-      }
+    // coordinates of this lane's node and of the next one
+    double X = 0.0, Y = 0.0, X1 = 0.0, Y1 = 0.0;
+    if (o >= 0 && o < N) {
+      X = in.xw[o];
+      Y = in.yw[o];
     }
-    // rn3 at nodes m = 1..3 (the cubic coefficients only at m = 2)
-    double u2[4], v2[4], A = 0.0, B = 0.0, Cc = 0.0;
-#pragma unroll
-    for (int m = 1; m < 4; m++) {
-      double u = e1[m] * (b[m + 1] + b[m]);
-      double cc = e1[m] * (b[m + 1] - b[m]);
-      if (m == 2) {
-        A = f16 * cc - f12 * u;
-        B = f12 * (u - cc);
-        Cc = f13 * cc;
-      }
-      double ww = 1.0 / (v[m] + c.dmsq);
-      u2[m] = ww * sqrt(c.elf * v[m] + u * u);
-      v2[m] = ww * e1[m];
+    if (lane == 31 && o + 1 < N) {
+      X1 = in.xw[o + 1];
+      Y1 = in.yw[o + 1];
     }
-    // rn4 at nodes 2, 3 and rn5 at node 2
-    const double d2 = (u2[1] + u2[2]) / (v2[1] + v2[2] + c.small);
-    const double d3 = (u2[2] + u2[3]) / (v2[2] + v2[3] + c.small);
-    const double uu = 0.5 * (d2 + d3);
-    const double t = c.densf * sqrt(uu) + uu;
-    s.dx[w] = dx[2];
-    s.dy[w] = dy[2];
-    s.e[w] = e1[2] * fmin(c.dmi, t);
-    s.A[w] = A;
-    s.B[w] = B;
-    s.Cc[w] = Cc;
-    s.corner[w] = corner2;
-    s.head[w] = (w == cs);
-    if (corner2) atomicAdd(&s.ccnt[k], 1);
+    double Xn = __shfl_down_sync(FULL, X, 1), Yn = __shfl_down_sync(FULL, Y, 1);
+    if (lane == 31) {
+      Xn = X1;
+      Yn = Y1;
+    }
+    // rn1: the segment to the next node
+    const double xx = Xn - X;
+    const double dx = xx - c.ellx * f_dint(xx * c.hlxi);
+    const double yy = Yn - Y;
+    const double dy = yy - c.elly * f_dint(yy * c.hlyi);
+    const double v = dx * dx + dy * dy;
+    const double e1 = sqrt(v);
+    // rn2 at this node, from the previous segment
+    const double up = __shfl_up_sync(FULL, v, 1);
+    const double a = -__shfl_up_sync(FULL, dx, 1), ccp = -__shfl_up_sync(FULL, dy, 1);
+    const int corner = dx * a + dy * ccp > 0.0;
+    double b;
+    if (corner) {
+      b = 0.0;
+    } else {
+      const double t1 = a * v - dx * up, t2 = ccp * v - dy * up;
+      b = (dx * ccp - a * dy) / sqrt(t1 * t1 + t2 * t2 + c.small3);
+    }
+    // rn3 at this node, with the next node's curvature
+    const double bn = __shfl_down_sync(FULL, b, 1);
+    const double u = e1 * (bn + b);
+    const double cc = e1 * (bn - b);
+    const double A = f16 * cc - f12 * u;
+    const double B = f12 * (u - cc);
+    const double Cc = f13 * cc;
+    const double ww = 1.0 / (v + c.dmsq);
+    const double u2 = ww * sqrt(c.elf * v + u * u);
+    const double v2 = ww * e1;
+    // rn4 at this node (with the previous node's rn3) and at the next one
+    const double u2p = __shfl_up_sync(FULL, u2, 1), v2p = __shfl_up_sync(FULL, v2, 1);
+    const double d = (u2p + u2) / (v2p + v2 + c.small);
+    const double dn = __shfl_down_sync(FULL, d, 1);
+    if (out) {
+      // rn5
+      const double uu = 0.5 * (d + dn);
+      const double t = c.densf * sqrt(uu) + uu;
+      s.dx[o] = dx;
+      s.dy[o] = dy;
+      s.e[o] = e1 * fmin(c.dmi, t);
+      s.A[o] = A;
+      s.B[o] = B;
+      s.Cc[o] = Cc;
+      s.corner[o] = corner;
+      s.head[o] = (o == cs);
+      if (corner) atomicAdd(&s.ccnt[k], 1);
+    }
   }
 }
 
