@@ -385,45 +385,41 @@ struct LoadVort {
 // ---------------------------------------------------------------------------
 // con2grid (contours.f90:173-346)
 // ---------------------------------------------------------------------------
-// Sparse con2grid.  The coarse cell is C(cx, cy) = sum_b w_b G(4cx-3+b, cy)
+// Packed con2grid.  The coarse cell is C(cx, cy) = sum_b w_b G(4cx-3+b, cy)
 // with G(fx, cy) = sum_a w_a L(fx, 4cy-3+a) the 7-tap of fine column fx at
-// coarse row cy, L(fx, r) = lbot(fx) + sum_{r' <= r} J(fx, r') (rows and
-// columns periodic, 0-based).  A crossing s at fine row r >= 1 adds to G(fx,
-// cy) s times the weight of the stencil rows at or above r: 16 for every
-// cy >= cf = (r+6)/4 (kept as a jump 16s at cf, summed up the column
-// later), a partial tail of the weights for the (at most two) cy between,
-// and for cy = 0, whose stencil wraps to the top rows, 6 for every crossing
-// below the top seven rows (formed from the column total later) with the
-// differences at rows 1..3 and nf-6..nf-1 added here.  DP(fx, cy) holds the
-// jumps (.x) and the direct terms (.y); integer sums, so the result is the
-// dense scan's to the bit in any order.
-__device__ __forceinline__ int c2g_tail(int k) {  // w_k + ... + w_6 for k = 1..6
-  return k == 1 ? 15 : (k == 2 ? 13 : (k == 3 ? 10 : (k == 4 ? 6 : (k == 5 ? 3 : 1))));
-}
-__device__ __forceinline__ void c2g_sparse_add(int2 *__restrict__ DP, int fx, int r, int s, int n,
-                                               int nf) {
-  int2 *col = DP + (long long)fx * n;
-  const int cf = (r + 6) >> 2;
-  if (cf <= n - 1) atomicAdd(&col[cf].x, 16 * s);
-  const int lo = max(1, r >> 2), hi = min(cf - 1, n - 1);
-  for (int cy = lo; cy <= hi; cy++) atomicAdd(&col[cy].y, s * c2g_tail(r - 4 * cy + 3));
-  int w0 = 0;
-  if (r <= 3)
-    w0 = r == 1 ? 6 : (r == 2 ? 3 : 1);
-  else if (r >= nf - 6)
-    w0 = r <= nf - 3 ? 6 : (r == nf - 2 ? 5 : 3);
-  if (w0) atomicAdd(&col[0].y, s * w0);
+// coarse row cy and L(fx, r) = lbot(fx) + sum_{r' <= r} J(fx, r') (rows and
+// columns periodic, 0-based).  The jumps J of the four fine rows 4k..4k+3 of
+// a column share one 64-bit word JW(fx, k) as signed 16-bit counts (a
+// crossing at row r adds s << 16(r%4)), so a crossing is one atomic and the
+// fine grid takes 2 bytes per cell.  A fine edge's net count is at most one
+// per contour level crossing it (a level's crossings of a short segment
+// alternate in sign), so the counts stay far inside +-32767 for the level
+// counts the host allows on this path.  The sum kernel decodes the words
+// and forms G from the column's running total and the seven rows around
+// each coarse row; integer sums, so the result is the dense scan's to the
+// bit in any order.
+__device__ __forceinline__ void c2g_decode(unsigned long long w, int &c0, int &c1, int &c2,
+                                           int &c3) {
+  long long v = (long long)w;
+  c0 = (int)(((v & 0xffff) ^ 0x8000) - 0x8000);
+  v = (v - c0) >> 16;
+  c1 = (int)(((v & 0xffff) ^ 0x8000) - 0x8000);
+  v = (v - c1) >> 16;
+  c2 = (int)(((v & 0xffff) ^ 0x8000) - 0x8000);
+  v = (v - c2) >> 16;
+  c3 = (int)v;
 }
 
 // Per segment (i, nextq(i)): x fine-grid-line crossings and the crossing of
 // y = ymin, counted as +-1 PV jumps (contours.f90:232-270): J += sgn at
-// each (SPARSE: the coarse-row terms above into DP), ljx the bottom-boundary
+// each (PACKED: into the row's 16-bit lane of JW), ljx the bottom-boundary
 // jumps.  The FP64 expressions are the reference's, evaluated in its order
 // without FMA, so every crossing lands in the same fine cell.
-template <bool SPARSE>
+template <bool PACKED>
 __global__ void k_c2g_scatter(const double *__restrict__ xq, const double *__restrict__ yq,
                               const int *__restrict__ nextq, const Scalars *__restrict__ s,
-                              int *__restrict__ J, int2 *__restrict__ DP, int *__restrict__ ljx,
+                              int *__restrict__ J, unsigned long long *__restrict__ JW,
+                              int *__restrict__ ljx,
                               Consts c, int *__restrict__ err,
                               unsigned long long *__restrict__ csum) {
   // the coarsening that follows accumulates the coarse-cell sum here
@@ -505,9 +501,11 @@ __global__ void k_c2g_scatter(const double *__restrict__ xq, const double *__res
         const double y2 = oyi + px0 * ody;
         const int iy = 2 + f_int(c.glyfi * (y2 - c.elly * f_dint(y2 * c.hlyi) - c.ymin));
         if (iy >= 2 && iy <= c.nyf) {
-          if (SPARSE)
-            c2g_sparse_add(DP, ix - 1, iy - 1, osgn, c.nx, c.nyf);
-          else
+          if (PACKED) {
+            const int r = iy - 1;
+            atomicAdd(&JW[(long long)(ix - 1) * c.nx + (r >> 2)],
+                      (unsigned long long)((long long)osgn << (16 * (r & 3))));
+          } else
             atomicAdd(&J[(long long)(ix - 1) * c.nyf + (iy - 1)], osgn);
         }
       }
@@ -614,17 +612,19 @@ __global__ void k_c2g_coarsen(const int *__restrict__ L, int *__restrict__ C,
 }
 
 
-// Sparse con2grid, second half: per fine column an inclusive scan of the
-// jumps up the coarse rows plus the direct terms gives G(fx, cy) (with
-// 16*lbot(fx)); G(fx, 0) takes 6/16 of the column's jump total.  Then the
-// 7-tap along x.  A CTA owns CW = 7 coarse columns and their 4*CW+3 = 31
-// fine columns, one warp per column, RPS = 32U coarse rows per step with
-// the next step's rows in flight; the rows of G pass through shared memory.
+// Packed con2grid, second half.  A CTA owns CW = 7 coarse columns and their
+// 4*CW+3 = 31 fine columns, one warp per column, RPS = 32U coarse rows per
+// step with the next step's words in flight.  Lane cy decodes its word,
+// the warp scans the word totals (ex = jumps of all rows below 4cy), and
+// with the two top counts of the word below (rows 4cy-2, 4cy-1) the seven
+// levels L(4cy-3 .. 4cy+3) follow: L(4cy-1) = lbot + ex, one count taken or
+// added per row on either side.  G passes through shared memory to the
+// 7-tap along x.  Coarse row 0 wraps to the top rows and is formed last.
 // Requires n % RPS == 0.
 #define C2G_CW 7
 #define C2G_FC (4 * C2G_CW + 3)
 template <int U>
-__global__ void __launch_bounds__(1024) k_c2g_sparse_sum(const int2 *__restrict__ DP,
+__global__ void __launch_bounds__(1024) k_c2g_packed_sum(const unsigned long long *__restrict__ JW,
                                                          const int *__restrict__ ljx,
                                                          int *__restrict__ C,
                                                          unsigned long long *__restrict__ csum,
@@ -633,36 +633,53 @@ __global__ void __launch_bounds__(1024) k_c2g_sparse_sum(const int2 *__restrict_
   __shared__ int G[RPS][C2G_FC + 2];  // row length 33: conflict-free both ways
   __shared__ int G0[C2G_FC];
   __shared__ long long red[32];
+  const unsigned FULL = 0xffffffffu;
   const int w7[7] = {1, 2, 3, 4, 3, 2, 1};
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int cx0 = blockIdx.x * C2G_CW;
   int col = 4 * cx0 - 3 + warp;  // this warp's fine column (0-based), wrapped
   if (col < 0) col += nf;
   if (col >= nf) col -= nf;
-  const int2 *cp = DP + (long long)col * n + lane;
+  const unsigned long long *cp = JW + (long long)col * n + lane;
   const int nsteps = n / RPS;
-  int2 v[U];
+  unsigned long long v[U];
   if (warp < C2G_FC) {
 #pragma unroll
     for (int u = 0; u < U; u++) v[u] = __ldcs(cp + u * 32);
   }
-  // 16 * lbot(col): the exclusive prefix of the bottom jumps (contours.f90:255-269)
+  // lbot(col): the exclusive prefix of the bottom jumps (contours.f90:255-269)
   int lb = 0;
   if (warp < C2G_FC) {
     for (int i = lane; i < col; i += 32) lb += ljx[i];
-    for (int o = 16; o > 0; o >>= 1) lb += __shfl_xor_sync(0xffffffffu, lb, o);
+    for (int o = 16; o > 0; o >>= 1) lb += __shfl_xor_sync(FULL, lb, o);
   }
-  const int lb16 = 16 * lb;
-  int carry = 0, p0 = 0;
+  int carry = 0, q2 = 0, q3 = 0;       // running total; rows 4cy-2, 4cy-1 below lane 0
+  int f0 = 0, f1 = 0, f2 = 0, f3 = 0;  // word 0 (rows 0..3), kept for coarse row 0
   long long local = 0;
   for (int s = 0; s < nsteps; s++) {
     if (warp < C2G_FC) {
 #pragma unroll
       for (int u = 0; u < U; u++) {
-        const int x = warp_incl_scan(v[u].x) + carry;
-        carry = __shfl_sync(0xffffffffu, x, 31);
-        G[u * 32 + lane][warp] = lb16 + v[u].y + x;
-        if (s == 0 && u == 0 && lane == 0) p0 = v[0].y;
+        int c0, c1, c2, c3;
+        c2g_decode(v[u], c0, c1, c2, c3);
+        const int tot = c0 + c1 + c2 + c3;
+        const int incl = warp_incl_scan(tot) + carry;
+        const int ex = incl - tot;
+        int p2 = __shfl_up_sync(FULL, c2, 1), p3 = __shfl_up_sync(FULL, c3, 1);
+        if (lane == 0) {
+          p2 = q2;
+          p3 = q3;
+        }
+        const int L2 = lb + ex, L1 = L2 - p3, L0 = L1 - p2;
+        const int L3 = L2 + c0, L4 = L3 + c1, L5 = L4 + c2, L6 = L5 + c3;
+        G[u * 32 + lane][warp] =
+            w7[0] * L0 + w7[1] * L1 + w7[2] * L2 + w7[3] * L3 + w7[4] * L4 + w7[5] * L5 + w7[6] * L6;
+        if (s == 0 && u == 0 && lane == 0) {
+          f0 = c0; f1 = c1; f2 = c2; f3 = c3;
+        }
+        carry = __shfl_sync(FULL, incl, 31);
+        q2 = __shfl_sync(FULL, c2, 31);
+        q3 = __shfl_sync(FULL, c3, 31);
       }
       if (s + 1 < nsteps) {
 #pragma unroll
@@ -683,8 +700,14 @@ __global__ void __launch_bounds__(1024) k_c2g_sparse_sum(const int2 *__restrict_
     }
     __syncthreads();
   }
-  // coarse row 0: its stencil wraps to the top rows
-  if (warp < C2G_FC && lane == 0) G0[warp] = lb16 + p0 + 6 * (carry / 16);
+  // coarse row 0: fine rows nf-3, nf-2, nf-1 (the top word: q2, q3 are its
+  // rows nf-2, nf-1; carry is the column total) and rows 0..3 (word 0)
+  if (warp < C2G_FC && lane == 0) {
+    const int L2 = lb + carry, L1 = L2 - q3, L0 = L1 - q2;
+    const int L3 = lb + f0, L4 = L3 + f1, L5 = L4 + f2, L6 = L5 + f3;
+    G0[warp] = w7[0] * L0 + w7[1] * L1 + w7[2] * L2 + w7[3] * L3 + w7[4] * L4 + w7[5] * L5 +
+               w7[6] * L6;
+  }
   __syncthreads();
   if (threadIdx.x < C2G_CW) {
     const int cx = cx0 + threadIdx.x;
@@ -696,12 +719,12 @@ __global__ void __launch_bounds__(1024) k_c2g_sparse_sum(const int2 *__restrict_
       local += acc;
     }
   }
-  for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xffffffffu, local, o);
+  for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(FULL, local, o);
   if (lane == 0) red[warp] = local;
   __syncthreads();
   if (warp == 0) {
     long long x = red[lane];
-    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(FULL, x, o);
     if (lane == 0) atomicAdd(csum, (unsigned long long)x);
   }
 }
@@ -738,25 +761,27 @@ int con2grid_dev(casl_handle *h, bool want_levels) {
   unsigned long long *csum = (unsigned long long *)&h->scal->csum;
   const int n = h->n;
   const int U = n % 128 == 0 ? 4 : (n % 64 == 0 ? 2 : (n % 32 == 0 ? 1 : 0));
-  if (!want_levels && c.nxf == c.nyf && U > 0) {
-    // sparse: jumps and direct terms per (fine column, coarse row), in the
-    // first half of the fine-grid buffer
-    int2 *DP = reinterpret_cast<int2 *>(h->fineJ);
-    CASL_CUDA_TRY(cudaMemsetAsync(DP, 0, (size_t)c.nxf * n * sizeof(int2), h->stream));
+  // packed path while the 16-bit counts cannot overflow (one net crossing
+  // per level and fine edge: levels well below 32767)
+  if (!want_levels && c.nxf == c.nyf && U > 0 && h->p.ncontq < 16384) {
+    // four fine rows of a column per 64-bit word, in the first half of the
+    // fine-grid buffer
+    unsigned long long *JW = reinterpret_cast<unsigned long long *>(h->fineJ);
+    CASL_CUDA_TRY(cudaMemsetAsync(JW, 0, (size_t)c.nxf * n * sizeof(unsigned long long), h->stream));
     CASL_CUDA_TRY(cudaMemsetAsync(h->ljx, 0, (size_t)c.nxf * sizeof(int), h->stream));
     if (h->nptq > 0) {
       CASL_K(k_c2g_scatter<true>, grid_for(h->nptq), 256, 0, h->stream)(
-          h->xq, h->yq, h->nextq, h->scal, nullptr, DP, h->ljx, c, err, csum);
+          h->xq, h->yq, h->nextq, h->scal, nullptr, JW, h->ljx, c, err, csum);
     } else {
       CASL_CUDA_TRY(cudaMemsetAsync(csum, 0, sizeof(unsigned long long), h->stream));
     }
     const int nblk = (n + C2G_CW - 1) / C2G_CW;
     if (U == 4)
-      CASL_K(k_c2g_sparse_sum<4>, nblk, 1024, 0, h->stream)(DP, h->ljx, h->coarseC, csum, n, c.nxf);
+      CASL_K(k_c2g_packed_sum<4>, nblk, 1024, 0, h->stream)(JW, h->ljx, h->coarseC, csum, n, c.nxf);
     else if (U == 2)
-      CASL_K(k_c2g_sparse_sum<2>, nblk, 1024, 0, h->stream)(DP, h->ljx, h->coarseC, csum, n, c.nxf);
+      CASL_K(k_c2g_packed_sum<2>, nblk, 1024, 0, h->stream)(JW, h->ljx, h->coarseC, csum, n, c.nxf);
     else
-      CASL_K(k_c2g_sparse_sum<1>, nblk, 1024, 0, h->stream)(DP, h->ljx, h->coarseC, csum, n, c.nxf);
+      CASL_K(k_c2g_packed_sum<1>, nblk, 1024, 0, h->stream)(JW, h->ljx, h->coarseC, csum, n, c.nxf);
     return check_launch(h);
   }
   // the fine-grid levels themselves are wanted: crossings onto the fine

@@ -93,9 +93,10 @@ def test_con2grid_levels_bit_exact(pair):
 
 @pytest.mark.parametrize("n,k0,levels", [(64, 6.0, 20), (128, 8.0, 30), (256, 8.0, 40)])
 def test_con2grid_fused_matches_oracle(oracle_mod, gpu_lib, n, k0, levels):
-    """con2grid without the fine levels runs the fused column scan +
-    coarsening (8 or 16 chunks of 32 rows per step, by size); its integer
-    coarse cells make qc agree with the oracle to rounding."""
+    """con2grid without the fine levels runs the packed path (four fine
+    rows of a column per 64-bit word of 16-bit jump counts, decoded by the
+    sum kernel into the 7x7 coarse cells); its integer coarse cells make qc
+    agree with the oracle to rounding."""
     from hydra_b200.casl import CaslGPU
     o = oracle_mod.Oracle(n, ncontq=levels, dtmax=0.05)
     o.initialise(random_pv(n, k0, 3))
