@@ -157,7 +157,7 @@ struct LoadDeriv {
   int n;
   __device__ __forceinline__ double base(int b, int kx0, int ky0) const {
     long long k = (long long)ky0 * n + kx0;
-    double v = f[b][k];
+    double v = pick(f, b)[k];
     return green ? green[k] * v : v;
   }
   // first pass of an inverse transform: vector v = ky, element j = kx.
@@ -166,7 +166,7 @@ struct LoadDeriv {
   // and the reflected index (n-k) mod n is always a valid element.
   __device__ __forceinline__ double operator()(int b, int v, int j) const {
     const int nw = n >> 1, kx = j, ky = v;
-    const bool dx = dir[b] == 0;
+    const bool dx = pick(dir, b) == 0;
     const int k = dx ? kx : ky;
     const int kr = (n - k) & (n - 1);
     const int hi = k < nw ? 2 * k - 1 : 2 * (n - k) - 1;
@@ -174,6 +174,25 @@ struct LoadDeriv {
     const double h = hrk[hi < 0 ? 0 : hi];
     const double fac = (k == 0 || k == nw) ? 0.0 : (k < nw ? -h : h);
     return fac * (dx ? base(b, kr, ky) : base(b, kx, kr));
+  }
+  // elements j, j+1 (j even).  For d/dy the factor is the vector's and the
+  // two values are adjacent: one 16-byte load each from f and green.  For
+  // d/dx the reflected indices n-j, n-j-1 run backwards from an odd start,
+  // so they stay two loads.
+  __device__ __forceinline__ double2 pair(int b, int v, int j) const {
+    if (pick(dir, b) == 0) return make_double2((*this)(b, v, j), (*this)(b, v, j + 1));
+    const int nw = n >> 1, k = v;
+    const int kr = (n - k) & (n - 1);
+    const int hi = k < nw ? 2 * k - 1 : 2 * (n - k) - 1;
+    const double h = hrky[hi < 0 ? 0 : hi];
+    const double fac = (k == 0 || k == nw) ? 0.0 : (k < nw ? -h : h);
+    const long long o = (long long)kr * n + j;
+    double2 q = *reinterpret_cast<const double2 *>(pick(f, b) + o);
+    if (green) {
+      const double2 g = *reinterpret_cast<const double2 *>(green + o);
+      q = make_double2(g.x * q.x, g.y * q.y);
+    }
+    return make_double2(fac * q.x, fac * q.y);
   }
 };
 
@@ -219,19 +238,21 @@ struct LoadAdvect {
   int n;
   __device__ __forceinline__ double operator()(int b, int v /*ix*/, int j /*iy*/) const {
     long long k = (long long)v * n + j;
-    double gx = fx[b][k], gy = fy[b][k];
-    if (betab[b] != 0.0) gy = gy + betab[b];
+    const double bb = pick(betab, b);
+    double gx = pick(fx, b)[k], gy = pick(fy, b)[k];
+    if (bb != 0.0) gy = gy + bb;
     return -uu[k] * gx - vv[k] * gy;
   }
   __device__ __forceinline__ double2 pair(int b, int v, int j) const {
     long long k = (long long)v * n + j;
-    const double2 gx = *reinterpret_cast<const double2 *>(fx[b] + k);
-    double2 gy = *reinterpret_cast<const double2 *>(fy[b] + k);
+    const double bb = pick(betab, b);
+    const double2 gx = *reinterpret_cast<const double2 *>(pick(fx, b) + k);
+    double2 gy = *reinterpret_cast<const double2 *>(pick(fy, b) + k);
     const double2 u = *reinterpret_cast<const double2 *>(uu + k);
     const double2 w = *reinterpret_cast<const double2 *>(vv + k);
-    if (betab[b] != 0.0) {
-      gy.x = gy.x + betab[b];
-      gy.y = gy.y + betab[b];
+    if (bb != 0.0) {
+      gy.x = gy.x + bb;
+      gy.y = gy.y + bb;
     }
     return make_double2(-u.x * gx.x - w.x * gy.x, -u.y * gx.y - w.y * gy.y);
   }
@@ -302,6 +323,104 @@ struct StoreSource {
       qd[idx] = emq[idx] * (qdf[idx] + sc->dt6 * bb);
     }
   }
+  // elements idx, idx+1 with 16-byte accesses; per element the expressions
+  // and their order are operator()'s
+  __device__ __forceinline__ void pair(int b, int v, int k, double2 x) const {
+    const long long i = (long long)v * n + k;
+    const double a[2] = {x.x, x.y};
+    auto L = [i](const double *p, double(&o)[2]) {
+      const double2 t = *reinterpret_cast<const double2 *>(p + i);
+      o[0] = t.x;
+      o[1] = t.y;
+    };
+    auto S = [i](double *p, const double(&o)[2]) {
+      *reinterpret_cast<double2 *>(p + i) = make_double2(o[0], o[1]);
+    };
+    double u[2], r[2], w[2];
+    if (b == 1) {
+      if (stage == 1) {
+        L(qs, u);
+        S(qsi, u);
+        for (int e = 0; e < 2; e++) r[e] = u[e] + sc->dt2 * a[e];
+        for (int e = 0; e < 2; e++) w[e] = u[e] + sc->dt6 * a[e];
+        S(qs, r);
+        S(qsf, w);
+      } else if (stage == 2) {
+        L(qsi, u);
+        for (int e = 0; e < 2; e++) r[e] = u[e] + sc->dt2 * a[e];
+        S(qs, r);
+        L(qsf, u);
+        for (int e = 0; e < 2; e++) w[e] = u[e] + sc->dt3 * a[e];
+        S(qsf, w);
+      } else if (stage == 3) {
+        L(qsi, u);
+        for (int e = 0; e < 2; e++) r[e] = u[e] + sc->dt * a[e];
+        S(qs, r);
+        L(qsf, u);
+        for (int e = 0; e < 2; e++) w[e] = u[e] + sc->dt3 * a[e];
+        S(qsf, w);
+      } else {
+        L(qsf, u);
+        for (int e = 0; e < 2; e++) r[e] = u[e] + sc->dt6 * a[e];
+        S(qs, r);
+      }
+      return;
+    }
+    double t[2], p2[2], q2[2];
+    L(pp, p2);
+    if (heating) {
+      if (friction) {
+        L(qq, q2);
+        for (int e = 0; e < 2; e++)
+          t[e] = a[e] + therm * (p2[e] - 0.0) - rekman * (q2[e] + kdsq * p2[e]);
+      } else {
+        for (int e = 0; e < 2; e++) t[e] = a[e] + therm * (p2[e] - 0.0);
+      }
+    } else {
+      L(qq, q2);
+      for (int e = 0; e < 2; e++) t[e] = a[e] - rekman * (q2[e] + kdsq * p2[e]);
+    }
+    if (lev == 1) {
+      L(epq, u);
+      for (int e = 0; e < 2; e++) t[e] = u[e] * t[e];
+    } else if (lev == 2) {
+      L(epq, u);
+      for (int e = 0; e < 2; e++) t[e] = u[e] * u[e] * t[e];
+    }
+    double em[2];
+    if (stage == 1) {
+      L(qd, u);
+      L(emq, em);
+      S(qdi, u);
+      for (int e = 0; e < 2; e++) r[e] = em[e] * (u[e] + sc->dt2 * t[e]);
+      for (int e = 0; e < 2; e++) w[e] = u[e] + sc->dt6 * t[e];
+      S(qd, r);
+      S(qdf, w);
+    } else if (stage == 2) {
+      L(qdi, u);
+      L(emq, em);
+      for (int e = 0; e < 2; e++) r[e] = em[e] * (u[e] + sc->dt2 * t[e]);
+      S(qd, r);
+      L(qdf, u);
+      for (int e = 0; e < 2; e++) w[e] = u[e] + sc->dt3 * t[e];
+      S(qdf, w);
+    } else if (stage == 3) {
+      L(emq, em);
+      for (int e = 0; e < 2; e++) em[e] = em[e] * em[e];
+      S(emq, em);
+      L(qdi, u);
+      for (int e = 0; e < 2; e++) r[e] = em[e] * (u[e] + sc->dt * t[e]);
+      S(qd, r);
+      L(qdf, u);
+      for (int e = 0; e < 2; e++) w[e] = u[e] + sc->dt3 * t[e];
+      S(qdf, w);
+    } else {
+      L(qdf, u);
+      L(emq, em);
+      for (int e = 0; e < 2; e++) r[e] = em[e] * (u[e] + sc->dt6 * t[e]);
+      S(qd, r);
+    }
+  }
 };
 
 // Last store of con2grid's forward transform with the filter combination
@@ -353,12 +472,13 @@ struct StoreScaled {
   int n;
   // last pass of an inverse transform: vector v = ix, element k = iy
   __device__ __forceinline__ void operator()(int b, int v, int k, double x) const {
-    p[b][(long long)v * n + k] = scale[b] == 1.0 ? x : scale[b] * x;
+    const double sc = pick(scale, b);
+    pick(p, b)[(long long)v * n + k] = sc == 1.0 ? x : sc * x;
   }
   __device__ __forceinline__ void pair(int b, int v, int k, double2 x) const {
-    const double sc = scale[b];
+    const double sc = pick(scale, b);
     if (sc != 1.0) x = make_double2(sc * x.x, sc * x.y);
-    *reinterpret_cast<double2 *>(p[b] + (long long)v * n + k) = x;
+    *reinterpret_cast<double2 *>(pick(p, b) + (long long)v * n + k) = x;
   }
 };
 struct LoadBatch {
@@ -366,7 +486,7 @@ struct LoadBatch {
   const double *p[4];
   long long vs, es;
   __device__ __forceinline__ double operator()(int b, int v, int j) const {
-    return p[b][(long long)v * vs + (long long)j * es];
+    return pick(p, b)[(long long)v * vs + (long long)j * es];
   }
 };
 // Load qq + kdsq*pp (adapt, evolution.f90:541-547).

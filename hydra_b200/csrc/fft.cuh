@@ -86,6 +86,19 @@ struct has_pair : std::false_type {};
 template <class T>
 struct has_pair<T, std::void_t<decltype(&T::pair)>> : std::true_type {};
 
+// a[b] for a functor's small per-batch array without indexing it at run
+// time: an indexed kernel-parameter array is copied to local memory and
+// every use costs a local load in front of the global one; the unrolled
+// select keeps the entries in the parameter bank.
+template <class T, int N>
+__device__ __forceinline__ T pick(const T (&a)[N], int b) {
+  T r = a[0];
+#pragma unroll
+  for (int i = 1; i < N; i++)
+    if (b == i) r = a[i];
+  return r;
+}
+
 // Plain strided load / store functors: element (b, v, j) at p[b*bs + v*vs + j*es].
 struct LoadStrided {
   __host__ double bytes() const { return 8.0; }
