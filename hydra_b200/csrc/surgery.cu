@@ -47,7 +47,15 @@ struct SurgState {
   const int *kb1, *bcnt, *bnode;       // segment lists per box
   const int *nb1, *nbcnt, *nbnode;     // nodes located per box
   unsigned char *pending;
+  // one bit per window of 512 nodes (a word per 16384) set wherever a
+  // pending flag is set, so the replay skips empty windows a word at a time
+  unsigned int *wsum;
 };
+
+__device__ __forceinline__ void set_pending(const SurgState &S, int x) {
+  S.pending[x] = 1;
+  atomicOr(&S.wsum[x >> 14], 1u << ((x >> 9) & 31));
+}
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
@@ -289,11 +297,12 @@ __global__ void k_sg_candidates(SurgState S, const LevelDesc *__restrict__ lev, 
                       S.dx0[is] * S.dx0[is] + S.dy0[is] * S.dy0[is], c);
     }
     S.pending[ib] = hit ? 1 : 0;
+    if (hit) atomicOr(&S.wsum[ib >> 14], 1u << ((ib >> 9) & 31));
   }
 }
 
 __device__ __forceinline__ void mark(SurgState &S, int x, int ib, int iend) {
-  if (x > ib && x <= iend) S.pending[x] = 1;
+  if (x > ib && x <= iend) set_pending(S, x);
 }
 
 // Mark every later node whose tests may read node j's changed data.  Called
@@ -340,6 +349,21 @@ __global__ void k_sg_replay(SurgState S, const LevelDesc *__restrict__ lev,
   long long pos = L.ibeg;
   while (pos <= L.iend) {
     int ib;
+    {
+      // skip the 512-node windows whose summary bit is clear (read from L2:
+      // this warp's own marks arrive there by atomics)
+      const long long W = pos >> 9;
+      const unsigned sw = __ldcg(&S.wsum[W >> 5]) >> (W & 31);
+      if (!sw) {
+        pos = ((W >> 5) + 1) << 14;
+        continue;
+      }
+      const int d = __ffs(sw) - 1;
+      if (d > 0) {
+        pos = (W + d) << 9;
+        if (pos > L.iend) break;
+      }
+    }
     // Windows start at the 16-aligned position at or below pos, so the wide
     // path is taken whatever the level's first node; flags below pos (already
     // visited, or another level's) are masked out.
@@ -739,6 +763,7 @@ int surgery_dev(casl_handle *h) {
   double *dx0 = ar.get<double>(npt), *dy0 = ar.get<double>(npt);
   int *nq0 = ar.get<int>(npt), *prev0 = ar.get<int>(npt);
   unsigned char *pending = ar.get<unsigned char>(npt + 16);
+  unsigned int *wsum = ar.get<unsigned int>((npt >> 14) + 2);
   int *ecount = ar.get<int>(npt), *eoff = ar.get<int>(npt), *nbox_of = ar.get<int>(npt);
   int *bcnt = ar.get<int>(nbox_cap), *kb1 = ar.get<int>(nbox_cap), *cursor = ar.get<int>(nbox_cap);
   int *nbcnt = ar.get<int>(nbox_cap), *nb1 = ar.get<int>(nbox_cap), *nbnode = ar.get<int>(npt);
@@ -762,6 +787,8 @@ int surgery_dev(casl_handle *h) {
   S.xq = h->xq; S.yq = h->yq; S.dx = dx; S.dy = dy; S.dsq = dsq; S.nextq = h->nextq;
   S.x0 = x0; S.y0 = y0; S.dx0 = dx0; S.dy0 = dy0; S.nq0 = nq0; S.prev0 = prev0; S.lvl = lvl;
   S.pending = pending;
+  S.wsum = wsum;
+  CASL_CUDA_TRY(cudaMemsetAsync(wsum, 0, ((npt >> 14) + 2) * sizeof(unsigned int), st));
   CASL_K(k_sg_count_entries, g, 256, 0, st)(S, dlev, npt, ecount, nbox_of, nbcnt, c);
   exclusive_scan<int>(st, ecount, eoff, npt, tmpi, dtot + 2);
   CASL_K(k_sg_emit, g, 256, 0, st)(S, dlev, npt, eoff, ecount, ne_cap, ebox, eib, bcnt, c, err);
