@@ -149,16 +149,26 @@ int spctop_dev(casl_handle *h, const double *spec, double *phys, double *tmp) {
 // a spectral field, optionally of green*field (main_invert, spectral.f90:321).
 // Batch index b selects field and direction.
 struct LoadDeriv {
-  __host__ double bytes() const { return green ? 16.0 : 8.0; }
-  const double *f[4];
-  int dir[4];  // 0: d/dx, 1: d/dy
+  // bytes per element, averaged over the batch's entries
+  __host__ double bytes() const {
+    int nb = 0, ng = 0;
+    for (int b = 0; b < 6; b++)
+      if (f[b]) {
+        nb++;
+        ng += wg[b];
+      }
+    return nb ? 8.0 + 8.0 * ng / nb : 8.0;
+  }
+  const double *f[6];
+  int dir[6];  // 0: d/dx, 1: d/dy
+  int wg[6];   // 1: entry multiplied by the Green function
   const double *green;
   const double *hrkx, *hrky;
   int n;
   __device__ __forceinline__ double base(int b, int kx0, int ky0) const {
     long long k = (long long)ky0 * n + kx0;
     double v = pick(f, b)[k];
-    return green ? green[k] * v : v;
+    return pick(wg, b) ? green[k] * v : v;
   }
   // first pass of an inverse transform: vector v = ky, element j = kx.
   // Branch-free, so that a thread's loads are issued together: the factor
@@ -188,7 +198,7 @@ struct LoadDeriv {
     const double fac = (k == 0 || k == nw) ? 0.0 : (k < nw ? -h : h);
     const long long o = (long long)kr * n + j;
     double2 q = *reinterpret_cast<const double2 *>(pick(f, b) + o);
-    if (green) {
+    if (pick(wg, b)) {
       const double2 g = *reinterpret_cast<const double2 *>(green + o);
       q = make_double2(g.x * q.x, g.y * q.y);
     }
@@ -467,8 +477,8 @@ struct StoreCombine {
 
 struct StoreScaled {
   __host__ double bytes() const { return 8.0; }
-  double *p[4];
-  double scale[4];
+  double *p[6];
+  double scale[6];
   int n;
   // last pass of an inverse transform: vector v = ix, element k = iy
   __device__ __forceinline__ void operator()(int b, int v, int k, double x) const {
@@ -483,7 +493,7 @@ struct StoreScaled {
 };
 struct LoadBatch {
   __host__ double bytes() const { return 8.0; }
-  const double *p[4];
+  const double *p[6];
   long long vs, es;
   __device__ __forceinline__ double operator()(int b, int v, int j) const {
     return pick(p, b)[(long long)v * vs + (long long)j * es];
@@ -553,14 +563,24 @@ __global__ void k_c2g_scatter(const double *__restrict__ xq, const double *__res
     const int i = base + lane;
     int cnt = 0, ixbeg = 0, jump = 0, sgn = 0;
     double xi = 0.0, yi = 0.0, dx = 1.0, dy = 0.0;
+    // the segment's far end is almost always the next node, which the next
+    // lane has loaded: taken by shuffle, so the loads do not wait on nextq
+    int ia = -1;
+    double x1 = 0.0, y1 = 0.0;
     if (i < npt) {
-      const int ia = nextq[i];
+      ia = nextq[i];
+      x1 = xq[i];
+      y1 = yq[i];
+    }
+    const double xs = __shfl_down_sync(FULL, x1, 1), ys = __shfl_down_sync(FULL, y1, 1);
+    if (i < npt) {
       if (ia < 0 || ia >= npt) {
         atomicExch(err, CASL_EINVAL);
       } else {
-        xi = xq[i];
-        yi = yq[i];
-        const double xa = xq[ia], ya = yq[ia];
+        xi = x1;
+        yi = y1;
+        const bool nb = ia == i + 1 && lane < 31;
+        const double xa = nb ? xs : xq[ia], ya = nb ? ys : yq[ia];
         if (!(xi >= c.xmin && xi < c.xmax && yi >= c.ymin && yi < c.ymax)) {
           atomicExch(err, CASL_EDOMAIN);
         } else {
@@ -1197,6 +1217,7 @@ static int main_invert_dev(casl_handle *h) {
   LoadDeriv ld{};
   ld.f[0] = h->qq; ld.f[1] = h->qq;
   ld.dir[0] = 0; ld.dir[1] = 1;
+  ld.wg[0] = 1; ld.wg[1] = 1;
   ld.green = h->green; ld.hrkx = h->hrkx; ld.hrky = h->hrky; ld.n = h->n;
   long long n = h->n;
   rc = RFFT_DISPATCH(false, false, false, ld, (StoreStrided{h->w[0], nn, n, 1}), 2);
@@ -1208,6 +1229,38 @@ static int main_invert_dev(casl_handle *h) {
   LoadBatch lb{};
   lb.p[0] = h->w[0]; lb.p[1] = h->w[0] + nn; lb.vs = 1; lb.es = n;
   return RFFT_DISPATCH(false, true, false, lb, st, 2);
+}
+
+// main_invert and the four gradients of source (evolution.f90:432-490,
+// spectral.f90:304-366) as one batch-6 inverse transform pair: vv, uu from
+// green*qq, and the x/y derivatives of qd (into w[4], w[5]) and of qs (into
+// sqs, sqd, as scratch for the advection products).  One batch of six fills
+// the SMs better than a batch of two beside a batch of four.  Scratch:
+// gtmp (6 fields).
+static int invert_and_gradients(casl_handle *h) {
+  long long nn = (long long)h->n * h->n, n = h->n;
+  LoadDeriv ld{};
+  const double *src[6] = {h->qq, h->qq, h->qd, h->qd, h->qs, h->qs};
+  for (int b = 0; b < 6; b++) {
+    ld.f[b] = src[b];
+    ld.dir[b] = b & 1;
+    ld.wg[b] = b < 2;
+  }
+  ld.green = h->green; ld.hrkx = h->hrkx; ld.hrky = h->hrky; ld.n = h->n;
+  double *tmp = h->gtmp;  // 6 contiguous fields
+  int rc = RFFT_DISPATCH(false, false, false, ld, (StoreStrided{tmp, nn, n, 1}), 6);
+  if (rc) return rc;
+  LoadBatch lb{};
+  for (int b = 0; b < 6; b++) lb.p[b] = tmp + b * nn;
+  lb.vs = 1; lb.es = n;
+  StoreScaled st{};
+  double *dst[6] = {h->vv, h->uu, h->w[4], h->w[5], h->sqs, h->sqd};
+  for (int b = 0; b < 6; b++) {
+    st.p[b] = dst[b];
+    st.scale[b] = b == 1 ? -1.0 : 1.0;
+  }
+  st.n = h->n;
+  return RFFT_DISPATCH(false, true, false, lb, st, 6);
 }
 
 int inversion_dev(casl_handle *h, bool reset) {
@@ -1230,33 +1283,9 @@ static int adapt_dev(casl_handle *h) {
   return check_launch(h);
 }
 
-// source (evolution.f90:432-490): gradients of qd and qs (4 spctop in one
-// batched pair of launches), the advection products fused into ptospc's
-// first pass, damping and integrating factor fused into its last store.
-// The gradients of qd and qs (4 spctop in one batched pair of launches) into
-// w[4], w[5], sqs, sqd; they read only qd and qs, so advance runs them on the
-// second stream beside the inversion.  Scratch: gtmp (4 fields).
-static int source_grad(casl_handle *h) {
-  long long nn = (long long)h->n * h->n, n = h->n;
-  LoadDeriv ld{};
-  ld.f[0] = h->qd; ld.f[1] = h->qd; ld.f[2] = h->qs; ld.f[3] = h->qs;
-  ld.dir[0] = 0; ld.dir[1] = 1; ld.dir[2] = 0; ld.dir[3] = 1;
-  ld.green = nullptr; ld.hrkx = h->hrkx; ld.hrky = h->hrky; ld.n = h->n;
-  double *tmp = h->gtmp;  // 4 contiguous fields
-  int rc = RFFT_DISPATCH(false, false, false, ld, (StoreStrided{tmp, nn, n, 1}), 4);
-  if (rc) return rc;
-  LoadBatch lb{};
-  for (int b = 0; b < 4; b++) lb.p[b] = tmp + b * nn;
-  lb.vs = 1; lb.es = n;
-  StoreScaled st{};
-  st.p[0] = h->w[4]; st.p[1] = h->w[5]; st.p[2] = h->sqs; st.p[3] = h->sqd;
-  for (int b = 0; b < 4; b++) st.scale[b] = 1.0;
-  st.n = h->n;
-  return RFFT_DISPATCH(false, true, false, lb, st, 4);
-}
-
-// The rest of source (evolution.f90:432-490): the advection products fused
-// into ptospc's first pass, damping and integrating factor into its store.
+// source (evolution.f90:432-490) after its gradients (invert_and_gradients):
+// the advection products fused into ptospc's first pass, damping, the
+// integrating factor and the spectral RK update into its store.
 static int source_prod(casl_handle *h, int stage) {
   const int lev = stage == 1 ? 0 : (stage == 4 ? 2 : 1);
   long long nn = (long long)h->n * h->n, n = h->n;
@@ -1283,34 +1312,6 @@ static int source_prod(casl_handle *h, int stage) {
 
 }  // namespace casl
 
-// advance (evolution.f90:166-326)
-// advance on two streams.  The side stream runs the four gradient
-// transforms of source (they read only qs and qd) beside con2grid and the
-// inversion, which are latency-bound.  Events: ev_fork marks a point of the
-// main stream the side stream waits for, ev_grad the gradients' end.
-static int side_after_main(casl_handle *h) {
-  CASL_CUDA_TRY(cudaEventRecord(h->ev_fork, h->stream));
-  CASL_CUDA_TRY(cudaStreamWaitEvent(h->stream2, h->ev_fork, 0));
-  return CASL_OK;
-}
-
-static int on_side(casl_handle *h, int (*fn)(casl_handle *, int), int arg, cudaEvent_t done) {
-  cudaStream_t a = h->stream;
-  h->stream = h->stream2;
-  int rc = fn(h, arg);
-  h->stream = a;
-  if (rc) return rc;
-  CASL_CUDA_TRY(cudaEventRecord(done, h->stream2));
-  return CASL_OK;
-}
-
-static int main_after(casl_handle *h, cudaEvent_t ev) {
-  CASL_CUDA_TRY(cudaStreamWaitEvent(h->stream, ev, 0));
-  return CASL_OK;
-}
-
-static int grad_task(casl_handle *h, int) { return source_grad(h); }
-
 static int nodes_task(casl_handle *h, int stage) {
   if (!h->contex) return CASL_OK;
   int gn = grid_for(h->nptq > 0 ? h->nptq : 1);
@@ -1324,26 +1325,18 @@ static int nodes_task(casl_handle *h, int stage) {
   return check_launch(h);
 }
 
-
+// advance (evolution.f90:166-326): four RK4 stages, each con2grid + the
+// filter combination, the batched inversion + source gradients, (stage 1)
+// adapt, source with the spectral update, and the node update.
 static int advance_dev(casl_handle *h) {
   int rc;
   for (int stage = 1; stage <= 4; stage++) {
-    if (stage == 1) {
-      // the reset inside the filter combination rewrites qs and qd, so the
-      // gradients start after it
-      if ((rc = inversion_qq(h, true))) return rc;
-      if ((rc = side_after_main(h))) return rc;
-      if ((rc = on_side(h, grad_task, 0, h->ev_grad))) return rc;
-    } else {
-      // gradients as soon as the previous spectral update is done
-      if ((rc = side_after_main(h))) return rc;
-      if ((rc = on_side(h, grad_task, 0, h->ev_grad))) return rc;
-      if (stage == 2 || stage == 4) CASL_K(k_advance_time, 1, 1, 0, h->stream)(h->scal);
-      if ((rc = inversion_qq(h, false))) return rc;
-    }
-    if ((rc = main_invert_dev(h))) return rc;
+    if (stage == 2 || stage == 4) CASL_K(k_advance_time, 1, 1, 0, h->stream)(h->scal);
+    // stage 1: the reset inside the filter combination rewrites qs and qd
+    // before the gradients read them
+    if ((rc = inversion_qq(h, stage == 1))) return rc;
+    if ((rc = invert_and_gradients(h))) return rc;
     if (stage == 1 && (rc = adapt_dev(h))) return rc;
-    if ((rc = main_after(h, h->ev_grad))) return rc;
     if ((rc = source_prod(h, stage))) return rc;  // with the spectral RK update
     if ((rc = nodes_task(h, stage))) return rc;
   }
@@ -1750,10 +1743,7 @@ static int alloc_all(casl_handle *h) {
   CASL_CUDA_TRY(cudaMalloc(&h->bety, n * sizeof(double)));
   CASL_CUDA_TRY(cudaMalloc(&h->betac, n * sizeof(double)));
   CASL_CUDA_TRY(cudaMalloc(&h->tw, n * sizeof(double2)));
-  CASL_CUDA_TRY(cudaMalloc(&h->gtmp, (size_t)4 * nn * sizeof(double)));
-  CASL_CUDA_TRY(cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking));
-  CASL_CUDA_TRY(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
-  CASL_CUDA_TRY(cudaEventCreateWithFlags(&h->ev_grad, cudaEventDisableTiming));
+  CASL_CUDA_TRY(cudaMalloc(&h->gtmp, (size_t)6 * nn * sizeof(double)));
   CASL_CUDA_TRY(cudaMalloc(&h->shell_idx, (size_t)nn * sizeof(int)));
   CASL_CUDA_TRY(cudaMalloc(&h->shell_off, (size_t)(2 * n + 2) * sizeof(int)));
   CASL_CUDA_TRY(cudaMalloc(&h->rkxf, n * sizeof(double)));
@@ -1777,12 +1767,6 @@ static void free_all(casl_handle *h) {
                   h->qdf, h->green, h->flo, h->fhi, h->qdiss, h->w[0], h->hrkx, h->hrky,
                   h->bety, h->betac, h->tw, h->fineJ, h->ljx, h->coarseC, h->part, h->scal,
                   h->sx, h->sx2, h->shell_idx, h->shell_off, h->rkxf, h->rkyf, h->gtmp};
-  if (h->stream2) {
-    cudaStreamSynchronize(h->stream2);
-    cudaStreamDestroy(h->stream2);
-  }
-  if (h->ev_fork) cudaEventDestroy(h->ev_fork);
-  if (h->ev_grad) cudaEventDestroy(h->ev_grad);
   for (void *p : ptrs)
     if (p) cudaFree(p);
   free(h->spmf_h);
@@ -2133,6 +2117,7 @@ int casl_main_invert(casl_handle *h, const double *qq, double *uu, double *vv, d
   long long n = h->n;
   LoadDeriv ld{};
   ld.f[0] = q; ld.f[1] = q; ld.dir[0] = 0; ld.dir[1] = 1;
+  ld.wg[0] = 1; ld.wg[1] = 1;
   ld.green = h->green; ld.hrkx = h->hrkx; ld.hrky = h->hrky; ld.n = h->n;
   int rc = RFFT_DISPATCH(false, false, false, ld, (StoreStrided{h->w[0], (long long)nn, n, 1}), 2);
   if (rc) return rc;

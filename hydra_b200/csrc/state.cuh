@@ -14,9 +14,7 @@ struct casl_handle {
   casl::Consts c;
   int device;
   cudaStream_t stream;
-  cudaStream_t stream2;          // side stream of advance (source gradients)
-  cudaEvent_t ev_fork, ev_grad;  // synchronisation between the two
-  double *gtmp;                  // 4 fields of scratch for the side stream
+  double *gtmp;                  // 6 fields of scratch for the batched inversion + gradients
   int last_cuda;
   int n;                 // nx == ny
   long long npm, nm;     // capacities
