@@ -552,6 +552,7 @@ __global__ void k_c2g_scatter(const double *__restrict__ xq, const double *__res
                               int *__restrict__ ljx,
                               Consts c, int *__restrict__ err,
                               unsigned long long *__restrict__ csum) {
+  CASL_PDL_ENTRY();
   // the coarsening that follows accumulates the coarse-cell sum here
   if (blockIdx.x == 0 && threadIdx.x == 0) *csum = 0;
   const unsigned FULL = 0xffffffffu;
@@ -655,6 +656,7 @@ __global__ void k_c2g_scatter(const double *__restrict__ xq, const double *__res
 
 // qbot: exclusive prefix of the bottom jumps along x -> row 0 of each column.
 __global__ void k_c2g_lbot(const int *__restrict__ ljx, int *__restrict__ J, int nxf, int nyf) {
+  CASL_PDL_ENTRY();
   __shared__ int warp_tot[32];
   __shared__ int carry;
   if (threadIdx.x == 0) carry = 0;
@@ -692,6 +694,7 @@ __global__ void k_c2g_lbot(const int *__restrict__ ljx, int *__restrict__ J, int
 // Inclusive scan down every fine column (contours.f90:272-277), in place:
 // J(row, col) -> level L(iy = row+1, ix = col+1).  One warp per column.
 __global__ void k_c2g_colscan(int *__restrict__ J, int nxf, int nyf) {
+  CASL_PDL_ENTRY();
   int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
   if (warp >= nxf) return;
@@ -716,6 +719,7 @@ __global__ void k_c2g_colscan(int *__restrict__ J, int nxf, int nyf) {
 // the exact integer C; the mean is removed exactly from the integer sum.
 __global__ void k_c2g_coarsen(const int *__restrict__ L, int *__restrict__ C,
                               unsigned long long *__restrict__ csum, int n, int nf) {
+  CASL_PDL_ENTRY();
   const int w7[7] = {1, 2, 3, 4, 3, 2, 1};
   long long local = 0;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)n * n;
@@ -769,6 +773,7 @@ __global__ void __launch_bounds__(1024) k_c2g_packed_sum(const unsigned long lon
                                                          int *__restrict__ C,
                                                          unsigned long long *__restrict__ csum,
                                                          int n, int nf) {
+  CASL_PDL_ENTRY();
   constexpr int RPS = 32 * U;
   __shared__ int G[RPS][C2G_FC + 2];  // row length 33: conflict-free both ways
   __shared__ int G0[C2G_FC];
@@ -873,6 +878,7 @@ __global__ void __launch_bounds__(1024) k_c2g_packed_sum(const unsigned long lon
 // c = a * b elementwise
 __global__ void k_mul2(const double *__restrict__ a, const double *__restrict__ b,
                        double *__restrict__ c, long long nn) {
+  CASL_PDL_ENTRY();
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nn;
        k += (long long)gridDim.x * blockDim.x)
     c[k] = a[k] * b[k];
@@ -880,6 +886,7 @@ __global__ void k_mul2(const double *__restrict__ a, const double *__restrict__ 
 
 __global__ void k_c2g_final(const int *__restrict__ C, const Scalars *__restrict__ s,
                             const double *__restrict__ betac, double *__restrict__ qc, int n) {
+  CASL_PDL_ENTRY();
   LoadQC ld{C, s, betac, (long long)n * n, 1.0 / (256.0 * (double)n * (double)n), n};
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)n * n;
        t += (long long)gridDim.x * blockDim.x) {
@@ -1004,6 +1011,7 @@ __device__ __forceinline__ void velint1(double x, double y, const double *__rest
 __global__ void k_velint(const double *__restrict__ xq, const double *__restrict__ yq, int npt,
                          const double *__restrict__ uu, const double *__restrict__ vv,
                          double *__restrict__ uq, double *__restrict__ vq, Consts c) {
+  CASL_PDL_ENTRY();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npt; i += gridDim.x * blockDim.x) {
     double u, v;
     velint1(xq[i], yq[i], uu, vv, c, u, v);
@@ -1018,6 +1026,7 @@ __global__ void k_nodes_rk(double *__restrict__ xq, double *__restrict__ yq,
                            double *__restrict__ xqf, double *__restrict__ yqf,
                            const double *__restrict__ uu, const double *__restrict__ vv,
                            const Scalars *__restrict__ s, Consts c) {
+  CASL_PDL_ENTRY();
   const int npt = s->nptq;
   const double dt = s->dt, dt2 = s->dt2, dt3 = s->dt3, dt6 = s->dt6;
   const double ex = c.ellx, ey = c.elly, hx = c.hlxi, hy = c.hlyi, oms = c.oms;
@@ -1061,6 +1070,7 @@ __global__ void k_combine(double *__restrict__ qs, double *__restrict__ qd,
                           double *__restrict__ pp, const double *__restrict__ flo,
                           const double *__restrict__ fhi, const double *__restrict__ green,
                           long long nn) {
+  CASL_PDL_ENTRY();
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nn;
        k += (long long)gridDim.x * blockDim.x) {
     double s = qs[k], c = qc[k], d = qd[k];
@@ -1082,6 +1092,7 @@ __global__ void k_combine(double *__restrict__ qs, double *__restrict__ qd,
 __global__ void k_reduce_adapt(const double *__restrict__ zz, const double *__restrict__ uu,
                                const double *__restrict__ vv, double *__restrict__ part,
                                long long nn) {
+  CASL_PDL_ENTRY();
   double sum = 0.0, zmax = 0.0, umax = 0.0;
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nn;
        k += (long long)gridDim.x * blockDim.x) {
@@ -1114,6 +1125,7 @@ __global__ void k_reduce_adapt(const double *__restrict__ zz, const double *__re
 
 __global__ void k_adapt_final(const double *__restrict__ part, int nparts, Scalars *s, Consts c,
                               double fixed_dt) {
+  CASL_PDL_ENTRY();
   __shared__ double s0[256], s1[256], s2[256];
   double a = 0.0, b = 0.0, d = 0.0;
   for (int i = threadIdx.x; i < nparts; i += blockDim.x) {
@@ -1159,6 +1171,7 @@ __global__ void k_adapt_final(const double *__restrict__ part, int nparts, Scala
 
 __global__ void k_epq(const double *__restrict__ qdiss, double *__restrict__ epq,
                       double *__restrict__ emq, const Scalars *__restrict__ s, long long nn) {
+  CASL_PDL_ENTRY();
   const double dfac = s->dt2 * s->zzrms;
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nn;
        k += (long long)gridDim.x * blockDim.x) {
@@ -1168,9 +1181,12 @@ __global__ void k_epq(const double *__restrict__ qdiss, double *__restrict__ epq
   }
 }
 
-__global__ void k_advance_time(Scalars *s) { s->t = s->t + s->dt2; }
-__global__ void k_twist_sub(Scalars *s, double twistmax) { s->twist = s->twist - twistmax; }
-__global__ void k_twist_zero(Scalars *s) { s->twist = 0.0; }
+__global__ void k_advance_time(Scalars *s) {
+  CASL_PDL_ENTRY(); s->t = s->t + s->dt2; }
+__global__ void k_twist_sub(Scalars *s, double twistmax) {
+  CASL_PDL_ENTRY(); s->twist = s->twist - twistmax; }
+__global__ void k_twist_zero(Scalars *s) {
+  CASL_PDL_ENTRY(); s->twist = 0.0; }
 
 // ---------------------------------------------------------------------------
 // Stages
@@ -1607,6 +1623,7 @@ int ensure_scratch2(casl_handle *h, size_t bytes) {
 // ---------------------------------------------------------------------------
 __global__ void k_diag_sumsq2(const double *__restrict__ a, const double *__restrict__ b,
                               double *__restrict__ part, long long nn) {
+  CASL_PDL_ENTRY();
   double s = 0.0;
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nn;
        k += (long long)gridDim.x * blockDim.x) {
@@ -1624,6 +1641,7 @@ __global__ void k_diag_sumsq2(const double *__restrict__ a, const double *__rest
   if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
 }
 __global__ void k_diag_final(const double *__restrict__ part, int np, double *__restrict__ out) {
+  CASL_PDL_ENTRY();
   __shared__ double sh[256];
   double s = 0.0;
   for (int i = threadIdx.x; i < np; i += blockDim.x) s += part[i];
@@ -1638,6 +1656,7 @@ __global__ void k_diag_final(const double *__restrict__ part, int np, double *__
 __global__ void k_diag_incr(const double *__restrict__ xq, const double *__restrict__ yq,
                             const int *__restrict__ nextq, int npt, double *__restrict__ dx,
                             double *__restrict__ dy, int *__restrict__ head, Consts c) {
+  CASL_PDL_ENTRY();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npt; i += gridDim.x * blockDim.x) {
     int a = nextq[i];
     double xx = xq[a] - xq[i];
@@ -1648,6 +1667,7 @@ __global__ void k_diag_incr(const double *__restrict__ xq, const double *__restr
   }
 }
 __global__ void k_diag_heads(const int *__restrict__ i1q, int nq, int *__restrict__ head) {
+  CASL_PDL_ENTRY();
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nq; j += gridDim.x * blockDim.x)
     head[i1q[j]] = 1;
 }
@@ -1658,6 +1678,7 @@ __global__ void k_diag_heads(const int *__restrict__ i1q, int nq, int *__restric
 // w = 1/4 for the mean, 1/2 for the kx = 0 and ky = 0 modes.
 __global__ void k_spec1d(const double *__restrict__ ss, const int *__restrict__ off,
                          const int *__restrict__ idx, int nx, int kmax, double *__restrict__ spec) {
+  CASL_PDL_ENTRY();
   const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (k > kmax) return;
   double acc = 0.0;
@@ -1674,6 +1695,7 @@ __global__ void k_spec1d(const double *__restrict__ ss, const int *__restrict__ 
 // ss <- ss * (rkxf^2 + rkyf^2), the filtered K^2 of spec1d's iopt = 1
 __global__ void k_mul_rksq(double *__restrict__ ss, const double *__restrict__ rkxf,
                            const double *__restrict__ rkyf, int nx, long long nn) {
+  CASL_PDL_ENTRY();
   for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < nn;
        m += (long long)gridDim.x * blockDim.x) {
     int kx = (int)(m % nx), ky = (int)(m / nx);
@@ -1684,6 +1706,7 @@ __global__ void k_mul_rksq(double *__restrict__ ss, const double *__restrict__ r
 __global__ void k_diag_shoelace(const double *__restrict__ dx, const double *__restrict__ dy,
                                 const double *__restrict__ X, const double *__restrict__ Y,
                                 int npt, double *__restrict__ part) {
+  CASL_PDL_ENTRY();
   double s = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npt; i += gridDim.x * blockDim.x) {
     double xe = X[i] - dx[i], ye = Y[i] - dy[i];
@@ -1891,6 +1914,7 @@ int get_scalars(casl_handle *h) {
 extern "C" {
 
 __global__ void k_to0(int *a, long long m, int off) {
+  CASL_PDL_ENTRY();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m;
        i += (long long)gridDim.x * blockDim.x)
     a[i] += off;
@@ -2202,6 +2226,7 @@ int casl_recontour(casl_handle *h, const double *qq) {
 // init (evolution.f90:96-131)
 __global__ void k_evo_init(double *qd, double *qspre, const double *qs, const double *qc,
                            const double *fhi, long long nn) {
+  CASL_PDL_ENTRY();
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nn;
        k += (long long)gridDim.x * blockDim.x) {
     qd[k] = fhi[k] * (qs[k] - qc[k]);
@@ -2211,6 +2236,7 @@ __global__ void k_evo_init(double *qd, double *qspre, const double *qs, const do
 // prepare (evolution.f90:135-162), spectral part
 __global__ void k_prepare(double *qs, double *qd, const double *qc, const double *flo,
                           long long nn) {
+  CASL_PDL_ENTRY();
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nn;
        k += (long long)gridDim.x * blockDim.x) {
     double s = flo[k] * (qs[k] - qc[k]) + qc[k] + qd[k];
@@ -2244,6 +2270,7 @@ static int evo_prepare(casl_handle *h) {
 }
 
 __global__ void k_sub_bety(double *q, const double *bety, int n) {
+  CASL_PDL_ENTRY();
   long long nn = (long long)n * n;
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nn;
        k += (long long)gridDim.x * blockDim.x)
@@ -2251,6 +2278,7 @@ __global__ void k_sub_bety(double *q, const double *bety, int n) {
 }
 
 __global__ void k_minmax(const double *q, long long nn, double *part) {
+  CASL_PDL_ENTRY();
   double mx = -1e308, mn = 1e308;
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nn;
        k += (long long)gridDim.x * blockDim.x) {

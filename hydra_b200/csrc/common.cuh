@@ -20,6 +20,42 @@ extern unsigned long long g_launches;
 bool kt_begin(const char *name, dim3 grid, dim3 block, size_t smem = 0, cudaStream_t st = 0);
 bool kt_end();
 
+// Programmatic dependent launch.  Every kernel of the library is launched
+// with programmatic stream serialization allowed and starts with
+// CASL_PDL_ENTRY(): it waits until the grid before it in the stream has
+// completed and its writes are visible (so stream order is kept), then lets
+// the grid after it begin launching, which hides that launch behind its own
+// execution.  A kernel launched without the attribute passes the wait at
+// once.
+#define CASL_PDL_ENTRY() \
+  asm volatile("griddepcontrol.wait;\n\tgriddepcontrol.launch_dependents;" ::: "memory")
+
+template <class F>
+struct Launch {
+  F f;
+  dim3 grid, block;
+  size_t smem;
+  cudaStream_t st;
+  template <class... A>
+  void operator()(A &&...args) const {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, f, static_cast<A &&>(args)...);
+  }
+};
+template <class F>
+Launch<F> launch_of(F f, dim3 grid, dim3 block, size_t smem = 0, cudaStream_t st = 0) {
+  return Launch<F>{f, grid, block, smem, st};
+}
+
 // Every kernel launch goes through CASL_K(kernel, grid, block, smem, stream)(args);
 // it counts the launch (and times it while per-launch timing is on).  The
 // for-statement form keeps it a single statement that is safe inside an
@@ -27,7 +63,7 @@ bool kt_end();
 #define CASL_K(name, ...)                                                            \
   for (bool casl_once_ = ::casl::kt_begin(#name, __VA_ARGS__); casl_once_;         \
        casl_once_ = ::casl::kt_end())                                               \
-  name<<<__VA_ARGS__>>>
+  ::casl::launch_of(name, __VA_ARGS__)
 
 // Constants of constants.f90 and contours.f90:17-42, computed once on the
 // host by the same operations as the reference's PARAMETER expressions.

@@ -243,6 +243,7 @@ __device__ __forceinline__ void rf_complex(double2 (&x)[8], double2 *S, int t,
 template <int LOGH, bool FWD, bool LVF, bool SVF, class LD, class ST>
 __global__ void __launch_bounds__(RfftShape<LOGH, LVF || SVF>::NT, RfftShape<LOGH, LVF || SVF>::MINB)
     k_rfft_r(LD ld, ST st, const double2 *__restrict__ tw) {
+  CASL_PDL_ENTRY();
   using Sh = RfftShape<LOGH, LVF || SVF>;
   constexpr int H = Sh::H, N = Sh::N, TPV = Sh::TPV, V = Sh::V, NT = Sh::NT, VS = Sh::VS;
   extern __shared__ double2 smem[];

@@ -213,6 +213,7 @@ void io_release(casl_handle *h) {
 
 __global__ void k_io_sub(const double *__restrict__ a, const double *__restrict__ b,
                          double *__restrict__ c, long long nn) {
+  CASL_PDL_ENTRY();
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nn;
        k += (long long)gridDim.x * blockDim.x)
     c[k] = a[k] - b[k];
@@ -221,6 +222,7 @@ __global__ void k_io_sub(const double *__restrict__ a, const double *__restrict_
 // real(a(iy,ix) + bety(iy)) as float32 (bety may be null)
 __global__ void k_io_add(const double *__restrict__ a, const double *__restrict__ b,
                          double *__restrict__ c, long long nn) {
+  CASL_PDL_ENTRY();
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nn;
        k += (long long)gridDim.x * blockDim.x)
     c[k] = a[k] + b[k];
@@ -228,12 +230,14 @@ __global__ void k_io_add(const double *__restrict__ a, const double *__restrict_
 
 __global__ void k_io_f32(const double *__restrict__ a, const double *__restrict__ bety,
                          float *__restrict__ out, int n, long long nn) {
+  CASL_PDL_ENTRY();
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nn;
        k += (long long)gridDim.x * blockDim.x)
     out[k] = (float)(bety ? a[k] + bety[k % n] : a[k]);
 }
 
 __global__ void k_io_i1q(const int *__restrict__ i1q, int *__restrict__ out, int nq) {
+  CASL_PDL_ENTRY();
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nq; j += gridDim.x * blockDim.x)
     out[j] = i1q[j] + 1;
 }

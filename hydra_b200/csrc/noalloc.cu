@@ -49,6 +49,7 @@ struct NaConsts {
 __global__ void k_na_scatter(const double *__restrict__ xq, const double *__restrict__ yq,
                              const int *__restrict__ nextq1, int npt, int *__restrict__ J,
                              int *__restrict__ ljx, NaConsts c, int *__restrict__ err) {
+  CASL_PDL_ENTRY();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npt; i += gridDim.x * blockDim.x) {
     int ia = nextq1[i] - 1;
     if (ia < 0 || ia >= npt) { atomicExch(err, CASL_EINVAL); continue; }
@@ -95,6 +96,7 @@ __global__ void k_na_scatter(const double *__restrict__ xq, const double *__rest
 // mean removed, as the handle-based con2grid computes them.
 __global__ void k_na_final(const int *__restrict__ C, const unsigned long long *__restrict__ csum,
                            double qjump, double *__restrict__ qc, int n) {
+  CASL_PDL_ENTRY();
   const long long nn = (long long)n * n;
   const double inv = 1.0 / (256.0 * (double)n * (double)n);
   const long long S = (long long)*csum;

@@ -35,6 +35,7 @@ __global__ void k_u_scatter(const double *__restrict__ xq, const double *__restr
                             const int *__restrict__ nextq, int npt, double qjump,
                             int *__restrict__ J, int *__restrict__ ljx, Consts c,
                             int *__restrict__ err) {
+  CASL_PDL_ENTRY();
   const int nxu = c.nxu, nyu = c.nyu;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npt; i += gridDim.x * blockDim.x) {
     int ia = nextq[i];
@@ -78,6 +79,7 @@ __global__ void k_u_scatter(const double *__restrict__ xq, const double *__restr
 }
 
 __global__ void k_u_lbot(const int *__restrict__ ljx, int *__restrict__ J, int nxu, int nyu) {
+  CASL_PDL_ENTRY();
   __shared__ int warp_tot[32];
   __shared__ int carry;
   if (threadIdx.x == 0) carry = 0;
@@ -106,6 +108,7 @@ __global__ void k_u_lbot(const int *__restrict__ ljx, int *__restrict__ J, int n
 // column sweep (congen.f90:419-423) with the column sums for the mean
 __global__ void k_u_colscan(int *__restrict__ J, int nxu, int nyu,
                             unsigned long long *__restrict__ total) {
+  CASL_PDL_ENTRY();
   int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
   if (warp >= nxu) return;
@@ -198,6 +201,7 @@ __global__ void k_u_field(const int *__restrict__ L, const unsigned long long *_
                           const double *__restrict__ qq, double qjump, int have_contours,
                           LevInfo lq, double *__restrict__ qa, unsigned short *__restrict__ lc,
                           double *__restrict__ part, Consts c) {
+  CASL_PDL_ENTRY();
   const int nxu = c.nxu, nyu = c.nyu, n = c.nx;
   const long long nruns = (long long)nxu * (nyu / 16);
   const double qavg = ufield_qavg(lsum, qjump, have_contours, nxu, nyu);
@@ -292,6 +296,7 @@ __global__ void __launch_bounds__(256) k_cr_tile(const unsigned short *__restric
                                                  const int *__restrict__ off,
                                                  unsigned long long *__restrict__ redge,
                                                  int *__restrict__ rlev) {
+  CASL_PDL_ENTRY();
   __shared__ int Cl[2][CR_CB + 1][CR_RB + 1];  // row length 65
   const int half = threadIdx.x >> 7, t = threadIdx.x & 127;
   const int ntx = nxu / CR_CB, nty = nyu / CR_RB;
@@ -358,6 +363,7 @@ __global__ void k_cr_geom(UField uf, const unsigned long long *__restrict__ redg
                           const int *__restrict__ rlev, long long ncr, LevInfo li, Consts c,
                           double *__restrict__ xcr, double *__restrict__ ycr,
                           unsigned int *__restrict__ kib, unsigned int *__restrict__ kob) {
+  CASL_PDL_ENTRY();
   const int nxu = c.nxu, nyu = c.nyu;
   const long long NE = (long long)nxu * nyu;
   const double qavg = ufield_qavg(uf.lsum, uf.qjump, uf.have, nxu, nyu);
@@ -429,6 +435,7 @@ struct __align__(16) HBucket {
 __global__ void k_h_insert(const int *__restrict__ rlev, const unsigned int *__restrict__ kob,
                            long long n, int base, HBucket *__restrict__ hb,
                            unsigned long long mask, int *__restrict__ err) {
+  CASL_PDL_ENTRY();
   for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n;
        r += (long long)gridDim.x * blockDim.x) {
     unsigned long long k = hkey(rlev[r], kob[r]);
@@ -454,6 +461,7 @@ __global__ void k_h_succ(const int *__restrict__ rlev, const unsigned int *__res
                          long long n, const HBucket *__restrict__ hb, unsigned long long mask,
                          int *__restrict__ succ, long long *__restrict__ sadslot,
                          int *__restrict__ err) {
+  CASL_PDL_ENTRY();
   for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n;
        r += (long long)gridDim.x * blockDim.x) {
     const unsigned long long k = hkey(rlev[r], kib[r]);
@@ -489,6 +497,7 @@ __global__ void k_h_succ(const int *__restrict__ rlev, const unsigned int *__res
 // first crossing of each level (crossings are sorted by level); lstart[nlev] = n
 __global__ void k_lev_starts(const int *__restrict__ rlev, long long n, int nlev,
                              long long *__restrict__ lstart) {
+  CASL_PDL_ENTRY();
   for (int l = blockIdx.x * blockDim.x + threadIdx.x; l <= nlev; l += gridDim.x * blockDim.x) {
     long long lo = 0, hi = n;
     while (lo < hi) {
@@ -503,6 +512,7 @@ __global__ void k_lev_starts(const int *__restrict__ rlev, long long n, int nlev
 __global__ void k_ct_plain(const int *__restrict__ lab, const int *__restrict__ term,
                            const int *__restrict__ val, long long ncr, int *__restrict__ startf,
                            int *__restrict__ clenr) {
+  CASL_PDL_ENTRY();
   for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
        r += (long long)gridDim.x * blockDim.x) {
     bool st = !term[r] && lab[r] == (int)r;
@@ -518,6 +528,7 @@ __global__ void k_ct_gather_plain(const int *__restrict__ lab, const int *__rest
                                   const double *__restrict__ xcr, const double *__restrict__ ycr,
                                   long long ncr, double *__restrict__ xw, double *__restrict__ yw,
                                   int *__restrict__ cidw) {
+  CASL_PDL_ENTRY();
   for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
        r += (long long)gridDim.x * blockDim.x) {
     if (term[r]) continue;
@@ -539,6 +550,7 @@ __global__ void k_ct_gather_chain(const int *__restrict__ term, const int *__res
                                   const double *__restrict__ ycr, long long ncr,
                                   double *__restrict__ xw, double *__restrict__ yw,
                                   int *__restrict__ cidw) {
+  CASL_PDL_ENTRY();
   for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
        r += (long long)gridDim.x * blockDim.x) {
     if (!term[r]) continue;
@@ -564,6 +576,7 @@ __global__ void k_ct_gather_chain(const int *__restrict__ term, const int *__res
 __global__ void k_lev_of_contour(const int *__restrict__ startf, const int *__restrict__ rlev,
                                  const int *__restrict__ cidx, long long ncr, LevInfo li,
                                  int nlevm, int *__restrict__ clevt) {
+  CASL_PDL_ENTRY();
   for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
        r += (long long)gridDim.x * blockDim.x) {
     if (!startf[r]) continue;
@@ -573,6 +586,7 @@ __global__ void k_lev_of_contour(const int *__restrict__ startf, const int *__re
 }
 
 __global__ void k_set_counts2(Scalars *s, const int *cnt) {
+  CASL_PDL_ENTRY();
   s->nq = cnt[0];
   s->nptq = cnt[1];
 }
@@ -580,6 +594,7 @@ __global__ void k_out_contours(const int *__restrict__ ocs, const int *__restric
                                const int *__restrict__ olev, int nq, int *__restrict__ i1q,
                                int *__restrict__ i2q, int *__restrict__ npq,
                                int *__restrict__ indq) {
+  CASL_PDL_ENTRY();
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nq; j += gridDim.x * blockDim.x) {
     i1q[j] = ocs[j];
     i2q[j] = ocs[j] + olen[j] - 1;
@@ -589,6 +604,7 @@ __global__ void k_out_contours(const int *__restrict__ ocs, const int *__restric
 }
 __global__ void k_out_links(const int *__restrict__ ocs, const int *__restrict__ olen, int nq,
                             int npt, int *__restrict__ nextq) {
+  CASL_PDL_ENTRY();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npt; i += gridDim.x * blockDim.x) {
     int j = contour_of(ocs, nq, i);
     nextq[i] = i + 1 < ocs[j] + olen[j] ? i + 1 : ocs[j];
@@ -608,6 +624,7 @@ __global__ void k_out_links(const int *__restrict__ ocs, const int *__restrict__
 // inclusive) and ep (chain end).
 // ---------------------------------------------------------------------------
 __global__ void k_sp_pred(const int *__restrict__ succ, long long N, int *__restrict__ pred) {
+  CASL_PDL_ENTRY();
   for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < N;
        r += (long long)gridDim.x * blockDim.x) {
     int s = succ[r];
@@ -657,6 +674,7 @@ __global__ void k_sp_flag(const int *__restrict__ pred, const int *__restrict__ 
                           int K, int *__restrict__ isspl, int2 *__restrict__ sf,
                           int2 *__restrict__ own, int *__restrict__ xlist,
                           int *__restrict__ nx) {
+  CASL_PDL_ENTRY();
   __shared__ int wtot[32], wbase;
   for (long long b0 = blockIdx.x * (long long)blockDim.x; b0 < N;
        b0 += (long long)gridDim.x * blockDim.x) {
@@ -679,6 +697,7 @@ __global__ void k_sp_walk(const int2 *__restrict__ sf, long long N, const int *_
                           int *__restrict__ nexts_c, int *__restrict__ seglen_c,
                           int *__restrict__ segmin_c, int *__restrict__ segend_c,
                           int *__restrict__ err) {
+  CASL_PDL_ENTRY();
   const int total = *nx;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
     const int s = xlist[t];
@@ -707,6 +726,7 @@ __global__ void k_sp_walk(const int2 *__restrict__ sf, long long N, const int *_
 __global__ void k_sp_unowned(long long N, const int2 *__restrict__ own, int *__restrict__ isspl,
                              int2 *__restrict__ sf, int *__restrict__ xlist,
                              int *__restrict__ nx) {
+  CASL_PDL_ENTRY();
   __shared__ int wtot[32], wbase;
   for (long long b0 = blockIdx.x * (long long)blockDim.x; b0 < N;
        b0 += (long long)gridDim.x * blockDim.x) {
@@ -725,6 +745,7 @@ __global__ void k_sp_compact(const int *__restrict__ isspl, const int *__restric
                              const int *__restrict__ segmin_c, const int *__restrict__ segend_c,
                              int *__restrict__ nexts, int *__restrict__ seglen,
                              int *__restrict__ segmin, int *__restrict__ segend) {
+  CASL_PDL_ENTRY();
   for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < N;
        r += (long long)gridDim.x * blockDim.x) {
     if (!isspl[r]) continue;
@@ -739,6 +760,7 @@ __global__ void k_sp_compact(const int *__restrict__ isspl, const int *__restric
 __global__ void k_sp_init(const int *__restrict__ nexts, const int *__restrict__ segmin, int S,
                           int *__restrict__ nx, int *__restrict__ mn, int *__restrict__ tm,
                           int *__restrict__ lastp) {
+  CASL_PDL_ENTRY();
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < S; k += gridDim.x * blockDim.x) {
     int n = nexts[k];
     nx[k] = n < 0 ? k : n;
@@ -751,6 +773,7 @@ __global__ void k_sp_jump1(const int *__restrict__ nx, const int *__restrict__ m
                            const int *__restrict__ tm, const int *__restrict__ lastp, int S,
                            int *__restrict__ nx2, int *__restrict__ mn2, int *__restrict__ tm2,
                            int *__restrict__ lastp2) {
+  CASL_PDL_ENTRY();
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < S; k += gridDim.x * blockDim.x) {
     int n = nx[k];
     mn2[k] = min(mn[k], mn[n]);
@@ -766,6 +789,7 @@ __global__ void k_sp_list(const int *__restrict__ nexts, const int *__restrict__
                           const int *__restrict__ srank, const int *__restrict__ seglen, int S,
                           int *__restrict__ sl, long long *__restrict__ suf,
                           int *__restrict__ head) {
+  CASL_PDL_ENTRY();
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < S; k += gridDim.x * blockDim.x) {
     int n = nexts[k];
     if (tm[k]) {
@@ -781,6 +805,7 @@ __global__ void k_sp_list(const int *__restrict__ nexts, const int *__restrict__
 }
 __global__ void k_sp_jump2(const int *__restrict__ sl, const long long *__restrict__ suf, int S,
                            int *__restrict__ sl2, long long *__restrict__ suf2) {
+  CASL_PDL_ENTRY();
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < S; k += gridDim.x * blockDim.x) {
     int n = sl[k];
     suf2[k] = suf[k] + (n >= 0 ? suf[n] : 0);
@@ -793,6 +818,7 @@ __global__ void k_sp_expand(long long N, const int2 *__restrict__ own,
                             const int *__restrict__ head, const int *__restrict__ lastp,
                             const int *__restrict__ segend, int *__restrict__ term,
                             int *__restrict__ lab, int *__restrict__ val, int *__restrict__ ep) {
+  CASL_PDL_ENTRY();
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < N;
        c += (long long)gridDim.x * blockDim.x) {
     const int2 oc = own[c];
@@ -818,6 +844,7 @@ __global__ void k_sp_expand(long long N, const int2 *__restrict__ own,
 
 // --- small device helpers for the saddle bookkeeping ------------------------
 __global__ void k_sd_endflag(const int *__restrict__ succ, long long ncr, int *__restrict__ flag) {
+  CASL_PDL_ENTRY();
   for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
        r += (long long)gridDim.x * blockDim.x)
     flag[r] = succ[r] < 0;
@@ -825,6 +852,7 @@ __global__ void k_sd_endflag(const int *__restrict__ succ, long long ncr, int *_
 __global__ void k_sd_compact(const int *__restrict__ flag, const int *__restrict__ pos,
                              const long long *__restrict__ sadslot, long long ncr,
                              int *__restrict__ oidx, long long *__restrict__ oslot) {
+  CASL_PDL_ENTRY();
   for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
        r += (long long)gridDim.x * blockDim.x)
     if (flag[r]) {
@@ -834,21 +862,25 @@ __global__ void k_sd_compact(const int *__restrict__ flag, const int *__restrict
 }
 __global__ void k_gather_i(const int *__restrict__ src, const int *__restrict__ idx, int m,
                            int *__restrict__ dst) {
+  CASL_PDL_ENTRY();
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x)
     dst[k] = src[idx[k]];
 }
 __global__ void k_ct_len(const int *__restrict__ startf, const int *__restrict__ clenr,
                          const int *__restrict__ cidx, long long ncr, int *__restrict__ clen) {
+  CASL_PDL_ENTRY();
   for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
        r += (long long)gridDim.x * blockDim.x)
     if (startf[r]) clen[cidx[r]] = clenr[r];
 }
 __global__ void k_chain_of_end(const int *__restrict__ ends, int nch, int *__restrict__ coe) {
+  CASL_PDL_ENTRY();
   for (int ch = blockIdx.x * blockDim.x + threadIdx.x; ch < nch; ch += gridDim.x * blockDim.x)
     coe[ends[ch]] = ch;
 }
 __global__ void k_set_starts(const int *__restrict__ st_idx, const int *__restrict__ st_len, int m,
                              int *__restrict__ startf, int *__restrict__ clenr) {
+  CASL_PDL_ENTRY();
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
     startf[st_idx[k]] = 1;
     clenr[st_idx[k]] = st_len[k];
@@ -1402,6 +1434,7 @@ namespace casl {
 // starts, out column-major (nyv, nxv)
 __global__ void k_gf_gather(const double *__restrict__ qa, int nxu, int nyu, int ix1, int nxv,
                             int iy1, int nyv, int stride, float *__restrict__ out) {
+  CASL_PDL_ENTRY();
   const long long m = (long long)nxv * nyv;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < m;
        t += (long long)gridDim.x * blockDim.x) {

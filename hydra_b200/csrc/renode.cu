@@ -13,6 +13,7 @@ __device__ __forceinline__ long long wprev(long long w, long long cs, long long 
 }
 
 __global__ void k_rn_cid(RenodeIn in, long long N, int *__restrict__ cid) {
+  CASL_PDL_ENTRY();
   const int C = contours_in(in);
   const int *cs = in.cs;
   for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < N;
@@ -113,6 +114,7 @@ __device__ __forceinline__ void rn_node(const RenodeIn &in, const RenodeScratch 
 // warp takes rn_node.
 constexpr int RN_OUT = 28;
 __global__ void k_rn_stencil(RenodeIn in, RenodeScratch s, Consts c) {
+  CASL_PDL_ENTRY();
   const double f12 = 0.5, f13 = 1.0 / 3.0, f16 = 1.0 / 6.0;
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
@@ -203,6 +205,7 @@ __global__ void k_rn_stencil(RenodeIn in, RenodeScratch s, Consts c) {
 
 __global__ void k_rn_cornerpos(const int *__restrict__ corner, const int *__restrict__ crank,
                                int *__restrict__ pos, long long N) {
+  CASL_PDL_ENTRY();
   for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < N;
        w += (long long)gridDim.x * blockDim.x)
     if (corner[w]) pos[crank[w]] = (int)w;
@@ -221,6 +224,7 @@ __device__ __forceinline__ int nint_d(double x) { return (int)llround(x); }
 
 // Per contour: node count, pieces (contours.f90:799-809, 813-930).
 __global__ void k_rn_count(RenodeIn in, RenodeScratch s, Consts c, int mode) {
+  CASL_PDL_ENTRY();
   const int Ce = contours_in(in);
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < in.C; k += gridDim.x * blockDim.x) {
     if (k >= Ce) {
@@ -242,6 +246,7 @@ __global__ void k_rn_count(RenodeIn in, RenodeScratch s, Consts c, int mode) {
 }
 
 __global__ void k_rn_fill(RenodeIn in, RenodeScratch s, Consts c, int mode) {
+  CASL_PDL_ENTRY();
   const int Ce = contours_in(in);
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < Ce; k += gridDim.x * blockDim.x) {
     long long cs = in.cs[k], L = in.len[k];
@@ -282,6 +287,7 @@ __global__ void k_rn_fill(RenodeIn in, RenodeScratch s, Consts c, int mode) {
 }
 
 __global__ void k_rn_pout(RenodeIn in, RenodeScratch s, RenodeOut out) {
+  CASL_PDL_ENTRY();
   if (out.d_counts[2]) return;  // overflow: the caller reports it
   const int Ce = contours_in(in);
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < Ce; k += gridDim.x * blockDim.x) {
@@ -300,6 +306,7 @@ __global__ void k_rn_pout(RenodeIn in, RenodeScratch s, RenodeOut out) {
 }
 
 __global__ void k_rn_place(RenodeIn in, RenodeScratch s, RenodeOut out, Consts c) {
+  CASL_PDL_ENTRY();
   if (out.d_counts[2]) return;  // overflow: the caller reports it
   for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < in.N;
        w += (long long)gridDim.x * blockDim.x) {
@@ -348,6 +355,7 @@ __global__ void k_rn_place(RenodeIn in, RenodeScratch s, RenodeOut out, Consts c
 }
 
 __global__ void k_rn_finish(int *counts_dev, const int *ntot, const int *ctot, long long cap) {
+  CASL_PDL_ENTRY();
   counts_dev[0] = *ctot;
   counts_dev[1] = *ntot;
   counts_dev[2] = (long long)*ntot > cap;

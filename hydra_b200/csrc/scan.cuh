@@ -71,6 +71,7 @@ template <class T>
 __global__ void __launch_bounds__(SCAN_BLOCK) k_scan_tiles(const T *__restrict__ in,
                                                            T *__restrict__ out,
                                                            T *__restrict__ tile_tot, long long n) {
+  CASL_PDL_ENTRY();
   __shared__ T tot;
   long long base = (long long)blockIdx.x * SCAN_TILE + (long long)threadIdx.x * SCAN_ITEMS;
   T v[SCAN_ITEMS];
@@ -93,6 +94,7 @@ __global__ void __launch_bounds__(SCAN_BLOCK) k_scan_tiles(const T *__restrict__
 template <class T>
 __global__ void __launch_bounds__(SCAN_BLOCK) k_scan_totals(T *__restrict__ tot, int ntiles,
                                                             T *__restrict__ grand) {
+  CASL_PDL_ENTRY();
   __shared__ T t;
   __shared__ T carry;
   if (threadIdx.x == 0) carry = 0;
@@ -111,6 +113,7 @@ __global__ void __launch_bounds__(SCAN_BLOCK) k_scan_totals(T *__restrict__ tot,
 
 template <class T>
 __global__ void k_scan_add(T *__restrict__ out, const T *__restrict__ tot, long long n) {
+  CASL_PDL_ENTRY();
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] += tot[i / SCAN_TILE];
 }
@@ -120,6 +123,7 @@ template <class T>
 __global__ void __launch_bounds__(SCAN_BLOCK) k_scan_small(const T *__restrict__ in,
                                                            T *__restrict__ out, long long n,
                                                            T *__restrict__ grand) {
+  CASL_PDL_ENTRY();
   __shared__ T tot;
   __shared__ T carry;
   if (threadIdx.x == 0) carry = 0;
@@ -165,6 +169,7 @@ __device__ __forceinline__ void scan_load(const T *__restrict__ in, long long ba
 template <class T, bool VEC>
 __global__ void __launch_bounds__(SCAN_BLOCK) k_scan_tilesum(const T *__restrict__ in,
                                                              T *__restrict__ tile_tot, long long n) {
+  CASL_PDL_ENTRY();
   __shared__ T part[32];
   long long base = (long long)blockIdx.x * SCAN_TILE + (long long)threadIdx.x * SCAN_ITEMS;
   T v[SCAN_ITEMS];
@@ -184,6 +189,7 @@ template <class T, bool VEC>
 __global__ void __launch_bounds__(SCAN_BLOCK) k_scan_apply(const T *in, T *out,
                                                            const T *__restrict__ tile_tot,
                                                            long long n, T *__restrict__ grand) {
+  CASL_PDL_ENTRY();
   __shared__ T part[32];
   __shared__ T tot;
   // offset of this tile: sum of the earlier tiles' totals (fixed order)
@@ -316,6 +322,7 @@ static __global__ void __launch_bounds__(SCAN_BLOCK) k_segscan_tiles(const doubl
                                                               double *__restrict__ out,
                                                               SegPair *__restrict__ tile_tot,
                                                               long long n) {
+  CASL_PDL_ENTRY();
   __shared__ SegPair tot;
   long long base = (long long)blockIdx.x * SCAN_TILE + (long long)threadIdx.x * SCAN_ITEMS;
   SegPair loc[SCAN_ITEMS];
@@ -340,6 +347,7 @@ static __global__ void __launch_bounds__(SCAN_BLOCK) k_segscan_tiles(const doubl
 // Exclusive segmented scan of tile totals (one block): carry into each tile.
 static __global__ void __launch_bounds__(SCAN_BLOCK) k_segscan_totals(SegPair *__restrict__ tot,
                                                                int ntiles) {
+  CASL_PDL_ENTRY();
   __shared__ SegPair t;
   __shared__ SegPair carry;
   if (threadIdx.x == 0) { carry.v = 0.0; carry.f = 0; }
@@ -359,6 +367,7 @@ static __global__ void __launch_bounds__(SCAN_BLOCK) k_segscan_totals(SegPair *_
 // Add each tile's incoming carry to its elements before the tile's first head.
 static __global__ void k_segscan_add(double *__restrict__ out, const int *__restrict__ head,
                               const SegPair *__restrict__ tot, long long n) {
+  CASL_PDL_ENTRY();
   long long tile = blockIdx.x;
   long long beg = tile * SCAN_TILE, end = beg + SCAN_TILE < n ? beg + SCAN_TILE : n;
   double c = tot[tile].v;

@@ -97,6 +97,7 @@ __device__ __forceinline__ int node_box(double x, double y, const LevelDesc &L, 
 // A new level starts where indq increases; contours arrive sorted by level.
 __global__ void k_lv_flags(const int *__restrict__ indq, int nq, int *__restrict__ flag,
                            int *__restrict__ err) {
+  CASL_PDL_ENTRY();
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nq; j += gridDim.x * blockDim.x) {
     flag[j] = j == 0 || indq[j] > indq[j - 1];
     if (j > 0 && indq[j] < indq[j - 1]) atomicExch(err, CASL_EINVAL);
@@ -106,6 +107,7 @@ __global__ void k_lv_flags(const int *__restrict__ indq, int nq, int *__restrict
 __global__ void k_lv_desc(const int *__restrict__ i1q, const int *__restrict__ i2q,
                           const int *__restrict__ indq, const int *__restrict__ flag,
                           const int *__restrict__ lex, int nq, LevelDesc *__restrict__ lev) {
+  CASL_PDL_ENTRY();
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nq; j += gridDim.x * blockDim.x) {
     int L = lex[j] + flag[j] - 1;
     if (flag[j]) {
@@ -118,6 +120,7 @@ __global__ void k_lv_desc(const int *__restrict__ i1q, const int *__restrict__ i
 
 __global__ void k_lv_boxes(LevelDesc *__restrict__ lev, const int *__restrict__ nlev_dev, int nq,
                            int npt, Consts c, int *__restrict__ nbox_l, int *__restrict__ err) {
+  CASL_PDL_ENTRY();
   const int nlev = *nlev_dev;
   for (int L = blockIdx.x * blockDim.x + threadIdx.x; L < nq; L += gridDim.x * blockDim.x) {
     if (L >= nlev) {
@@ -149,6 +152,7 @@ __global__ void k_lv_boxes(LevelDesc *__restrict__ lev, const int *__restrict__ 
 __global__ void k_lv_base(LevelDesc *__restrict__ lev, const int *__restrict__ nlev_dev,
                           const int *__restrict__ boxbase, const int *__restrict__ nbox_dev,
                           long long nbox_cap, int *__restrict__ err) {
+  CASL_PDL_ENTRY();
   const int nlev = *nlev_dev;
   for (int L = blockIdx.x * blockDim.x + threadIdx.x; L < nlev; L += gridDim.x * blockDim.x)
     lev[L].boxbase = boxbase[L];
@@ -157,12 +161,14 @@ __global__ void k_lv_base(LevelDesc *__restrict__ lev, const int *__restrict__ n
 
 __global__ void k_sg_endnext(const int *__restrict__ i1q, const int *__restrict__ i2q, int nq,
                              int *__restrict__ endnext) {
+  CASL_PDL_ENTRY();
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nq; j += gridDim.x * blockDim.x)
     endnext[i2q[j]] = i1q[j];
 }
 
 __global__ void k_sg_level_of(const LevelDesc *__restrict__ lev, const int *__restrict__ nlev_dev,
                               int npt, int *__restrict__ lvl) {
+  CASL_PDL_ENTRY();
   const int nlev = *nlev_dev;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npt; i += gridDim.x * blockDim.x) {
     int lo = 0, hi = nlev - 1;
@@ -180,6 +186,7 @@ __global__ void k_sg_init(const double *__restrict__ xq, const double *__restric
                           double *dx, double *dy, double *dsq, double *x0, double *y0,
                           double *dx0, double *dy0, int *nq0, int *prev0, unsigned char *pending,
                           Consts c, int *err) {
+  CASL_PDL_ENTRY();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npt; i += gridDim.x * blockDim.x) {
     int a = endnext[i] >= 0 ? endnext[i] : i + 1;
     double xi = xq[i], yi = yq[i];
@@ -203,6 +210,7 @@ __global__ void k_sg_init(const double *__restrict__ xq, const double *__restric
 __global__ void k_sg_count_entries(SurgState S, const LevelDesc *__restrict__ lev, int npt,
                                    int *__restrict__ ecount, int *__restrict__ nbox_of,
                                    int *__restrict__ nbcnt, Consts c) {
+  CASL_PDL_ENTRY();
   for (int ib = blockIdx.x * blockDim.x + threadIdx.x; ib < npt; ib += gridDim.x * blockDim.x) {
     LevelDesc L = lev[S.lvl[ib]];
     int i = S.nq0[ib];
@@ -219,6 +227,7 @@ __global__ void k_sg_emit(SurgState S, const LevelDesc *__restrict__ lev, int np
                           const int *__restrict__ eoff, const int *__restrict__ ecount,
                           long long ne_cap, int *__restrict__ ebox, int *__restrict__ eib,
                           int *__restrict__ bcnt, Consts c, int *__restrict__ err) {
+  CASL_PDL_ENTRY();
   for (int ib = blockIdx.x * blockDim.x + threadIdx.x; ib < npt; ib += gridDim.x * blockDim.x) {
     LevelDesc L = lev[S.lvl[ib]];
     int i = S.nq0[ib];
@@ -245,6 +254,7 @@ __global__ void k_sg_emit(SurgState S, const LevelDesc *__restrict__ lev, int np
 __global__ void k_sg_place(const int *__restrict__ ebox, const int *__restrict__ eib,
                            const int *__restrict__ ne_dev, const int *__restrict__ kb1,
                            int *__restrict__ cursor, int *__restrict__ bnode) {
+  CASL_PDL_ENTRY();
   const long long ne = *ne_dev;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ne;
        e += (long long)gridDim.x * blockDim.x) {
@@ -257,6 +267,7 @@ __global__ void k_sg_place(const int *__restrict__ ebox, const int *__restrict__
 __global__ void k_sg_place_nodes(const int *__restrict__ nbox_of, int npt,
                                  const int *__restrict__ nb1, int *__restrict__ cursor,
                                  int *__restrict__ nbnode) {
+  CASL_PDL_ENTRY();
   for (int ib = blockIdx.x * blockDim.x + threadIdx.x; ib < npt; ib += gridDim.x * blockDim.x) {
     int gb = nbox_of[ib];
     nbnode[nb1[gb] + atomicAdd(&cursor[gb], 1)] = ib;
@@ -283,6 +294,7 @@ __device__ __forceinline__ bool surg_test(double xi, double yi, double xs, doubl
 // Parallel candidate detection on the unmodified state.
 __global__ void k_sg_candidates(SurgState S, const LevelDesc *__restrict__ lev, int npt,
                                 const int *__restrict__ nbox_of, Consts c) {
+  CASL_PDL_ENTRY();
   for (int ib = blockIdx.x * blockDim.x + threadIdx.x; ib < npt; ib += gridDim.x * blockDim.x) {
     int i = S.nq0[ib];
     int mb = nbox_of[ib];
@@ -333,6 +345,7 @@ __device__ void mark_affected(SurgState &S, const LevelDesc &L, int j, int ib, c
 __global__ void k_sg_replay(SurgState S, const LevelDesc *__restrict__ lev,
                             const int *__restrict__ nlev_dev, Consts c, int *nsurg,
                             int *__restrict__ stats) {
+  CASL_PDL_ENTRY();
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (warp >= *nlev_dev) return;
@@ -504,6 +517,7 @@ __global__ void k_sg_replay(SurgState S, const LevelDesc *__restrict__ lev,
 // ---------------------------------------------------------------------------
 __global__ void k_rb_flags(const int *__restrict__ nextq, int npt, int *__restrict__ st,
                            int *__restrict__ brk) {
+  CASL_PDL_ENTRY();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npt; i += gridDim.x * blockDim.x) {
     brk[i] = nextq[i] != i + 1;
     st[i] = (i == 0) || (nextq[i - 1] != i);
@@ -513,6 +527,7 @@ __global__ void k_rb_flags(const int *__restrict__ nextq, int npt, int *__restri
 __global__ void k_rb_runs(const int *__restrict__ st, const int *__restrict__ brk,
                           const int *__restrict__ sx, int npt, int *__restrict__ rid,
                           int *__restrict__ rs, int *__restrict__ re) {
+  CASL_PDL_ENTRY();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npt; i += gridDim.x * blockDim.x) {
     int r = sx[i] + st[i] - 1;
     rid[i] = r;
@@ -541,6 +556,7 @@ __global__ void __launch_bounds__(1024) k_rb_cycles_block(
     int *lab, int *lab2, int *nrj, int *nrj2, int *__restrict__ hr, int *succ, int *succ2,
     long long *val, long long *val2, int *__restrict__ ishead, int *__restrict__ multi,
     long long **valout) {
+  CASL_PDL_ENTRY();
   __shared__ int nmulti;
   const int R = *R_dev;
   if (threadIdx.x == 0) nmulti = 0;
@@ -613,6 +629,7 @@ __global__ void k_rb_cycles2(const int *__restrict__ ishead, const int *__restri
                              const int *__restrict__ lvl, const LevelDesc *__restrict__ lev,
                              const int *__restrict__ R_dev, int *__restrict__ clen,
                              int *__restrict__ clev) {
+  CASL_PDL_ENTRY();
   const int R = *R_dev;
   const long long *val = *valp;
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < R; r += gridDim.x * blockDim.x) {
@@ -629,6 +646,7 @@ __global__ void k_rb_gather2(const double *__restrict__ xq, const double *__rest
                              long long *const *__restrict__ valp, const int *__restrict__ cst,
                              const int *__restrict__ clen, double *__restrict__ xw,
                              double *__restrict__ yw, int *__restrict__ cidw) {
+  CASL_PDL_ENTRY();
   const long long *val = *valp;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npt; i += gridDim.x * blockDim.x) {
     int r = rid[i];
@@ -651,6 +669,7 @@ __global__ void k_rb_writeback(const int *__restrict__ cnt, long long npm, long 
                                int *__restrict__ i1q, int *__restrict__ i2q,
                                int *__restrict__ npq, int *__restrict__ indq,
                                Scalars *__restrict__ s) {
+  CASL_PDL_ENTRY();
   const int nq = cnt[0], npt = cnt[1];
   if (cnt[2] || npt > npm || nq > nm) {
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(&s->error, CASL_ECAPACITY);
