@@ -57,6 +57,50 @@ bool kt_end() {
   return false;
 }
 
+struct FillJobs {
+  unsigned int *p[6];
+  long long n[6];
+  unsigned int v[6];
+  int nj;
+};
+__global__ void k_fill(FillJobs J) {
+  CASL_PDL_ENTRY();
+  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+#pragma unroll
+  for (int j = 0; j < 6; j++) {
+    if (j >= J.nj) break;
+    unsigned int *p = J.p[j];
+    const long long n = J.n[j];
+    const unsigned int v = J.v[j];
+    long long head = 0;
+    if (((uintptr_t)p & 15) == 0) {
+      uint4 *q = reinterpret_cast<uint4 *>(p);
+      const uint4 w = make_uint4(v, v, v, v);
+      for (long long i = tid; i < n / 4; i += stride) q[i] = w;
+      head = (n / 4) * 4;
+    }
+    for (long long i = head + tid; i < n; i += stride) p[i] = v;
+  }
+}
+
+int fill_words(cudaStream_t st, const FillJob *jobs, int njobs) {
+  if (njobs < 1 || njobs > 6) return CASL_EINVAL;
+  FillJobs J{};
+  long long most = 0;
+  for (int j = 0; j < njobs; j++) {
+    J.p[j] = static_cast<unsigned int *>(jobs[j].p);
+    J.n[j] = jobs[j].words;
+    J.v[j] = jobs[j].value;
+    most = std::max(most, jobs[j].words);
+  }
+  J.nj = njobs;
+  long long g = (most / 4 + 255) / 256;
+  g = std::max(1LL, std::min(g, 148LL * 16));
+  CASL_K(k_fill, (int)g, 256, 0, st)(J);
+  return check_launch(nullptr);
+}
+
 int set_cuda_error(casl_handle *h, cudaError_t e) {
   if (h) h->last_cuda = (int)e;
   cudaGetLastError();  // clear sticky non-fatal error state
@@ -914,8 +958,10 @@ int con2grid_dev(casl_handle *h, bool want_levels) {
     // four fine rows of a column per 64-bit word, in the first half of the
     // fine-grid buffer
     unsigned long long *JW = reinterpret_cast<unsigned long long *>(h->fineJ);
-    CASL_CUDA_TRY(cudaMemsetAsync(JW, 0, (size_t)c.nxf * n * sizeof(unsigned long long), h->stream));
-    CASL_CUDA_TRY(cudaMemsetAsync(h->ljx, 0, (size_t)c.nxf * sizeof(int), h->stream));
+    {
+      const FillJob z[2] = {{JW, 2LL * c.nxf * n, 0u}, {h->ljx, (long long)c.nxf, 0u}};
+      if (int rc = fill_words(h->stream, z, 2)) return rc;
+    }
     if (h->nptq > 0) {
       CASL_K(k_c2g_scatter<true>, grid_for(h->nptq), 256, 0, h->stream)(
           h->xq, h->yq, h->nextq, h->scal, nullptr, JW, h->ljx, c, err, csum);

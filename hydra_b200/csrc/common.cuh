@@ -56,6 +56,16 @@ Launch<F> launch_of(F f, dim3 grid, dim3 block, size_t smem = 0, cudaStream_t st
   return Launch<F>{f, grid, block, smem, st};
 }
 
+// Clears or fills up to six word arrays in one kernel launch: in-stream like
+// cudaMemsetAsync, but a kernel, so the launches around it keep the
+// programmatic overlap.  p is 4-byte aligned, words counts 32-bit words.
+struct FillJob {
+  void *p;
+  long long words;
+  unsigned int value;
+};
+int fill_words(cudaStream_t st, const FillJob *jobs, int njobs);
+
 // Every kernel launch goes through CASL_K(kernel, grid, block, smem, stream)(args);
 // it counts the launch (and times it while per-launch timing is on).  The
 // for-statement form keeps it a single statement that is safe inside an

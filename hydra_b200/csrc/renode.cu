@@ -399,7 +399,10 @@ int renode_batch(casl_handle *h, Arena &ar, const RenodeIn &in, RenodeOut &out, 
   s.pn = ar.get<int>(P); s.pout = ar.get<int>(P);
   s.psum = ar.get<double>(P); s.pfac = ar.get<double>(P);
   if (ar.failed) return CASL_ENOMEM;
-  cudaMemsetAsync(s.ccnt, 0, C * sizeof(int), st);
+  {
+    const FillJob z[1] = {{s.ccnt, C, 0u}};
+    if (int rc = fill_words(st, z, 1)) return rc;
+  }
   int g = gsz(N);
   if (!in.cid) CASL_K(k_rn_cid, g, 256, 0, st)(in, N, s.cid);
   CASL_K(k_rn_stencil, g, 256, 0, st)(in, s, c);

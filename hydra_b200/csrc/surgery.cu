@@ -727,8 +727,10 @@ static int rebuild_and_renode(casl_handle *h, Arena &ar, int npt, const int *lvl
   CASL_K(k_rb_flags, g, 256, 0, st)(h->nextq, npt, stf, brk);
   exclusive_scan<int>(st, stf, sx, npt, tmpi, dtot);           // dtot[0] = R
   CASL_K(k_rb_runs, g, 256, 0, st)(stf, brk, sx, npt, rid, rs, re);
-  CASL_CUDA_TRY(cudaMemsetAsync(ishead, 0, (size_t)npt * sizeof(int), st));
-  CASL_CUDA_TRY(cudaMemsetAsync(clen, 0, (size_t)npt * sizeof(int), st));
+  {
+    const FillJob z[2] = {{ishead, npt, 0u}, {clen, npt, 0u}};
+    if (int rc = fill_words(st, z, 2)) return rc;
+  }
   CASL_K(k_rb_cycles_block, 1, 1024, 0, st)(h->nextq, rid, rs, re, dtot, nr, lab, lab2, nrj, nrj2,
                                             hr, succ, succ2, val, val2, ishead, multi, valp);
   exclusive_scan<int>(st, ishead, cidx, npt, tmpi, dtot + 1);  // dtot[1] = C
@@ -795,9 +797,13 @@ int surgery_dev(casl_handle *h) {
   CASL_K(k_lv_boxes, gq, 256, 0, st)(dlev, dtot + 0, nq, npt, c, nbox_l, err);
   exclusive_scan<int>(st, nbox_l, boxbase, nq, tmpi, dtot + 1);
   CASL_K(k_lv_base, gq, 256, 0, st)(dlev, dtot + 0, boxbase, dtot + 1, nbox_cap, err);
-  CASL_CUDA_TRY(cudaMemsetAsync(endnext, 0xff, (size_t)npt * sizeof(int), st));
-  CASL_CUDA_TRY(cudaMemsetAsync(bcnt, 0, (size_t)nbox_cap * sizeof(int), st));
-  CASL_CUDA_TRY(cudaMemsetAsync(nbcnt, 0, (size_t)nbox_cap * sizeof(int), st));
+  {
+    const FillJob z[4] = {{endnext, npt, 0xffffffffu},
+                          {bcnt, nbox_cap, 0u},
+                          {nbcnt, nbox_cap, 0u},
+                          {wsum, (npt >> 14) + 2, 0u}};
+    if (int rc = fill_words(st, z, 4)) return rc;
+  }
   CASL_K(k_sg_endnext, gq, 256, 0, st)(h->i1q, h->i2q, nq, endnext);
   CASL_K(k_sg_level_of, g, 256, 0, st)(dlev, dtot + 0, npt, lvl);
   CASL_K(k_sg_init, g, 256, 0, st)(h->xq, h->yq, h->nextq, endnext, npt, dx, dy, dsq, x0, y0, dx0,
@@ -807,21 +813,26 @@ int surgery_dev(casl_handle *h) {
   S.x0 = x0; S.y0 = y0; S.dx0 = dx0; S.dy0 = dy0; S.nq0 = nq0; S.prev0 = prev0; S.lvl = lvl;
   S.pending = pending;
   S.wsum = wsum;
-  CASL_CUDA_TRY(cudaMemsetAsync(wsum, 0, ((npt >> 14) + 2) * sizeof(unsigned int), st));
   CASL_K(k_sg_count_entries, g, 256, 0, st)(S, dlev, npt, ecount, nbox_of, nbcnt, c);
   exclusive_scan<int>(st, ecount, eoff, npt, tmpi, dtot + 2);
   CASL_K(k_sg_emit, g, 256, 0, st)(S, dlev, npt, eoff, ecount, ne_cap, ebox, eib, bcnt, c, err);
   exclusive_scan<int>(st, bcnt, kb1, nbox_cap, tmpi, dtot + 4);
-  CASL_CUDA_TRY(cudaMemsetAsync(cursor, 0, (size_t)nbox_cap * sizeof(int), st));
+  {
+    const FillJob z[1] = {{cursor, nbox_cap, 0u}};
+    if (int rc = fill_words(st, z, 1)) return rc;
+  }
   CASL_K(k_sg_place, gs(ne_cap), 256, 0, st)(ebox, eib, dtot + 2, kb1, cursor, bnode);
   exclusive_scan<int>(st, nbcnt, nb1, nbox_cap, tmpi, dtot + 5);
-  CASL_CUDA_TRY(cudaMemsetAsync(cursor, 0, (size_t)nbox_cap * sizeof(int), st));
+  {
+    // the cursor again, and the replay's surgery count
+    const FillJob z[2] = {{cursor, nbox_cap, 0u}, {dtot + 3, 1, 0u}};
+    if (int rc = fill_words(st, z, 2)) return rc;
+  }
   CASL_K(k_sg_place_nodes, g, 256, 0, st)(nbox_of, npt, nb1, cursor, nbnode);
   S.kb1 = kb1; S.bcnt = bcnt; S.bnode = bnode; S.nb1 = nb1; S.nbcnt = nbcnt; S.nbnode = nbnode;
   tr.point("binning");
   CASL_K(k_sg_candidates, g, 256, 0, st)(S, dlev, npt, nbox_of, c);
   tr.point("candidates");
-  CASL_CUDA_TRY(cudaMemsetAsync(dtot + 3, 0, sizeof(int), st));
   int *stats = tr.on ? ar.get<int>(2 * (size_t)nq) : nullptr;
   if (stats) CASL_CUDA_TRY(cudaMemsetAsync(stats, 0, 2 * (size_t)nq * sizeof(int), st));
   CASL_K(k_sg_replay, (nq * 32 + 127) / 128, 128, 0, st)(S, dlev, dtot + 0, c, dtot + 3, stats);
