@@ -312,210 +312,49 @@ struct LoadAdvect {
   }
 };
 
-// Store of the source terms after ptospc pass B (evolution.f90:466-487),
-// b = 0 -> sqd with damping and the integrating factor, b = 1 -> sqs, with
-// the RK4 update of the spectral fields that uses them (evolution.f90:
-// 212-311, the qs/qd halves of each stage) done in the same store: b = 1
-// updates qs, qsi, qsf from sqs; b = 0 updates qd, qdi, qdf (and emq at
-// stage 3) from sqd.  The sources themselves never go to memory.
+// Store of the source terms after ptospc pass B (evolution.f90:466-487):
+// b = 0 -> sqd with damping and the integrating factor, b = 1 -> sqs.
 struct StoreSource {
-  __host__ double bytes() const { return 0.5 * 24.0 + 0.5 * (stage == 1 ? 40.0 : 32.0); }
+  __host__ double bytes() const { return 8.0 + 0.5 * 24.0; }  // sqd reads qq, pp, epq
+  double *sqd, *sqs;
   const double *qq, *pp, *epq;
-  double *qs, *qd, *qsi, *qsf, *qdi, *qdf, *emq;
-  const Scalars *sc;
   double rekman, kdsq, therm;
-  int heating, friction, lev, stage, n;
-  __device__ __forceinline__ void operator()(int b, int v /*ky*/, int k /*kx*/, double x) const {
-    long long idx = (long long)v * n + k;
-    if (b == 1) {
-      const double a = x;
-      if (stage == 1) {
-        const double si = qs[idx];
-        qsi[idx] = si;
-        qs[idx] = si + sc->dt2 * a;
-        qsf[idx] = si + sc->dt6 * a;
-      } else if (stage == 2) {
-        qs[idx] = qsi[idx] + sc->dt2 * a;
-        qsf[idx] = qsf[idx] + sc->dt3 * a;
-      } else if (stage == 3) {
-        qs[idx] = qsi[idx] + sc->dt * a;
-        qsf[idx] = qsf[idx] + sc->dt3 * a;
-      } else {
-        qs[idx] = qsf[idx] + sc->dt6 * a;
-      }
-      return;
-    }
+  int heating, friction, lev, n;
+  __device__ __forceinline__ double damped(double x, double p, double q, double e) const {
     double t;
     if (heating) {
       if (friction)
-        t = x + therm * (pp[idx] - 0.0) - rekman * (qq[idx] + kdsq * pp[idx]);
+        t = x + therm * (p - 0.0) - rekman * (q + kdsq * p);
       else
-        t = x + therm * (pp[idx] - 0.0);
+        t = x + therm * (p - 0.0);
     } else {
-      t = x - rekman * (qq[idx] + kdsq * pp[idx]);
+      t = x - rekman * (q + kdsq * p);
     }
     if (lev == 1)
-      t = epq[idx] * t;
+      t = e * t;
     else if (lev == 2)
-      t = epq[idx] * epq[idx] * t;
-    const double bb = t;
-    if (stage == 1) {
-      const double di = qd[idx];
-      qdi[idx] = di;
-      qd[idx] = emq[idx] * (di + sc->dt2 * bb);
-      qdf[idx] = di + sc->dt6 * bb;
-    } else if (stage == 2) {
-      qd[idx] = emq[idx] * (qdi[idx] + sc->dt2 * bb);
-      qdf[idx] = qdf[idx] + sc->dt3 * bb;
-    } else if (stage == 3) {
-      double e = emq[idx];
-      e = e * e;
-      emq[idx] = e;
-      qd[idx] = e * (qdi[idx] + sc->dt * bb);
-      qdf[idx] = qdf[idx] + sc->dt3 * bb;
-    } else {
-      qd[idx] = emq[idx] * (qdf[idx] + sc->dt6 * bb);
-    }
+      t = e * e * t;
+    return t;
   }
-  // elements idx, idx+1 with 16-byte accesses; per element the expressions
-  // and their order are operator()'s
-  __device__ __forceinline__ void pair(int b, int v, int k, double2 x) const {
-    const long long i = (long long)v * n + k;
-    const double a[2] = {x.x, x.y};
-    auto L = [i](const double *p, double(&o)[2]) {
-      const double2 t = *reinterpret_cast<const double2 *>(p + i);
-      o[0] = t.x;
-      o[1] = t.y;
-    };
-    auto S = [i](double *p, const double(&o)[2]) {
-      *reinterpret_cast<double2 *>(p + i) = make_double2(o[0], o[1]);
-    };
-    double u[2], r[2], w[2];
+  __device__ __forceinline__ void operator()(int b, int v /*ky*/, int k /*kx*/, double x) const {
+    const long long idx = (long long)v * n + k;
     if (b == 1) {
-      if (stage == 1) {
-        L(qs, u);
-        S(qsi, u);
-        for (int e = 0; e < 2; e++) r[e] = u[e] + sc->dt2 * a[e];
-        for (int e = 0; e < 2; e++) w[e] = u[e] + sc->dt6 * a[e];
-        S(qs, r);
-        S(qsf, w);
-      } else if (stage == 2) {
-        L(qsi, u);
-        for (int e = 0; e < 2; e++) r[e] = u[e] + sc->dt2 * a[e];
-        S(qs, r);
-        L(qsf, u);
-        for (int e = 0; e < 2; e++) w[e] = u[e] + sc->dt3 * a[e];
-        S(qsf, w);
-      } else if (stage == 3) {
-        L(qsi, u);
-        for (int e = 0; e < 2; e++) r[e] = u[e] + sc->dt * a[e];
-        S(qs, r);
-        L(qsf, u);
-        for (int e = 0; e < 2; e++) w[e] = u[e] + sc->dt3 * a[e];
-        S(qsf, w);
-      } else {
-        L(qsf, u);
-        for (int e = 0; e < 2; e++) r[e] = u[e] + sc->dt6 * a[e];
-        S(qs, r);
-      }
+      sqs[idx] = x;
       return;
     }
-    double t[2], p2[2], q2[2];
-    L(pp, p2);
-    if (heating) {
-      if (friction) {
-        L(qq, q2);
-        for (int e = 0; e < 2; e++)
-          t[e] = a[e] + therm * (p2[e] - 0.0) - rekman * (q2[e] + kdsq * p2[e]);
-      } else {
-        for (int e = 0; e < 2; e++) t[e] = a[e] + therm * (p2[e] - 0.0);
-      }
-    } else {
-      L(qq, q2);
-      for (int e = 0; e < 2; e++) t[e] = a[e] - rekman * (q2[e] + kdsq * p2[e]);
-    }
-    if (lev == 1) {
-      L(epq, u);
-      for (int e = 0; e < 2; e++) t[e] = u[e] * t[e];
-    } else if (lev == 2) {
-      L(epq, u);
-      for (int e = 0; e < 2; e++) t[e] = u[e] * u[e] * t[e];
-    }
-    double em[2];
-    if (stage == 1) {
-      L(qd, u);
-      L(emq, em);
-      S(qdi, u);
-      for (int e = 0; e < 2; e++) r[e] = em[e] * (u[e] + sc->dt2 * t[e]);
-      for (int e = 0; e < 2; e++) w[e] = u[e] + sc->dt6 * t[e];
-      S(qd, r);
-      S(qdf, w);
-    } else if (stage == 2) {
-      L(qdi, u);
-      L(emq, em);
-      for (int e = 0; e < 2; e++) r[e] = em[e] * (u[e] + sc->dt2 * t[e]);
-      S(qd, r);
-      L(qdf, u);
-      for (int e = 0; e < 2; e++) w[e] = u[e] + sc->dt3 * t[e];
-      S(qdf, w);
-    } else if (stage == 3) {
-      L(emq, em);
-      for (int e = 0; e < 2; e++) em[e] = em[e] * em[e];
-      S(emq, em);
-      L(qdi, u);
-      for (int e = 0; e < 2; e++) r[e] = em[e] * (u[e] + sc->dt * t[e]);
-      S(qd, r);
-      L(qdf, u);
-      for (int e = 0; e < 2; e++) w[e] = u[e] + sc->dt3 * t[e];
-      S(qdf, w);
-    } else {
-      L(qdf, u);
-      L(emq, em);
-      for (int e = 0; e < 2; e++) r[e] = em[e] * (u[e] + sc->dt6 * t[e]);
-      S(qd, r);
-    }
+    sqd[idx] = damped(x, pp[idx], qq[idx], lev ? epq[idx] : 0.0);
   }
-};
-
-// Last store of con2grid's forward transform with the filter combination
-// (evolution.f90:507-514) done in place of a separate pass: the coarse
-// spectral PV qc is kept, qq = flo*(qs - qc) + qc + qd and pp = green*qq
-// formed, and with RESET qs = qq, qd = fhi*(qq - qc).
-template <bool RESET>
-struct StoreCombine {
-  __host__ double bytes() const { return RESET ? 80.0 : 56.0; }
-  double *qs, *qd, *qc, *qq, *pp;
-  const double *flo, *fhi, *green;
-  int n;
-  __device__ __forceinline__ void one(long long i, double c) const {
-    const double s = qs[i], d = qd[i];
-    const double q = flo[i] * (s - c) + c + d;
-    qc[i] = c;
-    qq[i] = q;
-    pp[i] = green[i] * q;
-    if (RESET) {
-      qs[i] = q;
-      qd[i] = fhi[i] * (q - c);
-    }
-  }
-  __device__ __forceinline__ void operator()(int, int v, int k, double x) const {
-    one((long long)v * n + k, x);
-  }
-  __device__ __forceinline__ void pair(int, int v, int k, double2 x) const {
+  __device__ __forceinline__ void pair(int b, int v, int k, double2 x) const {
     const long long i = (long long)v * n + k;
-    const double2 s = *reinterpret_cast<const double2 *>(qs + i);
-    const double2 d = *reinterpret_cast<const double2 *>(qd + i);
-    const double2 f = *reinterpret_cast<const double2 *>(flo + i);
-    const double2 g = *reinterpret_cast<const double2 *>(green + i);
-    const double q0 = f.x * (s.x - x.x) + x.x + d.x, q1 = f.y * (s.y - x.y) + x.y + d.y;
-    *reinterpret_cast<double2 *>(qc + i) = x;
-    *reinterpret_cast<double2 *>(qq + i) = make_double2(q0, q1);
-    *reinterpret_cast<double2 *>(pp + i) = make_double2(g.x * q0, g.y * q1);
-    if (RESET) {
-      const double2 h = *reinterpret_cast<const double2 *>(fhi + i);
-      *reinterpret_cast<double2 *>(qs + i) = make_double2(q0, q1);
-      *reinterpret_cast<double2 *>(qd + i) = make_double2(h.x * (q0 - x.x), h.y * (q1 - x.y));
+    if (b == 1) {
+      *reinterpret_cast<double2 *>(sqs + i) = x;
+      return;
     }
+    const double2 p = *reinterpret_cast<const double2 *>(pp + i);
+    const double2 q = *reinterpret_cast<const double2 *>(qq + i);
+    const double2 e = lev ? *reinterpret_cast<const double2 *>(epq + i) : make_double2(0.0, 0.0);
+    *reinterpret_cast<double2 *>(sqd + i) =
+        make_double2(damped(x.x, p.x, q.x, e.x), damped(x.y, p.y, q.y, e.y));
   }
 };
 
@@ -1117,15 +956,22 @@ __global__ void k_combine(double *__restrict__ qs, double *__restrict__ qd,
                           const double *__restrict__ fhi, const double *__restrict__ green,
                           long long nn) {
   CASL_PDL_ENTRY();
-  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nn;
-       k += (long long)gridDim.x * blockDim.x) {
-    double s = qs[k], c = qc[k], d = qd[k];
-    double q = flo[k] * (s - c) + c + d;
-    qq[k] = q;
-    pp[k] = green[k] * q;
+  // two elements per thread with 16-byte accesses (nn is even)
+  for (long long k2 = blockIdx.x * (long long)blockDim.x + threadIdx.x; k2 < nn / 2;
+       k2 += (long long)gridDim.x * blockDim.x) {
+    const long long k = 2 * k2;
+    const double2 s = *reinterpret_cast<const double2 *>(qs + k);
+    const double2 c = *reinterpret_cast<const double2 *>(qc + k);
+    const double2 d = *reinterpret_cast<const double2 *>(qd + k);
+    const double2 f = *reinterpret_cast<const double2 *>(flo + k);
+    const double2 g = *reinterpret_cast<const double2 *>(green + k);
+    const double q0 = f.x * (s.x - c.x) + c.x + d.x, q1 = f.y * (s.y - c.y) + c.y + d.y;
+    *reinterpret_cast<double2 *>(qq + k) = make_double2(q0, q1);
+    *reinterpret_cast<double2 *>(pp + k) = make_double2(g.x * q0, g.y * q1);
     if (RESET) {
-      qs[k] = q;
-      qd[k] = fhi[k] * (q - c);
+      const double2 h = *reinterpret_cast<const double2 *>(fhi + k);
+      *reinterpret_cast<double2 *>(qs + k) = make_double2(q0, q1);
+      *reinterpret_cast<double2 *>(qd + k) = make_double2(h.x * (q0 - c.x), h.y * (q1 - c.y));
     }
   }
 }
@@ -1227,6 +1073,55 @@ __global__ void k_epq(const double *__restrict__ qdiss, double *__restrict__ epq
   }
 }
 
+// The RK4 update of the spectral fields (evolution.f90:212-311, the qs/qd
+// halves of each stage), two elements per thread with 16-byte accesses.
+template <int STAGE>
+__global__ void k_spec_rk(double *__restrict__ qs, double *__restrict__ qd,
+                          double *__restrict__ qsi, double *__restrict__ qsf,
+                          double *__restrict__ qdi, double *__restrict__ qdf,
+                          const double *__restrict__ sqs, const double *__restrict__ sqd,
+                          double *__restrict__ emq, const Scalars *__restrict__ s, long long nn) {
+  CASL_PDL_ENTRY();
+  const double dt = s->dt, dt2 = s->dt2, dt3 = s->dt3, dt6 = s->dt6;
+  auto L = [](const double *p, long long k) { return *reinterpret_cast<const double2 *>(p + k); };
+  auto S = [](double *p, long long k, double x, double y) {
+    *reinterpret_cast<double2 *>(p + k) = make_double2(x, y);
+  };
+  for (long long k2 = blockIdx.x * (long long)blockDim.x + threadIdx.x; k2 < nn / 2;
+       k2 += (long long)gridDim.x * blockDim.x) {
+    const long long k = 2 * k2;
+    const double2 a = L(sqs, k), b = L(sqd, k);
+    if (STAGE == 1) {
+      const double2 si = L(qs, k), di = L(qd, k), e = L(emq, k);
+      S(qsi, k, si.x, si.y);
+      S(qs, k, si.x + dt2 * a.x, si.y + dt2 * a.y);
+      S(qsf, k, si.x + dt6 * a.x, si.y + dt6 * a.y);
+      S(qdi, k, di.x, di.y);
+      S(qd, k, e.x * (di.x + dt2 * b.x), e.y * (di.y + dt2 * b.y));
+      S(qdf, k, di.x + dt6 * b.x, di.y + dt6 * b.y);
+    } else if (STAGE == 2) {
+      const double2 si = L(qsi, k), sf = L(qsf, k), di = L(qdi, k), df = L(qdf, k), e = L(emq, k);
+      S(qs, k, si.x + dt2 * a.x, si.y + dt2 * a.y);
+      S(qsf, k, sf.x + dt3 * a.x, sf.y + dt3 * a.y);
+      S(qd, k, e.x * (di.x + dt2 * b.x), e.y * (di.y + dt2 * b.y));
+      S(qdf, k, df.x + dt3 * b.x, df.y + dt3 * b.y);
+    } else if (STAGE == 3) {
+      const double2 si = L(qsi, k), sf = L(qsf, k), di = L(qdi, k), df = L(qdf, k);
+      double2 e = L(emq, k);
+      e = make_double2(e.x * e.x, e.y * e.y);
+      S(emq, k, e.x, e.y);
+      S(qs, k, si.x + dt * a.x, si.y + dt * a.y);
+      S(qsf, k, sf.x + dt3 * a.x, sf.y + dt3 * a.y);
+      S(qd, k, e.x * (di.x + dt * b.x), e.y * (di.y + dt * b.y));
+      S(qdf, k, df.x + dt3 * b.x, df.y + dt3 * b.y);
+    } else {
+      const double2 sf = L(qsf, k), df = L(qdf, k), e = L(emq, k);
+      S(qs, k, sf.x + dt6 * a.x, sf.y + dt6 * a.y);
+      S(qd, k, e.x * (df.x + dt6 * b.x), e.y * (df.y + dt6 * b.y));
+    }
+  }
+}
+
 __global__ void k_advance_time(Scalars *s) {
   CASL_PDL_ENTRY(); s->t = s->t + s->dt2; }
 __global__ void k_twist_sub(Scalars *s, double twistmax) {
@@ -1243,7 +1138,7 @@ static int inversion_qq(casl_handle *h, bool reset) {
   if (h->nptq == 0) {
     CASL_CUDA_TRY(cudaMemsetAsync(h->qc, 0, nn * sizeof(double), h->stream));
   } else {
-    // con2grid, then its forward transform whose last store combines
+    // con2grid, then its forward transform
     int rc = con2grid_dev(h, false);
     if (rc) return rc;
     long long n = h->n;
@@ -1251,16 +1146,12 @@ static int inversion_qq(casl_handle *h, bool reset) {
               1.0 / (256.0 * (double)n * (double)n), (int)n};
     rc = RFFT_DISPATCH(true, false, true, ld, (StoreStrided{h->qc, nn, 1, n}), 1);
     if (rc) return rc;
-    const LoadStrided lq{h->qc, nn, n, 1};
-    if (reset)
-      return RFFT_DISPATCH(true, false, false, lq,
-                           (StoreCombine<true>{h->qs, h->qd, h->qc, h->qq, h->pp, h->flo, h->fhi,
-                                               h->green, (int)n}),
-                           1);
-    return RFFT_DISPATCH(true, false, false, lq,
-                         (StoreCombine<false>{h->qs, h->qd, h->qc, h->qq, h->pp, h->flo, h->fhi,
-                                              h->green, (int)n}),
-                         1);
+    // The combination runs as its own elementwise pass: inside the batch-1
+    // transform's store (about 3.5 warps per SM) its extra loads were
+    // exposed and the fused pass took longer than the two apart.
+    rc = RFFT_DISPATCH(true, false, false, (LoadStrided{h->qc, nn, n, 1}),
+                       (StoreStrided{h->qc, nn, n, 1}), 1);
+    if (rc) return rc;
   }
   if (reset)
     CASL_K(k_combine<true>, grid_for(nn), 256, 0, h->stream)(h->qs, h->qd, h->qc, h->qq, h->pp,
@@ -1346,8 +1237,8 @@ static int adapt_dev(casl_handle *h) {
 }
 
 // source (evolution.f90:432-490) after its gradients (invert_and_gradients):
-// the advection products fused into ptospc's first pass, damping, the
-// integrating factor and the spectral RK update into its store.
+// the advection products fused into ptospc's first pass, damping and the
+// integrating factor into its store.
 static int source_prod(casl_handle *h, int stage) {
   const int lev = stage == 1 ? 0 : (stage == 4 ? 2 : 1);
   long long nn = (long long)h->n * h->n, n = h->n;
@@ -1363,12 +1254,9 @@ static int source_prod(casl_handle *h, int stage) {
   rc = RFFT_DISPATCH(true, false, true, la, (StoreStrided{tmp, nn, 1, n}), 2);
   if (rc) return rc;
   StoreSource ss{};
-  ss.qq = h->qq; ss.pp = h->pp; ss.epq = h->epq;
-  ss.qs = h->qs; ss.qd = h->qd; ss.qsi = h->qsi; ss.qsf = h->qsf; ss.qdi = h->qdi;
-  ss.qdf = h->qdf; ss.emq = h->emq; ss.sc = h->scal;
+  ss.sqd = h->sqd; ss.sqs = h->sqs; ss.qq = h->qq; ss.pp = h->pp; ss.epq = h->epq;
   ss.rekman = h->p.rekman; ss.kdsq = h->c.kdsq; ss.therm = h->c.therm;
-  ss.heating = h->c.heating; ss.friction = h->c.friction; ss.lev = lev; ss.stage = stage;
-  ss.n = h->n;
+  ss.heating = h->c.heating; ss.friction = h->c.friction; ss.lev = lev; ss.n = h->n;
   return RFFT_DISPATCH(true, false, false, (LoadStrided{tmp, nn, n, 1}), ss, 2);
 }
 
@@ -1387,9 +1275,22 @@ static int nodes_task(casl_handle *h, int stage) {
   return check_launch(h);
 }
 
+static int spec_update(casl_handle *h, int stage) {
+  const long long nn = (long long)h->n * h->n;
+  const int g = grid_for(nn / 2);
+  cudaStream_t st = h->stream;
+  switch (stage) {
+    case 1: CASL_K(k_spec_rk<1>, g, 256, 0, st)(h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs, h->sqd, h->emq, h->scal, nn); break;
+    case 2: CASL_K(k_spec_rk<2>, g, 256, 0, st)(h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs, h->sqd, h->emq, h->scal, nn); break;
+    case 3: CASL_K(k_spec_rk<3>, g, 256, 0, st)(h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs, h->sqd, h->emq, h->scal, nn); break;
+    default: CASL_K(k_spec_rk<4>, g, 256, 0, st)(h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs, h->sqd, h->emq, h->scal, nn); break;
+  }
+  return check_launch(h);
+}
+
 // advance (evolution.f90:166-326): four RK4 stages, each con2grid + the
 // filter combination, the batched inversion + source gradients, (stage 1)
-// adapt, source with the spectral update, and the node update.
+// adapt, source, the node update and the spectral RK update.
 static int advance_dev(casl_handle *h) {
   int rc;
   for (int stage = 1; stage <= 4; stage++) {
@@ -1399,8 +1300,9 @@ static int advance_dev(casl_handle *h) {
     if ((rc = inversion_qq(h, stage == 1))) return rc;
     if ((rc = invert_and_gradients(h))) return rc;
     if (stage == 1 && (rc = adapt_dev(h))) return rc;
-    if ((rc = source_prod(h, stage))) return rc;  // with the spectral RK update
+    if ((rc = source_prod(h, stage))) return rc;
     if ((rc = nodes_task(h, stage))) return rc;
+    if ((rc = spec_update(h, stage))) return rc;
   }
   return CASL_OK;
 }
