@@ -550,35 +550,45 @@ __global__ void k_rb_runs(const int *__restrict__ st, const int *__restrict__ br
 // is a single run that points to itself and is finished at once; pointer
 // jumping (min label, then list ranking) runs over the few remaining runs
 // only, rounds separated by block barriers.
-__global__ void __launch_bounds__(1024) k_rb_cycles_block(
-    const int *__restrict__ nextq, const int *__restrict__ rid, const int *__restrict__ rs,
-    const int *__restrict__ re, const int *__restrict__ R_dev, int *__restrict__ nr,
-    int *lab, int *lab2, int *nrj, int *nrj2, int *__restrict__ hr, int *succ, int *succ2,
-    long long *val, long long *val2, int *__restrict__ ishead, int *__restrict__ multi,
-    long long **valout) {
+// Every run: its successor run; a run that closes on itself is a whole
+// contour (head, length); the others (the few runs surgery cut and joined)
+// go to the multi list for k_rb_cycles_block.  Grid-wide.
+__global__ void k_rb_cycles_pre(const int *__restrict__ nextq, const int *__restrict__ rid,
+                                const int *__restrict__ rs, const int *__restrict__ re,
+                                const int *__restrict__ R_dev, int *__restrict__ nr,
+                                int *__restrict__ lab, int *__restrict__ nrj,
+                                int *__restrict__ hr, long long *__restrict__ val,
+                                long long *__restrict__ val2, int *__restrict__ ishead,
+                                int *__restrict__ multi, int *__restrict__ nmulti) {
   CASL_PDL_ENTRY();
-  __shared__ int nmulti;
   const int R = *R_dev;
-  if (threadIdx.x == 0) nmulti = 0;
-  __syncthreads();
-  for (int r = threadIdx.x; r < R; r += blockDim.x) {
-    int t = rid[nextq[re[r]]];
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < R; r += gridDim.x * blockDim.x) {
+    const int t = rid[nextq[re[r]]];
     nr[r] = t;
-    long long len = re[r] - rs[r] + 1;
+    const long long len = re[r] - rs[r] + 1;
+    lab[r] = rs[r];
     if (t == r) {  // a whole contour
-      lab[r] = rs[r];
       hr[r] = r;
       ishead[r] = 1;
       val[r] = len;
       val2[r] = len;
     } else {
       nrj[r] = t;
-      lab[r] = rs[r];
-      multi[atomicAdd(&nmulti, 1)] = r;
+      multi[atomicAdd(nmulti, 1)] = r;
     }
   }
-  __syncthreads();
-  const int M = nmulti;
+}
+
+// The cycles through the multi-run list: one block, pointer jumping over
+// the M runs in shared order.
+__global__ void __launch_bounds__(1024) k_rb_cycles_block(
+    const int *__restrict__ nextq, const int *__restrict__ rid, const int *__restrict__ rs,
+    const int *__restrict__ re, const int *__restrict__ R_dev, int *__restrict__ nr,
+    int *lab, int *lab2, int *nrj, int *nrj2, int *__restrict__ hr, int *succ, int *succ2,
+    long long *val, long long *val2, int *__restrict__ ishead, int *__restrict__ multi,
+    long long **valout, const int *__restrict__ nmulti) {
+  CASL_PDL_ENTRY();
+  const int M = *nmulti;
   int rounds = 1;
   while ((1 << rounds) < M) rounds++;
   rounds++;
@@ -722,17 +732,21 @@ static int rebuild_and_renode(casl_handle *h, Arena &ar, int npt, const int *lvl
   double *xw = ar.get<double>(npt), *yw = ar.get<double>(npt);
   int *ocs = ar.get<int>(npt), *olen = ar.get<int>(npt), *olev = ar.get<int>(npt);
   int *cnt = ar.get<int>(4);
+  int *nmulti = ar.get<int>(4);
   if (ar.failed) return CASL_ENOMEM;
   const int g = gs(npt);
   CASL_K(k_rb_flags, g, 256, 0, st)(h->nextq, npt, stf, brk);
   exclusive_scan<int>(st, stf, sx, npt, tmpi, dtot);           // dtot[0] = R
   CASL_K(k_rb_runs, g, 256, 0, st)(stf, brk, sx, npt, rid, rs, re);
   {
-    const FillJob z[2] = {{ishead, npt, 0u}, {clen, npt, 0u}};
-    if (int rc = fill_words(st, z, 2)) return rc;
+    const FillJob z[3] = {{ishead, npt, 0u}, {clen, npt, 0u}, {nmulti, 1, 0u}};
+    if (int rc = fill_words(st, z, 3)) return rc;
   }
+  CASL_K(k_rb_cycles_pre, g, 256, 0, st)(h->nextq, rid, rs, re, dtot, nr, lab, nrj, hr, val, val2,
+                                         ishead, multi, nmulti);
   CASL_K(k_rb_cycles_block, 1, 1024, 0, st)(h->nextq, rid, rs, re, dtot, nr, lab, lab2, nrj, nrj2,
-                                            hr, succ, succ2, val, val2, ishead, multi, valp);
+                                            hr, succ, succ2, val, val2, ishead, multi, valp,
+                                            nmulti);
   exclusive_scan<int>(st, ishead, cidx, npt, tmpi, dtot + 1);  // dtot[1] = C
   CASL_K(k_rb_cycles2, g, 256, 0, st)(ishead, cidx, valp, rs, lvl, dlev, dtot, clen, clev);
   exclusive_scan<int>(st, clen, cst, npt, tmpi, dtot + 2);
