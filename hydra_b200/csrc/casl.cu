@@ -906,16 +906,15 @@ __global__ void k_velint(const double *__restrict__ xq, const double *__restrict
 }
 
 template <int STAGE>
-__global__ void k_nodes_rk(double *__restrict__ xq, double *__restrict__ yq,
+__device__ __forceinline__ void nodes_rk_body(int bid, int nbk, double *__restrict__ xq, double *__restrict__ yq,
                            double *__restrict__ xqi, double *__restrict__ yqi,
                            double *__restrict__ xqf, double *__restrict__ yqf,
                            const double *__restrict__ uu, const double *__restrict__ vv,
-                           const Scalars *__restrict__ s, Consts c) {
-  CASL_PDL_ENTRY();
+                           const Scalars *__restrict__ s, const Consts &c) {
   const int npt = s->nptq;
   const double dt = s->dt, dt2 = s->dt2, dt3 = s->dt3, dt6 = s->dt6;
   const double ex = c.ellx, ey = c.elly, hx = c.hlxi, hy = c.hlyi, oms = c.oms;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npt; i += gridDim.x * blockDim.x) {
+  for (int i = bid * blockDim.x + threadIdx.x; i < npt; i += nbk * blockDim.x) {
     double uq, vq;
     velint1(xq[i], yq[i], uu, vv, c, uq, vq);
     if (STAGE == 1) {
@@ -1076,19 +1075,18 @@ __global__ void k_epq(const double *__restrict__ qdiss, double *__restrict__ epq
 // The RK4 update of the spectral fields (evolution.f90:212-311, the qs/qd
 // halves of each stage), two elements per thread with 16-byte accesses.
 template <int STAGE>
-__global__ void k_spec_rk(double *__restrict__ qs, double *__restrict__ qd,
+__device__ __forceinline__ void spec_rk_body(int bid, int nbk, double *__restrict__ qs, double *__restrict__ qd,
                           double *__restrict__ qsi, double *__restrict__ qsf,
                           double *__restrict__ qdi, double *__restrict__ qdf,
                           const double *__restrict__ sqs, const double *__restrict__ sqd,
                           double *__restrict__ emq, const Scalars *__restrict__ s, long long nn) {
-  CASL_PDL_ENTRY();
   const double dt = s->dt, dt2 = s->dt2, dt3 = s->dt3, dt6 = s->dt6;
   auto L = [](const double *p, long long k) { return *reinterpret_cast<const double2 *>(p + k); };
   auto S = [](double *p, long long k, double x, double y) {
     *reinterpret_cast<double2 *>(p + k) = make_double2(x, y);
   };
-  for (long long k2 = blockIdx.x * (long long)blockDim.x + threadIdx.x; k2 < nn / 2;
-       k2 += (long long)gridDim.x * blockDim.x) {
+  for (long long k2 = bid * (long long)blockDim.x + threadIdx.x; k2 < nn / 2;
+       k2 += (long long)nbk * blockDim.x) {
     const long long k = 2 * k2;
     const double2 a = L(sqs, k), b = L(sqd, k);
     if (STAGE == 1) {
@@ -1122,8 +1120,34 @@ __global__ void k_spec_rk(double *__restrict__ qs, double *__restrict__ qd,
   }
 }
 
-__global__ void k_advance_time(Scalars *s) {
-  CASL_PDL_ENTRY(); s->t = s->t + s->dt2; }
+// The end of an RK4 stage in one launch: blocks below nbn move the nodes
+// (velint + node update), the rest update the spectral fields; the two
+// parts touch disjoint data and read only dt from the scalars.
+struct NodeRkArgs {
+  double *xq, *yq, *xqi, *yqi, *xqf, *yqf;
+  const double *uu, *vv;
+};
+struct SpecRkArgs {
+  double *qs, *qd, *qsi, *qsf, *qdi, *qdf;
+  const double *sqs, *sqd;
+  double *emq;
+  long long nn;
+};
+template <int STAGE>
+__global__ void k_stage_rk(NodeRkArgs a, SpecRkArgs b, Scalars *__restrict__ s, Consts c,
+                           int nbn) {
+  CASL_PDL_ENTRY();
+  // the half-step time advance that opens stages 2 and 4 (nothing reads t
+  // in between)
+  if ((STAGE == 1 || STAGE == 3) && blockIdx.x == 0 && threadIdx.x == 0) s->t = s->t + s->dt2;
+  if ((int)blockIdx.x < nbn)
+    nodes_rk_body<STAGE>(blockIdx.x, nbn, a.xq, a.yq, a.xqi, a.yqi, a.xqf, a.yqf, a.uu, a.vv, s, c);
+  else
+    spec_rk_body<STAGE>(blockIdx.x - nbn, gridDim.x - nbn, b.qs, b.qd, b.qsi, b.qsf, b.qdi,
+                        b.qdf, b.sqs, b.sqd, b.emq, s, b.nn);
+}
+
+
 __global__ void k_twist_sub(Scalars *s, double twistmax) {
   CASL_PDL_ENTRY(); s->twist = s->twist - twistmax; }
 __global__ void k_twist_zero(Scalars *s) {
@@ -1262,28 +1286,19 @@ static int source_prod(casl_handle *h, int stage) {
 
 }  // namespace casl
 
-static int nodes_task(casl_handle *h, int stage) {
-  if (!h->contex) return CASL_OK;
-  int gn = grid_for(h->nptq > 0 ? h->nptq : 1);
-  cudaStream_t st = h->stream;
-  switch (stage) {
-    case 1: CASL_K(k_nodes_rk<1>, gn, 256, 0, st)(h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, h->uu, h->vv, h->scal, h->c); break;
-    case 2: CASL_K(k_nodes_rk<2>, gn, 256, 0, st)(h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, h->uu, h->vv, h->scal, h->c); break;
-    case 3: CASL_K(k_nodes_rk<3>, gn, 256, 0, st)(h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, h->uu, h->vv, h->scal, h->c); break;
-    default: CASL_K(k_nodes_rk<4>, gn, 256, 0, st)(h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, h->uu, h->vv, h->scal, h->c); break;
-  }
-  return check_launch(h);
-}
-
-static int spec_update(casl_handle *h, int stage) {
+// node update and spectral RK update of a stage, one launch
+static int stage_update(casl_handle *h, int stage) {
   const long long nn = (long long)h->n * h->n;
-  const int g = grid_for(nn / 2);
+  const int nbn = h->contex ? grid_for(h->nptq > 0 ? h->nptq : 1) : 0;
+  const int g = nbn + grid_for(nn / 2);
+  const NodeRkArgs a{h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, h->uu, h->vv};
+  const SpecRkArgs b{h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs, h->sqd, h->emq, nn};
   cudaStream_t st = h->stream;
   switch (stage) {
-    case 1: CASL_K(k_spec_rk<1>, g, 256, 0, st)(h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs, h->sqd, h->emq, h->scal, nn); break;
-    case 2: CASL_K(k_spec_rk<2>, g, 256, 0, st)(h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs, h->sqd, h->emq, h->scal, nn); break;
-    case 3: CASL_K(k_spec_rk<3>, g, 256, 0, st)(h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs, h->sqd, h->emq, h->scal, nn); break;
-    default: CASL_K(k_spec_rk<4>, g, 256, 0, st)(h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs, h->sqd, h->emq, h->scal, nn); break;
+    case 1: CASL_K(k_stage_rk<1>, g, 256, 0, st)(a, b, h->scal, h->c, nbn); break;
+    case 2: CASL_K(k_stage_rk<2>, g, 256, 0, st)(a, b, h->scal, h->c, nbn); break;
+    case 3: CASL_K(k_stage_rk<3>, g, 256, 0, st)(a, b, h->scal, h->c, nbn); break;
+    default: CASL_K(k_stage_rk<4>, g, 256, 0, st)(a, b, h->scal, h->c, nbn); break;
   }
   return check_launch(h);
 }
@@ -1294,15 +1309,13 @@ static int spec_update(casl_handle *h, int stage) {
 static int advance_dev(casl_handle *h) {
   int rc;
   for (int stage = 1; stage <= 4; stage++) {
-    if (stage == 2 || stage == 4) CASL_K(k_advance_time, 1, 1, 0, h->stream)(h->scal);
     // stage 1: the reset inside the filter combination rewrites qs and qd
     // before the gradients read them
     if ((rc = inversion_qq(h, stage == 1))) return rc;
     if ((rc = invert_and_gradients(h))) return rc;
     if (stage == 1 && (rc = adapt_dev(h))) return rc;
     if ((rc = source_prod(h, stage))) return rc;
-    if ((rc = nodes_task(h, stage))) return rc;
-    if ((rc = spec_update(h, stage))) return rc;
+    if ((rc = stage_update(h, stage))) return rc;
   }
   return CASL_OK;
 }
