@@ -226,13 +226,7 @@ __device__ __forceinline__ int nint_d(double x) { return (int)llround(x); }
 __global__ void k_rn_count(RenodeIn in, RenodeScratch s, Consts c, int mode) {
   CASL_PDL_ENTRY();
   const int Ce = contours_in(in);
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < in.C; k += gridDim.x * blockDim.x) {
-    if (k >= Ce) {
-      s.npiece[k] = 0;
-      s.cnpr[k] = 0;
-      s.ckeep[k] = 0;
-      continue;
-    }
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < Ce; k += gridDim.x * blockDim.x) {
     long long cs = in.cs[k], L = in.len[k];
     double total = s.S[cs + L - 1];
     s.ctot[k] = total;
@@ -354,11 +348,39 @@ __global__ void k_rn_place(RenodeIn in, RenodeScratch s, RenodeOut out, Consts c
   }
 }
 
-__global__ void k_rn_finish(int *counts_dev, const int *ntot, const int *ctot, long long cap) {
+// The kept contours' node counts and keep flags scanned (both over the
+// contours the device holds), then the output counts: one block.
+__global__ void __launch_bounds__(SCAN_BLOCK) k_rn_scan2_finish(RenodeIn in, RenodeScratch s,
+                                                                RenodeOut out) {
   CASL_PDL_ENTRY();
-  counts_dev[0] = *ctot;
-  counts_dev[1] = *ntot;
-  counts_dev[2] = (long long)*ntot > cap;
+  __shared__ int tot, carry[2];
+  const long long n = contours_in(in);
+  if (threadIdx.x < 2) carry[threadIdx.x] = 0;
+  __syncthreads();
+  for (long long base = 0; base < n; base += SCAN_BLOCK) {
+    const long long k = base + threadIdx.x;
+    const int a = k < n ? s.cnpr[k] : 0, b = k < n ? s.ckeep[k] : 0;
+    const int ea = block_excl_scan<int>(a, &tot);
+    const int ta = tot;
+    __syncthreads();  // every thread has read tot before the next scan reuses it
+    const int eb = block_excl_scan<int>(b, &tot);
+    const int tb = tot;
+    if (k < n) {
+      s.cout[k] = ea + carry[0];
+      s.ckidx[k] = eb + carry[1];
+    }
+    __syncthreads();  // every thread has read the carries
+    if (threadIdx.x == 0) {
+      carry[0] += ta;
+      carry[1] += tb;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out.d_counts[0] = carry[1];
+    out.d_counts[1] = carry[0];
+    out.d_counts[2] = (long long)carry[0] > out.cap;
+  }
 }
 
 static inline int gsz(long long work) {
@@ -409,13 +431,13 @@ int renode_batch(casl_handle *h, Arena &ar, const RenodeIn &in, RenodeOut &out, 
   segmented_scan(st, s.e, s.head, s.S, N, s.tmps);
   exclusive_scan<int>(st, s.corner, s.crank, N, s.tmpi, s.d_tot + 0);
   CASL_K(k_rn_cornerpos, g, 256, 0, st)(s.corner, s.crank, s.cornerpos, N);
-  int gc = gsz(C);
+  // per-contour passes: C may be a capacity (surgery: the count is on the
+  // device), so the grids are sized for the usual counts and loop
+  int gc = gsz(C < (1 << 16) ? C : (1 << 16));
   CASL_K(k_rn_count, gc, 256, 0, st)(in, s, c, mode);
-  exclusive_scan<int>(st, s.npiece, s.poff, C, s.tmpi, s.d_tot + 1);
+  exclusive_scan_dev<int>(st, s.npiece, s.poff, C, in.Cdev, s.tmpi, s.d_tot + 1);
   CASL_K(k_rn_fill, gc, 256, 0, st)(in, s, c, mode);
-  exclusive_scan<int>(st, s.cnpr, s.cout, C, s.tmpi, s.d_tot + 2);
-  exclusive_scan<int>(st, s.ckeep, s.ckidx, C, s.tmpi, s.d_tot + 3);
-  CASL_K(k_rn_finish, 1, 1, 0, st)(out.d_counts, s.d_tot + 2, s.d_tot + 3, out.cap);
+  CASL_K(k_rn_scan2_finish, 1, SCAN_BLOCK, 0, st)(in, s, out);
   CASL_K(k_rn_pout, gc, 256, 0, st)(in, s, out);
   CASL_K(k_rn_place, g, 256, 0, st)(in, s, out, c);
   return check_launch(h);

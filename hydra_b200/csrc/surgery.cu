@@ -95,99 +95,119 @@ __device__ __forceinline__ int node_box(double x, double y, const LevelDesc &L, 
 
 // --- levels (contours.f90:374-394) and box counts (contours.f90:429-454) ----
 // A new level starts where indq increases; contours arrive sorted by level.
-__global__ void k_lv_flags(const int *__restrict__ indq, int nq, int *__restrict__ flag,
-                           int *__restrict__ err) {
-  CASL_PDL_ENTRY();
-  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nq; j += gridDim.x * blockDim.x) {
-    flag[j] = j == 0 || indq[j] > indq[j - 1];
-    if (j > 0 && indq[j] < indq[j - 1]) atomicExch(err, CASL_EINVAL);
-  }
-}
 
-__global__ void k_lv_desc(const int *__restrict__ i1q, const int *__restrict__ i2q,
-                          const int *__restrict__ indq, const int *__restrict__ flag,
-                          const int *__restrict__ lex, int nq, LevelDesc *__restrict__ lev) {
+
+
+
+// The level table in one block (levels are few, contours ~1e4): level
+// starts where indq increases, their ranks, each level's node range, box
+// counts nint(1.2 sqrt(N_lev)) per side (contours.f90:403-416) and the
+// levels' first global boxes; and endnext, each contour's last node linked
+// to its first (the rest of endnext is -1 on entry).  dtot[0] = levels,
+// dtot[1] = boxes.
+__global__ void __launch_bounds__(SCAN_BLOCK) k_lv_all(const int *__restrict__ i1q,
+                                                       const int *__restrict__ i2q,
+                                                       const int *__restrict__ indq, int nq,
+                                                       int npt, Consts c,
+                                                       LevelDesc *__restrict__ lev,
+                                                       int *__restrict__ lidx,
+                                                       int *__restrict__ endnext,
+                                                       int *__restrict__ dtot,
+                                                       long long nbox_cap,
+                                                       int *__restrict__ err) {
   CASL_PDL_ENTRY();
-  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nq; j += gridDim.x * blockDim.x) {
-    int L = lex[j] + flag[j] - 1;
-    if (flag[j]) {
+  __shared__ int tot, carry;
+  const int tid = threadIdx.x;
+  if (tid == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < nq; base += SCAN_BLOCK) {
+    const int j = base + tid;
+    int f = 0;
+    if (j < nq) {
+      f = j == 0 || indq[j] > indq[j - 1];
+      if (j > 0 && indq[j] < indq[j - 1]) atomicExch(err, CASL_EINVAL);
+    }
+    const int ex = block_excl_scan<int>(f, &tot) + carry;
+    if (j < nq) lidx[j] = ex + f - 1;  // the level of contour j
+    __syncthreads();
+    if (tid == 0) carry += tot;
+    __syncthreads();
+  }
+  const int nlev = carry;
+  for (int j = tid; j < nq; j += SCAN_BLOCK) {
+    endnext[i2q[j]] = i1q[j];  // a contour's last node links back to its first
+    const int L = lidx[j];
+    if (j == 0 || indq[j] > indq[j - 1]) {
       lev[L].ibeg = i1q[j];
       lev[L].levt = indq[j];
     }
-    if (j == nq - 1 || flag[j + 1]) lev[L].iend = i2q[j];
+    if (j == nq - 1 || indq[j + 1] > indq[j]) lev[L].iend = i2q[j];
+  }
+  __syncthreads();
+  if (tid == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < nlev; base += SCAN_BLOCK) {
+    const int L = base + tid;
+    int nb = 0;
+    LevelDesc d{};
+    bool ok = false;
+    if (L < nlev) {
+      d = lev[L];
+      if (d.ibeg < 0 || d.iend >= npt || d.iend < d.ibeg) {
+        atomicExch(err, CASL_EINVAL);
+      } else {
+        ok = true;
+        double fnq = (double)(d.iend - d.ibeg + 1);
+        double fnbx = 1.2 * sqrt(fnq * c.aspect);
+        double fnby = fnbx / c.aspect;
+        int nbx = (int)llround(fnbx);
+        nbx = max(min(nbx, c.nx), 1);
+        int nby = (int)llround(fnby);
+        nby = max(min(nby, c.ny), 1);
+        d.nbx = nbx;
+        d.nby = nby;
+        d.bwxi = c.oms * (double)nbx / c.ellx;
+        d.bwyi = c.oms * (double)nby / c.elly;
+        nb = nbx * nby;
+      }
+    }
+    const int ex = block_excl_scan<int>(nb, &tot) + carry;
+    if (ok) {
+      d.boxbase = ex;
+      lev[L] = d;
+    }
+    __syncthreads();
+    if (tid == 0) carry += tot;
+    __syncthreads();
+  }
+  if (tid == 0) {
+    dtot[0] = nlev;
+    dtot[1] = carry;
+    if ((long long)carry > nbox_cap) atomicExch(err, CASL_ECAPACITY);
   }
 }
 
-__global__ void k_lv_boxes(LevelDesc *__restrict__ lev, const int *__restrict__ nlev_dev, int nq,
-                           int npt, Consts c, int *__restrict__ nbox_l, int *__restrict__ err) {
-  CASL_PDL_ENTRY();
-  const int nlev = *nlev_dev;
-  for (int L = blockIdx.x * blockDim.x + threadIdx.x; L < nq; L += gridDim.x * blockDim.x) {
-    if (L >= nlev) {
-      nbox_l[L] = 0;
-      continue;
-    }
-    LevelDesc d = lev[L];
-    if (d.ibeg < 0 || d.iend >= npt || d.iend < d.ibeg) {
-      atomicExch(err, CASL_EINVAL);
-      nbox_l[L] = 0;
-      continue;
-    }
-    double fnq = (double)(d.iend - d.ibeg + 1);
-    double fnbx = 1.2 * sqrt(fnq * c.aspect);
-    double fnby = fnbx / c.aspect;
-    int nbx = (int)llround(fnbx);
-    nbx = max(min(nbx, c.nx), 1);
-    int nby = (int)llround(fnby);
-    nby = max(min(nby, c.ny), 1);
-    d.nbx = nbx;
-    d.nby = nby;
-    d.bwxi = c.oms * (double)nbx / c.ellx;
-    d.bwyi = c.oms * (double)nby / c.elly;
-    lev[L] = d;
-    nbox_l[L] = nbx * nby;
-  }
-}
 
-__global__ void k_lv_base(LevelDesc *__restrict__ lev, const int *__restrict__ nlev_dev,
-                          const int *__restrict__ boxbase, const int *__restrict__ nbox_dev,
-                          long long nbox_cap, int *__restrict__ err) {
-  CASL_PDL_ENTRY();
-  const int nlev = *nlev_dev;
-  for (int L = blockIdx.x * blockDim.x + threadIdx.x; L < nlev; L += gridDim.x * blockDim.x)
-    lev[L].boxbase = boxbase[L];
-  if (blockIdx.x == 0 && threadIdx.x == 0 && *nbox_dev > nbox_cap) atomicExch(err, CASL_ECAPACITY);
-}
-
-__global__ void k_sg_endnext(const int *__restrict__ i1q, const int *__restrict__ i2q, int nq,
-                             int *__restrict__ endnext) {
-  CASL_PDL_ENTRY();
-  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nq; j += gridDim.x * blockDim.x)
-    endnext[i2q[j]] = i1q[j];
-}
-
-__global__ void k_sg_level_of(const LevelDesc *__restrict__ lev, const int *__restrict__ nlev_dev,
-                              int npt, int *__restrict__ lvl) {
-  CASL_PDL_ENTRY();
-  const int nlev = *nlev_dev;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npt; i += gridDim.x * blockDim.x) {
-    int lo = 0, hi = nlev - 1;
-    while (lo < hi) {
-      int mid = (lo + hi + 1) >> 1;
-      if (lev[mid].ibeg <= i) lo = mid; else hi = mid - 1;
-    }
-    lvl[i] = lo;
-  }
-}
 
 // work arrays dx, dy, dsq (contours.f90:397-415) and the original copies
 __global__ void k_sg_init(const double *__restrict__ xq, const double *__restrict__ yq,
                           const int *__restrict__ nextq, const int *__restrict__ endnext, int npt,
                           double *dx, double *dy, double *dsq, double *x0, double *y0,
                           double *dx0, double *dy0, int *nq0, int *prev0, unsigned char *pending,
-                          Consts c, int *err) {
+                          const LevelDesc *__restrict__ lev, const int *__restrict__ nlev_dev,
+                          int *__restrict__ lvl, Consts c, int *err) {
   CASL_PDL_ENTRY();
+  const int nlev = *nlev_dev;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npt; i += gridDim.x * blockDim.x) {
+    {
+      // the node's level: the last level starting at or below i
+      int lo = 0, hi = nlev - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (lev[mid].ibeg <= i) lo = mid; else hi = mid - 1;
+      }
+      lvl[i] = lo;
+    }
     int a = endnext[i] >= 0 ? endnext[i] : i + 1;
     double xi = xq[i], yi = yq[i];
     if (!(xi >= c.xmin && xi < c.xmax && yi >= c.ymin && yi < c.ymax)) atomicExch(err, CASL_EDOMAIN);
@@ -787,8 +807,7 @@ int surgery_dev(casl_handle *h) {
   Trace tr;
   tr.begin(st, "start");
   // levels and boxes, on the device
-  int *lflag = ar.get<int>(nq), *lex = ar.get<int>(nq), *nbox_l = ar.get<int>(nq);
-  int *boxbase = ar.get<int>(nq);
+  int *lex = ar.get<int>(nq);
   LevelDesc *dlev = ar.get<LevelDesc>(nq);
   int *tmpi = ar.get<int>(scan_tmp_elems(std::max<long long>(std::max<long long>(npt, nbox_cap), ne_cap)) + 4);
   int *dtot = ar.get<int>(16);  // [0] nlev, [1] nbox, [2] ne, [3] nsurg
@@ -804,13 +823,7 @@ int surgery_dev(casl_handle *h) {
   int *nbcnt = ar.get<int>(nbox_cap), *nb1 = ar.get<int>(nbox_cap), *nbnode = ar.get<int>(npt);
   int *ebox = ar.get<int>(ne_cap), *eib = ar.get<int>(ne_cap), *bnode = ar.get<int>(ne_cap);
   if (ar.failed) return CASL_ENOMEM;
-  const int g = gs(npt), gq = gs(nq), gb = gs(nbox_cap);
-  CASL_K(k_lv_flags, gq, 256, 0, st)(h->indq, nq, lflag, err);
-  exclusive_scan<int>(st, lflag, lex, nq, tmpi, dtot + 0);
-  CASL_K(k_lv_desc, gq, 256, 0, st)(h->i1q, h->i2q, h->indq, lflag, lex, nq, dlev);
-  CASL_K(k_lv_boxes, gq, 256, 0, st)(dlev, dtot + 0, nq, npt, c, nbox_l, err);
-  exclusive_scan<int>(st, nbox_l, boxbase, nq, tmpi, dtot + 1);
-  CASL_K(k_lv_base, gq, 256, 0, st)(dlev, dtot + 0, boxbase, dtot + 1, nbox_cap, err);
+  const int g = gs(npt), gb = gs(nbox_cap);
   {
     const FillJob z[4] = {{endnext, npt, 0xffffffffu},
                           {bcnt, nbox_cap, 0u},
@@ -818,10 +831,10 @@ int surgery_dev(casl_handle *h) {
                           {wsum, (npt >> 14) + 2, 0u}};
     if (int rc = fill_words(st, z, 4)) return rc;
   }
-  CASL_K(k_sg_endnext, gq, 256, 0, st)(h->i1q, h->i2q, nq, endnext);
-  CASL_K(k_sg_level_of, g, 256, 0, st)(dlev, dtot + 0, npt, lvl);
+  CASL_K(k_lv_all, 1, SCAN_BLOCK, 0, st)(h->i1q, h->i2q, h->indq, nq, npt, c, dlev, lex, endnext,
+                                         dtot, nbox_cap, err);
   CASL_K(k_sg_init, g, 256, 0, st)(h->xq, h->yq, h->nextq, endnext, npt, dx, dy, dsq, x0, y0, dx0,
-                                   dy0, nq0, prev0, pending, c, err);
+                                   dy0, nq0, prev0, pending, dlev, dtot, lvl, c, err);
   SurgState S{};
   S.xq = h->xq; S.yq = h->yq; S.dx = dx; S.dy = dy; S.dsq = dsq; S.nextq = h->nextq;
   S.x0 = x0; S.y0 = y0; S.dx0 = dx0; S.dy0 = dy0; S.nq0 = nq0; S.prev0 = prev0; S.lvl = lvl;
