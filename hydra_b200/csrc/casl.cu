@@ -790,7 +790,7 @@ int con2grid_dev(casl_handle *h, bool want_levels) {
   int *err = &h->scal->error;
   unsigned long long *csum = (unsigned long long *)&h->scal->csum;
   const int n = h->n;
-  const int U = n % 128 == 0 ? 4 : (n % 64 == 0 ? 2 : (n % 32 == 0 ? 1 : 0));
+  const int U = n % 256 == 0 ? 8 : (n % 128 == 0 ? 4 : (n % 64 == 0 ? 2 : (n % 32 == 0 ? 1 : 0)));
   // packed path while the 16-bit counts cannot overflow (one net crossing
   // per level and fine edge: levels well below 32767)
   if (!want_levels && c.nxf == c.nyf && U > 0 && h->p.ncontq < 16384) {
@@ -808,7 +808,9 @@ int con2grid_dev(casl_handle *h, bool want_levels) {
       CASL_CUDA_TRY(cudaMemsetAsync(csum, 0, sizeof(unsigned long long), h->stream));
     }
     const int nblk = (n + C2G_CW - 1) / C2G_CW;
-    if (U == 4)
+    if (U == 8)
+      CASL_K(k_c2g_packed_sum<8>, nblk, 1024, 0, h->stream)(JW, h->ljx, h->coarseC, csum, n, c.nxf);
+    else if (U == 4)
       CASL_K(k_c2g_packed_sum<4>, nblk, 1024, 0, h->stream)(JW, h->ljx, h->coarseC, csum, n, c.nxf);
     else if (U == 2)
       CASL_K(k_c2g_packed_sum<2>, nblk, 1024, 0, h->stream)(JW, h->ljx, h->coarseC, csum, n, c.nxf);
