@@ -193,6 +193,7 @@ int spctop_dev(casl_handle *h, const double *spec, double *phys, double *tmp) {
 // a spectral field, optionally of green*field (main_invert, spectral.f90:321).
 // Batch index b selects field and direction.
 struct LoadDeriv {
+  static constexpr bool wide = true;  // 80 registers: at 64 the derivative load spills
   // bytes per element, averaged over the batch's entries
   __host__ double bytes() const {
     int nb = 0, ng = 0;

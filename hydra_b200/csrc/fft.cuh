@@ -165,10 +165,9 @@ struct RfftShape {
   static constexpr int VW = VF ? 256 / TPV : 64 / TPV;
   static constexpr int V = VW < 1 ? 1 : (VW < N ? VW : N);  // vectors per CTA
   static constexpr int NT = V * TPV;        // threads per CTA
-  // CTAs per SM to fit: 768 threads (<= 85 registers, no spills; a cap of
-  // 64 registers, one full wave for a batch of 2 at 1024^2, spilled and
-  // measured no faster inside the time step)
-  static constexpr int MINB = 768 / NT > 0 ? 768 / NT : 1;
+  // CTAs per SM to fit: 1024 threads (<= 64 registers; a little faster in
+  // the step than 768 threads at 80 registers)
+  static constexpr int MINB = 1024 / NT > 0 ? 1024 / NT : 1;
   static constexpr int P8 = LOGH / 3;       // radix-8 passes
   static constexpr int REM = LOGH % 3;      // final radix-4 (2) or radix-2 (1) pass
   // forward transforms with a vector-fastest store stage their output in a
@@ -240,8 +239,23 @@ __device__ __forceinline__ void rf_complex(double2 (&x)[8], double2 *S, int t,
   if (Sh::REM == 1) rf_butterflies<2, FWD, Sh::TPV>(x, t, Ns, tw, n);
 }
 
+// A load or store functor may ask for fewer CTAs per SM (more registers)
+// through a static member `wide`: the derivative load keeps 80 registers,
+// where 64 would spill.
+template <class T, class = void>
+struct wants_wide : std::false_type {};
+template <class T>
+struct wants_wide<T, std::void_t<decltype(T::wide)>> : std::bool_constant<T::wide> {};
+template <int LOGH, bool VF, class LD, class ST>
+constexpr int rfft_minb() {
+  using Sh = RfftShape<LOGH, VF>;
+  return (wants_wide<LD>::value || wants_wide<ST>::value) ? (768 / Sh::NT > 0 ? 768 / Sh::NT : 1)
+                                                          : Sh::MINB;
+}
+
 template <int LOGH, bool FWD, bool LVF, bool SVF, class LD, class ST>
-__global__ void __launch_bounds__(RfftShape<LOGH, LVF || SVF>::NT, RfftShape<LOGH, LVF || SVF>::MINB)
+__global__ void __launch_bounds__(RfftShape<LOGH, LVF || SVF>::NT,
+                                  (rfft_minb<LOGH, LVF || SVF, LD, ST>()))
     k_rfft_r(LD ld, ST st, const double2 *__restrict__ tw) {
   CASL_PDL_ENTRY();
   using Sh = RfftShape<LOGH, LVF || SVF>;
