@@ -424,6 +424,16 @@ __device__ __forceinline__ void c2g_decode(unsigned long long w, int &c0, int &c
   c3 = (int)v;
 }
 
+// Fire-and-forget global additions (no value returned to the thread).
+__device__ __forceinline__ void red_add_u64(unsigned long long *p, unsigned long long v) {
+  asm volatile("red.relaxed.gpu.global.add.u64 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "l"(v)
+               : "memory");
+}
+__device__ __forceinline__ void red_add_s32(int *p, int v) {
+  asm volatile("red.relaxed.gpu.global.add.s32 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "r"(v)
+               : "memory");
+}
+
 // Per segment (i, nextq(i)): x fine-grid-line crossings and the crossing of
 // y = ymin, counted as +-1 PV jumps (contours.f90:232-270): J += sgn at
 // each (PACKED: into the row's 16-bit lane of JW), ljx the bottom-boundary
@@ -442,8 +452,7 @@ __global__ void k_c2g_scatter(const double *__restrict__ xq, const double *__res
   const unsigned FULL = 0xffffffffu;
   const int npt = s->nptq, nf = c.nxf, lane = threadIdx.x & 31;
   const int wstride = gridDim.x * blockDim.x;
-  // whole warps step through the nodes together, so that a segment's x-line
-  // crossings can be shared out over the warp's lanes below
+  // whole warps step through the nodes together (the shuffles below)
   for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < npt; base += wstride) {
     const int i = base + lane;
     int cnt = 0, ixbeg = 0, jump = 0, sgn = 0;
@@ -485,7 +494,7 @@ __global__ void k_c2g_scatter(const double *__restrict__ xq, const double *__res
             const double p = -(yi - c.hly * cc) / (dy + c.small);
             int ix = 1 + f_int(c.glxfi * fmod(c.ellx + c.hlx + xi + p * dx, c.ellx));
             ix = ix < 1 ? 1 : (ix > nf ? nf : ix);
-            atomicAdd(&ljx[ix - 1], -(int)cc);
+            red_add_s32(&ljx[ix - 1], -(int)cc);
           }
           if (nxc != 0) {
             jump = f_isign1(nxc);
@@ -496,43 +505,26 @@ __global__ void k_c2g_scatter(const double *__restrict__ xq, const double *__res
         }
       }
     }
-    // crossing q of the warp (all segments' crossings in lane order) goes
-    // to lane q % 32: its segment is the first lane whose inclusive count
-    // exceeds q
-    const int incl = warp_incl_scan(cnt);
-    const int excl = incl - cnt;
-    const int tot = __shfl_sync(FULL, incl, 31);
-    for (int b0 = 0; b0 < tot; b0 += 32) {
-      const int q = b0 + lane;
-      int o = 0;
-#pragma unroll
-      for (int st = 16; st > 0; st >>= 1)
-        if (__shfl_sync(FULL, incl, o + st - 1) <= q) o += st;
-      o = min(o, 31);
-      const int oex = __shfl_sync(FULL, excl, o), obeg = __shfl_sync(FULL, ixbeg, o);
-      const int ojump = __shfl_sync(FULL, jump, o), osgn = __shfl_sync(FULL, sgn, o);
-      const double oxi = __shfl_sync(FULL, xi, o), oyi = __shfl_sync(FULL, yi, o);
-      const double odx = __shfl_sync(FULL, dx, o), ody = __shfl_sync(FULL, dy, o);
-      if (q < tot) {
-        const int ncr = (q - oex) * ojump;
-        // (ixbeg + ncr) mod nf, the argument lying in (nf/2, 5nf/2)
-        int m = obeg + ncr;
-        m -= m >= nf ? nf : 0;
-        m -= m >= nf ? nf : 0;
-        const int ix = 1 + m;
-        const double xgf = c.xmin + c.glxf * (double)(ix - 1);
-        const double x2 = xgf - oxi;
-        const double px0 = (x2 - c.ellx * f_dint(x2 * c.hlxi)) / odx;
-        const double y2 = oyi + px0 * ody;
-        const int iy = 2 + f_int(c.glyfi * (y2 - c.elly * f_dint(y2 * c.hlyi) - c.ymin));
-        if (iy >= 2 && iy <= c.nyf) {
-          if (PACKED) {
-            const int r = iy - 1;
-            atomicAdd(&JW[(long long)(ix - 1) * c.nx + (r >> 2)],
-                      (unsigned long long)((long long)osgn << (16 * (r & 3))));
-          } else
-            atomicAdd(&J[(long long)(ix - 1) * c.nyf + (iy - 1)], osgn);
-        }
+    // this lane's own crossings: fine lines ixbeg + k*jump, k < cnt (a few
+    // per segment; the lanes' loops diverge but need no exchange)
+    for (int k = 0; k < cnt; k++) {
+      // (ixbeg + k*jump) mod nf, the argument lying in (nf/2, 5nf/2)
+      int m = ixbeg + k * jump;
+      m -= m >= nf ? nf : 0;
+      m -= m >= nf ? nf : 0;
+      const int ix = 1 + m;
+      const double xgf = c.xmin + c.glxf * (double)(ix - 1);
+      const double x2 = xgf - xi;
+      const double px0 = (x2 - c.ellx * f_dint(x2 * c.hlxi)) / dx;
+      const double y2 = yi + px0 * dy;
+      const int iy = 2 + f_int(c.glyfi * (y2 - c.elly * f_dint(y2 * c.hlyi) - c.ymin));
+      if (iy >= 2 && iy <= c.nyf) {
+        if (PACKED) {
+          const int r = iy - 1;
+          red_add_u64(&JW[(long long)(ix - 1) * c.nx + (r >> 2)],
+                      (unsigned long long)((long long)sgn << (16 * (r & 3))));
+        } else
+          red_add_s32(&J[(long long)(ix - 1) * c.nyf + (iy - 1)], sgn);
       }
     }
   }

@@ -18,6 +18,7 @@
 #include <cub/device/device_radix_sort.cuh>
 #include <math.h>
 #include <stdio.h>
+#include <stdlib.h>
 
 #include <algorithm>
 #include <vector>
@@ -1063,8 +1064,11 @@ int recontour_dev(casl_handle *h, const double *qq) {
   // a 64 MB table; 1M batches measured 20 % slower), so that the table (16
   // bytes per bucket, load <= 1/2) stays in L2 while the
   // batch's inserts and look-ups run; the keys carry the level, so a batch of
-  // several levels shares one table.
-  constexpr long long HB_BATCH = 1 << 21;
+  // several levels shares one table.  CASL_HASH_BATCH=<crossings> overrides
+  // the batch size (a test forces one level per batch with it).
+  long long HB_BATCH = 1 << 21;
+  if (const char *e = getenv("CASL_HASH_BATCH"))
+    if (atoll(e) > 0) HB_BATCH = atoll(e);
   long long *lstart = ar2.get<long long>(nlev + 1);
   if (ar2.failed) return CASL_ENOMEM;
   std::vector<long long> hl(nlev + 1);

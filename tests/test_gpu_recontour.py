@@ -89,3 +89,33 @@ def test_driver_steps_through_recontour(oracle_mod, gpu_lib):
         assert abs(dg[k] - do[k]) <= 1e-6 * abs(do[k]), (k, dg[k], do[k])
     assert dg["epot"] == 0.0 and do["epot"] == 0.0
     g.close()
+
+
+@pytest.mark.parametrize("batch", ["1", "5000"])
+def test_recontour_hash_batches(oracle_mod, gpu_lib, monkeypatch, batch):
+    """The crossing hash table run level batch by level batch.
+
+    Production batches hold about two million crossings, so at test sizes
+    every level shares one table; CASL_HASH_BATCH=1 gives each level its own
+    table (and its own clear), 5000 groups a few levels per table.  Topology
+    must come out identical to the oracle either way.
+    """
+    from hydra_b200.casl import CaslGPU
+    monkeypatch.setenv("CASL_HASH_BATCH", batch)
+    n = 128
+    q = random_pv(n, 8.0, 7)
+    o = oracle_mod.Oracle(n, ncontq=30, dtmax=0.05)
+    o.initialise(q)
+    g = CaslGPU(n, ncontq=30, dtmax=0.05)
+    g.initialise(q)
+    co, cg = o.contours(), g.contours()
+    same_topology(co, cg)
+    close_nodes(co, cg, 1e-10)
+    rng = np.random.default_rng(3)
+    resid = 0.05 * o.counts()[2] * rng.standard_normal((n, n))
+    o.recontour(resid)
+    g.recontour(resid)
+    co, cg = o.contours(), g.contours()
+    same_topology(co, cg)
+    close_nodes(co, cg, 1e-8)
+    g.close()
