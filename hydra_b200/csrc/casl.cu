@@ -424,16 +424,6 @@ __device__ __forceinline__ void c2g_decode(unsigned long long w, int &c0, int &c
   c3 = (int)v;
 }
 
-// Fire-and-forget global additions (no value returned to the thread).
-__device__ __forceinline__ void red_add_u64(unsigned long long *p, unsigned long long v) {
-  asm volatile("red.relaxed.gpu.global.add.u64 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "l"(v)
-               : "memory");
-}
-__device__ __forceinline__ void red_add_s32(int *p, int v) {
-  asm volatile("red.relaxed.gpu.global.add.s32 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "r"(v)
-               : "memory");
-}
-
 // Per segment (i, nextq(i)): x fine-grid-line crossings and the crossing of
 // y = ymin, counted as +-1 PV jumps (contours.f90:232-270): J += sgn at
 // each (PACKED: into the row's 16-bit lane of JW), ljx the bottom-boundary

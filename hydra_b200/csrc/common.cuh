@@ -103,6 +103,17 @@ __host__ __device__ __forceinline__ double wrapp(double xx, double ell, double h
   return oms * (xx - ell * f_dint(xx * hli));
 }
 
+// Fire-and-forget global additions: the counters are only read by later
+// launches, so no value comes back to the thread.
+__device__ __forceinline__ void red_add_u64(unsigned long long *p, unsigned long long v) {
+  asm volatile("red.relaxed.gpu.global.add.u64 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "l"(v)
+               : "memory");
+}
+__device__ __forceinline__ void red_add_s32(int *p, int v) {
+  asm volatile("red.relaxed.gpu.global.add.s32 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "r"(v)
+               : "memory");
+}
+
 // Device-resident scalars of one simulation (variables.f90 and adapt()).
 struct Scalars {
   double t, dt, dt2, dt3, dt6, twist;

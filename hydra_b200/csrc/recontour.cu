@@ -59,7 +59,7 @@ __global__ void k_u_scatter(const double *__restrict__ xq, const double *__restr
       double p = -(yi - c.hly * cc) / (dy + c.small);
       int ix = 1 + f_int(c.glxui * fmod(c.ellx + c.hlx + xi + p * dx, c.ellx));
       ix = ix < 1 ? 1 : (ix > nxu ? nxu : ix);
-      atomicAdd(&ljx[ix - 1], -(int)cc);
+      red_add_s32(&ljx[ix - 1], -(int)cc);
     }
     if (nxc != 0 && nxc >= -nxu && nxc <= nxu) {
       int jump = f_isign1(nxc);
@@ -73,7 +73,7 @@ __global__ void k_u_scatter(const double *__restrict__ xq, const double *__restr
         double px0 = (x2 - c.ellx * f_dint(x2 * c.hlxi)) / dx;
         double y2 = yi + px0 * dy;
         int iy = 2 + f_int(c.glyui * (y2 - c.elly * f_dint(y2 * c.hlyi) - c.ymin));
-        if (iy >= 2 && iy <= nyu) atomicAdd(&J[(long long)(ix - 1) * nyu + (iy - 1)], jump);
+        if (iy >= 2 && iy <= nyu) red_add_s32(&J[(long long)(ix - 1) * nyu + (iy - 1)], jump);
       }
     }
   }

@@ -102,7 +102,7 @@ __device__ __forceinline__ void rn_node(const RenodeIn &in, const RenodeScratch 
   s.Cc[w] = Cc;
   s.corner[w] = corner2;
   s.head[w] = (w == cs);
-  if (corner2) atomicAdd(&s.ccnt[k], 1);
+  if (corner2) red_add_s32(&s.ccnt[k], 1);
 }
 
 // One warp covers nodes base-2 .. base+29 (lane L holds node base-2+L) and
@@ -198,7 +198,7 @@ __global__ void k_rn_stencil(RenodeIn in, RenodeScratch s, Consts c) {
       s.Cc[o] = Cc;
       s.corner[o] = corner;
       s.head[o] = (o == cs);
-      if (corner) atomicAdd(&s.ccnt[k], 1);
+      if (corner) red_add_s32(&s.ccnt[k], 1);
     }
   }
 }
@@ -262,7 +262,8 @@ __global__ void k_rn_fill(RenodeIn in, RenodeScratch s, Consts c, int mode) {
       } else {
         st = s.cornerpos[cfirst + q];
         long long en = s.cornerpos[cfirst + (q + 1) % nc];
-        pl = (en - st + L) % L;
+        pl = en - st;  // both corners lie in [cs, cs+L)
+        if (pl < 0) pl += L;
         sum = sumrange(s.S, cs, L, st, pl);
         n = sum > c.small ? nint_d(sum) + 1 : 0;
       }
@@ -318,7 +319,9 @@ __global__ void k_rn_place(RenodeIn in, RenodeScratch s, RenodeOut out, Consts c
     int n = s.pn[p];
     if (n == 0) continue;
     long long st = s.pstart[p];
-    long long rel = (w - st + L) % L;
+    // w and the piece start both lie in the contour [cs, cs+L)
+    long long rel = w - st;
+    if (rel < 0) rel += L;
     if (rel >= s.plen[p]) continue;
     long long o = s.pout[p];
     if (rel == 0) {

@@ -45,6 +45,7 @@ struct SurgState {
   const double *x0, *y0, *dx0, *dy0;   // original
   const int *nq0, *prev0, *lvl;
   const int *kb1, *bcnt, *bnode;       // segment lists per box
+  const int *bnq;                      // nq0 of each bnode entry
   const int *nb1, *nbcnt, *nbnode;     // nodes located per box
   unsigned char *pending;
   // one bit per window of 512 nodes (a word per 16384) set wherever a
@@ -239,7 +240,7 @@ __global__ void k_sg_count_entries(SurgState S, const LevelDesc *__restrict__ le
     ecount[ib] = (mbx2 - mbx1 + 1) * (mby2 - mby1 + 1);
     int nb = node_box(S.x0[i], S.y0[i], L, c);
     nbox_of[ib] = nb;
-    atomicAdd(&nbcnt[nb], 1);
+    red_add_s32(&nbcnt[nb], 1);
   }
 }
 
@@ -265,7 +266,7 @@ __global__ void k_sg_emit(SurgState S, const LevelDesc *__restrict__ lev, int np
         ebox[e] = gb;
         eib[e] = ib;
         e++;
-        atomicAdd(&bcnt[gb], 1);
+        red_add_s32(&bcnt[gb], 1);
       }
     }
   }
@@ -273,14 +274,17 @@ __global__ void k_sg_emit(SurgState S, const LevelDesc *__restrict__ lev, int np
 
 __global__ void k_sg_place(const int *__restrict__ ebox, const int *__restrict__ eib,
                            const int *__restrict__ ne_dev, const int *__restrict__ kb1,
-                           int *__restrict__ cursor, int *__restrict__ bnode) {
+                           int *__restrict__ cursor, const int *__restrict__ nq0,
+                           int *__restrict__ bnode, int *__restrict__ bnq) {
   CASL_PDL_ENTRY();
   const long long ne = *ne_dev;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ne;
        e += (long long)gridDim.x * blockDim.x) {
     int gb = ebox[e];
     int pos = kb1[gb] + atomicAdd(&cursor[gb], 1);
-    bnode[pos] = eib[e];
+    const int isb = eib[e];
+    bnode[pos] = isb;
+    bnq[pos] = nq0[isb];  // the candidate search reads the segment's end node directly
   }
 }
 
@@ -321,12 +325,14 @@ __global__ void k_sg_candidates(SurgState S, const LevelDesc *__restrict__ lev, 
     double xi = S.x0[i], yi = S.y0[i];
     int k0 = S.kb1[mb], k1 = k0 + S.bcnt[mb];
     bool hit = false;
+    // the next entry's node index is loaded while this one is tested
+    int isn = k0 < k1 ? S.bnq[k0] : 0;
     for (int k = k0; k < k1 && !hit; k++) {
-      int isb = S.bnode[k];
-      int is = S.nq0[isb];
+      const int is = isn;
+      if (k + 1 < k1) isn = S.bnq[k + 1];
       if (is == ib || is == i) continue;
-      hit = surg_test(xi, yi, S.x0[is], S.y0[is], S.dx0[is], S.dy0[is],
-                      S.dx0[is] * S.dx0[is] + S.dy0[is] * S.dy0[is], c);
+      const double dxs = S.dx0[is], dys = S.dy0[is];
+      hit = surg_test(xi, yi, S.x0[is], S.y0[is], dxs, dys, dxs * dxs + dys * dys, c);
     }
     S.pending[ib] = hit ? 1 : 0;
     if (hit) atomicOr(&S.wsum[ib >> 14], 1u << ((ib >> 9) & 31));
@@ -799,7 +805,7 @@ int surgery_dev(casl_handle *h) {
   const long long nbox_cap = 2LL * npt + nq + 64;
   const long long ne_cap = 16LL * npt + 64;
   size_t need = (size_t)npt * 760 + (size_t)nq * 96 + (size_t)nbox_cap * 24 +
-                (size_t)ne_cap * 12 + ((size_t)64 << 20);
+                (size_t)ne_cap * 16 + ((size_t)64 << 20);
   int rc = ensure_scratch(h, need);
   if (rc) return rc;
   Arena ar{(char *)h->sx, h->sx_bytes, 0};
@@ -822,6 +828,7 @@ int surgery_dev(casl_handle *h) {
   int *bcnt = ar.get<int>(nbox_cap), *kb1 = ar.get<int>(nbox_cap), *cursor = ar.get<int>(nbox_cap);
   int *nbcnt = ar.get<int>(nbox_cap), *nb1 = ar.get<int>(nbox_cap), *nbnode = ar.get<int>(npt);
   int *ebox = ar.get<int>(ne_cap), *eib = ar.get<int>(ne_cap), *bnode = ar.get<int>(ne_cap);
+  int *bnq = ar.get<int>(ne_cap);
   if (ar.failed) return CASL_ENOMEM;
   const int g = gs(npt), gb = gs(nbox_cap);
   {
@@ -848,7 +855,7 @@ int surgery_dev(casl_handle *h) {
     const FillJob z[1] = {{cursor, nbox_cap, 0u}};
     if (int rc = fill_words(st, z, 1)) return rc;
   }
-  CASL_K(k_sg_place, gs(ne_cap), 256, 0, st)(ebox, eib, dtot + 2, kb1, cursor, bnode);
+  CASL_K(k_sg_place, gs(ne_cap), 256, 0, st)(ebox, eib, dtot + 2, kb1, cursor, nq0, bnode, bnq);
   exclusive_scan<int>(st, nbcnt, nb1, nbox_cap, tmpi, dtot + 5);
   {
     // the cursor again, and the replay's surgery count
@@ -856,7 +863,7 @@ int surgery_dev(casl_handle *h) {
     if (int rc = fill_words(st, z, 2)) return rc;
   }
   CASL_K(k_sg_place_nodes, g, 256, 0, st)(nbox_of, npt, nb1, cursor, nbnode);
-  S.kb1 = kb1; S.bcnt = bcnt; S.bnode = bnode; S.nb1 = nb1; S.nbcnt = nbcnt; S.nbnode = nbnode;
+  S.kb1 = kb1; S.bcnt = bcnt; S.bnode = bnode; S.bnq = bnq; S.nb1 = nb1; S.nbcnt = nbcnt; S.nbnode = nbnode;
   tr.point("binning");
   CASL_K(k_sg_candidates, g, 256, 0, st)(S, dlev, npt, nbox_of, c);
   tr.point("candidates");
