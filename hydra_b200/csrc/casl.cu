@@ -658,12 +658,34 @@ __global__ void __launch_bounds__(1024) k_c2g_packed_sum(const unsigned long lon
 #pragma unroll
     for (int u = 0; u < U; u++) v[u] = __ldcs(cp + u * 32);
   }
-  // lbot(col): the exclusive prefix of the bottom jumps (contours.f90:255-269)
-  int lb = 0;
-  if (warp < C2G_FC) {
-    for (int i = lane; i < col; i += 32) lb += ljx[i];
-    for (int o = 16; o > 0; o >>= 1) lb += __shfl_xor_sync(FULL, lb, o);
+  // lbot(col): the exclusive prefix of the bottom jumps (contours.f90:255-269),
+  // scanned by the whole block four entries a thread; the threads whose
+  // entries hold one of the block's columns keep that column's prefix
+  {
+    __shared__ int ptot;
+    const int c0 = 4 * cx0 - 3;
+    int pcarry = 0;
+    for (int base = 0; base < nf; base += 4 * SCAN_BLOCK) {
+      const int i0 = base + 4 * threadIdx.x;
+      int a[4];
+#pragma unroll
+      for (int k = 0; k < 4; k++) a[k] = i0 + k < nf ? ljx[i0 + k] : 0;
+      int pre = pcarry + block_excl_scan<int>(a[0] + a[1] + a[2] + a[3], &ptot);
+      int d = i0 - c0;  // this thread's first entry relative to the block's first column
+      d = d < 0 ? d + nf : (d >= nf ? d - nf : d);
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        int w = d + k;
+        if (w >= nf) w -= nf;
+        if (i0 + k < nf && w < C2G_FC) G0[w] = pre;
+        pre += a[k];
+      }
+      pcarry += ptot;
+      __syncthreads();
+    }
   }
+  const int lb = warp < C2G_FC ? G0[warp] : 0;
+  __syncthreads();  // G0 is reused for coarse row 0
   int carry = 0, q2 = 0, q3 = 0;       // running total; rows 4cy-2, 4cy-1 below lane 0
   int f0 = 0, f1 = 0, f2 = 0, f3 = 0;  // word 0 (rows 0..3), kept for coarse row 0
   long long local = 0;
