@@ -222,20 +222,32 @@ __device__ __forceinline__ double sumrange(const double *__restrict__ S, long lo
 
 __device__ __forceinline__ int nint_d(double x) { return (int)llround(x); }
 
-// Per contour: node count, pieces (contours.f90:799-809, 813-930).
+// Per contour: node count, pieces (contours.f90:799-809, 813-930), and
+// where its pieces are stored (block by block from a running total in
+// d_tot[1]; piece storage order is free, the output order comes from the
+// contour scan).
 __global__ void k_rn_count(RenodeIn in, RenodeScratch s, Consts c, int mode) {
   CASL_PDL_ENTRY();
+  __shared__ int btot, bbase;
   const int Ce = contours_in(in);
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < Ce; k += gridDim.x * blockDim.x) {
-    long long cs = in.cs[k], L = in.len[k];
-    double total = s.S[cs + L - 1];
-    s.ctot[k] = total;
+  for (int base = blockIdx.x * blockDim.x; base < Ce; base += gridDim.x * blockDim.x) {
+    const int k = base + threadIdx.x;
     int np = 0;
-    if (!(mode == RENODE_SURGERY && L <= 3)) {
-      int npr0 = nint_d(total) + 1;
-      if (npr0 >= 3) np = s.ccnt[k] > 1 ? s.ccnt[k] : 1;
+    if (k < Ce) {
+      long long cs = in.cs[k], L = in.len[k];
+      double total = s.S[cs + L - 1];
+      s.ctot[k] = total;
+      if (!(mode == RENODE_SURGERY && L <= 3)) {
+        int npr0 = nint_d(total) + 1;
+        if (npr0 >= 3) np = s.ccnt[k] > 1 ? s.ccnt[k] : 1;
+      }
+      s.npiece[k] = np;
     }
-    s.npiece[k] = np;
+    const int ex = block_excl_scan_any<int>(np, &btot);
+    if (threadIdx.x == 0) bbase = atomicAdd(&s.d_tot[1], btot);
+    __syncthreads();
+    if (k < Ce) s.poff[k] = bbase + ex;
+    __syncthreads();
   }
 }
 
@@ -425,8 +437,8 @@ int renode_batch(casl_handle *h, Arena &ar, const RenodeIn &in, RenodeOut &out, 
   s.psum = ar.get<double>(P); s.pfac = ar.get<double>(P);
   if (ar.failed) return CASL_ENOMEM;
   {
-    const FillJob z[1] = {{s.ccnt, C, 0u}};
-    if (int rc = fill_words(st, z, 1)) return rc;
+    const FillJob z[2] = {{s.ccnt, C, 0u}, {s.d_tot + 1, 1, 0u}};
+    if (int rc = fill_words(st, z, 2)) return rc;
   }
   int g = gsz(N);
   if (!in.cid) CASL_K(k_rn_cid, g, 256, 0, st)(in, N, s.cid);
@@ -438,7 +450,6 @@ int renode_batch(casl_handle *h, Arena &ar, const RenodeIn &in, RenodeOut &out, 
   // device), so the grids are sized for the usual counts and loop
   int gc = gsz(C < (1 << 16) ? C : (1 << 16));
   CASL_K(k_rn_count, gc, 256, 0, st)(in, s, c, mode);
-  exclusive_scan_dev<int>(st, s.npiece, s.poff, C, in.Cdev, s.tmpi, s.d_tot + 1);
   CASL_K(k_rn_fill, gc, 256, 0, st)(in, s, c, mode);
   CASL_K(k_rn_scan2_finish, 1, SCAN_BLOCK, 0, st)(in, s, out);
   CASL_K(k_rn_pout, gc, 256, 0, st)(in, s, out);

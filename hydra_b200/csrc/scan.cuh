@@ -67,6 +67,26 @@ __device__ T block_excl_scan(T v, T *total) {
   return r;
 }
 
+// Block-wide exclusive scan for any block size (a multiple of 32).
+template <class T>
+__device__ T block_excl_scan_any(T v, T *total) {
+  __shared__ T wsum[32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  T incl = warp_incl_scan(v);
+  if (lane == 31) wsum[wid] = incl;
+  __syncthreads();
+  if (wid == 0) {
+    T w = lane < nw ? wsum[lane] : T(0);
+    T wi = warp_incl_scan(w);
+    wsum[lane] = wi - w;
+    if (lane == 31) *total = wi;
+  }
+  __syncthreads();
+  T r = incl - v + wsum[wid];
+  __syncthreads();
+  return r;
+}
+
 template <class T>
 __global__ void __launch_bounds__(SCAN_BLOCK) k_scan_tiles(const T *__restrict__ in,
                                                            T *__restrict__ out,

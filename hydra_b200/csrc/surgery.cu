@@ -228,24 +228,93 @@ __global__ void k_sg_init(const double *__restrict__ xq, const double *__restric
   }
 }
 
+// Per segment: the number of box entries it makes, and where they start
+// relative to its block's share of the entries.  Block b takes the nodes
+// [b*chunk, (b+1)*chunk) in steps of blockDim.x with a running carry, then
+// takes its share of the entry array with one atomic on the running total
+// (bbase[b]); the entries' order in memory is free, since every box list is
+// read as a set.
 __global__ void k_sg_count_entries(SurgState S, const LevelDesc *__restrict__ lev, int npt,
-                                   int *__restrict__ ecount, int *__restrict__ nbox_of,
-                                   int *__restrict__ nbcnt, Consts c) {
+                                   int chunk, int *__restrict__ ecount, int *__restrict__ eoff,
+                                   int *__restrict__ bbase, int *__restrict__ ne_tot,
+                                   int *__restrict__ nbox_of, int *__restrict__ nbcnt, Consts c) {
   CASL_PDL_ENTRY();
-  for (int ib = blockIdx.x * blockDim.x + threadIdx.x; ib < npt; ib += gridDim.x * blockDim.x) {
-    LevelDesc L = lev[S.lvl[ib]];
-    int i = S.nq0[ib];
-    int mbx1, mbx2, mby1, mby2;
-    seg_boxes(S.x0[i], S.y0[i], S.dx0[i], S.dy0[i], L, c, mbx1, mbx2, mby1, mby2);
-    ecount[ib] = (mbx2 - mbx1 + 1) * (mby2 - mby1 + 1);
-    int nb = node_box(S.x0[i], S.y0[i], L, c);
-    nbox_of[ib] = nb;
-    red_add_s32(&nbcnt[nb], 1);
+  __shared__ int btot;
+  const int b0 = blockIdx.x * chunk, b1 = min(npt, b0 + chunk);
+  int carry = 0;
+  for (int base = b0; base < b1; base += blockDim.x) {
+    const int ib = base + threadIdx.x;
+    int cnt = 0;
+    if (ib < b1) {
+      LevelDesc L = lev[S.lvl[ib]];
+      int i = S.nq0[ib];
+      int mbx1, mbx2, mby1, mby2;
+      seg_boxes(S.x0[i], S.y0[i], S.dx0[i], S.dy0[i], L, c, mbx1, mbx2, mby1, mby2);
+      cnt = (mbx2 - mbx1 + 1) * (mby2 - mby1 + 1);
+      ecount[ib] = cnt;
+      int nb = node_box(S.x0[i], S.y0[i], L, c);
+      nbox_of[ib] = nb;
+      red_add_s32(&nbcnt[nb], 1);
+    }
+    const int ex = block_excl_scan_any<int>(cnt, &btot);
+    if (ib < b1) eoff[ib] = carry + ex;
+    carry += btot;
+  }
+  if (threadIdx.x == 0) bbase[blockIdx.x] = atomicAdd(ne_tot, carry);
+}
+
+// Start of every box's segment list and of its node list.  Block b takes
+// the boxes [b*chunk, (b+1)*chunk): it sums their counts, takes its share
+// of both lists with one atomic each (box order in memory is free), then
+// scans the counts again (from L2) and writes each start twice, the start
+// itself and the placement cursor.
+__global__ void __launch_bounds__(1024) k_sg_box_alloc(const int *__restrict__ bcnt,
+                                                       const int *__restrict__ nbcnt,
+                                                       const int *__restrict__ nbox_dev,
+                                                       long long nbox_cap, long long chunk,
+                                                       int *__restrict__ kb1,
+                                                       int *__restrict__ cb,
+                                                       int *__restrict__ nb1,
+                                                       int *__restrict__ cn,
+                                                       int *__restrict__ tot) {
+  CASL_PDL_ENTRY();
+  __shared__ unsigned long long btot;
+  __shared__ int bb[2];
+  const long long nbox = *nbox_dev < nbox_cap ? (long long)*nbox_dev : nbox_cap;
+  const long long g0 = (long long)blockIdx.x * chunk;
+  const long long g1 = g0 + chunk < nbox ? g0 + chunk : nbox;
+  if (g0 >= g1) return;
+  // both counts in one word: segment entries in the high half, nodes in the
+  // low half (each total stays below 2^31)
+  auto pack = [&](long long gb) -> unsigned long long {
+    return gb < g1 ? ((unsigned long long)bcnt[gb] << 32) | (unsigned)nbcnt[gb] : 0ull;
+  };
+  unsigned long long sum = 0;
+  for (long long gb = g0 + threadIdx.x; gb < g1; gb += blockDim.x) sum += pack(gb);
+  block_excl_scan_any<unsigned long long>(sum, &btot);
+  if (threadIdx.x == 0) {
+    bb[0] = atomicAdd(&tot[0], (int)(btot >> 32));
+    bb[1] = atomicAdd(&tot[1], (int)(btot & 0xffffffffu));
+  }
+  __syncthreads();
+  unsigned long long carry = ((unsigned long long)(unsigned)bb[0] << 32) | (unsigned)bb[1];
+  for (long long base = g0; base < g1; base += blockDim.x) {
+    const long long gb = base + threadIdx.x;
+    const unsigned long long ex = block_excl_scan_any<unsigned long long>(pack(gb), &btot) + carry;
+    if (gb < g1) {
+      const int k = (int)(ex >> 32), m = (int)(ex & 0xffffffffu);
+      kb1[gb] = k;
+      cb[gb] = k;
+      nb1[gb] = m;
+      cn[gb] = m;
+    }
+    carry += btot;
   }
 }
 
 __global__ void k_sg_emit(SurgState S, const LevelDesc *__restrict__ lev, int npt,
-                          const int *__restrict__ eoff, const int *__restrict__ ecount,
+                          const int *__restrict__ eoff, const int *__restrict__ bbase, int chunk,
+                          const int *__restrict__ ecount,
                           long long ne_cap, int *__restrict__ ebox, int *__restrict__ eib,
                           int *__restrict__ bcnt, Consts c, int *__restrict__ err) {
   CASL_PDL_ENTRY();
@@ -254,7 +323,7 @@ __global__ void k_sg_emit(SurgState S, const LevelDesc *__restrict__ lev, int np
     int i = S.nq0[ib];
     int mbx1, mbx2, mby1, mby2;
     seg_boxes(S.x0[i], S.y0[i], S.dx0[i], S.dy0[i], L, c, mbx1, mbx2, mby1, mby2);
-    int e = eoff[ib];
+    int e = eoff[ib] + bbase[ib / chunk];
     if ((long long)e + ecount[ib] > ne_cap) {
       atomicExch(err, CASL_ECAPACITY);
       continue;
@@ -273,7 +342,7 @@ __global__ void k_sg_emit(SurgState S, const LevelDesc *__restrict__ lev, int np
 }
 
 __global__ void k_sg_place(const int *__restrict__ ebox, const int *__restrict__ eib,
-                           const int *__restrict__ ne_dev, const int *__restrict__ kb1,
+                           const int *__restrict__ ne_dev,
                            int *__restrict__ cursor, const int *__restrict__ nq0,
                            int *__restrict__ bnode, int *__restrict__ bnq) {
   CASL_PDL_ENTRY();
@@ -281,7 +350,7 @@ __global__ void k_sg_place(const int *__restrict__ ebox, const int *__restrict__
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ne;
        e += (long long)gridDim.x * blockDim.x) {
     int gb = ebox[e];
-    int pos = kb1[gb] + atomicAdd(&cursor[gb], 1);
+    int pos = atomicAdd(&cursor[gb], 1);  // starts at the box's list start
     const int isb = eib[e];
     bnode[pos] = isb;
     bnq[pos] = nq0[isb];  // the candidate search reads the segment's end node directly
@@ -289,12 +358,12 @@ __global__ void k_sg_place(const int *__restrict__ ebox, const int *__restrict__
 }
 
 __global__ void k_sg_place_nodes(const int *__restrict__ nbox_of, int npt,
-                                 const int *__restrict__ nb1, int *__restrict__ cursor,
+                                 int *__restrict__ cursor,
                                  int *__restrict__ nbnode) {
   CASL_PDL_ENTRY();
   for (int ib = blockIdx.x * blockDim.x + threadIdx.x; ib < npt; ib += gridDim.x * blockDim.x) {
     int gb = nbox_of[ib];
-    nbnode[nb1[gb] + atomicAdd(&cursor[gb], 1)] = ib;
+    nbnode[atomicAdd(&cursor[gb], 1)] = ib;  // cursor starts at the box's list start
   }
 }
 
@@ -815,8 +884,8 @@ int surgery_dev(casl_handle *h) {
   // levels and boxes, on the device
   int *lex = ar.get<int>(nq);
   LevelDesc *dlev = ar.get<LevelDesc>(nq);
-  int *tmpi = ar.get<int>(scan_tmp_elems(std::max<long long>(std::max<long long>(npt, nbox_cap), ne_cap)) + 4);
-  int *dtot = ar.get<int>(16);  // [0] nlev, [1] nbox, [2] ne, [3] nsurg
+  // [0] nlev, [1] nbox, [2] ne, [3] nsurg, [4] box segment entries, [5] box nodes
+  int *dtot = ar.get<int>(16);
   int *endnext = ar.get<int>(npt), *lvl = ar.get<int>(npt);
   double *dx = ar.get<double>(npt), *dy = ar.get<double>(npt), *dsq = ar.get<double>(npt);
   double *x0 = ar.get<double>(npt), *y0 = ar.get<double>(npt);
@@ -827,16 +896,18 @@ int surgery_dev(casl_handle *h) {
   int *ecount = ar.get<int>(npt), *eoff = ar.get<int>(npt), *nbox_of = ar.get<int>(npt);
   int *bcnt = ar.get<int>(nbox_cap), *kb1 = ar.get<int>(nbox_cap), *cursor = ar.get<int>(nbox_cap);
   int *nbcnt = ar.get<int>(nbox_cap), *nb1 = ar.get<int>(nbox_cap), *nbnode = ar.get<int>(npt);
+  int *ncursor = ar.get<int>(nbox_cap), *bbase = ar.get<int>(148 * 16 + 1);
   int *ebox = ar.get<int>(ne_cap), *eib = ar.get<int>(ne_cap), *bnode = ar.get<int>(ne_cap);
   int *bnq = ar.get<int>(ne_cap);
   if (ar.failed) return CASL_ENOMEM;
   const int g = gs(npt), gb = gs(nbox_cap);
   {
-    const FillJob z[4] = {{endnext, npt, 0xffffffffu},
+    const FillJob z[5] = {{endnext, npt, 0xffffffffu},
                           {bcnt, nbox_cap, 0u},
                           {nbcnt, nbox_cap, 0u},
-                          {wsum, (npt >> 14) + 2, 0u}};
-    if (int rc = fill_words(st, z, 4)) return rc;
+                          {wsum, (npt >> 14) + 2, 0u},
+                          {dtot + 2, 4, 0u}};
+    if (int rc = fill_words(st, z, 5)) return rc;
   }
   CASL_K(k_lv_all, 1, SCAN_BLOCK, 0, st)(h->i1q, h->i2q, h->indq, nq, npt, c, dlev, lex, endnext,
                                          dtot, nbox_cap, err);
@@ -847,22 +918,23 @@ int surgery_dev(casl_handle *h) {
   S.x0 = x0; S.y0 = y0; S.dx0 = dx0; S.dy0 = dy0; S.nq0 = nq0; S.prev0 = prev0; S.lvl = lvl;
   S.pending = pending;
   S.wsum = wsum;
-  CASL_K(k_sg_count_entries, g, 256, 0, st)(S, dlev, npt, ecount, nbox_of, nbcnt, c);
-  exclusive_scan<int>(st, ecount, eoff, npt, tmpi, dtot + 2);
-  CASL_K(k_sg_emit, g, 256, 0, st)(S, dlev, npt, eoff, ecount, ne_cap, ebox, eib, bcnt, c, err);
-  exclusive_scan<int>(st, bcnt, kb1, nbox_cap, tmpi, dtot + 4);
+  // count_entries: at most 148*16 blocks, each a whole number of 256-node steps
+  const int echunk = (int)((((long long)npt + g - 1) / g + 255) / 256 * 256);
+  const int eg = (int)(((long long)npt + echunk - 1) / echunk);
+  CASL_K(k_sg_count_entries, eg, 256, 0, st)(S, dlev, npt, echunk, ecount, eoff, bbase, dtot + 2,
+                                             nbox_of, nbcnt, c);
+  CASL_K(k_sg_emit, g, 256, 0, st)(S, dlev, npt, eoff, bbase, echunk, ecount, ne_cap, ebox, eib,
+                                   bcnt, c, err);
   {
-    const FillJob z[1] = {{cursor, nbox_cap, 0u}};
-    if (int rc = fill_words(st, z, 1)) return rc;
+    // boxes in 296 chunks (two blocks of 1024 per SM), each a whole number
+    // of 1024-box steps
+    const long long bchunk = ((nbox_cap + 295) / 296 + 1023) / 1024 * 1024;
+    const int bg = (int)((nbox_cap + bchunk - 1) / bchunk);
+    CASL_K(k_sg_box_alloc, bg, 1024, 0, st)(bcnt, nbcnt, dtot + 1, nbox_cap, bchunk, kb1, cursor,
+                                            nb1, ncursor, dtot + 4);
   }
-  CASL_K(k_sg_place, gs(ne_cap), 256, 0, st)(ebox, eib, dtot + 2, kb1, cursor, nq0, bnode, bnq);
-  exclusive_scan<int>(st, nbcnt, nb1, nbox_cap, tmpi, dtot + 5);
-  {
-    // the cursor again, and the replay's surgery count
-    const FillJob z[2] = {{cursor, nbox_cap, 0u}, {dtot + 3, 1, 0u}};
-    if (int rc = fill_words(st, z, 2)) return rc;
-  }
-  CASL_K(k_sg_place_nodes, g, 256, 0, st)(nbox_of, npt, nb1, cursor, nbnode);
+  CASL_K(k_sg_place, gs(ne_cap), 256, 0, st)(ebox, eib, dtot + 2, cursor, nq0, bnode, bnq);
+  CASL_K(k_sg_place_nodes, g, 256, 0, st)(nbox_of, npt, ncursor, nbnode);
   S.kb1 = kb1; S.bcnt = bcnt; S.bnode = bnode; S.bnq = bnq; S.nb1 = nb1; S.nbcnt = nbcnt; S.nbnode = nbnode;
   tr.point("binning");
   CASL_K(k_sg_candidates, g, 256, 0, st)(S, dlev, npt, nbox_of, c);
