@@ -368,33 +368,29 @@ __global__ void k_rn_place(RenodeIn in, RenodeScratch s, RenodeOut out, Consts c
 __global__ void __launch_bounds__(SCAN_BLOCK) k_rn_scan2_finish(RenodeIn in, RenodeScratch s,
                                                                 RenodeOut out) {
   CASL_PDL_ENTRY();
-  __shared__ int tot, carry[2];
+  __shared__ unsigned long long tot;
   const long long n = contours_in(in);
-  if (threadIdx.x < 2) carry[threadIdx.x] = 0;
-  __syncthreads();
-  for (long long base = 0; base < n; base += SCAN_BLOCK) {
-    const long long k = base + threadIdx.x;
-    const int a = k < n ? s.cnpr[k] : 0, b = k < n ? s.ckeep[k] : 0;
-    const int ea = block_excl_scan<int>(a, &tot);
-    const int ta = tot;
-    __syncthreads();  // every thread has read tot before the next scan reuses it
-    const int eb = block_excl_scan<int>(b, &tot);
-    const int tb = tot;
-    if (k < n) {
-      s.cout[k] = ea + carry[0];
-      s.ckidx[k] = eb + carry[1];
-    }
-    __syncthreads();  // every thread has read the carries
-    if (threadIdx.x == 0) {
-      carry[0] += ta;
-      carry[1] += tb;
-    }
-    __syncthreads();
+  // each thread takes a run of consecutive contours; both counts go through
+  // one scan, the node counts in the high word and the keep flags in the low
+  // word (each total stays below 2^31)
+  auto pack = [&](long long k) -> unsigned long long {
+    return ((unsigned long long)(unsigned)s.cnpr[k] << 32) | (unsigned)s.ckeep[k];
+  };
+  const long long per = (n + SCAN_BLOCK - 1) / SCAN_BLOCK;
+  const long long k0 = min(n, (long long)threadIdx.x * per), k1 = min(n, k0 + per);
+  unsigned long long sum = 0;
+  for (long long k = k0; k < k1; k++) sum += pack(k);
+  unsigned long long ex = block_excl_scan<unsigned long long>(sum, &tot);
+  for (long long k = k0; k < k1; k++) {
+    s.cout[k] = (int)(ex >> 32);
+    s.ckidx[k] = (int)(ex & 0xffffffffu);
+    ex += pack(k);
   }
   if (threadIdx.x == 0) {
-    out.d_counts[0] = carry[1];
-    out.d_counts[1] = carry[0];
-    out.d_counts[2] = (long long)carry[0] > out.cap;
+    const long long nodes = (long long)(tot >> 32);
+    out.d_counts[0] = (int)(tot & 0xffffffffu);
+    out.d_counts[1] = (int)nodes;
+    out.d_counts[2] = nodes > out.cap;
   }
 }
 

@@ -119,30 +119,39 @@ __global__ void __launch_bounds__(SCAN_BLOCK) k_lv_all(const int *__restrict__ i
   CASL_PDL_ENTRY();
   __shared__ int tot, carry;
   const int tid = threadIdx.x;
-  if (tid == 0) carry = 0;
-  __syncthreads();
-  for (int base = 0; base < nq; base += SCAN_BLOCK) {
-    const int j = base + tid;
-    int f = 0;
-    if (j < nq) {
-      f = j == 0 || indq[j] > indq[j - 1];
-      if (j > 0 && indq[j] < indq[j - 1]) atomicExch(err, CASL_EINVAL);
+  // each thread takes a run of consecutive contours: it counts the level
+  // starts in its run, one block scan numbers them, and a second pass over
+  // the run writes the levels (two rounds of loads instead of one per
+  // 1024 contours)
+  const int per = (nq + SCAN_BLOCK - 1) / SCAN_BLOCK;
+  const int j0 = min(nq, tid * per), j1 = min(nq, j0 + per);
+  int cnt = 0;
+  {
+    int prev = j0 > 0 ? indq[j0 - 1] : 0;
+    for (int j = j0; j < j1; j++) {
+      const int v = indq[j];
+      cnt += j == 0 || v > prev;
+      if (j > 0 && v < prev) atomicExch(err, CASL_EINVAL);
+      prev = v;
     }
-    const int ex = block_excl_scan<int>(f, &tot) + carry;
-    if (j < nq) lidx[j] = ex + f - 1;  // the level of contour j
-    __syncthreads();
-    if (tid == 0) carry += tot;
-    __syncthreads();
   }
-  const int nlev = carry;
-  for (int j = tid; j < nq; j += SCAN_BLOCK) {
-    endnext[i2q[j]] = i1q[j];  // a contour's last node links back to its first
-    const int L = lidx[j];
-    if (j == 0 || indq[j] > indq[j - 1]) {
-      lev[L].ibeg = i1q[j];
-      lev[L].levt = indq[j];
+  int lv = block_excl_scan<int>(cnt, &tot) - 1;
+  const int nlev = tot;
+  {
+    int prev = j0 > 0 ? indq[j0 - 1] : 0;
+    for (int j = j0; j < j1; j++) {
+      const int v = indq[j], a = i1q[j], b = i2q[j];
+      const bool first = j == 0 || v > prev;
+      lv += first;
+      lidx[j] = lv;  // the level of contour j
+      endnext[b] = a;  // a contour's last node links back to its first
+      if (first) {
+        lev[lv].ibeg = a;
+        lev[lv].levt = v;
+      }
+      if (j == nq - 1 || indq[j + 1] > v) lev[lv].iend = b;
+      prev = v;
     }
-    if (j == nq - 1 || indq[j + 1] > indq[j]) lev[L].iend = i2q[j];
   }
   __syncthreads();
   if (tid == 0) carry = 0;
