@@ -246,7 +246,7 @@ __global__ void __launch_bounds__(SCAN_BLOCK) k_scan_apply(const T *in, T *out,
   if (grand && blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) *grand = off + tot;
 }
 
-constexpr int SCAN_TWO_PASS_MAX_TILES = 2048;
+constexpr int SCAN_TWO_PASS_MAX_TILES = 8192;  // 33.5M elements; above, three phases
 
 // out[i] = sum_{j<i} in[j]; *grand (device, optional) = sum of all.
 // in and out may alias.  tmp needs ceil(n/SCAN_TILE) elements.
