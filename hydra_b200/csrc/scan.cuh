@@ -281,53 +281,6 @@ int exclusive_scan(cudaStream_t st, const T *in, T *out, long long n, T *tmp, T 
 
 inline long long scan_tmp_elems(long long n) { return (n + SCAN_TILE - 1) / SCAN_TILE + 1; }
 
-// One block scans min(*n_dev, cap) elements, the count read on the device
-// (arrays sized by a capacity whose filled part only the device knows);
-// any count is handled, tile by tile.
-template <class T>
-__global__ void __launch_bounds__(SCAN_BLOCK) k_scan_small_dev(const T *__restrict__ in,
-                                                               T *__restrict__ out, long long cap,
-                                                               const int *__restrict__ n_dev,
-                                                               T *__restrict__ grand) {
-  CASL_PDL_ENTRY();
-  __shared__ T tot;
-  __shared__ T carry;
-  const long long n = *n_dev < cap ? (long long)*n_dev : cap;
-  if (threadIdx.x == 0) carry = 0;
-  __syncthreads();
-  for (long long tile = 0; tile * SCAN_TILE < n; tile++) {
-    long long base = tile * SCAN_TILE + (long long)threadIdx.x * SCAN_ITEMS;
-    T v[SCAN_ITEMS];
-    T s = 0;
-#pragma unroll
-    for (int k = 0; k < SCAN_ITEMS; k++) {
-      v[k] = (base + k < n) ? in[base + k] : T(0);
-      s += v[k];
-    }
-    T ex = block_excl_scan<T>(s, &tot) + carry;
-#pragma unroll
-    for (int k = 0; k < SCAN_ITEMS; k++) {
-      if (base + k < n) out[base + k] = ex;
-      ex += v[k];
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) carry += tot;
-    __syncthreads();
-  }
-  if (threadIdx.x == 0 && grand) *grand = carry;
-}
-
-// exclusive_scan over the first *n_dev (at most cap) elements; n_dev null:
-// all cap elements
-template <class T>
-int exclusive_scan_dev(cudaStream_t st, const T *in, T *out, long long cap, const int *n_dev,
-                       T *tmp, T *grand) {
-  if (!n_dev) return exclusive_scan<T>(st, in, out, cap, tmp, grand);
-  CASL_K(k_scan_small_dev<T>, 1, SCAN_BLOCK, 0, st)(in, out, cap, n_dev, grand);
-  return (int)cudaGetLastError();
-}
-
-
 // ---------------------------------------------------------------------------
 // Segmented inclusive scan of doubles: out[i] = sum of in[j] for j from the
 // last head at or before i through i.  head[i] != 0 starts a segment.
