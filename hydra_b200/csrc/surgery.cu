@@ -332,30 +332,33 @@ __global__ void k_sg_emit(SurgState S, const LevelDesc *__restrict__ lev, int np
     int i = S.nq0[ib];
     int mbx1, mbx2, mby1, mby2;
     seg_boxes(S.x0[i], S.y0[i], S.dx0[i], S.dy0[i], L, c, mbx1, mbx2, mby1, mby2);
-    int e = eoff[ib] + bbase[ib / chunk];
-    if ((long long)e + ecount[ib] > ne_cap) {
-      atomicExch(err, CASL_ECAPACITY);
-      continue;
-    }
+    long long e = (long long)eoff[ib] + bbase[ib / chunk];
+    // Past the capacity nothing is written (CASL_ECAPACITY is raised): the
+    // offsets tile [0, total) densely, so every entry below the capacity is
+    // written, and the box counts count exactly the entries written.
+    if (e + ecount[ib] > ne_cap) atomicExch(err, CASL_ECAPACITY);
     for (int mbx = mbx1; mbx <= mbx2; mbx++) {
       int mmbx = mbx % L.nbx;
       for (int mby = mby1; mby <= mby2; mby++) {
         int gb = L.boxbase + L.nby * mmbx + mby % L.nby;
-        ebox[e] = gb;
-        eib[e] = ib;
+        if (e < ne_cap) {
+          ebox[e] = gb;
+          eib[e] = ib;
+          red_add_s32(&bcnt[gb], 1);
+        }
         e++;
-        red_add_s32(&bcnt[gb], 1);
       }
     }
   }
 }
 
 __global__ void k_sg_place(const int *__restrict__ ebox, const int *__restrict__ eib,
-                           const int *__restrict__ ne_dev,
+                           const int *__restrict__ ne_dev, long long ne_cap,
                            int *__restrict__ cursor, const int *__restrict__ nq0,
                            int *__restrict__ bnode, int *__restrict__ bnq) {
   CASL_PDL_ENTRY();
-  const long long ne = *ne_dev;
+  // the emit pass wrote the entries below the capacity only
+  const long long ne = *ne_dev < ne_cap ? (long long)*ne_dev : ne_cap;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ne;
        e += (long long)gridDim.x * blockDim.x) {
     int gb = ebox[e];
@@ -942,7 +945,7 @@ int surgery_dev(casl_handle *h) {
     CASL_K(k_sg_box_alloc, bg, 1024, 0, st)(bcnt, nbcnt, dtot + 1, nbox_cap, bchunk, kb1, cursor,
                                             nb1, ncursor, dtot + 4);
   }
-  CASL_K(k_sg_place, gs(ne_cap), 256, 0, st)(ebox, eib, dtot + 2, cursor, nq0, bnode, bnq);
+  CASL_K(k_sg_place, gs(ne_cap), 256, 0, st)(ebox, eib, dtot + 2, ne_cap, cursor, nq0, bnode, bnq);
   CASL_K(k_sg_place_nodes, g, 256, 0, st)(nbox_of, npt, ncursor, nbnode);
   S.kb1 = kb1; S.bcnt = bcnt; S.bnode = bnode; S.bnq = bnq; S.nb1 = nb1; S.nbcnt = nbcnt; S.nbnode = nbnode;
   tr.point("binning");
