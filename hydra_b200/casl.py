@@ -51,6 +51,7 @@ class CaslParams(C.Structure):
 _lib = None
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
+_fp = C.POINTER(C.c_float)
 
 # name -> (restype, argtypes); the same list is checked against the header by tests
 SIGNATURES = {
@@ -111,6 +112,22 @@ SIGNATURES = {
     "casl_readcont": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int]),
     "casl_genfg": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                              C.POINTER(C.c_float)]),
+    "casl_net_param_count": (C.c_int, []),
+    "casl_net_create": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "casl_net_destroy": (None, [C.c_void_p]),
+    "casl_net_set_params": (C.c_int, [C.c_void_p, _fp, C.c_float, C.c_float]),
+    "casl_net_get_params": (C.c_int, [C.c_void_p, _fp, _fp, _fp]),
+    "casl_net_forward": (C.c_int, [C.c_void_p, _fp, _fp]),
+    "casl_net_backward": (C.c_int, [C.c_void_p, _fp, _fp]),
+    "casl_net_adam": (C.c_int, [C.c_void_p, C.c_float]),
+    "casl_closure_judge": (C.c_int, [C.c_void_p, C.c_void_p, _dp, _dp, _dp, _dp]),
+    "casl_closure_attach": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_double]),
+    "casl_closure_status": (C.c_int, [C.c_void_p, _ip, _dp, _dp, C.POINTER(C.c_longlong),
+                                      C.POINTER(C.c_longlong)]),
+    "casl_closure_check": (C.c_int, [C.c_void_p, _dp, _dp]),
+    "casl_closure_train": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, _dp]),
+    "casl_closure_evaluate": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, _dp]),
+    "casl_closure_features": (C.c_int, [C.c_void_p, C.c_void_p, _fp]),
 }
 
 
@@ -358,6 +375,53 @@ class CaslGPU:
         self._check(self.lib.casl_spec1d(self.h, _d(a), _d(spec), int(iopt)), "casl_spec1d")
         return spec, a
 
+    # --- learned velocity closure ---------------------------------------------------
+    def judge(self, fine):
+        """Node velocities of the fine-grid judge (handle `fine`, 2-8x the grid)
+        and of the plain velint: (uJ, vJ, uP, vP)."""
+        _, npt, _ = self.counts()
+        out = [np.empty(npt) for _ in range(4)]
+        self._check(self.lib.casl_closure_judge(self.h, fine.h, *[_d(a) for a in out]),
+                    "casl_closure_judge")
+        return tuple(out)
+
+    def closure_attach(self, net, judge=None, check_every=0, budget=1e-3):
+        self._check(self.lib.casl_closure_attach(self.h, net.h if net else None,
+                                                 judge.h if judge else None, int(check_every),
+                                                 float(budget)), "casl_closure_attach")
+
+    def closure_status(self):
+        a, ep, en = C.c_int(), C.c_double(), C.c_double()
+        ch, fb = C.c_longlong(), C.c_longlong()
+        self._check(self.lib.casl_closure_status(self.h, C.byref(a), C.byref(ep), C.byref(en),
+                                                 C.byref(ch), C.byref(fb)), "casl_closure_status")
+        return dict(active=a.value, err_plain=ep.value, err_net=en.value, checks=ch.value,
+                    fallbacks=fb.value)
+
+    def closure_check(self):
+        ep, en = C.c_double(), C.c_double()
+        self._check(self.lib.casl_closure_check(self.h, C.byref(ep), C.byref(en)), "casl_closure_check")
+        return ep.value, en.value
+
+    def closure_train(self, net, judge, lr):
+        """One training sample; returns (plain error, corrected error, loss)."""
+        out = np.zeros(3)
+        self._check(self.lib.casl_closure_train(self.h, net.h, judge.h, float(lr), _d(out)),
+                    "casl_closure_train")
+        return tuple(out)
+
+    def closure_evaluate(self, net, judge):
+        out = np.zeros(3)
+        self._check(self.lib.casl_closure_evaluate(self.h, net.h, judge.h, _d(out)),
+                    "casl_closure_evaluate")
+        return tuple(out)
+
+    def closure_features(self, net):
+        x = np.empty((3, self.nx, self.ny), np.float32)
+        self._check(self.lib.casl_closure_features(self.h, net.h, x.ctypes.data_as(_fp)),
+                    "casl_closure_features")
+        return x
+
     def spec_tables(self):
         """kmax, kmaxred, spmf, alk of init_spectral (spectral.f90:109-134)."""
         kmax, kred = C.c_int(), C.c_int()
@@ -365,3 +429,70 @@ class CaslGPU:
         self._check(self.lib.casl_spec_tables(self.h, C.byref(kmax), C.byref(kred), _d(spmf), _d(alk)),
                     "casl_spec_tables")
         return dict(kmax=kmax.value, kmaxred=kred.value, spmf=spmf, alk=alk)
+
+
+def _f32(a, shape=None):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    if shape is not None and a.shape != shape:
+        raise ValueError(f"expected shape {shape}, got {a.shape}")
+    return a
+
+
+def _fptr(a):
+    return a.ctypes.data_as(_fp) if a is not None else None
+
+
+class CaslNet:
+    """The learned velocity closure's network on one GPU (casl_net_*): four
+    periodic 5x5 convolutions 3 -> 32 -> 32 -> 32 -> 2 with GELU, BF16
+    weights and activations, FP32 accumulation, on the tensor cores.  Arrays
+    are channel-major (C, n, n) float32 with rows = ix, columns = iy."""
+
+    def __init__(self, n, device=0):
+        self.lib = load_library()
+        h = C.c_void_p()
+        self._check(self.lib.casl_net_create(int(n), int(device), C.byref(h)), "casl_net_create")
+        self.h = h
+        self.n = n
+        self.count = self.lib.casl_net_param_count()
+
+    _check = CaslGPU._check
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.casl_net_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_params(self, params, qscale=1.0, uscale=1.0):
+        p = _f32(params, (self.count,))
+        self._check(self.lib.casl_net_set_params(self.h, _fptr(p), float(qscale), float(uscale)),
+                    "casl_net_set_params")
+
+    def params(self):
+        p = np.empty(self.count, np.float32)
+        qs, us = C.c_float(), C.c_float()
+        self._check(self.lib.casl_net_get_params(self.h, _fptr(p), C.byref(qs), C.byref(us)),
+                    "casl_net_get_params")
+        return p, qs.value, us.value
+
+    def forward(self, x):
+        x = _f32(x, (3, self.n, self.n))
+        y = np.empty((2, self.n, self.n), np.float32)
+        self._check(self.lib.casl_net_forward(self.h, _fptr(x), _fptr(y)), "casl_net_forward")
+        return y
+
+    def backward(self, dy):
+        """Gradient of sum(dy * y) for the last forward, flat in parameter order."""
+        dy = _f32(dy, (2, self.n, self.n))
+        g = np.empty(self.count, np.float32)
+        self._check(self.lib.casl_net_backward(self.h, _fptr(dy), _fptr(g)), "casl_net_backward")
+        return g
+
+    def adam(self, lr):
+        self._check(self.lib.casl_net_adam(self.h, float(lr)), "casl_net_adam")

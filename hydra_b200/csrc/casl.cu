@@ -136,8 +136,9 @@ static int launch_rfft(casl_handle *h, LD ld, ST st, int batch) {
   if (prof) {
     cudaEventRecord(h->prof_ev[2 * h->prof_n + 1], h->stream);
     h->prof_n++;
-    // algorithmic bytes: every element of every vector read once and written once
-    h->prof_bytes += (double)batch * (double)Sh::N * (double)Sh::N * (ld.bytes() + st.bytes());
+    // algorithmic bytes of a 2-D transform: each field read once and written
+    // once (16 B per FP64 element); each of its two passes accounts for half
+    h->prof_bytes += (double)batch * (double)Sh::N * (double)Sh::N * 8.0;
   }
   return check_launch(h);
 }
@@ -1293,12 +1294,13 @@ static int source_prod(casl_handle *h, int stage) {
 
 }  // namespace casl
 
-// node update and spectral RK update of a stage, one launch
-static int stage_update(casl_handle *h, int stage) {
+// node update and spectral RK update of a stage, one launch; velint reads
+// the velocity fields u, v
+static int stage_update(casl_handle *h, int stage, const double *u, const double *v) {
   const long long nn = (long long)h->n * h->n;
   const int nbn = h->contex ? grid_for(h->nptq > 0 ? h->nptq : 1) : 0;
   const int g = nbn + grid_for(nn / 2);
-  const NodeRkArgs a{h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, h->uu, h->vv};
+  const NodeRkArgs a{h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, u, v};
   const SpecRkArgs b{h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs, h->sqd, h->emq, nn};
   cudaStream_t st = h->stream;
   switch (stage) {
@@ -1322,10 +1324,126 @@ static int advance_dev(casl_handle *h) {
     if ((rc = invert_and_gradients(h))) return rc;
     if (stage == 1 && (rc = adapt_dev(h))) return rc;
     if ((rc = source_prod(h, stage))) return rc;
-    if ((rc = stage_update(h, stage))) return rc;
+    const double *u = h->uu, *v = h->vv;
+    if (h->closure && (rc = closure_stage(h, &u, &v))) return rc;
+    if ((rc = stage_update(h, stage, u, v))) return rc;
   }
   return CASL_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Fine-grid judge of node velocities
+// ---------------------------------------------------------------------------
+namespace casl {
+// Stafft-layout spectral coefficient of wavenumber k along an axis of length
+// m: index k (cosine, 0 <= k <= m/2) or m - k (sine, 0 < k < m/2).  The same
+// band-limited field transformed on grids of n and nf = r n points has
+// coefficients in the ratio sqrt(r) per axis, except that the cosine at the
+// coarse Nyquist wavenumber n/2 (a regular mode of the fine grid) is in the
+// ratio sqrt(r)/2 (stafft.f90:187-287 normalises forward transforms by
+// 1/sqrt(n)).
+__device__ __forceinline__ bool pad_axis(int idxf, int nf, int n, int &idx, double &fac) {
+  const bool sine = idxf > nf / 2;
+  const int k = sine ? nf - idxf : idxf;
+  if (k > n / 2 || (sine && k == n / 2)) return false;
+  idx = sine ? n - k : k;
+  const double s = sqrt((double)nf / (double)n);
+  fac = (k == n / 2) ? 0.5 * s : s;
+  return true;
+}
+
+// qqf = qcf + the spectrum of (qq - qc) on the coarse grid, carried to the
+// fine grid (spectral arrays [ky][kx], kx fastest).
+__global__ void k_pad_add(const double *__restrict__ qq, const double *__restrict__ qc, int n,
+                          const double *__restrict__ qcf, double *__restrict__ qqf, int nf) {
+  CASL_PDL_ENTRY();
+  const long long nnf = (long long)nf * nf;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nnf;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int kyf = (int)(t / nf), kxf = (int)(t % nf);
+    int ix, iy;
+    double fx, fy;
+    double v = qcf[t];
+    if (pad_axis(kxf, nf, n, ix, fx) && pad_axis(kyf, nf, n, iy, fy)) {
+      const long long k = (long long)iy * n + ix;
+      v += (qq[k] - qc[k]) * (fx * fy);
+    }
+    qqf[t] = v;
+  }
+}
+
+int judge_velocity(casl_handle *h, casl_handle *hf, double *uJ, double *vJ, double *uP,
+                   double *vP) {
+  const int n = h->n, nf = hf->n;
+  if (nf != 2 * n && nf != 4 * n && nf != 8 * n) return CASL_EINVAL;
+  if (h->c.ellx != hf->c.ellx || h->c.elly != hf->c.elly) return CASL_EINVAL;
+  int rc = sync_counts(h);
+  if (rc) return rc;
+  const int npt = h->nptq, nq = h->nq;
+  if (npt > hf->npm || nq > hf->nm) return CASL_ECAPACITY;
+  // the coarse inversion: qq, qc (spectral), uu, vv of h
+  if ((rc = inversion_dev(h, false))) return rc;
+  if (uP && npt)
+    CASL_K(k_velint, grid_for(npt), 256, 0, h->stream)(h->xq, h->yq, npt, h->uu, h->vv, uP, vP,
+                                                     h->c);
+  // contours to the fine handle (internal 0-based links on both)
+  cudaEvent_t ev;
+  CASL_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  CASL_CUDA_TRY(cudaEventRecord(ev, h->stream));
+  CASL_CUDA_TRY(cudaStreamWaitEvent(hf->stream, ev, 0));
+  cudaStream_t s = hf->stream;
+  if (npt) {
+    CASL_CUDA_TRY(cudaMemcpyAsync(hf->xq, h->xq, npt * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    CASL_CUDA_TRY(cudaMemcpyAsync(hf->yq, h->yq, npt * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    CASL_CUDA_TRY(cudaMemcpyAsync(hf->nextq, h->nextq, npt * sizeof(int), cudaMemcpyDeviceToDevice, s));
+  }
+  if (nq) {
+    int *src[4] = {h->i1q, h->i2q, h->npq, h->indq}, *dst[4] = {hf->i1q, hf->i2q, hf->npq, hf->indq};
+    for (int i = 0; i < 4; i++)
+      CASL_CUDA_TRY(cudaMemcpyAsync(dst[i], src[i], nq * sizeof(int), cudaMemcpyDeviceToDevice, s));
+  }
+  if ((rc = get_scalars(hf))) return rc;
+  hf->hscal->nq = nq;
+  hf->hscal->nptq = npt;
+  hf->hscal->qjump = h->qjump;
+  hf->hscal->error = 0;
+  hf->nq = nq;
+  hf->nptq = npt;
+  hf->qjump = h->qjump;
+  hf->contex = npt > 0;
+  if ((rc = put_scalars(hf))) return rc;
+  // contour PV on the fine grid (its con2grid and forward transform), then
+  // the coarse non-contour spectrum added, then the fine inversion
+  const long long nnf = (long long)nf * nf;
+  if (npt) {
+    if ((rc = con2grid_dev(hf, false))) return rc;
+    LoadQC ld{hf->coarseC, hf->scal, hf->c.beffect ? hf->betac : nullptr, nnf,
+              1.0 / (256.0 * (double)nf * (double)nf), nf};
+    casl_handle *hh = hf;
+    {
+      casl_handle *h = hh;  // RFFT_DISPATCH launches on h's stream at h's size
+      if ((rc = RFFT_DISPATCH(true, false, true, ld, (StoreStrided{h->qc, nnf, 1, (long long)nf}), 1)))
+        return rc;
+      if ((rc = RFFT_DISPATCH(true, false, false, (LoadStrided{h->qc, nnf, (long long)nf, 1}),
+                              (StoreStrided{h->qc, nnf, (long long)nf, 1}), 1)))
+        return rc;
+    }
+  } else {
+    CASL_CUDA_TRY(cudaMemsetAsync(hf->qc, 0, nnf * sizeof(double), s));
+  }
+  CASL_CUDA_TRY(cudaEventRecord(ev, h->stream));
+  CASL_CUDA_TRY(cudaStreamWaitEvent(s, ev, 0));
+  CASL_K(k_pad_add, grid_for(nnf), 256, 0, s)(h->qq, h->qc, n, hf->qc, hf->qq, nf);
+  if ((rc = main_invert_dev(hf))) return rc;
+  if (npt)
+    CASL_K(k_velint, grid_for(npt), 256, 0, s)(hf->xq, hf->yq, npt, hf->uu, hf->vv, uJ, vJ,
+                                             hf->c);
+  CASL_CUDA_TRY(cudaEventRecord(ev, s));
+  CASL_CUDA_TRY(cudaStreamWaitEvent(h->stream, ev, 0));
+  CASL_CUDA_TRY(cudaEventDestroy(ev));
+  return check_launch(hf);
+}
+}  // namespace casl
 
 // ---------------------------------------------------------------------------
 // Host-side set-up: constants.f90, spectral.f90:42-158 (same operations and
@@ -1843,6 +1961,7 @@ void casl_destroy(casl_handle *h) {
   cudaSetDevice(h->device);
   io_release(h);
   cudaStreamSynchronize(h->stream);
+  closure_release(h);
   free_all(h);
   if (h->prof_ev) {
     for (int i = 0; i < 2 * CASL_PROF_MAX; i++) cudaEventDestroy(h->prof_ev[i]);
@@ -1888,6 +2007,29 @@ __global__ void k_to0(int *a, long long m, int off) {
     a[i] += off;
 }
 
+// The checks casl_set_contours makes on the uploaded state, reported through
+// the sticky error word: every node finite and inside the domain
+// [xmin,xmax) x [ymin,ymax) that con2grid and the box searches index with
+// (CASL_EDOMAIN); every successor, and every contour's node range, inside the
+// node arrays (CASL_EINVAL).  Links are 0-based here.
+__global__ void k_validate(const double *__restrict__ xq, const double *__restrict__ yq,
+                           const int *__restrict__ nextq, int npt, const int *__restrict__ i1q,
+                           const int *__restrict__ i2q, const int *__restrict__ npq, int nq,
+                           Consts c, Scalars *__restrict__ s) {
+  CASL_PDL_ENTRY();
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < npt; i += stride) {
+    double x = xq[i], y = yq[i];
+    if (!(x >= c.xmin && x < c.xmax && y >= c.ymin && y < c.ymax)) atomicExch(&s->error, CASL_EDOMAIN);
+    int nx = nextq[i];
+    if (nx < 0 || nx >= npt) atomicExch(&s->error, CASL_EINVAL);
+  }
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < nq; j += stride) {
+    int a = i1q[j], b = i2q[j];
+    if (a < 0 || b >= npt || b < a || npq[j] != b - a + 1) atomicExch(&s->error, CASL_EINVAL);
+  }
+}
+
 int casl_set_contours(casl_handle *h, int nq, int nptq, double qjump, const double *xq,
                       const double *yq, const int *nextq, const int *indq, const int *npq,
                       const int *i1q, const int *i2q) {
@@ -1910,8 +2052,23 @@ int casl_set_contours(casl_handle *h, int nq, int nptq, double qjump, const doub
     CASL_K(k_to0, grid_for(nq), 256, 0, s)(h->i1q, nq, -1);
     CASL_K(k_to0, grid_for(nq), 256, 0, s)(h->i2q, nq, -1);
   }
+  // a new state replaces the old one, and with it any error the old one left
+  const FillJob z[1] = {{&h->scal->error, 1, 0u}};
+  if (int rc = fill_words(s, z, 1)) return rc;
+  if (nptq || nq)
+    CASL_K(k_validate, grid_for(nptq > nq ? nptq : nq), 256, 0, s)(
+        h->xq, h->yq, h->nextq, nptq, h->i1q, h->i2q, h->npq, nq, h->c, h->scal);
   int rc = get_scalars(h);
   if (rc) return rc;
+  if (int bad = h->hscal->error) {
+    // rejected: leave an empty state rather than one that would fault later
+    h->hscal->error = 0;
+    h->hscal->nq = h->hscal->nptq = 0;
+    h->nq = h->nptq = 0;
+    h->contex = 0;
+    if ((rc = put_scalars(h))) return rc;
+    return bad;
+  }
   h->hscal->nq = nq;
   h->hscal->nptq = nptq;
   h->hscal->qjump = qjump;
@@ -2344,6 +2501,7 @@ int casl_step(casl_handle *h, int nsteps) {
         CASL_K(k_twist_sub, 1, 1, 0, h->stream)(h->scal, h->p.twistmax);
       }
     }
+    if (h->closure && (rc = closure_step_check(h))) return rc;
     h->node_steps += (double)h->nptq;
     if ((rc = advance_dev(h))) return rc;
   }

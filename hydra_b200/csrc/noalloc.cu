@@ -32,8 +32,16 @@ constexpr int NA_MAX_N = 256;                         // largest grid served
 constexpr long long NA_FINE = 16LL * NA_MAX_N * NA_MAX_N;  // (4n)^2 fine cells
 constexpr long long NA_LJX = 4LL * NA_MAX_N;
 constexpr long long NA_COARSE = 1LL * NA_MAX_N * NA_MAX_N;
-constexpr long long NA_MISC = 64;                     // csum (8 B) + error flag
+constexpr long long NA_MISC = 64;                     // csum (8 B) + error flag + spare
 constexpr long long NA_INTS = NA_FINE + NA_LJX + NA_COARSE + NA_MISC;
+// Offsets (in ints) of the per-call counters inside the misc region; the
+// whole region is cleared at the start of every call.
+constexpr long long NA_MISC_OFF = NA_FINE + NA_LJX + NA_COARSE;
+constexpr long long NA_CSUM_OFF = NA_MISC_OFF;        // unsigned long long, 2 ints
+constexpr long long NA_ERR_OFF = NA_MISC_OFF + 2;     // int
+static_assert(NA_MISC_OFF % 2 == 0, "csum must be 8-byte aligned");
+static_assert(NA_CSUM_OFF + 2 <= NA_MISC_OFF + NA_MISC && NA_ERR_OFF + 1 <= NA_MISC_OFF + NA_MISC,
+              "the per-call counters must lie inside the cleared misc region");
 
 // The scratch.  Every GPU that loads the library holds it (4.3 MB) until the
 // process exits; all calls on a device share it.
@@ -107,7 +115,10 @@ __global__ void k_na_final(const int *__restrict__ C, const unsigned long long *
   }
 }
 
-// Device address of g_na_scratch per device, looked up once per device.
+// Device address of g_na_scratch per device, looked up once per device in the
+// device's primary context (the runtime API's context).  The lookup is also
+// where CUDA's lazy module loading brings the library's device code, and with
+// it the array, onto the device.
 std::mutex g_na_mutex;
 int *g_na_ptr[64] = {nullptr};
 
@@ -137,6 +148,10 @@ extern "C" int casl_con2grid_noalloc(int n, double ellx, double elly, int nptq, 
       !qc_dev)
     return CASL_EINVAL;
   if (nptq > 0 && (!xq_dev || !yq_dev || !nextq_dev)) return CASL_EINVAL;
+  // An error the caller left pending is the caller's: report it without
+  // consuming it, so that the error checks after the launches below see only
+  // this call's own errors.
+  if (cudaPeekAtLastError() != cudaSuccess) return CASL_ECUDA;
   cudaStream_t st = (cudaStream_t)stream;
   const long long nn = (long long)n * n;
   if (nptq == 0) {
@@ -150,8 +165,8 @@ extern "C" int casl_con2grid_noalloc(int n, double ellx, double elly, int nptq, 
   int *J = base;                                   // (nf, nf) jump counts -> levels
   int *ljx = base + NA_FINE;                       // (nf) bottom-row jumps
   int *C = base + NA_FINE + NA_LJX;                // (n, n) coarse integer cells
-  unsigned long long *csum = (unsigned long long *)(base + NA_FINE + NA_LJX + NA_COARSE);
-  int *err = base + NA_FINE + NA_LJX + NA_COARSE + 4;
+  unsigned long long *csum = (unsigned long long *)(base + NA_CSUM_OFF);
+  int *err = base + NA_ERR_OFF;
 
   // constants as constants.f90 / contours.f90 define them
   NaConsts c;
@@ -175,7 +190,8 @@ extern "C" int casl_con2grid_noalloc(int n, double ellx, double elly, int nptq, 
   // The array keeps the previous call's contents: clear what accumulates.
   if (cudaMemsetAsync(J, 0, (size_t)nf * nf * sizeof(int), st) != cudaSuccess) return CASL_ECUDA;
   if (cudaMemsetAsync(ljx, 0, (size_t)nf * sizeof(int), st) != cudaSuccess) return CASL_ECUDA;
-  if (cudaMemsetAsync(csum, 0, NA_MISC * sizeof(int) / 2, st) != cudaSuccess) return CASL_ECUDA;
+  if (cudaMemsetAsync(base + NA_MISC_OFF, 0, NA_MISC * sizeof(int), st) != cudaSuccess)
+    return CASL_ECUDA;
   int g = (nptq + 255) / 256;
   if (g > 148 * 16) g = 148 * 16;
   CASL_K(k_na_scatter, g, 256, 0, st)(xq_dev, yq_dev, nextq_dev, nptq, J, ljx, c, err);

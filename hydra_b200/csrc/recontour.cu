@@ -442,15 +442,19 @@ __global__ void k_h_insert(const int *__restrict__ rlev, const unsigned int *__r
     unsigned long long k = hkey(rlev[r], kob[r]);
     unsigned long long p = hmix(k) & mask;
     const int slot = base + (int)r;
+    bool inserted = false;
     for (unsigned long long probe = 0; probe <= mask; probe++) {
       unsigned long long prev = atomicCAS(&hb[p].key, HEMPTY, k);
       if (prev == HEMPTY || prev == k) {
         if (atomicCAS(&hb[p].s0, -1, slot) != -1)
           if (atomicCAS(&hb[p].s1, -1, slot) != -1) atomicExch(err, CASL_ECAPACITY);
+        inserted = true;
         break;
       }
       p = (p + 1) & mask;
     }
+    // a full table would leave this crossing out of the (level, box) table
+    if (!inserted) atomicExch(err, CASL_ECAPACITY);
   }
 }
 

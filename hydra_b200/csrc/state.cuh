@@ -9,6 +9,10 @@
 #include "../../include/hydra_casl.h"
 #include "common.cuh"
 
+namespace casl {
+struct ClosureState;  // the learned velocity closure attached to a handle (closure.cu)
+}
+
 struct casl_handle {
   casl_params p;
   casl::Consts c;
@@ -65,6 +69,8 @@ struct casl_handle {
   int prof_n;
   double prof_bytes;
   cudaEvent_t *prof_ev;  // 2 * CASL_PROF_MAX events, created on first use
+
+  casl::ClosureState *closure;  // learned velocity closure (nullable)
 };
 
 #define CASL_PROF_MAX 8192
@@ -112,5 +118,20 @@ struct Trace {
 };
 int ensure_scratch(casl_handle *h, size_t bytes);
 int ensure_scratch2(casl_handle *h, size_t bytes);
+
+// The fine-grid judge of node velocities: hf (nf = 2, 4 or 8 times h's n)
+// inverts h's contours at its own resolution plus the spectrum of h's
+// non-contour PV (qq - qc, after an inversion of h) and interpolates the
+// result bilinearly to the nodes.  uJ, vJ, uP, vP: device arrays of nptq
+// doubles (uP, vP = plain velint of h's inversion; nullable).  On h's stream.
+int judge_velocity(casl_handle *h, casl_handle *hf, double *uJ, double *vJ, double *uP,
+                   double *vP);
+// Learned velocity closure hooks (closure.cu).  closure_stage runs after a
+// stage's inversion; it returns the velocity fields velint should read (the
+// corrected ones while the closure is active, else h->uu, h->vv).
+int closure_stage(casl_handle *h, const double **u, const double **v);
+// Before each advance of casl_step: the periodic fine-grid check.
+int closure_step_check(casl_handle *h);
+void closure_release(casl_handle *h);
 
 }  // namespace casl

@@ -97,7 +97,12 @@ int casl_synchronize(casl_handle *h);
 
 /* ---- state transfer (host <-> device) ------------------------------------ */
 /* Replaces the module state xq,yq,nextq,indq,npq,i1q,i2q,nq,nptq,qjump
- * (contours.f90:12-15).  Arrays are 1-based in content (nextq values). */
+ * (contours.f90:12-15).  Arrays are 1-based in content (nextq values).
+ * The uploaded state is checked on the device before it is accepted: a
+ * non-finite node or one outside [-ellx/2,ellx/2) x [-elly/2,elly/2) returns
+ * CASL_EDOMAIN, a successor or contour range outside 1..nptq (or npq !=
+ * i2q-i1q+1) CASL_EINVAL, more nodes or contours than the capacities
+ * CASL_ECAPACITY; a rejected state leaves the handle with no contours. */
 int casl_set_contours(casl_handle *h, int nq, int nptq, double qjump,
                       const double *xq, const double *yq, const int *nextq,
                       const int *indq, const int *npq, const int *i1q, const int *i2q);
@@ -233,9 +238,17 @@ int casl_genfg(casl_handle *h, int ix1v, int nxv, int iy1v, int nyv, int stride,
  * in the reference) and qc_dev (n*n doubles, Fortran (ny,nx) order).  It
  * allocates nothing: its scratch is one fixed file-scope device array of
  * 4.3 MB, so n is limited to 32..256 (a power of two; larger n returns
- * CASL_EINVAL), and every GPU that loads the library holds that array until
- * the process exits.  The first call on a device looks the array's address
- * up (cudaGetSymbolAddress); make that first call before any stream capture.
+ * CASL_EINVAL), and every GPU on which the library's device code is loaded
+ * holds that array until the process exits.  The first call on a device
+ * looks the array's address up (cudaGetSymbolAddress); under CUDA's default
+ * lazy module loading that first call is also what loads the library's
+ * device code and the array onto the device, so it may allocate and
+ * synchronise: make it once as a warm-up, outside any time-critical loop and
+ * before any stream capture.  The address is kept per device for the
+ * device's primary context (the runtime API's), so the entry point serves
+ * that context only, and not across a cudaDeviceReset.  An error the caller
+ * left pending in the runtime (cudaPeekAtLastError) makes the call return
+ * CASL_ECUDA at once and is left in place for the caller.
  * All calls on a device share the array and it keeps the last call's
  * contents (the call clears what must start at zero), so calls that overlap
  * on the GPU (e.g. on two streams at once) race.  `stream` is a cudaStream_t
@@ -243,6 +256,70 @@ int casl_genfg(casl_handle *h, int ix1v, int nxv, int iy1v, int nyv, int stride,
 int casl_con2grid_noalloc(int n, double ellx, double elly, int nptq, double qjump,
                           const double *xq_dev, const double *yq_dev, const int *nextq_dev,
                           double *qc_dev, void *stream);
+
+/* ---- learned velocity closure (no counterpart in the reference) ----------- */
+/* The reference interpolates the coarse inversion's velocity bilinearly to
+ * the nodes (velint, contours.f90:136-169).  The closure adds to the gridded
+ * velocity that velint reads a correction predicted by a small CNN from the
+ * coarse grid's PV and velocity: four periodic 5x5 convolutions 3 -> 32 ->
+ * 32 -> 32 -> 2 channels with GELU after the first three, BF16 weights and
+ * activations, FP32 accumulation, forward and backward on the tensor cores.
+ * Parameters are float32 in the order W1[co][ci][ky][kx], b1, ..., W4, b4
+ * (casl_net_param_count of them).  Host arrays are channel-major
+ * (C, nx, ny) float32 with ny fastest, like the physical fields.  n is a
+ * multiple of 128, 128..2048. */
+typedef struct casl_net casl_net;
+int casl_net_param_count(void);
+int casl_net_create(int n, int device, casl_net **out);
+void casl_net_destroy(casl_net *net);
+/* qscale, uscale: the PV and velocity scales the network's inputs are
+ * divided by and its output multiplied by when it runs inside a step. */
+int casl_net_set_params(casl_net *net, const float *params, float qscale, float uscale);
+int casl_net_get_params(casl_net *net, float *params, float *qscale, float *uscale);
+/* x: (3, n, n) network input (already scaled); y: (2, n, n) output.  Keeps
+ * what casl_net_backward needs. */
+int casl_net_forward(casl_net *net, const float *x, float *y);
+/* Gradient of sum(dy * y) for the last casl_net_forward with respect to the
+ * parameters (grad: casl_net_param_count floats, may be NULL); also keeps it
+ * for casl_net_adam. */
+int casl_net_backward(casl_net *net, const float *dy, float *grad);
+/* One Adam step (b1 = 0.9, b2 = 0.999, eps = 1e-8) with the last gradient. */
+int casl_net_adam(casl_net *net, float lr);
+
+/* The fine-grid judge of node velocities.  `judge` is a handle of the same
+ * domain with 2, 4 or 8 times h's grid (the reference's main_invert,
+ * spectral.f90:304-342, at that resolution): it inverts h's contours on its
+ * own grid plus the spectrum of h's non-contour PV (qq - qc of an inversion
+ * of h, carried over unchanged) and interpolates its velocity bilinearly to
+ * the nodes.  uJ, vJ (and uP, vP, the plain velint of h's own inversion,
+ * nullable) are host arrays of nptq doubles. */
+int casl_closure_judge(casl_handle *h, casl_handle *judge, double *uJ, double *vJ, double *uP,
+                       double *vP);
+/* Attach a network to h: from now on every RK4 stage of casl_advance /
+ * casl_step runs it on the stage's coarse PV and velocity and velint reads
+ * u + uscale*y0, v + uscale*y1.  With a judge and check_every > 0, every
+ * check_every-th casl_step first compares the node velocities of both forms
+ * with the judge's: the correction stays on while its relative error
+ * (sqrt(sum |u - uJ|^2 / sum |uJ|^2) over the nodes) is at most `budget` and
+ * at most the plain form's, and falls back to plain velint otherwise, until a
+ * later check passes.  net = NULL detaches.  The network and judge are not
+ * owned by h. */
+int casl_closure_attach(casl_handle *h, casl_net *net, casl_handle *judge, int check_every,
+                        double budget);
+int casl_closure_status(casl_handle *h, int *active, double *err_plain, double *err_net,
+                        long long *checks, long long *fallbacks);
+/* One check now (needs an attached network and judge). */
+int casl_closure_check(casl_handle *h, double *err_plain, double *err_net);
+/* One training sample at h's current state: judge, network forward, the node
+ * loss sum |corrected - judge|^2 / (nptq uscale^2), backward and one Adam
+ * step.  out: plain relative error, corrected relative error (before the
+ * step), loss.  casl_closure_evaluate does the same without training. */
+int casl_closure_train(casl_handle *h, casl_net *net, casl_handle *judge, float lr,
+                       double out[3]);
+int casl_closure_evaluate(casl_handle *h, casl_net *net, casl_handle *judge, double out[3]);
+/* The network input of h's latest inversion, (3, n, n) float32, already
+ * divided by the network's scales: contour PV, u, v. */
+int casl_closure_features(casl_handle *h, casl_net *net, float *x);
 
 /* ---- benchmarking hooks (no counterpart in the reference) ---------------- */
 /* The cudaStream_t (as void*) on which all of the handle's work is ordered,
@@ -253,7 +330,8 @@ int casl_launch_count(long long *count);
 /* Kernel-class timing: while a class is selected, each launch of that class
  * is bracketed by CUDA events on the handle's stream; casl_profile_read
  * returns the summed device time, the number of launches and their
- * algorithmic bytes (each input read once, each output written once), then
+ * algorithmic bytes (a 2-D transform reads each field once and writes it
+ * once, 16 B per FP64 element; each of its two passes counts half), then
  * resets the tally.  Classes: */
 #define CASL_PROF_OFF 0
 #define CASL_PROF_FFT 1   /* the batched real-FFT passes (ptospc/spctop halves) */

@@ -1,0 +1,147 @@
+"""Parity at the benchmarked scale and over the C1 run length.
+
+1. The bench workload's state (1024^2, k0 = 16, 80 levels, seed 0, about
+   1.3M nodes after initialise): initialise (recontour from the field),
+   con2grid levels on the 4096^2 fine grid, one RK4 advance, one surgery and
+   a recontour with a residual, each against the oracle on identical input.
+2. The C1 configuration (256^2, k0 = 6, 40 levels, surgery every step,
+   recontour every 20 regularisations) for 400 steps on both sides, with dt
+   adaptive and capped at the configuration's 0.025 (the fixed 0.025 breaks
+   the reference's CFL limit for this field): energy, enstrophy and
+   circulation within 1e-6 relative at every step; node and contour counts
+   compared at every step, and the first step at which they differ (if any)
+   is reported.
+
+The oracle needs about half a minute to initialise the 1024^2 state and a
+few seconds per advance, surgery or recontour there.
+"""
+import numpy as np
+import pytest
+
+from hydra_b200.synthetic import random_pv
+
+pytestmark = pytest.mark.gpu
+
+REL = 1e-12
+NPM, NM = 16_000_000, 1_000_000
+
+
+def rel_err(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def same_topology(co, cg):
+    assert (cg["nq"], cg["nptq"]) == (co["nq"], co["nptq"])
+    for k in ("npq", "i1q", "i2q", "indq", "nextq"):
+        assert np.array_equal(cg[k], co[k]), k
+
+
+@pytest.fixture(scope="module")
+def bench_pair(oracle_mod, gpu_lib):
+    from hydra_b200.casl import CaslGPU
+    n, levels = 1024, 80
+    kw = dict(ncontq=levels, force_surgery=1, dtmax=0.05, npm=NPM, nm=NM)
+    q0 = random_pv(n, 16.0, 0)
+    o = oracle_mod.Oracle(n, **kw)
+    o.initialise(q0)
+    g = CaslGPU(n, **kw)
+    g.initialise(q0)
+    yield n, o, g
+    g.close()
+    o.close()
+
+
+def load(o, g):
+    g.set_contours(o.contours())
+    for f in ("qs", "qd", "qr"):
+        g.set_field(f, o.field(f))
+    for s in ("t", "twist"):
+        g.set_scalar(s, o.scalar(s))
+
+
+def test_bench_state_initialise(bench_pair):
+    n, o, g = bench_pair
+    co, cg = o.contours(), g.contours()
+    assert co["nptq"] > 1_000_000
+    assert co["qjump"] == cg["qjump"]
+    same_topology(co, cg)
+    assert np.abs(cg["xq"] - co["xq"]).max() <= 1e-10 * np.pi
+    assert np.abs(cg["yq"] - co["yq"]).max() <= 1e-10 * np.pi
+    for f in ("qs", "qd", "qc"):
+        assert rel_err(g.field(f), o.field(f)) <= 1e-10, f
+
+
+def test_bench_state_con2grid(bench_pair):
+    n, o, g = bench_pair
+    load(o, g)
+    qc_o, lv_o = o.con2grid(levels=True)
+    qc_g, lv_g = g.con2grid(levels=True)
+    assert np.array_equal(lv_g, lv_o)  # 4096^2 fine-grid PV levels
+    assert rel_err(qc_g, qc_o) < REL
+    assert rel_err(g.con2grid(), qc_o) < REL  # packed path (the one the step runs)
+
+
+def test_bench_state_advance(bench_pair):
+    n, o, g = bench_pair
+    load(o, g)
+    o.advance()
+    g.advance()
+    co, cg = o.contours(), g.contours()
+    assert rel_err(cg["xq"], co["xq"]) < REL and rel_err(cg["yq"], co["yq"]) < REL
+    assert abs(g.scalar("dt") - o.scalar("dt")) <= 1e-14 * o.scalar("dt")
+    for f in ("qs", "qd"):
+        assert rel_err(g.field(f), o.field(f)) < 1e-11, f
+    for f in ("uu", "vv"):
+        assert rel_err(g.field(f), o.field(f)) < REL, f
+
+
+def test_bench_state_surgery(bench_pair):
+    n, o, g = bench_pair
+    load(o, g)  # the advanced state of the previous test, on both sides
+    o.surgery()
+    g.surgery()
+    co, cg = o.contours(), g.contours()
+    same_topology(co, cg)
+    assert np.abs(cg["xq"] - co["xq"]).max() <= 1e-12 * np.pi
+
+
+def test_bench_state_recontour(bench_pair):
+    n, o, g = bench_pair
+    load(o, g)
+    rng = np.random.default_rng(1)
+    resid = 0.05 * o.counts()[2] * rng.standard_normal((n, n))
+    o.recontour(resid)
+    g.recontour(resid)
+    co, cg = o.contours(), g.contours()
+    same_topology(co, cg)
+    assert np.abs(cg["xq"] - co["xq"]).max() <= 1e-8 * np.pi
+
+
+def test_c1_400_steps(oracle_mod, gpu_lib, capsys):
+    from hydra_b200.casl import CaslGPU
+    n, steps = 256, 400
+    kw = dict(ncontq=40, force_surgery=1, dtmax=0.025, nregmax=20, npm=NPM // 8, nm=NM // 8)
+    q0 = random_pv(n, 6.0, 0)
+    o = oracle_mod.Oracle(n, **kw)
+    g = CaslGPU(n, **kw)
+    o.initialise(q0)
+    g.initialise(q0)
+    first_diff = None
+    worst = {"ekin": 0.0, "enstrophy": 0.0, "circulation": 0.0}
+    for step in range(1, steps + 1):
+        o.step()
+        g.step(1)
+        no, ng = o.counts()[:2], g.counts()[:2]
+        if no != ng and first_diff is None:
+            first_diff = (step, no, ng)
+        do, dg = o.diagnostics(), g.diagnostics()
+        for k in worst:
+            e = abs(dg[k] - do[k]) / abs(do[k])
+            worst[k] = max(worst[k], e)
+            assert e <= 1e-6, (step, k, dg[k], do[k])
+    with capsys.disabled():
+        print(f"\nC1 400 steps: t = {o.scalar('t'):.4f}; worst relative differences {worst}; "
+              f"first count divergence: {first_diff or 'none'}")
+    assert abs(g.scalar("t") - o.scalar("t")) <= 1e-9 * o.scalar("t")
+    g.close()
+    o.close()
