@@ -208,6 +208,103 @@ def run_reference(a):
 
 
 # ---------------------------------------------------------------------------
+# learned-closure leg (the "chosen" form of the metric)
+# ---------------------------------------------------------------------------
+CLOSURE_WEIGHTS = os.path.join(ROOT, "hydra_b200", "closure_512.npz")
+
+
+def run_closure_leg(a, torch, device, steps=40, warmup=5, check_every=50):
+    """The learned-closure configuration (512^2 grid, k0 = 12, 80 levels, the
+    trained weights shipped with the library) against the plain form, every
+    node-velocity error measured against the 2048^2 FP64 judge on states of
+    an evaluation seed disjoint from the training seeds.  Throughput of the
+    closure form includes its periodic fine-grid check (every check_every
+    steps).  Plain forms at 512^2 and 1024^2 give the error-versus-cost curve
+    the closure is placed on; their states are the same seed's field at that
+    resolution.  Time to solution (simulated time per second) is reported
+    beside node-steps/s because the node count grows with the grid."""
+    from hydra_b200 import train_closure as tc
+    from hydra_b200.casl import CaslGPU, CaslNet
+    from hydra_b200.synthetic import random_pv
+    if not os.path.exists(CLOSURE_WEIGHTS):
+        return {"unavailable": "no trained weights (hydra_b200/closure_512.npz)"}
+    d = np.load(CLOSURE_WEIGHTS)
+    params, qs, us = tc.load(CLOSURE_WEIGHTS)
+    n, k0, levels, seed = 512, 12.0, 80, 0
+    kw = dict(ncontq=levels, force_surgery=1, dtmax=0.05, npm=8_000_000, nm=500_000, device=device)
+    gf = CaslGPU(2048, ncontq=levels, npm=16_000_000, nm=1_000_000, device=device)
+    out = {"config": f"learned closure: {n}^2 grid, k0={k0:g}, {levels} levels, seed {seed} "
+                     "(training seeds from 1000), judge 2048^2 FP64",
+           "training": {"pairs": int(d["pairs"]), "seconds": float(d["seconds"]),
+                        "pairs_per_s": float(d["pairs"]) / float(d["seconds"])}}
+
+    def timed(g, k):
+        st = torch.cuda.ExternalStream(g.stream_ptr(), device=device)
+        torch.cuda.synchronize()
+        ns0, t0 = g.scalar("node_steps"), g.scalar("t")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        g.step(k)
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        return {"ms_per_step": ms / k, "node_steps_per_s": (g.scalar("node_steps") - ns0) / (ms * 1e-3),
+                "sim_time_per_s": (g.scalar("t") - t0) / (ms * 1e-3)}
+
+    def errors(g, net=None, samples=4, gap=10):
+        ep, en = [], []
+        for _ in range(samples):
+            g.step(gap)
+            if net is not None:
+                e = g.closure_evaluate(net, gf)
+                ep.append(e[0]); en.append(e[1])
+            else:
+                uJ, vJ, uP, vP = g.judge(gf)
+                ep.append(float(np.sqrt(((uP - uJ) ** 2 + (vP - vJ) ** 2).sum() / (uJ ** 2 + vJ ** 2).sum())))
+        return float(np.mean(ep)), (float(np.mean(en)) if en else None)
+
+    # closure form at 512^2
+    g = CaslGPU(n, **kw)
+    net = CaslNet(n, device=device)
+    net.set_params(params, qs, us)
+    g.initialise(random_pv(n, k0, seed))
+    g.step(warmup)
+    ep, en = errors(g, net)
+    g.closure_attach(net, judge=gf, check_every=check_every, budget=1e-3)
+    t_c = timed(g, steps)
+    st = g.closure_status()
+    g.closure_attach(None)
+    t_p = timed(g, steps)
+    out["closure_512"] = dict(t_c, err=en, active=st["active"], checks=st["checks"],
+                              fallbacks=st["fallbacks"])
+    out["plain_512"] = dict(t_p, err=ep)
+    g.close()
+    net.close()
+    # plain form at 1024^2 (judge twice as fine)
+    g = CaslGPU(1024, ncontq=levels, force_surgery=1, dtmax=0.05, npm=16_000_000, nm=1_000_000,
+                device=device)
+    g.initialise(random_pv(1024, k0, seed))
+    g.step(warmup)
+    e1024, _ = errors(g)
+    out["plain_1024"] = dict(timed(g, steps), err=e1024)
+    g.close()
+    gf.close()
+    # the plain resolution with the closure's error, on the log-log line through
+    # the two plain points, and the time to solution there
+    c, p5, p10 = out["closure_512"], out["plain_512"], out["plain_1024"]
+    if c["err"] and p5["err"] > p10["err"] > 0:
+        order = np.log(p5["err"] / p10["err"]) / np.log(2.0)
+        n_eq = 512.0 * (p5["err"] / c["err"]) ** (1.0 / order)
+        cost_order = np.log(p5["sim_time_per_s"] / p10["sim_time_per_s"]) / np.log(2.0)
+        sim_eq = p5["sim_time_per_s"] * (n_eq / 512.0) ** (-cost_order)
+        out["equal_error"] = {"plain_grid_with_closure_error": n_eq, "error_order": order,
+                              "speedup_time_to_solution": c["sim_time_per_s"] / sim_eq,
+                              "note": "plain grid extrapolated on the log-log line through the "
+                                      "512^2 and 1024^2 plain points"}
+    return out
+
+
+# ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
 def reduce_over_ranks(vals, world, device):
@@ -293,6 +390,10 @@ def run_gpu(a):
                "sample": f"{steps} oracle steps ({dt:.1f} s) from the GPU run's state after "
                          "its timed steps (surgery + advance; no recontouring in the sample)"}
 
+    closure = None
+    if rank == 0 and world == 1 and not a.no_closure:
+        closure = run_closure_leg(a, torch, local)
+
     # ---- reduce over ranks ---------------------------------------------------------------
     ms_max, ns_sum, e2e_ms, e2e_ns = reduce_over_ranks(
         [ms, node_steps, e2e["ms"], e2e["node_steps"]], world, f"cuda:{local}")
@@ -327,6 +428,7 @@ def run_gpu(a):
                          "launches": fft_n, "kernel_ms_per_step": fft_ms / a.steps,
                          "peak_source": f"{peak_kind} hbm_gbs"},
             "cpu_baseline": cpu,
+            "closure": closure,
             "gpu_launches": launches,
             "clocks": clk,
         }
@@ -403,6 +505,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=20.0,
                     help="time budget of the cpu_baseline leg of the GPU arm")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-closure", action="store_true", help="skip the learned-closure leg")
     a = ap.parse_args()
     if a.warmup < 3 and a.impl == "hydra":
         print("bench: at least 3 warm-up steps are required", file=sys.stderr)

@@ -128,6 +128,8 @@ SIGNATURES = {
     "casl_closure_train": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, _dp]),
     "casl_closure_evaluate": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, _dp]),
     "casl_closure_features": (C.c_int, [C.c_void_p, C.c_void_p, _fp]),
+    "casl_set_precision": (C.c_int, [C.c_void_p, C.c_int]),
+    "casl_get_precision": (C.c_int, [C.c_void_p, _ip]),
 }
 
 
@@ -374,6 +376,10 @@ class CaslGPU:
         spec = np.zeros(self.nx + 1)
         self._check(self.lib.casl_spec1d(self.h, _d(a), _d(spec), int(iopt)), "casl_spec1d")
         return spec, a
+
+    def set_precision(self, mode):
+        """0 = FP64 (default); 1 = FP32 inversion (casl_set_precision)."""
+        self._check(self.lib.casl_set_precision(self.h, int(mode)), "casl_set_precision")
 
     # --- learned velocity closure ---------------------------------------------------
     def judge(self, fine):

@@ -286,26 +286,33 @@ struct LoadQC {
 
 // Advection product -u*fx - v*(fy [+ beta]) of evolution.f90:449,456-461,
 // read from physical arrays ([ix][iy]); b = 0 for qd, 1 for qs.
-struct LoadAdvect {
-  __host__ double bytes() const { return 32.0; }
-  const double *uu, *vv;
-  const double *fx[2], *fy[2];
+// Two adjacent elements of an FP64 or FP32 field, as FP64.
+__device__ __forceinline__ double2 ld2(const double *p) { return *reinterpret_cast<const double2 *>(p); }
+__device__ __forceinline__ double2 ld2(const float *p) {
+  const float2 f = *reinterpret_cast<const float2 *>(p);
+  return make_double2((double)f.x, (double)f.y);
+}
+template <class T>
+struct LoadAdvectT {
+  __host__ double bytes() const { return 4.0 * sizeof(T); }
+  const T *uu, *vv;
+  const T *fx[2], *fy[2];
   double betab[2];  // beta added to fy for the qs term when beffect
   int n;
   __device__ __forceinline__ double operator()(int b, int v /*ix*/, int j /*iy*/) const {
     long long k = (long long)v * n + j;
     const double bb = pick(betab, b);
-    double gx = pick(fx, b)[k], gy = pick(fy, b)[k];
+    double gx = (double)pick(fx, b)[k], gy = (double)pick(fy, b)[k];
     if (bb != 0.0) gy = gy + bb;
-    return -uu[k] * gx - vv[k] * gy;
+    return -(double)uu[k] * gx - (double)vv[k] * gy;
   }
   __device__ __forceinline__ double2 pair(int b, int v, int j) const {
     long long k = (long long)v * n + j;
     const double bb = pick(betab, b);
-    const double2 gx = *reinterpret_cast<const double2 *>(pick(fx, b) + k);
-    double2 gy = *reinterpret_cast<const double2 *>(pick(fy, b) + k);
-    const double2 u = *reinterpret_cast<const double2 *>(uu + k);
-    const double2 w = *reinterpret_cast<const double2 *>(vv + k);
+    const double2 gx = ld2(pick(fx, b) + k);
+    double2 gy = ld2(pick(fy, b) + k);
+    const double2 u = ld2(uu + k);
+    const double2 w = ld2(vv + k);
     if (bb != 0.0) {
       gy.x = gy.x + bb;
       gy.y = gy.y + bb;
@@ -313,6 +320,7 @@ struct LoadAdvect {
     return make_double2(-u.x * gx.x - w.x * gy.x, -u.y * gx.y - w.y * gy.y);
   }
 };
+using LoadAdvect = LoadAdvectT<double>;
 
 // Store of the source terms after ptospc pass B (evolution.f90:466-487):
 // b = 0 -> sqd with damping and the integrating factor, b = 1 -> sqs.
@@ -384,6 +392,51 @@ struct LoadBatch {
     return pick(p, b)[(long long)v * vs + (long long)j * es];
   }
 };
+// FP32 storage for the inverse transform pair of the FP32-inversion mode:
+// the kernel's arithmetic stays FP64 in registers; the intermediate and the
+// physical outputs are rounded to FP32 once, when stored.
+struct StoreStridedF {
+  __host__ double bytes() const { return 4.0; }
+  float *p;
+  long long bs, vs, es;
+  __device__ __forceinline__ void operator()(int b, int v, int k, double x) const {
+    p[b * bs + (long long)v * vs + (long long)k * es] = (float)x;
+  }
+  __device__ __forceinline__ void pair(int b, int v, int k, double2 x) const {
+    const long long o = b * bs + (long long)v * vs + (long long)k * es;
+    if (es == 1) {
+      *reinterpret_cast<float2 *>(p + o) = make_float2((float)x.x, (float)x.y);
+    } else {
+      p[o] = (float)x.x;
+      p[o + es] = (float)x.y;
+    }
+  }
+};
+struct LoadBatchF {
+  __host__ double bytes() const { return 4.0; }
+  const float *p[6];
+  long long vs, es;
+  __device__ __forceinline__ double operator()(int b, int v, int j) const {
+    return (double)pick(p, b)[(long long)v * vs + (long long)j * es];
+  }
+};
+struct StoreScaledF {
+  __host__ double bytes() const { return 4.0; }
+  float *p[6];
+  double scale[6];
+  int n;
+  __device__ __forceinline__ void operator()(int b, int v, int k, double x) const {
+    const double sc = pick(scale, b);
+    pick(p, b)[(long long)v * n + k] = (float)(sc == 1.0 ? x : sc * x);
+  }
+  __device__ __forceinline__ void pair(int b, int v, int k, double2 x) const {
+    const double sc = pick(scale, b);
+    if (sc != 1.0) x = make_double2(sc * x.x, sc * x.y);
+    *reinterpret_cast<float2 *>(pick(p, b) + (long long)v * n + k) =
+        make_float2((float)x.x, (float)x.y);
+  }
+};
+
 // Load qq + kdsq*pp (adapt, evolution.f90:541-547).
 struct LoadVort {
   __host__ double bytes() const { return btropic ? 8.0 : 16.0; }
@@ -874,8 +927,9 @@ int con2grid_to_phys(casl_handle *h, double *phys, bool want_levels) {
 // ---------------------------------------------------------------------------
 // velint (contours.f90:136-169) and the RK4 node updates (evolution.f90:212-311)
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void velint1(double x, double y, const double *__restrict__ uu,
-                                        const double *__restrict__ vv, const Consts &c,
+template <class T>
+__device__ __forceinline__ void velint1(double x, double y, const T *__restrict__ uu,
+                                        const T *__restrict__ vv, const Consts &c,
                                         double &uq, double &vq) {
   double xx = c.glxi * (x - c.xmin);
   int ix0 = 1 + f_int(xx);
@@ -895,10 +949,10 @@ __device__ __forceinline__ void velint1(double x, double y, const double *__rest
   long long a01 = (long long)(ix1 - 1) * c.ny + (iy0 - 1);
   long long a10 = (long long)(ix0 - 1) * c.ny + (iy1 - 1);
   long long a11 = (long long)(ix1 - 1) * c.ny + (iy1 - 1);
-  uq = pyc * (pxc * __ldg(&uu[a00]) + px * __ldg(&uu[a01])) +
-       py * (pxc * __ldg(&uu[a10]) + px * __ldg(&uu[a11]));
-  vq = pyc * (pxc * __ldg(&vv[a00]) + px * __ldg(&vv[a01])) +
-       py * (pxc * __ldg(&vv[a10]) + px * __ldg(&vv[a11]));
+  uq = pyc * (pxc * (double)__ldg(&uu[a00]) + px * (double)__ldg(&uu[a01])) +
+       py * (pxc * (double)__ldg(&uu[a10]) + px * (double)__ldg(&uu[a11]));
+  vq = pyc * (pxc * (double)__ldg(&vv[a00]) + px * (double)__ldg(&vv[a01])) +
+       py * (pxc * (double)__ldg(&vv[a10]) + px * (double)__ldg(&vv[a11]));
 }
 
 __global__ void k_velint(const double *__restrict__ xq, const double *__restrict__ yq, int npt,
@@ -913,11 +967,11 @@ __global__ void k_velint(const double *__restrict__ xq, const double *__restrict
   }
 }
 
-template <int STAGE>
+template <int STAGE, class T>
 __device__ __forceinline__ void nodes_rk_body(int bid, int nbk, double *__restrict__ xq, double *__restrict__ yq,
                            double *__restrict__ xqi, double *__restrict__ yqi,
                            double *__restrict__ xqf, double *__restrict__ yqf,
-                           const double *__restrict__ uu, const double *__restrict__ vv,
+                           const T *__restrict__ uu, const T *__restrict__ vv,
                            const Scalars *__restrict__ s, const Consts &c) {
   const int npt = s->nptq;
   const double dt = s->dt, dt2 = s->dt2, dt3 = s->dt3, dt6 = s->dt6;
@@ -988,8 +1042,9 @@ __global__ void k_combine(double *__restrict__ qs, double *__restrict__ qd,
 // adapt (evolution.f90:524-608): deterministic two-level reductions
 // ---------------------------------------------------------------------------
 #define RED_BLOCKS 296
-__global__ void k_reduce_adapt(const double *__restrict__ zz, const double *__restrict__ uu,
-                               const double *__restrict__ vv, double *__restrict__ part,
+template <class T>
+__global__ void k_reduce_adapt(const double *__restrict__ zz, const T *__restrict__ uu,
+                               const T *__restrict__ vv, double *__restrict__ part,
                                long long nn) {
   CASL_PDL_ENTRY();
   double sum = 0.0, zmax = 0.0, umax = 0.0;
@@ -999,7 +1054,8 @@ __global__ void k_reduce_adapt(const double *__restrict__ zz, const double *__re
     z = z * z;
     sum += z;
     zmax = fmax(zmax, z);
-    double w = uu[k] * uu[k] + vv[k] * vv[k];
+    const double u = (double)uu[k], v = (double)vv[k];
+    double w = u * u + v * v;
     umax = fmax(umax, w);
   }
   __shared__ double s0[256], s1[256], s2[256];
@@ -1131,9 +1187,10 @@ __device__ __forceinline__ void spec_rk_body(int bid, int nbk, double *__restric
 // The end of an RK4 stage in one launch: blocks below nbn move the nodes
 // (velint + node update), the rest update the spectral fields; the two
 // parts touch disjoint data and read only dt from the scalars.
+template <class T>
 struct NodeRkArgs {
   double *xq, *yq, *xqi, *yqi, *xqf, *yqf;
-  const double *uu, *vv;
+  const T *uu, *vv;
 };
 struct SpecRkArgs {
   double *qs, *qd, *qsi, *qsf, *qdi, *qdf;
@@ -1141,15 +1198,15 @@ struct SpecRkArgs {
   double *emq;
   long long nn;
 };
-template <int STAGE>
-__global__ void k_stage_rk(NodeRkArgs a, SpecRkArgs b, Scalars *__restrict__ s, Consts c,
+template <int STAGE, class T>
+__global__ void k_stage_rk(NodeRkArgs<T> a, SpecRkArgs b, Scalars *__restrict__ s, Consts c,
                            int nbn) {
   CASL_PDL_ENTRY();
   // the half-step time advance that opens stages 2 and 4 (nothing reads t
   // in between)
   if ((STAGE == 1 || STAGE == 3) && blockIdx.x == 0 && threadIdx.x == 0) s->t = s->t + s->dt2;
   if ((int)blockIdx.x < nbn)
-    nodes_rk_body<STAGE>(blockIdx.x, nbn, a.xq, a.yq, a.xqi, a.yqi, a.xqf, a.yqf, a.uu, a.vv, s, c);
+    nodes_rk_body<STAGE, T>(blockIdx.x, nbn, a.xq, a.yq, a.xqi, a.yqi, a.xqf, a.yqf, a.uu, a.vv, s, c);
   else
     spec_rk_body<STAGE>(blockIdx.x - nbn, gridDim.x - nbn, b.qs, b.qd, b.qsi, b.qsf, b.qdi,
                         b.qdf, b.sqs, b.sqd, b.emq, s, b.nn);
@@ -1248,9 +1305,40 @@ static int invert_and_gradients(casl_handle *h) {
   return RFFT_DISPATCH(false, true, false, lb, st, 6);
 }
 
+// The same batch-6 inverse pair with FP32 storage (CASL_PREC_FP32_INVERSION):
+// the intermediate in gtmp as floats, the outputs in f32 = [u, v, dqd/dx,
+// dqd/dy, dqs/dx, dqs/dy].
+static int invert_and_gradients32(casl_handle *h) {
+  long long nn = (long long)h->n * h->n, n = h->n;
+  LoadDeriv ld{};
+  const double *src[6] = {h->qq, h->qq, h->qd, h->qd, h->qs, h->qs};
+  for (int b = 0; b < 6; b++) {
+    ld.f[b] = src[b];
+    ld.dir[b] = b & 1;
+    ld.wg[b] = b < 2;
+  }
+  ld.green = h->green; ld.hrkx = h->hrkx; ld.hrky = h->hrky; ld.n = h->n;
+  float *tmp = reinterpret_cast<float *>(h->gtmp);  // 6 contiguous FP32 fields
+  int rc = RFFT_DISPATCH(false, false, false, ld, (StoreStridedF{tmp, nn, n, 1}), 6);
+  if (rc) return rc;
+  LoadBatchF lb{};
+  for (int b = 0; b < 6; b++) lb.p[b] = tmp + b * nn;
+  lb.vs = 1; lb.es = n;
+  StoreScaledF st{};
+  const int slot[6] = {1, 0, 2, 3, 4, 5};  // b = 0: d/dx of green*qq = v; b = 1: -d/dy = u
+  for (int b = 0; b < 6; b++) {
+    st.p[b] = h->f32 + slot[b] * nn;
+    st.scale[b] = b == 1 ? -1.0 : 1.0;
+  }
+  st.n = h->n;
+  h->uv_fp32 = 1;
+  return RFFT_DISPATCH(false, true, false, lb, st, 6);
+}
+
 int inversion_dev(casl_handle *h, bool reset) {
   int rc = inversion_qq(h, reset);
   if (rc) return rc;
+  h->uv_fp32 = 0;
   return main_invert_dev(h);
 }
 
@@ -1262,7 +1350,12 @@ static int adapt_dev(casl_handle *h) {
   rc = RFFT_DISPATCH(false, true, false, (LoadStrided{h->w[0], nn, 1, n}),
                      (StoreStrided{h->w[1], nn, n, 1}), 1);
   if (rc) return rc;
-  CASL_K(k_reduce_adapt, RED_BLOCKS, 256, 0, h->stream)(h->w[1], h->uu, h->vv, h->part, nn);
+  if (h->prec == CASL_PREC_FP32_INVERSION)
+    CASL_K(k_reduce_adapt<float>, RED_BLOCKS, 256, 0, h->stream)(h->w[1], h->f32, h->f32 + nn,
+                                                                 h->part, nn);
+  else
+    CASL_K(k_reduce_adapt<double>, RED_BLOCKS, 256, 0, h->stream)(h->w[1], h->uu, h->vv, h->part,
+                                                                  nn);
   CASL_K(k_adapt_final, 1, 256, 0, h->stream)(h->part, RED_BLOCKS, h->scal, h->c, h->p.fixed_dt);
   CASL_K(k_epq, grid_for(nn), 256, 0, h->stream)(h->qdiss, h->epq, h->emq, h->scal, nn);
   return check_launch(h);
@@ -1277,13 +1370,24 @@ static int source_prod(casl_handle *h, int stage) {
   double *tmp = h->w[0];  // w[0..1]
   int rc;
   // products -> ptospc's first pass into tmp, its second pass with the source store
-  LoadAdvect la{};
-  la.uu = h->uu; la.vv = h->vv;
-  la.fx[0] = h->w[4]; la.fy[0] = h->w[5];
-  la.fx[1] = h->sqs; la.fy[1] = h->sqd;
-  la.betab[0] = 0.0; la.betab[1] = h->c.beffect ? h->c.beta : 0.0;
-  la.n = h->n;
-  rc = RFFT_DISPATCH(true, false, true, la, (StoreStrided{tmp, nn, 1, n}), 2);
+  if (h->prec == CASL_PREC_FP32_INVERSION) {
+    const float *f = h->f32;
+    LoadAdvectT<float> la{};
+    la.uu = f; la.vv = f + nn;
+    la.fx[0] = f + 2 * nn; la.fy[0] = f + 3 * nn;
+    la.fx[1] = f + 4 * nn; la.fy[1] = f + 5 * nn;
+    la.betab[0] = 0.0; la.betab[1] = h->c.beffect ? h->c.beta : 0.0;
+    la.n = h->n;
+    rc = RFFT_DISPATCH(true, false, true, la, (StoreStrided{tmp, nn, 1, n}), 2);
+  } else {
+    LoadAdvect la{};
+    la.uu = h->uu; la.vv = h->vv;
+    la.fx[0] = h->w[4]; la.fy[0] = h->w[5];
+    la.fx[1] = h->sqs; la.fy[1] = h->sqd;
+    la.betab[0] = 0.0; la.betab[1] = h->c.beffect ? h->c.beta : 0.0;
+    la.n = h->n;
+    rc = RFFT_DISPATCH(true, false, true, la, (StoreStrided{tmp, nn, 1, n}), 2);
+  }
   if (rc) return rc;
   StoreSource ss{};
   ss.sqd = h->sqd; ss.sqs = h->sqs; ss.qq = h->qq; ss.pp = h->pp; ss.epq = h->epq;
@@ -1295,19 +1399,20 @@ static int source_prod(casl_handle *h, int stage) {
 }  // namespace casl
 
 // node update and spectral RK update of a stage, one launch; velint reads
-// the velocity fields u, v
-static int stage_update(casl_handle *h, int stage, const double *u, const double *v) {
+// the velocity fields u, v (FP64, or FP32 in the FP32-inversion mode)
+template <class T>
+static int stage_update(casl_handle *h, int stage, const T *u, const T *v) {
   const long long nn = (long long)h->n * h->n;
   const int nbn = h->contex ? grid_for(h->nptq > 0 ? h->nptq : 1) : 0;
   const int g = nbn + grid_for(nn / 2);
-  const NodeRkArgs a{h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, u, v};
+  const NodeRkArgs<T> a{h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, u, v};
   const SpecRkArgs b{h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs, h->sqd, h->emq, nn};
   cudaStream_t st = h->stream;
   switch (stage) {
-    case 1: CASL_K(k_stage_rk<1>, g, 256, 0, st)(a, b, h->scal, h->c, nbn); break;
-    case 2: CASL_K(k_stage_rk<2>, g, 256, 0, st)(a, b, h->scal, h->c, nbn); break;
-    case 3: CASL_K(k_stage_rk<3>, g, 256, 0, st)(a, b, h->scal, h->c, nbn); break;
-    default: CASL_K(k_stage_rk<4>, g, 256, 0, st)(a, b, h->scal, h->c, nbn); break;
+    case 1: CASL_K((k_stage_rk<1, T>), g, 256, 0, st)(a, b, h->scal, h->c, nbn); break;
+    case 2: CASL_K((k_stage_rk<2, T>), g, 256, 0, st)(a, b, h->scal, h->c, nbn); break;
+    case 3: CASL_K((k_stage_rk<3, T>), g, 256, 0, st)(a, b, h->scal, h->c, nbn); break;
+    default: CASL_K((k_stage_rk<4, T>), g, 256, 0, st)(a, b, h->scal, h->c, nbn); break;
   }
   return check_launch(h);
 }
@@ -1321,12 +1426,20 @@ static int advance_dev(casl_handle *h) {
     // stage 1: the reset inside the filter combination rewrites qs and qd
     // before the gradients read them
     if ((rc = inversion_qq(h, stage == 1))) return rc;
-    if ((rc = invert_and_gradients(h))) return rc;
+    const bool f32 = h->prec == CASL_PREC_FP32_INVERSION;
+    if ((rc = f32 ? invert_and_gradients32(h) : invert_and_gradients(h))) return rc;
     if (stage == 1 && (rc = adapt_dev(h))) return rc;
     if ((rc = source_prod(h, stage))) return rc;
-    const double *u = h->uu, *v = h->vv;
-    if (h->closure && (rc = closure_stage(h, &u, &v))) return rc;
-    if ((rc = stage_update(h, stage, u, v))) return rc;
+    if (f32) {
+      const long long nn = (long long)h->n * h->n;
+      const float *u = h->f32, *v = h->f32 + nn;
+      if (h->closure && (rc = closure_stage32(h, &u, &v))) return rc;
+      if ((rc = stage_update<float>(h, stage, u, v))) return rc;
+    } else {
+      const double *u = h->uu, *v = h->vv;
+      if (h->closure && (rc = closure_stage(h, &u, &v))) return rc;
+      if ((rc = stage_update<double>(h, stage, u, v))) return rc;
+    }
   }
   return CASL_OK;
 }
@@ -1962,6 +2075,7 @@ void casl_destroy(casl_handle *h) {
   io_release(h);
   cudaStreamSynchronize(h->stream);
   closure_release(h);
+  cudaFree(h->f32);
   free_all(h);
   if (h->prof_ev) {
     for (int i = 0; i < 2 * CASL_PROF_MAX; i++) cudaEventDestroy(h->prof_ev[i]);
@@ -2144,11 +2258,24 @@ int casl_set_field(casl_handle *h, int which, const double *host) {
   return CASL_OK;
 }
 
+__global__ void k_widen(const float *__restrict__ a, double *__restrict__ b, long long nn) {
+  CASL_PDL_ENTRY();
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nn;
+       t += (long long)gridDim.x * blockDim.x)
+    b[t] = (double)a[t];
+}
+
 int casl_get_field(casl_handle *h, int which, double *host) {
   if (!h || !host) return CASL_EINVAL;
   double *d = field_ptr(h, which);
   if (!d) return CASL_EINVAL;
   size_t nn = (size_t)h->n * h->n;
+  if (h->uv_fp32 && (which == CASL_UU || which == CASL_VV)) {
+    // the last stage's FP32 velocity, widened (FP32-inversion mode)
+    d = h->w[5];
+    CASL_K(k_widen, grid_for((long long)nn), 256, 0, h->stream)(
+        h->f32 + (which == CASL_UU ? 0 : nn), d, (long long)nn);
+  }
   CASL_CUDA_TRY(cudaMemcpyAsync(host, d, nn * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   CASL_CUDA_TRY(cudaStreamSynchronize(h->stream));
   return CASL_OK;
@@ -2508,6 +2635,24 @@ int casl_step(casl_handle *h, int nsteps) {
   return sync_counts(h);
 }
 
+int casl_set_precision(casl_handle *h, int mode) {
+  if (!h || (mode != CASL_PREC_FP64 && mode != CASL_PREC_FP32_INVERSION)) return CASL_EINVAL;
+  cudaSetDevice(h->device);
+  if (mode == CASL_PREC_FP32_INVERSION && !h->f32) {
+    const size_t bytes = (size_t)6 * h->n * h->n * sizeof(float);
+    CASL_CUDA_TRY(cudaMalloc(&h->f32, bytes));
+    CASL_CUDA_TRY(cudaMemset(h->f32, 0, bytes));
+  }
+  h->prec = mode;
+  return CASL_OK;
+}
+
+int casl_get_precision(casl_handle *h, int *mode) {
+  if (!h || !mode) return CASL_EINVAL;
+  *mode = h->prec;
+  return CASL_OK;
+}
+
 int casl_get_stream(casl_handle *h, void **stream) {
   if (!h || !stream) return CASL_EINVAL;
   *stream = (void *)h->stream;
@@ -2599,6 +2744,12 @@ int casl_diagnostics(casl_handle *h, double out[4]) {
   if (!h || !out) return CASL_EINVAL;
   cudaStream_t st = h->stream;
   const long long nn = (long long)h->n * h->n;
+  if (h->uv_fp32) {
+    // FP32-inversion mode: the energies from the FP64 velocity of qq
+    int rc = main_invert_dev(h);
+    if (rc) return rc;
+    h->uv_fp32 = 0;
+  }
   // ekin = 1/2 garea sum(u^2+v^2) (evolution.f90:628-629)
   CASL_K(k_diag_sumsq2, RED_BLOCKS, 256, 0, st)(h->uu, h->vv, h->part, nn);
   CASL_K(k_diag_final, 1, 256, 0, st)(h->part, RED_BLOCKS, h->part + 2 * RED_BLOCKS);

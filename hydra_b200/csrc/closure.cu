@@ -697,8 +697,9 @@ namespace net {
 // The network's input from the inversion of a stage: the contour PV on the
 // coarse grid (the integer cells of con2grid with its mean removed, as the
 // transform's load forms it), u and v, divided by the scales.
+template <class T>
 __global__ void k_features(const int *__restrict__ C, const Scalars *__restrict__ s,
-                           const double *__restrict__ uu, const double *__restrict__ vv,
+                           const T *__restrict__ uu, const T *__restrict__ vv,
                            float iq, float iu, bf16 *__restrict__ x0, int n, int contex) {
   CASL_PDL_ENTRY();
   const long long nn = (long long)n * n;
@@ -718,15 +719,17 @@ __global__ void k_features(const int *__restrict__ C, const Scalars *__restrict_
   }
 }
 
-// Corrected fields: u + us * y0, v + us * y1.
-__global__ void k_apply(const double *__restrict__ uu, const double *__restrict__ vv,
-                        const float *__restrict__ y, float us, double *__restrict__ uc,
-                        double *__restrict__ vc, long long nn) {
+// Corrected fields: u + us * y0, v + us * y1 (FP64 fields, or FP32 ones in
+// the FP32-inversion mode).
+template <class T>
+__global__ void k_apply(const T *__restrict__ uu, const T *__restrict__ vv,
+                        const float *__restrict__ y, float us, T *__restrict__ uc,
+                        T *__restrict__ vc, long long nn) {
   CASL_PDL_ENTRY();
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nn;
        t += (long long)gridDim.x * blockDim.x) {
-    uc[t] = uu[t] + (double)us * (double)y[t];
-    vc[t] = vv[t] + (double)us * (double)y[nn + t];
+    uc[t] = (T)((double)uu[t] + (double)us * (double)y[t]);
+    vc[t] = (T)((double)vv[t] + (double)us * (double)y[nn + t]);
   }
 }
 
@@ -847,17 +850,24 @@ static inline int gsz(long long work) {
 
 // Network input, forward (train keeps the pre-activations) and the corrected
 // fields, from h's latest inversion, on h's stream.
-static int net_correct(casl_handle *h, casl_net *N, ClosureState *cs, bool train) {
+template <class T>
+static int net_correct_t(casl_handle *h, casl_net *N, const T *uu, const T *vv, T *uc, T *vc,
+                         bool train) {
   const long long nn = (long long)h->n * h->n;
   cudaStream_t st = h->stream;
-  CASL_K(net::k_features, gsz(nn), 256, 0, st)(h->coarseC, h->scal, h->uu, h->vv,
-                                                1.0f / N->qscale, 1.0f / N->uscale, N->x0, h->n,
-                                                h->nptq > 0 ? 1 : 0);
+  CASL_K(net::k_features<T>, gsz(nn), 256, 0, st)(h->coarseC, h->scal, uu, vv, 1.0f / N->qscale,
+                                                   1.0f / N->uscale, N->x0, h->n,
+                                                   h->nptq > 0 ? 1 : 0);
   int rc = net::forward(N, st, train, &h->scal->error);
   if (rc) return rc;
-  CASL_K(net::k_apply, gsz(nn), 256, 0, st)(h->uu, h->vv, N->fout, N->uscale, cs->ucor, cs->vcor,
-                                             nn);
+  CASL_K(net::k_apply<T>, gsz(nn), 256, 0, st)(uu, vv, N->fout, N->uscale, uc, vc, nn);
   return cudaPeekAtLastError() == cudaSuccess ? CASL_OK : CASL_ECUDA;
+}
+
+// Network input, forward (train keeps the pre-activations) and the corrected
+// FP64 fields, from h's latest FP64 inversion, on h's stream.
+static int net_correct(casl_handle *h, casl_net *N, ClosureState *cs, bool train) {
+  return net_correct_t<double>(h, N, h->uu, h->vv, cs->ucor, cs->vcor, train);
 }
 
 int closure_stage(casl_handle *h, const double **u, const double **v) {
@@ -867,6 +877,17 @@ int closure_stage(casl_handle *h, const double **u, const double **v) {
   if (rc) return rc;
   *u = cs->ucor;
   *v = cs->vcor;
+  return CASL_OK;
+}
+
+int closure_stage32(casl_handle *h, const float **u, const float **v) {
+  ClosureState *cs = h->closure;
+  if (!cs || !cs->net || !cs->active) return CASL_OK;
+  float *uc = reinterpret_cast<float *>(cs->ucor), *vc = reinterpret_cast<float *>(cs->vcor);
+  int rc = net_correct_t<float>(h, cs->net, *u, *v, uc, vc, false);
+  if (rc) return rc;
+  *u = uc;
+  *v = vc;
   return CASL_OK;
 }
 
@@ -1185,7 +1206,7 @@ int casl_closure_features(casl_handle *h, casl_net *net, float *x) {
   cudaSetDevice(h->device);
   const long long nn = (long long)h->n * h->n;
   cudaStream_t st = h->stream;
-  CASL_K(casl::net::k_features, casl::gsz(nn), 256, 0, st)(h->coarseC, h->scal, h->uu, h->vv,
+  CASL_K(casl::net::k_features<double>, casl::gsz(nn), 256, 0, st)(h->coarseC, h->scal, h->uu, h->vv,
                                                       1.0f / net->qscale, 1.0f / net->uscale,
                                                       net->x0, h->n, h->nptq > 0 ? 1 : 0);
   // unpack channels 0..2 of the padded planes on the host

@@ -71,6 +71,12 @@ struct casl_handle {
   cudaEvent_t *prof_ev;  // 2 * CASL_PROF_MAX events, created on first use
 
   casl::ClosureState *closure;  // learned velocity closure (nullable)
+
+  // FP32-inversion mode (casl_set_precision): the velocity and gradient
+  // fields of each stage in FP32, u, v, dqd/dx, dqd/dy, dqs/dx, dqs/dy
+  int prec;
+  float *f32;            // 6 * n*n floats, allocated when the mode is first selected
+  int uv_fp32;           // the latest stage velocity exists only in f32 (uu, vv stale)
 };
 
 #define CASL_PROF_MAX 8192
@@ -130,6 +136,7 @@ int judge_velocity(casl_handle *h, casl_handle *hf, double *uJ, double *vJ, doub
 // stage's inversion; it returns the velocity fields velint should read (the
 // corrected ones while the closure is active, else h->uu, h->vv).
 int closure_stage(casl_handle *h, const double **u, const double **v);
+int closure_stage32(casl_handle *h, const float **u, const float **v);  // FP32-inversion mode
 // Before each advance of casl_step: the periodic fine-grid check.
 int closure_step_check(casl_handle *h);
 void closure_release(casl_handle *h);

@@ -165,6 +165,22 @@ int casl_initialise(casl_handle *h, const double *qq_init);
  * (surgery; or prepare + recontour + init every nregmax) then advance. */
 int casl_step(casl_handle *h, int nsteps);
 
+/* Precision of the inversion inside casl_advance / casl_step.
+ * CASL_PREC_FP64 (default): everything FP64, the parity mode.
+ * CASL_PREC_FP32_INVERSION: the inverse transform pair of every RK4 stage
+ * (velocities from green*qq and the x/y derivatives of qd and qs,
+ * spectral.f90:304-366) stores its intermediate and its physical outputs in
+ * FP32 (arithmetic stays FP64 in registers); velint and the advection
+ * products read those FP32 fields; the state (qs, qd, nodes), the forward
+ * transforms, adapt's reductions and every contour operation stay FP64.
+ * casl_get_field(CASL_UU / CASL_VV) then returns the last stage's FP32
+ * velocity widened to FP64; casl_diagnostics recomputes the FP64 velocity
+ * from qq first. */
+#define CASL_PREC_FP64 0
+#define CASL_PREC_FP32_INVERSION 1
+int casl_set_precision(casl_handle *h, int mode);
+int casl_get_precision(casl_handle *h, int *mode);
+
 /* Diagnostics: out[0] kinetic energy, out[1] potential energy
  * (evolution.f90:612-644), out[2] integral of (q - beta y)^2 (generic.f90:48),
  * out[3] contour circulation qjump * sum of signed contour areas. */
