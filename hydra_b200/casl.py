@@ -130,6 +130,9 @@ SIGNATURES = {
     "casl_closure_features": (C.c_int, [C.c_void_p, C.c_void_p, _fp]),
     "casl_set_precision": (C.c_int, [C.c_void_p, C.c_int]),
     "casl_get_precision": (C.c_int, [C.c_void_p, _ip]),
+    "casl_pvforce": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_int, _dp]),
+    "casl_nb_forcing_init": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double, _ip]),
+    "casl_nb_forcing": (C.c_int, [C.c_void_p, C.c_double, _dp]),
 }
 
 
@@ -376,6 +379,24 @@ class CaslGPU:
         spec = np.zeros(self.nx + 1)
         self._check(self.lib.casl_spec1d(self.h, _d(a), _d(spec), int(iopt)), "casl_spec1d")
         return spec, a
+
+    def pvforce(self, ivor, vorvor, rnd):
+        """pvforce (evolution.f90:330-428) with the caller's uniforms in [0,1)
+        (2 per vortex for ivor = 1, else 3)."""
+        r = _f64(rnd).ravel()
+        m = 2 if ivor == 1 else 3
+        self._check(self.lib.casl_pvforce(self.h, int(ivor), float(vorvor), len(r) // m, _d(r)),
+                    "casl_pvforce")
+
+    def nb_forcing_init(self, kfmid, fwid, famp):
+        k = C.c_int()
+        self._check(self.lib.casl_nb_forcing_init(self.h, float(kfmid), float(fwid), float(famp),
+                                                  C.byref(k)), "casl_nb_forcing_init")
+        return k.value
+
+    def nb_forcing(self, dt, rnd):
+        r = _f64(rnd).ravel()
+        self._check(self.lib.casl_nb_forcing(self.h, float(dt), _d(r)), "casl_nb_forcing")
 
     def set_precision(self, mode):
         """0 = FP64 (default); 1 = FP32 inversion (casl_set_precision)."""

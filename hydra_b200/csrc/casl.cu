@@ -2075,6 +2075,7 @@ void casl_destroy(casl_handle *h) {
   io_release(h);
   cudaStreamSynchronize(h->stream);
   closure_release(h);
+  forcing_release(h);
   cudaFree(h->f32);
   free_all(h);
   if (h->prof_ev) {

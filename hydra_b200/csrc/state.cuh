@@ -11,6 +11,7 @@
 
 namespace casl {
 struct ClosureState;  // the learned velocity closure attached to a handle (closure.cu)
+struct ForcingState;  // narrow-band spectral forcing tables (forcing.cu)
 }
 
 struct casl_handle {
@@ -77,6 +78,8 @@ struct casl_handle {
   int prec;
   float *f32;            // 6 * n*n floats, allocated when the mode is first selected
   int uv_fp32;           // the latest stage velocity exists only in f32 (uu, vv stale)
+
+  casl::ForcingState *forcing;  // nb_forcing tables (nullable)
 };
 
 #define CASL_PROF_MAX 8192
@@ -140,5 +143,6 @@ int closure_stage32(casl_handle *h, const float **u, const float **v);  // FP32-
 // Before each advance of casl_step: the periodic fine-grid check.
 int closure_step_check(casl_handle *h);
 void closure_release(casl_handle *h);
+void forcing_release(casl_handle *h);  // forcing.cu
 
 }  // namespace casl

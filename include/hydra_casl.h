@@ -165,6 +165,28 @@ int casl_initialise(casl_handle *h, const double *qq_init);
  * (surgery; or prepare + recontour + init every nregmax) then advance. */
 int casl_step(casl_handle *h, int nsteps);
 
+/* ---- forcing of the residual PV (row f3) ---------------------------------- */
+/* The reference adds these to qd at the end of advance (evolution.f90:316-
+ * 323); a host that runs them calls them after casl_advance.  The reference
+ * draws its random numbers from GNU rand() inside the procedures; here the
+ * caller passes them in, in the reference's draw order.
+ * pvforce (evolution.f90:330-428): nvor point vortices of alternating sign
+ * +-vorvor (ivor = 1; rnd holds x, y in [0,1) per vortex, in grid units of
+ * nx, ny) or dipoles of strength vorvor (ivor != 1; theta, x, y in [0,1)),
+ * spread over their grid box by inverse bilinear interpolation, transformed
+ * and added to qd.  The caller computes nvor as the reference does,
+ * 2*nint((dnvor*t - totnvor)/2) or nint(dnvor*t - totnvor). */
+int casl_pvforce(casl_handle *h, int ivor, double vorvor, int nvor, const double *rnd);
+/* init_forcing (spectral.f90:160-229): the band |k - kfmid| <= fwid of the
+ * narrow-band forcing with amplitude famp = fbase*2^nfamp; *nrand receives
+ * the number of random values each casl_nb_forcing call consumes.  A band
+ * reaching wavenumber 0 or the Nyquist wavenumber (where the reference
+ * stops) returns CASL_EINVAL. */
+int casl_nb_forcing_init(casl_handle *h, double kfmid, double fwid, double famp, int *nrand);
+/* nb_forcing (spectral.f90:232-285) then qd = qd + dqdt: rnd holds nrand
+ * values of myrand (2*rand()-1) in the reference's order. */
+int casl_nb_forcing(casl_handle *h, double dt, const double *rnd);
+
 /* Precision of the inversion inside casl_advance / casl_step.
  * CASL_PREC_FP64 (default): everything FP64, the parity mode.
  * CASL_PREC_FP32_INVERSION: the inverse transform pair of every RK4 stage

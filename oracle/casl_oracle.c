@@ -2035,3 +2035,129 @@ void o_diagnostics(o_state *s, double *out) {
   free(ss);
   free(zz);
 }
+
+/* ======================================================================
+ * Forcing (evolution.f90:330-428, spectral.f90:160-285), with the uniform
+ * random numbers supplied by the caller in the order the reference draws
+ * them (its GNU rand() stream is not restated)
+ * ====================================================================== */
+/* pvforce (evolution.f90:330-428): nvor point vortices (ivor = 1, two
+ * numbers in [0,1) each: x, y) or dipoles (three: theta, x, y) scattered to
+ * the grid by inverse bilinear interpolation, transformed, added to qd. */
+void o_pvforce(o_state *s, int ivor, double vorvor, int nvor, const double *rnd) {
+  const int nx = s->nx, ny = s->ny;
+  size_t nn = (size_t)nx * ny;
+  double *wkp = xcalloc(nn, sizeof(double)), *wks = xcalloc(nn, sizeof(double));
+  const double dnx = (double)nx, dny = (double)ny;
+  if (ivor == 1) {
+    double svor = -vorvor;
+    for (int k = 0; k < nvor; k++) {
+      svor = -svor;
+      double xx = dnx * rnd[2 * k];
+      int ix0 = 1 + f_int(xx);
+      double pxc = (double)ix0 - xx, px = ONE - pxc;
+      int ix1 = s->ixp[ix0];
+      double yy = dny * rnd[2 * k + 1];
+      int iy0 = 1 + f_int(yy);
+      double pyc = (double)iy0 - yy, py = ONE - pyc;
+      int iy1 = s->iyp[iy0];
+      wkp[PHY(s, iy0, ix0)] = wkp[PHY(s, iy0, ix0)] + svor * pyc * pxc;
+      wkp[PHY(s, iy0, ix1)] = wkp[PHY(s, iy0, ix1)] + svor * pyc * px;
+      wkp[PHY(s, iy1, ix0)] = wkp[PHY(s, iy1, ix0)] + svor * py * pxc;
+      wkp[PHY(s, iy1, ix1)] = wkp[PHY(s, iy1, ix1)] + svor * py * px;
+    }
+  } else {
+    for (int k = 0; k < nvor; k++) {
+      double theta = s->twopi * rnd[3 * k];
+      double cth = cos(theta), sth = sin(theta);
+      double xx = dnx * rnd[3 * k + 1];
+      int ix0 = 1 + f_int(xx);
+      double pxc = (double)ix0 - xx, px = ONE - pxc;
+      int ix1 = s->ixp[ix0];
+      double yy = dny * rnd[3 * k + 2];
+      int iy0 = 1 + f_int(yy);
+      double pyc = (double)iy0 - yy, py = ONE - pyc;
+      int iy1 = s->iyp[iy0];
+      wkp[PHY(s, iy0, ix0)] = wkp[PHY(s, iy0, ix0)] - vorvor * (pyc * cth + pxc * sth);
+      wkp[PHY(s, iy0, ix1)] = wkp[PHY(s, iy0, ix1)] + vorvor * (pyc * cth - px * sth);
+      wkp[PHY(s, iy1, ix0)] = wkp[PHY(s, iy1, ix0)] + vorvor * (pxc * sth - py * cth);
+      wkp[PHY(s, iy1, ix1)] = wkp[PHY(s, iy1, ix1)] + vorvor * (px * sth + py * cth);
+    }
+  }
+  o_ptospc(s, wkp, wks);
+  for (size_t k = 0; k < nn; k++) s->qd[k] = s->qd[k] + wks[k];
+  free(wkp);
+  free(wks);
+}
+
+/* init_forcing (spectral.f90:160-229): the wavenumbers of the band
+ * |k - kfmid| <= fwid (zero-y, zero-x and interior lists) and the amplitude
+ * factor; famp = fbase*2**nfamp.  Returns the number of uniform numbers one
+ * nb_forcing call draws, or -1 where the reference stops. */
+static int *g_kxfxo, *g_kyfyo, *g_kxf, *g_kyf, g_nkfxo, g_nkfyo, g_nkf;
+static double g_forfac;
+int o_nb_forcing_init(o_state *s, double kfmid, double fwid, double famp) {
+  const int nx = s->nx, ny = s->ny, nwx = nx / 2, nwy = ny / 2;
+  if (fwid >= kfmid) return -1;
+  int mn = (nwx - (int)kfmid) < (nwy - (int)kfmid) ? (nwx - (int)kfmid) : (nwy - (int)kfmid);
+  if (fwid >= (double)mn) return -1;
+  free(g_kxfxo); free(g_kyfyo); free(g_kxf); free(g_kyf);
+  g_kxfxo = xcalloc(nx, sizeof(int));
+  g_kyfyo = xcalloc(ny, sizeof(int));
+  g_kxf = xcalloc((size_t)nx * ny, sizeof(int));
+  g_kyf = xcalloc((size_t)nx * ny, sizeof(int));
+  g_nkfxo = 0;
+  for (int kx = 1; kx <= nx; kx++)
+    if (fabs(s->rkx[kx - 1] - kfmid) <= fwid + s->small) g_kxfxo[g_nkfxo++] = kx;
+  g_nkfyo = 0;
+  for (int ky = 1; ky <= ny; ky++)
+    if (fabs(s->rky[ky - 1] - kfmid) <= fwid + s->small) g_kyfyo[g_nkfyo++] = ky;
+  g_nkf = 0;
+  for (int ky = 2; ky <= nwy; ky++)
+    for (int kx = 2; kx <= nwx; kx++)
+      if (fabs(s->rk[SPC(s, kx, ky)] - kfmid) <= fwid + s->small) {
+        g_kxf[g_nkf] = kx;
+        g_kyf[g_nkf] = ky;
+        g_nkf++;
+      }
+  g_forfac = (double)(nx * ny / 2) * famp / (s->twopi * fwid);
+  return 2 * g_nkfxo + 2 * g_nkfyo + 4 * g_nkf;
+}
+
+/* nb_forcing (spectral.f90:232-285) then qd = qd + dqdt (evolution.f90:320-
+ * 323); rnd holds the myrand values 2*rand()-1 in the reference's order. */
+void o_nb_forcing(o_state *s, double dt, const double *rnd) {
+  const int nx = s->nx, ny = s->ny, nx2 = nx + 2, ny2 = ny + 2;
+  size_t nn = (size_t)nx * ny;
+  double *dqdt = xcalloc(nn, sizeof(double));
+  const double ffac = g_forfac * dt;
+  int r = 0;
+  for (int k = 0; k < g_nkfxo; k++) {
+    int kxfl = g_kxfxo[k];
+    double f1 = rnd[r++], f2 = rnd[r++];
+    double fmag = sqrt(TWO * ffac * s->rkx[kxfl - 1] / (f1 * f1 + f2 * f2));
+    dqdt[SPC(s, kxfl, 1)] = fmag * f1;
+    dqdt[SPC(s, nx2 - kxfl, 1)] = fmag * f2;
+  }
+  for (int k = 0; k < g_nkfyo; k++) {
+    int kyfl = g_kyfyo[k];
+    double f1 = rnd[r++], f2 = rnd[r++];
+    double fmag = sqrt(TWO * ffac * s->rky[kyfl - 1] / (f1 * f1 + f2 * f2));
+    dqdt[SPC(s, 1, kyfl)] = fmag * f1;
+    dqdt[SPC(s, 1, ny2 - kyfl)] = fmag * f2;
+  }
+  for (int k = 0; k < g_nkf; k++) {
+    int kxfl = g_kxf[k], kyfl = g_kyf[k];
+    double f1 = rnd[r++], f2 = rnd[r++];
+    double fmag = sqrt(ffac * s->rk[SPC(s, kxfl, kyfl)] / (f1 * f1 + f2 * f2));
+    dqdt[SPC(s, kxfl, kyfl)] = fmag * f1;
+    dqdt[SPC(s, nx2 - kxfl, kyfl)] = fmag * f2;
+    f1 = rnd[r++];
+    f2 = rnd[r++];
+    fmag = sqrt(ffac * s->rk[SPC(s, kxfl, kyfl)] / (f1 * f1 + f2 * f2));
+    dqdt[SPC(s, kxfl, ny2 - kyfl)] = fmag * f2;
+    dqdt[SPC(s, nx2 - kxfl, ny2 - kyfl)] = -fmag * f1;
+  }
+  for (size_t k = 0; k < nn; k++) s->qd[k] = s->qd[k] + dqdt[k];
+  free(dqdt);
+}

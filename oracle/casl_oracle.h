@@ -121,6 +121,12 @@ void o_spec_tables(o_state *s, int *kmax, int *kmaxred, double *spmf, double *al
 /* genfg's ultra-fine PV (post/genfg.f90:79-113): float32 (nyu, nxu). */
 void o_genfg(o_state *s, const double *qq, float *out);
 
+/* Forcing (evolution.f90:330-428, spectral.f90:160-285) with the uniform
+ * random numbers supplied by the caller, in the reference's draw order. */
+void o_pvforce(o_state *s, int ivor, double vorvor, int nvor, const double *rnd);
+int o_nb_forcing_init(o_state *s, double kfmid, double fwid, double famp);
+void o_nb_forcing(o_state *s, double dt, const double *rnd);
+
 #ifdef __cplusplus
 }
 #endif

@@ -87,6 +87,10 @@ def lib():
         L.o_spec1d.argtypes = [C.c_void_p, dp, dp, C.c_int]
         L.o_spec_tables.argtypes = [C.c_void_p, ip, ip, dp, dp]
         L.o_genfg.argtypes = [C.c_void_p, dp, C.POINTER(C.c_float)]
+        L.o_pvforce.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int, dp]
+        L.o_nb_forcing_init.restype = C.c_int
+        L.o_nb_forcing_init.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double]
+        L.o_nb_forcing.argtypes = [C.c_void_p, C.c_double, dp]
     return _lib
 
 
@@ -294,6 +298,19 @@ class Oracle:
         out = np.zeros((16 * self.nx, 16 * self.nx), np.float32)
         lib().o_genfg(self.h, _dp(r), out.ctypes.data_as(C.POINTER(C.c_float)))
         return out
+
+    def pvforce(self, ivor, vorvor, rnd):
+        """pvforce (evolution.f90:330-428) with the given uniforms."""
+        r = np.ascontiguousarray(rnd, np.float64).ravel()
+        m = 2 if ivor == 1 else 3
+        lib().o_pvforce(self.h, int(ivor), float(vorvor), len(r) // m, _dp(r))
+
+    def nb_forcing_init(self, kfmid, fwid, famp):
+        return lib().o_nb_forcing_init(self.h, float(kfmid), float(fwid), float(famp))
+
+    def nb_forcing(self, dt, rnd):
+        r = np.ascontiguousarray(rnd, np.float64).ravel()
+        lib().o_nb_forcing(self.h, float(dt), _dp(r))
 
     def spec_tables(self):
         """kmax, kmaxred, spmf, alk of init_spectral (spectral.f90:109-134)."""
