@@ -13,7 +13,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libhydra_casl.so")
-SOURCES = ["casl.cu", "surgery.cu", "renode.cu", "recontour.cu", "noalloc.cu", "io.cu", "closure.cu", "forcing.cu"]
+SOURCES = ["casl.cu", "surgery.cu", "renode.cu", "recontour.cu", "noalloc.cu", "io.cu", "closure.cu", "forcing.cu", "ensemble.cu"]
 HEADERS = ["common.cuh", "fft.cuh", "state.cuh", "scan.cuh", "renode.cuh", "tc.cuh"]
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 

@@ -133,6 +133,12 @@ SIGNATURES = {
     "casl_pvforce": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_int, _dp]),
     "casl_nb_forcing_init": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double, _ip]),
     "casl_nb_forcing": (C.c_int, [C.c_void_p, C.c_double, _dp]),
+    "casl_ensemble_create": (C.c_int, [C.POINTER(CaslParams), C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "casl_ensemble_members": (C.c_int, [C.c_void_p, _ip]),
+    "casl_ensemble_initialise": (C.c_int, [C.c_void_p, _dp, _ip]),
+    "casl_ensemble_member_counts": (C.c_int, [C.c_void_p, C.c_int, _ip, _ip, _dp]),
+    "casl_ensemble_member_contours": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp, _ip, _ip, _ip, _ip, _ip]),
+    "casl_ensemble_member_scalar": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _dp]),
 }
 
 
@@ -523,3 +529,60 @@ class CaslNet:
 
     def adam(self, lr):
         self._check(self.lib.casl_net_adam(self.h, float(lr)), "casl_net_adam")
+
+
+class CaslEnsemble(CaslGPU):
+    """M independent simulations of one grid size in one handle
+    (casl_ensemble_*): step() advances all members with single launches per
+    stage; member_*() read one member back in its own numbering."""
+
+    def __init__(self, nx, members, device=0, **kw):
+        self.lib = load_library()
+        kw = dict(kw)
+        elly = kw.pop("elly", None)
+        ellx = kw.pop("ellx", 2 * np.pi)
+        elly = ellx if elly is None else elly
+        npm = kw.pop("npm", None) or 60 * nx * nx * members
+        d = dict(ncontq=40, kd=0.0, beta=0.0, rtherm=0.0, rekman=0.0, cdamp=2.0, nnu=3.0, nm=0,
+                 nlevm=2000, fixed_dt=0.0, dtmax=0.05, force_surgery=1, nregmax=20, twistmax=2.5)
+        d.update(kw)
+        self.p = CaslParams(nx, nx, d["ncontq"], ellx, elly, d["kd"], d["beta"], d["rtherm"],
+                            d["rekman"], d["cdamp"], d["nnu"], int(npm), int(d["nm"]), d["nlevm"],
+                            d["fixed_dt"], d["dtmax"], d["force_surgery"], d["nregmax"],
+                            d["twistmax"])
+        h = C.c_void_p()
+        self._check(self.lib.casl_ensemble_create(C.byref(self.p), int(members), int(device),
+                                                  C.byref(h)), "casl_ensemble_create")
+        self.h = h
+        self.nx = self.ny = nx
+        self.members = members
+
+    def initialise_members(self, fields, ncontq=None):
+        q = np.ascontiguousarray(np.stack([_f64(f, (self.nx, self.ny)) for f in fields]))
+        if q.shape[0] != self.members:
+            raise ValueError("one field per member")
+        nc = None if ncontq is None else np.ascontiguousarray(ncontq, np.int32)
+        self._check(self.lib.casl_ensemble_initialise(self.h, _d(q), _i(nc)), "casl_ensemble_initialise")
+
+    def member_counts(self, m):
+        nq, npt, qj = C.c_int(), C.c_int(), C.c_double()
+        self._check(self.lib.casl_ensemble_member_counts(self.h, int(m), C.byref(nq), C.byref(npt),
+                                                         C.byref(qj)), "casl_ensemble_member_counts")
+        return nq.value, npt.value, qj.value
+
+    def member_contours(self, m):
+        nq, npt, qj = self.member_counts(m)
+        xq = np.zeros(npt); yq = np.zeros(npt); nextq = np.zeros(npt, np.int32)
+        indq = np.zeros(nq, np.int32); npq = np.zeros(nq, np.int32)
+        i1q = np.zeros(nq, np.int32); i2q = np.zeros(nq, np.int32)
+        self._check(self.lib.casl_ensemble_member_contours(self.h, int(m), _d(xq), _d(yq), _i(nextq),
+                                                           _i(indq), _i(npq), _i(i1q), _i(i2q)),
+                    "casl_ensemble_member_contours")
+        return dict(nq=nq, nptq=npt, qjump=qj, xq=xq, yq=yq, nextq=nextq, indq=indq, npq=npq,
+                    i1q=i1q, i2q=i2q)
+
+    def member_scalar(self, m, name):
+        v = C.c_double()
+        self._check(self.lib.casl_ensemble_member_scalar(self.h, int(m), SCALARS[name], C.byref(v)),
+                    "casl_ensemble_member_scalar")
+        return v.value

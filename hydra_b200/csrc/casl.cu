@@ -164,26 +164,26 @@ static int rfft_dispatch(casl_handle *h, LD ld, ST st, int batch) {
 // along kx (spectral rows, v = ky) and then along ky (v = ix).  Only one of
 // the four global sides is vector-fastest.  The intermediate of both is
 // T[ky*n + ix].  The order of the axes changes results by rounding only.
-int ptospc_dev(casl_handle *h, const double *phys, double *spec) {
+int ptospc_dev(casl_handle *h, const double *phys, double *spec, int batch) {
   long long n = h->n, nn = n * n;
   // along iy for each ix: phys[ix*n+iy] -> spec[ky*n+ix] (spec != phys)
   int rc = RFFT_DISPATCH(true, false, true, (LoadStrided{phys, nn, n, 1}),
-                         (StoreStrided{spec, nn, 1, n}), 1);
+                         (StoreStrided{spec, nn, 1, n}), batch);
   if (rc) return rc;
   // along ix for each ky, in place by rows: spec[ky*n + kx]
   return RFFT_DISPATCH(true, false, false, (LoadStrided{spec, nn, n, 1}),
-                       (StoreStrided{spec, nn, n, 1}), 1);
+                       (StoreStrided{spec, nn, n, 1}), batch);
 }
 
-int spctop_dev(casl_handle *h, const double *spec, double *phys, double *tmp) {
+int spctop_dev(casl_handle *h, const double *spec, double *phys, double *tmp, int batch) {
   long long n = h->n, nn = n * n;
   // along kx for each ky: spec[ky*n+kx] -> tmp[ky*n+ix]
   int rc = RFFT_DISPATCH(false, false, false, (LoadStrided{spec, nn, n, 1}),
-                         (StoreStrided{tmp, nn, n, 1}), 1);
+                         (StoreStrided{tmp, nn, n, 1}), batch);
   if (rc) return rc;
   // along ky for each ix: tmp[ky*n+ix] -> phys[ix*n+iy]
   return RFFT_DISPATCH(false, true, false, (LoadStrided{tmp, nn, 1, n}),
-                       (StoreStrided{phys, nn, n, 1}), 1);
+                       (StoreStrided{phys, nn, n, 1}), batch);
 }
 
 // ---------------------------------------------------------------------------
@@ -211,10 +211,15 @@ struct LoadDeriv {
   const double *green;
   const double *hrkx, *hrky;
   int n;
+  // ensemble: batch entry b is entry b % nb of member b / nb, whose fields
+  // lie ms elements after the previous member's (nb = 6, ms = 0: one member)
+  int nb = 6;
+  long long ms = 0;
   __device__ __forceinline__ double base(int b, int kx0, int ky0) const {
     long long k = (long long)ky0 * n + kx0;
-    double v = pick(f, b)[k];
-    return pick(wg, b) ? green[k] * v : v;
+    const int e = b % nb;
+    double v = pick(f, e)[(long long)(b / nb) * ms + k];
+    return pick(wg, e) ? green[k] * v : v;
   }
   // first pass of an inverse transform: vector v = ky, element j = kx.
   // Branch-free, so that a thread's loads are issued together: the factor
@@ -222,7 +227,7 @@ struct LoadDeriv {
   // and the reflected index (n-k) mod n is always a valid element.
   __device__ __forceinline__ double operator()(int b, int v, int j) const {
     const int nw = n >> 1, kx = j, ky = v;
-    const bool dx = pick(dir, b) == 0;
+    const bool dx = pick(dir, b % nb) == 0;
     const int k = dx ? kx : ky;
     const int kr = (n - k) & (n - 1);
     const int hi = k < nw ? 2 * k - 1 : 2 * (n - k) - 1;
@@ -236,15 +241,16 @@ struct LoadDeriv {
   // d/dx the reflected indices n-j, n-j-1 run backwards from an odd start,
   // so they stay two loads.
   __device__ __forceinline__ double2 pair(int b, int v, int j) const {
-    if (pick(dir, b) == 0) return make_double2((*this)(b, v, j), (*this)(b, v, j + 1));
+    const int e = b % nb;
+    if (pick(dir, e) == 0) return make_double2((*this)(b, v, j), (*this)(b, v, j + 1));
     const int nw = n >> 1, k = v;
     const int kr = (n - k) & (n - 1);
     const int hi = k < nw ? 2 * k - 1 : 2 * (n - k) - 1;
     const double h = hrky[hi < 0 ? 0 : hi];
     const double fac = (k == 0 || k == nw) ? 0.0 : (k < nw ? -h : h);
     const long long o = (long long)kr * n + j;
-    double2 q = *reinterpret_cast<const double2 *>(pick(f, b) + o);
-    if (pick(wg, b)) {
+    double2 q = *reinterpret_cast<const double2 *>(pick(f, e) + (long long)(b / nb) * ms + o);
+    if (pick(wg, e)) {
       const double2 g = *reinterpret_cast<const double2 *>(green + o);
       q = make_double2(g.x * q.x, g.y * q.y);
     }
@@ -262,18 +268,19 @@ struct LoadQC {
   long long nn;
   double inv;           // 1/(256 n^2)
   int n;
+  // batch entry b = ensemble member b (its cells and scalars)
   __device__ __forceinline__ double operator()(int b, int v /*ix*/, int j /*iy*/) const {
-    long long k = (long long)v * n + j;
-    long long num = (long long)C[k] * nn - s->csum;
-    double q = s->qjump * ((double)num * inv);
+    long long k = (long long)b * nn + (long long)v * n + j;
+    long long num = (long long)C[k] * nn - s[b].csum;
+    double q = s[b].qjump * ((double)num * inv);
     if (betac) q = q + betac[j];
     return q;
   }
   __device__ __forceinline__ double2 pair(int b, int v, int j) const {
-    long long k = (long long)v * n + j;
+    long long k = (long long)b * nn + (long long)v * n + j;
     const int2 c = *reinterpret_cast<const int2 *>(C + k);
-    const long long S = s->csum;
-    const double qj = s->qjump;
+    const long long S = s[b].csum;
+    const double qj = s[b].qjump;
     double q0 = qj * ((double)((long long)c.x * nn - S) * inv);
     double q1 = qj * ((double)((long long)c.y * nn - S) * inv);
     if (betac) {
@@ -299,18 +306,21 @@ struct LoadAdvectT {
   const T *fx[2], *fy[2];
   double betab[2];  // beta added to fy for the qs term when beffect
   int n;
+  long long ms = 0;  // ensemble: entry b is term b % 2 of member b / 2, fields ms apart
   __device__ __forceinline__ double operator()(int b, int v /*ix*/, int j /*iy*/) const {
-    long long k = (long long)v * n + j;
-    const double bb = pick(betab, b);
-    double gx = (double)pick(fx, b)[k], gy = (double)pick(fy, b)[k];
+    const int e = b & 1;
+    long long k = (long long)(b >> 1) * ms + (long long)v * n + j;
+    const double bb = pick(betab, e);
+    double gx = (double)pick(fx, e)[k], gy = (double)pick(fy, e)[k];
     if (bb != 0.0) gy = gy + bb;
     return -(double)uu[k] * gx - (double)vv[k] * gy;
   }
   __device__ __forceinline__ double2 pair(int b, int v, int j) const {
-    long long k = (long long)v * n + j;
-    const double bb = pick(betab, b);
-    const double2 gx = ld2(pick(fx, b) + k);
-    double2 gy = ld2(pick(fy, b) + k);
+    const int e = b & 1;
+    long long k = (long long)(b >> 1) * ms + (long long)v * n + j;
+    const double bb = pick(betab, e);
+    const double2 gx = ld2(pick(fx, e) + k);
+    double2 gy = ld2(pick(fy, e) + k);
     const double2 u = ld2(uu + k);
     const double2 w = ld2(vv + k);
     if (bb != 0.0) {
@@ -330,6 +340,7 @@ struct StoreSource {
   const double *qq, *pp, *epq;
   double rekman, kdsq, therm;
   int heating, friction, lev, n;
+  long long ms = 0;  // ensemble: entry b is term b % 2 of member b / 2
   __device__ __forceinline__ double damped(double x, double p, double q, double e) const {
     double t;
     if (heating) {
@@ -347,16 +358,16 @@ struct StoreSource {
     return t;
   }
   __device__ __forceinline__ void operator()(int b, int v /*ky*/, int k /*kx*/, double x) const {
-    const long long idx = (long long)v * n + k;
-    if (b == 1) {
+    const long long idx = (long long)(b >> 1) * ms + (long long)v * n + k;
+    if (b & 1) {
       sqs[idx] = x;
       return;
     }
     sqd[idx] = damped(x, pp[idx], qq[idx], lev ? epq[idx] : 0.0);
   }
   __device__ __forceinline__ void pair(int b, int v, int k, double2 x) const {
-    const long long i = (long long)v * n + k;
-    if (b == 1) {
+    const long long i = (long long)(b >> 1) * ms + (long long)v * n + k;
+    if (b & 1) {
       *reinterpret_cast<double2 *>(sqs + i) = x;
       return;
     }
@@ -368,28 +379,33 @@ struct StoreSource {
   }
 };
 
+// (ensemble: entry b is entry b % nb of member b / nb, fields ms apart)
 struct StoreScaled {
   __host__ double bytes() const { return 8.0; }
   double *p[6];
   double scale[6];
   int n;
+  int nb = 6;
+  long long ms = 0;
   // last pass of an inverse transform: vector v = ix, element k = iy
   __device__ __forceinline__ void operator()(int b, int v, int k, double x) const {
-    const double sc = pick(scale, b);
-    pick(p, b)[(long long)v * n + k] = sc == 1.0 ? x : sc * x;
+    const double sc = pick(scale, b % nb);
+    pick(p, b % nb)[(long long)(b / nb) * ms + (long long)v * n + k] = sc == 1.0 ? x : sc * x;
   }
   __device__ __forceinline__ void pair(int b, int v, int k, double2 x) const {
-    const double sc = pick(scale, b);
+    const double sc = pick(scale, b % nb);
     if (sc != 1.0) x = make_double2(sc * x.x, sc * x.y);
-    *reinterpret_cast<double2 *>(pick(p, b) + (long long)v * n + k) = x;
+    *reinterpret_cast<double2 *>(pick(p, b % nb) + (long long)(b / nb) * ms + (long long)v * n + k) = x;
   }
 };
 struct LoadBatch {
   __host__ double bytes() const { return 8.0; }
   const double *p[6];
   long long vs, es;
+  int nb = 6;
+  long long ms = 0;
   __device__ __forceinline__ double operator()(int b, int v, int j) const {
-    return pick(p, b)[(long long)v * vs + (long long)j * es];
+    return pick(p, b % nb)[(long long)(b / nb) * ms + (long long)v * vs + (long long)j * es];
   }
 };
 // FP32 storage for the inverse transform pair of the FP32-inversion mode:
@@ -443,9 +459,10 @@ struct LoadVort {
   const double *qq, *pp;
   double kdsq;
   int btropic, n;
+  long long ms = 0;  // ensemble: entry b = member b, fields ms apart
   // first pass of an inverse transform: vector v = ky, element j = kx
   __device__ __forceinline__ double operator()(int b, int v, int j) const {
-    long long k = (long long)v * n + j;
+    long long k = (long long)b * ms + (long long)v * n + j;
     return btropic ? qq[k] : qq[k] + kdsq * pp[k];
   }
 };
@@ -478,6 +495,26 @@ __device__ __forceinline__ void c2g_decode(unsigned long long w, int &c0, int &c
   c3 = (int)v;
 }
 
+// Member of node i in an ensemble (mnode[m] <= i < mnode[m+1]; members
+// without nodes have equal bounds and are skipped); 0 without an ensemble.
+__device__ __forceinline__ int member_of(const int *__restrict__ mnode, int M, int i) {
+  if (!mnode) return 0;
+  int lo = 0, hi = M;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(&mnode[mid]) <= i) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+// Per-member strides of con2grid's scratch in an ensemble.
+struct C2GMembers {
+  const int *mnode;  // nullptr: one simulation
+  int M;
+  long long jws;     // packed words per member
+  int ljs;           // bottom-row jumps per member
+  int cs;            // Scalars stride in 64-bit words (member m's csum = csum + m*cs)
+};
+
 // Per segment (i, nextq(i)): x fine-grid-line crossings and the crossing of
 // y = ymin, counted as +-1 PV jumps (contours.f90:232-270): J += sgn at
 // each (PACKED: into the row's 16-bit lane of JW), ljx the bottom-boundary
@@ -489,10 +526,11 @@ __global__ void k_c2g_scatter(const double *__restrict__ xq, const double *__res
                               int *__restrict__ J, unsigned long long *__restrict__ JW,
                               int *__restrict__ ljx,
                               Consts c, int *__restrict__ err,
-                              unsigned long long *__restrict__ csum) {
+                              unsigned long long *__restrict__ csum, C2GMembers mb) {
   CASL_PDL_ENTRY();
   // the coarsening that follows accumulates the coarse-cell sum here
-  if (blockIdx.x == 0 && threadIdx.x == 0) *csum = 0;
+  if (blockIdx.x == 0)
+    for (int m = threadIdx.x; m < mb.M; m += blockDim.x) csum[(long long)m * mb.cs] = 0;
   const unsigned FULL = 0xffffffffu;
   const int npt = s->nptq, nf = c.nxf, lane = threadIdx.x & 31;
   const int wstride = gridDim.x * blockDim.x;
@@ -511,6 +549,8 @@ __global__ void k_c2g_scatter(const double *__restrict__ xq, const double *__res
       y1 = yq[i];
     }
     const double xs = __shfl_down_sync(FULL, x1, 1), ys = __shfl_down_sync(FULL, y1, 1);
+    int mi = 0;
+    if (i < npt) mi = member_of(mb.mnode, mb.M, i);
     if (i < npt) {
       if (ia < 0 || ia >= npt) {
         atomicExch(err, CASL_EINVAL);
@@ -538,7 +578,7 @@ __global__ void k_c2g_scatter(const double *__restrict__ xq, const double *__res
             const double p = -(yi - c.hly * cc) / (dy + c.small);
             int ix = 1 + f_int(c.glxfi * fmod(c.ellx + c.hlx + xi + p * dx, c.ellx));
             ix = ix < 1 ? 1 : (ix > nf ? nf : ix);
-            red_add_s32(&ljx[ix - 1], -(int)cc);
+            red_add_s32(&ljx[(long long)mi * mb.ljs + ix - 1], -(int)cc);
           }
           if (nxc != 0) {
             jump = f_isign1(nxc);
@@ -565,7 +605,7 @@ __global__ void k_c2g_scatter(const double *__restrict__ xq, const double *__res
       if (iy >= 2 && iy <= c.nyf) {
         if (PACKED) {
           const int r = iy - 1;
-          red_add_u64(&JW[(long long)(ix - 1) * c.nx + (r >> 2)],
+          red_add_u64(&JW[(long long)mi * mb.jws + (long long)(ix - 1) * c.nx + (r >> 2)],
                       (unsigned long long)((long long)sgn << (16 * (r & 3))));
         } else
           red_add_s32(&J[(long long)(ix - 1) * c.nyf + (iy - 1)], sgn);
@@ -692,8 +732,15 @@ __global__ void __launch_bounds__(1024) k_c2g_packed_sum(const unsigned long lon
                                                          const int *__restrict__ ljx,
                                                          int *__restrict__ C,
                                                          unsigned long long *__restrict__ csum,
-                                                         int n, int nf) {
+                                                         int n, int nf, C2GMembers mb) {
   CASL_PDL_ENTRY();
+  {  // ensemble member blockIdx.y
+    const long long m = blockIdx.y;
+    JW += m * mb.jws;
+    ljx += m * mb.ljs;
+    C += m * (long long)n * n;
+    csum += m * mb.cs;
+  }
   constexpr int RPS = 32 * U;
   __shared__ int G[RPS][C2G_FC + 2];  // row length 33: conflict-free both ways
   __shared__ int G0[C2G_FC];
@@ -852,29 +899,31 @@ int con2grid_dev(casl_handle *h, bool want_levels) {
   const int U = n % 256 == 0 ? 8 : (n % 128 == 0 ? 4 : (n % 64 == 0 ? 2 : (n % 32 == 0 ? 1 : 0)));
   // packed path while the 16-bit counts cannot overflow (one net crossing
   // per level and fine edge: levels well below 32767)
+  // an ensemble always takes the packed path (its scratch holds only that)
+  if (h->M > 1 && (want_levels || U == 0 || h->p.ncontq >= 16384)) return CASL_EUNSUPPORTED;
   if (!want_levels && c.nxf == c.nyf && U > 0 && h->p.ncontq < 16384) {
     // four fine rows of a column per 64-bit word, in the first half of the
-    // fine-grid buffer
+    // fine-grid buffer (an ensemble: one such block per member)
     unsigned long long *JW = reinterpret_cast<unsigned long long *>(h->fineJ);
+    const C2GMembers mb{h->M > 1 ? h->mnode : nullptr, h->M, (long long)c.nxf * n, c.nxf,
+                        (int)(sizeof(Scalars) / 8)};
     {
-      const FillJob z[2] = {{JW, 2LL * c.nxf * n, 0u}, {h->ljx, (long long)c.nxf, 0u}};
+      const FillJob z[2] = {{JW, 2LL * c.nxf * n * h->M, 0u},
+                            {h->ljx, (long long)c.nxf * h->M, 0u}};
       if (int rc = fill_words(h->stream, z, 2)) return rc;
     }
-    if (h->nptq > 0) {
-      CASL_K(k_c2g_scatter<true>, grid_for(h->nptq), 256, 0, h->stream)(
-          h->xq, h->yq, h->nextq, h->scal, nullptr, JW, h->ljx, c, err, csum);
-    } else {
-      CASL_CUDA_TRY(cudaMemsetAsync(csum, 0, sizeof(unsigned long long), h->stream));
-    }
-    const int nblk = (n + C2G_CW - 1) / C2G_CW;
+    // with no nodes the scatter still runs (its first block clears the sums)
+    CASL_K(k_c2g_scatter<true>, grid_for(h->nptq > 0 ? h->nptq : 1), 256, 0, h->stream)(
+        h->xq, h->yq, h->nextq, h->scal, nullptr, JW, h->ljx, c, err, csum, mb);
+    const dim3 nblk((n + C2G_CW - 1) / C2G_CW, h->M);
     if (U == 8)
-      CASL_K(k_c2g_packed_sum<8>, nblk, 1024, 0, h->stream)(JW, h->ljx, h->coarseC, csum, n, c.nxf);
+      CASL_K(k_c2g_packed_sum<8>, nblk, 1024, 0, h->stream)(JW, h->ljx, h->coarseC, csum, n, c.nxf, mb);
     else if (U == 4)
-      CASL_K(k_c2g_packed_sum<4>, nblk, 1024, 0, h->stream)(JW, h->ljx, h->coarseC, csum, n, c.nxf);
+      CASL_K(k_c2g_packed_sum<4>, nblk, 1024, 0, h->stream)(JW, h->ljx, h->coarseC, csum, n, c.nxf, mb);
     else if (U == 2)
-      CASL_K(k_c2g_packed_sum<2>, nblk, 1024, 0, h->stream)(JW, h->ljx, h->coarseC, csum, n, c.nxf);
+      CASL_K(k_c2g_packed_sum<2>, nblk, 1024, 0, h->stream)(JW, h->ljx, h->coarseC, csum, n, c.nxf, mb);
     else
-      CASL_K(k_c2g_packed_sum<1>, nblk, 1024, 0, h->stream)(JW, h->ljx, h->coarseC, csum, n, c.nxf);
+      CASL_K(k_c2g_packed_sum<1>, nblk, 1024, 0, h->stream)(JW, h->ljx, h->coarseC, csum, n, c.nxf, mb);
     return check_launch(h);
   }
   // the fine-grid levels themselves are wanted: crossings onto the fine
@@ -883,8 +932,9 @@ int con2grid_dev(casl_handle *h, bool want_levels) {
   CASL_CUDA_TRY(cudaMemsetAsync(h->fineJ, 0, fine * sizeof(int), h->stream));
   CASL_CUDA_TRY(cudaMemsetAsync(h->ljx, 0, (size_t)c.nxf * sizeof(int), h->stream));
   if (h->nptq > 0) {
+    const C2GMembers mb{nullptr, 1, 0, 0, (int)(sizeof(Scalars) / 8)};
     CASL_K(k_c2g_scatter<false>, grid_for(h->nptq), 256, 0, h->stream)(
-        h->xq, h->yq, h->nextq, h->scal, h->fineJ, nullptr, h->ljx, c, err, csum);
+        h->xq, h->yq, h->nextq, h->scal, h->fineJ, nullptr, h->ljx, c, err, csum, mb);
   } else {
     CASL_CUDA_TRY(cudaMemsetAsync(csum, 0, sizeof(unsigned long long), h->stream));
   }
@@ -895,20 +945,22 @@ int con2grid_dev(casl_handle *h, bool want_levels) {
   return check_launch(h);
 }
 
+// (an ensemble: every member's, spec being M fields long)
 int con2grid_to_spec(casl_handle *h, double *spec) {
   long long n = h->n, nn = n * n;
+  const int M = h->M;
   if (h->nptq == 0) {
-    CASL_CUDA_TRY(cudaMemsetAsync(spec, 0, nn * sizeof(double), h->stream));
+    CASL_CUDA_TRY(cudaMemsetAsync(spec, 0, M * nn * sizeof(double), h->stream));
     return CASL_OK;
   }
   int rc = con2grid_dev(h, false);
   if (rc) return rc;
   LoadQC ld{h->coarseC, h->scal, h->c.beffect ? h->betac : nullptr, nn,
             1.0 / (256.0 * (double)n * (double)n), (int)n};
-  rc = RFFT_DISPATCH(true, false, true, ld, (StoreStrided{spec, nn, 1, n}), 1);
+  rc = RFFT_DISPATCH(true, false, true, ld, (StoreStrided{spec, nn, 1, n}), M);
   if (rc) return rc;
   return RFFT_DISPATCH(true, false, false, (LoadStrided{spec, nn, n, 1}),
-                       (StoreStrided{spec, nn, n, 1}), 1);
+                       (StoreStrided{spec, nn, n, 1}), M);
 }
 
 int con2grid_to_phys(casl_handle *h, double *phys, bool want_levels) {
@@ -972,13 +1024,18 @@ __device__ __forceinline__ void nodes_rk_body(int bid, int nbk, double *__restri
                            double *__restrict__ xqi, double *__restrict__ yqi,
                            double *__restrict__ xqf, double *__restrict__ yqf,
                            const T *__restrict__ uu, const T *__restrict__ vv,
-                           const Scalars *__restrict__ s, const Consts &c) {
+                           const Scalars *__restrict__ s, const Consts &c,
+                           const int *__restrict__ mnode, int M) {
   const int npt = s->nptq;
-  const double dt = s->dt, dt2 = s->dt2, dt3 = s->dt3, dt6 = s->dt6;
   const double ex = c.ellx, ey = c.elly, hx = c.hlxi, hy = c.hlyi, oms = c.oms;
+  const long long nn = (long long)c.nx * c.ny;
   for (int i = bid * blockDim.x + threadIdx.x; i < npt; i += nbk * blockDim.x) {
+    // the node's ensemble member: its time step and velocity field
+    const int m = member_of(mnode, M, i);
+    const Scalars &sm = s[m];
+    const double dt = sm.dt, dt2 = sm.dt2, dt3 = sm.dt3, dt6 = sm.dt6;
     double uq, vq;
-    velint1(xq[i], yq[i], uu, vv, c, uq, vq);
+    velint1(xq[i], yq[i], uu + m * nn, vv + m * nn, c, uq, vq);
     if (STAGE == 1) {
       double x0 = xq[i], y0 = yq[i];
       xqi[i] = x0;
@@ -1015,22 +1072,23 @@ __global__ void k_combine(double *__restrict__ qs, double *__restrict__ qd,
                           const double *__restrict__ qc, double *__restrict__ qq,
                           double *__restrict__ pp, const double *__restrict__ flo,
                           const double *__restrict__ fhi, const double *__restrict__ green,
-                          long long nn) {
+                          long long nn, long long tot) {
   CASL_PDL_ENTRY();
-  // two elements per thread with 16-byte accesses (nn is even)
-  for (long long k2 = blockIdx.x * (long long)blockDim.x + threadIdx.x; k2 < nn / 2;
+  // two elements per thread with 16-byte accesses (nn is even); tot = M*nn
+  // over the members of an ensemble, whose tables are shared
+  for (long long k2 = blockIdx.x * (long long)blockDim.x + threadIdx.x; k2 < tot / 2;
        k2 += (long long)gridDim.x * blockDim.x) {
-    const long long k = 2 * k2;
+    const long long k = 2 * k2, kt = k & (nn - 1);  // nn is a power of two
     const double2 s = *reinterpret_cast<const double2 *>(qs + k);
     const double2 c = *reinterpret_cast<const double2 *>(qc + k);
     const double2 d = *reinterpret_cast<const double2 *>(qd + k);
-    const double2 f = *reinterpret_cast<const double2 *>(flo + k);
-    const double2 g = *reinterpret_cast<const double2 *>(green + k);
+    const double2 f = *reinterpret_cast<const double2 *>(flo + kt);
+    const double2 g = *reinterpret_cast<const double2 *>(green + kt);
     const double q0 = f.x * (s.x - c.x) + c.x + d.x, q1 = f.y * (s.y - c.y) + c.y + d.y;
     *reinterpret_cast<double2 *>(qq + k) = make_double2(q0, q1);
     *reinterpret_cast<double2 *>(pp + k) = make_double2(g.x * q0, g.y * q1);
     if (RESET) {
-      const double2 h = *reinterpret_cast<const double2 *>(fhi + k);
+      const double2 h = *reinterpret_cast<const double2 *>(fhi + kt);
       *reinterpret_cast<double2 *>(qs + k) = make_double2(q0, q1);
       *reinterpret_cast<double2 *>(qd + k) = make_double2(h.x * (q0 - c.x), h.y * (q1 - c.y));
     }
@@ -1047,6 +1105,13 @@ __global__ void k_reduce_adapt(const double *__restrict__ zz, const T *__restric
                                const T *__restrict__ vv, double *__restrict__ part,
                                long long nn) {
   CASL_PDL_ENTRY();
+  {  // ensemble member blockIdx.y: its fields and its gridDim.x partials
+    const long long m = blockIdx.y;
+    zz += m * nn;
+    uu += m * nn;
+    vv += m * nn;
+    part += m * 3 * gridDim.x;
+  }
   double sum = 0.0, zmax = 0.0, umax = 0.0;
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nn;
        k += (long long)gridDim.x * blockDim.x) {
@@ -1081,6 +1146,9 @@ __global__ void k_reduce_adapt(const double *__restrict__ zz, const T *__restric
 __global__ void k_adapt_final(const double *__restrict__ part, int nparts, Scalars *s, Consts c,
                               double fixed_dt) {
   CASL_PDL_ENTRY();
+  // ensemble member blockIdx.x
+  part += (long long)blockIdx.x * 3 * nparts;
+  s += blockIdx.x;
   __shared__ double s0[256], s1[256], s2[256];
   double a = 0.0, b = 0.0, d = 0.0;
   for (int i = threadIdx.x; i < nparts; i += blockDim.x) {
@@ -1125,12 +1193,14 @@ __global__ void k_adapt_final(const double *__restrict__ part, int nparts, Scala
 }
 
 __global__ void k_epq(const double *__restrict__ qdiss, double *__restrict__ epq,
-                      double *__restrict__ emq, const Scalars *__restrict__ s, long long nn) {
+                      double *__restrict__ emq, const Scalars *__restrict__ s, long long nn,
+                      long long tot) {
   CASL_PDL_ENTRY();
-  const double dfac = s->dt2 * s->zzrms;
-  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nn;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < tot;
        k += (long long)gridDim.x * blockDim.x) {
-    double e = exp(dfac * qdiss[k]);
+    const Scalars &sm = s[k / nn];  // ensemble member of element k
+    const double dfac = sm.dt2 * sm.zzrms;
+    double e = exp(dfac * qdiss[k & (nn - 1)]);
     epq[k] = e;
     emq[k] = 1.0 / e;
   }
@@ -1143,15 +1213,17 @@ __device__ __forceinline__ void spec_rk_body(int bid, int nbk, double *__restric
                           double *__restrict__ qsi, double *__restrict__ qsf,
                           double *__restrict__ qdi, double *__restrict__ qdf,
                           const double *__restrict__ sqs, const double *__restrict__ sqd,
-                          double *__restrict__ emq, const Scalars *__restrict__ s, long long nn) {
-  const double dt = s->dt, dt2 = s->dt2, dt3 = s->dt3, dt6 = s->dt6;
+                          double *__restrict__ emq, const Scalars *__restrict__ s, long long nn,
+                          long long tot) {
   auto L = [](const double *p, long long k) { return *reinterpret_cast<const double2 *>(p + k); };
   auto S = [](double *p, long long k, double x, double y) {
     *reinterpret_cast<double2 *>(p + k) = make_double2(x, y);
   };
-  for (long long k2 = bid * (long long)blockDim.x + threadIdx.x; k2 < nn / 2;
+  for (long long k2 = bid * (long long)blockDim.x + threadIdx.x; k2 < tot / 2;
        k2 += (long long)nbk * blockDim.x) {
     const long long k = 2 * k2;
+    const Scalars &sm = s[tot == nn ? 0 : k / nn];  // ensemble member of element k
+    const double dt = sm.dt, dt2 = sm.dt2, dt3 = sm.dt3, dt6 = sm.dt6;
     const double2 a = L(sqs, k), b = L(sqd, k);
     if (STAGE == 1) {
       const double2 si = L(qs, k), di = L(qd, k), e = L(emq, k);
@@ -1191,12 +1263,14 @@ template <class T>
 struct NodeRkArgs {
   double *xq, *yq, *xqi, *yqi, *xqf, *yqf;
   const T *uu, *vv;
+  const int *mnode;  // ensemble: first node of each member (nullptr: one simulation)
+  int M;
 };
 struct SpecRkArgs {
   double *qs, *qd, *qsi, *qsf, *qdi, *qdf;
   const double *sqs, *sqd;
   double *emq;
-  long long nn;
+  long long nn, tot;  // tot = M*nn
 };
 template <int STAGE, class T>
 __global__ void k_stage_rk(NodeRkArgs<T> a, SpecRkArgs b, Scalars *__restrict__ s, Consts c,
@@ -1204,19 +1278,25 @@ __global__ void k_stage_rk(NodeRkArgs<T> a, SpecRkArgs b, Scalars *__restrict__ 
   CASL_PDL_ENTRY();
   // the half-step time advance that opens stages 2 and 4 (nothing reads t
   // in between)
-  if ((STAGE == 1 || STAGE == 3) && blockIdx.x == 0 && threadIdx.x == 0) s->t = s->t + s->dt2;
+  if ((STAGE == 1 || STAGE == 3) && blockIdx.x == 0)
+    for (int m = threadIdx.x; m < a.M; m += blockDim.x) s[m].t = s[m].t + s[m].dt2;
   if ((int)blockIdx.x < nbn)
-    nodes_rk_body<STAGE, T>(blockIdx.x, nbn, a.xq, a.yq, a.xqi, a.yqi, a.xqf, a.yqf, a.uu, a.vv, s, c);
+    nodes_rk_body<STAGE, T>(blockIdx.x, nbn, a.xq, a.yq, a.xqi, a.yqi, a.xqf, a.yqf, a.uu, a.vv, s, c,
+                            a.mnode, a.M);
   else
     spec_rk_body<STAGE>(blockIdx.x - nbn, gridDim.x - nbn, b.qs, b.qd, b.qsi, b.qsf, b.qdi,
-                        b.qdf, b.sqs, b.sqd, b.emq, s, b.nn);
+                        b.qdf, b.sqs, b.sqd, b.emq, s, b.nn, b.tot);
 }
 
 
-__global__ void k_twist_sub(Scalars *s, double twistmax) {
-  CASL_PDL_ENTRY(); s->twist = s->twist - twistmax; }
-__global__ void k_twist_zero(Scalars *s) {
-  CASL_PDL_ENTRY(); s->twist = 0.0; }
+__global__ void k_twist_sub(Scalars *s, double twistmax, int M) {
+  CASL_PDL_ENTRY();
+  for (int m = threadIdx.x; m < M; m += blockDim.x) s[m].twist = s[m].twist - twistmax;
+}
+__global__ void k_twist_zero(Scalars *s, int M) {
+  CASL_PDL_ENTRY();
+  for (int m = threadIdx.x; m < M; m += blockDim.x) s[m].twist = 0.0;
+}
 
 // ---------------------------------------------------------------------------
 // Stages
@@ -1224,8 +1304,9 @@ __global__ void k_twist_zero(Scalars *s) {
 // con2grid + the filter combination that forms qq and pp (evolution.f90:507-514)
 static int inversion_qq(casl_handle *h, bool reset) {
   long long nn = (long long)h->n * h->n;
+  const int M = h->M;  // ensemble members: one transform batch entry each
   if (h->nptq == 0) {
-    CASL_CUDA_TRY(cudaMemsetAsync(h->qc, 0, nn * sizeof(double), h->stream));
+    CASL_CUDA_TRY(cudaMemsetAsync(h->qc, 0, M * nn * sizeof(double), h->stream));
   } else {
     // con2grid, then its forward transform
     int rc = con2grid_dev(h, false);
@@ -1233,21 +1314,21 @@ static int inversion_qq(casl_handle *h, bool reset) {
     long long n = h->n;
     LoadQC ld{h->coarseC, h->scal, h->c.beffect ? h->betac : nullptr, nn,
               1.0 / (256.0 * (double)n * (double)n), (int)n};
-    rc = RFFT_DISPATCH(true, false, true, ld, (StoreStrided{h->qc, nn, 1, n}), 1);
+    rc = RFFT_DISPATCH(true, false, true, ld, (StoreStrided{h->qc, nn, 1, n}), M);
     if (rc) return rc;
     // The combination runs as its own elementwise pass: inside the batch-1
     // transform's store (about 3.5 warps per SM) its extra loads were
     // exposed and the fused pass took longer than the two apart.
     rc = RFFT_DISPATCH(true, false, false, (LoadStrided{h->qc, nn, n, 1}),
-                       (StoreStrided{h->qc, nn, n, 1}), 1);
+                       (StoreStrided{h->qc, nn, n, 1}), M);
     if (rc) return rc;
   }
   if (reset)
-    CASL_K(k_combine<true>, grid_for(nn), 256, 0, h->stream)(h->qs, h->qd, h->qc, h->qq, h->pp,
-                                                          h->flo, h->fhi, h->green, nn);
+    CASL_K(k_combine<true>, grid_for(M * nn), 256, 0, h->stream)(
+        h->qs, h->qd, h->qc, h->qq, h->pp, h->flo, h->fhi, h->green, nn, M * nn);
   else
-    CASL_K(k_combine<false>, grid_for(nn), 256, 0, h->stream)(h->qs, h->qd, h->qc, h->qq, h->pp,
-                                                           h->flo, h->fhi, h->green, nn);
+    CASL_K(k_combine<false>, grid_for(M * nn), 256, 0, h->stream)(
+        h->qs, h->qd, h->qc, h->qq, h->pp, h->flo, h->fhi, h->green, nn, M * nn);
   return check_launch(h);
 }
 
@@ -1261,16 +1342,22 @@ static int main_invert_dev(casl_handle *h) {
   ld.dir[0] = 0; ld.dir[1] = 1;
   ld.wg[0] = 1; ld.wg[1] = 1;
   ld.green = h->green; ld.hrkx = h->hrkx; ld.hrky = h->hrky; ld.n = h->n;
+  ld.nb = 2; ld.ms = nn;  // ensemble: two entries per member
   long long n = h->n;
-  rc = RFFT_DISPATCH(false, false, false, ld, (StoreStrided{h->w[0], nn, n, 1}), 2);
+  const int M = h->M;
+  // intermediate of entry b at w[0] + b*nn (2M contiguous fields: w[0..1]
+  // are 2M fields long)
+  rc = RFFT_DISPATCH(false, false, false, ld, (StoreStrided{h->w[0], nn, n, 1}), 2 * M);
   if (rc) return rc;
   StoreScaled st{};
   st.p[0] = h->vv; st.p[1] = h->uu;
   st.scale[0] = 1.0; st.scale[1] = -1.0; st.n = h->n;
+  st.nb = 2; st.ms = nn;
   // second pass reads tmp[ky*n + ix] (v = ix fastest, j = ky) and writes phys [ix][iy]
   LoadBatch lb{};
   lb.p[0] = h->w[0]; lb.p[1] = h->w[0] + nn; lb.vs = 1; lb.es = n;
-  return RFFT_DISPATCH(false, true, false, lb, st, 2);
+  lb.nb = 2; lb.ms = 2 * nn;
+  return RFFT_DISPATCH(false, true, false, lb, st, 2 * M);
 }
 
 // main_invert and the four gradients of source (evolution.f90:432-490,
@@ -1281,6 +1368,7 @@ static int main_invert_dev(casl_handle *h) {
 // gtmp (6 fields).
 static int invert_and_gradients(casl_handle *h) {
   long long nn = (long long)h->n * h->n, n = h->n;
+  const int M = h->M;  // ensemble: six entries per member
   LoadDeriv ld{};
   const double *src[6] = {h->qq, h->qq, h->qd, h->qd, h->qs, h->qs};
   for (int b = 0; b < 6; b++) {
@@ -1289,12 +1377,14 @@ static int invert_and_gradients(casl_handle *h) {
     ld.wg[b] = b < 2;
   }
   ld.green = h->green; ld.hrkx = h->hrkx; ld.hrky = h->hrky; ld.n = h->n;
-  double *tmp = h->gtmp;  // 6 contiguous fields
-  int rc = RFFT_DISPATCH(false, false, false, ld, (StoreStrided{tmp, nn, n, 1}), 6);
+  ld.nb = 6; ld.ms = nn;
+  double *tmp = h->gtmp;  // 6M contiguous fields
+  int rc = RFFT_DISPATCH(false, false, false, ld, (StoreStrided{tmp, nn, n, 1}), 6 * M);
   if (rc) return rc;
   LoadBatch lb{};
   for (int b = 0; b < 6; b++) lb.p[b] = tmp + b * nn;
   lb.vs = 1; lb.es = n;
+  lb.nb = 6; lb.ms = 6 * nn;
   StoreScaled st{};
   double *dst[6] = {h->vv, h->uu, h->w[4], h->w[5], h->sqs, h->sqd};
   for (int b = 0; b < 6; b++) {
@@ -1302,7 +1392,8 @@ static int invert_and_gradients(casl_handle *h) {
     st.scale[b] = b == 1 ? -1.0 : 1.0;
   }
   st.n = h->n;
-  return RFFT_DISPATCH(false, true, false, lb, st, 6);
+  st.nb = 6; st.ms = nn;
+  return RFFT_DISPATCH(false, true, false, lb, st, 6 * M);
 }
 
 // The same batch-6 inverse pair with FP32 storage (CASL_PREC_FP32_INVERSION):
@@ -1344,20 +1435,23 @@ int inversion_dev(casl_handle *h, bool reset) {
 
 static int adapt_dev(casl_handle *h) {
   long long nn = (long long)h->n * h->n, n = h->n;
+  const int M = h->M;  // ensemble: one entry, one reduction and one dt per member
   LoadVort lv{h->qq, h->pp, h->c.kdsq, h->c.btropic, h->n};
-  int rc = RFFT_DISPATCH(false, false, false, lv, (StoreStrided{h->w[0], nn, n, 1}), 1);
+  lv.ms = nn;
+  int rc = RFFT_DISPATCH(false, false, false, lv, (StoreStrided{h->w[0], nn, n, 1}), M);
   if (rc) return rc;
   rc = RFFT_DISPATCH(false, true, false, (LoadStrided{h->w[0], nn, 1, n}),
-                     (StoreStrided{h->w[1], nn, n, 1}), 1);
+                     (StoreStrided{h->w[1], nn, n, 1}), M);
   if (rc) return rc;
   if (h->prec == CASL_PREC_FP32_INVERSION)
     CASL_K(k_reduce_adapt<float>, RED_BLOCKS, 256, 0, h->stream)(h->w[1], h->f32, h->f32 + nn,
                                                                  h->part, nn);
   else
-    CASL_K(k_reduce_adapt<double>, RED_BLOCKS, 256, 0, h->stream)(h->w[1], h->uu, h->vv, h->part,
-                                                                  nn);
-  CASL_K(k_adapt_final, 1, 256, 0, h->stream)(h->part, RED_BLOCKS, h->scal, h->c, h->p.fixed_dt);
-  CASL_K(k_epq, grid_for(nn), 256, 0, h->stream)(h->qdiss, h->epq, h->emq, h->scal, nn);
+    CASL_K(k_reduce_adapt<double>, dim3(RED_BLOCKS, M), 256, 0, h->stream)(h->w[1], h->uu, h->vv,
+                                                                           h->part, nn);
+  CASL_K(k_adapt_final, M, 256, 0, h->stream)(h->part, RED_BLOCKS, h->scal, h->c, h->p.fixed_dt);
+  CASL_K(k_epq, grid_for(M * nn), 256, 0, h->stream)(h->qdiss, h->epq, h->emq, h->scal, nn,
+                                                     M * nn);
   return check_launch(h);
 }
 
@@ -1386,14 +1480,17 @@ static int source_prod(casl_handle *h, int stage) {
     la.fx[1] = h->sqs; la.fy[1] = h->sqd;
     la.betab[0] = 0.0; la.betab[1] = h->c.beffect ? h->c.beta : 0.0;
     la.n = h->n;
-    rc = RFFT_DISPATCH(true, false, true, la, (StoreStrided{tmp, nn, 1, n}), 2);
+    la.ms = nn;
+    // ensemble: two entries per member; tmp (w[0..1]) is 2M fields long
+    rc = RFFT_DISPATCH(true, false, true, la, (StoreStrided{tmp, nn, 1, n}), 2 * h->M);
   }
   if (rc) return rc;
   StoreSource ss{};
   ss.sqd = h->sqd; ss.sqs = h->sqs; ss.qq = h->qq; ss.pp = h->pp; ss.epq = h->epq;
   ss.rekman = h->p.rekman; ss.kdsq = h->c.kdsq; ss.therm = h->c.therm;
   ss.heating = h->c.heating; ss.friction = h->c.friction; ss.lev = lev; ss.n = h->n;
-  return RFFT_DISPATCH(true, false, false, (LoadStrided{tmp, nn, n, 1}), ss, 2);
+  ss.ms = nn;
+  return RFFT_DISPATCH(true, false, false, (LoadStrided{tmp, nn, n, 1}), ss, 2 * h->M);
 }
 
 }  // namespace casl
@@ -1402,11 +1499,13 @@ static int source_prod(casl_handle *h, int stage) {
 // the velocity fields u, v (FP64, or FP32 in the FP32-inversion mode)
 template <class T>
 static int stage_update(casl_handle *h, int stage, const T *u, const T *v) {
-  const long long nn = (long long)h->n * h->n;
+  const long long nn = (long long)h->n * h->n, tot = h->M * nn;
   const int nbn = h->contex ? grid_for(h->nptq > 0 ? h->nptq : 1) : 0;
-  const int g = nbn + grid_for(nn / 2);
-  const NodeRkArgs<T> a{h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, u, v};
-  const SpecRkArgs b{h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs, h->sqd, h->emq, nn};
+  const int g = nbn + grid_for(tot / 2);
+  const NodeRkArgs<T> a{h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, u, v,
+                        h->M > 1 ? h->mnode : nullptr, h->M};
+  const SpecRkArgs b{h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs, h->sqd, h->emq,
+                     nn, tot};
   cudaStream_t st = h->stream;
   switch (stage) {
     case 1: CASL_K((k_stage_rk<1, T>), g, 256, 0, st)(a, b, h->scal, h->c, nbn); break;
@@ -1944,41 +2043,61 @@ int casl_last_cuda_error(casl_handle *h) { return h ? h->last_cuda : 0; }
 static int alloc_all(casl_handle *h) {
   long long n = h->n, nn = n * n;
   long long npm = h->npm, nm = h->nm;
+  const long long M = h->M;
   double **nodes[] = {&h->xq, &h->yq, &h->xqi, &h->yqi, &h->xqf, &h->yqf, &h->uq, &h->vq};
   for (auto pp : nodes) CASL_CUDA_TRY(cudaMalloc(pp, (size_t)npm * sizeof(double)));
   CASL_CUDA_TRY(cudaMalloc(&h->nextq, (size_t)npm * sizeof(int)));
   int **cont[] = {&h->i1q, &h->i2q, &h->npq, &h->indq};
   for (auto pp : cont) CASL_CUDA_TRY(cudaMalloc(pp, (size_t)nm * sizeof(int)));
+  // per-member fields (M stacked), then the shared tables
   double **fields[] = {&h->qr, &h->qs, &h->qd, &h->qc, &h->qq, &h->pp, &h->uu, &h->vv, &h->emq,
-                       &h->epq, &h->qspre, &h->sqs, &h->sqd, &h->qsi, &h->qsf, &h->qdi, &h->qdf,
-                       &h->green, &h->flo, &h->fhi, &h->qdiss};
+                       &h->epq, &h->qspre, &h->sqs, &h->sqd, &h->qsi, &h->qsf, &h->qdi, &h->qdf};
   for (auto pp : fields) {
+    CASL_CUDA_TRY(cudaMalloc(pp, (size_t)(M * nn) * sizeof(double)));
+    CASL_CUDA_TRY(cudaMemset(*pp, 0, (size_t)(M * nn) * sizeof(double)));
+  }
+  double **tables[] = {&h->green, &h->flo, &h->fhi, &h->qdiss};
+  for (auto pp : tables) {
     CASL_CUDA_TRY(cudaMalloc(pp, (size_t)nn * sizeof(double)));
     CASL_CUDA_TRY(cudaMemset(*pp, 0, (size_t)nn * sizeof(double)));
   }
-  // work fields: w[0..3] contiguous (batched transforms), w[4], w[5]
+  // work fields: w[0..3] contiguous (batched transforms), w[4], w[5]; each
+  // M fields wide
   double *wk;
-  CASL_CUDA_TRY(cudaMalloc(&wk, (size_t)6 * nn * sizeof(double)));
-  for (int i = 0; i < 6; i++) h->w[i] = wk + i * nn;
+  CASL_CUDA_TRY(cudaMalloc(&wk, (size_t)(6 * M * nn) * sizeof(double)));
+  for (int i = 0; i < 6; i++) h->w[i] = wk + i * M * nn;
   CASL_CUDA_TRY(cudaMalloc(&h->hrkx, n * sizeof(double)));
   CASL_CUDA_TRY(cudaMalloc(&h->hrky, n * sizeof(double)));
   CASL_CUDA_TRY(cudaMalloc(&h->bety, n * sizeof(double)));
   CASL_CUDA_TRY(cudaMalloc(&h->betac, n * sizeof(double)));
   CASL_CUDA_TRY(cudaMalloc(&h->tw, n * sizeof(double2)));
-  CASL_CUDA_TRY(cudaMalloc(&h->gtmp, (size_t)6 * nn * sizeof(double)));
+  CASL_CUDA_TRY(cudaMalloc(&h->gtmp, (size_t)(6 * M * nn) * sizeof(double)));
   CASL_CUDA_TRY(cudaMalloc(&h->shell_idx, (size_t)nn * sizeof(int)));
   CASL_CUDA_TRY(cudaMalloc(&h->shell_off, (size_t)(2 * n + 2) * sizeof(int)));
   CASL_CUDA_TRY(cudaMalloc(&h->rkxf, n * sizeof(double)));
   CASL_CUDA_TRY(cudaMalloc(&h->rkyf, n * sizeof(double)));
-  size_t fine = (size_t)h->c.nxf * h->c.nyf;
+  // one simulation: the dense (4n)^2 levels grid (the packed words use its
+  // first half); an ensemble: the packed words of every member (4n x n
+  // 64-bit words = 8 n^2 ints each)
+  size_t fine = M == 1 ? (size_t)h->c.nxf * h->c.nyf : (size_t)(M * 8 * nn);
   CASL_CUDA_TRY(cudaMalloc(&h->fineJ, fine * sizeof(int)));
-  CASL_CUDA_TRY(cudaMalloc(&h->ljx, (size_t)h->c.nxf * sizeof(int)));
-  CASL_CUDA_TRY(cudaMalloc(&h->coarseC, (size_t)nn * sizeof(int)));
-  CASL_CUDA_TRY(cudaMalloc(&h->part, 3 * RED_BLOCKS * sizeof(double)));
-  CASL_CUDA_TRY(cudaMalloc(&h->scal, sizeof(Scalars)));
-  CASL_CUDA_TRY(cudaMemset(h->scal, 0, sizeof(Scalars)));
-  CASL_CUDA_TRY(cudaMallocHost(&h->hscal, sizeof(Scalars)));
-  memset(h->hscal, 0, sizeof(Scalars));
+  CASL_CUDA_TRY(cudaMalloc(&h->ljx, (size_t)(M * h->c.nxf) * sizeof(int)));
+  CASL_CUDA_TRY(cudaMalloc(&h->coarseC, (size_t)(M * nn) * sizeof(int)));
+  CASL_CUDA_TRY(cudaMalloc(&h->part, (size_t)(3 * RED_BLOCKS * M) * sizeof(double)));
+  CASL_CUDA_TRY(cudaMalloc(&h->scal, (size_t)M * sizeof(Scalars)));
+  CASL_CUDA_TRY(cudaMemset(h->scal, 0, (size_t)M * sizeof(Scalars)));
+  CASL_CUDA_TRY(cudaMallocHost(&h->hscal, (size_t)M * sizeof(Scalars)));
+  memset(h->hscal, 0, (size_t)M * sizeof(Scalars));
+  CASL_CUDA_TRY(cudaMalloc(&h->mnode, (size_t)(M + 1) * sizeof(int)));
+  CASL_CUDA_TRY(cudaMalloc(&h->mcont, (size_t)(M + 1) * sizeof(int)));
+  CASL_CUDA_TRY(cudaMemset(h->mnode, 0, (size_t)(M + 1) * sizeof(int)));
+  CASL_CUDA_TRY(cudaMemset(h->mcont, 0, (size_t)(M + 1) * sizeof(int)));
+  CASL_CUDA_TRY(cudaMallocHost(&h->hmnode, (size_t)(M + 1) * sizeof(int)));
+  CASL_CUDA_TRY(cudaMallocHost(&h->hmcont, (size_t)(M + 1) * sizeof(int)));
+  memset(h->hmnode, 0, (size_t)(M + 1) * sizeof(int));
+  memset(h->hmcont, 0, (size_t)(M + 1) * sizeof(int));
+  h->mqjump = (double *)calloc((size_t)M, sizeof(double));
+  if (!h->mqjump) return CASL_ENOMEM;
   return CASL_OK;
 }
 
@@ -1991,13 +2110,25 @@ static void free_all(casl_handle *h) {
                   h->sx, h->sx2, h->shell_idx, h->shell_off, h->rkxf, h->rkyf, h->gtmp};
   for (void *p : ptrs)
     if (p) cudaFree(p);
+  if (h->mnode) cudaFree(h->mnode);
+  if (h->mcont) cudaFree(h->mcont);
+  if (h->hmnode) cudaFreeHost(h->hmnode);
+  if (h->hmcont) cudaFreeHost(h->hmcont);
+  free(h->mqjump);
   free(h->spmf_h);
   free(h->alk_h);
   if (h->hscal) cudaFreeHost(h->hscal);
 }
 
 int casl_create(const casl_params *p, int device, casl_handle **out) {
-  if (!p || !out) return CASL_EINVAL;
+  return casl::create_handle_members(p, device, 1, out);
+}
+
+}  // extern "C"
+
+// A handle of M ensemble members (M = 1: one simulation).
+int casl::create_handle_members(const casl_params *p, int device, int M, casl_handle **out) {
+  if (!p || !out || M < 1) return CASL_EINVAL;
   *out = nullptr;
   int n = p->nx;
   if (p->nx != p->ny || n < 32 || n > 2048 || (n & (n - 1)) || p->ellx <= 0 || p->elly <= 0 ||
@@ -2012,6 +2143,7 @@ int casl_create(const casl_params *p, int device, casl_handle **out) {
   if (h->p.nregmax <= 0) h->p.nregmax = 20;
   if (h->p.twistmax <= 0) h->p.twistmax = 2.5;
   h->n = n;
+  h->M = M;
   h->npm = h->p.npm;
   h->nm = h->p.nm;
   h->device = device;
@@ -2063,11 +2195,13 @@ int casl_create(const casl_params *p, int device, casl_handle **out) {
     free(h);
     return CASL_ECUDA;
   }
-  h->hscal->dtmax = h->p.dtmax > 0 ? h->p.dtmax : 1.0e30;
-  cudaMemcpy(h->scal, h->hscal, sizeof(Scalars), cudaMemcpyHostToDevice);
+  for (int m = 0; m < M; m++) h->hscal[m].dtmax = h->p.dtmax > 0 ? h->p.dtmax : 1.0e30;
+  cudaMemcpy(h->scal, h->hscal, (size_t)M * sizeof(Scalars), cudaMemcpyHostToDevice);
   *out = h;
   return CASL_OK;
 }
+
+extern "C" {
 
 void casl_destroy(casl_handle *h) {
   if (!h) return;
@@ -2076,6 +2210,7 @@ void casl_destroy(casl_handle *h) {
   cudaStreamSynchronize(h->stream);
   closure_release(h);
   forcing_release(h);
+  ensemble_release(h);
   cudaFree(h->f32);
   free_all(h);
   if (h->prof_ev) {
@@ -2477,22 +2612,23 @@ int casl_recontour(casl_handle *h, const double *qq) {
 }
 
 // init (evolution.f90:96-131)
+// (tot = M*nn over an ensemble's members; the tables are shared)
 __global__ void k_evo_init(double *qd, double *qspre, const double *qs, const double *qc,
-                           const double *fhi, long long nn) {
+                           const double *fhi, long long nn, long long tot) {
   CASL_PDL_ENTRY();
-  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nn;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < tot;
        k += (long long)gridDim.x * blockDim.x) {
-    qd[k] = fhi[k] * (qs[k] - qc[k]);
+    qd[k] = fhi[k & (nn - 1)] * (qs[k] - qc[k]);
     qspre[k] = qs[k];
   }
 }
 // prepare (evolution.f90:135-162), spectral part
 __global__ void k_prepare(double *qs, double *qd, const double *qc, const double *flo,
-                          long long nn) {
+                          long long nn, long long tot) {
   CASL_PDL_ENTRY();
-  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nn;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < tot;
        k += (long long)gridDim.x * blockDim.x) {
-    double s = flo[k] * (qs[k] - qc[k]) + qc[k] + qd[k];
+    double s = flo[k & (nn - 1)] * (qs[k] - qc[k]) + qc[k] + qd[k];
     qs[k] = s;
     qd[k] = s - qc[k];
   }
@@ -2506,7 +2642,8 @@ int evo_init(casl_handle *h) {
   h->contex = h->nptq > 0;
   int rc = con2grid_to_spec(h, h->qc);
   if (rc) return rc;
-  CASL_K(k_evo_init, grid_for(nn), 256, 0, h->stream)(h->qd, h->qspre, h->qs, h->qc, h->fhi, nn);
+  CASL_K(k_evo_init, grid_for(h->M * nn), 256, 0, h->stream)(h->qd, h->qspre, h->qs, h->qc,
+                                                             h->fhi, nn, h->M * nn);
   return check_launch(h);
 }
 }  // namespace casl
@@ -2517,9 +2654,10 @@ static int evo_prepare(casl_handle *h) {
   long long nn = (long long)h->n * h->n;
   int rc = con2grid_to_spec(h, h->qc);
   if (rc) return rc;
-  CASL_K(k_prepare, grid_for(nn), 256, 0, h->stream)(h->qs, h->qd, h->qc, h->flo, nn);
+  CASL_K(k_prepare, grid_for(h->M * nn), 256, 0, h->stream)(h->qs, h->qd, h->qc, h->flo, nn,
+                                                            h->M * nn);
   if ((rc = check_launch(h))) return rc;
-  return spctop_dev(h, h->qd, h->qr, h->w[0]);
+  return spctop_dev(h, h->qd, h->qr, h->w[0], h->M);
 }
 
 __global__ void k_sub_bety(double *q, const double *bety, int n) {
@@ -2612,21 +2750,24 @@ int casl_step(casl_handle *h, int nsteps) {
     if (reg) {
       h->ireg++;
       if (h->ireg == h->p.nregmax) {
-        // prepare + recontour + init (evolution.f90:62-66; caps.f90:83-91)
+        // prepare + recontour + init (evolution.f90:62-66; caps.f90:83-91);
+        // an ensemble recontours member by member
         if ((rc = evo_prepare(h))) return rc;
-        if ((rc = recontour_dev(h, h->qr))) return rc;
+        if ((rc = h->M > 1 ? ensemble_recontour(h) : recontour_dev(h, h->qr))) return rc;
         if ((rc = sync_counts(h))) return rc;
         if ((rc = evo_init(h))) return rc;
-        CASL_K(k_twist_zero, 1, 1, 0, h->stream)(h->scal);
+        CASL_K(k_twist_zero, 1, 256, 0, h->stream)(h->scal, h->M);
         h->ireg = 0;
         if (force) {
           h->ireg = 1;
           if ((rc = surgery_dev(h))) return rc;
-          CASL_K(k_twist_sub, 1, 1, 0, h->stream)(h->scal, h->p.twistmax);
+          if (h->M > 1 && (rc = member_ranges(h))) return rc;
+          CASL_K(k_twist_sub, 1, 256, 0, h->stream)(h->scal, h->p.twistmax, h->M);
         }
       } else {
         if ((rc = surgery_dev(h))) return rc;
-        CASL_K(k_twist_sub, 1, 1, 0, h->stream)(h->scal, h->p.twistmax);
+        if (h->M > 1 && (rc = member_ranges(h))) return rc;
+        CASL_K(k_twist_sub, 1, 256, 0, h->stream)(h->scal, h->p.twistmax, h->M);
       }
     }
     if (h->closure && (rc = closure_step_check(h))) return rc;

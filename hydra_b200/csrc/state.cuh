@@ -80,7 +80,22 @@ struct casl_handle {
   int uv_fp32;           // the latest stage velocity exists only in f32 (uu, vv stale)
 
   casl::ForcingState *forcing;  // nb_forcing tables (nullable)
+
+  // Ensemble of M independent members (casl_ensemble_create; M = 1 for one
+  // simulation).  Members share the grid size and parameters; their fields
+  // are stacked (member m's field at offset m*n*n), their contours
+  // concatenated member after member with member m's levels offset by
+  // m*CASL_LSTRIDE, and scal holds one Scalars per member (member 0's also
+  // carries the total counts and the error word).
+  int M;
+  int *mnode;            // device, M+1: first node of each member (mnode[M] = nptq)
+  int *mcont;            // device, M+1: first contour of each member
+  int *hmnode, *hmcont;  // pinned host copies
+  double *mqjump;        // host, M: each member's qjump
+  casl_handle *view;     // one-member view used to recontour each member in turn
 };
+#define CASL_LSTRIDE (1 << 20)   // level offset between ensemble members
+#define CASL_LBIAS (1 << 19)     // |level| < CASL_LBIAS within a member
 
 #define CASL_PROF_MAX 8192
 
@@ -91,9 +106,9 @@ int check_launch(casl_handle *h);
 
 // Spectral transforms on device buffers (in/out may alias only where noted).
 // ptospc: phys (n*n, [ix][iy]) -> spec ([ky][kx]); spec must not alias phys.
-int ptospc_dev(casl_handle *h, const double *phys, double *spec);
+int ptospc_dev(casl_handle *h, const double *phys, double *spec, int batch = 1);
 // spctop: spec -> phys using tmp (n*n); spec is preserved.
-int spctop_dev(casl_handle *h, const double *spec, double *phys, double *tmp);
+int spctop_dev(casl_handle *h, const double *spec, double *phys, double *tmp, int batch = 1);
 
 int con2grid_dev(casl_handle *h, bool want_levels);  // -> coarseC, scal->csum
 int con2grid_to_spec(casl_handle *h, double *spec); // con2grid + ptospc fused load
@@ -144,5 +159,12 @@ int closure_stage32(casl_handle *h, const float **u, const float **v);  // FP32-
 int closure_step_check(casl_handle *h);
 void closure_release(casl_handle *h);
 void forcing_release(casl_handle *h);  // forcing.cu
+// Ensembles (ensemble.cu): handle creation with M members, each member's
+// node and contour ranges (mnode, mcont) from the level offsets, the
+// member-by-member recontouring, and the view's release.
+int create_handle_members(const casl_params *p, int device, int M, casl_handle **out);
+int member_ranges(casl_handle *h);
+int ensemble_recontour(casl_handle *h);
+void ensemble_release(casl_handle *h);
 
 }  // namespace casl

@@ -187,6 +187,29 @@ int casl_nb_forcing_init(casl_handle *h, double kfmid, double fwid, double famp,
  * values of myrand (2*rand()-1) in the reference's order. */
 int casl_nb_forcing(casl_handle *h, double dt, const double *rnd);
 
+/* ---- batched ensembles (no counterpart in the reference) ------------------ */
+/* M independent simulations of one grid size and parameter set in one
+ * handle, stepped together by casl_step: every stage of the RK4 advance, the
+ * surgery and the renode run as single launches over all members (each
+ * member keeps its own dt, qjump and scalars, as M separate runs of the
+ * reference would); recontouring runs member by member.  force_surgery is
+ * set (every member regularises every step, so all members recontour at the
+ * same step).  Members' contours are stored one member after another with
+ * member m's levels offset by m*2^20 (casl_get_contours returns that raw
+ * form; casl_ensemble_member_contours one member in its own numbering).
+ * The closure and the FP32-inversion mode serve single simulations only. */
+int casl_ensemble_create(const casl_params *p, int members, int device, casl_handle **out);
+int casl_ensemble_members(casl_handle *h, int *members);
+/* initialise (caps.f90:106-361) of every member: q_all holds the M initial
+ * fields (ny,nx) one after another; ncontq (nullable) each member's number
+ * of PV jumps. */
+int casl_ensemble_initialise(casl_handle *h, const double *q_all, const int *ncontq);
+int casl_ensemble_member_counts(casl_handle *h, int m, int *nq, int *nptq, double *qjump);
+int casl_ensemble_member_contours(casl_handle *h, int m, double *xq, double *yq, int *nextq,
+                                  int *indq, int *npq, int *i1q, int *i2q);
+/* which: CASL_T, CASL_DT, CASL_TWIST, CASL_ZZRMS, CASL_ZZMAX, CASL_UUMAX, CASL_QJUMP */
+int casl_ensemble_member_scalar(casl_handle *h, int m, int which, double *value);
+
 /* Precision of the inversion inside casl_advance / casl_step.
  * CASL_PREC_FP64 (default): everything FP64, the parity mode.
  * CASL_PREC_FP32_INVERSION: the inverse transform pair of every RK4 stage

@@ -176,11 +176,18 @@ def test_zero_network_leaves_the_step_unchanged(oracle_mod, gpu_lib):
 
 def test_constant_correction_shifts_the_nodes(oracle_mod, gpu_lib):
     """Output bias (b0, b1) and zero weights: velint reads u + us*b0,
-    v + us*b1 at every stage, so one RK4 step moves every node by dt*us*b
-    more than the plain step does."""
+    v + us*b1 at every stage.  With qjump = 0 and qs = qd = 0 the flow
+    itself is zero, so the plain step leaves the nodes in place and one RK4
+    step of the corrected one moves every node by exactly dt*us*b."""
     from hydra_b200.casl import CaslNet
     n = 128
     a, b = _pair(oracle_mod, n, 4)
+    for g in (a, b):
+        c = g.contours()
+        c["qjump"] = 0.0
+        g.set_contours(c)
+        for f in ("qs", "qd"):
+            g.set_field(f, np.zeros((n, n)))
     p = np.zeros(co.param_count(), np.float32)
     p[-2:] = [0.5, -0.25]
     net = CaslNet(n)
@@ -194,8 +201,9 @@ def test_constant_correction_shifts_the_nodes(oracle_mod, gpu_lib):
     L = 2 * np.pi
     dx = (cb["xq"] - ca["xq"] + np.pi) % L - np.pi
     dy = (cb["yq"] - ca["yq"] + np.pi) % L - np.pi
-    assert np.abs(dx - dt * 2.0 * 0.5).max() <= 1e-9
-    assert np.abs(dy - dt * 2.0 * (-0.25)).max() <= 1e-9
+    assert dt > 0.0
+    assert np.abs(dx - dt * 2.0 * 0.5).max() <= 1e-12
+    assert np.abs(dy - dt * 2.0 * (-0.25)).max() <= 1e-12
     net.close(); a.close(); b.close()
 
 

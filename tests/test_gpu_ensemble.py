@@ -1,0 +1,85 @@
+"""Batched ensembles: M members of uneven size stepped together in one handle
+(one launch per stage across members) against the same members run one by
+one, and one member against the oracle.
+
+Members differ in k0 and level count, so their node counts and qjump
+differ.  25 forced-surgery steps take every member through surgery, renode,
+a recontouring (step 20) and more surgery.  Per member the batched run must
+keep the separate run's node and contour counts at every step and end with
+identical topology; node positions agree to the rounding of the renode
+density sums, which run as segmented scans over the whole ensemble (another
+grouping than over one member), so they are compared at 1e-8 of the domain
+as the driver test compares the oracle.
+"""
+import numpy as np
+import pytest
+
+from hydra_b200.synthetic import random_pv
+
+pytestmark = pytest.mark.gpu
+
+MEMBERS = [(4.0, 12), (6.0, 20), (9.0, 28)]  # (k0, ncontq) per member
+
+
+def same_topology(a, b):
+    assert (a["nq"], a["nptq"]) == (b["nq"], b["nptq"])
+    for k in ("npq", "i1q", "i2q", "indq", "nextq"):
+        assert np.array_equal(a[k], b[k]), k
+
+
+def test_ensemble_matches_separate_runs(oracle_mod, gpu_lib):
+    from hydra_b200.casl import CaslEnsemble, CaslGPU
+    n, steps = 64, 25
+    fields = [random_pv(n, k0, 10 + m) for m, (k0, _) in enumerate(MEMBERS)]
+    levels = [lv for _, lv in MEMBERS]
+    e = CaslEnsemble(n, len(MEMBERS), dtmax=0.05, nregmax=20)
+    e.initialise_members(fields, levels)
+    singles = []
+    for f, lv in zip(fields, levels):
+        g = CaslGPU(n, ncontq=lv, force_surgery=1, dtmax=0.05, nregmax=20)
+        g.initialise(f)
+        singles.append(g)
+    for m, g in enumerate(singles):
+        same_topology(e.member_contours(m), g.contours())
+        assert e.member_counts(m)[2] == g.counts()[2]  # qjump
+    sizes = [g.counts()[1] for g in singles]
+    assert len(set(sizes)) == len(sizes)  # uneven members
+    for step in range(steps):
+        e.step(1)
+        for m, g in enumerate(singles):
+            g.step(1)
+            assert e.member_counts(m)[:2] == g.counts()[:2], (step, m)
+    for m, g in enumerate(singles):
+        a, b = e.member_contours(m), g.contours()
+        same_topology(a, b)
+        assert np.abs(a["xq"] - b["xq"]).max() <= 1e-8 * np.pi
+        assert np.abs(a["yq"] - b["yq"]).max() <= 1e-8 * np.pi
+        assert abs(e.member_scalar(m, "t") - g.scalar("t")) <= 1e-12
+        g.close()
+    # one member against the oracle over the same steps
+    o = oracle_mod.Oracle(n, ncontq=levels[1], force_surgery=1, dtmax=0.05, nregmax=20)
+    o.initialise(fields[1])
+    for _ in range(steps):
+        o.step()
+    a, b = e.member_contours(1), o.contours()
+    same_topology(a, b)
+    assert np.abs(a["xq"] - b["xq"]).max() <= 1e-8 * np.pi
+    o.close()
+    e.close()
+
+
+def test_ensemble_of_one_is_the_single_run(gpu_lib):
+    """M = 1 through the ensemble entry points is the plain handle."""
+    from hydra_b200.casl import CaslEnsemble, CaslGPU
+    n = 64
+    f = random_pv(n, 6.0, 3)
+    e = CaslEnsemble(n, 1, ncontq=20, dtmax=0.05)
+    e.initialise_members([f], [20])
+    g = CaslGPU(n, ncontq=20, force_surgery=1, dtmax=0.05)
+    g.initialise(f)
+    e.step(3)
+    g.step(3)
+    a, b = e.member_contours(0), g.contours()
+    same_topology(a, b)
+    assert np.array_equal(a["xq"], b["xq"]) and np.array_equal(a["yq"], b["yq"])
+    e.close(); g.close()

@@ -55,7 +55,7 @@ def thin(c):
 def test_capacity_on_upload(gpu_lib, state):
     from hydra_b200.casl import CaslError, CaslGPU
     n, c = state
-    g = CaslGPU(n, ncontq=20, npm=c["nptq"] - 1)
+    g = CaslGPU(n, ncontq=20, npm=c["nptq"] - 1, nm=10_000)
     with pytest.raises(CaslError) as e:
         g.set_contours(c)
     assert e.value.code == CASL_ECAPACITY
@@ -66,7 +66,7 @@ def test_capacity_on_renode_growth(gpu_lib, state):
     from hydra_b200.casl import CaslError, CaslGPU
     n, c = state
     t = thin(c)
-    g = CaslGPU(n, ncontq=20, npm=t["nptq"] + 16, force_surgery=1)
+    g = CaslGPU(n, ncontq=20, npm=t["nptq"] + 16, nm=10_000, force_surgery=1)
     g.set_contours(t)
     assert g.counts()[1] == t["nptq"]
     with pytest.raises(CaslError) as e:
@@ -74,7 +74,7 @@ def test_capacity_on_renode_growth(gpu_lib, state):
     assert e.value.code == CASL_ECAPACITY
     g.close()
     # the same state with room to grow renodes without error
-    g = CaslGPU(n, ncontq=20, npm=4 * c["nptq"], force_surgery=1)
+    g = CaslGPU(n, ncontq=20, npm=4 * c["nptq"], nm=10_000, force_surgery=1)
     g.set_contours(t)
     g.surgery()
     assert g.counts()[1] > t["nptq"] + 16
