@@ -305,6 +305,63 @@ def run_closure_leg(a, torch, device, steps=40, warmup=5, check_every=50):
 
 
 # ---------------------------------------------------------------------------
+# batched-ensemble leg (the batched half of the "chosen" form)
+# ---------------------------------------------------------------------------
+def run_ensemble_leg(a, torch, device, members=256, n=256, steps=20, warmup=3, singles=8):
+    """The batched ensemble configuration: `members` members of n^2 (seeds
+    0.., k0 uniform in [4, 12], 20-60 levels, as ensemble_member_params
+    draws them), surgery every step, recontouring every 20 regularisations,
+    all stepped together by one handle; beside it the same members advanced
+    one handle at a time (the plain form), on the first `singles` members.
+    Both timed with CUDA events on the library's stream."""
+    from hydra_b200.casl import CaslEnsemble, CaslGPU
+    from hydra_b200.synthetic import ensemble_member_params, random_pv
+    params = [ensemble_member_params(m) for m in range(members)]
+    fields = [random_pv(n, k0, m) for m, (k0, _) in enumerate(params)]
+    levels = [lv for _, lv in params]
+
+    def timed(g, k):
+        st = torch.cuda.ExternalStream(g.stream_ptr(), device=device)
+        torch.cuda.synchronize()
+        ns0 = g.scalar("node_steps")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        g.step(k)
+        e1.record(st)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), g.scalar("node_steps") - ns0
+
+    e = CaslEnsemble(n, members, dtmax=a.dtmax, nregmax=20, npm=80_000_000, nm=4_000_000,
+                     device=device)
+    t0 = time.perf_counter()
+    e.initialise_members(fields, levels)
+    t_init = time.perf_counter() - t0
+    e.step(warmup)
+    ms, ns = timed(e, steps)
+    sizes = [e.member_counts(m)[1] for m in range(members)]
+    e.close()
+    sms, sns = 0.0, 0.0
+    for m in range(singles):
+        g = CaslGPU(n, ncontq=levels[m], force_surgery=1, dtmax=a.dtmax, nregmax=20,
+                    npm=4_000_000, nm=250_000, device=device)
+        g.initialise(fields[m])
+        g.step(warmup)
+        x, y = timed(g, steps)
+        sms += x
+        sns += y
+        g.close()
+    return {"config": f"batched ensemble: {members} members of {n}^2, k0 ~ U[4,12], levels ~ "
+                      f"U[20,60], seeds 0..{members - 1}, surgery every step, recontour every 20 "
+                      f"regularisations; {steps} steps after {warmup} (one recontouring inside)",
+            "node_steps_per_s": ns / (ms * 1e-3), "ms_per_step": ms / steps,
+            "nodes_min": int(min(sizes)), "nodes_max": int(max(sizes)),
+            "nodes_total": int(sum(sizes)), "initialise_s": t_init,
+            "one_at_a_time": {"members_timed": singles, "node_steps_per_s": sns / (sms * 1e-3),
+                              "ms_per_member_step": sms / (singles * steps)},
+            "speedup_vs_one_at_a_time": (ns / ms) / (sns / sms) if sms > 0 else None}
+
+
+# ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
 def reduce_over_ranks(vals, world, device):
@@ -393,6 +450,9 @@ def run_gpu(a):
     closure = None
     if rank == 0 and world == 1 and not a.no_closure:
         closure = run_closure_leg(a, torch, local)
+    ensemble = None
+    if rank == 0 and world == 1 and not a.no_ensemble:
+        ensemble = run_ensemble_leg(a, torch, local)
 
     # ---- reduce over ranks ---------------------------------------------------------------
     ms_max, ns_sum, e2e_ms, e2e_ns = reduce_over_ranks(
@@ -429,6 +489,7 @@ def run_gpu(a):
                          "peak_source": f"{peak_kind} hbm_gbs"},
             "cpu_baseline": cpu,
             "closure": closure,
+            "ensemble": ensemble,
             "gpu_launches": launches,
             "clocks": clk,
         }
@@ -506,6 +567,7 @@ def main():
                     help="time budget of the cpu_baseline leg of the GPU arm")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-closure", action="store_true", help="skip the learned-closure leg")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble leg")
     a = ap.parse_args()
     if a.warmup < 3 and a.impl == "hydra":
         print("bench: at least 3 warm-up steps are required", file=sys.stderr)

@@ -2284,6 +2284,7 @@ int casl_set_contours(casl_handle *h, int nq, int nptq, double qjump, const doub
                       const double *yq, const int *nextq, const int *indq, const int *npq,
                       const int *i1q, const int *i2q) {
   if (!h || nq < 0 || nptq < 0) return CASL_EINVAL;
+  if (h->M > 1) return CASL_EUNSUPPORTED;  // ensembles: casl_ensemble_initialise
   if (nptq > h->npm || nq > h->nm) return CASL_ECAPACITY;
   if (nptq > 0 && (!xq || !yq || !nextq)) return CASL_EINVAL;
   if (nq > 0 && (!indq || !npq || !i1q || !i2q)) return CASL_EINVAL;
@@ -2479,6 +2480,7 @@ int casl_spctop(casl_handle *h, const double *svar, double *rvar) {
 }
 
 int casl_con2grid(casl_handle *h, double *qc, int *levels) {
+  if (h && h->M > 1) return CASL_EUNSUPPORTED;
   if (!h) return CASL_EINVAL;
   size_t nn = (size_t)h->n * h->n;
   int rc = con2grid_to_phys(h, h->w[5], levels != nullptr);
@@ -2590,6 +2592,13 @@ int casl_advance(casl_handle *h) {
 }
 
 int casl_surgery(casl_handle *h) {
+  if (h && h->M > 1) {  // an ensemble: surgery on every member, then the member ranges
+    int rc = sync_counts(h);
+    if (rc) return rc;
+    if ((rc = surgery_dev(h))) return rc;
+    if ((rc = member_ranges(h))) return rc;
+    return sync_counts(h);
+  }
   if (!h) return CASL_EINVAL;
   int rc = surgery_dev(h);
   if (rc) return rc;
@@ -2603,6 +2612,7 @@ int casl_renode(casl_handle *h, const double *xd, const double *yd, int npd, dou
 }
 
 int casl_recontour(casl_handle *h, const double *qq) {
+  if (h && h->M > 1) return CASL_EUNSUPPORTED;  // ensembles recontour inside casl_step
   if (!h || !qq) return CASL_EINVAL;
   size_t nn = (size_t)h->n * h->n;
   CASL_CUDA_TRY(cudaMemcpyAsync(h->qr, qq, nn * sizeof(double), cudaMemcpyHostToDevice, h->stream));
@@ -2695,6 +2705,7 @@ __global__ void k_minmax(const double *q, long long nn, double *part) {
 
 int casl_initialise(casl_handle *h, const double *qq_init) {
   if (!h || !qq_init) return CASL_EINVAL;
+  if (h->M > 1) return CASL_EUNSUPPORTED;  // casl_ensemble_initialise
   long long nn = (long long)h->n * h->n;
   cudaStream_t s = h->stream;
   int rc = get_scalars(h);
@@ -2779,6 +2790,7 @@ int casl_step(casl_handle *h, int nsteps) {
 
 int casl_set_precision(casl_handle *h, int mode) {
   if (!h || (mode != CASL_PREC_FP64 && mode != CASL_PREC_FP32_INVERSION)) return CASL_EINVAL;
+  if (h->M > 1 && mode != CASL_PREC_FP64) return CASL_EUNSUPPORTED;
   cudaSetDevice(h->device);
   if (mode == CASL_PREC_FP32_INVERSION && !h->f32) {
     const size_t bytes = (size_t)6 * h->n * h->n * sizeof(float);
@@ -2884,6 +2896,7 @@ int casl_profile_read(casl_handle *h, double *total_ms, long long *launches, dou
 
 int casl_diagnostics(casl_handle *h, double out[4]) {
   if (!h || !out) return CASL_EINVAL;
+  if (h->M > 1) return CASL_EUNSUPPORTED;  // one simulation's energies and circulation
   cudaStream_t st = h->stream;
   const long long nn = (long long)h->n * h->n;
   if (h->uv_fp32) {

@@ -1121,6 +1121,7 @@ int casl_closure_attach(casl_handle *h, casl_net *net, casl_handle *judge, int c
   }
   if (net->n != h->n || net->device != h->device || check_every < 0 || !(budget > 0.0))
     return CASL_EINVAL;
+  if (h->M > 1) return CASL_EUNSUPPORTED;  // one simulation
   if (judge && (judge->device != h->device || judge->n % h->n)) return CASL_EINVAL;
   cudaSetDevice(h->device);
   int rc;

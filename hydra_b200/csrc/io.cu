@@ -397,6 +397,7 @@ int casl_io_read_synopsis(const char *path, int iind, int *nq, int *nptq, double
 // copies; the files are written by a host thread (casl_io_wait joins it).
 int casl_savecont(casl_handle *h, const char *dir, int icrec) {
   if (!h || !dir || icrec < 1 || icrec > 999) return CASL_EINVAL;
+  if (h->M > 1) return CASL_EUNSUPPORTED;  // the files of one simulation
   int rc = io_join(h);
   if (rc) return rc;
   rc = sync_counts(h);
@@ -464,6 +465,7 @@ int casl_savecont(casl_handle *h, const char *dir, int icrec) {
 // save time between two steps (pt); here the state is written at t itself.
 int casl_savegrid(casl_handle *h, const char *dir, int irec) {
   if (!h || !dir || irec < 1) return CASL_EINVAL;
+  if (h->M > 1) return CASL_EUNSUPPORTED;
   int rc = io_join(h);
   if (rc) return rc;
   rc = get_scalars(h);
@@ -537,6 +539,7 @@ int casl_io_wait(casl_handle *h) {
 // qs = ptospc(con2grid + qr) on the device, qd = 0.
 int casl_readcont(casl_handle *h, const char *dir, int iind) {
   if (!h || !dir || iind < 1 || iind > 999) return CASL_EINVAL;
+  if (h->M > 1) return CASL_EUNSUPPORTED;
   int rc = io_join(h);
   if (rc) return rc;
   std::string d(dir);

@@ -1461,6 +1461,7 @@ using namespace casl;
 extern "C" int casl_genfg(casl_handle *h, int ix1v, int nxv, int iy1v, int nyv, int stride,
                           float *out) {
   if (!h || !out) return CASL_EINVAL;
+  if (h->M > 1) return CASL_EUNSUPPORTED;  // one simulation's image
   const Consts &c = h->c;
   const int nxu = c.nxu, nyu = c.nyu;
   if (ix1v < 1 || ix1v > nxu || iy1v < 1 || iy1v > nyu || nxv < 1 || nyv < 1 || stride < 1 ||
