@@ -96,7 +96,7 @@ __device__ __forceinline__ void store_px(bf16 *buf, int n, int row, int col, con
 // ---------------------------------------------------------------------------
 struct ConvArgs {
   const bf16 *in;     // CIN channels, padded layout
-  const bf16 *wimg;   // [25 taps][CIN/8][COUT][8]: the shared-memory image of the weights
+  const bf16 *wimg;   // [5 kx][CIN/8][5 (4-ky)][COUT][8]: the shared-memory image of the weights
   const float *bias;  // FWD modes: COUT entries
   bf16 *out;          // FWD_GELU / BWD_GELU: COUT channels, padded layout
   bf16 *zout;         // FWD_GELU: pre-activations (nullable)
@@ -120,9 +120,14 @@ struct ConvSmem {
 
 // One CTA: output columns [x0, x0+128) of rows [y0, y0+R).  Thread t owns
 // output column x0+t (TMEM lane t); row r's COUT accumulators are TMEM
-// columns [r*COUT, (r+1)*COUT).  A[m][k] = input(row y0+r+ky-2, column
-// x0+m+kx-2, channel k of the pair of planes), B[co][k] = W(co, k, ky, kx);
-// 25 taps x CIN/16 plane pairs accumulate into each row.
+// columns [r*COUT, (r+1)*COUT), cleared first.  Staged input row i (global
+// row y0+i-2) feeds output rows r = i-4 .. i (those inside the CTA) through
+// tap row ky = i - r: one MMA per (i, kx, plane pair) with
+// A[m][k] = input(row y0+i-2, column x0+m+kx-2, channel k of the pair) and
+// B the weights of all those rows' ky stacked along N -- the image keeps ky
+// descending so that ascending output rows (ascending TMEM columns) meet
+// their ky in order.  N = 32..160: each staged A tile is read once per kx
+// and plane pair for up to five output rows.
 template <int CIN, int COUT, int R, int MODE>
 __global__ void __launch_bounds__(128, 1) k_conv5(ConvArgs a) {
   using S = ConvSmem<CIN, COUT, R>;
@@ -154,23 +159,28 @@ __global__ void __launch_bounds__(128, 1) k_conv5(ConvArgs a) {
   __syncthreads();
   tc::tc_fence_after();
   const uint32_t tbase = *tslot;
+  // every MMA accumulates: clear this warp's lanes of all accumulators
+  for (int c0 = 0; c0 < S::TCOLS; c0 += 32)
+    tc::tmem_zero32(tbase + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0);
+  tc::tmem_wait_st();
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
   bool ok = tc::mbar_wait(&bars[0], 0);
   if (tid == 0 && ok) {
     const uint32_t in_a = tc::smem_u32(in_s), w_a = tc::smem_u32(w_s);
-    constexpr uint32_t IDESC = tc::idesc_bf16(128, COUT, false, false);
-    for (int r = 0; r < R; r++) {
-      uint32_t acc = 0;
-      for (int ky = 0; ky < 5; ky++)
-        for (int kx = 0; kx < 5; kx++)
+    for (int i = 0; i < R + 4; i++) {
+      const int r_lo = i - 4 > 0 ? i - 4 : 0, r_hi = i < R - 1 ? i : R - 1;
+      const int nrow = r_hi - r_lo + 1, ky_hi = i - r_lo;
+      const uint32_t idesc = tc::idesc_bf16(128, nrow * COUT, false, false);
+      for (int kx = 0; kx < 5; kx++)
 #pragma unroll
-          for (int cp = 0; cp < CIN / 16; cp++) {
-            const uint64_t ad =
-                tc::sdesc(in_a + (r + ky) * S::RS + 2 * cp * CS + kx * 16, CS, 128);
-            const uint64_t bd =
-                tc::sdesc(w_a + ((ky * 5 + kx) * (CIN / 8) + 2 * cp) * COUT * 16, COUT * 16, 128);
-            tc::mma_bf16(tbase + r * COUT, ad, bd, IDESC, acc);
-            acc = 1;
-          }
+        for (int cp = 0; cp < CIN / 16; cp++) {
+          const uint64_t ad = tc::sdesc(in_a + i * S::RS + 2 * cp * CS + kx * 16, CS, 128);
+          const uint64_t bd = tc::sdesc(
+              w_a + ((kx * (CIN / 8) + 2 * cp) * 5 + (4 - ky_hi)) * COUT * 16, 5 * COUT * 16, 128);
+          tc::mma_bf16(tbase + r_lo * COUT, ad, bd, idesc, 1u);
+        }
     }
     tc::mma_commit(&bars[1]);
   }
@@ -405,21 +415,24 @@ __global__ void k_weight_images(Params P) {
     const float *W = P.w + P.m.offw[l];
     const long long nimg = 25LL * ci_p * co_p;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nimg; t += stride) {
-      // forward image: t = ((tap*(ci_p/8) + c)*co_p + co)*8 + e, ci = 8c + e
+      // forward image: t = (((kx*(ci_p/8) + c)*5 + kyd)*co_p + co)*8 + e with
+      // ci = 8c + e and ky = 4 - kyd
       {
         const int e = (int)(t % 8), co = (int)((t / 8) % co_p);
-        const int c = (int)((t / 8 / co_p) % (ci_p / 8)), tap = (int)(t / 8 / co_p / (ci_p / 8));
-        const int ci = 8 * c + e;
+        const int kyd = (int)((t / 8 / co_p) % 5), c = (int)((t / 8 / co_p / 5) % (ci_p / 8));
+        const int kx = (int)(t / 8 / co_p / 5 / (ci_p / 8));
+        const int ci = 8 * c + e, tap = (4 - kyd) * 5 + kx;
         const float v = (ci < ci_r && co < co_r) ? W[(co * ci_r + ci) * 25 + tap] : 0.0f;
         P.L[l].wf[t] = __float2bfloat16_rn(v);
       }
-      // input-gradient image: t = ((tap'*(co_p/8) + c')*ci_p + ci)*8 + e, co = 8c' + e,
-      // tap' = (4-ky)*5 + (4-kx)
+      // input-gradient image (the convolution of the output gradient with the
+      // taps flipped and ci, co exchanged): t = (((kx'*(co_p/8) + c')*5 + kyd')*ci_p
+      // + ci)*8 + e with co = 8c' + e, ky' = 4 - kyd', tap = (4-ky')*5 + (4-kx')
       {
         const int e = (int)(t % 8), ci = (int)((t / 8) % ci_p);
-        const int c = (int)((t / 8 / ci_p) % (co_p / 8)), tp = (int)(t / 8 / ci_p / (co_p / 8));
-        const int co = 8 * c + e;
-        const int tap = 24 - tp;
+        const int kyd = (int)((t / 8 / ci_p) % 5), c = (int)((t / 8 / ci_p / 5) % (co_p / 8));
+        const int kxp = (int)(t / 8 / ci_p / 5 / (co_p / 8));
+        const int co = 8 * c + e, tap = kyd * 5 + (4 - kxp);
         const float v = (ci < ci_r && co < co_r) ? W[(co * ci_r + ci) * 25 + tap] : 0.0f;
         P.L[l].wb[t] = __float2bfloat16_rn(v);
       }

@@ -150,5 +150,19 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
   tmem_ld16(taddr + 16, v + 16);
 }
 
+// Registers -> TMEM: 32 consecutive 32-bit columns of this warp's lanes set
+// to zero (accumulators that every MMA then adds into).
+__device__ __forceinline__ void tmem_zero32(uint32_t taddr) {
+  const uint32_t z = 0;
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,"
+      "%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1};" ::"r"(taddr),
+      "r"(z)
+      : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() {
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+
 }  // namespace tc
 }  // namespace casl
