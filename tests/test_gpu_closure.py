@@ -202,8 +202,9 @@ def test_constant_correction_shifts_the_nodes(oracle_mod, gpu_lib):
     dx = (cb["xq"] - ca["xq"] + np.pi) % L - np.pi
     dy = (cb["yq"] - ca["yq"] + np.pi) % L - np.pi
     assert dt > 0.0
-    assert np.abs(dx - dt * 2.0 * 0.5).max() <= 1e-12
-    assert np.abs(dy - dt * 2.0 * (-0.25)).max() <= 1e-12
+    # every stage's wrap multiplies by oms = 1 - 1e-11 (evolution.f90:219)
+    assert np.abs(dx - dt * 2.0 * 0.5).max() <= 1e-9
+    assert np.abs(dy - dt * 2.0 * (-0.25)).max() <= 1e-9
     net.close(); a.close(); b.close()
 
 
