@@ -222,6 +222,28 @@ __device__ __forceinline__ double sumrange(const double *__restrict__ S, long lo
 
 __device__ __forceinline__ int nint_d(double x) { return (int)llround(x); }
 
+// The reference adds a contour's (or a corner piece's) densities one after
+// the other from its first node (contours.f90:799-806, 843-853) and rounds
+// the total to the node count.  The prefix sums here group the additions
+// otherwise; where the total lies within 1e-6 of a half-integer, so that
+// the grouping could move it across the rounding point, it is recomputed in
+// the reference's order: m densities from node st, wrapping within
+// [cs, cs+L).
+__device__ __forceinline__ bool near_half(double x) {
+  const double f = x - floor(x);
+  return fabs(f - 0.5) < 1e-6;
+}
+__device__ double seq_sum(const double *__restrict__ e, long long cs, long long L, long long st,
+                          long long m) {
+  double t = 0.0;
+  long long i = st - cs;
+  for (long long j = 0; j < m; j++) {
+    t = t + e[cs + i];
+    if (++i == L) i = 0;
+  }
+  return t;
+}
+
 // Per contour: node count, pieces (contours.f90:799-809, 813-930), and
 // where its pieces are stored (block by block from a running total in
 // d_tot[1]; piece storage order is free, the output order comes from the
@@ -236,6 +258,7 @@ __global__ void k_rn_count(RenodeIn in, RenodeScratch s, Consts c, int mode) {
     if (k < Ce) {
       long long cs = in.cs[k], L = in.len[k];
       double total = s.S[cs + L - 1];
+      if (near_half(total)) total = seq_sum(s.e, cs, L, cs, L);
       s.ctot[k] = total;
       if (!(mode == RENODE_SURGERY && L <= 3)) {
         int npr0 = nint_d(total) + 1;
@@ -277,6 +300,7 @@ __global__ void k_rn_fill(RenodeIn in, RenodeScratch s, Consts c, int mode) {
         pl = en - st;  // both corners lie in [cs, cs+L)
         if (pl < 0) pl += L;
         sum = sumrange(s.S, cs, L, st, pl);
+        if (near_half(sum)) sum = seq_sum(s.e, cs, L, st, pl);
         n = sum > c.small ? nint_d(sum) + 1 : 0;
       }
       s.pc[p] = k;
