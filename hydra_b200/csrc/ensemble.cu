@@ -229,22 +229,31 @@ int ensemble_recontour(casl_handle *h) {
     const int a = h->hmnode[m], npt = h->hmnode[m + 1] - a;
     const int ca = h->hmcont[m], nq = h->hmcont[m + 1] - ca;
     const int loff = m * CASL_LSTRIDE;
-    if (npt > 0 || nq > 0)
-      CASL_K(k_slice_member, gsz(npt > nq ? npt : nq), 256, 0, st)(
-          h->xq, h->yq, h->nextq, h->i1q, h->i2q, h->npq, h->indq, a, npt, ca, nq, loff, v->xq,
-          v->yq, v->nextq, v->i1q, v->i2q, v->npq, v->indq);
-    Scalars &vs = *v->hscal;
-    memset(&vs, 0, sizeof(Scalars));
-    vs.nq = nq;
-    vs.nptq = npt;
-    vs.qjump = h->mqjump[m];
-    v->nq = nq;
-    v->nptq = npt;
-    v->qjump = h->mqjump[m];
-    v->contex = npt > 0;
-    if ((rc = put_scalars(v))) return rc;
-    if ((rc = recontour_dev(v, h->qr + m * nn))) return rc;
-    if ((rc = sync_counts(v))) return rc;
+    // a member whose new contours do not fit the view is recontoured again
+    // with a view four times larger (up to the ensemble's capacities)
+    for (;;) {
+      if (npt > 0 || nq > 0)
+        CASL_K(k_slice_member, gsz(npt > nq ? npt : nq), 256, 0, st)(
+            h->xq, h->yq, h->nextq, h->i1q, h->i2q, h->npq, h->indq, a, npt, ca, nq, loff, v->xq,
+            v->yq, v->nextq, v->i1q, v->i2q, v->npq, v->indq);
+      Scalars &vs = *v->hscal;
+      memset(&vs, 0, sizeof(Scalars));
+      vs.nq = nq;
+      vs.nptq = npt;
+      vs.qjump = h->mqjump[m];
+      v->nq = nq;
+      v->nptq = npt;
+      v->qjump = h->mqjump[m];
+      v->contex = npt > 0;
+      if ((rc = put_scalars(v))) return rc;
+      rc = recontour_dev(v, h->qr + m * nn);
+      if (rc == CASL_OK) rc = sync_counts(v);
+      if (rc != CASL_ECAPACITY || (v->npm >= h->npm && v->nm >= h->nm)) break;
+      long long gn = 4 * v->npm < h->npm ? 4 * v->npm : h->npm;
+      long long gc = 4 * v->nm < h->nm ? 4 * v->nm : h->nm;
+      if ((rc = view_get(h, gn, gc, &v))) return rc;
+    }
+    if (rc) return rc;
     const int onpt = v->nptq, onq = v->nq;
     if (No + onpt > h->npm || Co + onq > h->nm) return CASL_ECAPACITY;
     if (onpt > 0 || onq > 0)

@@ -56,7 +56,7 @@ def load(path):
 
 
 def train(n=512, pairs=20000, pairs_per_run=500, lr=1e-3, lr_end=1e-4, k0=12.0, levels=80,
-          seed0=1000, fine=4, device=0, log_every=500, out=None, quiet=False):
+          seed0=1000, fine=4, device=0, log_every=250, out=None, quiet=False):
     kw = dict(ncontq=levels, force_surgery=1, dtmax=0.05, npm=8_000_000, nm=500_000)
     g = CaslGPU(n, device=device, **kw)
     gf = CaslGPU(fine * n, device=device, ncontq=levels, npm=8_000_000, nm=500_000)
@@ -69,6 +69,9 @@ def train(n=512, pairs=20000, pairs_per_run=500, lr=1e-3, lr_end=1e-4, k0=12.0, 
     done, run = 0, 0
     while done < pairs:
         g.initialise(random_pv(n, k0, seed0 + run))
+        if not quiet:
+            print(f"run {run}: seed {seed0 + run}, {g.counts()[1]} nodes "
+                  f"({time.perf_counter() - t0:.0f} s)", flush=True)
         for _ in range(min(pairs_per_run, pairs - done)):
             g.step(1)
             frac = done / max(pairs - 1, 1)
@@ -78,7 +81,8 @@ def train(n=512, pairs=20000, pairs_per_run=500, lr=1e-3, lr_end=1e-4, k0=12.0, 
             if not quiet and done % log_every == 0:
                 h = np.array(hist[-log_every:])
                 print(f"pairs {done}: plain {h[:, 0].mean():.3e} net {h[:, 1].mean():.3e} "
-                      f"loss {h[:, 2].mean():.3e} ({time.perf_counter() - t0:.0f} s)", flush=True)
+                      f"loss {h[:, 2].mean():.3e}, nodes {g.counts()[1]} "
+                      f"({time.perf_counter() - t0:.0f} s)", flush=True)
         run += 1
     secs = time.perf_counter() - t0
     params, qs, us = net.params()
