@@ -24,7 +24,6 @@ from __future__ import annotations
 import argparse
 import json
 import os
-import subprocess
 import sys
 import threading
 import time
@@ -58,65 +57,86 @@ def config_dict(a, nodes, mean_dt=None):
 # clocks sampled during the timed region
 # ---------------------------------------------------------------------------
 class ClockSampler:
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clock, its maximum, power and the active clock-event reasons of
+    this process's GPU, read through NVML every 2 ms by a thread that stamps
+    each sample with its own wall-clock time (a piped nvidia-smi delivers
+    its lines in buffered bursts, whose arrival times say nothing about when
+    they were taken).  Only reads; no setting of the GPU is touched."""
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
 
     def __init__(self, device):
         self.device = device
-        self.proc = None
-        self.lines = []  # (arrival time, csv line)
+        self.samples = []  # (time, sm MHz, max sm MHz, power W, reason mask)
         self.window = None
+        self.nvml = None
+        self.stop_flag = threading.Event()
+
+    def _handle(self, nv):
+        try:
+            import torch
+            p = torch.cuda.get_device_properties(self.device)
+            bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+            return nv.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.device)
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "50"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
+            import pynvml as nv
+            nv.nvmlInit()
+            self.nvml = nv
+            self.h = self._handle(nv)
+            self.max_sm = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
+            self.thread = threading.Thread(target=self._run, daemon=True)
             self.thread.start()
-        except Exception:
-            self.proc = None
+        except Exception as e:
+            self.nvml = None
+            self.why = f"nvml unavailable: {type(e).__name__}"
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append((time.time(), line.strip()))
+    def _run(self):
+        nv = self.nvml
+        while not self.stop_flag.is_set():
+            try:
+                t = time.time()
+                sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                pw = nv.nvmlDeviceGetPowerUsage(self.h) / 1000.0
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                self.samples.append((t, sm, self.max_sm, pw, rs))
+            except Exception:
+                pass
+            time.sleep(0.002)
 
     def mark(self, t0, t1):
-        """The timed region in wall-clock seconds; only samples that arrive
-        inside it are kept (the sampler runs from before the warm-up so that
-        its start-up does not fall into the region)."""
+        """The timed region in wall-clock seconds; only samples taken inside
+        it are kept (the sampler runs from before the warm-up so that its
+        start-up does not fall into the region)."""
         self.window = (t0, t1)
 
     def stop(self):
-        if not self.proc:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        lines = self.lines
+        if not self.nvml:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [getattr(self, "why", "nvml unavailable")]}
+        self.stop_flag.set()
+        self.thread.join(timeout=5)
+        nv = self.nvml
+        xs = self.samples
         if self.window:
-            lines = [l for l in lines if self.window[0] <= l[0] <= self.window[1]]
-        for _, ln in lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                smax.append(float(parts[2]))
-            except ValueError:
-                continue
-            for nm, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
+            xs = [x for x in xs if self.window[0] <= x[0] <= self.window[1]]
+        reasons = set()
+        for x in xs:
+            for nm, attr in self.REASONS:
+                if x[4] & getattr(nv, attr, 0):
                     reasons.add(nm)
-        return {"sm_mhz": float(np.median(sm)) if sm else None,
-                "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        try:
+            nv.nvmlShutdown()
+        except Exception:
+            pass
+        return {"sm_mhz": float(np.median([x[1] for x in xs])) if xs else None,
+                "sm_max_mhz": float(self.max_sm),
+                "power_w": float(np.median([x[3] for x in xs])) if xs else None,
+                "reasons": sorted(reasons), "samples": len(xs)}
 
 
 def measured_peak():

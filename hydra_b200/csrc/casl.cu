@@ -3,6 +3,7 @@
 //
 // Reference: basic_hydra/ca/plane/qg/caps (Fortran 90).  File:line citations
 // name the reference procedure each piece restates.
+#include <chrono>
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdio.h>
@@ -217,8 +218,8 @@ struct LoadDeriv {
   long long ms = 0;
   __device__ __forceinline__ double base(int b, int kx0, int ky0) const {
     long long k = (long long)ky0 * n + kx0;
-    const int e = b % nb;
-    double v = pick(f, e)[(long long)(b / nb) * ms + k];
+    const int e = bentry(b, nb, ms);
+    double v = pick(f, e)[bmember(b, nb, ms) + k];
     return pick(wg, e) ? green[k] * v : v;
   }
   // first pass of an inverse transform: vector v = ky, element j = kx.
@@ -227,7 +228,7 @@ struct LoadDeriv {
   // and the reflected index (n-k) mod n is always a valid element.
   __device__ __forceinline__ double operator()(int b, int v, int j) const {
     const int nw = n >> 1, kx = j, ky = v;
-    const bool dx = pick(dir, b % nb) == 0;
+    const bool dx = pick(dir, bentry(b, nb, ms)) == 0;
     const int k = dx ? kx : ky;
     const int kr = (n - k) & (n - 1);
     const int hi = k < nw ? 2 * k - 1 : 2 * (n - k) - 1;
@@ -241,7 +242,7 @@ struct LoadDeriv {
   // d/dx the reflected indices n-j, n-j-1 run backwards from an odd start,
   // so they stay two loads.
   __device__ __forceinline__ double2 pair(int b, int v, int j) const {
-    const int e = b % nb;
+    const int e = bentry(b, nb, ms);
     if (pick(dir, e) == 0) return make_double2((*this)(b, v, j), (*this)(b, v, j + 1));
     const int nw = n >> 1, k = v;
     const int kr = (n - k) & (n - 1);
@@ -249,7 +250,7 @@ struct LoadDeriv {
     const double h = hrky[hi < 0 ? 0 : hi];
     const double fac = (k == 0 || k == nw) ? 0.0 : (k < nw ? -h : h);
     const long long o = (long long)kr * n + j;
-    double2 q = *reinterpret_cast<const double2 *>(pick(f, e) + (long long)(b / nb) * ms + o);
+    double2 q = *reinterpret_cast<const double2 *>(pick(f, e) + bmember(b, nb, ms) + o);
     if (pick(wg, e)) {
       const double2 g = *reinterpret_cast<const double2 *>(green + o);
       q = make_double2(g.x * q.x, g.y * q.y);
@@ -389,13 +390,15 @@ struct StoreScaled {
   long long ms = 0;
   // last pass of an inverse transform: vector v = ix, element k = iy
   __device__ __forceinline__ void operator()(int b, int v, int k, double x) const {
-    const double sc = pick(scale, b % nb);
-    pick(p, b % nb)[(long long)(b / nb) * ms + (long long)v * n + k] = sc == 1.0 ? x : sc * x;
+    const int e = bentry(b, nb, ms);
+    const double sc = pick(scale, e);
+    pick(p, e)[bmember(b, nb, ms) + (long long)v * n + k] = sc == 1.0 ? x : sc * x;
   }
   __device__ __forceinline__ void pair(int b, int v, int k, double2 x) const {
-    const double sc = pick(scale, b % nb);
+    const int e = bentry(b, nb, ms);
+    const double sc = pick(scale, e);
     if (sc != 1.0) x = make_double2(sc * x.x, sc * x.y);
-    *reinterpret_cast<double2 *>(pick(p, b % nb) + (long long)(b / nb) * ms + (long long)v * n + k) = x;
+    *reinterpret_cast<double2 *>(pick(p, e) + bmember(b, nb, ms) + (long long)v * n + k) = x;
   }
 };
 struct LoadBatch {
@@ -405,7 +408,7 @@ struct LoadBatch {
   int nb = 6;
   long long ms = 0;
   __device__ __forceinline__ double operator()(int b, int v, int j) const {
-    return pick(p, b % nb)[(long long)(b / nb) * ms + (long long)v * vs + (long long)j * es];
+    return pick(p, bentry(b, nb, ms))[bmember(b, nb, ms) + (long long)v * vs + (long long)j * es];
   }
 };
 // FP32 storage for the inverse transform pair of the FP32-inversion mode:
@@ -559,7 +562,11 @@ __global__ void k_c2g_scatter(const double *__restrict__ xq, const double *__res
         yi = y1;
         const bool nb = ia == i + 1 && lane < 31;
         const double xa = nb ? xs : xq[ia], ya = nb ? ys : yq[ia];
-        if (!(xi >= c.xmin && xi < c.xmax && yi >= c.ymin && yi < c.ymax)) {
+        // both ends in the domain: an end outside it (or not finite) would
+        // give a crossing count without bound; the node itself is reported
+        // by its own lane
+        if (!(xi >= c.xmin && xi < c.xmax && yi >= c.ymin && yi < c.ymax) ||
+            !(xa >= c.xmin && xa < c.xmax && ya >= c.ymin && ya < c.ymax)) {
           atomicExch(err, CASL_EDOMAIN);
         } else {
           const int ixci = 1 + f_int(c.glxfi * (xi - c.xmin));
@@ -1521,14 +1528,19 @@ static int stage_update(casl_handle *h, int stage, const T *u, const T *v) {
 // adapt, source, the node update and the spectral RK update.
 static int advance_dev(casl_handle *h) {
   int rc;
+  Trace tr;
+  tr.begin(h->stream, "advance");
   for (int stage = 1; stage <= 4; stage++) {
     // stage 1: the reset inside the filter combination rewrites qs and qd
     // before the gradients read them
     if ((rc = inversion_qq(h, stage == 1))) return rc;
+    tr.point("con2grid+qq");
     const bool f32 = h->prec == CASL_PREC_FP32_INVERSION;
     if ((rc = f32 ? invert_and_gradients32(h) : invert_and_gradients(h))) return rc;
+    tr.point("invert");
     if (stage == 1 && (rc = adapt_dev(h))) return rc;
     if ((rc = source_prod(h, stage))) return rc;
+    tr.point("adapt+source");
     if (f32) {
       const long long nn = (long long)h->n * h->n;
       const float *u = h->f32, *v = h->f32 + nn;
@@ -1539,7 +1551,12 @@ static int advance_dev(casl_handle *h) {
       if (h->closure && (rc = closure_stage(h, &u, &v))) return rc;
       if ((rc = stage_update<double>(h, stage, u, v))) return rc;
     }
+    tr.point("stage update");
+    static const char *const names[4] = {"RK4 stage 1", "RK4 stage 2", "RK4 stage 3",
+                                         "RK4 stage 4"};
+    if ((rc = debug_check(h, names[stage - 1]))) return rc;
   }
+  tr.flush("advance");
   return CASL_OK;
 }
 
@@ -1855,6 +1872,54 @@ int sync_counts(casl_handle *h) {
   return CASL_OK;
 }
 
+// Opt-in state check (environment variable CASL_CHECK=1), run by casl_step
+// after recontouring, after surgery and after each RK4 stage: the first node
+// that is not finite, lies outside the domain or links outside the node
+// arrays is printed with the phase that left it, and the step returns
+// CASL_EDOMAIN there instead of carrying the bad node on.
+__global__ void k_first_bad(const double *__restrict__ xq, const double *__restrict__ yq,
+                            const int *__restrict__ nextq, int npt, Consts c, int *first) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < npt;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double x = xq[i], y = yq[i];
+    const int nx = nextq[i];
+    if (!(x >= c.xmin && x < c.xmax && y >= c.ymin && y < c.ymax) || nx < 0 || nx >= npt)
+      atomicMin(first, (int)i);
+  }
+}
+
+int debug_check(casl_handle *h, const char *phase) {
+  static int enabled = -1;
+  if (enabled < 0) {
+    const char *e = getenv("CASL_CHECK");
+    enabled = e && e[0] == '1';
+  }
+  if (!enabled) return CASL_OK;
+  int rc = sync_counts(h);
+  if (rc) {
+    fprintf(stderr, "[casl check] %s: error %d\n", phase, rc);
+    return rc;
+  }
+  const int npt = h->nptq;
+  if (npt == 0) return CASL_OK;
+  int *d = nullptr, first = INT_MAX;
+  CASL_CUDA_TRY(cudaMalloc(&d, sizeof(int)));
+  CASL_CUDA_TRY(cudaMemcpyAsync(d, &first, sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  k_first_bad<<<148 * 8, 256, 0, h->stream>>>(h->xq, h->yq, h->nextq, npt, h->c, d);
+  CASL_CUDA_TRY(cudaMemcpyAsync(&first, d, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CASL_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  cudaFree(d);
+  if (first == INT_MAX) return CASL_OK;
+  double x = 0, y = 0;
+  int nx = -1;
+  cudaMemcpy(&x, h->xq + first, sizeof(double), cudaMemcpyDeviceToHost);
+  cudaMemcpy(&y, h->yq + first, sizeof(double), cudaMemcpyDeviceToHost);
+  cudaMemcpy(&nx, h->nextq + first, sizeof(int), cudaMemcpyDeviceToHost);
+  fprintf(stderr, "[casl check] %s: node %d of %d at (%.17g, %.17g), next %d\n", phase, first,
+          npt, x, y, nx);
+  return CASL_EDOMAIN;
+}
+
 // Scratch arenas grow with 50% headroom: their sizes follow node and
 // crossing counts, which drift from step to step, and re-allocating several
 // GB costs far more than the spare memory.
@@ -1869,27 +1934,45 @@ int ensure_scratch(casl_handle *h, size_t bytes) {
   return CASL_OK;
 }
 
+static double wall_ms() {
+  return std::chrono::duration<double, std::milli>(
+             std::chrono::steady_clock::now().time_since_epoch())
+      .count();
+}
+
 void Trace::begin(cudaStream_t s, const char *what) {
   static int enabled = -1;
   if (enabled < 0) {
     const char *e = getenv("CASL_TRACE");
-    enabled = e && e[0] == '1';
+    enabled = e ? (e[0] == '1' ? 1 : e[0] == '2' ? 2 : 0) : 0;
   }
-  on = enabled == 1;
+  on = enabled >= 1;
+  eager = enabled == 2;
   n = 0;
   st = s;
+  t_last = wall_ms();
   if (on) point(what);
 }
 
 void Trace::point(const char *what) {
-  if (!on || n >= 64) return;
+  if (!on) return;
+  if (eager) {
+    cudaError_t e = cudaStreamSynchronize(st);
+    const double t = wall_ms();
+    fprintf(stderr, "[casl trace] at %s +%.3f ms%s\n", what, t - t_last,
+            e == cudaSuccess ? "" : " (stream error)");
+    fflush(stderr);
+    t_last = t;
+    return;
+  }
+  if (n >= 64) return;
   cudaEventCreate(&ev[n]);
   cudaEventRecord(ev[n], st);
   name[n++] = what;
 }
 
 void Trace::flush(const char *title) {
-  if (!on) return;
+  if (!on || eager) return;
   cudaStreamSynchronize(st);
   fprintf(stderr, "[casl trace] %s:", title);
   for (int i = 1; i < n; i++) {
@@ -2765,6 +2848,7 @@ int casl_step(casl_handle *h, int nsteps) {
         // an ensemble recontours member by member
         if ((rc = evo_prepare(h))) return rc;
         if ((rc = h->M > 1 ? ensemble_recontour(h) : recontour_dev(h, h->qr))) return rc;
+        if ((rc = debug_check(h, "recontour"))) return rc;
         if ((rc = sync_counts(h))) return rc;
         if ((rc = evo_init(h))) return rc;
         CASL_K(k_twist_zero, 1, 256, 0, h->stream)(h->scal, h->M);
@@ -2772,11 +2856,13 @@ int casl_step(casl_handle *h, int nsteps) {
         if (force) {
           h->ireg = 1;
           if ((rc = surgery_dev(h))) return rc;
+          if ((rc = debug_check(h, "surgery after recontouring"))) return rc;
           if (h->M > 1 && (rc = member_ranges(h))) return rc;
           CASL_K(k_twist_sub, 1, 256, 0, h->stream)(h->scal, h->p.twistmax, h->M);
         }
       } else {
         if ((rc = surgery_dev(h))) return rc;
+        if ((rc = debug_check(h, "surgery"))) return rc;
         if (h->M > 1 && (rc = member_ranges(h))) return rc;
         CASL_K(k_twist_sub, 1, 256, 0, h->stream)(h->scal, h->p.twistmax, h->M);
       }

@@ -929,8 +929,12 @@ static int evaluate(casl_handle *h, casl_net *N, casl_handle *hf, bool train, fl
     return CASL_OK;
   }
   if ((rc = cs_grow(cs, npt))) return rc;
+  Trace tr;
+  tr.begin(h->stream, "evaluate");
   if ((rc = judge_velocity(h, hf, cs->uJ, cs->vJ, cs->uP, cs->vP))) return rc;
+  tr.point("judge");
   if ((rc = net_correct(h, N, cs, train))) return rc;
+  tr.point("network");
   cudaStream_t st = h->stream;
   CASL_K(k_velint, gsz(npt), 256, 0, st)(h->xq, h->yq, npt, cs->ucor, cs->vcor, cs->uC, cs->vC,
                                           h->c);
@@ -946,6 +950,8 @@ static int evaluate(casl_handle *h, casl_net *N, casl_handle *hf, bool train, fl
     if ((rc = net::backward(N, st, &h->scal->error))) return rc;
     if ((rc = net::adam_step(N, st, lr))) return rc;
   }
+  tr.point(train ? "loss+backward+adam" : "loss");
+  tr.flush("evaluate");
   double a[3];
   if (cudaMemcpyAsync(a, cs->acc, 3 * sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess)
     return CASL_ECUDA;

@@ -99,6 +99,15 @@ __device__ __forceinline__ T pick(const T (&a)[N], int b) {
   return r;
 }
 
+// Batch entry b of an ensemble transform is entry b % nb of member b / nb,
+// whose fields lie ms elements after the previous member's.  One member
+// (ms = 0, b < nb) takes the branch without the integer division, which
+// would otherwise run for every element the functor loads or stores.
+__device__ __forceinline__ int bentry(int b, int nb, long long ms) { return ms ? b % nb : b; }
+__device__ __forceinline__ long long bmember(int b, int nb, long long ms) {
+  return ms ? (long long)(b / nb) * ms : 0;
+}
+
 // Plain strided load / store functors: element (b, v, j) at p[b*bs + v*vs + j*es].
 struct LoadStrided {
   __host__ double bytes() const { return 8.0; }

@@ -378,6 +378,15 @@ __global__ void k_rn_place(RenodeIn in, RenodeScratch s, RenodeOut out, Consts c
     for (long long t = t0; t <= t1; t++) {
       double acc = Ec - (double)t;
       double pp = 1.0 - acc / ew;
+      // Targets are assigned by prefix sums, whose grouping rounds: a
+      // segment of density zero or at the rounding level (the zero-length
+      // segments that surgery leaves where it joins two nodes) can receive
+      // a target that the reference's running sum gives its neighbour, and
+      // 1 - acc/ew is then far outside [0, 1] or 0/0.  Such a target is
+      // placed by the prefix values that assigned it (Ep < t <= Ec, so the
+      // fraction lies in (0, 1]): the segment's start, within rounding of
+      // where the reference puts it.
+      if (!(pp >= -1e-9 && pp <= 1.0 + 1e-9)) pp = ((double)t - Ep) / (Ec - Ep);
       double eta = pp * (A + pp * (B + pp * Cc));
       double xx = xd + pp * dx - eta * dy;
       double yy = yd + pp * dy + eta * dx;

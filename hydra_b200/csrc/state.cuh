@@ -120,6 +120,7 @@ int renode_host(casl_handle *h, const double *xd, const double *yd, int npd, dou
                 double *yr, int cap, int *npr);
 
 int sync_counts(casl_handle *h);    // device counts -> host copies
+int debug_check(casl_handle *h, const char *phase);  // CASL_CHECK=1: node sanity after a phase
 int get_scalars(casl_handle *h);    // device scalars -> hscal
 int put_scalars(casl_handle *h);    // hscal -> device scalars
 int inversion_dev(casl_handle *h, bool reset);  // evolution.f90:494-520
@@ -129,9 +130,14 @@ void io_release(casl_handle *h);    // joins the output writer, frees its stagin
 
 // Opt-in phase trace (environment variable CASL_TRACE=1): records CUDA
 // events at named points on the handle's stream and prints the device time
-// between consecutive points to stderr when flushed.
+// between consecutive points to stderr when flushed.  CASL_TRACE=2 instead
+// synchronises the stream at every point and prints the point's name and
+// the host time since the previous point at once, so that a phase which
+// never ends is named by the last line printed.
 struct Trace {
   bool on = false;
+  bool eager = false;
+  double t_last = 0.0;
   int n = 0;
   cudaEvent_t ev[64];
   const char *name[64];

@@ -7,7 +7,10 @@ against the fine-grid judge's node velocities (the same contours inverted on
 is made, by the library's own tensor-core forward and backward kernels and an
 Adam step (casl_closure_train).  States come from runs of the plain solver
 (surgery every step, recontouring every 20 regularisations) started from
-random-phase fields of seeds disjoint from the evaluation seeds.
+random-phase fields of seeds disjoint from the evaluation seeds; each run
+gives its first 250 states (the node count about quadruples over them), after
+which a new seed starts, so the pairs cover the early turbulent states that
+the closure is evaluated on.
 
   python -m hydra_b200.train_closure --n 512 --pairs 20000 --out hydra_b200/closure_512.npz
 """
@@ -55,7 +58,7 @@ def load(path):
     return d["params"], float(d["qscale"]), float(d["uscale"])
 
 
-def train(n=512, pairs=20000, pairs_per_run=500, lr=1e-3, lr_end=1e-4, k0=12.0, levels=80,
+def train(n=512, pairs=20000, pairs_per_run=250, lr=1e-3, lr_end=1e-4, k0=12.0, levels=80,
           seed0=1000, fine=4, device=0, log_every=250, out=None, quiet=False):
     kw = dict(ncontq=levels, force_surgery=1, dtmax=0.05, npm=8_000_000, nm=500_000)
     g = CaslGPU(n, device=device, **kw)
@@ -99,7 +102,7 @@ def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--n", type=int, default=512)
     ap.add_argument("--pairs", type=int, default=20000)
-    ap.add_argument("--pairs-per-run", type=int, default=500)
+    ap.add_argument("--pairs-per-run", type=int, default=250)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--k0", type=float, default=12.0)
     ap.add_argument("--levels", type=int, default=80)

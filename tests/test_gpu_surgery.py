@@ -28,10 +28,16 @@ def gpu64(gpu_lib):
     g.close()
 
 
-@pytest.mark.parametrize("case", ["circle", "wobbly", "corners", "tiny"])
+@pytest.mark.parametrize("case", ["circle", "wobbly", "corners", "tiny", "duplicates"])
 def test_renode_single(oracle_mod, gpu64, case):
     o = oracle_mod.Oracle(64, ncontq=20)
-    if case == "circle":
+    if case == "duplicates":
+        # surgery joins nodes by moving one onto the other: zero-length
+        # segments, whose density is zero, between every pair here; each
+        # must receive no node however the density sums round
+        x, y = circle(700, 0.9, 0.2, -0.1, wobble=0.25, k=7)
+        x, y = np.repeat(x, 2), np.repeat(y, 2)
+    elif case == "circle":
         x, y = circle(300, 1.0, 0.1, -0.2)
     elif case == "wobbly":
         x, y = circle(500, 0.8, -0.3, 0.4, wobble=0.3, k=5)
@@ -45,6 +51,7 @@ def test_renode_single(oracle_mod, gpu64, case):
     xo, yo = o.renode(x, y)
     xg, yg = gpu64.renode(x, y)
     assert len(xg) == len(xo)
+    assert np.all(np.isfinite(xg)) and np.all(np.isfinite(yg))
     if len(xo):
         assert np.abs(xg - xo).max() <= REL * np.pi
         assert np.abs(yg - yo).max() <= REL * np.pi
