@@ -3,6 +3,9 @@
 //
 // Reference: basic_hydra/ca/plane/qg/caps (Fortran 90).  File:line citations
 // name the reference procedure each piece restates.
+#include <cxxabi.h>
+#include <string>
+#include <typeinfo>
 #include <chrono>
 #include <cuda_runtime.h>
 #include <math.h>
@@ -119,6 +122,16 @@ int check_launch(casl_handle *h) {
 // ---------------------------------------------------------------------------
 // Transform launches
 // ---------------------------------------------------------------------------
+// A functor type's name without its namespace, for launch names.
+static std::string short_type_name(const std::type_info &t) {
+  int status = 0;
+  char *d = abi::__cxa_demangle(t.name(), nullptr, nullptr, &status);
+  std::string r = (status == 0 && d) ? d : t.name();
+  free(d);
+  for (size_t at; (at = r.find("casl::")) != std::string::npos;) r.erase(at, 6);
+  return r;
+}
+
 // One batched transform pass (all vectors of `batch` fields along one axis).
 template <int LOGH, bool FWD, bool LVF, bool SVF, class LD, class ST>
 static int launch_rfft(casl_handle *h, LD ld, ST st, int batch) {
@@ -127,13 +140,19 @@ static int launch_rfft(casl_handle *h, LD ld, ST st, int batch) {
   const bool prof = h->prof_class == CASL_PROF_FFT && h->prof_ev && h->prof_n < CASL_PROF_MAX;
   if (prof) cudaEventRecord(h->prof_ev[2 * h->prof_n], h->stream);
   auto kern = k_rfft_r<LOGH, FWD, LVF, SVF, LD, ST>;
-  const size_t sm = Sh::smem(FWD && SVF);
+  const size_t sm = rfft_smem<LOGH, FWD, LVF, SVF, staged_rows<LD, LVF>()>();
   static bool configured = false;  // one per template instance
   if (!configured) {
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     configured = true;
   }
-  CASL_K(kern, grid, Sh::NT, sm, h->stream)(ld, st, h->tw);
+  // named by size, direction and functors for the per-launch timing report
+  static char name[160];
+  if (!name[0])
+    snprintf(name, sizeof name, "k_rfft_r<%d %s, %s, %s>", Sh::N, FWD ? "fwd" : "inv",
+             short_type_name(typeid(LD)).c_str(), short_type_name(typeid(ST)).c_str());
+  for (bool once = kt_begin(name, grid, Sh::NT, sm, h->stream); once; once = kt_end())
+    launch_of(kern, grid, Sh::NT, sm, h->stream)(ld, st, h->tw);
   if (prof) {
     cudaEventRecord(h->prof_ev[2 * h->prof_n + 1], h->stream);
     h->prof_n++;
@@ -168,18 +187,18 @@ static int rfft_dispatch(casl_handle *h, LD ld, ST st, int batch) {
 int ptospc_dev(casl_handle *h, const double *phys, double *spec, int batch) {
   long long n = h->n, nn = n * n;
   // along iy for each ix: phys[ix*n+iy] -> spec[ky*n+ix] (spec != phys)
-  int rc = RFFT_DISPATCH(true, false, true, (LoadStrided{phys, nn, n, 1}),
+  int rc = RFFT_DISPATCH(true, false, true, (LoadRow{phys, nn, n, (int)n, &h->scal->error}),
                          (StoreStrided{spec, nn, 1, n}), batch);
   if (rc) return rc;
   // along ix for each ky, in place by rows: spec[ky*n + kx]
-  return RFFT_DISPATCH(true, false, false, (LoadStrided{spec, nn, n, 1}),
+  return RFFT_DISPATCH(true, false, false, (LoadRow{spec, nn, n, (int)n, &h->scal->error}),
                        (StoreStrided{spec, nn, n, 1}), batch);
 }
 
 int spctop_dev(casl_handle *h, const double *spec, double *phys, double *tmp, int batch) {
   long long n = h->n, nn = n * n;
   // along kx for each ky: spec[ky*n+kx] -> tmp[ky*n+ix]
-  int rc = RFFT_DISPATCH(false, false, false, (LoadStrided{spec, nn, n, 1}),
+  int rc = RFFT_DISPATCH(false, false, false, (LoadRow{spec, nn, n, (int)n, &h->scal->error}),
                          (StoreStrided{tmp, nn, n, 1}), batch);
   if (rc) return rc;
   // along ky for each ix: tmp[ky*n+ix] -> phys[ix*n+iy]
@@ -194,8 +213,13 @@ int spctop_dev(casl_handle *h, const double *spec, double *phys, double *tmp, in
 // Element (v = kx-1, j = ky-1) of xderiv / yderiv (sta2dfft.f90:169-245) of
 // a spectral field, optionally of green*field (main_invert, spectral.f90:321).
 // Batch index b selects field and direction.
-struct LoadDeriv {
-  static constexpr bool wide = true;  // 80 registers: at 64 the derivative load spills
+// MB: an ensemble transform (batch entry b is entry b % nb of member b / nb,
+// whose fields lie ms elements after the previous member's).  A single
+// simulation instantiates MB = false, whose index arithmetic has no integer
+// division: with it the derivative load, at its 80-register budget, spilled.
+template <bool MB>
+struct LoadDerivT {
+  static constexpr bool wide = MB;  // the ensemble's index arithmetic needs 80 registers
   // bytes per element, averaged over the batch's entries
   __host__ double bytes() const {
     int nb = 0, ng = 0;
@@ -212,14 +236,14 @@ struct LoadDeriv {
   const double *green;
   const double *hrkx, *hrky;
   int n;
-  // ensemble: batch entry b is entry b % nb of member b / nb, whose fields
-  // lie ms elements after the previous member's (nb = 6, ms = 0: one member)
   int nb = 6;
   long long ms = 0;
+  __device__ __forceinline__ int ent(int b) const { return MB ? b % nb : b; }
+  __device__ __forceinline__ long long mof(int b) const { return MB ? (long long)(b / nb) * ms : 0; }
   __device__ __forceinline__ double base(int b, int kx0, int ky0) const {
     long long k = (long long)ky0 * n + kx0;
-    const int e = bentry(b, nb, ms);
-    double v = pick(f, e)[bmember(b, nb, ms) + k];
+    const int e = ent(b);
+    double v = pick(f, e)[mof(b) + k];
     return pick(wg, e) ? green[k] * v : v;
   }
   // first pass of an inverse transform: vector v = ky, element j = kx.
@@ -228,7 +252,7 @@ struct LoadDeriv {
   // and the reflected index (n-k) mod n is always a valid element.
   __device__ __forceinline__ double operator()(int b, int v, int j) const {
     const int nw = n >> 1, kx = j, ky = v;
-    const bool dx = pick(dir, bentry(b, nb, ms)) == 0;
+    const bool dx = pick(dir, ent(b)) == 0;
     const int k = dx ? kx : ky;
     const int kr = (n - k) & (n - 1);
     const int hi = k < nw ? 2 * k - 1 : 2 * (n - k) - 1;
@@ -242,7 +266,7 @@ struct LoadDeriv {
   // d/dx the reflected indices n-j, n-j-1 run backwards from an odd start,
   // so they stay two loads.
   __device__ __forceinline__ double2 pair(int b, int v, int j) const {
-    const int e = bentry(b, nb, ms);
+    const int e = ent(b);
     if (pick(dir, e) == 0) return make_double2((*this)(b, v, j), (*this)(b, v, j + 1));
     const int nw = n >> 1, k = v;
     const int kr = (n - k) & (n - 1);
@@ -250,14 +274,45 @@ struct LoadDeriv {
     const double h = hrky[hi < 0 ? 0 : hi];
     const double fac = (k == 0 || k == nw) ? 0.0 : (k < nw ? -h : h);
     const long long o = (long long)kr * n + j;
-    double2 q = *reinterpret_cast<const double2 *>(pick(f, e) + bmember(b, nb, ms) + o);
+    double2 q = *reinterpret_cast<const double2 *>(pick(f, e) + mof(b) + o);
     if (pick(wg, e)) {
       const double2 g = *reinterpret_cast<const double2 *>(green + o);
       q = make_double2(g.x * q.x, g.y * q.y);
     }
     return make_double2(fac * q.x, fac * q.y);
   }
+  // Bulk staging (the pass is along kx, one row per vector): vector v of
+  // entry b reads row v of f (d/dx, reflected within the row) or row
+  // (n - v) mod n (d/dy), and the same row of the Green function.
+  static constexpr int NROWS = 2;
+  int *err = nullptr;
+  __device__ __forceinline__ uint32_t stage_bytes(int b, int) const {
+    return (uint32_t)n * 8u * (pick(wg, ent(b)) ? 2u : 1u);
+  }
+  __device__ __forceinline__ void stage(int b, int v, double *dst, uint64_t *bar) const {
+    const int e = ent(b);
+    const long long r = (long long)(pick(dir, e) == 0 ? v : (n - v) & (n - 1)) * n;
+    tc::bulk_g2s(dst, pick(f, e) + mof(b) + r, (uint32_t)n * 8u, bar);
+    if (pick(wg, e)) tc::bulk_g2s(dst + n, green + r, (uint32_t)n * 8u, bar);
+  }
+  __device__ __forceinline__ void fail() const {
+    if (err) atomicExch(err, CASL_ETIMEOUT);
+  }
+  // operator() on the staged rows R (f, then the Green function)
+  __device__ __forceinline__ double staged(int b, int v, int j, const double *R) const {
+    const int e = ent(b);
+    const bool dx = pick(dir, e) == 0;
+    const int nw = n >> 1;
+    const int k = dx ? j : v;
+    const int idx = dx ? (n - j) & (n - 1) : j;
+    const int hi = k < nw ? 2 * k - 1 : 2 * (n - k) - 1;
+    const double h = (dx ? hrkx : hrky)[hi < 0 ? 0 : hi];
+    const double fac = (k == 0 || k == nw) ? 0.0 : (k < nw ? -h : h);
+    const double val = R[idx];
+    return fac * (pick(wg, e) ? R[n + idx] * val : val);
+  }
 };
+using LoadDeriv = LoadDerivT<false>;
 
 // qa(iy,ix) of con2grid from the exact integer coarse cells:
 // qc = qjump*(C*n^2 - S)/(256 n^2) (+ beta field), phys layout [ix][iy].
@@ -380,37 +435,45 @@ struct StoreSource {
   }
 };
 
-// (ensemble: entry b is entry b % nb of member b / nb, fields ms apart)
-struct StoreScaled {
+// (MB: an ensemble, entry b is entry b % nb of member b / nb, fields ms apart)
+template <bool MB>
+struct StoreScaledT {
   __host__ double bytes() const { return 8.0; }
   double *p[6];
   double scale[6];
   int n;
   int nb = 6;
   long long ms = 0;
+  __device__ __forceinline__ int ent(int b) const { return MB ? b % nb : b; }
+  __device__ __forceinline__ long long mof(int b) const { return MB ? (long long)(b / nb) * ms : 0; }
   // last pass of an inverse transform: vector v = ix, element k = iy
   __device__ __forceinline__ void operator()(int b, int v, int k, double x) const {
-    const int e = bentry(b, nb, ms);
+    const int e = ent(b);
     const double sc = pick(scale, e);
-    pick(p, e)[bmember(b, nb, ms) + (long long)v * n + k] = sc == 1.0 ? x : sc * x;
+    pick(p, e)[mof(b) + (long long)v * n + k] = sc == 1.0 ? x : sc * x;
   }
   __device__ __forceinline__ void pair(int b, int v, int k, double2 x) const {
-    const int e = bentry(b, nb, ms);
+    const int e = ent(b);
     const double sc = pick(scale, e);
     if (sc != 1.0) x = make_double2(sc * x.x, sc * x.y);
-    *reinterpret_cast<double2 *>(pick(p, e) + bmember(b, nb, ms) + (long long)v * n + k) = x;
+    *reinterpret_cast<double2 *>(pick(p, e) + mof(b) + (long long)v * n + k) = x;
   }
 };
-struct LoadBatch {
+using StoreScaled = StoreScaledT<false>;
+template <bool MB>
+struct LoadBatchT {
   __host__ double bytes() const { return 8.0; }
   const double *p[6];
   long long vs, es;
   int nb = 6;
   long long ms = 0;
   __device__ __forceinline__ double operator()(int b, int v, int j) const {
-    return pick(p, bentry(b, nb, ms))[bmember(b, nb, ms) + (long long)v * vs + (long long)j * es];
+    const int e = MB ? b % nb : b;
+    const long long o = MB ? (long long)(b / nb) * ms : 0;
+    return pick(p, e)[o + (long long)v * vs + (long long)j * es];
   }
 };
+using LoadBatch = LoadBatchT<false>;
 // FP32 storage for the inverse transform pair of the FP32-inversion mode:
 // the kernel's arithmetic stays FP64 in registers; the intermediate and the
 // physical outputs are rounded to FP32 once, when stored.
@@ -966,7 +1029,7 @@ int con2grid_to_spec(casl_handle *h, double *spec) {
             1.0 / (256.0 * (double)n * (double)n), (int)n};
   rc = RFFT_DISPATCH(true, false, true, ld, (StoreStrided{spec, nn, 1, n}), M);
   if (rc) return rc;
-  return RFFT_DISPATCH(true, false, false, (LoadStrided{spec, nn, n, 1}),
+  return RFFT_DISPATCH(true, false, false, (LoadRow{spec, nn, n, (int)n, &h->scal->error}),
                        (StoreStrided{spec, nn, n, 1}), M);
 }
 
@@ -1326,7 +1389,7 @@ static int inversion_qq(casl_handle *h, bool reset) {
     // The combination runs as its own elementwise pass: inside the batch-1
     // transform's store (about 3.5 warps per SM) its extra loads were
     // exposed and the fused pass took longer than the two apart.
-    rc = RFFT_DISPATCH(true, false, false, (LoadStrided{h->qc, nn, n, 1}),
+    rc = RFFT_DISPATCH(true, false, false, (LoadRow{h->qc, nn, n, (int)n, &h->scal->error}),
                        (StoreStrided{h->qc, nn, n, 1}), M);
     if (rc) return rc;
   }
@@ -1341,14 +1404,16 @@ static int inversion_qq(casl_handle *h, bool reset) {
 
 // main_invert (spectral.f90:304-342): vv = spctop(xderiv(green*qq)),
 // uu = -spctop(yderiv(green*qq))
-static int main_invert_dev(casl_handle *h) {
+template <bool MB>
+static int main_invert_t(casl_handle *h) {
   long long nn = (long long)h->n * h->n;
   int rc;
-  LoadDeriv ld{};
+  LoadDerivT<MB> ld{};
   ld.f[0] = h->qq; ld.f[1] = h->qq;
   ld.dir[0] = 0; ld.dir[1] = 1;
   ld.wg[0] = 1; ld.wg[1] = 1;
   ld.green = h->green; ld.hrkx = h->hrkx; ld.hrky = h->hrky; ld.n = h->n;
+  ld.err = &h->scal->error;
   ld.nb = 2; ld.ms = nn;  // ensemble: two entries per member
   long long n = h->n;
   const int M = h->M;
@@ -1356,15 +1421,18 @@ static int main_invert_dev(casl_handle *h) {
   // are 2M fields long)
   rc = RFFT_DISPATCH(false, false, false, ld, (StoreStrided{h->w[0], nn, n, 1}), 2 * M);
   if (rc) return rc;
-  StoreScaled st{};
+  StoreScaledT<MB> st{};
   st.p[0] = h->vv; st.p[1] = h->uu;
   st.scale[0] = 1.0; st.scale[1] = -1.0; st.n = h->n;
   st.nb = 2; st.ms = nn;
   // second pass reads tmp[ky*n + ix] (v = ix fastest, j = ky) and writes phys [ix][iy]
-  LoadBatch lb{};
+  LoadBatchT<MB> lb{};
   lb.p[0] = h->w[0]; lb.p[1] = h->w[0] + nn; lb.vs = 1; lb.es = n;
   lb.nb = 2; lb.ms = 2 * nn;
   return RFFT_DISPATCH(false, true, false, lb, st, 2 * M);
+}
+static int main_invert_dev(casl_handle *h) {
+  return h->M > 1 ? main_invert_t<true>(h) : main_invert_t<false>(h);
 }
 
 // main_invert and the four gradients of source (evolution.f90:432-490,
@@ -1373,10 +1441,11 @@ static int main_invert_dev(casl_handle *h) {
 // sqs, sqd, as scratch for the advection products).  One batch of six fills
 // the SMs better than a batch of two beside a batch of four.  Scratch:
 // gtmp (6 fields).
-static int invert_and_gradients(casl_handle *h) {
+template <bool MB>
+static int invert_and_gradients_t(casl_handle *h) {
   long long nn = (long long)h->n * h->n, n = h->n;
   const int M = h->M;  // ensemble: six entries per member
-  LoadDeriv ld{};
+  LoadDerivT<MB> ld{};
   const double *src[6] = {h->qq, h->qq, h->qd, h->qd, h->qs, h->qs};
   for (int b = 0; b < 6; b++) {
     ld.f[b] = src[b];
@@ -1384,15 +1453,16 @@ static int invert_and_gradients(casl_handle *h) {
     ld.wg[b] = b < 2;
   }
   ld.green = h->green; ld.hrkx = h->hrkx; ld.hrky = h->hrky; ld.n = h->n;
+  ld.err = &h->scal->error;
   ld.nb = 6; ld.ms = nn;
   double *tmp = h->gtmp;  // 6M contiguous fields
   int rc = RFFT_DISPATCH(false, false, false, ld, (StoreStrided{tmp, nn, n, 1}), 6 * M);
   if (rc) return rc;
-  LoadBatch lb{};
+  LoadBatchT<MB> lb{};
   for (int b = 0; b < 6; b++) lb.p[b] = tmp + b * nn;
   lb.vs = 1; lb.es = n;
   lb.nb = 6; lb.ms = 6 * nn;
-  StoreScaled st{};
+  StoreScaledT<MB> st{};
   double *dst[6] = {h->vv, h->uu, h->w[4], h->w[5], h->sqs, h->sqd};
   for (int b = 0; b < 6; b++) {
     st.p[b] = dst[b];
@@ -1401,6 +1471,9 @@ static int invert_and_gradients(casl_handle *h) {
   st.n = h->n;
   st.nb = 6; st.ms = nn;
   return RFFT_DISPATCH(false, true, false, lb, st, 6 * M);
+}
+static int invert_and_gradients(casl_handle *h) {
+  return h->M > 1 ? invert_and_gradients_t<true>(h) : invert_and_gradients_t<false>(h);
 }
 
 // The same batch-6 inverse pair with FP32 storage (CASL_PREC_FP32_INVERSION):
@@ -1416,6 +1489,7 @@ static int invert_and_gradients32(casl_handle *h) {
     ld.wg[b] = b < 2;
   }
   ld.green = h->green; ld.hrkx = h->hrkx; ld.hrky = h->hrky; ld.n = h->n;
+  ld.err = &h->scal->error;
   float *tmp = reinterpret_cast<float *>(h->gtmp);  // 6 contiguous FP32 fields
   int rc = RFFT_DISPATCH(false, false, false, ld, (StoreStridedF{tmp, nn, n, 1}), 6);
   if (rc) return rc;
@@ -1497,7 +1571,7 @@ static int source_prod(casl_handle *h, int stage) {
   ss.rekman = h->p.rekman; ss.kdsq = h->c.kdsq; ss.therm = h->c.therm;
   ss.heating = h->c.heating; ss.friction = h->c.friction; ss.lev = lev; ss.n = h->n;
   ss.ms = nn;
-  return RFFT_DISPATCH(true, false, false, (LoadStrided{tmp, nn, n, 1}), ss, 2 * h->M);
+  return RFFT_DISPATCH(true, false, false, (LoadRow{tmp, nn, n, (int)n, &h->scal->error}), ss, 2 * h->M);
 }
 
 }  // namespace casl
@@ -1653,7 +1727,7 @@ int judge_velocity(casl_handle *h, casl_handle *hf, double *uJ, double *vJ, doub
       casl_handle *h = hh;  // RFFT_DISPATCH launches on h's stream at h's size
       if ((rc = RFFT_DISPATCH(true, false, true, ld, (StoreStrided{h->qc, nnf, 1, (long long)nf}), 1)))
         return rc;
-      if ((rc = RFFT_DISPATCH(true, false, false, (LoadStrided{h->qc, nnf, (long long)nf, 1}),
+      if ((rc = RFFT_DISPATCH(true, false, false, (LoadRow{h->qc, nnf, (long long)nf, nf, &h->scal->error}),
                               (StoreStrided{h->qc, nnf, (long long)nf, 1}), 1)))
         return rc;
     }
@@ -2190,7 +2264,7 @@ static void free_all(casl_handle *h) {
                   h->vv, h->emq, h->epq, h->qspre, h->sqs, h->sqd, h->qsi, h->qsf, h->qdi,
                   h->qdf, h->green, h->flo, h->fhi, h->qdiss, h->w[0], h->hrkx, h->hrky,
                   h->bety, h->betac, h->tw, h->fineJ, h->ljx, h->coarseC, h->part, h->scal,
-                  h->sx, h->sx2, h->shell_idx, h->shell_off, h->rkxf, h->rkyf, h->gtmp};
+                  h->sx, h->sx2, h->sxe, h->shell_idx, h->shell_off, h->rkxf, h->rkyf, h->gtmp};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (h->mnode) cudaFree(h->mnode);
@@ -2616,6 +2690,7 @@ int casl_main_invert(casl_handle *h, const double *qq, double *uu, double *vv, d
   ld.f[0] = q; ld.f[1] = q; ld.dir[0] = 0; ld.dir[1] = 1;
   ld.wg[0] = 1; ld.wg[1] = 1;
   ld.green = h->green; ld.hrkx = h->hrkx; ld.hrky = h->hrky; ld.n = h->n;
+  ld.err = &h->scal->error;
   int rc = RFFT_DISPATCH(false, false, false, ld, (StoreStrided{h->w[0], (long long)nn, n, 1}), 2);
   if (rc) return rc;
   StoreScaled st{};
@@ -2645,6 +2720,7 @@ int casl_gradient(casl_handle *h, const double *ff, double *ffx, double *ffy) {
   LoadDeriv ld{};
   ld.f[0] = f; ld.f[1] = f; ld.dir[0] = 0; ld.dir[1] = 1;
   ld.green = nullptr; ld.hrkx = h->hrkx; ld.hrky = h->hrky; ld.n = h->n;
+  ld.err = &h->scal->error;
   int rc = RFFT_DISPATCH(false, false, false, ld, (StoreStrided{h->w[0], (long long)nn, n, 1}), 2);
   if (rc) return rc;
   StoreScaled st{};

@@ -142,7 +142,7 @@ static int member_ranges_host(casl_handle *h) {
 // scratch of its own, sized for the largest member seen so far.
 static void view_free(casl_handle *v) {
   if (!v) return;
-  void *ps[] = {v->xq, v->yq, v->nextq, v->i1q, v->i2q, v->npq, v->indq, v->scal, v->sx, v->sx2};
+  void *ps[] = {v->xq, v->yq, v->nextq, v->i1q, v->i2q, v->npq, v->indq, v->scal, v->sx, v->sx2, v->sxe};
   for (void *p : ps) cudaFree(p);
   if (v->hscal) cudaFreeHost(v->hscal);
   free(v);

@@ -21,6 +21,8 @@
 #include <type_traits>
 
 #include "common.cuh"
+#include "hydra_casl.h"
+#include "tc.cuh"
 
 namespace casl {
 
@@ -99,15 +101,6 @@ __device__ __forceinline__ T pick(const T (&a)[N], int b) {
   return r;
 }
 
-// Batch entry b of an ensemble transform is entry b % nb of member b / nb,
-// whose fields lie ms elements after the previous member's.  One member
-// (ms = 0, b < nb) takes the branch without the integer division, which
-// would otherwise run for every element the functor loads or stores.
-__device__ __forceinline__ int bentry(int b, int nb, long long ms) { return ms ? b % nb : b; }
-__device__ __forceinline__ long long bmember(int b, int nb, long long ms) {
-  return ms ? (long long)(b / nb) * ms : 0;
-}
-
 // Plain strided load / store functors: element (b, v, j) at p[b*bs + v*vs + j*es].
 struct LoadStrided {
   __host__ double bytes() const { return 8.0; }
@@ -121,6 +114,28 @@ struct LoadStrided {
     if (es == 1) return *reinterpret_cast<const double2 *>(p + o);
     return make_double2(p[o], p[o + es]);
   }
+};
+// A contiguous row per vector, element (b, v, j) at p[b*bs + v*vs + j]: the
+// plain load of a pass whose load side is element-contiguous, staged in
+// shared memory by one bulk copy per vector (see has_rows below).
+struct LoadRow {
+  __host__ double bytes() const { return 8.0; }
+  const double *p;
+  long long bs, vs;
+  int n;
+  int *err = nullptr;
+  static constexpr int NROWS = 1;
+  __device__ __forceinline__ double operator()(int b, int v, int j) const {
+    return p[b * bs + (long long)v * vs + j];
+  }
+  __device__ __forceinline__ uint32_t stage_bytes(int, int) const { return (uint32_t)n * 8u; }
+  __device__ __forceinline__ void stage(int b, int v, double *dst, uint64_t *bar) const {
+    tc::bulk_g2s(dst, p + b * bs + (long long)v * vs, (uint32_t)n * 8u, bar);
+  }
+  __device__ __forceinline__ void fail() const {
+    if (err) atomicExch(err, CASL_ETIMEOUT);
+  }
+  __device__ __forceinline__ double staged(int, int, int j, const double *R) const { return R[j]; }
 };
 struct StoreStrided {
   __host__ double bytes() const { return 8.0; }
@@ -248,6 +263,25 @@ __device__ __forceinline__ void rf_complex(double2 (&x)[8], double2 *S, int t,
   if (Sh::REM == 1) rf_butterflies<2, FWD, Sh::TPV>(x, t, Ns, tw, n);
 }
 
+// A load functor with a static member NROWS (1 or 2) stages its input rows
+// in shared memory by bulk copies instead of loading elements one by one: in
+// a pass whose load side is element-contiguous, vector v of batch entry b
+// reads NROWS rows of n doubles, which stage(b, v, dst, bar) copies to dst
+// (NROWS * n doubles) against the barrier, returning the bytes it copies;
+// staged(b, v, j, rows) then gives element j from them.  The copies put a
+// whole vector's input in flight at once without holding registers, where
+// element loads left the pass bound by load latency.  A copy that does not
+// arrive in about a second is reported through fail().
+template <class T, class = void>
+struct has_rows : std::false_type {};
+template <class T>
+struct has_rows<T, std::void_t<decltype(T::NROWS)>> : std::true_type {};
+template <class LD, bool LVF>
+constexpr int staged_rows() {
+  if constexpr (has_rows<LD>::value && !LVF) return LD::NROWS;
+  else return 0;
+}
+
 // A load or store functor may ask for fewer CTAs per SM (more registers)
 // through a static member `wide`: the derivative load keeps 80 registers,
 // where 64 would spill.
@@ -260,6 +294,21 @@ constexpr int rfft_minb() {
   using Sh = RfftShape<LOGH, VF>;
   return (wants_wide<LD>::value || wants_wide<ST>::value) ? (768 / Sh::NT > 0 ? 768 / Sh::NT : 1)
                                                           : Sh::MINB;
+}
+
+// Shared memory of a pass: the exchange (and forward staging) regions, or
+// the staged input rows over them where larger, then the staging barrier.
+template <int LOGH, bool FWD, bool LVF, bool SVF, int NR>
+constexpr size_t rfft_bar_offset() {
+  using Sh = RfftShape<LOGH, LVF || SVF>;
+  const size_t ex = Sh::smem(FWD && SVF);
+  const size_t rows = (size_t)Sh::V * NR * Sh::N * sizeof(double);
+  return ((ex > rows ? ex : rows) + 15) / 16 * 16;
+}
+template <int LOGH, bool FWD, bool LVF, bool SVF, int NR>
+constexpr size_t rfft_smem() {
+  using Sh = RfftShape<LOGH, LVF || SVF>;
+  return NR ? rfft_bar_offset<LOGH, FWD, LVF, SVF, NR>() + 16 : Sh::smem(FWD && SVF);
 }
 
 template <int LOGH, bool FWD, bool LVF, bool SVF, class LD, class ST>
@@ -277,6 +326,33 @@ __global__ void __launch_bounds__(RfftShape<LOGH, LVF || SVF>::NT,
   double2 *S = smem + vl * VS;
   double *SdV = Sd + 2 * vl * VS;
   double2 x[8];
+
+  // Bulk-staged contiguous input: this CTA's V vectors' rows at the start
+  // of shared memory, over the exchange (and forward staging) regions, which
+  // are first written after every thread has read its inputs; the barrier
+  // after both.
+  constexpr int NR = staged_rows<LD, LVF>();
+  [[maybe_unused]] const double *Rw = nullptr;
+  if constexpr (NR > 0) {
+    double *R0 = Sd;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(
+        reinterpret_cast<unsigned char *>(smem) + rfft_bar_offset<LOGH, FWD, LVF, SVF, NR>());
+    Rw = R0 + vl * NR * N;
+    if (threadIdx.x == 0) {
+      tc::mbar_init(bar, 1);
+      tc::mbar_fence_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t bytes = 0;
+#pragma unroll 1
+      for (int q = 0; q < V; q++) bytes += ld.stage_bytes(b, v0 + q);
+      tc::mbar_expect_tx(bar, bytes);
+#pragma unroll 1
+      for (int q = 0; q < V; q++) ld.stage(b, v0 + q, R0 + q * NR * N, bar);
+    }
+    if (!tc::mbar_wait(bar, 0) && threadIdx.x == 0) ld.fail();
+  }
 
   // Vector-fastest input: stage V vectors, lanes over vectors (16 values per
   // thread, loaded 8 at a time).
@@ -308,11 +384,14 @@ __global__ void __launch_bounds__(RfftShape<LOGH, LVF || SVF>::NT,
 #pragma unroll
       for (int m = 0; m < 8; m++) {
         int e = t + m * TPV;
-        if constexpr (has_pair<LD>::value)
+        if constexpr (NR > 0)
+          x[m] = make_double2(ld.staged(b, vg, 2 * e, Rw), ld.staged(b, vg, 2 * e + 1, Rw));
+        else if constexpr (has_pair<LD>::value)
           x[m] = ld.pair(b, vg, 2 * e);
         else
           x[m] = make_double2(ld(b, vg, 2 * e), ld(b, vg, 2 * e + 1));
       }
+      if constexpr (NR > 0) __syncthreads();  // rows read before the slots overwrite them
     }
     rf_complex<LOGH, true>(x, S, t, tw, N);
     // untangle: pairs (k, H-k) live in threads t and TPV-t, so exchange once
@@ -362,7 +441,10 @@ __global__ void __launch_bounds__(RfftShape<LOGH, LVF || SVF>::NT,
   } else {
     // Hermitian -> Z (even/odd packing): thread t forms Z at k and H-k for
     // k = t + m*TPV (m < 4), thread 0 also k = H/2.
-    auto X = [&](int j) -> double { return LVF ? SdV[dpos(j)] : ld(b, vg, j); };
+    auto X = [&](int j) -> double {
+      if constexpr (NR > 0) return ld.staged(b, vg, j, Rw);
+      else return LVF ? SdV[dpos(j)] : ld(b, vg, j);
+    };
     double2 zp[9];
     int zk[9];
 #pragma unroll
@@ -404,7 +486,7 @@ __global__ void __launch_bounds__(RfftShape<LOGH, LVF || SVF>::NT,
       zk[8] = -1;
       zp[8] = make_double2(0.0, 0.0);
     }
-    if (LVF) __syncthreads();  // staged input fully read before Z overwrites it
+    if (LVF || NR > 0) __syncthreads();  // staged input fully read before Z overwrites it
 #pragma unroll
     for (int q = 0; q < 9; q++)
       if (zk[q] >= 0) S[cpad(zk[q])] = zp[q];

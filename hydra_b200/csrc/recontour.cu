@@ -15,6 +15,13 @@
 // 4. Each contour starts at its lowest-numbered crossing (the reference's
 //    `free` loop); contours are ordered by level then by that crossing,
 //    gathered into walk order and renoded three times (congen.f90:295-310).
+// With beta != 0 the PV is not periodic in y and recontouring follows
+// econgen.f90 (the reference's ecaps build) instead: the level range and the
+// rows iymin..iymax that it needs come from the field's row extremes, the
+// rows outside the basic box are its periodic images offset by beta*Ly per
+// box, crossings are enumerated over that extended grid in econgen's order,
+// and of the traced contours only one periodic image each is kept, its y
+// folded back into the box, before the renodes.
 #include <cub/device/device_radix_sort.cuh>
 #include <math.h>
 #include <stdio.h>
@@ -177,6 +184,7 @@ struct UField {
   const double *qq;
   double qjump;
   int have;
+  double bnc;  // beta != 0 without contours: beta*ygu(iy) is added (econgen.f90:94-110)
 };
 __device__ __forceinline__ double ufield_at(const UField &u, double qavg, int ix, int iy,
                                             const Consts &c) {
@@ -189,7 +197,8 @@ __device__ __forceinline__ double ufield_at(const UField &u, double qavg, int ix
   const double q01 = u.qq[(long long)(ix1 - 1) * n + iy0 - 1];
   const double q11 = u.qq[(long long)(ix1 - 1) * n + iy1 - 1];
   const int lv = u.have ? u.L[(long long)(ix - 1) * c.nyu + iy - 1] : 0;
-  return ufield_elem(lv, ixf, iyf, q00, q10, q01, q11, u.qjump, qavg, u.have);
+  const double v = ufield_elem(lv, ixf, iyf, q00, q10, q01, q11, u.qjump, qavg, u.have);
+  return u.bnc != 0.0 ? v + u.bnc * (c.ymin + c.glyu * (double)(iy - 1)) : v;
 }
 
 // The ultra-fine field, one thread per run of 16 rows of a column: the run
@@ -201,7 +210,7 @@ __device__ __forceinline__ double ufield_at(const UField &u, double qavg, int ix
 __global__ void k_u_field(const int *__restrict__ L, const unsigned long long *__restrict__ lsum,
                           const double *__restrict__ qq, double qjump, int have_contours,
                           LevInfo lq, double *__restrict__ qa, unsigned short *__restrict__ lc,
-                          double *__restrict__ part, Consts c) {
+                          double *__restrict__ part, Consts c, double bnc) {
   CASL_PDL_ENTRY();
   const int nxu = c.nxu, nyu = c.nyu, n = c.nx;
   const long long nruns = (long long)nxu * (nyu / 16);
@@ -234,8 +243,9 @@ __global__ void k_u_field(const int *__restrict__ L, const unsigned long long *_
       double out[2];
 #pragma unroll
       for (int h = 0; h < 2; h++) {
-        const double v = ufield_elem(lv[2 * k + h], ixf, 2 * k + h + 1, q00, q10, q01, q11, qjump,
-                                     qavg, have_contours);
+        double v = ufield_elem(lv[2 * k + h], ixf, 2 * k + h + 1, q00, q10, q01, q11, qjump,
+                               qavg, have_contours);
+        if (bnc != 0.0) v = v + bnc * (c.ymin + c.glyu * (double)(16 * iyy + 2 * k + h));
         out[h] = v;
         mx = fmax(mx, v);
         mn = fmin(mn, v);
@@ -403,6 +413,261 @@ __global__ void k_cr_geom(UField uf, const unsigned long long *__restrict__ redg
       double xx = xgu - c.glxu * q0 / (q1 - q0);
       xcr[r] = c.oms * (xx - c.ellx * f_dint(xx * c.hlxi));
     }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// beta != 0 (econgen.f90:27-488): the grid extended in y
+// ---------------------------------------------------------------------------
+// PV on a beta-plane is not periodic in y: the periodic image of row iy0 one
+// box up carries an extra beta*Ly.  The field is extended over rows
+// iymin..iymax, row iy taking the values of basic row iy0 = 1 + mod(iy-1,
+// nyu) plus bfac*(iy - iy0), bfac = beta*glyu; contours are traced on the
+// extended grid and only one periodic image of each is kept.
+struct ExtGrid {
+  int iymin, iymax, nby;       // nby: boxes below the basic one (econgen.f90:217)
+  double bfac;
+  const unsigned short *lc;    // basic rows' level codes, [ix][iy]
+  const unsigned short *lcb;   // rows iymin..0, [ix][iy - iymin]
+  const unsigned short *lca;   // rows nyu+1..iymax, [ix][iy - nyu - 1]
+};
+__device__ __forceinline__ int ext_row0(const ExtGrid &g, int iy, int nyu) {
+  return iy < 1 ? 1 + (g.nby * nyu + iy - 1) % nyu : (iy > nyu ? 1 + (iy - 1) % nyu : iy);
+}
+// level code of the 1-based point (ix, iy) of the extended grid
+__device__ __forceinline__ int ext_code(const ExtGrid &g, int ix, int iy, int nyu) {
+  if (iy < 1) return g.lcb[(long long)(ix - 1) * (1 - g.iymin) + (iy - g.iymin)];
+  if (iy > nyu) return g.lca[(long long)(ix - 1) * (g.iymax - nyu) + (iy - nyu - 1)];
+  return g.lc[(long long)(ix - 1) * nyu + iy - 1];
+}
+
+// Minimum and maximum of the field along every basic row (econgen.f90:
+// 114-129): one block per 16 rows, threads over the columns.
+__global__ void __launch_bounds__(256) k_u_rowmm(UField uf, Consts c, double *__restrict__ rmin,
+                                                 double *__restrict__ rmax) {
+  CASL_PDL_ENTRY();
+  const int nxu = c.nxu, nyu = c.nyu;
+  const double qavg = ufield_qavg(uf.lsum, uf.qjump, uf.have, nxu, nyu);
+  const int r0 = 16 * blockIdx.x;
+  double mn[16], mx[16];
+#pragma unroll
+  for (int k = 0; k < 16; k++) {
+    mn[k] = 1.0e308;
+    mx[k] = -1.0e308;
+  }
+  for (int ix = threadIdx.x + 1; ix <= nxu; ix += blockDim.x) {
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+      const double v = ufield_at(uf, qavg, ix, r0 + k + 1, c);
+      mn[k] = fmin(mn[k], v);
+      mx[k] = fmax(mx[k], v);
+    }
+  }
+  __shared__ double smn[8][16], smx[8][16];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 16; k++) {
+    double a = mn[k], b = mx[k];
+    for (int o = 16; o > 0; o >>= 1) {
+      a = fmin(a, __shfl_xor_sync(0xffffffffu, a, o));
+      b = fmax(b, __shfl_xor_sync(0xffffffffu, b, o));
+    }
+    if (lane == 0) {
+      smn[w][k] = a;
+      smx[w][k] = b;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 16 && r0 + threadIdx.x < nyu) {
+    double a = smn[0][threadIdx.x], b = smx[0][threadIdx.x];
+    for (int q = 1; q < (int)(blockDim.x >> 5); q++) {
+      a = fmin(a, smn[q][threadIdx.x]);
+      b = fmax(b, smx[q][threadIdx.x]);
+    }
+    rmin[r0 + threadIdx.x] = a;
+    rmax[r0 + threadIdx.x] = b;
+  }
+}
+
+// Level codes of the extension rows: the level index of qa(iy0) +
+// bfac*(iy - iy0), the value rounded once as the reference's x-line scan
+// forms it (econgen.f90:247-258).
+__global__ void k_u_ext(UField uf, ExtGrid g, LevInfo li, Consts c, unsigned short *__restrict__ lcb,
+                        unsigned short *__restrict__ lca) {
+  CASL_PDL_ENTRY();
+  const int nxu = c.nxu, nyu = c.nyu;
+  const int nb = 1 - g.iymin, na = g.iymax - nyu, nr = nb + na;
+  const double qavg = ufield_qavg(uf.lsum, uf.qjump, uf.have, nxu, nyu);
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)nxu * nr;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int ix = (int)(t / nr) + 1, r = (int)(t % nr);
+    const int iy = r < nb ? g.iymin + r : nyu + 1 + (r - nb);
+    const int iy0 = ext_row0(g, iy, nyu);
+    const double v = ufield_at(uf, qavg, ix, iy0, c) + g.bfac * (double)(iy - iy0);
+    const unsigned short code = (unsigned short)min(max(level_index(v, li), 0), 65535);
+    if (r < nb) lcb[(long long)(ix - 1) * nb + r] = code;
+    else lca[(long long)(ix - 1) * na + (r - nb)] = code;
+  }
+}
+
+// Crossings of the extended grid, counted or emitted per chunk of 16 edges
+// in the reference's numbering (econgen.f90:238-348): x-line edges (ix, iy)
+// -(ix, iy+1) for iy = iymin..iymax-1, e = (ix-1)(nye-1) + iy - iymin; then
+// y-line edges (ix, iy)-(ix+1, iy) for iy = iymin+1..iymax-1,
+// e = NEX + (iy-iymin-1) nxu + ix-1.  An edge crosses the levels between its
+// ends' codes (the y lines of the extension use the same once-rounded
+// values; the reference adds (offset - qtmp) there, which can differ from
+// them only when qa lies within an ulp of a level).
+template <bool EMIT>
+__global__ void k_cre(ExtGrid g, LevInfo li, int nxu, int nyu, long long nedge, long long nex,
+                      int *__restrict__ cnt, const int *__restrict__ off,
+                      unsigned long long *__restrict__ redge, int *__restrict__ rlev) {
+  CASL_PDL_ENTRY();
+  const int nye = g.iymax - g.iymin + 1;
+  const long long nchunks = (nedge + EDGES_PER_THREAD - 1) / EDGES_PER_THREAD;
+  for (long long ch = blockIdx.x * (long long)blockDim.x + threadIdx.x; ch < nchunks;
+       ch += (long long)gridDim.x * blockDim.x) {
+    const long long e0 = ch * EDGES_PER_THREAD;
+    const long long e1 = e0 + EDGES_PER_THREAD < nedge ? e0 + EDGES_PER_THREAD : nedge;
+    int pos = EMIT ? off[ch] : 0, total = 0;
+    for (long long e = e0; e < e1; e++) {
+      int ca, cb;
+      if (e < nex) {
+        const int ix = (int)(e / (nye - 1)) + 1, iy = g.iymin + (int)(e % (nye - 1));
+        ca = ext_code(g, ix, iy, nyu);
+        cb = ext_code(g, ix, iy + 1, nyu);
+      } else {
+        const long long f = e - nex;
+        const int iy = g.iymin + 1 + (int)(f / nxu), ix = (int)(f % nxu) + 1;
+        ca = ext_code(g, ix, iy, nyu);
+        cb = ext_code(g, ix == nxu ? 1 : ix + 1, iy, nyu);
+      }
+      const int l1 = max(min(ca, cb) + 1, li.levbeg), l2 = min(max(ca, cb), li.levend);
+      if (!EMIT) {
+        total += l2 >= l1 ? l2 - l1 + 1 : 0;
+      } else {
+        for (int l = l1; l <= l2; l++) {
+          redge[pos] = (unsigned long long)e;
+          rlev[pos] = l - li.levbeg;
+          pos++;
+        }
+      }
+    }
+    if (!EMIT) cnt[ch] = total;
+  }
+}
+
+// Position and box transitions of every crossing of the extended grid
+// (econgen.f90:238-348): y is not folded here; boxes are numbered over the
+// extended grid, row by row from iymin (1-based, as the reference's).
+__global__ void k_cre_geom(UField uf, ExtGrid g, const unsigned long long *__restrict__ redge,
+                           const int *__restrict__ rlev, long long ncr, long long nex, LevInfo li,
+                           Consts c, double *__restrict__ xcr, double *__restrict__ ycr,
+                           unsigned int *__restrict__ kib, unsigned int *__restrict__ kob) {
+  CASL_PDL_ENTRY();
+  const int nxu = c.nxu, nyu = c.nyu, nye = g.iymax - g.iymin + 1;
+  const double qavg = ufield_qavg(uf.lsum, uf.qjump, uf.have, nxu, nyu);
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
+       r += (long long)gridDim.x * blockDim.x) {
+    const long long e = (long long)redge[r];
+    const double qtmp = qtmp_of(rlev[r] + li.levbeg, li);
+    if (e < nex) {
+      const int ix = (int)(e / (nye - 1)) + 1, iy = g.iymin + (int)(e % (nye - 1));
+      double q[2];
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int yy = iy + h, y0 = ext_row0(g, yy, nyu);
+        const double v = (yy >= 1 && yy <= nyu)
+                             ? ufield_at(uf, qavg, ix, yy, c)
+                             : ufield_at(uf, qavg, ix, y0, c) + g.bfac * (double)(yy - y0);
+        q[h] = v - qtmp;
+      }
+      const int isy = (int)f_sign1(q[0]);
+      const int inc = (1 - isy) / 2;
+      const long long kaa = (long long)(iy - g.iymin) * nxu + 1;
+      const int j1 = ix + inc, j2 = ix + 1 - inc;
+      const long long bx1 = j1 == 1 ? nxu - 1 : j1 - 2, bx2 = j2 == 1 ? nxu - 1 : j2 - 2;
+      kib[r] = (unsigned int)(kaa + bx1);
+      kob[r] = (unsigned int)(kaa + bx2);
+      xcr[r] = c.xmin + c.glxu * (double)(ix - 1);
+      ycr[r] = (c.glyu * (double)(iy - 1) + c.ymin) - c.glyu * q[0] / (q[1] - q[0]);
+    } else {
+      const long long f = e - nex;
+      const int iy = g.iymin + 1 + (int)(f / nxu), ix = (int)(f % nxu) + 1;
+      const int y0 = ext_row0(g, iy, nyu);
+      const bool basic = iy >= 1 && iy <= nyu;
+      const double qadd = g.bfac * (double)(iy - y0) - qtmp;
+      double q[2];
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int xx = h == 0 ? ix : (ix == nxu ? 1 : ix + 1);
+        q[h] = basic ? ufield_at(uf, qavg, xx, iy, c) - qtmp : ufield_at(uf, qavg, xx, y0, c) + qadd;
+      }
+      const int isx = (int)f_sign1(q[0]);
+      const int inc = (1 - isx) / 2;
+      const long long kaa = (long long)(iy - 1 - g.iymin) * nxu + ix;
+      kib[r] = (unsigned int)(kaa + (long long)(1 - inc) * nxu);
+      kob[r] = (unsigned int)(kaa + (long long)inc * nxu);
+      ycr[r] = c.glyu * (double)(iy - 1) + c.ymin;
+      const double xgu = c.xmin + c.glxu * (double)(ix - 1);
+      const double xx = xgu - c.glxu * q[0] / (q[1] - q[0]);
+      xcr[r] = c.oms * (xx - c.ellx * f_dint(xx * c.hlxi));
+    }
+  }
+}
+
+// One periodic image per contour (econgen.f90:238-246): bit 0 of flags[k]
+// is set when a crossing of contour k lies below ymin, bit 1 when one lies
+// below ymax; k is kept when bit 0 is clear and bit 1 set.
+__global__ void k_ec_flags(const double *__restrict__ yw, const int *__restrict__ cidw, long long N,
+                           Consts c, int *__restrict__ flags) {
+  CASL_PDL_ENTRY();
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < N;
+       w += (long long)gridDim.x * blockDim.x) {
+    const double y = yw[w];
+    const int f = (y < c.ymin ? 1 : 0) | (y < c.ymax ? 2 : 0);
+    if (f) atomicOr(&flags[cidw[w]], f);
+  }
+}
+__global__ void k_ec_keep(const int *__restrict__ flags, const int *__restrict__ clen, int C,
+                          int *__restrict__ klen, int *__restrict__ kone) {
+  CASL_PDL_ENTRY();
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < C; k += gridDim.x * blockDim.x) {
+    const bool keep = !(flags[k] & 1) && (flags[k] & 2);
+    klen[k] = keep ? clen[k] : 0;
+    kone[k] = keep ? 1 : 0;
+  }
+}
+// The kept contours' crossings, y folded into [ymin, ymax) by
+// mod(y + yoff, elly) + ymin (econgen.f90:249-252), and their contour list.
+__global__ void k_ec_compact(const double *__restrict__ xw, const double *__restrict__ yw,
+                             const int *__restrict__ cidw, long long N, const int *__restrict__ coff,
+                             const int *__restrict__ klen, const int *__restrict__ koff,
+                             const int *__restrict__ kidx, Consts c, double yoff,
+                             double *__restrict__ xw2, double *__restrict__ yw2,
+                             int *__restrict__ cidw2) {
+  CASL_PDL_ENTRY();
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < N;
+       w += (long long)gridDim.x * blockDim.x) {
+    const int k = cidw[w];
+    if (!klen[k]) continue;
+    const long long d = koff[k] + (w - coff[k]);
+    xw2[d] = xw[w];
+    yw2[d] = fmod(yw[w] + yoff, c.elly) + c.ymin;
+    cidw2[d] = kidx[k];
+  }
+}
+__global__ void k_ec_contours(const int *__restrict__ clen, const int *__restrict__ clevt, int C,
+                              const int *__restrict__ klen, const int *__restrict__ koff,
+                              const int *__restrict__ kidx, int *__restrict__ cs2,
+                              int *__restrict__ len2, int *__restrict__ lev2) {
+  CASL_PDL_ENTRY();
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < C; k += gridDim.x * blockDim.x) {
+    if (!klen[k]) continue;
+    const int j = kidx[k];
+    cs2[j] = koff[k];
+    len2[j] = clen[k];
+    lev2[j] = clevt[k];
   }
 }
 
@@ -916,11 +1181,20 @@ static int fetch_err(casl_handle *h) {
 int recontour_dev(casl_handle *h, const double *qq) {
   cudaStream_t st = h->stream;
   const Consts &c = h->c;
-  if (c.beffect) return CASL_EUNSUPPORTED;  // beta != 0 uses econgen.f90
   const int nxu = c.nxu, nyu = c.nyu;
   const long long NU = (long long)nxu * nyu;
   const double qjump = h->qjump;
   const int have = h->nptq > 0 && h->nq > 0;
+  // beta != 0 recontours as econgen.f90 does (the reference's ecaps build):
+  // beta*Ly must be a whole number of contour intervals (econgen.f90:52-60,
+  // where the reference stops)
+  const bool econ = c.beffect != 0;
+  const double bfac = c.beta * c.glyu, ppvdif = c.beta * c.elly;
+  if (econ) {
+    const double brat = ppvdif * (1.0 / qjump);
+    if (!(fabs(brat - (double)llround(brat)) <= 1.0e-7)) return CASL_EINVAL;
+  }
+  const double bnc = econ && !have ? c.beta : 0.0;
   cudaMemsetAsync(&h->scal->error, 0, sizeof(int), st);
   Trace tr;
   tr.begin(st, "start");
@@ -930,7 +1204,7 @@ int recontour_dev(casl_handle *h, const double *qq) {
   } flush_at_exit{tr};
 
   // --- 1. ultra-fine field ---------------------------------------------------
-  if (!have) {
+  if (!have && !econ) {
     // l1norm (generic.f90:180-194) of the full field: nothing to contour if ~0
     std::vector<double> hq((size_t)c.nx * c.ny);
     CASL_CUDA_TRY(cudaMemcpyAsync(hq.data(), qq, hq.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -951,7 +1225,7 @@ int recontour_dev(casl_handle *h, const double *qq) {
   // kept for the whole call.
   const long long nchunks_f = (2 * NU + EDGES_PER_THREAD - 1) / EDGES_PER_THREAD;
   size_t need_field = (size_t)NU * 6 + (size_t)nchunks_f * 8 + (size_t)nxu * 4 +
-                      ((size_t)64 << 20);
+                      (size_t)nyu * 16 + ((size_t)64 << 20);
   RC_TRY(ensure_scratch(h, need_field));
   Arena ar{(char *)h->sx, h->sx_bytes, 0};
   unsigned short *lc = ar.get<unsigned short>(NU);
@@ -959,6 +1233,8 @@ int recontour_dev(casl_handle *h, const double *qq) {
   int *ljx = ar.get<int>(nxu);
   unsigned long long *lsum = ar.get<unsigned long long>(4);
   double *part = ar.get<double>(2 * 4096);
+  double *rmn = ar.get<double>(nyu), *rmx = ar.get<double>(nyu);
+  int *dtot = ar.get<int>(16);
   if (ar.failed) return CASL_ENOMEM;
   if (have) {
     CASL_CUDA_TRY(cudaMemsetAsync(Lu, 0, (size_t)NU * sizeof(int), st));
@@ -979,7 +1255,7 @@ int recontour_dev(casl_handle *h, const double *qq) {
   li.qoff = qjump * (double)h->p.nlevm;
   li.levbeg = li.levend = 0;
   const int fb = 4096;
-  CASL_K(k_u_field, fb, 256, 0, st)(Lu, lsum, qq, qjump, have, li, nullptr, lc, part, c);
+  CASL_K(k_u_field, fb, 256, 0, st)(Lu, lsum, qq, qjump, have, li, nullptr, lc, part, c, bnc);
   RC_TRY(check_launch(h));
   RC_TRY(fetch_err(h));
   std::vector<double> hp(2 * fb);
@@ -991,7 +1267,53 @@ int recontour_dev(casl_handle *h, const double *qq) {
     qamin = std::min(qamin, hp[2 * b + 1]);
   }
   tr.point("field");
-  // --- 2. levels (congen.f90:156-173) ----------------------------------------
+  const UField uf{have ? Lu : nullptr, lsum, qq, qjump, have, bnc};
+  // beta != 0: the extent of the y-extended grid (econgen.f90:112-171), on
+  // the host from the rows' minima and maxima
+  ExtGrid eg{};
+  if (econ) {
+    CASL_K(k_u_rowmm, nyu / 16, 256, 0, st)(uf, c, rmn, rmx);
+    std::vector<double> qqmin(nyu + 2), qqmax(nyu + 2);
+    CASL_CUDA_TRY(cudaMemcpyAsync(qqmin.data() + 1, rmn, nyu * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CASL_CUDA_TRY(cudaMemcpyAsync(qqmax.data() + 1, rmx, nyu * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CASL_CUDA_TRY(cudaStreamSynchronize(st));
+    qqmin[nyu + 1] = qqmin[1] + ppvdif;
+    qqmax[nyu + 1] = qqmax[1] + ppvdif;
+    qamin = qqmin[1];
+    qamax = qqmax[1];
+    for (int iy = 2; iy <= nyu + 1; iy++) {
+      qamin = std::min(qamin, qqmin[iy]);
+      qamax = std::max(qamax, qqmax[iy]);
+    }
+    // the lowest and highest rows that meet a level of the basic box; the
+    // reference assumes fewer than 100 periodic boxes
+    const int levmin = (int)(qamin * li.qjumpi - 0.5);
+    double qlev = ((double)levmin + 0.5) * qjump;
+    int iy = 1;
+    for (;;) {
+      iy = iy - 1;
+      if (iy < -100 * nyu) return CASL_ECAPACITY;
+      const int iy0 = 1 + (100 * nyu + iy - 1) % nyu;
+      if (bfac * (double)(iy - iy0) + qqmax[iy0] <= qlev) break;
+    }
+    eg.iymin = iy;
+    const int levmax = (int)(qamax * li.qjumpi + 0.5);
+    qlev = ((double)levmax - 0.5) * qjump;
+    iy = nyu + 1;
+    for (;;) {
+      iy = iy + 1;
+      if (iy > 101 * nyu) return CASL_ECAPACITY;
+      const int iy0 = 1 + (iy - 1) % nyu;
+      if (bfac * (double)(iy - iy0) + qqmin[iy0] >= qlev) break;
+    }
+    eg.iymax = iy;
+    eg.nby = 1 - eg.iymin / nyu;
+    eg.bfac = bfac;
+    eg.lc = lc;
+    // box numbers of the extended grid are 32-bit
+    if ((long long)nxu * (eg.iymax - eg.iymin + 2) >= (1LL << 32)) return CASL_ECAPACITY;
+  }
+  // --- 2. levels (congen.f90:156-173; econgen.f90:131-134) -------------------
   li.levbeg = (int)((li.qoff + qamin) * li.qjumpi + 0.5) + 1;
   li.levend = (int)((li.qoff + qamax) * li.qjumpi + 0.5);
   // the level codes hold 0..65535: levels must lie inside
@@ -1008,15 +1330,48 @@ int recontour_dev(casl_handle *h, const double *qq) {
 
   tr.point("levels");
   // --- 3. crossings in reference order, stably sorted by level ----------------
-  const long long NE2 = 2 * NU;
+  // beta != 0: the extension rows' codes, then the extended grid's edges
+  const int nye = econ ? eg.iymax - eg.iymin + 1 : 0;
+  const long long nex = econ ? (long long)nxu * (nye - 1) : 0;
+  const long long NE2 = econ ? nex + (long long)nxu * (nye - 2) : 2 * NU;
   const long long nchunks = (NE2 + EDGES_PER_THREAD - 1) / EDGES_PER_THREAD;
-  int *ccnt = ar.get<int>(nchunks), *coffs = ar.get<int>(nchunks);
-  int *tmpi = ar.get<int>(scan_tmp_elems(nchunks) + 4);
-  int *dtot = ar.get<int>(16);
-  if (ar.failed) return CASL_ENOMEM;
+  int *ccnt, *coffs, *tmpi;
+  if (econ) {
+    // codes and chunk counts in a buffer of their own (the field arena is
+    // sized before the extension is known)
+    const int nb = 1 - eg.iymin, na = eg.iymax - nyu;
+    const size_t bcodes = ((size_t)nxu * (nb + na) * 2 + 255) / 256 * 256;
+    const size_t need = bcodes + (size_t)nchunks * 8 + (size_t)(scan_tmp_elems(nchunks) + 4) * 4 +
+                        ((size_t)1 << 20);
+    if (h->sxe_bytes < need) {
+      if (h->sxe) cudaFree(h->sxe);
+      h->sxe = nullptr;
+      h->sxe_bytes = 0;
+      CASL_CUDA_TRY(cudaMalloc(&h->sxe, need + need / 2));
+      h->sxe_bytes = need + need / 2;
+    }
+    Arena are{(char *)h->sxe, h->sxe_bytes, 0};
+    unsigned short *lcb = are.get<unsigned short>((long long)nxu * nb);
+    unsigned short *lca = are.get<unsigned short>((long long)nxu * na);
+    ccnt = are.get<int>(nchunks);
+    coffs = are.get<int>(nchunks);
+    tmpi = are.get<int>(scan_tmp_elems(nchunks) + 4);
+    if (are.failed) return CASL_ENOMEM;
+    eg.lcb = lcb;
+    eg.lca = lca;
+    CASL_K(k_u_ext, gsz((long long)nxu * (nb + na)), 256, 0, st)(uf, eg, li, c, lcb, lca);
+    CASL_K(k_cre<false>, gsz(nchunks), 256, 0, st)(eg, li, nxu, nyu, NE2, nex, ccnt, nullptr,
+                                                   nullptr, nullptr);
+  } else {
+    ccnt = ar.get<int>(nchunks);
+    coffs = ar.get<int>(nchunks);
+    tmpi = ar.get<int>(scan_tmp_elems(nchunks) + 4);
+    if (ar.failed) return CASL_ENOMEM;
+  }
   const long long ntile = (long long)(nxu / CR_CB) * (nyu / CR_RB);
   const int tgrid = (int)((ntile + 1) / 2);
-  CASL_K(k_cr_tile<false>, tgrid, 256, 0, st)(lc, li, nxu, nyu, ccnt, nullptr, nullptr, nullptr);
+  if (!econ)
+    CASL_K(k_cr_tile<false>, tgrid, 256, 0, st)(lc, li, nxu, nyu, ccnt, nullptr, nullptr, nullptr);
   tr.point("cr_count");
   exclusive_scan<int>(st, ccnt, coffs, nchunks, tmpi, dtot);
   int ncr_i = 0;
@@ -1048,7 +1403,11 @@ int recontour_dev(casl_handle *h, const double *qq) {
   void *sort_tmp = ar2.get<char>(sort_bytes + 16);
   if (ar2.failed) return CASL_ENOMEM;
   tr.point("cr_alloc");
-  CASL_K(k_cr_tile<true>, tgrid, 256, 0, st)(lc, li, nxu, nyu, nullptr, coffs, redge, rlev);
+  if (econ)
+    CASL_K(k_cre<true>, gsz(nchunks), 256, 0, st)(eg, li, nxu, nyu, NE2, nex, nullptr, coffs,
+                                                  redge, rlev);
+  else
+    CASL_K(k_cr_tile<true>, tgrid, 256, 0, st)(lc, li, nxu, nyu, nullptr, coffs, redge, rlev);
   tr.point("cr_emit");
   CASL_CUDA_TRY(cub::DeviceRadixSort::SortPairs(sort_tmp, sort_bytes, rlev, rlev2, redge, redge2,
                                                 (int)ncr, 0, endbit, st));
@@ -1058,8 +1417,11 @@ int recontour_dev(casl_handle *h, const double *qq) {
   double *xcr = ar2.get<double>(ncr), *ycr = ar2.get<double>(ncr);
   unsigned int *kib = ar2.get<unsigned int>(ncr), *kob = ar2.get<unsigned int>(ncr);
   if (ar2.failed) return CASL_ENOMEM;
-  const UField uf{have ? Lu : nullptr, lsum, qq, qjump, have};
-  CASL_K(k_cr_geom, gsz(ncr), 256, 0, st)(uf, redge, rlev, ncr, li, c, xcr, ycr, kib, kob);
+  if (econ)
+    CASL_K(k_cre_geom, gsz(ncr), 256, 0, st)(uf, eg, redge, rlev, ncr, nex, li, c, xcr, ycr, kib,
+                                             kob);
+  else
+    CASL_K(k_cr_geom, gsz(ncr), 256, 0, st)(uf, redge, rlev, ncr, li, c, xcr, ycr, kib, kob);
   RC_TRY(check_launch(h));
 
   tr.point("crossings");
@@ -1388,8 +1750,33 @@ int recontour_dev(casl_handle *h, const double *qq) {
   RC_TRY(check_launch(h));
 
   tr.point("layout");
-  // --- 8. renode three times (congen.f90:295-310) -----------------------------
   RenodeIn cur{xw, yw, coff, clen, clevt, C, ncr, nullptr, cidw};
+  if (econ) {
+    // one periodic image of each contour, y folded (econgen.f90:238-252)
+    int *flags = ar2.get<int>(C), *klen = ar2.get<int>(C), *kone = ar2.get<int>(C);
+    int *koff = ar2.get<int>(C), *kidx = ar2.get<int>(C);
+    int *cs2 = ar2.get<int>(C), *len2 = ar2.get<int>(C), *lev2 = ar2.get<int>(C);
+    double *xw2 = ar2.get<double>(ncr), *yw2 = ar2.get<double>(ncr);
+    int *cidw2 = ar2.get<int>(ncr);
+    if (ar2.failed) return CASL_ENOMEM;
+    CASL_CUDA_TRY(cudaMemsetAsync(flags, 0, (size_t)C * sizeof(int), st));
+    CASL_K(k_ec_flags, g, 256, 0, st)(yw, cidw, ncr, c, flags);
+    CASL_K(k_ec_keep, gsz(C), 256, 0, st)(flags, clen, C, klen, kone);
+    exclusive_scan<int>(st, klen, koff, C, tmpi2, dtot + 4);
+    exclusive_scan<int>(st, kone, kidx, C, tmpi2, dtot + 5);
+    int kc[2] = {0, 0};
+    CASL_CUDA_TRY(cudaMemcpyAsync(kc, dtot + 4, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CASL_CUDA_TRY(cudaStreamSynchronize(st));
+    if (kc[1] == 0) return set_empty();
+    const double yoff = c.hly + c.elly * (double)eg.nby;
+    CASL_K(k_ec_compact, g, 256, 0, st)(xw, yw, cidw, ncr, coff, klen, koff, kidx, c, yoff, xw2,
+                                        yw2, cidw2);
+    CASL_K(k_ec_contours, gsz(C), 256, 0, st)(clen, clevt, C, klen, koff, kidx, cs2, len2, lev2);
+    RC_TRY(check_launch(h));
+    cur = RenodeIn{xw2, yw2, cs2, len2, lev2, kc[1], kc[0], nullptr, cidw2};
+    tr.point("one image");
+  }
+  // --- 8. renode three times (congen.f90:295-310) -----------------------------
   long long capn = std::max<long long>(ncr * 2, h->npm);
   double *xa = ar2.get<double>(capn), *ya = ar2.get<double>(capn);
   double *xb = ar2.get<double>(capn), *yb = ar2.get<double>(capn);
@@ -1492,7 +1879,7 @@ extern "C" int casl_genfg(casl_handle *h, int ix1v, int nxv, int iy1v, int nyv, 
   CASL_K(k_u_lbot, 1, 1024, 0, st)(ljx, Lu, nxu, nyu);
   CASL_K(k_u_colscan, (nxu * 32 + 255) / 256, 256, 0, st)(Lu, nxu, nyu, lsum);
   LevInfo lq{0, 0, h->qjump, 0.0, 1.0};
-  CASL_K(k_u_field, 4096, 256, 0, st)(Lu, lsum, h->qr, h->qjump, 1, lq, qa, nullptr, part, c);
+  CASL_K(k_u_field, 4096, 256, 0, st)(Lu, lsum, h->qr, h->qjump, 1, lq, qa, nullptr, part, c, 0.0);
   CASL_K(k_gf_gather, gsz(m), 256, 0, st)(qa, nxu, nyu, ix1v - 1, nxv, iy1v - 1, nyv, stride, img);
   RC_TRY(check_launch(h));
   CASL_CUDA_TRY(cudaMemcpyAsync(out, img, (size_t)m * sizeof(float), cudaMemcpyDeviceToHost, st));

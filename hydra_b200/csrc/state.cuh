@@ -64,6 +64,8 @@ struct casl_handle {
   size_t sx_bytes;
   void *sx2;             // second arena (recontouring's per-crossing data)
   size_t sx2_bytes;
+  void *sxe;             // beta != 0 recontouring: the extension rows' level codes
+  size_t sxe_bytes;
 
   // kernel-class timing for benchmarks (events on the handle's stream)
   int prof_class;

@@ -1812,6 +1812,323 @@ static int ugrid2con(o_state *s, ugrid *g) {
   return err;
 }
 
+/* ugrid2con of econgen.f90:198-488 (beta != 0): the field qa on rows
+ * 1..nyu is extended periodically in y, row iy taking the values of row
+ * iy0 = 1 + mod(iy-1, nyu) plus bfac*(iy - iy0) (the beta*y offset of the
+ * periodic image), over rows iymin..iymax, which the caller chooses so that
+ * every contour level within the basic box is met.  Contours are traced on
+ * the extended grid; only those with no crossing below ymin and at least
+ * one below ymax are kept, their y folded into [ymin, ymax).  The sign
+ * tests and crossing positions use the reference's expressions: on the
+ * x lines (qa + offset) - qtmp, on the y lines qa + (offset - qtmp). */
+static int ugrid2con_e(o_state *s, ugrid *g, int iymin, int iymax, int levbeg, int levend,
+                       double bfac) {
+  const int nxu = s->nxu, nyu = s->nyu, nlevm = s->p.nlevm;
+  const double elly = s->p.elly, ellx = s->p.ellx, hlxi = s->hlxi, hly = s->hly;
+  const double oms = s->oms, glxu = s->glxu, glyu = s->glyu, qjump = s->qjump;
+  const double ymin = s->ymin, ymax = s->ymax;
+  const int nye = iymax - iymin + 1;           /* extended rows */
+  const long long ngps = (long long)nxu * nye; /* boxes of the extended grid */
+  const int nby = 1 - iymin / nyu;
+  const double yoff = hly + elly * (double)nby;
+  int *icrtab = xcalloc((size_t)ngps * 2 + 2, sizeof(int));
+  signed char *noctab = xcalloc((size_t)ngps + 1, 1);
+  double *yguext = xcalloc((size_t)nye + 1, sizeof(double));
+  int *row0 = xcalloc((size_t)nye + 1, sizeof(int));
+  for (int iy = iymin; iy <= iymax; iy++) {
+    yguext[iy - iymin] = glyu * (double)(iy - 1) + ymin;
+    row0[iy - iymin] = iy < 1 ? 1 + (nby * nyu + iy - 1) % nyu : (iy > nyu ? 1 + (iy - 1) % nyu : iy);
+  }
+  size_t crcap = 1 << 16;
+  long long *kib = xcalloc(crcap + 1, sizeof(long long));
+  double *xcr = xcalloc(crcap + 1, sizeof(double)), *ycr = xcalloc(crcap + 1, sizeof(double));
+  char *freec = xcalloc(crcap + 1, 1);
+  long npm = s->p.npm;
+  double *xa = xcalloc(npm + 2, sizeof(double)), *ya = xcalloc(npm + 2, sizeof(double));
+  size_t dcap = 1 << 16;
+  double *xd = xcalloc(dcap + 1, sizeof(double)), *yd = xcalloc(dcap + 1, sizeof(double));
+  int na = 0, npta = 0, err = 0;
+#define ICR(k, j) icrtab[(size_t)((j)-1) * (size_t)ngps + (size_t)((k)-1)]
+  const double qjumpi = ONE / qjump, qoff = qjump * (double)nlevm;
+#define QTMP(l) (((double)(l)-F12) * qjump - qoff)
+#define ROW0(iy) row0[(iy)-iymin]
+#define OFFS(iy) (bfac * (double)((iy)-ROW0(iy)))
+  /* x-line scan value before qtmp: qa, or (qa + offset) in the extension */
+#define VX(ix, iy) (((iy) >= 1 && (iy) <= nyu) ? UQA(g, (iy), (ix)) : UQA(g, ROW0(iy), (ix)) + OFFS(iy))
+  /* y-line scan: the sign of the reference's qdx at level l */
+#define QDX(ix, iy, qt) (((iy) >= 1 && (iy) <= nyu) ? UQA(g, (iy), (ix)) - (qt) \
+                                                      : UQA(g, ROW0(iy), (ix)) + (OFFS(iy) - (qt)))
+  /* edges in the reference's order: x lines (ix outer, iy = iymin..iymax-1
+   * inner), then y lines (iy = iymin+1..iymax-1 outer, ix inner) */
+  const long long NEX = (long long)nxu * (nye - 1), NEY = (long long)nxu * (nye - 2);
+  int nlv = levend >= levbeg ? levend - levbeg + 1 : 0;
+  long long *lstart = xcalloc((size_t)nlv + 2, sizeof(long long));
+  long long *ledge = NULL;
+  /* levels crossed by edge e, written to lv[]; returns their number */
+  int lvbuf_cap = 64;
+  int *lv = xcalloc((size_t)lvbuf_cap, sizeof(int));
+#define EDGE_LEVELS(e, cnt)                                                                  \
+  do {                                                                                       \
+    cnt = 0;                                                                                 \
+    if ((e) < NEX) {                                                                         \
+      int ix_ = (int)((e) / (nye - 1)) + 1, iy_ = iymin + (int)((e) % (nye - 1));            \
+      double a_ = VX(ix_, iy_), b_ = VX(ix_, iy_ + 1);                                       \
+      if (a_ != b_) {                                                                        \
+        double lo_ = a_ < b_ ? a_ : b_, hi_ = a_ < b_ ? b_ : a_;                             \
+        int l1_ = (int)floor((lo_ + qoff) * qjumpi + F12) - 1;                               \
+        int l2_ = (int)floor((hi_ + qoff) * qjumpi + F12) + 2;                               \
+        if (l1_ < levbeg) l1_ = levbeg;                                                      \
+        if (l2_ > levend) l2_ = levend;                                                       \
+        for (int l_ = l1_; l_ <= l2_; l_++)                                                  \
+          if (QTMP(l_) > lo_ && QTMP(l_) <= hi_) {                                           \
+            if (cnt == lvbuf_cap) { lvbuf_cap *= 2; lv = realloc(lv, lvbuf_cap * sizeof(int)); } \
+            lv[cnt++] = l_;                                                                  \
+          }                                                                                  \
+      }                                                                                      \
+    } else {                                                                                 \
+      long long f_ = (e) - NEX;                                                              \
+      int iy_ = iymin + 1 + (int)(f_ / nxu), ix_ = (int)(f_ % nxu) + 1;                       \
+      int ix2_ = ix_ == nxu ? 1 : ix_ + 1;                                                   \
+      double a_ = VX(ix_, iy_), b_ = VX(ix2_, iy_);                                          \
+      double lo_ = a_ < b_ ? a_ : b_, hi_ = a_ < b_ ? b_ : a_;                               \
+      int l1_ = (int)floor((lo_ + qoff) * qjumpi + F12) - 3;                                 \
+      int l2_ = (int)floor((hi_ + qoff) * qjumpi + F12) + 3;                                 \
+      if (l1_ < levbeg) l1_ = levbeg;                                                        \
+      if (l2_ > levend) l2_ = levend;                                                         \
+      for (int l_ = l1_; l_ <= l2_; l_++) {                                                  \
+        double qt_ = QTMP(l_);                                                               \
+        if (f_sign1(QDX(ix_, iy_, qt_)) != f_sign1(QDX(ix2_, iy_, qt_))) {                   \
+          if (cnt == lvbuf_cap) { lvbuf_cap *= 2; lv = realloc(lv, lvbuf_cap * sizeof(int)); } \
+          lv[cnt++] = l_;                                                                    \
+        }                                                                                    \
+      }                                                                                      \
+    }                                                                                        \
+  } while (0)
+  if (nlv > 0) {
+    for (long long e = 0; e < NEX + NEY; e++) {
+      int cnt;
+      EDGE_LEVELS(e, cnt);
+      for (int q = 0; q < cnt; q++) lstart[lv[q] - levbeg + 1]++;
+    }
+    for (int l = 0; l < nlv; l++) lstart[l + 1] += lstart[l];
+    ledge = xcalloc((size_t)lstart[nlv] + 1, sizeof(long long));
+    long long *cur = xcalloc((size_t)nlv + 1, sizeof(long long));
+    for (long long e = 0; e < NEX + NEY; e++) {
+      int cnt;
+      EDGE_LEVELS(e, cnt);
+      for (int q = 0; q < cnt; q++) ledge[lstart[lv[q] - levbeg] + cur[lv[q] - levbeg]++] = e;
+    }
+    free(cur);
+  }
+  for (int lev = levbeg; lev <= levend && !err; lev++) {
+    int levt = lev - nlevm + (lev - 1) / nlevm - 1;
+    long ncr = 0;
+    double qtmp = QTMP(lev);
+    long long b0 = lstart[lev - levbeg], b1 = lstart[lev - levbeg + 1];
+    for (long long q = b0; q < b1; q++) {
+      long long e = ledge[q];
+      if ((size_t)ncr + 1 > crcap) {
+        crcap *= 2;
+        kib = realloc(kib, (crcap + 1) * sizeof(long long));
+        xcr = realloc(xcr, (crcap + 1) * sizeof(double));
+        ycr = realloc(ycr, (crcap + 1) * sizeof(double));
+        freec = realloc(freec, crcap + 1);
+      }
+      ncr = ncr + 1;
+      if (e < NEX) {
+        int ix = (int)(e / (nye - 1)) + 1, iy = iymin + (int)(e % (nye - 1));
+        double qd0 = VX(ix, iy) - qtmp, qd1 = VX(ix, iy + 1) - qtmp;
+        int is0 = (int)f_sign1(qd0);
+        int inc = (1 - is0) / 2;
+        long long kaa = (long long)(iy - iymin) * nxu + 1;
+        kib[ncr] = kaa + s->ibx[ix + inc];
+        long long kob = kaa + s->ibx[ix + 1 - inc];
+        noctab[kob] = noctab[kob] + 1;
+        ICR(kob, noctab[kob]) = (int)ncr;
+        xcr[ncr] = s->xgu[ix];
+        ycr[ncr] = yguext[iy - iymin] - glyu * qd0 / (qd1 - qd0);
+      } else {
+        long long f = e - NEX;
+        int iy = iymin + 1 + (int)(f / nxu), ix = (int)(f % nxu) + 1;
+        double qd0 = QDX(ix, iy, qtmp), qd1 = QDX(ix == nxu ? 1 : ix + 1, iy, qtmp);
+        int is0 = (int)f_sign1(qd0);
+        int inc = (1 - is0) / 2;
+        long long kaa = (long long)(iy - 1 - iymin) * nxu + ix;
+        kib[ncr] = kaa + (long long)(1 - inc) * nxu;
+        long long kob = kaa + (long long)inc * nxu;
+        noctab[kob] = noctab[kob] + 1;
+        ICR(kob, noctab[kob]) = (int)ncr;
+        ycr[ncr] = yguext[iy - iymin];
+        double xx = s->xgu[ix] - glxu * qd0 / (qd1 - qd0);
+        xcr[ncr] = oms * (xx - ellx * f_dint(xx * hlxi));
+      }
+    }
+    for (long icr = 1; icr <= ncr; icr++) freec[icr] = 1;
+    for (long icr = 1; icr <= ncr; icr++) {
+      if (!freec[icr]) continue;
+      if (na + 1 > s->p.nm) { err = 2; break; }
+      na = na + 1;
+      s->indq[na] = levt;
+      int ibeg = npta + 1;
+      s->i1q[na] = ibeg;
+      int below = 0, above = 1;
+      int npd = 1;
+      xd[1] = xcr[icr];
+      yd[1] = ycr[icr];
+      if (ycr[icr] < ymin) below = 1;
+      if (ycr[icr] < ymax) above = 0;
+      long long k = kib[icr];
+      int noc = noctab[k];
+      long icrn = ICR(k, noc);
+      while (icrn != icr) {
+        noctab[k] = (signed char)(noc - 1);
+        npd = npd + 1;
+        if ((size_t)npd > dcap) {
+          dcap *= 2;
+          xd = realloc(xd, (dcap + 1) * sizeof(double));
+          yd = realloc(yd, (dcap + 1) * sizeof(double));
+        }
+        xd[npd] = xcr[icrn];
+        yd[npd] = ycr[icrn];
+        if (ycr[icrn] < ymin) below = 1;
+        if (ycr[icrn] < ymax) above = 0;
+        freec[icrn] = 0;
+        k = kib[icrn];
+        noc = noctab[k];
+        icrn = ICR(k, noc);
+      }
+      int keep = 0, npa = 0;
+      if (!(below || above)) {
+        for (int i = 1; i <= npd; i++) yd[i] = fmod(yd[i] + yoff, elly) + ymin;
+        long room = npm - npta;
+        do {
+          npa = renode_cap(s, xd + 1, yd + 1, npd, xa + ibeg, ya + ibeg, room);
+          if (npa <= 0) break;
+          npd = renode_cap(s, xa + ibeg, ya + ibeg, npa, xd + 1, yd + 1, (long)dcap);
+          if (npd <= 0) break;
+          npa = renode_cap(s, xd + 1, yd + 1, npd, xa + ibeg, ya + ibeg, room);
+          if (npa <= 0) break;
+          keep = 1;
+        } while (0);
+        if (npa < 0 || npd < 0) { err = 1; break; }
+      }
+      if (keep) {
+        s->npq[na] = npa;
+        npta = npta + npa;
+        int iend = ibeg + npa - 1;
+        s->i2q[na] = iend;
+        for (int i = ibeg; i <= iend - 1; i++) s->nextq[i] = i + 1;
+        s->nextq[iend] = ibeg;
+      } else {
+        na = na - 1;
+      }
+      freec[icr] = 0;
+    }
+    for (long icr = 1; icr <= ncr; icr++) noctab[kib[icr]] = 0;
+  }
+#undef EDGE_LEVELS
+#undef QDX
+#undef VX
+#undef OFFS
+#undef ROW0
+#undef QTMP
+#undef ICR
+  for (int i = 1; i <= npta; i++) {
+    s->xq[i] = xa[i];
+    s->yq[i] = ya[i];
+  }
+  s->nq = na;
+  s->nptq = npta;
+  free(icrtab); free(noctab); free(yguext); free(row0); free(kib); free(xcr); free(ycr);
+  free(freec); free(xa); free(ya); free(xd); free(yd); free(lstart); free(ledge); free(lv);
+  return err;
+}
+
+/* recontour of econgen.f90:27-194 (beta != 0).  Returns 3 when beta*Ly
+ * is not an integer multiple of qjump (the reference stops there), 5 when
+ * the extension would reach beyond the reference's 100 periodic boxes. */
+static int recontour_e(o_state *s, const double *qq) {
+  const int nxu = s->nxu, nyu = s->nyu;
+  const double qjump = s->qjump, beta = s->p.beta;
+  const double qjumpi = ONE / qjump, qoff = qjump * (double)s->p.nlevm;
+  const double bfac = beta * s->glyu, ppvdif = beta * s->p.elly;
+  const double brat = ppvdif * qjumpi;
+  const int ibrat = (int)lround(brat);
+  if (fabs(brat - (double)ibrat) > 1.0e-7) return 3;
+  ugrid g;
+  g.ldq = (size_t)nyu + 1;
+  g.qa = xcalloc(g.ldq * nxu, sizeof(double));
+  if (s->nq > 0) {
+    con2ugrid(s, &g);
+    for (int ix = 1; ix <= nxu; ix++) {
+      int ixf = s->ixfw[ix], ix0 = s->ix0w[ix], ix1 = s->ix1w[ix];
+      for (int iy = 1; iy <= nyu; iy++) {
+        int iyf = s->iyfw[iy], iy0 = s->iy0w[iy], iy1 = s->iy1w[iy];
+        int w = (ixf - 1) * 16 + (iyf - 1);
+        UQA(&g, iy, ix) = UQA(&g, iy, ix) + s->w00[w] * qq[PHY(s, iy0, ix0)] +
+                          s->w10[w] * qq[PHY(s, iy1, ix0)] + s->w01[w] * qq[PHY(s, iy0, ix1)] +
+                          s->w11[w] * qq[PHY(s, iy1, ix1)];
+      }
+    }
+  } else {
+    for (int ix = 1; ix <= nxu; ix++) {
+      int ixf = s->ixfw[ix], ix0 = s->ix0w[ix], ix1 = s->ix1w[ix];
+      for (int iy = 1; iy <= nyu; iy++) {
+        int iyf = s->iyfw[iy], iy0 = s->iy0w[iy], iy1 = s->iy1w[iy];
+        int w = (ixf - 1) * 16 + (iyf - 1);
+        UQA(&g, iy, ix) = s->w00[w] * qq[PHY(s, iy0, ix0)] + s->w10[w] * qq[PHY(s, iy1, ix0)] +
+                          s->w01[w] * qq[PHY(s, iy0, ix1)] + s->w11[w] * qq[PHY(s, iy1, ix1)] +
+                          beta * s->ygu[iy];
+      }
+    }
+  }
+  double *qqmin = xcalloc((size_t)nyu + 2, sizeof(double)), *qqmax = xcalloc((size_t)nyu + 2, sizeof(double));
+  for (int iy = 1; iy <= nyu; iy++) qqmin[iy] = qqmax[iy] = UQA(&g, iy, 1);
+  for (int ix = 2; ix <= nxu; ix++)
+    for (int iy = 1; iy <= nyu; iy++) {
+      double v = UQA(&g, iy, ix);
+      qqmin[iy] = qqmin[iy] < v ? qqmin[iy] : v;
+      qqmax[iy] = qqmax[iy] > v ? qqmax[iy] : v;
+    }
+  qqmin[nyu + 1] = qqmin[1] + ppvdif;
+  qqmax[nyu + 1] = qqmax[1] + ppvdif;
+  double qamin = qqmin[1], qamax = qqmax[1];
+  for (int iy = 2; iy <= nyu + 1; iy++) {
+    qamin = qamin < qqmin[iy] ? qamin : qqmin[iy];
+    qamax = qamax > qqmax[iy] ? qamax : qqmax[iy];
+  }
+  int levbeg = f_int((qoff + qamin) * qjumpi + F12) + 1;
+  int levend = f_int((qoff + qamax) * qjumpi + F12);
+  int levmin = f_int(qamin * qjumpi - F12);
+  double qlev = ((double)levmin + F12) * qjump;
+  int iy = 1, err = 0;
+  for (;;) {
+    iy = iy - 1;
+    if (iy < -100 * nyu) { err = 5; break; }
+    int iy0 = 1 + (100 * nyu + iy - 1) % nyu;
+    double qadd = bfac * (double)(iy - iy0);
+    if (qadd + qqmax[iy0] <= qlev) break;
+  }
+  int iymin = iy;
+  int levmax = f_int(qamax * qjumpi + F12);
+  qlev = ((double)levmax - F12) * qjump;
+  iy = nyu + 1;
+  while (!err) {
+    iy = iy + 1;
+    if (iy > 101 * nyu) { err = 5; break; }
+    int iy0 = 1 + (iy - 1) % nyu;
+    double qadd = bfac * (double)(iy - iy0);
+    if (qadd + qqmin[iy0] >= qlev) break;
+  }
+  int iymax = iy;
+  free(qqmin);
+  free(qqmax);
+  if (!err) err = ugrid2con_e(s, &g, iymin, iymax, levbeg, levend, bfac);
+  free(g.qa);
+  s->contex = s->nptq > 0;
+  return err;
+}
+
 /* recontour (congen.f90:24-128); qq(ny,nx) is the residual (or full) field. */
 /* genfg's ugridsave (post/genfg.f90:79-113): con2ugrid of the contours
  * plus the bilinear interpolation of the residual qq, as float32 in the
@@ -1836,6 +2153,7 @@ void o_genfg(o_state *s, const double *qq, float *out) {
 }
 
 int o_recontour(o_state *s, double *qq) {
+  if (s->beffect) return recontour_e(s, qq);  /* the ecaps build (econgen.f90) */
   int nx = s->nx, ny = s->ny, nxu = s->nxu, nyu = s->nyu;
   ugrid g;
   g.ldq = (size_t)nyu + 1;
