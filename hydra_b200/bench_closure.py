@@ -24,11 +24,11 @@ from .casl import CaslNet
 # pattern: forward layers, input gradients (CIN = the layer's COUT), weight
 # gradients
 _SHAPES = {
-    "k_conv5<16, 32, 8, 0>": [(16, 32)],            # layer 1 forward
-    "k_conv5<32, 32, 8, 0>": [(32, 32), (32, 32)],  # layers 2, 3 forward
-    "k_conv5<32, 16, 8, 1>": [(32, 16)],            # layer 4 forward
-    "k_conv5<16, 32, 8, 2>": [(16, 32)],            # layer 4 input gradient
-    "k_conv5<32, 32, 8, 2>": [(32, 32), (32, 32)],  # layers 3, 2 input gradients
+    "k_conv5<16, 32, 4, 0>": [(16, 32)],            # layer 1 forward
+    "k_conv5<32, 32, 4, 0>": [(32, 32), (32, 32)],  # layers 2, 3 forward
+    "k_conv5<32, 16, 4, 1>": [(32, 16)],            # layer 4 forward
+    "k_conv5<16, 32, 4, 2>": [(16, 32)],            # layer 4 input gradient
+    "k_conv5<32, 32, 4, 2>": [(32, 32), (32, 32)],  # layers 3, 2 input gradients
     "k_conv5_wgrad<32, 16, 8>": [(32, 16)],
     "k_conv5_wgrad<32, 32, 8>": [(32, 32), (32, 32)],
     "k_conv5_wgrad<16, 32, 8>": [(16, 32)],

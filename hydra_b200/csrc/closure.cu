@@ -110,130 +110,217 @@ struct ConvArgs {
 
 template <int CIN, int COUT, int R>
 struct ConvSmem {
-  static constexpr int RS = (CIN / 8) * CS;
-  static constexpr int IN_BYTES = (R + 4) * RS;
+  static constexpr int RS = (CIN / 8) * CS;            // one staged row, all planes
+  static constexpr int IN_BYTES = (R + 4) * RS;        // one tile's input rows
   static constexpr int W_BYTES = 25 * (CIN / 8) * COUT * 16;
-  static constexpr int TOTAL = IN_BYTES + W_BYTES + 64;
-  static constexpr int TCOLS = R * COUT;
-  static_assert(TCOLS >= 32 && TCOLS <= 512 && (TCOLS & (TCOLS - 1)) == 0, "TMEM columns");
+  static constexpr int BAR_OFF = W_BYTES + 2 * IN_BYTES;  // weights, two input buffers
+  static constexpr int TOTAL = BAR_OFF + 80;
+  static constexpr int ACC = R * COUT;                 // TMEM columns of one tile
+  static constexpr int TCOLS = 2 * ACC < 32 ? 32 : 2 * ACC;
+  static_assert(TCOLS <= 512 && (TCOLS & (TCOLS - 1)) == 0, "TMEM columns");
   static_assert(CIN % 16 == 0 && COUT % 16 == 0 && COUT <= 32, "channel counts");
+  static_assert(R % 2 == 0, "rows split between two warp halves");
 };
 
-// One CTA: output columns [x0, x0+128) of rows [y0, y0+R).  Thread t owns
-// output column x0+t (TMEM lane t); row r's COUT accumulators are TMEM
-// columns [r*COUT, (r+1)*COUT), cleared first.  Staged input row i (global
-// row y0+i-2) feeds output rows r = i-4 .. i (those inside the CTA) through
-// tap row ky = i - r: one MMA per (i, kx, plane pair) with
-// A[m][k] = input(row y0+i-2, column x0+m+kx-2, channel k of the pair) and
-// B the weights of all those rows' ky stacked along N -- the image keeps ky
-// descending so that ascending output rows (ascending TMEM columns) meet
-// their ky in order.  N = 32..160: each staged A tile is read once per kx
-// and plane pair for up to five output rows.
+// A persistent CTA per SM walks a list of tiles (128 output columns x R
+// rows; tile j: column strip j % (n/128), rows (j / (n/128)) * R ...).
+// Warp-specialised: the last warp (one thread) stages the weight image once and
+// each tile's input rows by bulk copies into one of two buffers, and issues
+// the tile's MMAs into one of two TMEM accumulators; the others drain the
+// accumulators (bias, GELU, stores) and clear them.  Barriers, not block
+// syncs, couple them: full[b] (rows of buffer b arrived), mdone[b] (MMAs
+// into accumulator b complete, which also frees input buffer b) and
+// afree[b] (accumulator b drained and cleared), so the tensor core, the
+// copy engine and the epilogue warps all run at once.  Within a tile,
+// staged input row i (global row y0+i-2) feeds output rows r = i-4 .. i
+// (those inside the tile) through tap row ky = i - r: one MMA per (i, kx,
+// plane pair) with A[m][k] = input(row y0+i-2, column x0+m+kx-2, channel k
+// of the pair) and B the weights of all those rows' ky stacked along N --
+// the image keeps ky descending so that ascending output rows (ascending
+// TMEM columns) meet their ky in order.  TMEM lane m is output column x0+m;
+// row r's COUT accumulators are columns [r*COUT, (r+1)*COUT) of the tile's
+// accumulator.  Epilogue warp w drains lanes 32(w%4).. of rows r = w/4,
+// w/4 + EPI/4, ...  Every wait is bounded: one that gives up sets CASL_ETIMEOUT
+// and stops the CTA once the copies and MMAs it issued have completed (again
+// bounded).
+// Epilogue warps: four per row of a tile in the forward modes (one row
+// each); the input-gradient mode, whose epilogue holds more registers, uses
+// half as many, two rows each.
+template <int R, int MODE>
+constexpr int conv_epi_warps() { return MODE == BWD_GELU ? 2 * R : 4 * R; }
+template <int R, int MODE>
+constexpr int conv_threads() { return 32 * (conv_epi_warps<R, MODE>() + 1); }
+
 template <int CIN, int COUT, int R, int MODE>
-__global__ void __launch_bounds__(128, 1) k_conv5(ConvArgs a) {
+__global__ void __launch_bounds__(conv_threads<R, MODE>(), 1) k_conv5(ConvArgs a) {
+  constexpr int EPI = conv_epi_warps<R, MODE>();
   using S = ConvSmem<CIN, COUT, R>;
   extern __shared__ __align__(128) unsigned char smem[];
-  unsigned char *in_s = smem;
-  unsigned char *w_s = smem + S::IN_BYTES;
-  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + S::IN_BYTES + S::W_BYTES);
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 2);
+  unsigned char *w_s = smem;
+  unsigned char *in_s0 = smem + S::W_BYTES;
+  // barriers: [0] weights, [1 + b] full, [3 + b] mdone, [5 + b] afree
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + S::BAR_OFF);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 7);
+  volatile int *abort_s = reinterpret_cast<volatile int *>(tslot + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int n = a.n;
-  const int x0 = blockIdx.x * SEG, y0 = blockIdx.y * R;
+  const int nstrip = n / SEG, ntiles = nstrip * (n / R);
+  const int G = gridDim.x;
   CASL_PDL_ENTRY();
   if (tid == 0) {
-    tc::mbar_init(&bars[0], 1);
-    tc::mbar_init(&bars[1], 1);
+    for (int q = 0; q < 5; q++) tc::mbar_init(&bars[q], 1);
+    tc::mbar_init(&bars[5], EPI);
+    tc::mbar_init(&bars[6], EPI);
     tc::mbar_fence_init();
+    *abort_s = 0;
   }
   __syncthreads();
   if (warp == 0) tc::tmem_alloc(tslot, S::TCOLS);
-  if (tid == 0) {
-    tc::mbar_expect_tx(&bars[0], S::IN_BYTES + S::W_BYTES);
-    for (int i = 0; i < R + 4; i++)
-      for (int c = 0; c < CIN / 8; c++)
-        tc::bulk_g2s(in_s + i * S::RS + c * CS, a.in + act_off(n, CIN, y0 - 2 + i, x0 - 2, c), CS,
-                     &bars[0]);
-    tc::bulk_g2s(w_s, a.wimg, S::W_BYTES, &bars[0]);
-  }
   tc::tc_fence_before();
   __syncthreads();
   tc::tc_fence_after();
   const uint32_t tbase = *tslot;
-  // every MMA accumulates: clear this warp's lanes of all accumulators
-  for (int c0 = 0; c0 < S::TCOLS; c0 += 32)
-    tc::tmem_zero32(tbase + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0);
+  const uint32_t lane_base = (uint32_t)(32 * (warp & 3)) << 16;
+  // every MMA accumulates: clear both accumulators (warps 0-3 hold the 128 lanes)
+  if (warp < 4)
+    for (int c0 = 0; c0 < S::TCOLS; c0 += 32) tc::tmem_zero32(tbase + lane_base + (uint32_t)c0);
   tc::tmem_wait_st();
   tc::tc_fence_before();
   __syncthreads();
   tc::tc_fence_after();
-  bool ok = tc::mbar_wait(&bars[0], 0);
-  if (tid == 0 && ok) {
-    const uint32_t in_a = tc::smem_u32(in_s), w_a = tc::smem_u32(w_s);
-    for (int i = 0; i < R + 4; i++) {
-      const int r_lo = i - 4 > 0 ? i - 4 : 0, r_hi = i < R - 1 ? i : R - 1;
-      const int nrow = r_hi - r_lo + 1, ky_hi = i - r_lo;
-      const uint32_t idesc = tc::idesc_bf16(128, nrow * COUT, false, false);
-      for (int kx = 0; kx < 5; kx++)
+  const int ntile_cta = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / G + 1 : 0;
+  if (warp == EPI) {
+    if (lane == 0) {
+      // tile t's R+4 input rows (all planes) into buffer t & 1
+      auto load_tile = [&](int t) {
+        const int j = blockIdx.x + t * G, b = t & 1;
+        const int x0 = (j % nstrip) * SEG, y0 = (j / nstrip) * R;
+        unsigned char *dst = in_s0 + b * S::IN_BYTES;
+        tc::mbar_expect_tx(&bars[1 + b], S::IN_BYTES);
+        for (int i = 0; i < R + 4; i++)
+          for (int c = 0; c < CIN / 8; c++)
+            tc::bulk_g2s(dst + i * S::RS + c * CS, a.in + act_off(n, CIN, y0 - 2 + i, x0 - 2, c),
+                         CS, &bars[1 + b]);
+      };
+      tc::mbar_expect_tx(&bars[0], S::W_BYTES);
+      tc::bulk_g2s(w_s, a.wimg, S::W_BYTES, &bars[0]);
+      if (ntile_cta > 0) load_tile(0);
+      int loaded = ntile_cta > 0 ? 1 : 0, issued = 0;  // tiles loaded / with MMAs issued
+      bool ok = tc::mbar_wait(&bars[0], 0);
+      for (int t = 0; ok && t < ntile_cta; t++) {
+        const int b = t & 1;
+        // rows of tile t, accumulator b drained (tile t-2)
+        ok = tc::mbar_wait(&bars[1 + b], (t >> 1) & 1);
+        if (ok && t >= 2) ok = tc::mbar_wait(&bars[5 + b], ((t - 2) >> 1) & 1);
+        if (!ok || *abort_s) break;
+        tc::tc_fence_after();
+        const uint32_t in_a = tc::smem_u32(in_s0 + b * S::IN_BYTES), w_a = tc::smem_u32(w_s);
+        const uint32_t acc = tbase + (uint32_t)(b * S::ACC);
+        for (int i = 0; i < R + 4; i++) {
+          const int r_lo = i - 4 > 0 ? i - 4 : 0, r_hi = i < R - 1 ? i : R - 1;
+          const int nrow = r_hi - r_lo + 1, ky_hi = i - r_lo;
+          const uint32_t idesc = tc::idesc_bf16(128, nrow * COUT, false, false);
+          for (int kx = 0; kx < 5; kx++)
 #pragma unroll
-        for (int cp = 0; cp < CIN / 16; cp++) {
-          const uint64_t ad = tc::sdesc(in_a + i * S::RS + 2 * cp * CS + kx * 16, CS, 128);
-          const uint64_t bd = tc::sdesc(
-              w_a + ((kx * (CIN / 8) + 2 * cp) * 5 + (4 - ky_hi)) * COUT * 16, 5 * COUT * 16, 128);
-          tc::mma_bf16(tbase + r_lo * COUT, ad, bd, idesc, 1u);
+            for (int cp = 0; cp < CIN / 16; cp++) {
+              const uint64_t ad = tc::sdesc(in_a + i * S::RS + 2 * cp * CS + kx * 16, CS, 128);
+              const uint64_t bd =
+                  tc::sdesc(w_a + ((kx * (CIN / 8) + 2 * cp) * 5 + (4 - ky_hi)) * COUT * 16,
+                            5 * COUT * 16, 128);
+              tc::mma_bf16(acc + (uint32_t)(r_lo * COUT), ad, bd, idesc, 1u);
+            }
         }
+        tc::mma_commit(&bars[3 + b]);
+        issued = t + 1;
+        // tile t+1's rows into the other buffer once tile t-1's MMAs (its
+        // readers) have completed
+        if (t + 1 < ntile_cta) {
+          if (t >= 1) ok = tc::mbar_wait(&bars[3 + (b ^ 1)], ((t - 1) >> 1) & 1);
+          if (!ok) break;
+          load_tile(t + 1);
+          loaded = t + 2;
+        }
+      }
+      if (!ok) {
+        *abort_s = 1;
+        atomicExch(a.err, CASL_ETIMEOUT);
+      }
+      // before the CTA ends: the last copies and MMAs issued have landed
+      if (loaded > issued && loaded >= 1) {
+        const int t = loaded - 1;
+        tc::mbar_wait(&bars[1 + (t & 1)], (t >> 1) & 1);
+      }
+      if (issued >= 1) {
+        const int t = issued - 1;
+        tc::mbar_wait(&bars[3 + (t & 1)], (t >> 1) & 1);
+      }
     }
-    tc::mma_commit(&bars[1]);
-  }
-  ok = ok && tc::mbar_wait(&bars[1], 0);
-  tc::tc_fence_after();
-  if (!ok) {
-    if (lane == 0) atomicExch(a.err, CASL_ETIMEOUT);
   } else {
-    const int col = x0 + warp * 32 + lane;
     float dsum[COUT];
 #pragma unroll
     for (int co = 0; co < COUT; co++) dsum[co] = 0.0f;
-    for (int r = 0; r < R; r++) {
-      const int row = y0 + r;
-      float v[COUT];
-      const uint32_t taddr = tbase + ((uint32_t)(warp * 32) << 16) + (uint32_t)(r * COUT);
-      if (COUT == 32)
-        tc::tmem_ld32(taddr, v);
-      else
-        tc::tmem_ld16(taddr, v);
-      if (MODE == FWD_LINEAR) {
-        for (int co = 0; co < a.cout_real; co++)
-          a.fout[((long long)co * n + row) * n + col] = v[co] + a.bias[co];
-      } else if (MODE == FWD_GELU) {
-#pragma unroll
-        for (int co = 0; co < COUT; co++) v[co] += a.bias[co];
-        if (a.zout) store_px<COUT>(a.zout, n, row, col, v);
-#pragma unroll
-        for (int co = 0; co < COUT; co++) v[co] = gelu_f(v[co]);
-        store_px<COUT>(a.out, n, row, col, v);
-      } else {
-#pragma unroll
-        for (int c = 0; c < COUT / 8; c++) {
-          float z[8];
-          unpack8(*reinterpret_cast<const uint4 *>(a.zprev + act_off(n, COUT, row, col, c)), z);
-#pragma unroll
-          for (int e = 0; e < 8; e++) {
-            const float g = v[8 * c + e] * gelu_d(z[e]);
-            const float gr = __bfloat162float(__float2bfloat16_rn(g));
-            v[8 * c + e] = gr;
-            dsum[8 * c + e] += gr;
-          }
-        }
-        store_px<COUT>(a.out, n, row, col, v);
+    const int r0 = warp >> 2;  // this warp's rows: r0, r0 + EPI/4, ...
+    for (int t = 0; t < ntile_cta; t++) {
+      const int b = t & 1;
+      const bool okp = !*abort_s && tc::mbar_wait(&bars[3 + b], (t >> 1) & 1);
+      tc::tc_fence_after();
+      if (!okp) {
+        *abort_s = 1;
+        atomicExch(a.err, CASL_ETIMEOUT);
+        break;
       }
+      const int j = blockIdx.x + t * G;
+      const int x0 = (j % nstrip) * SEG, y0 = (j / nstrip) * R;
+      const int col = x0 + (warp & 3) * 32 + lane;
+      for (int r = r0; r < R; r += EPI / 4) {
+        const int row = y0 + r;
+        float v[COUT];
+        const uint32_t taddr = tbase + lane_base + (uint32_t)(b * S::ACC + r * COUT);
+        if (COUT == 32) {
+          tc::tmem_ld32(taddr, v);
+          tc::tmem_zero32(taddr);
+        } else {
+          tc::tmem_ld16(taddr, v);
+          tc::tmem_zero16(taddr);
+        }
+        if (MODE == FWD_LINEAR) {
+          for (int co = 0; co < a.cout_real; co++)
+            a.fout[((long long)co * n + row) * n + col] = v[co] + a.bias[co];
+        } else if (MODE == FWD_GELU) {
+#pragma unroll
+          for (int co = 0; co < COUT; co++) v[co] += a.bias[co];
+          if (a.zout) store_px<COUT>(a.zout, n, row, col, v);
+#pragma unroll
+          for (int co = 0; co < COUT; co++) v[co] = gelu_f(v[co]);
+          store_px<COUT>(a.out, n, row, col, v);
+        } else {
+#pragma unroll
+          for (int c = 0; c < COUT / 8; c++) {
+            float z[8];
+            unpack8(*reinterpret_cast<const uint4 *>(a.zprev + act_off(n, COUT, row, col, c)), z);
+#pragma unroll
+            for (int e = 0; e < 8; e++) {
+              const float g = v[8 * c + e] * gelu_d(z[e]);
+              const float gr = __bfloat162float(__float2bfloat16_rn(g));
+              v[8 * c + e] = gr;
+              dsum[8 * c + e] += gr;
+            }
+          }
+          store_px<COUT>(a.out, n, row, col, v);
+        }
+      }
+      // accumulator b drained and cleared: one arrival per warp
+      tc::tmem_wait_st();
+      tc::tc_fence_before();
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(&bars[5 + b]);
     }
     if (MODE == BWD_GELU && a.dbias) {
 #pragma unroll
       for (int co = 0; co < COUT; co++) {
         float s = dsum[co];
         for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) atomicAdd(&a.dbias[co], s);
+        if (lane == 0 && s != 0.0f) atomicAdd(&a.dbias[co], s);
       }
     }
   }
@@ -533,7 +620,7 @@ __global__ void k_pack_grad(const float *__restrict__ g, bf16 *__restrict__ dz, 
 // ---------------------------------------------------------------------------
 // Launches
 // ---------------------------------------------------------------------------
-constexpr int RF = 8;  // output rows per CTA of the convolutions
+constexpr int RF = 4;  // output rows per tile of the convolutions
 constexpr int RW = 8;  // gradient rows per CTA of the weight gradients
 
 template <int CIN, int COUT, int MODE>
@@ -550,9 +637,12 @@ static int launch_conv(const ConvArgs &a, cudaStream_t st) {
   // named by its template arguments for the per-launch timing report
   static char name[48];
   if (!name[0]) snprintf(name, sizeof name, "k_conv5<%d, %d, %d, %d>", CIN, COUT, RF, MODE);
-  const dim3 grid(a.n / SEG, a.n / RF);
-  for (bool once = kt_begin(name, grid, 128, S::TOTAL, st); once; once = kt_end())
-    launch_of(k, grid, 128, S::TOTAL, st)(a);
+  // persistent: one CTA per SM (at most one per tile)
+  const int ntiles = (a.n / SEG) * (a.n / RF);
+  const dim3 grid(ntiles < 148 ? ntiles : 148);
+  constexpr int NT = conv_threads<RF, MODE>();
+  for (bool once = kt_begin(name, grid, NT, S::TOTAL, st); once; once = kt_end())
+    launch_of(k, grid, NT, S::TOTAL, st)(a);
   return cudaPeekAtLastError() == cudaSuccess ? CASL_OK : CASL_ECUDA;
 }
 
