@@ -233,7 +233,7 @@ def run_reference(a):
 CLOSURE_WEIGHTS = os.path.join(ROOT, "hydra_b200", "closure_512.npz")
 
 
-def run_closure_leg(a, torch, device, steps=40, warmup=5, check_every=20, budget=1e-2):
+def run_closure_leg(a, torch, device, steps=40, warmup=5, check_every=40, budget=1e-2):
     """The learned-closure configuration (512^2 grid, k0 = 12, 80 levels, the
     trained weights shipped with the library) against the plain form, every
     node-velocity error measured against the 2048^2 FP64 judge on states of

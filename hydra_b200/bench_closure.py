@@ -18,7 +18,7 @@ import re
 
 import numpy as np
 
-from .casl import CaslNet
+from .casl import NET_OUT, CaslNet
 
 # padded (CIN, COUT) of each convolution the kernels run, by kernel name
 # pattern: forward layers, input gradients (CIN = the layer's COUT), weight
@@ -50,7 +50,7 @@ def run(n=512, reps=20, device=0):
     p = (rng.standard_normal(net.count) * 0.05).astype(np.float32)
     net.set_params(p)
     x = rng.standard_normal((3, n, n)).astype(np.float32)
-    dy = rng.standard_normal((2, n, n)).astype(np.float32)
+    dy = rng.standard_normal((NET_OUT, n, n)).astype(np.float32)
     net.forward(x)
     net.backward(dy)
     lib = net.lib

@@ -50,6 +50,11 @@ class CaslParams(C.Structure):
 
 _lib = None
 _dp = C.POINTER(C.c_double)
+
+# The network's output channels (CASL_NET_OUT): the velocity correction on a
+# grid twice as fine as n, channel comp*4 + a*2 + b = component comp (u, v)
+# at the fine point (2 ix + a, 2 iy + b).
+NET_OUT = 8
 _ip = C.POINTER(C.c_int)
 _fp = C.POINTER(C.c_float)
 
@@ -128,6 +133,7 @@ SIGNATURES = {
     "casl_closure_train": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, _dp]),
     "casl_closure_evaluate": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, _dp]),
     "casl_closure_features": (C.c_int, [C.c_void_p, C.c_void_p, _fp]),
+    "casl_closure_correction": (C.c_int, [C.c_void_p, C.c_void_p, _dp, _dp]),
     "casl_set_precision": (C.c_int, [C.c_void_p, C.c_int]),
     "casl_get_precision": (C.c_int, [C.c_void_p, _ip]),
     "casl_pvforce": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_int, _dp]),
@@ -449,6 +455,14 @@ class CaslGPU:
                     "casl_closure_evaluate")
         return tuple(out)
 
+    def closure_correction(self, net):
+        """The network's correction at the nodes (du, dv) from the latest inversion."""
+        _, npt, _ = self.counts()
+        du, dv = np.empty(npt), np.empty(npt)
+        self._check(self.lib.casl_closure_correction(self.h, net.h, _d(du), _d(dv)),
+                    "casl_closure_correction")
+        return du, dv
+
     def closure_features(self, net):
         x = np.empty((3, self.nx, self.ny), np.float32)
         self._check(self.lib.casl_closure_features(self.h, net.h, x.ctypes.data_as(_fp)),
@@ -477,7 +491,7 @@ def _fptr(a):
 
 class CaslNet:
     """The learned velocity closure's network on one GPU (casl_net_*): four
-    periodic 5x5 convolutions 3 -> 32 -> 32 -> 32 -> 2 with GELU, BF16
+    periodic 5x5 convolutions 3 -> 32 -> 32 -> 32 -> NET_OUT with GELU, BF16
     weights and activations, FP32 accumulation, on the tensor cores.  Arrays
     are channel-major (C, n, n) float32 with rows = ix, columns = iy."""
 
@@ -516,13 +530,13 @@ class CaslNet:
 
     def forward(self, x):
         x = _f32(x, (3, self.n, self.n))
-        y = np.empty((2, self.n, self.n), np.float32)
+        y = np.empty((NET_OUT, self.n, self.n), np.float32)
         self._check(self.lib.casl_net_forward(self.h, _fptr(x), _fptr(y)), "casl_net_forward")
         return y
 
     def backward(self, dy):
         """Gradient of sum(dy * y) for the last forward, flat in parameter order."""
-        dy = _f32(dy, (2, self.n, self.n))
+        dy = _f32(dy, (NET_OUT, self.n, self.n))
         g = np.empty(self.count, np.float32)
         self._check(self.lib.casl_net_backward(self.h, _fptr(dy), _fptr(g)), "casl_net_backward")
         return g

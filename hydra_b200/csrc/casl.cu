@@ -1095,7 +1095,8 @@ __device__ __forceinline__ void nodes_rk_body(int bid, int nbk, double *__restri
                            double *__restrict__ xqf, double *__restrict__ yqf,
                            const T *__restrict__ uu, const T *__restrict__ vv,
                            const Scalars *__restrict__ s, const Consts &c,
-                           const int *__restrict__ mnode, int M) {
+                           const int *__restrict__ mnode, int M,
+                           const double *__restrict__ du, const double *__restrict__ dv) {
   const int npt = s->nptq;
   const double ex = c.ellx, ey = c.elly, hx = c.hlxi, hy = c.hlyi, oms = c.oms;
   const long long nn = (long long)c.nx * c.ny;
@@ -1106,6 +1107,10 @@ __device__ __forceinline__ void nodes_rk_body(int bid, int nbk, double *__restri
     const double dt = sm.dt, dt2 = sm.dt2, dt3 = sm.dt3, dt6 = sm.dt6;
     double uq, vq;
     velint1(xq[i], yq[i], uu + m * nn, vv + m * nn, c, uq, vq);
+    if (du) {
+      uq = uq + du[i];
+      vq = vq + dv[i];
+    }
     if (STAGE == 1) {
       double x0 = xq[i], y0 = yq[i];
       xqi[i] = x0;
@@ -1335,6 +1340,7 @@ struct NodeRkArgs {
   const T *uu, *vv;
   const int *mnode;  // ensemble: first node of each member (nullptr: one simulation)
   int M;
+  const double *du, *dv;  // learned closure: correction at every node (nullable)
 };
 struct SpecRkArgs {
   double *qs, *qd, *qsi, *qsf, *qdi, *qdf;
@@ -1352,7 +1358,7 @@ __global__ void k_stage_rk(NodeRkArgs<T> a, SpecRkArgs b, Scalars *__restrict__ 
     for (int m = threadIdx.x; m < a.M; m += blockDim.x) s[m].t = s[m].t + s[m].dt2;
   if ((int)blockIdx.x < nbn)
     nodes_rk_body<STAGE, T>(blockIdx.x, nbn, a.xq, a.yq, a.xqi, a.yqi, a.xqf, a.yqf, a.uu, a.vv, s, c,
-                            a.mnode, a.M);
+                            a.mnode, a.M, a.du, a.dv);
   else
     spec_rk_body<STAGE>(blockIdx.x - nbn, gridDim.x - nbn, b.qs, b.qd, b.qsi, b.qsf, b.qdi,
                         b.qdf, b.sqs, b.sqd, b.emq, s, b.nn, b.tot);
@@ -1579,12 +1585,13 @@ static int source_prod(casl_handle *h, int stage) {
 // node update and spectral RK update of a stage, one launch; velint reads
 // the velocity fields u, v (FP64, or FP32 in the FP32-inversion mode)
 template <class T>
-static int stage_update(casl_handle *h, int stage, const T *u, const T *v) {
+static int stage_update(casl_handle *h, int stage, const T *u, const T *v, const double *du,
+                        const double *dv) {
   const long long nn = (long long)h->n * h->n, tot = h->M * nn;
   const int nbn = h->contex ? grid_for(h->nptq > 0 ? h->nptq : 1) : 0;
   const int g = nbn + grid_for(tot / 2);
   const NodeRkArgs<T> a{h->xq, h->yq, h->xqi, h->yqi, h->xqf, h->yqf, u, v,
-                        h->M > 1 ? h->mnode : nullptr, h->M};
+                        h->M > 1 ? h->mnode : nullptr, h->M, du, dv};
   const SpecRkArgs b{h->qs, h->qd, h->qsi, h->qsf, h->qdi, h->qdf, h->sqs, h->sqd, h->emq,
                      nn, tot};
   cudaStream_t st = h->stream;
@@ -1615,15 +1622,16 @@ static int advance_dev(casl_handle *h) {
     if (stage == 1 && (rc = adapt_dev(h))) return rc;
     if ((rc = source_prod(h, stage))) return rc;
     tr.point("adapt+source");
+    // the learned closure's correction at the nodes (null without it)
+    const double *du = nullptr, *dv = nullptr;
     if (f32) {
       const long long nn = (long long)h->n * h->n;
       const float *u = h->f32, *v = h->f32 + nn;
-      if (h->closure && (rc = closure_stage32(h, &u, &v))) return rc;
-      if ((rc = stage_update<float>(h, stage, u, v))) return rc;
+      if (h->closure && (rc = closure_stage32(h, u, v, &du, &dv))) return rc;
+      if ((rc = stage_update<float>(h, stage, u, v, du, dv))) return rc;
     } else {
-      const double *u = h->uu, *v = h->vv;
-      if (h->closure && (rc = closure_stage(h, &u, &v))) return rc;
-      if ((rc = stage_update<double>(h, stage, u, v))) return rc;
+      if (h->closure && (rc = closure_stage(h, &du, &dv))) return rc;
+      if ((rc = stage_update<double>(h, stage, h->uu, h->vv, du, dv))) return rc;
     }
     tr.point("stage update");
     static const char *const names[4] = {"RK4 stage 1", "RK4 stage 2", "RK4 stage 3",

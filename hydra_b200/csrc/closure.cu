@@ -457,9 +457,18 @@ __global__ void __launch_bounds__(128, 1) k_conv5_wgrad(WgradArgs a) {
 // Layer table, parameters, weight images
 // ---------------------------------------------------------------------------
 constexpr int NL = 4;
-// real channel counts 3 -> 32 -> 32 -> 32 -> 2, padded to the MMA's multiples of 16
+// The network's output is the velocity correction on a grid SUB times as
+// fine as the inversion's, as SUB x SUB sub-cells per coarse cell: channel
+// comp*SUB^2 + a*SUB + b holds component comp (0: u, 1: v) at the point
+// (SUB ix + a, SUB iy + b) of the fine grid.  A correction on the coarse
+// grid itself cannot do better than about 1.1e-3 relative at 512^2 (the
+// least-squares optimum of any coarse field under velint's bilinear
+// interpolation), since the error is mostly the interpolation's own.
+constexpr int SUB = 2;
+constexpr int NOUT = 2 * SUB * SUB;
+// real channel counts 3 -> 32 -> 32 -> 32 -> NOUT, padded to the MMA's multiples of 16
 __host__ __device__ constexpr int cin_r(int l) { return l == 0 ? 3 : 32; }
-__host__ __device__ constexpr int cout_r(int l) { return l == NL - 1 ? 2 : 32; }
+__host__ __device__ constexpr int cout_r(int l) { return l == NL - 1 ? NOUT : 32; }
 __host__ __device__ constexpr int cin_p(int l) { return l == 0 ? 16 : 32; }
 __host__ __device__ constexpr int cout_p(int l) { return l == NL - 1 ? 16 : 32; }
 
@@ -595,25 +604,25 @@ __global__ void k_pack_grad(const float *__restrict__ g, bf16 *__restrict__ dz, 
                             float *__restrict__ db) {
   CASL_PDL_ENTRY();
   const long long nn = (long long)n * n;
-  float s0 = 0.0f, s1 = 0.0f;
+  float sum[16];
+#pragma unroll
+  for (int c = 0; c < 16; c++) sum[c] = 0.0f;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nn;
        t += (long long)gridDim.x * blockDim.x) {
     const int row = (int)(t / n), col = (int)(t % n);
     float v[16];
 #pragma unroll
-    for (int c = 0; c < 16; c++)
+    for (int c = 0; c < 16; c++) {
       v[c] = c < cout ? __bfloat162float(__float2bfloat16_rn(g[c * nn + t])) : 0.0f;
-    s0 += v[0];
-    s1 += v[1];
+      sum[c] += v[c];
+    }
     store_px<16>(dz, n, row, col, v);
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    s0 += __shfl_xor_sync(0xffffffffu, s0, o);
-    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
-  }
-  if ((threadIdx.x & 31) == 0) {
-    atomicAdd(&db[0], s0);
-    if (cout > 1) atomicAdd(&db[1], s1);
+#pragma unroll
+  for (int c = 0; c < 16; c++) {
+    float x = sum[c];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if ((threadIdx.x & 31) == 0 && c < cout) atomicAdd(&db[c], x);
   }
 }
 
@@ -680,7 +689,7 @@ struct casl_net {
   bf16 *a[3], *z[3];          // activations and pre-activations of layers 1-3
   bf16 *dc;                   // output gradient planes (16 channels)
   bf16 *dz[3];                // pre-activation gradients of layers 1-3
-  float *fout;                // [2][n][n] network output
+  float *fout;                // [NOUT][n][n] network output
   float *stage;               // host<->device staging, [3][n][n]
   int *err;
   float qscale, uscale;
@@ -711,7 +720,7 @@ int forward(casl_net *N, cudaStream_t st, bool train, int *err) {
   }
   ConvArgs b{};
   b.n = n; b.err = err;
-  b.in = N->a[2]; b.wimg = N->L[3].wf; b.bias = N->L[3].bias; b.fout = N->fout; b.cout_real = 2;
+  b.in = N->a[2]; b.wimg = N->L[3].wf; b.bias = N->L[3].bias; b.fout = N->fout; b.cout_real = NOUT;
   return launch_conv<32, 16, FWD_LINEAR>(b, st);
 }
 
@@ -786,10 +795,6 @@ static int read_err(casl_net *N, cudaStream_t st) {
 // ---------------------------------------------------------------------------
 namespace casl {
 
-__global__ void k_velint(const double *__restrict__ xq, const double *__restrict__ yq, int npt,
-                         const double *__restrict__ uu, const double *__restrict__ vv,
-                         double *__restrict__ uq, double *__restrict__ vq, Consts c);
-
 struct ClosureState {
   casl_net *net;            // the attached network (not owned); nullptr = none
   casl_handle *judge;       // fine-grid judge for the periodic check (not owned, nullable)
@@ -798,10 +803,10 @@ struct ClosureState {
   int active;               // the correction is applied inside the step
   long long steps, checks, fallbacks;
   double last_plain, last_net;
-  double *ucor, *vcor;      // corrected velocity fields (n*n each)
   double *uJ, *vJ, *uP, *vP, *uC, *vC;  // node arrays (capacity cap)
+  double *du, *dv;          // the correction at the nodes inside a step (capacity cap)
   long long cap;
-  float *dcf;               // [2][n][n] output gradient of the node loss
+  float *dcf;               // [NOUT][n][n] output gradient of the node loss
   double *acc;              // [4] sums of the node errors
 };
 
@@ -832,43 +837,60 @@ __global__ void k_features(const int *__restrict__ C, const Scalars *__restrict_
   }
 }
 
-// Corrected fields: u + us * y0, v + us * y1 (FP64 fields, or FP32 ones in
-// the FP32-inversion mode).
-template <class T>
-__global__ void k_apply(const T *__restrict__ uu, const T *__restrict__ vv,
-                        const float *__restrict__ y, float us, T *__restrict__ uc,
-                        T *__restrict__ vc, long long nn) {
-  CASL_PDL_ENTRY();
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nn;
-       t += (long long)gridDim.x * blockDim.x) {
-    uc[t] = (T)((double)uu[t] + (double)us * (double)y[t]);
-    vc[t] = (T)((double)vv[t] + (double)us * (double)y[nn + t]);
-  }
+// Corners and weights of the bilinear interpolation of the correction at
+// node (x, y) on the SUB-times finer grid, as offsets into one component's
+// SUB^2 channels: point (I, J) of the fine grid is sub-cell (I % SUB,
+// J % SUB) of coarse cell (I / SUB, J / SUB).  Indices are clamped so that
+// no input reads outside the output (valid nodes never need the clamp).
+__device__ __forceinline__ void sub_corners(double x, double y, const Consts &c, long long *k,
+                                            double *w) {
+  const int mx = SUB * c.nx, my = SUB * c.ny;
+  const double xx = ((double)SUB * c.glxi) * (x - c.xmin);
+  const double yy = ((double)SUB * c.glyi) * (y - c.ymin);
+  int i0 = f_int(xx), j0 = f_int(yy);
+  const double px = xx - (double)i0, py = yy - (double)j0;
+  i0 = i0 < 0 ? 0 : (i0 > mx - 1 ? mx - 1 : i0);
+  j0 = j0 < 0 ? 0 : (j0 > my - 1 ? my - 1 : j0);
+  const int i1 = i0 + 1 == mx ? 0 : i0 + 1, j1 = j0 + 1 == my ? 0 : j0 + 1;
+  const long long nn = (long long)c.nx * c.ny;
+  auto at = [&](int I, int J) -> long long {
+    return (long long)((I % SUB) * SUB + (J % SUB)) * nn + (long long)(I / SUB) * c.ny + (J / SUB);
+  };
+  k[0] = at(i0, j0); w[0] = (1.0 - px) * (1.0 - py);
+  k[1] = at(i1, j0); w[1] = px * (1.0 - py);
+  k[2] = at(i0, j1); w[2] = (1.0 - px) * py;
+  k[3] = at(i1, j1); w[3] = px * py;
 }
 
-// The corner indices and weights of velint's bilinear interpolation
-// (contours.f90:136-169) at node (x, y).
-__device__ __forceinline__ void bilinear_corners(double x, double y, const Consts &c,
-                                                 long long *k, double *w) {
-  const double xx = c.glxi * (x - c.xmin);
-  int ix0 = 1 + f_int(xx);
-  const double pxc = (double)ix0 - xx, px = 1.0 - pxc;
-  const double yy = c.glyi * (y - c.ymin);
-  int iy0 = 1 + f_int(yy);
-  const double pyc = (double)iy0 - yy, py = 1.0 - pyc;
-  ix0 = ix0 < 1 ? 1 : (ix0 > c.nx ? c.nx : ix0);
-  iy0 = iy0 < 1 ? 1 : (iy0 > c.ny ? c.ny : iy0);
-  const int ix1 = ix0 == c.nx ? 1 : ix0 + 1, iy1 = iy0 == c.ny ? 1 : iy0 + 1;
-  k[0] = (long long)(ix0 - 1) * c.ny + (iy0 - 1); w[0] = pyc * pxc;
-  k[1] = (long long)(ix1 - 1) * c.ny + (iy0 - 1); w[1] = pyc * px;
-  k[2] = (long long)(ix0 - 1) * c.ny + (iy1 - 1); w[2] = py * pxc;
-  k[3] = (long long)(ix1 - 1) * c.ny + (iy1 - 1); w[3] = py * px;
+// The correction at the nodes, us * (bilinear interpolation of y on the
+// fine grid), added to the plain node velocities (up, vp) when they are
+// given.
+__global__ void k_corr_nodes(const double *__restrict__ xq, const double *__restrict__ yq,
+                             int npt, const float *__restrict__ y, float us, Consts c,
+                             const double *__restrict__ up, const double *__restrict__ vp,
+                             double *__restrict__ uo, double *__restrict__ vo) {
+  CASL_PDL_ENTRY();
+  const long long cv = (long long)SUB * SUB * c.nx * c.ny;  // the v channels
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npt; i += gridDim.x * blockDim.x) {
+    long long k[4];
+    double w[4];
+    sub_corners(xq[i], yq[i], c, k, w);
+    double du = 0.0, dv = 0.0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      du += w[j] * (double)y[k[j]];
+      dv += w[j] * (double)y[cv + k[j]];
+    }
+    uo[i] = (up ? up[i] : 0.0) + (double)us * du;
+    vo[i] = (vp ? vp[i] : 0.0) + (double)us * dv;
+  }
 }
 
 // Node errors against the judge: acc[0] += |corrected - judge|^2,
 // acc[1] += |plain - judge|^2, acc[2] += |judge|^2.  With g non-null, the
 // gradient of the loss sum |corrected - judge|^2 / (npt us^2) with respect
-// to the network output is scattered into g ([2][n][n]).
+// to the network output is scattered into g ([NOUT][n][n]) with the fine
+// grid's bilinear weights.
 __global__ void k_node_loss(const double *__restrict__ xq, const double *__restrict__ yq, int npt,
                             const double *__restrict__ uC, const double *__restrict__ vC,
                             const double *__restrict__ uP, const double *__restrict__ vP,
@@ -876,7 +898,7 @@ __global__ void k_node_loss(const double *__restrict__ xq, const double *__restr
                             Consts c, float us, float *__restrict__ g, double *__restrict__ acc) {
   CASL_PDL_ENTRY();
   double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-  const long long nn = (long long)c.nx * c.ny;
+  const long long cv = (long long)SUB * SUB * c.nx * c.ny;  // the v channels
   const double gs = 2.0 / ((double)npt * (double)us);
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npt; i += gridDim.x * blockDim.x) {
     const double ru = uC[i] - uJ[i], rv = vC[i] - vJ[i];
@@ -887,11 +909,11 @@ __global__ void k_node_loss(const double *__restrict__ xq, const double *__restr
     if (g) {
       long long k[4];
       double w[4];
-      bilinear_corners(xq[i], yq[i], c, k, w);
+      sub_corners(xq[i], yq[i], c, k, w);
 #pragma unroll
       for (int j = 0; j < 4; j++) {
         atomicAdd(&g[k[j]], (float)(gs * ru * w[j]));
-        atomicAdd(&g[nn + k[j]], (float)(gs * rv * w[j]));
+        atomicAdd(&g[cv + k[j]], (float)(gs * rv * w[j]));
       }
     }
   }
@@ -911,7 +933,7 @@ __global__ void k_node_loss(const double *__restrict__ xq, const double *__restr
 
 static int cs_grow(ClosureState *cs, long long npt) {
   if (npt <= cs->cap) return CASL_OK;
-  double **arrs[] = {&cs->uJ, &cs->vJ, &cs->uP, &cs->vP, &cs->uC, &cs->vC};
+  double **arrs[] = {&cs->uJ, &cs->vJ, &cs->uP, &cs->vP, &cs->uC, &cs->vC, &cs->du, &cs->dv};
   for (auto a : arrs) {
     cudaFree(*a);
     *a = nullptr;
@@ -935,10 +957,9 @@ static ClosureState *cs_get(casl_handle *h, int *rc) {
     return nullptr;
   }
   const size_t nn = (size_t)h->n * h->n;
-  bool ok = cudaMalloc(&cs->ucor, nn * 8) == cudaSuccess && cudaMalloc(&cs->vcor, nn * 8) == cudaSuccess &&
-            cudaMalloc(&cs->dcf, 2 * nn * 4) == cudaSuccess && cudaMalloc(&cs->acc, 64) == cudaSuccess;
+  bool ok = cudaMalloc(&cs->dcf, NOUT * nn * 4) == cudaSuccess && cudaMalloc(&cs->acc, 64) == cudaSuccess;
   if (!ok) {
-    cudaFree(cs->ucor); cudaFree(cs->vcor); cudaFree(cs->dcf); cudaFree(cs->acc);
+    cudaFree(cs->dcf); cudaFree(cs->acc);
     free(cs);
     *rc = CASL_ENOMEM;
     return nullptr;
@@ -950,7 +971,7 @@ static ClosureState *cs_get(casl_handle *h, int *rc) {
 void closure_release(casl_handle *h) {
   ClosureState *cs = h->closure;
   if (!cs) return;
-  void *ps[] = {cs->ucor, cs->vcor, cs->dcf, cs->acc, cs->uJ, cs->vJ, cs->uP, cs->vP, cs->uC, cs->vC};
+  void *ps[] = {cs->dcf, cs->acc, cs->uJ, cs->vJ, cs->uP, cs->vP, cs->uC, cs->vC, cs->du, cs->dv};
   for (void *p : ps) cudaFree(p);
   free(cs);
   h->closure = nullptr;
@@ -961,47 +982,42 @@ static inline int gsz(long long work) {
   return (int)(g < 1 ? 1 : (g > 148 * 16 ? 148 * 16 : g));
 }
 
-// Network input, forward (train keeps the pre-activations) and the corrected
-// fields, from h's latest inversion, on h's stream.
+// Network input and forward (train keeps the pre-activations) from h's
+// latest inversion (FP64 fields, or FP32 ones in the FP32-inversion mode),
+// on h's stream: the correction is left in N->fout.
 template <class T>
-static int net_correct_t(casl_handle *h, casl_net *N, const T *uu, const T *vv, T *uc, T *vc,
-                         bool train) {
+static int net_run_t(casl_handle *h, casl_net *N, const T *uu, const T *vv, bool train) {
   const long long nn = (long long)h->n * h->n;
   cudaStream_t st = h->stream;
   CASL_K(net::k_features<T>, gsz(nn), 256, 0, st)(h->coarseC, h->scal, uu, vv, 1.0f / N->qscale,
                                                    1.0f / N->uscale, N->x0, h->n,
                                                    h->nptq > 0 ? 1 : 0);
-  int rc = net::forward(N, st, train, &h->scal->error);
+  return net::forward(N, st, train, &h->scal->error);
+}
+
+// The correction at the nodes for a stage's node update: the network on
+// the stage's fields, interpolated to the nodes' current positions.
+template <class T>
+static int closure_stage_t(casl_handle *h, const T *uu, const T *vv, const double **du,
+                           const double **dv) {
+  ClosureState *cs = h->closure;
+  if (!cs || !cs->net || !cs->active || h->nptq == 0) return CASL_OK;
+  int rc = cs_grow(cs, h->nptq);
   if (rc) return rc;
-  CASL_K(net::k_apply<T>, gsz(nn), 256, 0, st)(uu, vv, N->fout, N->uscale, uc, vc, nn);
+  if ((rc = net_run_t<T>(h, cs->net, uu, vv, false))) return rc;
+  CASL_K(net::k_corr_nodes, gsz(h->nptq), 256, 0, h->stream)(h->xq, h->yq, h->nptq,
+                                                             cs->net->fout, cs->net->uscale, h->c,
+                                                             nullptr, nullptr, cs->du, cs->dv);
+  *du = cs->du;
+  *dv = cs->dv;
   return cudaPeekAtLastError() == cudaSuccess ? CASL_OK : CASL_ECUDA;
 }
-
-// Network input, forward (train keeps the pre-activations) and the corrected
-// FP64 fields, from h's latest FP64 inversion, on h's stream.
-static int net_correct(casl_handle *h, casl_net *N, ClosureState *cs, bool train) {
-  return net_correct_t<double>(h, N, h->uu, h->vv, cs->ucor, cs->vcor, train);
+int closure_stage(casl_handle *h, const double **du, const double **dv) {
+  return closure_stage_t<double>(h, h->uu, h->vv, du, dv);
 }
-
-int closure_stage(casl_handle *h, const double **u, const double **v) {
-  ClosureState *cs = h->closure;
-  if (!cs || !cs->net || !cs->active) return CASL_OK;
-  int rc = net_correct(h, cs->net, cs, false);
-  if (rc) return rc;
-  *u = cs->ucor;
-  *v = cs->vcor;
-  return CASL_OK;
-}
-
-int closure_stage32(casl_handle *h, const float **u, const float **v) {
-  ClosureState *cs = h->closure;
-  if (!cs || !cs->net || !cs->active) return CASL_OK;
-  float *uc = reinterpret_cast<float *>(cs->ucor), *vc = reinterpret_cast<float *>(cs->vcor);
-  int rc = net_correct_t<float>(h, cs->net, *u, *v, uc, vc, false);
-  if (rc) return rc;
-  *u = uc;
-  *v = vc;
-  return CASL_OK;
+int closure_stage32(casl_handle *h, const float *u, const float *v, const double **du,
+                    const double **dv) {
+  return closure_stage_t<float>(h, u, v, du, dv);
 }
 
 // Judge, network and node errors at h's current state: out[0] the plain
@@ -1023,20 +1039,20 @@ static int evaluate(casl_handle *h, casl_net *N, casl_handle *hf, bool train, fl
   tr.begin(h->stream, "evaluate");
   if ((rc = judge_velocity(h, hf, cs->uJ, cs->vJ, cs->uP, cs->vP))) return rc;
   tr.point("judge");
-  if ((rc = net_correct(h, N, cs, train))) return rc;
+  if ((rc = net_run_t<double>(h, N, h->uu, h->vv, train))) return rc;
   tr.point("network");
   cudaStream_t st = h->stream;
-  CASL_K(k_velint, gsz(npt), 256, 0, st)(h->xq, h->yq, npt, cs->ucor, cs->vcor, cs->uC, cs->vC,
-                                          h->c);
+  CASL_K(net::k_corr_nodes, gsz(npt), 256, 0, st)(h->xq, h->yq, npt, N->fout, N->uscale, h->c,
+                                                   cs->uP, cs->vP, cs->uC, cs->vC);
   const long long nn = (long long)h->n * h->n;
   if (cudaMemsetAsync(cs->acc, 0, 64, st) != cudaSuccess) return CASL_ECUDA;
-  if (train && cudaMemsetAsync(cs->dcf, 0, 2 * nn * 4, st) != cudaSuccess) return CASL_ECUDA;
+  if (train && cudaMemsetAsync(cs->dcf, 0, NOUT * nn * 4, st) != cudaSuccess) return CASL_ECUDA;
   CASL_K(net::k_node_loss, gsz(npt), 256, 0, st)(h->xq, h->yq, npt, cs->uC, cs->vC, cs->uP,
                                                   cs->vP, cs->uJ, cs->vJ, h->c, N->uscale,
                                                   train ? cs->dcf : nullptr, cs->acc);
   if (train) {
     if (cudaMemsetAsync(N->L[3].db, 0, cout_p(3) * 4, st) != cudaSuccess) return CASL_ECUDA;
-    CASL_K(net::k_pack_grad, 148 * 4, 256, 0, st)(cs->dcf, N->dc, h->n, 2, N->L[3].db);
+    CASL_K(net::k_pack_grad, 148 * 4, 256, 0, st)(cs->dcf, N->dc, h->n, NOUT, N->L[3].db);
     if ((rc = net::backward(N, st, &h->scal->error))) return rc;
     if ((rc = net::adam_step(N, st, lr))) return rc;
   }
@@ -1135,8 +1151,8 @@ int casl_net_create(int n, int device, casl_net **out) {
     A((void **)&N->z[i], act_elems(n, 32) * 2);
     A((void **)&N->dz[i], act_elems(n, 32) * 2);
   }
-  A((void **)&N->fout, 2ull * n * n * 4);
-  A((void **)&N->stage, 3ull * n * n * 4);
+  A((void **)&N->fout, (size_t)NOUT * n * n * 4);
+  A((void **)&N->stage, (size_t)(NOUT > 3 ? NOUT : 3) * n * n * 4);
   A((void **)&N->err, 64);
   for (int l = 0; l < NL; l++) {
     const size_t img = 25ull * cin_p(l) * cout_p(l);
@@ -1192,7 +1208,7 @@ int casl_net_forward(casl_net *N, const float *x, float *y) {
   CASL_K(k_pack_input, 148 * 4, 256, 0, st)(N->stage, N->x0, n, 3);
   int rc = forward(N, st, true, N->err);
   if (rc) return rc;
-  if (cudaMemcpyAsync(y, N->fout, 2 * nn * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+  if (cudaMemcpyAsync(y, N->fout, NOUT * nn * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess)
     return CASL_ECUDA;
   return read_err(N, st);
 }
@@ -1203,10 +1219,10 @@ int casl_net_backward(casl_net *N, const float *dy, float *grad) {
   const int n = N->n;
   const size_t nn = (size_t)n * n;
   cudaStream_t st = N->stream;
-  if (cudaMemcpyAsync(N->stage, dy, 2 * nn * 4, cudaMemcpyHostToDevice, st) != cudaSuccess)
+  if (cudaMemcpyAsync(N->stage, dy, NOUT * nn * 4, cudaMemcpyHostToDevice, st) != cudaSuccess)
     return CASL_ECUDA;
   if (cudaMemsetAsync(N->L[3].db, 0, cout_p(3) * 4, st) != cudaSuccess) return CASL_ECUDA;
-  CASL_K(k_pack_grad, 148 * 4, 256, 0, st)(N->stage, N->dc, n, 2, N->L[3].db);
+  CASL_K(k_pack_grad, 148 * 4, 256, 0, st)(N->stage, N->dc, n, NOUT, N->L[3].db);
   int rc = backward(N, st, N->err);
   if (rc) return rc;
   if (grad) {
@@ -1317,6 +1333,30 @@ int casl_closure_judge(casl_handle *h, casl_handle *judge, double *uJ, double *v
   if (uP && cudaMemcpyAsync(uP, cs->uP, b, cudaMemcpyDeviceToHost, st) != cudaSuccess)
     return CASL_ECUDA;
   if (vP && cudaMemcpyAsync(vP, cs->vP, b, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    return CASL_ECUDA;
+  return casl::sync_counts(h);
+}
+
+// The network's correction at h's nodes from h's latest inversion.
+int casl_closure_correction(casl_handle *h, casl_net *net, double *du, double *dv) {
+  if (!h || !net || !du || !dv || net->n != h->n) return CASL_EINVAL;
+  if (net->device != h->device) return CASL_EINVAL;
+  cudaSetDevice(h->device);
+  int rc;
+  casl::ClosureState *cs = casl::cs_get(h, &rc);
+  if (!cs) return rc;
+  if ((rc = casl::sync_counts(h))) return rc;
+  const int npt = h->nptq;
+  if (npt == 0) return CASL_OK;
+  if ((rc = casl::cs_grow(cs, npt))) return rc;
+  if ((rc = casl::net_run_t<double>(h, net, h->uu, h->vv, false))) return rc;
+  cudaStream_t st = h->stream;
+  CASL_K(casl::net::k_corr_nodes, casl::gsz(npt), 256, 0, st)(h->xq, h->yq, npt, net->fout,
+                                                             net->uscale, h->c, nullptr, nullptr,
+                                                             cs->du, cs->dv);
+  const size_t b = (size_t)npt * sizeof(double);
+  if (cudaMemcpyAsync(du, cs->du, b, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaMemcpyAsync(dv, cs->dv, b, cudaMemcpyDeviceToHost, st) != cudaSuccess)
     return CASL_ECUDA;
   return casl::sync_counts(h);
 }

@@ -159,10 +159,12 @@ int ensure_scratch2(casl_handle *h, size_t bytes);
 int judge_velocity(casl_handle *h, casl_handle *hf, double *uJ, double *vJ, double *uP,
                    double *vP);
 // Learned velocity closure hooks (closure.cu).  closure_stage runs after a
-// stage's inversion; it returns the velocity fields velint should read (the
-// corrected ones while the closure is active, else h->uu, h->vv).
-int closure_stage(casl_handle *h, const double **u, const double **v);
-int closure_stage32(casl_handle *h, const float **u, const float **v);  // FP32-inversion mode
+// stage's inversion; while the closure is active it sets du, dv to the
+// correction at every node (added to velint's velocity in the node update),
+// else leaves them null.
+int closure_stage(casl_handle *h, const double **du, const double **dv);
+int closure_stage32(casl_handle *h, const float *u, const float *v, const double **du,
+                    const double **dv);  // FP32-inversion mode
 // Before each advance of casl_step: the periodic fine-grid check.
 int closure_step_check(casl_handle *h);
 void closure_release(casl_handle *h);

@@ -25,7 +25,9 @@ import numpy as np
 from .casl import CaslGPU, CaslNet
 from .synthetic import random_pv
 
-LAYERS = [(3, 32), (32, 32), (32, 32), (32, 2)]
+# the last layer's 8 channels: the u and v correction at the 2 x 2 points of
+# the twice-finer grid inside each coarse cell
+LAYERS = [(3, 32), (32, 32), (32, 32), (32, 8)]
 
 
 def init_params(seed: int) -> np.ndarray:

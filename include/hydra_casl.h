@@ -337,8 +337,11 @@ void casl_net_destroy(casl_net *net);
  * divided by and its output multiplied by when it runs inside a step. */
 int casl_net_set_params(casl_net *net, const float *params, float qscale, float uscale);
 int casl_net_get_params(casl_net *net, float *params, float *qscale, float *uscale);
-/* x: (3, n, n) network input (already scaled); y: (2, n, n) output.  Keeps
- * what casl_net_backward needs. */
+/* x: (3, n, n) network input (already scaled); y: (CASL_NET_OUT, n, n)
+ * output, the velocity correction on a grid twice as fine as n: channel
+ * comp*4 + a*2 + b holds component comp (0: u, 1: v) at the fine point
+ * (2 ix + a, 2 iy + b).  Keeps what casl_net_backward needs. */
+#define CASL_NET_OUT 8
 int casl_net_forward(casl_net *net, const float *x, float *y);
 /* Gradient of sum(dy * y) for the last casl_net_forward with respect to the
  * parameters (grad: casl_net_param_count floats, may be NULL); also keeps it
@@ -357,8 +360,9 @@ int casl_net_adam(casl_net *net, float lr);
 int casl_closure_judge(casl_handle *h, casl_handle *judge, double *uJ, double *vJ, double *uP,
                        double *vP);
 /* Attach a network to h: from now on every RK4 stage of casl_advance /
- * casl_step runs it on the stage's coarse PV and velocity and velint reads
- * u + uscale*y0, v + uscale*y1.  With a judge and check_every > 0, every
+ * casl_step runs it on the stage's coarse PV and velocity, and each node's
+ * velocity is velint's plus uscale times the bilinear interpolation of the
+ * network's output on the grid twice as fine (see casl_net_forward).  With a judge and check_every > 0, every
  * check_every-th casl_step first compares the node velocities of both forms
  * with the judge's: the correction stays on while its relative error
  * (sqrt(sum |u - uJ|^2 / sum |uJ|^2) over the nodes) is at most `budget` and
@@ -381,6 +385,10 @@ int casl_closure_evaluate(casl_handle *h, casl_net *net, casl_handle *judge, dou
 /* The network input of h's latest inversion, (3, n, n) float32, already
  * divided by the network's scales: contour PV, u, v. */
 int casl_closure_features(casl_handle *h, casl_net *net, float *x);
+/* The network's correction at h's nodes (du, dv: host arrays of nptq
+ * doubles) from h's latest inversion, as the node update inside a step adds
+ * it. */
+int casl_closure_correction(casl_handle *h, casl_net *net, double *du, double *dv);
 
 /* ---- benchmarking hooks (no counterpart in the reference) ---------------- */
 /* The cudaStream_t (as void*) on which all of the handle's work is ordered,

@@ -7,8 +7,12 @@ contours.f90:136-169, interpolates the coarse inversion bilinearly), so this
 file restates the network the library defines, not a reference algorithm:
 
 * four periodic 5x5 convolutions (cross-correlation: out[y, x] reads
-  in[y + ky - 2, x + kx - 2], indices modulo n), 3 -> 32 -> 32 -> 32 -> 2
+  in[y + ky - 2, x + kx - 2], indices modulo n), 3 -> 32 -> 32 -> 32 -> 8
   channels, GELU (0.5 x (1 + erf(x / sqrt 2))) after the first three;
+* the output is the velocity correction on a grid twice as fine as n:
+  channel comp*4 + a*2 + b is component comp (u, v) at the fine point
+  (2 ix + a, 2 iy + b), interpolated bilinearly to the nodes on that grid
+  (``node_correction``);
 * parameters in the order W1[co][ci][ky][kx], b1, ..., W4, b4 (FP32);
 * BF16 rounding (round to nearest even) wherever the GPU stores BF16: the
   input, the weights, every pre-activation and activation, the output
@@ -24,7 +28,8 @@ from __future__ import annotations
 import numpy as np
 from scipy.special import erf
 
-LAYERS = [(3, 32), (32, 32), (32, 32), (32, 2)]
+LAYERS = [(3, 32), (32, 32), (32, 32), (32, 8)]
+SUB = 2  # the output grid is SUB times as fine as the input
 
 
 def param_count() -> int:
@@ -159,3 +164,30 @@ def pad_spectrum(s, nf):
     sub = s[np.ix_(ix[ok], ix[ok])] * np.outer(fx[ok], fx[ok])
     out[np.ix_(np.nonzero(ok)[0], np.nonzero(ok)[0])] = sub
     return out
+
+
+def node_correction(y, xq, yq, us, n, ell=2 * np.pi):
+    """us times the bilinear interpolation of the output y ([8][n][n]) on the
+    2n grid at the nodes (xq, yq) of the domain [-ell/2, ell/2)^2: fine point
+    (I, J) is sub-cell (I % 2, J % 2) of coarse cell (I // 2, J // 2)."""
+    m = SUB * n
+    h = ell / m
+    fx = (np.asarray(xq) + ell / 2) / h
+    fy = (np.asarray(yq) + ell / 2) / h
+    i0 = np.floor(fx).astype(np.int64)
+    j0 = np.floor(fy).astype(np.int64)
+    px, py = fx - i0, fy - j0
+    i0 %= m
+    j0 %= m
+    i1, j1 = (i0 + 1) % m, (j0 + 1) % m
+    y = np.asarray(y, np.float64)
+
+    def at(comp, I, J):
+        return y[comp * SUB * SUB + (I % SUB) * SUB + (J % SUB), I // SUB, J // SUB]
+
+    out = []
+    for comp in range(2):
+        v = ((1 - px) * (1 - py) * at(comp, i0, j0) + px * (1 - py) * at(comp, i1, j0)
+             + (1 - px) * py * at(comp, i0, j1) + px * py * at(comp, i1, j1))
+        out.append(us * v)
+    return out[0], out[1]

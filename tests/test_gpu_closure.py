@@ -29,7 +29,7 @@ def inputs(n, seed):
 def test_forward_matches_oracle(gpu_lib, n):
     from hydra_b200.casl import CaslNet
     p = co.init_params(3)
-    p[co.param_count() - 2:] = [0.3, -0.2]  # output bias
+    p[co.param_count() - 8:] = np.linspace(-0.3, 0.3, 8)  # output bias
     x = inputs(n, n)
     net = CaslNet(n)
     net.set_params(p)
@@ -48,7 +48,7 @@ def test_backward_matches_oracle(gpu_lib):
     n = 128
     p = co.init_params(4)
     x = inputs(n, 5)
-    dy = np.random.default_rng(6).standard_normal((2, n, n)).astype(np.float32)
+    dy = np.random.default_rng(6).standard_normal((8, n, n)).astype(np.float32)
     net = CaslNet(n)
     net.set_params(p)
     net.forward(x)
@@ -74,7 +74,7 @@ def test_adam_step(gpu_lib):
     net = CaslNet(n)
     net.set_params(p)
     net.forward(inputs(n, 8))
-    g = net.backward(np.random.default_rng(9).standard_normal((2, n, n)).astype(np.float32))
+    g = net.backward(np.random.default_rng(9).standard_normal((8, n, n)).astype(np.float32))
     net.adam(1e-3)
     p1, _, _ = net.params()
     moved = p1 - p
@@ -158,6 +158,29 @@ def test_features_are_the_inversion_fields(oracle_mod, gpu_lib):
     net.close(); g.close(); _.close()
 
 
+def test_node_correction_is_the_fine_grid_interpolation(oracle_mod, gpu_lib):
+    """The correction added to each node's velocity is us times the bilinear
+    interpolation, on the grid twice as fine, of the network's 8 output
+    channels (restated in numpy by oracle/closure_oracle.node_correction)."""
+    from hydra_b200.casl import CaslNet
+    n = 128
+    g, _ = _pair(oracle_mod, n, 2)
+    p = co.init_params(7)
+    p[-8:] = np.linspace(-0.2, 0.2, 8)
+    net = CaslNet(n)
+    net.set_params(p, qscale=5.0, uscale=2.0)
+    g.inversion()
+    du, dv = g.closure_correction(net)
+    y = net.forward(g.closure_features(net))
+    c = g.contours()
+    ru, rv = co.node_correction(y, c["xq"], c["yq"], 2.0, n)
+    scale = max(np.abs(ru).max(), np.abs(rv).max())
+    assert scale > 1e-3
+    assert np.abs(du - ru).max() <= 1e-9 * scale
+    assert np.abs(dv - rv).max() <= 1e-9 * scale
+    net.close(); g.close(); _.close()
+
+
 def test_zero_network_leaves_the_step_unchanged(oracle_mod, gpu_lib):
     """A network whose output is zero corrects nothing: the step is bit-for-bit
     the plain one."""
@@ -175,8 +198,9 @@ def test_zero_network_leaves_the_step_unchanged(oracle_mod, gpu_lib):
 
 
 def test_constant_correction_shifts_the_nodes(oracle_mod, gpu_lib):
-    """Output bias (b0, b1) and zero weights: velint reads u + us*b0,
-    v + us*b1 at every stage.  With qjump = 0 and qs = qd = 0 the flow
+    """Output bias b0 on the four u channels, b1 on the four v channels, zero
+    weights: the correction is us*(b0, b1) everywhere on the fine grid, so
+    every node moves with velint's velocity plus us*(b0, b1) at every stage.  With qjump = 0 and qs = qd = 0 the flow
     itself is zero, so the plain step leaves the nodes in place and one RK4
     step of the corrected one moves every node by exactly dt*us*b."""
     from hydra_b200.casl import CaslNet
@@ -189,7 +213,7 @@ def test_constant_correction_shifts_the_nodes(oracle_mod, gpu_lib):
         for f in ("qs", "qd"):
             g.set_field(f, np.zeros((n, n)))
     p = np.zeros(co.param_count(), np.float32)
-    p[-2:] = [0.5, -0.25]
+    p[-8:] = [0.5] * 4 + [-0.25] * 4
     net = CaslNet(n)
     net.set_params(p, 4.0, 2.0)
     b.closure_attach(net)
