@@ -20,19 +20,11 @@ import numpy as np
 
 from .casl import NET_OUT, CaslNet
 
-# padded (CIN, COUT) of each convolution the kernels run, by kernel name
-# pattern: forward layers, input gradients (CIN = the layer's COUT), weight
-# gradients
-_SHAPES = {
-    "k_conv5<16, 32, 4, 0>": [(16, 32)],            # layer 1 forward
-    "k_conv5<32, 32, 4, 0>": [(32, 32), (32, 32)],  # layers 2, 3 forward
-    "k_conv5<32, 16, 4, 1>": [(32, 16)],            # layer 4 forward
-    "k_conv5<16, 32, 4, 2>": [(16, 32)],            # layer 4 input gradient
-    "k_conv5<32, 32, 4, 2>": [(32, 32), (32, 32)],  # layers 3, 2 input gradients
-    "k_conv5_wgrad<32, 16, 8>": [(32, 16)],
-    "k_conv5_wgrad<32, 32, 8>": [(32, 32), (32, 32)],
-    "k_conv5_wgrad<16, 32, 8>": [(16, 32)],
-}
+# padded channel counts of each convolution, from the kernel's name: the
+# forward and input-gradient kernels k_conv5<CIN, COUT, R, MODE> and the
+# weight gradients k_conv5_wgrad<CIN, COUT, R> (CIN the layer input, COUT
+# its output; an input gradient runs with the layer's COUT as its CIN)
+_NAME = re.compile(r"(k_conv5(?:_wgrad)?)<(\d+), (\d+), \d+(?:, (\d+))?>")
 
 
 def peak_tflops():
@@ -70,13 +62,13 @@ def run(n=512, reps=20, device=0):
         if not m:
             continue
         name, launches, total_ms, mean_us = m.group(1), int(m.group(2)), float(m.group(3)), float(m.group(4))
-        key = name if name in _SHAPES else None
-        if key is None:
+        k = _NAME.match(name)
+        if not k:
             continue
-        shapes = _SHAPES[key]
-        flops = sum(2.0 * n * n * 25 * ci * co for ci, co in shapes) / len(shapes)  # per launch
+        ci, co = int(k.group(2)), int(k.group(3))
+        flops = 2.0 * n * n * 25 * ci * co  # per launch
         tf = flops / (mean_us * 1e-6) / 1e12
-        rows.append(dict(kernel=key, launches=launches, mean_us=mean_us,
+        rows.append(dict(kernel=name, launches=launches, mean_us=mean_us,
                          tflops=tf, frac=tf / peak))
     return dict(n=n, reps=reps, peak_tflops=peak, peak_source=kind, kernels=rows)
 

@@ -466,11 +466,12 @@ constexpr int NL = 4;
 // interpolation), since the error is mostly the interpolation's own.
 constexpr int SUB = 2;
 constexpr int NOUT = 2 * SUB * SUB;
-// real channel counts 3 -> 32 -> 32 -> 32 -> NOUT, padded to the MMA's multiples of 16
-__host__ __device__ constexpr int cin_r(int l) { return l == 0 ? 3 : 32; }
-__host__ __device__ constexpr int cout_r(int l) { return l == NL - 1 ? NOUT : 32; }
-__host__ __device__ constexpr int cin_p(int l) { return l == 0 ? 16 : 32; }
-__host__ __device__ constexpr int cout_p(int l) { return l == NL - 1 ? 16 : 32; }
+constexpr int HID = 16;  // hidden channels
+// real channel counts 3 -> HID -> HID -> HID -> NOUT, padded to the MMA's multiples of 16
+__host__ __device__ constexpr int cin_r(int l) { return l == 0 ? 3 : HID; }
+__host__ __device__ constexpr int cout_r(int l) { return l == NL - 1 ? NOUT : HID; }
+__host__ __device__ constexpr int cin_p(int l) { return l == 0 ? 16 : HID; }
+__host__ __device__ constexpr int cout_p(int l) { return l == NL - 1 ? 16 : HID; }
 
 struct ParamMap {
   int offw[NL], offb[NL], total;
@@ -712,16 +713,16 @@ int forward(casl_net *N, cudaStream_t st, bool train, int *err) {
   a.err = err;
   a.in = N->x0; a.wimg = N->L[0].wf; a.bias = N->L[0].bias; a.out = N->a[0];
   a.zout = train ? N->z[0] : nullptr;
-  if ((rc = launch_conv<16, 32, FWD_GELU>(a, st))) return rc;
+  if ((rc = launch_conv<16, HID, FWD_GELU>(a, st))) return rc;
   for (int l = 1; l < 3; l++) {
     a.in = N->a[l - 1]; a.wimg = N->L[l].wf; a.bias = N->L[l].bias; a.out = N->a[l];
     a.zout = train ? N->z[l] : nullptr;
-    if ((rc = launch_conv<32, 32, FWD_GELU>(a, st))) return rc;
+    if ((rc = launch_conv<HID, HID, FWD_GELU>(a, st))) return rc;
   }
   ConvArgs b{};
   b.n = n; b.err = err;
   b.in = N->a[2]; b.wimg = N->L[3].wf; b.bias = N->L[3].bias; b.fout = N->fout; b.cout_real = NOUT;
-  return launch_conv<32, 16, FWD_LINEAR>(b, st);
+  return launch_conv<HID, 16, FWD_LINEAR>(b, st);
 }
 
 // The backward pass after a training forward, from the packed output
@@ -737,20 +738,20 @@ int backward(casl_net *N, cudaStream_t st, int *err) {
   WgradArgs w{};
   w.n = n; w.err = err;
   w.in = N->a[2]; w.dz = N->dc; w.dw = N->L[3].dw;
-  if ((rc = launch_wgrad<32, 16>(w, st))) return rc;
+  if ((rc = launch_wgrad<HID, 16>(w, st))) return rc;
   ConvArgs a{};
   a.n = n; a.err = err;
   a.in = N->dc; a.wimg = N->L[3].wb; a.out = N->dz[2]; a.zprev = N->z[2]; a.dbias = N->L[2].db;
-  if ((rc = launch_conv<16, 32, BWD_GELU>(a, st))) return rc;
+  if ((rc = launch_conv<16, HID, BWD_GELU>(a, st))) return rc;
   for (int l = 2; l >= 1; l--) {
     w.in = N->a[l - 1]; w.dz = N->dz[l]; w.dw = N->L[l].dw;
-    if ((rc = launch_wgrad<32, 32>(w, st))) return rc;
+    if ((rc = launch_wgrad<HID, HID>(w, st))) return rc;
     a.in = N->dz[l]; a.wimg = N->L[l].wb; a.out = N->dz[l - 1]; a.zprev = N->z[l - 1];
     a.dbias = N->L[l - 1].db;
-    if ((rc = launch_conv<32, 32, BWD_GELU>(a, st))) return rc;
+    if ((rc = launch_conv<HID, HID, BWD_GELU>(a, st))) return rc;
   }
   w.in = N->x0; w.dz = N->dz[0]; w.dw = N->L[0].dw;
-  return launch_wgrad<16, 32>(w, st);
+  return launch_wgrad<16, HID>(w, st);
 }
 
 static Params params_of(casl_net *N) {
@@ -1147,9 +1148,9 @@ int casl_net_create(int n, int device, casl_net **out) {
   A((void **)&N->x0, act_elems(n, 16) * 2);
   A((void **)&N->dc, act_elems(n, 16) * 2);
   for (int i = 0; i < 3; i++) {
-    A((void **)&N->a[i], act_elems(n, 32) * 2);
-    A((void **)&N->z[i], act_elems(n, 32) * 2);
-    A((void **)&N->dz[i], act_elems(n, 32) * 2);
+    A((void **)&N->a[i], act_elems(n, HID) * 2);
+    A((void **)&N->z[i], act_elems(n, HID) * 2);
+    A((void **)&N->dz[i], act_elems(n, HID) * 2);
   }
   A((void **)&N->fout, (size_t)NOUT * n * n * 4);
   A((void **)&N->stage, (size_t)(NOUT > 3 ? NOUT : 3) * n * n * 4);

@@ -27,7 +27,8 @@ from .synthetic import random_pv
 
 # the last layer's 8 channels: the u and v correction at the 2 x 2 points of
 # the twice-finer grid inside each coarse cell
-LAYERS = [(3, 32), (32, 32), (32, 32), (32, 8)]
+HID = 16  # hidden channels (the library's HID)
+LAYERS = [(3, HID), (HID, HID), (HID, HID), (HID, 8)]
 
 
 def init_params(seed: int) -> np.ndarray:

@@ -28,7 +28,8 @@ from __future__ import annotations
 import numpy as np
 from scipy.special import erf
 
-LAYERS = [(3, 32), (32, 32), (32, 32), (32, 8)]
+HID = 16  # hidden channels
+LAYERS = [(3, HID), (HID, HID), (HID, HID), (HID, 8)]
 SUB = 2  # the output grid is SUB times as fine as the input
 
 
