@@ -18,7 +18,7 @@ import re
 
 import numpy as np
 
-from .casl import NET_OUT, CaslNet
+from .casl import NET_IN, NET_OUT, CaslNet
 
 # padded channel counts of each convolution, from the kernel's name: the
 # forward and input-gradient kernels k_conv5<CIN, COUT, R, MODE> and the
@@ -41,7 +41,7 @@ def run(n=512, reps=20, device=0):
     rng = np.random.default_rng(0)
     p = (rng.standard_normal(net.count) * 0.05).astype(np.float32)
     net.set_params(p)
-    x = rng.standard_normal((3, n, n)).astype(np.float32)
+    x = rng.standard_normal((NET_IN, n, n)).astype(np.float32)
     dy = rng.standard_normal((NET_OUT, n, n)).astype(np.float32)
     net.forward(x)
     net.backward(dy)

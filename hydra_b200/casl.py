@@ -55,6 +55,9 @@ _dp = C.POINTER(C.c_double)
 # grid twice as fine as n, channel comp*4 + a*2 + b = component comp (u, v)
 # at the fine point (2 ix + a, 2 iy + b).
 NET_OUT = 8
+# Its input channels (CASL_NET_IN): coarse contour PV, u, v, and the nine
+# sub-cell deviations of the fine contour levels.
+NET_IN = 12
 _ip = C.POINTER(C.c_int)
 _fp = C.POINTER(C.c_float)
 
@@ -464,7 +467,7 @@ class CaslGPU:
         return du, dv
 
     def closure_features(self, net):
-        x = np.empty((3, self.nx, self.ny), np.float32)
+        x = np.empty((NET_IN, self.nx, self.ny), np.float32)
         self._check(self.lib.casl_closure_features(self.h, net.h, x.ctypes.data_as(_fp)),
                     "casl_closure_features")
         return x
@@ -529,7 +532,7 @@ class CaslNet:
         return p, qs.value, us.value
 
     def forward(self, x):
-        x = _f32(x, (3, self.n, self.n))
+        x = _f32(x, (NET_IN, self.n, self.n))
         y = np.empty((NET_OUT, self.n, self.n), np.float32)
         self._check(self.lib.casl_net_forward(self.h, _fptr(x), _fptr(y)), "casl_net_forward")
         return y

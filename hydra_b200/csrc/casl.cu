@@ -797,12 +797,42 @@ __global__ void k_c2g_coarsen(const int *__restrict__ L, int *__restrict__ C,
 // Requires n % RPS == 0.
 #define C2G_CW 7
 #define C2G_FC (4 * C2G_CW + 3)
+
+// The learned closure's sub-cell input: the fine levels at the 3 x 3 points
+// (4cx + 2a - 2, 4cy + 2b - 2), a, b = 0..2, of every coarse cell (cx, cy),
+// channel-major, F[3a + b][cx][cy].  Warp w of a CTA holds fine column
+// 4 cx0 - 3 + w: a column 4k+1 is the a = 0 sample of coarse column k and
+// the a = 2 sample of column k - 1, a column 4k+3 the a = 1 sample of k.
+// La, Lb, Lc are the levels at fine rows 4cy - 2, 4cy, 4cy + 2.
+__device__ __forceinline__ void c2g_feature(int *__restrict__ F, int n, int cx0, int w, int cy,
+                                            int La, int Lb, int Lc) {
+  const int r = w & 3, k = w >> 2;
+  if (r != 1 && r != 3) return;
+  const long long nn = (long long)n * n;
+  int cxl[2], aa[2], m = 0;
+  if (r == 3) {
+    cxl[0] = k; aa[0] = 1; m = 1;
+  } else {
+    if (k < C2G_CW) { cxl[m] = k; aa[m++] = 0; }
+    if (k >= 1) { cxl[m] = k - 1; aa[m++] = 2; }
+  }
+  for (int q = 0; q < m; q++) {
+    const int cx = cx0 + cxl[q];
+    if (cx >= n) continue;
+    int *f = F + (long long)(3 * aa[q]) * nn + (long long)cx * n + cy;
+    f[0] = La;
+    f[nn] = Lb;
+    f[2 * nn] = Lc;
+  }
+}
+
 template <int U>
 __global__ void __launch_bounds__(1024) k_c2g_packed_sum(const unsigned long long *__restrict__ JW,
                                                          const int *__restrict__ ljx,
                                                          int *__restrict__ C,
                                                          unsigned long long *__restrict__ csum,
-                                                         int n, int nf, C2GMembers mb) {
+                                                         int n, int nf, C2GMembers mb,
+                                                         int *__restrict__ F) {
   CASL_PDL_ENTRY();
   {  // ensemble member blockIdx.y
     const long long m = blockIdx.y;
@@ -878,6 +908,10 @@ __global__ void __launch_bounds__(1024) k_c2g_packed_sum(const unsigned long lon
         const int L3 = L2 + c0, L4 = L3 + c1, L5 = L4 + c2, L6 = L5 + c3;
         G[u * 32 + lane][warp] =
             w7[0] * L0 + w7[1] * L1 + w7[2] * L2 + w7[3] * L3 + w7[4] * L4 + w7[5] * L5 + w7[6] * L6;
+        if (F) {
+          const int cy = s * RPS + u * 32 + lane;
+          if (cy > 0) c2g_feature(F, n, cx0, warp, cy, L1, L3, L5);
+        }
         if (s == 0 && u == 0 && lane == 0) {
           f0 = c0; f1 = c1; f2 = c2; f3 = c3;
         }
@@ -911,6 +945,7 @@ __global__ void __launch_bounds__(1024) k_c2g_packed_sum(const unsigned long lon
     const int L3 = lb + f0, L4 = L3 + f1, L5 = L4 + f2, L6 = L5 + f3;
     G0[warp] = w7[0] * L0 + w7[1] * L1 + w7[2] * L2 + w7[3] * L3 + w7[4] * L4 + w7[5] * L5 +
                w7[6] * L6;
+    if (F) c2g_feature(F, n, cx0, warp, 0, L1, L3, L5);
   }
   __syncthreads();
   if (threadIdx.x < C2G_CW) {
@@ -986,14 +1021,16 @@ int con2grid_dev(casl_handle *h, bool want_levels) {
     CASL_K(k_c2g_scatter<true>, grid_for(h->nptq > 0 ? h->nptq : 1), 256, 0, h->stream)(
         h->xq, h->yq, h->nextq, h->scal, nullptr, JW, h->ljx, c, err, csum, mb);
     const dim3 nblk((n + C2G_CW - 1) / C2G_CW, h->M);
+    // the learned closure's sub-cell levels, while it is attached (one simulation)
+    int *feat = h->M == 1 ? h->c2g_feat : nullptr;
     if (U == 8)
-      CASL_K(k_c2g_packed_sum<8>, nblk, 1024, 0, h->stream)(JW, h->ljx, h->coarseC, csum, n, c.nxf, mb);
+      CASL_K(k_c2g_packed_sum<8>, nblk, 1024, 0, h->stream)(JW, h->ljx, h->coarseC, csum, n, c.nxf, mb, feat);
     else if (U == 4)
-      CASL_K(k_c2g_packed_sum<4>, nblk, 1024, 0, h->stream)(JW, h->ljx, h->coarseC, csum, n, c.nxf, mb);
+      CASL_K(k_c2g_packed_sum<4>, nblk, 1024, 0, h->stream)(JW, h->ljx, h->coarseC, csum, n, c.nxf, mb, feat);
     else if (U == 2)
-      CASL_K(k_c2g_packed_sum<2>, nblk, 1024, 0, h->stream)(JW, h->ljx, h->coarseC, csum, n, c.nxf, mb);
+      CASL_K(k_c2g_packed_sum<2>, nblk, 1024, 0, h->stream)(JW, h->ljx, h->coarseC, csum, n, c.nxf, mb, feat);
     else
-      CASL_K(k_c2g_packed_sum<1>, nblk, 1024, 0, h->stream)(JW, h->ljx, h->coarseC, csum, n, c.nxf, mb);
+      CASL_K(k_c2g_packed_sum<1>, nblk, 1024, 0, h->stream)(JW, h->ljx, h->coarseC, csum, n, c.nxf, mb, feat);
     return check_launch(h);
   }
   // the fine-grid levels themselves are wanted: crossings onto the fine

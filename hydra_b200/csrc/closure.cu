@@ -466,12 +466,21 @@ constexpr int NL = 4;
 // interpolation), since the error is mostly the interpolation's own.
 constexpr int SUB = 2;
 constexpr int NOUT = 2 * SUB * SUB;
+constexpr int OUTP = NOUT <= 16 ? 16 : 32;  // the output channels the MMAs run
+static_assert(NOUT <= 32, "output channels");
 constexpr int HID = 16;  // hidden channels
-// real channel counts 3 -> HID -> HID -> HID -> NOUT, padded to the MMA's multiples of 16
-__host__ __device__ constexpr int cin_r(int l) { return l == 0 ? 3 : HID; }
+// Input channels: the coarse contour PV, u and v of the inversion, and the
+// deviations of the fine (4n) contour levels at the 3 x 3 points (4cx +
+// 2a - 2, 4cy + 2b - 2) of each coarse cell from the cell's weighted mean
+// (the sub-cell shape of the contours that the coarse PV smooths away).
+constexpr int NSUBF = 9;
+constexpr int NIN = 3 + NSUBF;
+static_assert(NIN <= 16, "input channels");
+// real channel counts NIN -> HID -> HID -> HID -> NOUT, padded to the MMA's multiples of 16
+__host__ __device__ constexpr int cin_r(int l) { return l == 0 ? NIN : HID; }
 __host__ __device__ constexpr int cout_r(int l) { return l == NL - 1 ? NOUT : HID; }
 __host__ __device__ constexpr int cin_p(int l) { return l == 0 ? 16 : HID; }
-__host__ __device__ constexpr int cout_p(int l) { return l == NL - 1 ? 16 : HID; }
+__host__ __device__ constexpr int cout_p(int l) { return l == NL - 1 ? OUTP : HID; }
 
 struct ParamMap {
   int offw[NL], offb[NL], total;
@@ -601,26 +610,27 @@ __global__ void k_pack_input(const float *__restrict__ x, bf16 *__restrict__ x0,
 
 // FP32 [cout][n][n] output gradient -> padded 16-channel planes, and its sum
 // over pixels (the last layer's bias gradient).
+template <int C>
 __global__ void k_pack_grad(const float *__restrict__ g, bf16 *__restrict__ dz, int n, int cout,
                             float *__restrict__ db) {
   CASL_PDL_ENTRY();
   const long long nn = (long long)n * n;
-  float sum[16];
+  float sum[C];
 #pragma unroll
-  for (int c = 0; c < 16; c++) sum[c] = 0.0f;
+  for (int c = 0; c < C; c++) sum[c] = 0.0f;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nn;
        t += (long long)gridDim.x * blockDim.x) {
     const int row = (int)(t / n), col = (int)(t % n);
-    float v[16];
+    float v[C];
 #pragma unroll
-    for (int c = 0; c < 16; c++) {
+    for (int c = 0; c < C; c++) {
       v[c] = c < cout ? __bfloat162float(__float2bfloat16_rn(g[c * nn + t])) : 0.0f;
       sum[c] += v[c];
     }
-    store_px<16>(dz, n, row, col, v);
+    store_px<C>(dz, n, row, col, v);
   }
 #pragma unroll
-  for (int c = 0; c < 16; c++) {
+  for (int c = 0; c < C; c++) {
     float x = sum[c];
     for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
     if ((threadIdx.x & 31) == 0 && c < cout) atomicAdd(&db[c], x);
@@ -722,7 +732,7 @@ int forward(casl_net *N, cudaStream_t st, bool train, int *err) {
   ConvArgs b{};
   b.n = n; b.err = err;
   b.in = N->a[2]; b.wimg = N->L[3].wf; b.bias = N->L[3].bias; b.fout = N->fout; b.cout_real = NOUT;
-  return launch_conv<HID, 16, FWD_LINEAR>(b, st);
+  return launch_conv<HID, OUTP, FWD_LINEAR>(b, st);
 }
 
 // The backward pass after a training forward, from the packed output
@@ -738,11 +748,11 @@ int backward(casl_net *N, cudaStream_t st, int *err) {
   WgradArgs w{};
   w.n = n; w.err = err;
   w.in = N->a[2]; w.dz = N->dc; w.dw = N->L[3].dw;
-  if ((rc = launch_wgrad<HID, 16>(w, st))) return rc;
+  if ((rc = launch_wgrad<HID, OUTP>(w, st))) return rc;
   ConvArgs a{};
   a.n = n; a.err = err;
   a.in = N->dc; a.wimg = N->L[3].wb; a.out = N->dz[2]; a.zprev = N->z[2]; a.dbias = N->L[2].db;
-  if ((rc = launch_conv<16, HID, BWD_GELU>(a, st))) return rc;
+  if ((rc = launch_conv<OUTP, HID, BWD_GELU>(a, st))) return rc;
   for (int l = 2; l >= 1; l--) {
     w.in = N->a[l - 1]; w.dz = N->dz[l]; w.dw = N->L[l].dw;
     if ((rc = launch_wgrad<HID, HID>(w, st))) return rc;
@@ -808,6 +818,7 @@ struct ClosureState {
   double *du, *dv;          // the correction at the nodes inside a step (capacity cap)
   long long cap;
   float *dcf;               // [NOUT][n][n] output gradient of the node loss
+  int *feat;                // [NSUBF][n][n] sub-cell levels, written by con2grid
   double *acc;              // [4] sums of the node errors
 };
 
@@ -815,11 +826,15 @@ namespace net {
 
 // The network's input from the inversion of a stage: the contour PV on the
 // coarse grid (the integer cells of con2grid with its mean removed, as the
-// transform's load forms it), u and v, divided by the scales.
+// transform's load forms it), u and v, and the sub-cell levels F that the
+// same con2grid wrote, as qjump (L - C/256): the fine level's deviation from
+// the cell's weighted mean (the 7 x 7 weights sum to 256); all divided by
+// the scales.
 template <class T>
-__global__ void k_features(const int *__restrict__ C, const Scalars *__restrict__ s,
-                           const T *__restrict__ uu, const T *__restrict__ vv,
-                           float iq, float iu, bf16 *__restrict__ x0, int n, int contex) {
+__global__ void k_features(const int *__restrict__ C, const int *__restrict__ F,
+                           const Scalars *__restrict__ s, const T *__restrict__ uu,
+                           const T *__restrict__ vv, float iq, float iu, bf16 *__restrict__ x0,
+                           int n, int contex) {
   CASL_PDL_ENTRY();
   const long long nn = (long long)n * n;
   const double inv = 1.0 / (256.0 * (double)n * (double)n);
@@ -832,8 +847,12 @@ __global__ void k_features(const int *__restrict__ C, const Scalars *__restrict_
     v[0] = (float)q * iq;
     v[1] = (float)uu[t] * iu;
     v[2] = (float)vv[t] * iu;
+    const double cm = contex ? (double)C[t] * (1.0 / 256.0) : 0.0;
 #pragma unroll
-    for (int c = 3; c < 16; c++) v[c] = 0.0f;
+    for (int k = 0; k < NSUBF; k++)
+      v[3 + k] = contex && F ? (float)(qj * ((double)F[k * nn + t] - cm)) * iq : 0.0f;
+#pragma unroll
+    for (int c = NIN; c < 16; c++) v[c] = 0.0f;
     store_px<16>(x0, n, (int)(t / n), (int)(t % n), v);
   }
 }
@@ -958,24 +977,30 @@ static ClosureState *cs_get(casl_handle *h, int *rc) {
     return nullptr;
   }
   const size_t nn = (size_t)h->n * h->n;
-  bool ok = cudaMalloc(&cs->dcf, NOUT * nn * 4) == cudaSuccess && cudaMalloc(&cs->acc, 64) == cudaSuccess;
+  bool ok = cudaMalloc(&cs->dcf, NOUT * nn * 4) == cudaSuccess && cudaMalloc(&cs->acc, 64) == cudaSuccess &&
+            cudaMalloc(&cs->feat, NSUBF * nn * 4) == cudaSuccess &&
+            cudaMemset(cs->feat, 0, NSUBF * nn * 4) == cudaSuccess;
   if (!ok) {
-    cudaFree(cs->dcf); cudaFree(cs->acc);
+    cudaFree(cs->dcf); cudaFree(cs->acc); cudaFree(cs->feat);
     free(cs);
     *rc = CASL_ENOMEM;
     return nullptr;
   }
   h->closure = cs;
+  // con2grid writes the network's sub-cell input from now on
+  if (h->M == 1) h->c2g_feat = cs->feat;
   return cs;
 }
 
 void closure_release(casl_handle *h) {
   ClosureState *cs = h->closure;
   if (!cs) return;
-  void *ps[] = {cs->dcf, cs->acc, cs->uJ, cs->vJ, cs->uP, cs->vP, cs->uC, cs->vC, cs->du, cs->dv};
+  void *ps[] = {cs->dcf, cs->acc, cs->uJ, cs->vJ, cs->uP, cs->vP, cs->uC, cs->vC, cs->du, cs->dv,
+                cs->feat};
   for (void *p : ps) cudaFree(p);
   free(cs);
   h->closure = nullptr;
+  h->c2g_feat = nullptr;
 }
 
 static inline int gsz(long long work) {
@@ -990,9 +1015,9 @@ template <class T>
 static int net_run_t(casl_handle *h, casl_net *N, const T *uu, const T *vv, bool train) {
   const long long nn = (long long)h->n * h->n;
   cudaStream_t st = h->stream;
-  CASL_K(net::k_features<T>, gsz(nn), 256, 0, st)(h->coarseC, h->scal, uu, vv, 1.0f / N->qscale,
-                                                   1.0f / N->uscale, N->x0, h->n,
-                                                   h->nptq > 0 ? 1 : 0);
+  CASL_K(net::k_features<T>, gsz(nn), 256, 0, st)(h->coarseC, h->c2g_feat, h->scal, uu, vv,
+                                                   1.0f / N->qscale, 1.0f / N->uscale, N->x0,
+                                                   h->n, h->nptq > 0 ? 1 : 0);
   return net::forward(N, st, train, &h->scal->error);
 }
 
@@ -1053,7 +1078,7 @@ static int evaluate(casl_handle *h, casl_net *N, casl_handle *hf, bool train, fl
                                                   train ? cs->dcf : nullptr, cs->acc);
   if (train) {
     if (cudaMemsetAsync(N->L[3].db, 0, cout_p(3) * 4, st) != cudaSuccess) return CASL_ECUDA;
-    CASL_K(net::k_pack_grad, 148 * 4, 256, 0, st)(cs->dcf, N->dc, h->n, NOUT, N->L[3].db);
+    CASL_K(net::k_pack_grad<OUTP>, 148 * 4, 256, 0, st)(cs->dcf, N->dc, h->n, NOUT, N->L[3].db);
     if ((rc = net::backward(N, st, &h->scal->error))) return rc;
     if ((rc = net::adam_step(N, st, lr))) return rc;
   }
@@ -1146,14 +1171,14 @@ int casl_net_create(int n, int device, casl_net **out) {
   A((void **)&N->w, P * 4); A((void **)&N->mo, P * 4); A((void **)&N->vo, P * 4);
   A((void **)&N->grad, P * 4);
   A((void **)&N->x0, act_elems(n, 16) * 2);
-  A((void **)&N->dc, act_elems(n, 16) * 2);
+  A((void **)&N->dc, act_elems(n, OUTP) * 2);
   for (int i = 0; i < 3; i++) {
     A((void **)&N->a[i], act_elems(n, HID) * 2);
     A((void **)&N->z[i], act_elems(n, HID) * 2);
     A((void **)&N->dz[i], act_elems(n, HID) * 2);
   }
   A((void **)&N->fout, (size_t)NOUT * n * n * 4);
-  A((void **)&N->stage, (size_t)(NOUT > 3 ? NOUT : 3) * n * n * 4);
+  A((void **)&N->stage, (size_t)(NOUT > NIN ? NOUT : NIN) * n * n * 4);
   A((void **)&N->err, 64);
   for (int l = 0; l < NL; l++) {
     const size_t img = 25ull * cin_p(l) * cout_p(l);
@@ -1204,9 +1229,9 @@ int casl_net_forward(casl_net *N, const float *x, float *y) {
   const int n = N->n;
   const size_t nn = (size_t)n * n;
   cudaStream_t st = N->stream;
-  if (cudaMemcpyAsync(N->stage, x, 3 * nn * 4, cudaMemcpyHostToDevice, st) != cudaSuccess)
+  if (cudaMemcpyAsync(N->stage, x, NIN * nn * 4, cudaMemcpyHostToDevice, st) != cudaSuccess)
     return CASL_ECUDA;
-  CASL_K(k_pack_input, 148 * 4, 256, 0, st)(N->stage, N->x0, n, 3);
+  CASL_K(k_pack_input, 148 * 4, 256, 0, st)(N->stage, N->x0, n, NIN);
   int rc = forward(N, st, true, N->err);
   if (rc) return rc;
   if (cudaMemcpyAsync(y, N->fout, NOUT * nn * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess)
@@ -1223,7 +1248,7 @@ int casl_net_backward(casl_net *N, const float *dy, float *grad) {
   if (cudaMemcpyAsync(N->stage, dy, NOUT * nn * 4, cudaMemcpyHostToDevice, st) != cudaSuccess)
     return CASL_ECUDA;
   if (cudaMemsetAsync(N->L[3].db, 0, cout_p(3) * 4, st) != cudaSuccess) return CASL_ECUDA;
-  CASL_K(k_pack_grad, 148 * 4, 256, 0, st)(N->stage, N->dc, n, NOUT, N->L[3].db);
+  CASL_K(k_pack_grad<OUTP>, 148 * 4, 256, 0, st)(N->stage, N->dc, n, NOUT, N->L[3].db);
   int rc = backward(N, st, N->err);
   if (rc) return rc;
   if (grad) {
@@ -1350,6 +1375,7 @@ int casl_closure_correction(casl_handle *h, casl_net *net, double *du, double *d
   const int npt = h->nptq;
   if (npt == 0) return CASL_OK;
   if ((rc = casl::cs_grow(cs, npt))) return rc;
+  if ((rc = casl::inversion_dev(h, false))) return rc;  // con2grid writes the sub-cell levels
   if ((rc = casl::net_run_t<double>(h, net, h->uu, h->vv, false))) return rc;
   cudaStream_t st = h->stream;
   CASL_K(casl::net::k_corr_nodes, casl::gsz(npt), 256, 0, st)(h->xq, h->yq, npt, net->fout,
@@ -1362,27 +1388,31 @@ int casl_closure_correction(casl_handle *h, casl_net *net, double *du, double *d
   return casl::sync_counts(h);
 }
 
-// The network input of h's latest inversion (after casl_inversion or a step),
-// (3, n, n) float32, already divided by net's scales.
+// The network input of an inversion of h's current state (run here, so that
+// con2grid writes the sub-cell levels), (NIN, n, n) float32, already divided
+// by net's scales.
 int casl_closure_features(casl_handle *h, casl_net *net, float *x) {
   if (!h || !net || !x || net->n != h->n) return CASL_EINVAL;
   cudaSetDevice(h->device);
+  int rc;
+  if (!casl::cs_get(h, &rc)) return rc;
+  if ((rc = casl::inversion_dev(h, false))) return rc;
   const long long nn = (long long)h->n * h->n;
   cudaStream_t st = h->stream;
-  CASL_K(casl::net::k_features<double>, casl::gsz(nn), 256, 0, st)(h->coarseC, h->scal, h->uu, h->vv,
-                                                      1.0f / net->qscale, 1.0f / net->uscale,
-                                                      net->x0, h->n, h->nptq > 0 ? 1 : 0);
-  // unpack channels 0..2 of the padded planes on the host
+  CASL_K(casl::net::k_features<double>, casl::gsz(nn), 256, 0, st)(
+      h->coarseC, h->c2g_feat, h->scal, h->uu, h->vv, 1.0f / net->qscale, 1.0f / net->uscale,
+      net->x0, h->n, h->nptq > 0 ? 1 : 0);
+  // unpack channels 0..NIN-1 of the padded planes on the host
   std::vector<uint16_t> buf((size_t)act_elems(h->n, 16));
   if (cudaMemcpyAsync(buf.data(), net->x0, buf.size() * 2, cudaMemcpyDeviceToHost, st) !=
       cudaSuccess)
     return CASL_ECUDA;
   if (cudaStreamSynchronize(st) != cudaSuccess) return CASL_ECUDA;
   const int n = h->n;
-  for (int c = 0; c < 3; c++)
+  for (int c = 0; c < casl::net::NIN; c++)
     for (int r = 0; r < n; r++)
       for (int q = 0; q < n; q++) {
-        const uint32_t bits = (uint32_t)buf[act_off(n, 16, r, q, 0) + c] << 16;
+        const uint32_t bits = (uint32_t)buf[act_off(n, 16, r, q, c / 8) + c % 8] << 16;
         float f;
         memcpy(&f, &bits, 4);
         x[((size_t)c * n + r) * n + q] = f;

@@ -74,6 +74,7 @@ struct casl_handle {
   cudaEvent_t *prof_ev;  // 2 * CASL_PROF_MAX events, created on first use
 
   casl::ClosureState *closure;  // learned velocity closure (nullable)
+  int *c2g_feat;                // its sub-cell input, written by con2grid when set (9 n^2)
 
   // FP32-inversion mode (casl_set_precision): the velocity and gradient
   // fields of each stage in FP32, u, v, dqd/dx, dqd/dy, dqs/dx, dqs/dy

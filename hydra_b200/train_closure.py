@@ -25,10 +25,12 @@ import numpy as np
 from .casl import CaslGPU, CaslNet
 from .synthetic import random_pv
 
-# the last layer's 8 channels: the u and v correction at the 2 x 2 points of
-# the twice-finer grid inside each coarse cell
+# the last layer's channels: the u and v correction at the points of the
+# finer grid inside each coarse cell
 HID = 16  # hidden channels (the library's HID)
-LAYERS = [(3, HID), (HID, HID), (HID, HID), (HID, 8)]
+NOUT = 8  # output channels (the library's NOUT, CASL_NET_OUT)
+NIN = 12  # input channels (the library's NIN, CASL_NET_IN)
+LAYERS = [(NIN, HID), (HID, HID), (HID, HID), (HID, NOUT)]
 
 
 def init_params(seed: int) -> np.ndarray:

@@ -337,10 +337,14 @@ void casl_net_destroy(casl_net *net);
  * divided by and its output multiplied by when it runs inside a step. */
 int casl_net_set_params(casl_net *net, const float *params, float qscale, float uscale);
 int casl_net_get_params(casl_net *net, float *params, float *qscale, float *uscale);
-/* x: (3, n, n) network input (already scaled); y: (CASL_NET_OUT, n, n)
+/* x: (CASL_NET_IN, n, n) network input (already scaled: the coarse contour
+ * PV, u and v, then qjump (L - C/256) for the fine contour levels L at the
+ * 3 x 3 points (4ix + 2a - 2, 4iy + 2b - 2) of each coarse cell, channel
+ * 3 + 3a + b, C the cell's con2grid sum); y: (CASL_NET_OUT, n, n)
  * output, the velocity correction on a grid twice as fine as n: channel
  * comp*4 + a*2 + b holds component comp (0: u, 1: v) at the fine point
  * (2 ix + a, 2 iy + b).  Keeps what casl_net_backward needs. */
+#define CASL_NET_IN 12
 #define CASL_NET_OUT 8
 int casl_net_forward(casl_net *net, const float *x, float *y);
 /* Gradient of sum(dy * y) for the last casl_net_forward with respect to the
@@ -382,12 +386,12 @@ int casl_closure_check(casl_handle *h, double *err_plain, double *err_net);
 int casl_closure_train(casl_handle *h, casl_net *net, casl_handle *judge, float lr,
                        double out[3]);
 int casl_closure_evaluate(casl_handle *h, casl_net *net, casl_handle *judge, double out[3]);
-/* The network input of h's latest inversion, (3, n, n) float32, already
- * divided by the network's scales: contour PV, u, v. */
+/* The network input of an inversion of h's current state (run by the call),
+ * (CASL_NET_IN, n, n) float32, already divided by the network's scales. */
 int casl_closure_features(casl_handle *h, casl_net *net, float *x);
 /* The network's correction at h's nodes (du, dv: host arrays of nptq
- * doubles) from h's latest inversion, as the node update inside a step adds
- * it. */
+ * doubles) from an inversion of h's current state, as the node update inside
+ * a step adds it. */
 int casl_closure_correction(casl_handle *h, casl_net *net, double *du, double *dv);
 
 /* ---- benchmarking hooks (no counterpart in the reference) ---------------- */

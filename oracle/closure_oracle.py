@@ -7,11 +7,11 @@ contours.f90:136-169, interpolates the coarse inversion bilinearly), so this
 file restates the network the library defines, not a reference algorithm:
 
 * four periodic 5x5 convolutions (cross-correlation: out[y, x] reads
-  in[y + ky - 2, x + kx - 2], indices modulo n), 3 -> 32 -> 32 -> 32 -> 8
-  channels, GELU (0.5 x (1 + erf(x / sqrt 2))) after the first three;
-* the output is the velocity correction on a grid twice as fine as n:
-  channel comp*4 + a*2 + b is component comp (u, v) at the fine point
-  (2 ix + a, 2 iy + b), interpolated bilinearly to the nodes on that grid
+  in[y + ky - 2, x + kx - 2], indices modulo n), NIN -> HID -> HID -> HID ->
+  NOUT channels, GELU (0.5 x (1 + erf(x / sqrt 2))) after the first three;
+* the output is the velocity correction on a grid SUB times as fine as n:
+  channel comp*SUB^2 + a*SUB + b is component comp (u, v) at the fine point
+  (SUB ix + a, SUB iy + b), interpolated bilinearly to the nodes on that grid
   (``node_correction``);
 * parameters in the order W1[co][ci][ky][kx], b1, ..., W4, b4 (FP32);
 * BF16 rounding (round to nearest even) wherever the GPU stores BF16: the
@@ -29,8 +29,10 @@ import numpy as np
 from scipy.special import erf
 
 HID = 16  # hidden channels
-LAYERS = [(3, HID), (HID, HID), (HID, HID), (HID, 8)]
 SUB = 2  # the output grid is SUB times as fine as the input
+NOUT = 2 * SUB * SUB  # output channels
+NIN = 12  # input channels: coarse PV, u, v, nine sub-cell level deviations
+LAYERS = [(NIN, HID), (HID, HID), (HID, HID), (HID, NOUT)]
 
 
 def param_count() -> int:
@@ -168,9 +170,10 @@ def pad_spectrum(s, nf):
 
 
 def node_correction(y, xq, yq, us, n, ell=2 * np.pi):
-    """us times the bilinear interpolation of the output y ([8][n][n]) on the
-    2n grid at the nodes (xq, yq) of the domain [-ell/2, ell/2)^2: fine point
-    (I, J) is sub-cell (I % 2, J % 2) of coarse cell (I // 2, J // 2)."""
+    """us times the bilinear interpolation of the output y ([NOUT][n][n]) on
+    the SUB*n grid at the nodes (xq, yq) of the domain [-ell/2, ell/2)^2: fine
+    point (I, J) is sub-cell (I % SUB, J % SUB) of coarse cell (I // SUB,
+    J // SUB)."""
     m = SUB * n
     h = ell / m
     fx = (np.asarray(xq) + ell / 2) / h
@@ -192,3 +195,19 @@ def node_correction(y, xq, yq, us, n, ell=2 * np.pi):
              + (1 - px) * py * at(comp, i0, j1) + px * py * at(comp, i1, j1))
         out.append(us * v)
     return out[0], out[1]
+
+
+def subcell_features(levels, C, qjump, iq):
+    """The network's sub-cell input channels 3..11 from the fine (4n) contour
+    levels ([4n][4n], rows = fine x) and the coarse con2grid sums C ([n][n]):
+    qjump (L(4cx + 2a - 2, 4cy + 2b - 2) - C/256) * iq, channel 3a + b."""
+    nf = levels.shape[0]
+    n = nf // 4
+    cx = np.arange(n)[:, None]
+    cy = np.arange(n)[None, :]
+    out = []
+    for a in range(3):
+        for b in range(3):
+            L = levels[(4 * cx + 2 * a - 2) % nf, (4 * cy + 2 * b - 2) % nf].astype(np.float64)
+            out.append(qjump * (L - C.astype(np.float64) / 256.0) * iq)
+    return np.stack(out)

@@ -11,8 +11,8 @@ def test_oracle_gradient_matches_finite_differences():
     rng = np.random.default_rng(0)
     p = co.init_params(1).astype(np.float64)
     p += 0.05 * rng.standard_normal(p.size)  # non-zero biases too
-    x = rng.standard_normal((3, n, n))
-    dy = rng.standard_normal((8, n, n))
+    x = rng.standard_normal((co.NIN, n, n))
+    dy = rng.standard_normal((co.NOUT, n, n))
     y, cache = co.forward(p, x, rounding=False)
     g = co.backward(p, cache, dy, rounding=False)
     assert g.shape == (co.param_count(),)

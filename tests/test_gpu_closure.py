@@ -18,7 +18,7 @@ pytestmark = pytest.mark.gpu
 
 def inputs(n, seed):
     rng = np.random.default_rng(seed)
-    x = rng.standard_normal((3, n, n)).astype(np.float32)
+    x = rng.standard_normal((co.NIN, n, n)).astype(np.float32)
     # smooth structure too, as the solver's fields have
     yy, xx = np.meshgrid(np.arange(n), np.arange(n))
     x[0] += np.sin(2 * np.pi * 3 * xx / n) * np.cos(2 * np.pi * 2 * yy / n)
@@ -29,7 +29,7 @@ def inputs(n, seed):
 def test_forward_matches_oracle(gpu_lib, n):
     from hydra_b200.casl import CaslNet
     p = co.init_params(3)
-    p[co.param_count() - 8:] = np.linspace(-0.3, 0.3, 8)  # output bias
+    p[co.param_count() - co.NOUT:] = np.linspace(-0.3, 0.3, co.NOUT)  # output bias
     x = inputs(n, n)
     net = CaslNet(n)
     net.set_params(p)
@@ -48,7 +48,7 @@ def test_backward_matches_oracle(gpu_lib):
     n = 128
     p = co.init_params(4)
     x = inputs(n, 5)
-    dy = np.random.default_rng(6).standard_normal((8, n, n)).astype(np.float32)
+    dy = np.random.default_rng(6).standard_normal((co.NOUT, n, n)).astype(np.float32)
     net = CaslNet(n)
     net.set_params(p)
     net.forward(x)
@@ -74,7 +74,7 @@ def test_adam_step(gpu_lib):
     net = CaslNet(n)
     net.set_params(p)
     net.forward(inputs(n, 8))
-    g = net.backward(np.random.default_rng(9).standard_normal((8, n, n)).astype(np.float32))
+    g = net.backward(np.random.default_rng(9).standard_normal((co.NOUT, n, n)).astype(np.float32))
     net.adam(1e-3)
     p1, _, _ = net.params()
     moved = p1 - p
@@ -150,23 +150,35 @@ def test_features_are_the_inversion_fields(oracle_mod, gpu_lib):
     g, _ = _pair(oracle_mod, n, 1)
     net = CaslNet(n)
     net.set_params(np.zeros(co.param_count(), np.float32), qscale=5.0, uscale=2.0)
-    g.inversion()
     x = g.closure_features(net)
-    qc = g.con2grid()
+    qc, lv = g.con2grid(levels=True)
     ref = np.stack([qc / 5.0, g.field("uu") / 2.0, g.field("vv") / 2.0])
-    assert np.abs(x - co.bf16(ref)).max() <= 1e-2 * np.abs(ref).max()
+    assert np.abs(x[:3] - co.bf16(ref)).max() <= 1e-2 * np.abs(ref).max()
+    # the sub-cell channels: fine levels against the coarse cell's 7 x 7
+    # weighted sum C of the same levels (con2grid's coarsening, weights
+    # [1,2,3,4,3,2,1]^2 centred on fine point 4cx, 4cy)
+    qj = g.contours()["qjump"]
+    nf = lv.shape[0]
+    w7 = np.array([1, 2, 3, 4, 3, 2, 1], np.int64)
+    cx = np.arange(n)
+    C = np.zeros((n, n), np.int64)
+    for a in range(7):
+        for b in range(7):
+            C += w7[a] * w7[b] * lv[np.ix_((4 * cx - 3 + a) % nf, (4 * cx - 3 + b) % nf)]
+    sub = co.subcell_features(lv, C, qj, 1.0 / 5.0)
+    assert np.abs(sub).max() > 0.0
+    assert np.abs(x[3:12] - co.bf16(sub)).max() <= 1e-2 * np.abs(sub).max()
     net.close(); g.close(); _.close()
 
 
 def test_node_correction_is_the_fine_grid_interpolation(oracle_mod, gpu_lib):
     """The correction added to each node's velocity is us times the bilinear
-    interpolation, on the grid twice as fine, of the network's 8 output
-    channels (restated in numpy by oracle/closure_oracle.node_correction)."""
+    interpolation, on the finer grid, of the network's output channels (restated in numpy by oracle/closure_oracle.node_correction)."""
     from hydra_b200.casl import CaslNet
     n = 128
     g, _ = _pair(oracle_mod, n, 2)
     p = co.init_params(7)
-    p[-8:] = np.linspace(-0.2, 0.2, 8)
+    p[-co.NOUT:] = np.linspace(-0.2, 0.2, co.NOUT)
     net = CaslNet(n)
     net.set_params(p, qscale=5.0, uscale=2.0)
     g.inversion()
@@ -198,7 +210,7 @@ def test_zero_network_leaves_the_step_unchanged(oracle_mod, gpu_lib):
 
 
 def test_constant_correction_shifts_the_nodes(oracle_mod, gpu_lib):
-    """Output bias b0 on the four u channels, b1 on the four v channels, zero
+    """Output bias b0 on the u channels, b1 on the v channels, zero
     weights: the correction is us*(b0, b1) everywhere on the fine grid, so
     every node moves with velint's velocity plus us*(b0, b1) at every stage.  With qjump = 0 and qs = qd = 0 the flow
     itself is zero, so the plain step leaves the nodes in place and one RK4
@@ -213,7 +225,7 @@ def test_constant_correction_shifts_the_nodes(oracle_mod, gpu_lib):
         for f in ("qs", "qd"):
             g.set_field(f, np.zeros((n, n)))
     p = np.zeros(co.param_count(), np.float32)
-    p[-8:] = [0.5] * 4 + [-0.25] * 4
+    p[-co.NOUT:] = [0.5] * (co.NOUT // 2) + [-0.25] * (co.NOUT // 2)
     net = CaslNet(n)
     net.set_params(p, 4.0, 2.0)
     b.closure_attach(net)
