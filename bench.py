@@ -340,18 +340,20 @@ def run_closure_leg(a, torch, device, steps=40, warmup=5, check_every=40, budget
 # ---------------------------------------------------------------------------
 # batched-ensemble leg (the batched half of the "chosen" form)
 # ---------------------------------------------------------------------------
-def run_ensemble_leg(a, torch, device, members=256, n=256, steps=20, warmup=3, singles=8):
+def run_ensemble_leg(a, torch, device, members=256, n=256, steps=20, warmup=3, singles=8,
+                     candidates=(32, 64, 128, 256)):
     """The batched ensemble configuration: `members` members of n^2 (seeds
     0.., k0 uniform in [4, 12], 20-60 levels, as ensemble_member_params
-    draws them), surgery every step, recontouring every 20 regularisations,
-    all stepped together by one handle; beside it the same members advanced
+    draws them), surgery every step, recontouring every 20 regularisations.
+    The members per handle are chosen by the autotuner
+    (hydra_b200.ensemble_tune: every candidate batch steps all members, in
+    consecutive batches, for 3 steps after 2); the chosen batch is then timed
+    over `steps` steps after `warmup`.  Beside it the same members advanced
     one handle at a time (the plain form), on the first `singles` members.
     Both timed with CUDA events on the library's stream."""
     from hydra_b200.casl import CaslEnsemble, CaslGPU
-    from hydra_b200.synthetic import ensemble_member_params, random_pv
-    params = [ensemble_member_params(m) for m in range(members)]
-    fields = [random_pv(n, k0, m) for m, (k0, _) in enumerate(params)]
-    levels = [lv for _, lv in params]
+    from hydra_b200 import ensemble_tune as et
+    fields, levels = et.members(n, members)
 
     def timed(g, k):
         st = torch.cuda.ExternalStream(g.stream_ptr(), device=device)
@@ -364,15 +366,22 @@ def run_ensemble_leg(a, torch, device, members=256, n=256, steps=20, warmup=3, s
         torch.cuda.synchronize()
         return e0.elapsed_time(e1), g.scalar("node_steps") - ns0
 
-    e = CaslEnsemble(n, members, dtmax=a.dtmax, nregmax=20, npm=80_000_000, nm=4_000_000,
-                     device=device)
-    t0 = time.perf_counter()
-    e.initialise_members(fields, levels)
-    t_init = time.perf_counter() - t0
-    e.step(warmup)
-    ms, ns = timed(e, steps)
-    sizes = [e.member_counts(m)[1] for m in range(members)]
-    e.close()
+    rates, batch = et.tune_batch(fields, levels, candidates=candidates, steps=3, warmup=2,
+                                 device=device, dtmax=a.dtmax, timer=timed)
+    npm, nm = et._capacity(fields, levels, batch)
+    ms, ns, sizes, t_init = 0.0, 0.0, [], 0.0
+    for b0 in range(0, members, batch):
+        e = CaslEnsemble(n, min(batch, members - b0), dtmax=a.dtmax, nregmax=20, npm=npm, nm=nm,
+                         device=device)
+        t0 = time.perf_counter()
+        e.initialise_members(fields[b0:b0 + batch], levels[b0:b0 + batch])
+        t_init += time.perf_counter() - t0
+        e.step(warmup)
+        x, y = timed(e, steps)
+        ms += x
+        ns += y
+        sizes += [e.member_counts(m)[1] for m in range(e.members)]
+        e.close()
     sms, sns = 0.0, 0.0
     for m in range(singles):
         g = CaslGPU(n, ncontq=levels[m], force_surgery=1, dtmax=a.dtmax, nregmax=20,
@@ -386,6 +395,8 @@ def run_ensemble_leg(a, torch, device, members=256, n=256, steps=20, warmup=3, s
     return {"config": f"batched ensemble: {members} members of {n}^2, k0 ~ U[4,12], levels ~ "
                       f"U[20,60], seeds 0..{members - 1}, surgery every step, recontour every 20 "
                       f"regularisations; {steps} steps after {warmup} (one recontouring inside)",
+            "autotune": {"members_per_handle": batch,
+                         "node_steps_per_s": {str(k): v for k, v in rates.items()}},
             "node_steps_per_s": ns / (ms * 1e-3), "ms_per_step": ms / steps,
             "nodes_min": int(min(sizes)), "nodes_max": int(max(sizes)),
             "nodes_total": int(sum(sizes)), "initialise_s": t_init,
