@@ -303,23 +303,37 @@ int casl_ensemble_members(casl_handle *h, int *members) {
 // number of PV jumps.
 int casl_ensemble_initialise(casl_handle *h, const double *q_all, const int *ncontq) {
   if (!h || !q_all) return CASL_EINVAL;
-  if (h->c.beffect) return CASL_EUNSUPPORTED;
   cudaSetDevice(h->device);
   const int M = h->M, n = h->n;
   const long long nn = (long long)n * n;
   cudaStream_t st = h->stream;
-  CASL_CUDA_TRY(cudaMemcpyAsync(h->qr, q_all, M * nn * sizeof(double), cudaMemcpyHostToDevice, st));
-  // qjump of each member from its range (contint, generic.f90:216-229)
-  for (int m = 0; m < M; m++) {
-    const double *q = q_all + m * nn;
-    double mx = q[0], mn = q[0];
-    for (long long k = 1; k < nn; k++) {
-      mx = q[k] > mx ? q[k] : mx;
-      mn = q[k] < mn ? q[k] : mn;
+  if (h->c.beffect) {
+    // PV anomaly q - beta*y of every member and qjump = beta*Ly/ncontq
+    // (caps.f90:149-163), with the same bety values one simulation subtracts
+    std::vector<double> bety(n), qa((size_t)(M * nn));
+    CASL_CUDA_TRY(cudaMemcpy(bety.data(), h->bety, n * sizeof(double), cudaMemcpyDeviceToHost));
+    for (long long k = 0; k < M * nn; k++) qa[k] = q_all[k] - bety[k % n];
+    CASL_CUDA_TRY(cudaMemcpyAsync(h->qr, qa.data(), M * nn * sizeof(double), cudaMemcpyHostToDevice, st));
+    CASL_CUDA_TRY(cudaStreamSynchronize(st));
+    for (int m = 0; m < M; m++) {
+      const int nc = ncontq ? ncontq[m] : h->p.ncontq;
+      if (nc <= 0) return CASL_EINVAL;
+      h->mqjump[m] = h->p.beta * h->p.elly / (double)nc;
     }
-    const int nc = ncontq ? ncontq[m] : h->p.ncontq;
-    if (nc <= 0) return CASL_EINVAL;
-    h->mqjump[m] = (mx - mn) / (double)nc;
+  } else {
+    CASL_CUDA_TRY(cudaMemcpyAsync(h->qr, q_all, M * nn * sizeof(double), cudaMemcpyHostToDevice, st));
+    // qjump of each member from its range (contint, generic.f90:216-229)
+    for (int m = 0; m < M; m++) {
+      const double *q = q_all + m * nn;
+      double mx = q[0], mn = q[0];
+      for (long long k = 1; k < nn; k++) {
+        mx = q[k] > mx ? q[k] : mx;
+        mn = q[k] < mn ? q[k] : mn;
+      }
+      const int nc = ncontq ? ncontq[m] : h->p.ncontq;
+      if (nc <= 0) return CASL_EINVAL;
+      h->mqjump[m] = (mx - mn) / (double)nc;
+    }
   }
   // qs = ptospc(q) for every member
   int rc = ptospc_dev(h, h->qr, h->qs, M);

@@ -304,3 +304,39 @@ def test_training_reduces_node_velocity_error(oracle_mod, gpu_lib, capsys):
               f"plain {ep:.3e}, net {en:.3e} (gain {ep / en:.2f}x)")
     assert en < ep
     net.close(); g.close(); gf.close()
+
+
+def test_closure_in_the_fp32_inversion_mode(oracle_mod, gpu_lib):
+    """With FP32 storage of the inverse transforms the closure reads the FP32
+    fields: one RK4 step moves the nodes by the same correction as in the
+    FP64 mode.  The network's inputs are BF16, and a field value near a BF16
+    rounding boundary rounds to neighbouring BF16 values (2^-8 apart,
+    relative) in the two modes, so the bar is statistical: the median node
+    within 1e-3 of the largest correction, every node within 5e-2."""
+    from hydra_b200.casl import CaslNet
+    n = 128
+    p = co.init_params(11)
+    p[-co.NOUT:] = np.linspace(-0.2, 0.2, co.NOUT)
+    net = CaslNet(n)
+    net.set_params(p, qscale=5.0, uscale=2.0)
+    moves = []
+    for prec in (0, 1):
+        a, b = _pair(oracle_mod, n, 5)
+        for g in (a, b):
+            g.set_precision(prec)
+        b.closure_attach(net)
+        a.advance()
+        b.advance()
+        ca, cb = a.contours(), b.contours()
+        assert ca["nptq"] == cb["nptq"]
+        L = 2 * np.pi
+        moves.append(np.stack([(cb["xq"] - ca["xq"] + np.pi) % L - np.pi,
+                               (cb["yq"] - ca["yq"] + np.pi) % L - np.pi]))
+        a.close(); b.close()
+    d64, d32 = moves
+    scale = np.abs(d64).max()
+    assert scale > 0.0
+    err = np.abs(d32 - d64)
+    assert np.median(err) <= 1e-3 * scale
+    assert err.max() <= 5e-2 * scale
+    net.close()
