@@ -116,6 +116,9 @@ SIGNATURES = {
     "casl_io_read_synopsis": (C.c_int, [C.c_char_p, C.c_int, _ip, _ip, _dp, _dp]),
     "casl_savecont": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int]),
     "casl_savegrid": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int]),
+    "casl_set_saves": (C.c_int, [C.c_void_p, C.c_char_p, C.c_double, C.c_double, C.c_double,
+                                 C.c_int, C.c_int]),
+    "casl_get_saves": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "casl_io_wait": (C.c_int, [C.c_void_p]),
     "casl_readcont": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int]),
     "casl_genfg": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
@@ -368,6 +371,20 @@ class CaslGPU:
     def savegrid(self, rundir, irec):
         """savegrid (evolution.f90:648-727) at the current time."""
         self._check(self.lib.casl_savegrid(self.h, os.fsencode(rundir), int(irec)), "casl_savegrid")
+
+    def set_saves(self, rundir, tgsave, tcsave, tinit=0.0, igrec=0, icrec=1):
+        """The time loop's save schedule (evolution.f90:586-600): step() writes
+        savegrid output (interpolated to each save time) every tgsave and
+        savecont output every tcsave time units from tinit; rundir None
+        turns it off."""
+        d = None if rundir is None else os.fsencode(rundir)
+        self._check(self.lib.casl_set_saves(self.h, d, float(tinit), float(tgsave), float(tcsave),
+                                            int(igrec), int(icrec)), "casl_set_saves")
+
+    def save_counters(self):
+        g, c = C.c_int(), C.c_int()
+        self._check(self.lib.casl_get_saves(self.h, C.byref(g), C.byref(c)), "casl_get_saves")
+        return g.value, c.value
 
     def io_wait(self):
         self._check(self.lib.casl_io_wait(self.h), "casl_io_wait")

@@ -2972,6 +2972,7 @@ int casl_step(casl_handle *h, int nsteps) {
         if ((rc = debug_check(h, "recontour"))) return rc;
         if ((rc = sync_counts(h))) return rc;
         if ((rc = evo_init(h))) return rc;
+        saves_recontoured(h);
         CASL_K(k_twist_zero, 1, 256, 0, h->stream)(h->scal, h->M);
         h->ireg = 0;
         if (force) {
@@ -2988,9 +2989,11 @@ int casl_step(casl_handle *h, int nsteps) {
         CASL_K(k_twist_sub, 1, 256, 0, h->stream)(h->scal, h->p.twistmax, h->M);
       }
     }
+    if ((rc = saves_before_advance(h))) return rc;
     if (h->closure && (rc = closure_step_check(h))) return rc;
     h->node_steps += (double)h->nptq;
     if ((rc = advance_dev(h))) return rc;
+    if ((rc = saves_after_advance(h))) return rc;
   }
   return sync_counts(h);
 }

@@ -34,6 +34,7 @@
 #include <string.h>
 #include <sys/stat.h>
 
+#include <cmath>
 #include <string>
 #include <thread>
 #include <vector>
@@ -163,6 +164,25 @@ static void ensure_cont_dir(const char *dir) {
 // ---------------------------------------------------------------------------
 // Asynchronous writer state kept on the handle
 // ---------------------------------------------------------------------------
+// Save schedule of the time loop (evolution.f90:586-600, 200-204): gridded
+// data every tgsave and contours every tcsave time units from tinit.  adapt
+// of step k flags a save when t_k + dt_k reaches the next save time; step
+// k+1 writes it after its inversion (and surgery), the gridded data
+// interpolated between the two steps.
+struct SaveSchedule {
+  bool on = false;
+  std::string dir;
+  double tinit = 0.0, tgsave = 0.0, tcsave = 0.0;
+  int igrec = 0, icrec = 1;       // the reference's record counters
+  double tgrid = 0.0, tcont = 0.0;
+  double tstep = 0.0;             // t at the start of the current step
+  bool snap = false;              // qspre and the energies hold this step's values
+  bool gpend = false, cpend = false;  // gsave / csave set by the previous step
+  double ekinpre = 0.0, epotpre = 0.0;
+  double *qspre = nullptr;        // spectral PV at the flagging step (n^2, device)
+  double *qqs = nullptr;          // the interpolated PV (n^2, device)
+};
+
 struct IoJob {
   std::thread th;
   int status = CASL_OK;
@@ -170,6 +190,7 @@ struct IoJob {
   // pinned staging
   void *pin = nullptr;
   size_t pin_bytes = 0;
+  SaveSchedule sv;
 };
 
 static IoJob *job_of(casl_handle *h) {
@@ -207,6 +228,8 @@ void io_release(casl_handle *h) {
   io_join(h);
   IoJob *j = (IoJob *)h->io;
   if (j->pin) cudaFreeHost(j->pin);
+  cudaFree(j->sv.qspre);
+  cudaFree(j->sv.qqs);
   delete j;
   h->io = nullptr;
 }
@@ -234,6 +257,31 @@ __global__ void k_io_f32(const double *__restrict__ a, const double *__restrict_
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nn;
        k += (long long)gridDim.x * blockDim.x)
     out[k] = (float)(bety ? a[k] + bety[k % n] : a[k]);
+}
+
+// qqs = pt*qspre + ptc*qq (evolution.f90:669), each product rounded
+__global__ void k_io_interp(const double *__restrict__ qspre, const double *__restrict__ qq,
+                            double pt, double ptc, double *__restrict__ out, long long nn) {
+  CASL_PDL_ENTRY();
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nn;
+       k += (long long)gridDim.x * blockDim.x)
+    out[k] = __dadd_rn(__dmul_rn(pt, qspre[k]), __dmul_rn(ptc, qq[k]));
+}
+
+// sum of a^2 over nn values, one block (the sum of l2norm, generic.f90:198-212)
+__global__ void __launch_bounds__(1024) k_io_sumsq(const double *__restrict__ a, long long nn,
+                                                    double *__restrict__ out) {
+  CASL_PDL_ENTRY();
+  __shared__ double sh[1024];
+  double v = 0.0;
+  for (long long k = threadIdx.x; k < nn; k += blockDim.x) v += a[k] * a[k];
+  sh[threadIdx.x] = v;
+  __syncthreads();
+  for (int o = 512; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = sh[0];
 }
 
 __global__ void k_io_i1q(const int *__restrict__ i1q, int *__restrict__ out, int nq) {
@@ -460,9 +508,75 @@ int casl_savecont(casl_handle *h, const char *dir, int icrec) {
   return CASL_OK;
 }
 
-// savegrid (evolution.f90:648-727) at the current time: ene.asc, spectra.asc,
-// norms.asc and record irec of qq.r4.  The reference interpolates to the
-// save time between two steps (pt); here the state is written at t itself.
+// savegrid's output (evolution.f90:648-727) for the spectral PV anomaly qsrc
+// (device, not one of the work fields) at time tsave with the energies
+// given: ene.asc, spectra.asc (spec1d), norms.asc (l2norm of spctop(qsrc))
+// and record irec of qq.r4 (spctop(qsrc) + beta*y as float32).  The device
+// work and copies are enqueued; a host thread writes the files.  The caller
+// has joined the previous writer.
+static int savegrid_write(casl_handle *h, const char *dir, int irec, double tsave,
+                          const double *qsrc, double ekin, double epot) {
+  const int n = h->n, kmax = h->kmax, kred = h->kmaxred;
+  const long long nn = (long long)n * n;
+  cudaStream_t st = h->stream;
+  double *dspec = h->w[3];
+  double *dl2 = h->w[3] + n + 8;
+  int rc = spec1d_dev(h, qsrc, dspec);
+  if (rc) return rc;
+  rc = spctop_dev(h, qsrc, h->w[5], h->w[0]);
+  if (rc) return rc;
+  CASL_K(k_io_sumsq, 1, 1024, 0, st)(h->w[5], nn, dl2);
+  float *q4_d = (float *)h->w[4];
+  CASL_K(k_io_f32, 1184, 256, 0, st)(h->w[5], h->c.beffect ? h->bety : nullptr, q4_d, n, nn);
+  rc = check_launch(h);
+  if (rc) return rc;
+  void *pin;
+  rc = io_stage(h, (size_t)nn * 4 + (size_t)(n + 2) * 8, &pin);
+  if (rc) return rc;
+  float *q4 = (float *)pin;
+  double *spec = (double *)(q4 + nn), *l2 = spec + n + 1;
+  CASL_CUDA_TRY(cudaMemcpyAsync(q4, q4_d, nn * 4, cudaMemcpyDeviceToHost, st));
+  CASL_CUDA_TRY(cudaMemcpyAsync(spec, dspec, (n + 1) * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CASL_CUDA_TRY(cudaMemcpyAsync(l2, dl2, sizeof(double), cudaMemcpyDeviceToHost, st));
+  cudaEvent_t ev;
+  CASL_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  CASL_CUDA_TRY(cudaEventRecord(ev, st));
+  const double dsumi = h->c.dsumi, garea = h->c.garea;
+  std::vector<double> spmf(h->spmf_h, h->spmf_h + n + 1), alk(h->alk_h, h->alk_h + n + 1);
+  IoJob *j = job_of(h);
+  std::string d(dir);
+  j->active = true;
+  j->th = std::thread([=]() mutable {
+    int s = cudaEventSynchronize(ev) == cudaSuccess ? CASL_OK : CASL_ECUDA;
+    cudaEventDestroy(ev);
+    if (!s) {
+      mkdir(d.c_str(), 0777);
+      s = casl_io_append_ene((d + "/ene.asc").c_str(), tsave, ekin, epot);
+    }
+    if (!s) {
+      // evolution.f90:685-692
+      double sum = 0.0;
+      std::vector<double> q(spec, spec + n + 1);
+      for (int k = 1; k <= kmax; k++) {
+        sum = sum + q[k];
+        q[k] = spmf[k] * q[k];
+      }
+      sum = 8.0 * sum * dsumi;
+      const double qql2 = garea * l2[0];
+      s = write_r4_record((d + "/qq.r4").c_str(), irec, n, n, (float)tsave, q4);
+      if (!s) s = casl_io_append_norms((d + "/norms.asc").c_str(), tsave, qql2);
+      if (!s)
+        s = casl_io_append_spectrum((d + "/spectra.asc").c_str(), tsave, sum, qql2, kred,
+                                    alk.data(), q.data());
+    }
+    j->status = s;
+  });
+  return CASL_OK;
+}
+
+// savegrid (evolution.f90:648-727) at the current time: the inversion, the
+// energies (evolution.f90:612-644) and savegrid_write of qq.  The schedule
+// of casl_set_saves writes the same files interpolated to each save time.
 int casl_savegrid(casl_handle *h, const char *dir, int irec) {
   if (!h || !dir || irec < 1) return CASL_EINVAL;
   if (h->M > 1) return CASL_EUNSUPPORTED;
@@ -474,59 +588,42 @@ int casl_savegrid(casl_handle *h, const char *dir, int irec) {
   rc = inversion_dev(h, false);
   if (rc) return rc;
   double diag[4];
-  rc = casl_diagnostics(h, diag);  // energy (evolution.f90:612-644) and l2norm of spctop(qq)
+  rc = casl_diagnostics(h, diag);  // energy (evolution.f90:612-644)
   if (rc) return rc;
-  const int n = h->n, kmax = h->kmax, kred = h->kmaxred;
-  const long long nn = (long long)n * n;
-  cudaStream_t st = h->stream;
-  double *dspec = h->w[3];
-  rc = spec1d_dev(h, h->qq, dspec);
-  if (rc) return rc;
-  rc = spctop_dev(h, h->qq, h->w[5], h->w[0]);
-  if (rc) return rc;
-  float *q4_d = (float *)h->w[4];
-  CASL_K(k_io_f32, 1184, 256, 0, st)(h->w[5], h->c.beffect ? h->bety : nullptr, q4_d, n, nn);
-  rc = check_launch(h);
-  if (rc) return rc;
-  void *pin;
-  rc = io_stage(h, (size_t)nn * 4 + (size_t)(n + 1) * 8, &pin);
-  if (rc) return rc;
-  float *q4 = (float *)pin;
-  double *spec = (double *)(q4 + nn);
-  CASL_CUDA_TRY(cudaMemcpyAsync(q4, q4_d, nn * 4, cudaMemcpyDeviceToHost, st));
-  CASL_CUDA_TRY(cudaMemcpyAsync(spec, dspec, (n + 1) * sizeof(double), cudaMemcpyDeviceToHost, st));
-  cudaEvent_t ev;
-  CASL_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-  CASL_CUDA_TRY(cudaEventRecord(ev, st));
-  const double ekin = diag[0], epot = diag[1], qql2 = diag[2], dsumi = h->c.dsumi;
-  std::vector<double> spmf(h->spmf_h, h->spmf_h + n + 1), alk(h->alk_h, h->alk_h + n + 1);
+  return savegrid_write(h, dir, irec, t, h->qq, diag[0], diag[1]);
+}
+
+int casl_set_saves(casl_handle *h, const char *dir, double tinit, double tgsave, double tcsave,
+                   int igrec, int icrec) {
+  if (!h) return CASL_EINVAL;
+  if (h->M > 1) return CASL_EUNSUPPORTED;  // the files of one simulation
   IoJob *j = job_of(h);
-  std::string d(dir);
-  j->active = true;
-  j->th = std::thread([=]() mutable {
-    int s = cudaEventSynchronize(ev) == cudaSuccess ? CASL_OK : CASL_ECUDA;
-    cudaEventDestroy(ev);
-    if (!s) {
-      mkdir(d.c_str(), 0777);
-      s = casl_io_append_ene((d + "/ene.asc").c_str(), t, ekin, epot);
-    }
-    if (!s) {
-      // evolution.f90:685-692
-      double sum = 0.0;
-      std::vector<double> q(spec, spec + n + 1);
-      for (int k = 1; k <= kmax; k++) {
-        sum = sum + q[k];
-        q[k] = spmf[k] * q[k];
-      }
-      sum = 8.0 * sum * dsumi;
-      s = write_r4_record((d + "/qq.r4").c_str(), irec, n, n, (float)t, q4);
-      if (!s) s = casl_io_append_norms((d + "/norms.asc").c_str(), t, qql2);
-      if (!s)
-        s = casl_io_append_spectrum((d + "/spectra.asc").c_str(), t, sum, qql2, kred, alk.data(),
-                                    q.data());
-    }
-    j->status = s;
-  });
+  SaveSchedule &s = j->sv;
+  if (!dir) {
+    s.on = false;
+    return CASL_OK;
+  }
+  if (!(tgsave > 0.0 || tcsave > 0.0) || igrec < 0 || icrec < 1) return CASL_EINVAL;
+  if (!std::isfinite(tinit) || !std::isfinite(tgsave) || !std::isfinite(tcsave)) return CASL_EINVAL;
+  const size_t bytes = (size_t)h->n * h->n * sizeof(double);
+  if (!s.qspre) CASL_CUDA_TRY(cudaMalloc(&s.qspre, bytes));
+  if (!s.qqs) CASL_CUDA_TRY(cudaMalloc(&s.qqs, bytes));
+  s.dir = dir;
+  s.tinit = tinit;
+  s.tgsave = tgsave;
+  s.tcsave = tcsave;
+  s.igrec = igrec;
+  s.icrec = icrec;
+  s.snap = s.gpend = s.cpend = false;
+  s.on = true;
+  return CASL_OK;
+}
+
+int casl_get_saves(casl_handle *h, int *igrec, int *icrec) {
+  if (!h || !igrec || !icrec) return CASL_EINVAL;
+  const IoJob *j = (const IoJob *)h->io;
+  *igrec = j ? j->sv.igrec : 0;
+  *icrec = j ? j->sv.icrec : 1;
   return CASL_OK;
 }
 
@@ -600,3 +697,84 @@ int casl_readcont(casl_handle *h, const char *dir, int iind) {
 }
 
 }  // extern "C"
+
+namespace casl {
+static SaveSchedule *schedule_of(casl_handle *h) {
+  if (!h->io) return nullptr;
+  SaveSchedule *s = &((IoJob *)h->io)->sv;
+  return s->on ? s : nullptr;
+}
+
+// Start of a step, after its surgery or recontouring: the saves flagged by
+// the previous step (advance at evolution.f90:200-204: savegrid, then
+// savecont), then this step's save times and, when this step's adapt can
+// reach the next grid save time (t + dtmax >= tgrid, dt <= dtmax), the
+// copies that the interpolation needs (evolution.f90:587-595).
+int saves_before_advance(casl_handle *h) {
+  SaveSchedule *s = schedule_of(h);
+  if (!s) return CASL_OK;
+  int rc = sync_counts(h);
+  if (rc) return rc;
+  if ((rc = get_scalars(h))) return rc;
+  const double t = h->hscal->t, dtprev = h->hscal->dt, dtmax = h->hscal->dtmax;
+  const long long nn = (long long)h->n * h->n;
+  double diag[4];
+  bool have = false;  // an inversion of this state and its energies in diag
+  if (s->gpend) {
+    if ((rc = io_join(h))) return rc;
+    if ((rc = inversion_dev(h, false))) return rc;
+    if ((rc = casl_diagnostics(h, diag))) return rc;
+    have = true;
+    // weights for time interpolation (evolution.f90:665-677)
+    const double pt = (t - s->tgrid) / dtprev, ptc = 1.0 - pt;
+    CASL_K(k_io_interp, 1184, 256, 0, h->stream)(s->qspre, h->qq, pt, ptc, s->qqs, nn);
+    const double ekin = pt * s->ekinpre + ptc * diag[0];
+    const double epot = pt * s->epotpre + ptc * diag[1];
+    if ((rc = savegrid_write(h, s->dir.c_str(), s->igrec + 1, s->tgrid, s->qqs, ekin, epot)))
+      return rc;
+    s->igrec++;
+    s->gpend = false;
+  }
+  if (s->cpend) {
+    if ((rc = casl_savecont(h, s->dir.c_str(), s->icrec))) return rc;
+    s->icrec++;
+    s->cpend = false;
+  }
+  s->tgrid = s->tinit + s->tgsave * (double)s->igrec;
+  s->tcont = s->tinit + s->tcsave * (double)s->icrec;
+  s->tstep = t;
+  s->snap = s->tgsave > 0.0 && t + dtmax >= s->tgrid;
+  if (s->snap) {
+    if (!have) {
+      if ((rc = inversion_dev(h, false))) return rc;
+      if ((rc = casl_diagnostics(h, diag))) return rc;
+    }
+    // qspre = qs after the reset, the same values as qq (evolution.f90:592)
+    CASL_CUDA_TRY(cudaMemcpyAsync(s->qspre, h->qq, nn * sizeof(double), cudaMemcpyDeviceToDevice,
+                                  h->stream));
+    s->ekinpre = diag[0];
+    s->epotpre = diag[1];
+  }
+  return CASL_OK;
+}
+
+// End of a step: adapt's flags, t + dt >= tgrid and t + dt >= tcont with the
+// step's own t and dt (evolution.f90:589, 599).
+int saves_after_advance(casl_handle *h) {
+  SaveSchedule *s = schedule_of(h);
+  if (!s) return CASL_OK;
+  int rc = get_scalars(h);
+  if (rc) return rc;
+  const double tnext = s->tstep + h->hscal->dt;
+  if (s->snap && tnext >= s->tgrid) s->gpend = true;
+  if (s->tcsave > 0.0 && tnext >= s->tcont) s->cpend = true;
+  return CASL_OK;
+}
+
+// init after a recontouring clears both flags (evolution.f90:113-116): a
+// save flagged by the step before is taken up again by the next adapt.
+void saves_recontoured(casl_handle *h) {
+  SaveSchedule *s = schedule_of(h);
+  if (s) s->gpend = s->cpend = false;
+}
+}  // namespace casl

@@ -153,6 +153,21 @@ __device__ __forceinline__ int level_index(double v, const LevInfo &li) {
   return l;
 }
 
+// level_index with the exact checks only near a level boundary: the
+// estimate x = (v + qoff)/qjump + 1/2 carries a rounding error of a few
+// units of 1e-16 relative (x is at most 65536 + nlevm), as do the qtmp
+// values, so a fractional part of x farther than 1e-6 from 0 and 1 fixes
+// the level; anything else (and a non-finite v) takes level_index's steps.
+__device__ __forceinline__ int level_index_fast(double v, const LevInfo &li) {
+  const double x = (v + li.qoff) * li.qjumpi + 0.5;
+  const double fl = floor(x), fr = x - fl;
+  int l = (int)fl;
+  if (fr > 1.0e-6 && fr < 1.0 - 1.0e-6) return l;
+  while (qtmp_of(l + 1, li) <= v) l++;
+  while (qtmp_of(l, li) > v) l--;
+  return l;
+}
+
 // One element of the ultra-fine field: (L*qjump - qavg) + bilinear residual,
 // or the bilinear residual alone; (ixf, iyf) is the point's 1-based place in
 // its coarse cell, q00..q11 the cell's corner values.  Per element the
@@ -252,8 +267,8 @@ __global__ void k_u_field(const int *__restrict__ L, const unsigned long long *_
       }
       if (qa) reinterpret_cast<double2 *>(qa + base)[k] = make_double2(out[0], out[1]);
       if (lc) {
-        const unsigned int c0 = (unsigned int)min(max(level_index(out[0], lq), 0), 65535);
-        const unsigned int c1 = (unsigned int)min(max(level_index(out[1], lq), 0), 65535);
+        const unsigned int c0 = (unsigned int)min(max(level_index_fast(out[0], lq), 0), 65535);
+        const unsigned int c1 = (unsigned int)min(max(level_index_fast(out[1], lq), 0), 65535);
         code[k] = c0 | (c1 << 16);
       }
     }
@@ -791,13 +806,39 @@ __global__ void k_ct_plain(const int *__restrict__ lab, const int *__restrict__ 
   }
 }
 
+// A crossing in walk layout: its position and contour in one 32-byte record,
+// so that the scattered store of each crossing fills one whole sector (a
+// partial sector costs a read of the sector as well); k_walk_split then
+// turns the records into the walk arrays with coalesced accesses.
+struct __align__(32) WalkRec {
+  double x, y;
+  int cid, pad[3];
+};
+__device__ __forceinline__ void put_rec(WalkRec *__restrict__ rec, long long pos, double x,
+                                        double y, int cid) {
+  double2 *p = reinterpret_cast<double2 *>(rec + pos);
+  p[0] = make_double2(x, y);
+  reinterpret_cast<int4 *>(p + 1)[0] = make_int4(cid, 0, 0, 0);
+}
+__global__ void k_walk_split(const WalkRec *__restrict__ rec, long long ncr,
+                             double *__restrict__ xw, double *__restrict__ yw,
+                             int *__restrict__ cidw) {
+  CASL_PDL_ENTRY();
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < ncr;
+       p += (long long)gridDim.x * blockDim.x) {
+    const double2 v = reinterpret_cast<const double2 *>(rec + p)[0];
+    xw[p] = v.x;
+    yw[p] = v.y;
+    cidw[p] = rec[p].cid;  // the contour of every walk position, for the first renode
+  }
+}
+
 // positions of plain-cycle crossings in walk layout
 __global__ void k_ct_gather_plain(const int *__restrict__ lab, const int *__restrict__ term,
                                   const int *__restrict__ val, const int *__restrict__ cidx,
                                   const int *__restrict__ coff, const int *__restrict__ clen,
                                   const double *__restrict__ xcr, const double *__restrict__ ycr,
-                                  long long ncr, double *__restrict__ xw, double *__restrict__ yw,
-                                  int *__restrict__ cidw) {
+                                  long long ncr, WalkRec *__restrict__ rec) {
   CASL_PDL_ENTRY();
   for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
        r += (long long)gridDim.x * blockDim.x) {
@@ -805,9 +846,7 @@ __global__ void k_ct_gather_plain(const int *__restrict__ lab, const int *__rest
     int s = lab[r];
     int c = cidx[s];
     long long pos = (long long)coff[c] + (clen[c] - val[r]);
-    xw[pos] = xcr[r];
-    yw[pos] = ycr[r];
-    cidw[pos] = c;  // the contour of every walk position, for the first renode
+    put_rec(rec, pos, xcr[r], ycr[r], c);
   }
 }
 
@@ -818,8 +857,7 @@ __global__ void k_ct_gather_chain(const int *__restrict__ term, const int *__res
                                   const int *__restrict__ chrot, const int *__restrict__ chclen,
                                   const int *__restrict__ chcont, const double *__restrict__ xcr,
                                   const double *__restrict__ ycr, long long ncr,
-                                  double *__restrict__ xw, double *__restrict__ yw,
-                                  int *__restrict__ cidw) {
+                                  WalkRec *__restrict__ rec) {
   CASL_PDL_ENTRY();
   for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < ncr;
        r += (long long)gridDim.x * blockDim.x) {
@@ -837,9 +875,7 @@ __global__ void k_ct_gather_chain(const int *__restrict__ term, const int *__res
       int rel = local >= rot ? local - rot : L - rot + local;
       pos = chpos[ch] + rel;
     }
-    xw[pos] = xcr[r];
-    yw[pos] = ycr[r];
-    cidw[pos] = chcont[ch];
+    put_rec(rec, pos, xcr[r], ycr[r], chcont[ch]);
   }
 }
 
@@ -1392,7 +1428,7 @@ int recontour_dev(casl_handle *h, const double *qq) {
     unsigned long long capb = 1;
     while (capb < (unsigned long long)(2 * ncr)) capb <<= 1;
     long long capn = std::max<long long>(ncr * 2, h->npm);
-    size_t need2 = (size_t)ncr * 600 + (size_t)capb * 16 + (size_t)capn * 32 + sort_bytes +
+    size_t need2 = (size_t)ncr * 640 + (size_t)capb * 16 + (size_t)capn * 32 + sort_bytes +
                    ((size_t)64 << 20);
     RC_TRY(ensure_scratch2(h, need2));
   }
@@ -1707,12 +1743,12 @@ int recontour_dev(casl_handle *h, const double *qq) {
   int *clen = ar2.get<int>(C), *coff = ar2.get<int>(C), *clevt = ar2.get<int>(C);
   double *xw = ar2.get<double>(ncr), *yw = ar2.get<double>(ncr);
   int *cidw = ar2.get<int>(ncr);
+  WalkRec *rec = ar2.get<WalkRec>(ncr);
   if (ar2.failed) return CASL_ENOMEM;
   // contour lengths in contour order, and their offsets
   CASL_K(k_ct_len, g, 256, 0, st)(startf, clenr, cidx, ncr, clen);
   exclusive_scan<int>(st, clen, coff, C, tmpi2, dtot + 2);
-  CASL_K(k_ct_gather_plain, g, 256, 0, st)(lab, term, val, cidx, coff, clen, xcr, ycr, ncr, xw, yw,
-                                           cidw);
+  CASL_K(k_ct_gather_plain, g, 256, 0, st)(lab, term, val, cidx, coff, clen, xcr, ycr, ncr, rec);
   int nch = (int)ch_end.size();
   if (nch > 0) {
     // absolute position of every chain; the first chain of a contour is
@@ -1744,8 +1780,9 @@ int recontour_dev(casl_handle *h, const double *qq) {
     CASL_CUDA_TRY(cudaMemsetAsync(chain_of_end, 0xff, ncr * sizeof(int), st));
     CASL_K(k_chain_of_end, gsz(nch), 256, 0, st)(d_ends, nch, chain_of_end);
     CASL_K(k_ct_gather_chain, g, 256, 0, st)(term, ep, val, chain_of_end, d_pos, d_len, d_rot, d_cl,
-                                             d_cc, xcr, ycr, ncr, xw, yw, cidw);
+                                             d_cc, xcr, ycr, ncr, rec);
   }
+  CASL_K(k_walk_split, g, 256, 0, st)(rec, ncr, xw, yw, cidw);
   CASL_K(k_lev_of_contour, g, 256, 0, st)(startf, rlev, cidx, ncr, li, h->p.nlevm, clevt);
   RC_TRY(check_launch(h));
 

@@ -130,6 +130,12 @@ int inversion_dev(casl_handle *h, bool reset);  // evolution.f90:494-520
 int evo_init(casl_handle *h);       // evolution.f90:96-131 (qc, qd, qspre)
 int spec1d_dev(casl_handle *h, const double *ss, double *dspec);
 void io_release(casl_handle *h);    // joins the output writer, frees its staging
+// Save schedule of casl_step (casl_set_saves; no-ops without one): the saves
+// flagged by the previous step and this step's copies before the advance,
+// adapt's flags after it; a recontouring clears the flags.
+int saves_before_advance(casl_handle *h);
+int saves_after_advance(casl_handle *h);
+void saves_recontoured(casl_handle *h);
 
 // Opt-in phase trace (environment variable CASL_TRACE=1): records CUDA
 // events at named points on the handle's stream and prints the device time

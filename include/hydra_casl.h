@@ -276,6 +276,21 @@ int casl_savecont(casl_handle *h, const char *dir, int icrec);
  * between steps): ene.asc, norms.asc, spectra.asc and record irec of qq.r4,
  * written by the same host thread. */
 int casl_savegrid(casl_handle *h, const char *dir, int irec);
+/* The save schedule of the time loop (evolution.f90:586-600, 200-204):
+ * casl_step writes savegrid output every tgsave and savecont output every
+ * tcsave time units from tinit into dir (a value <= 0 turns that kind off;
+ * dir NULL turns the schedule off).  The step whose t + dt reaches a grid
+ * save time keeps its PV and energies; the next step writes qq.r4 record
+ * igrec+1, ene.asc, norms.asc and spectra.asc at the save time, interpolated
+ * linearly between the two steps (evolution.f90:665-677), then (for a
+ * contour save time) savecont record icrec at its own time.  igrec and
+ * icrec are the reference's counters (a fresh run: 0 and 1; caps.f90:
+ * 227-230); each save advances its own.  A recontouring drops the flags of
+ * the step before it, as the reference's init does.  Replaces the save
+ * logic of advect/adapt; one simulation (M = 1) only. */
+int casl_set_saves(casl_handle *h, const char *dir, double tinit, double tgsave, double tcsave,
+                   int igrec, int icrec);
+int casl_get_saves(casl_handle *h, int *igrec, int *icrec);
 int casl_io_wait(casl_handle *h);
 /* readcont (common.f90:30-100) followed by init (evolution.f90:96-131):
  * contours, residual and time of save iind; qs = ptospc(con2grid + qr). */

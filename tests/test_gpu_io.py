@@ -119,3 +119,95 @@ def test_genfg_matches_oracle(oracle_mod, gpu_lib):
     rows = [(6 + i) % nu for i in range(nu)]
     assert np.array_equal(win, full[np.ix_(cols, rows)])
     g.close()
+
+
+def _ene_lines(path):
+    return [list(map(float, ln.split())) for ln in path.read_text().splitlines() if ln.strip()]
+
+
+def test_scheduled_saves_interpolate_to_the_save_times(oracle_mod, gpu_lib, tmp_path):
+    """casl_set_saves: the time loop's own save schedule (evolution.f90:
+    586-600, 200-204, 648-774).  The oracle steps beside the GPU run; the
+    reference's flags (t + dt >= tgrid at adapt), the interpolation weights
+    pt = (t - tgrid)/dt and the record counters are replayed here on its
+    states, and every written value is compared: ene.asc, norms.asc, the
+    spectra headers, qq.r4 records at the save times, and the contour saves'
+    times."""
+    from hydra_b200 import io
+    from hydra_b200.casl import CaslGPU
+
+    n, K = 64, 14
+    q0 = random_pv(n, 6.0, 7)
+    kw = dict(ncontq=20, force_surgery=1, dtmax=0.05)
+    o = oracle_mod.Oracle(n, **kw)
+    o.initialise(q0)
+    ts, dts, qqs, ens = [], [], [], []
+    # with force_surgery and no recontouring inside K < nregmax steps, a step
+    # is surgery then advance; the saves read the state after the surgery
+    for _ in range(K):
+        o.surgery()
+        o.inversion()
+        d = o.diagnostics()
+        ts.append(o.scalar("t"))
+        qqs.append(o.field("qq").copy())
+        ens.append((d["ekin"], d["epot"]))
+        o.advance()
+        dts.append(o.scalar("dt"))
+
+    # save intervals from the run's own length: about 5 grid and 3 contour saves
+    tg, tc = ts[-1] / 5.3, ts[-1] / 3.4
+    g = CaslGPU(n, **kw)
+    g.initialise(q0)
+    g.set_saves(tmp_path, tg, tc)
+    g.step(K)
+    g.io_wait()
+
+    # the reference's schedule on the oracle's states
+    grid, cont = [], []
+    igrec, icrec, gpend, cpend, tgrid = 0, 1, False, False, 0.0
+    for k in range(K):
+        if gpend:
+            pt = (ts[k] - tgrid) / dts[k - 1]
+            ptc = 1.0 - pt
+            grid.append((tgrid, pt * qqs[k - 1] + ptc * qqs[k],
+                         pt * ens[k - 1][0] + ptc * ens[k][0], pt * ens[k - 1][1] + ptc * ens[k][1],
+                         pt))
+            igrec += 1
+            gpend = False
+        if cpend:
+            cont.append(ts[k])
+            icrec += 1
+            cpend = False
+        tgrid, tcont = tg * igrec, tc * icrec
+        gpend = ts[k] + dts[k] >= tgrid
+        cpend = ts[k] + dts[k] >= tcont
+    assert len(grid) >= 4 and len(cont) >= 3
+    assert any(0.0 < gr[4] < 1.0 for gr in grid)  # saves between two steps
+    assert g.save_counters() == (len(grid), 1 + len(cont))
+
+    ene = _ene_lines(tmp_path / "ene.asc")
+    norms = _ene_lines(tmp_path / "norms.asc")
+    assert len(ene) == len(norms) == len(grid)
+    tb = o.spec_tables()
+    heads = [ln.split() for ln in (tmp_path / "spectra.asc").read_text().splitlines()
+             if len(ln.split()) == 4]
+    assert len(heads) == len(grid)
+    for r, (tgr, qs_, ek, ep, _) in enumerate(grid):
+        assert abs(ene[r][0] - tgr) <= 5e-3 and abs(norms[r][0] - tgr) <= 5e-3
+        assert abs(ene[r][1] - ek) <= 1e-10 * max(1.0, ek)
+        assert abs(ene[r][2] - ep) <= 1e-10 * max(1.0, ep)
+        phys = o.spctop(qs_)
+        l2 = (2 * np.pi / n) ** 2 * (phys ** 2).sum()
+        assert abs(norms[r][1] - l2) <= 1e-9 * l2 + 1e-9
+        spec, _ = o.spec1d(qs_, 0)
+        sumq = 8.0 * spec[1:tb["kmax"] + 1].sum() / (n * n)
+        assert abs(float(heads[r][1]) - sumq) <= 1e-9 * sumq + 1e-9
+        tr, q4 = io.read_r4(tmp_path / "qq.r4", r + 1, n, n)
+        assert abs(tr - tgr) <= 1e-6
+        assert np.abs(q4 - phys).max() <= 1e-6 * np.abs(phys).max()
+    syn = (tmp_path / "cont" / "qqsynopsis.asc").read_text().splitlines()
+    assert len(syn) == len(cont)
+    for line, t in zip(syn, cont):
+        assert abs(float(line.split()[2]) - t) <= 5e-6
+    g.close()
+    o.close()
