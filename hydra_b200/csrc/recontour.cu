@@ -222,7 +222,7 @@ __device__ __forceinline__ double ufield_at(const UField &u, double qavg, int ix
 // asked for) and/or its level code lc = level_index(v) clipped to
 // [0, 65535], with the field's extremes.  qtmp depends only on qjump and
 // nlevm, so the code is known before the level range is.
-__global__ void k_u_field(const int *__restrict__ L, const unsigned long long *__restrict__ lsum,
+__global__ void __launch_bounds__(256, 4) k_u_field(const int *__restrict__ L, const unsigned long long *__restrict__ lsum,
                           const double *__restrict__ qq, double qjump, int have_contours,
                           LevInfo lq, double *__restrict__ qa, unsigned short *__restrict__ lc,
                           double *__restrict__ part, Consts c, double bnc) {
@@ -240,42 +240,42 @@ __global__ void k_u_field(const int *__restrict__ L, const unsigned long long *_
     const double q00 = qq[(long long)(ix0 - 1) * n + iy0 - 1], q10 = qq[(long long)(ix0 - 1) * n + iy1 - 1];
     const double q01 = qq[(long long)(ix1 - 1) * n + iy0 - 1], q11 = qq[(long long)(ix1 - 1) * n + iy1 - 1];
     const long long base = (long long)(ix - 1) * nyu + 16LL * iyy;
-    int lv[16];
-    if (have_contours) {
-      const int4 *l4 = reinterpret_cast<const int4 *>(L + base);
+    // the run in two halves of 8 points (fewer live registers)
+#pragma unroll 1
+    for (int hf = 0; hf < 2; hf++) {
+      int lv[8];
+      if (have_contours) {
+        const int4 *l4 = reinterpret_cast<const int4 *>(L + base) + 2 * hf;
+        const int4 q0 = l4[0], q1 = l4[1];
+        lv[0] = q0.x; lv[1] = q0.y; lv[2] = q0.z; lv[3] = q0.w;
+        lv[4] = q1.x; lv[5] = q1.y; lv[6] = q1.z; lv[7] = q1.w;
+      } else {
+#pragma unroll
+        for (int k = 0; k < 8; k++) lv[k] = 0;
+      }
+      unsigned int code[4];
 #pragma unroll
       for (int k = 0; k < 4; k++) {
-        int4 q = l4[k];
-        lv[4 * k] = q.x; lv[4 * k + 1] = q.y; lv[4 * k + 2] = q.z; lv[4 * k + 3] = q.w;
-      }
-    } else {
+        double out[2];
 #pragma unroll
-      for (int k = 0; k < 16; k++) lv[k] = 0;
-    }
-    unsigned int code[8];
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
-      double out[2];
-#pragma unroll
-      for (int h = 0; h < 2; h++) {
-        double v = ufield_elem(lv[2 * k + h], ixf, 2 * k + h + 1, q00, q10, q01, q11, qjump,
-                               qavg, have_contours);
-        if (bnc != 0.0) v = v + bnc * (c.ymin + c.glyu * (double)(16 * iyy + 2 * k + h));
-        out[h] = v;
-        mx = fmax(mx, v);
-        mn = fmin(mn, v);
+        for (int h = 0; h < 2; h++) {
+          const int iyf = 8 * hf + 2 * k + h;  // 0-based place in the run
+          double v = ufield_elem(lv[2 * k + h], ixf, iyf + 1, q00, q10, q01, q11, qjump, qavg,
+                                 have_contours);
+          if (bnc != 0.0) v = v + bnc * (c.ymin + c.glyu * (double)(16 * iyy + iyf));
+          out[h] = v;
+          mx = fmax(mx, v);
+          mn = fmin(mn, v);
+        }
+        if (qa) reinterpret_cast<double2 *>(qa + base)[4 * hf + k] = make_double2(out[0], out[1]);
+        if (lc) {
+          const unsigned int c0 = (unsigned int)min(max(level_index_fast(out[0], lq), 0), 65535);
+          const unsigned int c1 = (unsigned int)min(max(level_index_fast(out[1], lq), 0), 65535);
+          code[k] = c0 | (c1 << 16);
+        }
       }
-      if (qa) reinterpret_cast<double2 *>(qa + base)[k] = make_double2(out[0], out[1]);
-      if (lc) {
-        const unsigned int c0 = (unsigned int)min(max(level_index_fast(out[0], lq), 0), 65535);
-        const unsigned int c1 = (unsigned int)min(max(level_index_fast(out[1], lq), 0), 65535);
-        code[k] = c0 | (c1 << 16);
-      }
-    }
-    if (lc) {
-      uint4 *o4 = reinterpret_cast<uint4 *>(lc + base);
-      o4[0] = make_uint4(code[0], code[1], code[2], code[3]);
-      o4[1] = make_uint4(code[4], code[5], code[6], code[7]);
+      if (lc)
+        reinterpret_cast<uint4 *>(lc + base)[hf] = make_uint4(code[0], code[1], code[2], code[3]);
     }
   }
   __shared__ double a[256], b[256];

@@ -113,7 +113,7 @@ __device__ __forceinline__ void rn_node(const RenodeIn &in, const RenodeScratch 
 // stencil w-2..w+3 lies inside its contour without wrapping; otherwise the
 // warp takes rn_node.
 constexpr int RN_OUT = 28;
-__global__ void k_rn_stencil(RenodeIn in, RenodeScratch s, Consts c) {
+__global__ void __launch_bounds__(256, 4) k_rn_stencil(RenodeIn in, RenodeScratch s, Consts c) {
   CASL_PDL_ENTRY();
   const double f12 = 0.5, f13 = 1.0 / 3.0, f16 = 1.0 / 6.0;
   const unsigned FULL = 0xffffffffu;
