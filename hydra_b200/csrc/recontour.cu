@@ -1063,60 +1063,77 @@ __global__ void k_sp_compact(const int *__restrict__ isspl, const int *__restric
     segend[k] = segend_c[r];
   }
 }
+// Pointer jumping over the splitters.  Each splitter's jump state is one
+// 16-byte record (next, minimum, terminal flag, last), so that a round
+// gathers two records (at next and at last) instead of four separate words.
 __global__ void k_sp_init(const int *__restrict__ nexts, const int *__restrict__ segmin, int S,
-                          int *__restrict__ nx, int *__restrict__ mn, int *__restrict__ tm,
-                          int *__restrict__ lastp) {
+                          int4 *__restrict__ J) {
   CASL_PDL_ENTRY();
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < S; k += gridDim.x * blockDim.x) {
-    int n = nexts[k];
-    nx[k] = n < 0 ? k : n;
-    mn[k] = segmin[k];
-    tm[k] = n < 0;
-    lastp[k] = n < 0 ? k : n;
+    const int n = nexts[k];
+    J[k] = make_int4(n < 0 ? k : n, segmin[k], n < 0, n < 0 ? k : n);
   }
 }
-__global__ void k_sp_jump1(const int *__restrict__ nx, const int *__restrict__ mn,
-                           const int *__restrict__ tm, const int *__restrict__ lastp, int S,
-                           int *__restrict__ nx2, int *__restrict__ mn2, int *__restrict__ tm2,
-                           int *__restrict__ lastp2) {
+__global__ void k_sp_jump1(const int4 *__restrict__ J, int S, int4 *__restrict__ J2) {
   CASL_PDL_ENTRY();
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < S; k += gridDim.x * blockDim.x) {
-    int n = nx[k];
-    mn2[k] = min(mn[k], mn[n]);
-    tm2[k] = tm[k] | tm[n];
-    nx2[k] = nx[n];
-    lastp2[k] = lastp[lastp[k]];
+    const int4 a = J[k];
+    const int4 b = J[a.x];
+    J2[k] = make_int4(b.x, min(a.y, b.y), a.z | b.z, J[a.w].w);
+  }
+}
+// the jump results as the separate arrays the later passes read
+__global__ void k_sp_unpack1(const int4 *__restrict__ J, int S, int *__restrict__ mn,
+                             int *__restrict__ tm, int *__restrict__ lastp) {
+  CASL_PDL_ENTRY();
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < S; k += gridDim.x * blockDim.x) {
+    const int4 a = J[k];
+    mn[k] = a.y;
+    tm[k] = a.z;
+    lastp[k] = a.w;
   }
 }
 // list for suffix sums: cycles are cut before the splitter holding the cycle
 // minimum; chains end at their last splitter
+// (link, suffix sum) of the suffix-sum jumps, one 16-byte record
+struct __align__(16) SlSuf {
+  long long suf;
+  int sl, pad;
+};
 __global__ void k_sp_list(const int *__restrict__ nexts, const int *__restrict__ mn,
                           const int *__restrict__ tm, const int2 *__restrict__ own,
                           const int *__restrict__ srank, const int *__restrict__ seglen, int S,
-                          int *__restrict__ sl, long long *__restrict__ suf,
-                          int *__restrict__ head) {
+                          SlSuf *__restrict__ L, int *__restrict__ head) {
   CASL_PDL_ENTRY();
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < S; k += gridDim.x * blockDim.x) {
-    int n = nexts[k];
+    int n = nexts[k], sl;
     if (tm[k]) {
-      sl[k] = n;
+      sl = n;
       head[k] = -1;
     } else {
       int h = srank[own[mn[k]].x];
       head[k] = h;
-      sl[k] = n == h ? -1 : n;
+      sl = n == h ? -1 : n;
     }
-    suf[k] = seglen[k];
+    L[k] = SlSuf{(long long)seglen[k], sl, 0};
   }
 }
-__global__ void k_sp_jump2(const int *__restrict__ sl, const long long *__restrict__ suf, int S,
-                           int *__restrict__ sl2, long long *__restrict__ suf2) {
+__global__ void k_sp_jump2(const SlSuf *__restrict__ L, int S, SlSuf *__restrict__ L2) {
   CASL_PDL_ENTRY();
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < S; k += gridDim.x * blockDim.x) {
-    int n = sl[k];
-    suf2[k] = suf[k] + (n >= 0 ? suf[n] : 0);
-    sl2[k] = n >= 0 ? sl[n] : -1;
+    const SlSuf a = L[k];
+    if (a.sl >= 0) {
+      const SlSuf b = L[a.sl];
+      L2[k] = SlSuf{a.suf + b.suf, b.sl, 0};
+    } else {
+      L2[k] = a;
+    }
   }
+}
+__global__ void k_sp_unpack2(const SlSuf *__restrict__ L, int S, long long *__restrict__ suf) {
+  CASL_PDL_ENTRY();
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < S; k += gridDim.x * blockDim.x)
+    suf[k] = L[k].suf;
 }
 __global__ void k_sp_expand(long long N, const int2 *__restrict__ own,
                             const int *__restrict__ srank, const int *__restrict__ tm,
@@ -1171,6 +1188,18 @@ __global__ void k_gather_i(const int *__restrict__ src, const int *__restrict__ 
   CASL_PDL_ENTRY();
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x)
     dst[k] = src[idx[k]];
+}
+// three arrays gathered at the same indices: dst[j*m + k] = src_j[idx[k]]
+__global__ void k_gather3_i(const int *__restrict__ s0, const int *__restrict__ s1,
+                            const int *__restrict__ s2, const int *__restrict__ idx, int m,
+                            int *__restrict__ dst) {
+  CASL_PDL_ENTRY();
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
+    const int i = idx[k];
+    dst[k] = s0[i];
+    dst[m + k] = s1[i];
+    dst[2 * m + k] = s2[i];
+  }
 }
 __global__ void k_ct_len(const int *__restrict__ startf, const int *__restrict__ clenr,
                          const int *__restrict__ cidx, long long ncr, int *__restrict__ clen) {
@@ -1545,11 +1574,11 @@ int recontour_dev(casl_handle *h, const double *qq) {
   if (S <= 0) return CASL_EINVAL;
   int *nexts = ar2.get<int>(S), *seglen = ar2.get<int>(S), *segmin = ar2.get<int>(S),
       *segend = ar2.get<int>(S);
-  int *snx = ar2.get<int>(S), *snx2 = ar2.get<int>(S), *smn = ar2.get<int>(S),
-      *smn2 = ar2.get<int>(S), *stm = ar2.get<int>(S), *stm2 = ar2.get<int>(S),
-      *slp = ar2.get<int>(S), *slp2 = ar2.get<int>(S), *ssl = ar2.get<int>(S),
-      *ssl2 = ar2.get<int>(S), *shead = ar2.get<int>(S);
-  long long *ssuf = ar2.get<long long>(S), *ssuf2 = ar2.get<long long>(S);
+  int *smn = ar2.get<int>(S), *stm = ar2.get<int>(S), *slp = ar2.get<int>(S),
+      *shead = ar2.get<int>(S);
+  long long *ssuf = ar2.get<long long>(S);
+  int4 *jA = ar2.get<int4>(S), *jB = ar2.get<int4>(S);
+  SlSuf *lA = ar2.get<SlSuf>(S), *lB = ar2.get<SlSuf>(S);
   if (ar2.failed) return CASL_ENOMEM;
   tr.point("rk_scan");
   CASL_K(k_sp_compact, g, 256, 0, st)(isspl, srank, ncr, nexts_c, seglen_c, segmin_c, segend_c,
@@ -1558,16 +1587,18 @@ int recontour_dev(casl_handle *h, const double *qq) {
   int rounds = 1;
   while ((1LL << rounds) < S) rounds++;
   rounds++;
-  CASL_K(k_sp_init, gsS, 256, 0, st)(nexts, segmin, S, snx, smn, stm, slp);
+  CASL_K(k_sp_init, gsS, 256, 0, st)(nexts, segmin, S, jA);
   for (int it = 0; it < rounds; it++) {
-    CASL_K(k_sp_jump1, gsS, 256, 0, st)(snx, smn, stm, slp, S, snx2, smn2, stm2, slp2);
-    std::swap(snx, snx2); std::swap(smn, smn2); std::swap(stm, stm2); std::swap(slp, slp2);
+    CASL_K(k_sp_jump1, gsS, 256, 0, st)(jA, S, jB);
+    std::swap(jA, jB);
   }
-  CASL_K(k_sp_list, gsS, 256, 0, st)(nexts, smn, stm, own, srank, seglen, S, ssl, ssuf, shead);
+  CASL_K(k_sp_unpack1, gsS, 256, 0, st)(jA, S, smn, stm, slp);
+  CASL_K(k_sp_list, gsS, 256, 0, st)(nexts, smn, stm, own, srank, seglen, S, lA, shead);
   for (int it = 0; it < rounds; it++) {
-    CASL_K(k_sp_jump2, gsS, 256, 0, st)(ssl, ssuf, S, ssl2, ssuf2);
-    std::swap(ssl, ssl2); std::swap(ssuf, ssuf2);
+    CASL_K(k_sp_jump2, gsS, 256, 0, st)(lA, S, lB);
+    std::swap(lA, lB);
   }
+  CASL_K(k_sp_unpack2, gsS, 256, 0, st)(lA, S, ssuf);
   tr.point("rk_jump");
   CASL_K(k_sp_expand, g, 256, 0, st)(ncr, own, srank, stm, smn, ssuf, shead, slp, segend,
                                      term, lab, val, ep);
@@ -1643,10 +1674,20 @@ int recontour_dev(casl_handle *h, const double *qq) {
     }
     // chain starts (the saddle out-crossings) and their ends, lengths, minima
     int nch = 2 * nsb;
-    std::vector<int> cstart(slot2), cend, clen, cmin;
-    RC_TRY(gather(ep, cstart, cend));
-    RC_TRY(gather(val, cstart, clen));
-    RC_TRY(gather(lab, cstart, cmin));
+    std::vector<int> cstart(slot2), cend(nch), clen(nch), cmin(nch);
+    {
+      // ends, lengths and minima at the chain starts: one gather, one copy
+      int *d_idx = ar2.get<int>(nch), *d_out = ar2.get<int>(3LL * nch);
+      if (ar2.failed) return CASL_ENOMEM;
+      std::vector<int> h_out(3 * (size_t)nch);
+      CASL_CUDA_TRY(cudaMemcpyAsync(d_idx, cstart.data(), nch * sizeof(int), cudaMemcpyHostToDevice, st));
+      CASL_K(k_gather3_i, gsz(nch), 256, 0, st)(ep, val, lab, d_idx, nch, d_out);
+      CASL_CUDA_TRY(cudaMemcpyAsync(h_out.data(), d_out, h_out.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
+      CASL_CUDA_TRY(cudaStreamSynchronize(st));
+      std::copy(h_out.begin(), h_out.begin() + nch, cend.begin());
+      std::copy(h_out.begin() + nch, h_out.begin() + 2 * nch, clen.begin());
+      std::copy(h_out.begin() + 2 * nch, h_out.end(), cmin.begin());
+    }
     std::vector<int> val_at_min;
     RC_TRY(gather(val, cmin, val_at_min));
     std::vector<std::pair<int, int>> start2ch;
