@@ -8,7 +8,10 @@ table for a block of regular steps and one for the step that recontours.
 The event pairs add a few microseconds per launch, so the step time printed
 here is above the bench's; use the tables for shares, the bench for speed.
 
-    python -m hydra_b200.bench_step --n 1024 --steps 10
+    python -m hydra_b200.bench_step --n 1024 --steps 10 [--which 2]
+
+With CASL_TRACE=1 the library also prints each recontouring's phases
+(CUDA events between its stages).
 """
 import argparse
 import time
@@ -26,6 +29,9 @@ def main(argv=None):
     ap.add_argument("--levels", type=int, default=80)
     ap.add_argument("--steps", type=int, default=10, help="regular steps in the first table")
     ap.add_argument("--nregmax", type=int, default=20)
+    ap.add_argument("--which", type=int, default=1,
+                    help="tabulate the step of this recontouring (1: step nregmax; each later "
+                         "one nregmax - 1 steps on, the step after a recontouring regularising)")
     a = ap.parse_args(argv)
     g = CaslGPU(a.n, ncontq=a.levels, force_surgery=1, dtmax=0.05, nregmax=a.nregmax,
                 npm=16_000_000, nm=1_000_000)
@@ -40,9 +46,10 @@ def main(argv=None):
     ms = 1e3 * (time.perf_counter() - t) / a.steps
     print(f"# {a.steps} regular steps, {ms:.2f} ms/step with the per-launch timer on")
     print(g.kernel_times(2), end="")
-    # up to the step before the next recontouring, then that step alone
+    # up to the step before the chosen recontouring, then that step alone
     done = warm + a.steps
-    left = a.nregmax - 1 - done
+    target = a.nregmax + (a.which - 1) * (a.nregmax - 1)
+    left = target - 1 - done
     if left >= 0:
         if left:
             g.step(left)
