@@ -109,13 +109,14 @@ def main():
     ap.add_argument("--pairs", type=int, default=20000)
     ap.add_argument("--pairs-per-run", type=int, default=250)
     ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--lr-end", type=float, default=1e-4, help="final rate of the geometric decay")
     ap.add_argument("--k0", type=float, default=12.0)
     ap.add_argument("--levels", type=int, default=80)
     ap.add_argument("--seed0", type=int, default=1000)
     ap.add_argument("--out", default=None)
     a = ap.parse_args()
-    _, _, _, hist, secs = train(a.n, a.pairs, a.pairs_per_run, a.lr, k0=a.k0, levels=a.levels,
-                                seed0=a.seed0, out=a.out)
+    _, _, _, hist, secs = train(a.n, a.pairs, a.pairs_per_run, a.lr, lr_end=a.lr_end, k0=a.k0,
+                                levels=a.levels, seed0=a.seed0, out=a.out)
     print(f"trained on {len(hist)} pairs in {secs:.1f} s")
 
 
