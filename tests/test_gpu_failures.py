@@ -18,7 +18,7 @@ from hydra_b200.synthetic import random_pv
 
 pytestmark = pytest.mark.gpu
 
-CASL_EINVAL, CASL_ECAPACITY, CASL_EDOMAIN, CASL_EIO = 1, 2, 5, 8
+CASL_EINVAL, CASL_ECAPACITY, CASL_EDOMAIN, CASL_EUNSUPPORTED, CASL_EIO = 1, 2, 5, 7, 8
 
 
 @pytest.fixture(scope="module")
@@ -126,3 +126,30 @@ def test_truncated_restart_file(gpu_lib, tmp_path):
         g2.readcont(tmp_path, 2)  # no such save
     assert e.value.code == CASL_EIO
     g2.close()
+
+
+def test_save_schedule_arguments(gpu_lib, tmp_path):
+    """casl_set_saves: both kinds off, a negative record counter or a
+    contour counter below 1 is CASL_EINVAL; an ensemble handle has no save
+    schedule (CASL_EUNSUPPORTED); a NULL directory turns the schedule off,
+    after which steps write nothing."""
+    from hydra_b200.casl import CaslEnsemble, CaslError, CaslGPU
+    n = 32
+    g = CaslGPU(n, ncontq=10, force_surgery=1, dtmax=0.05)
+    g.initialise(random_pv(n, 4.0, 1))
+    for args in [dict(tgsave=0.0, tcsave=0.0), dict(tgsave=0.1, tcsave=0.0, igrec=-1),
+                 dict(tgsave=0.1, tcsave=0.2, icrec=0), dict(tgsave=float("nan"), tcsave=0.2)]:
+        with pytest.raises(CaslError) as e:
+            g.set_saves(tmp_path, **args)
+        assert e.value.code == CASL_EINVAL, args
+    g.set_saves(tmp_path / "on", tgsave=0.01, tcsave=0.0)
+    g.set_saves(None, 0.0, 0.0)  # off again: nothing is written
+    g.step(3)
+    g.io_wait()
+    assert not (tmp_path / "on").exists()
+    assert g.save_counters() == (0, 1)
+    g.close()
+    e = CaslEnsemble(n, 2, dtmax=0.05)
+    rc = e.lib.casl_set_saves(e.h, os.fsencode(str(tmp_path)), 0.0, 0.1, 0.1, 0, 1)
+    assert rc == CASL_EUNSUPPORTED
+    e.close()
