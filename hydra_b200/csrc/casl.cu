@@ -2858,6 +2858,8 @@ int evo_init(casl_handle *h) {
   if (rc) return rc;
   CASL_K(k_evo_init, grid_for(h->M * nn), 256, 0, h->stream)(h->qd, h->qspre, h->qs, h->qc,
                                                              h->fhi, nn, h->M * nn);
+  // init also clears the save flags (evolution.f90:113-116)
+  saves_clear_flags(h);
   return check_launch(h);
 }
 }  // namespace casl
@@ -2972,7 +2974,6 @@ int casl_step(casl_handle *h, int nsteps) {
         if ((rc = debug_check(h, "recontour"))) return rc;
         if ((rc = sync_counts(h))) return rc;
         if ((rc = evo_init(h))) return rc;
-        saves_recontoured(h);
         CASL_K(k_twist_zero, 1, 256, 0, h->stream)(h->scal, h->M);
         h->ireg = 0;
         if (force) {

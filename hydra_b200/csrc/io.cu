@@ -166,9 +166,10 @@ static void ensure_cont_dir(const char *dir) {
 // ---------------------------------------------------------------------------
 // Save schedule of the time loop (evolution.f90:586-600, 200-204): gridded
 // data every tgsave and contours every tcsave time units from tinit.  adapt
-// of step k flags a save when t_k + dt_k reaches the next save time; step
-// k+1 writes it after its inversion (and surgery), the gridded data
-// interpolated between the two steps.
+// of step k flags a save when t_k + dt_k reaches the next save time (and
+// keeps its PV in the handle's qspre); step k+1 writes it after its
+// inversion (and surgery), the gridded data interpolated between the two
+// steps.
 struct SaveSchedule {
   bool on = false;
   std::string dir;
@@ -178,8 +179,7 @@ struct SaveSchedule {
   double tstep = 0.0;             // t at the start of the current step
   bool snap = false;              // qspre and the energies hold this step's values
   bool gpend = false, cpend = false;  // gsave / csave set by the previous step
-  double ekinpre = 0.0, epotpre = 0.0;
-  double *qspre = nullptr;        // spectral PV at the flagging step (n^2, device)
+  double ekinpre = 0.0, epotpre = 0.0;  // the flagging step's PV is the handle's qspre
   double *qqs = nullptr;          // the interpolated PV (n^2, device)
 };
 
@@ -228,7 +228,6 @@ void io_release(casl_handle *h) {
   io_join(h);
   IoJob *j = (IoJob *)h->io;
   if (j->pin) cudaFreeHost(j->pin);
-  cudaFree(j->sv.qspre);
   cudaFree(j->sv.qqs);
   delete j;
   h->io = nullptr;
@@ -606,7 +605,6 @@ int casl_set_saves(casl_handle *h, const char *dir, double tinit, double tgsave,
   if (!(tgsave > 0.0 || tcsave > 0.0) || igrec < 0 || icrec < 1) return CASL_EINVAL;
   if (!std::isfinite(tinit) || !std::isfinite(tgsave) || !std::isfinite(tcsave)) return CASL_EINVAL;
   const size_t bytes = (size_t)h->n * h->n * sizeof(double);
-  if (!s.qspre) CASL_CUDA_TRY(cudaMalloc(&s.qspre, bytes));
   if (!s.qqs) CASL_CUDA_TRY(cudaMalloc(&s.qqs, bytes));
   s.dir = dir;
   s.tinit = tinit;
@@ -727,7 +725,7 @@ int saves_before_advance(casl_handle *h) {
     have = true;
     // weights for time interpolation (evolution.f90:665-677)
     const double pt = (t - s->tgrid) / dtprev, ptc = 1.0 - pt;
-    CASL_K(k_io_interp, 1184, 256, 0, h->stream)(s->qspre, h->qq, pt, ptc, s->qqs, nn);
+    CASL_K(k_io_interp, 1184, 256, 0, h->stream)(h->qspre, h->qq, pt, ptc, s->qqs, nn);
     const double ekin = pt * s->ekinpre + ptc * diag[0];
     const double epot = pt * s->epotpre + ptc * diag[1];
     if ((rc = savegrid_write(h, s->dir.c_str(), s->igrec + 1, s->tgrid, s->qqs, ekin, epot)))
@@ -750,7 +748,7 @@ int saves_before_advance(casl_handle *h) {
       if ((rc = casl_diagnostics(h, diag))) return rc;
     }
     // qspre = qs after the reset, the same values as qq (evolution.f90:592)
-    CASL_CUDA_TRY(cudaMemcpyAsync(s->qspre, h->qq, nn * sizeof(double), cudaMemcpyDeviceToDevice,
+    CASL_CUDA_TRY(cudaMemcpyAsync(h->qspre, h->qq, nn * sizeof(double), cudaMemcpyDeviceToDevice,
                                   h->stream));
     s->ekinpre = diag[0];
     s->epotpre = diag[1];
@@ -771,9 +769,9 @@ int saves_after_advance(casl_handle *h) {
   return CASL_OK;
 }
 
-// init after a recontouring clears both flags (evolution.f90:113-116): a
+// init clears both flags (evolution.f90:113-116): after a recontouring, a
 // save flagged by the step before is taken up again by the next adapt.
-void saves_recontoured(casl_handle *h) {
+void saves_clear_flags(casl_handle *h) {
   SaveSchedule *s = schedule_of(h);
   if (s) s->gpend = s->cpend = false;
 }

@@ -132,10 +132,11 @@ int spec1d_dev(casl_handle *h, const double *ss, double *dspec);
 void io_release(casl_handle *h);    // joins the output writer, frees its staging
 // Save schedule of casl_step (casl_set_saves; no-ops without one): the saves
 // flagged by the previous step and this step's copies before the advance,
-// adapt's flags after it; a recontouring clears the flags.
+// adapt's flags after it; evo_init (initialise, restart, recontouring)
+// clears the flags.
 int saves_before_advance(casl_handle *h);
 int saves_after_advance(casl_handle *h);
-void saves_recontoured(casl_handle *h);
+void saves_clear_flags(casl_handle *h);
 
 // Opt-in phase trace (environment variable CASL_TRACE=1): records CUDA
 // events at named points on the handle's stream and prints the device time

@@ -285,9 +285,11 @@ int casl_savegrid(casl_handle *h, const char *dir, int irec);
  * linearly between the two steps (evolution.f90:665-677), then (for a
  * contour save time) savecont record icrec at its own time.  igrec and
  * icrec are the reference's counters (a fresh run: 0 and 1; caps.f90:
- * 227-230); each save advances its own.  A recontouring drops the flags of
- * the step before it, as the reference's init does.  Replaces the save
- * logic of advect/adapt; one simulation (M = 1) only. */
+ * 227-230); each save advances its own.  The flagging step's PV is kept in
+ * CASL_QSPRE, the reference's qspre.  Every init (casl_initialise,
+ * casl_readcont, a recontouring) drops pending flags, as the reference's
+ * init does.  Replaces the save logic of advect/adapt; one simulation
+ * (M = 1) only. */
 int casl_set_saves(casl_handle *h, const char *dir, double tinit, double tgsave, double tcsave,
                    int igrec, int icrec);
 int casl_get_saves(casl_handle *h, int *igrec, int *icrec);
